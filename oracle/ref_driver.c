@@ -1,0 +1,378 @@
+/*
+ * Driver around elegant's own hot-path routines, compiled unmodified from the
+ * reference sources (see oracle/Makefile.ref).  It is the pinned CPU oracle:
+ * the restatement in oracle/b2e_oracle.c and the CUDA path are both checked
+ * against what this file produces.
+ *
+ * What is the reference's and what is restated here:
+ *  - element physics: multipole_tracking2 (multipole.c:693), track_through_csbend
+ *    (csbend.c:665), track_through_csbendCSR (csbend.c:1899),
+ *    track_through_driftCSR (csbend.c:3176), simple_rf_cavity (simple_rfca.c:264),
+ *    exactDrift (csbend.c:3767), track_particles (matrix.c:294),
+ *    limit_amplitudes / elimit_amplitudes (limit_amplitudes.c:193, :472) -- all
+ *    called as compiled from the reference;
+ *  - element construction: parameter names, storage offsets and defaults come
+ *    from the reference's own tables (track_data.c entity_description); this
+ *    file only walks them (restating the default-setting of mad_parse.c);
+ *  - the pass/element loop restates do_tracking.c:488-2640 for the supported
+ *    element subset: z bookkeeping (:1077-1084), sticky MAXAMP (:1848-1858),
+ *    aperture after each element (:2455-2475), NaN sweep and loss recording
+ *    (:2629-2636, recordLostParticles :4584-4605), effort counter (:2758).
+ *
+ * Interface (ctypes): b2e_ref_track().  Particle rows are
+ * (x, xp, y, yp, s, delta, id, lossPass, bunch, weight) as in track.h:81-100.
+ */
+#include "mdb.h"
+#include "track.h"
+#include "csbend.h"
+#include <setjmp.h>
+#include <ctype.h>
+
+extern jmp_buf b2e_ref_trap;
+extern int b2e_ref_trap_armed;
+extern char b2e_ref_errmsg[512];
+extern long b2e_ref_warning_count;
+
+typedef struct {
+  const char *name;
+  long type;
+} B2E_REF_TYPE;
+
+static const B2E_REF_TYPE b2e_ref_types[] = {
+  {"DRIF", T_DRIF}, {"DRIFT", T_DRIF}, {"EDRIFT", T_EDRIFT}, {"KQUAD", T_KQUAD},
+  {"KSEXT", T_KSEXT}, {"CSBEND", T_CSBEND}, {"SBEN", T_CSBEND}, {"RFCA", T_RFCA},
+  {"MAXAMP", T_MAXAMP}, {"MARK", T_MARK}, {"CHARGE", T_CHARGE},
+  {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {NULL, 0}};
+
+static long lookup_type(const char *name) {
+  long i;
+  for (i = 0; b2e_ref_types[i].name; i++)
+    if (strcmp(name, b2e_ref_types[i].name) == 0)
+      return b2e_ref_types[i].type;
+  return -1;
+}
+
+/* Fill an element structure with the defaults of its parameter table. */
+static void set_defaults(char *p_elem, long type) {
+  PARAMETER *par = entity_description[type].parameter;
+  long i;
+  for (i = 0; i < entity_description[type].n_params; i++) {
+    char *where = p_elem + par[i].offset;
+    switch (par[i].type) {
+    case IS_DOUBLE:
+      *(double *)where = par[i].number;
+      break;
+    case IS_LONG:
+      *(long *)where = par[i].integer;
+      break;
+    case IS_SHORT:
+      *(short *)where = (short)par[i].integer;
+      break;
+    case IS_STRING:
+      *(char **)where = par[i].string ? strdup(par[i].string) : NULL;
+      break;
+    }
+  }
+}
+
+static int set_parameter(char *p_elem, long type, const char *key, const char *value) {
+  PARAMETER *par = entity_description[type].parameter;
+  long i;
+  for (i = 0; i < entity_description[type].n_params; i++) {
+    if (strcmp(par[i].name, key) == 0) {
+      char *where = p_elem + par[i].offset;
+      switch (par[i].type) {
+      case IS_DOUBLE:
+        *(double *)where = strtod(value, NULL);
+        break;
+      case IS_LONG:
+        *(long *)where = strtol(value, NULL, 10);
+        break;
+      case IS_SHORT:
+        *(short *)where = (short)strtol(value, NULL, 10);
+        break;
+      case IS_STRING:
+        *(char **)where = strdup(value);
+        break;
+      }
+      return 1;
+    }
+  }
+  return 0;
+}
+
+/* Parse "NAME:TYPE KEY=VALUE ...;NAME:TYPE ..." into an ELEMENT_LIST chain. */
+static ELEMENT_LIST *build_line(const char *spec, long *n_out) {
+  char *text = strdup(spec), *save1 = NULL, *item;
+  ELEMENT_LIST *head = NULL, *tail = NULL;
+  double pos = 0;
+  long n = 0;
+  for (item = strtok_r(text, ";\n", &save1); item; item = strtok_r(NULL, ";\n", &save1)) {
+    char *save2 = NULL, *tok, *colon;
+    ELEMENT_LIST *e;
+    long type;
+    while (isspace((unsigned char)*item))
+      item++;
+    if (!*item)
+      continue;
+    tok = strtok_r(item, " \t", &save2);
+    e = calloc(1, sizeof(*e));
+    colon = strchr(tok, ':');
+    if (colon) {
+      *colon = 0;
+      e->name = strdup(tok);
+      tok = colon + 1;
+    } else {
+      char buf[32];
+      snprintf(buf, sizeof(buf), "E%ld", n);
+      e->name = strdup(buf);
+    }
+    if ((type = lookup_type(tok)) < 0) {
+      snprintf(b2e_ref_errmsg, sizeof(b2e_ref_errmsg), "unsupported element type %s", tok);
+      free(text);
+      return NULL;
+    }
+    e->type = type;
+    e->p_elem = calloc(1, entity_description[type].structure_size + 64);
+    set_defaults(e->p_elem, type);
+    while ((tok = strtok_r(NULL, " \t", &save2))) {
+      char *eq = strchr(tok, '=');
+      if (!eq)
+        continue;
+      *eq = 0;
+      if (!set_parameter(e->p_elem, type, tok, eq + 1)) {
+        snprintf(b2e_ref_errmsg, sizeof(b2e_ref_errmsg), "unknown parameter %s for %s", tok, entity_name[type]);
+        free(text);
+        return NULL;
+      }
+    }
+    switch (type) {
+    case T_CSBEND:
+      ((CSBEND *)e->p_elem)->e1Index = 0;
+      ((CSBEND *)e->p_elem)->e2Index = 1;
+      ((CSBEND *)e->p_elem)->etiltSign = 1;
+      break;
+    case T_CSRCSBEND:
+      ((CSRCSBEND *)e->p_elem)->e1Index = 0;
+      ((CSRCSBEND *)e->p_elem)->e2Index = 1;
+      ((CSRCSBEND *)e->p_elem)->etiltSign = 1;
+      break;
+    default:
+      break;
+    }
+    e->beg_pos = pos;
+    if (entity_description[type].flags & HAS_LENGTH)
+      pos += ((DRIFT *)e->p_elem)->length;
+    e->end_pos = pos;
+    e->occurence = 1;
+    if (!head)
+      head = e;
+    else {
+      tail->succ = e;
+      e->pred = tail;
+    }
+    tail = e;
+    n++;
+  }
+  free(text);
+  *n_out = n;
+  return head;
+}
+
+static void record_lost(double **coord, long nLeft, long nToTrack, long pass) {
+  /* do_tracking.c:4584-4605 (recordLostParticles) */
+  long i;
+  for (i = nLeft; i < nToTrack; i++)
+    coord[i][lossPassIndex] = pass;
+}
+
+/* CSR wake capture for parity tests: the reference keeps the last dipole wake
+ * in the global csrWake (csbend.h); after each CSRCSBEND we copy dGamma out. */
+static double *wake_out = NULL;
+static long wake_cap = 0, wake_count = 0;
+
+long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long np, long n_passes,
+                   double *rows_out, long *n_left, double *effort, double *wake_buffer, long wake_capacity,
+                   long *wake_written, char *errbuf, long errlen) {
+  ELEMENT_LIST *line, *eptr;
+  double **coord = NULL;
+  long nElems = 0, nToTrack, nLeft, i_pass, i, j;
+  double z, z_travel, last_z;
+  MAXAMP *maxamp = NULL;
+  double x_max = 0, y_max = 0;
+  long elliptical = 0, maxampOpenCode = 0, maxampExponent = 0, maxampYExponent = 0;
+  CHARGE *charge = NULL;
+  APERTURE_DATA apertureData;
+  double P_central = p_central;
+  double revolution_length;
+  long status = 0;
+
+  static int offsets_done = 0;
+  if (!offsets_done) {
+    /* track_data.c:4066: parameter offsets are stored as addresses into the
+     * *_example structures until compute_offsets() rebases them */
+    compute_offsets();
+    offsets_done = 1;
+  }
+  memset(&apertureData, 0, sizeof(apertureData));
+  b2e_ref_errmsg[0] = 0;
+  sizeOfParticle = totalPropertiesPerParticle * sizeof(double);
+  particleMass = me_mks;
+  particleCharge = e_mks;
+  particleMassMV = me_mev;
+  particleRadius = re_mks;
+  particleRelSign = 1;
+  particleIsElectron = 1;
+  wake_out = wake_buffer;
+  wake_cap = wake_capacity;
+  wake_count = 0;
+
+  if (setjmp(b2e_ref_trap)) {
+    b2e_ref_trap_armed = 0;
+    if (errbuf && errlen > 0)
+      snprintf(errbuf, errlen, "%s", b2e_ref_errmsg);
+    return -1;
+  }
+  b2e_ref_trap_armed = 1;
+
+  if (!(line = build_line(lattice, &nElems))) {
+    b2e_ref_trap_armed = 0;
+    if (errbuf && errlen > 0)
+      snprintf(errbuf, errlen, "%s", b2e_ref_errmsg);
+    return -2;
+  }
+
+  for (eptr = line, revolution_length = 0; eptr; eptr = eptr->succ)
+    revolution_length = eptr->end_pos - line->beg_pos;
+
+  coord = (double **)czarray_2d(sizeof(double), np ? np : 1, totalPropertiesPerParticle);
+  for (i = 0; i < np; i++) {
+    for (j = 0; j < 7; j++)
+      coord[i][j] = rows_in[i * 7 + j];
+    coord[i][lossPassIndex] = -1;
+    coord[i][bunchIndex] = 0;
+    coord[i][weightIndex] = 1;
+  }
+  nToTrack = nLeft = np;
+  *effort = 0;
+
+  for (i_pass = 0; i_pass < n_passes; i_pass++) {
+    long nParticlesStartPass = nToTrack;
+    z = z_travel = last_z = line->beg_pos;
+    eptr = line;
+    while (eptr && nToTrack) {
+      unsigned long classFlags = entity_description[eptr->type].flags;
+      last_z = z;
+      if (classFlags & HAS_LENGTH && eptr->p_elem) {
+        z += ((DRIFT *)eptr->p_elem)->length;
+        z_travel += ((DRIFT *)eptr->p_elem)->length;
+      } else {
+        z += eptr->end_pos - eptr->beg_pos;
+        z_travel += eptr->end_pos - eptr->beg_pos;
+      }
+      setTrackingContext(eptr->name, eptr->occurence, eptr->type, "b2e", eptr);
+      nLeft = nToTrack;
+      if (classFlags & MATRIX_TRACKING) {
+        if (!eptr->matrix) {
+          DRIFT *drift = (DRIFT *)eptr->p_elem;
+          /* default_order = 2 (elegant.nl run_setup default) */
+          eptr->matrix = drift_matrix(drift->length, drift->order ? drift->order : 2);
+        }
+        if (nParticlesStartPass)
+          track_particles(coord, eptr->matrix, coord, nToTrack);
+      } else if (nParticlesStartPass) {
+        switch (eptr->type) {
+        case T_CHARGE:
+          if (i_pass == 0) {
+            charge = (CHARGE *)eptr->p_elem;
+            charge->macroParticleCharge = 0;
+            if (np)
+              charge->macroParticleCharge = charge->charge / np;
+            if (charge->chargePerParticle)
+              charge->macroParticleCharge = charge->chargePerParticle;
+          }
+          break;
+        case T_MARK:
+          break;
+        case T_MAXAMP:
+          maxamp = (MAXAMP *)eptr->p_elem;
+          x_max = maxamp->x_max;
+          y_max = maxamp->y_max;
+          elliptical = maxamp->elliptical;
+          maxampOpenCode = determineOpenSideCode(maxamp->openSide);
+          maxampExponent = maxamp->exponent;
+          maxampYExponent = maxamp->yExponent;
+          break;
+        case T_RFCA:
+          nLeft = simple_rf_cavity(coord, nToTrack, (RFCA *)eptr->p_elem, NULL, &P_central, z_travel);
+          break;
+        case T_EDRIFT:
+          exactDrift(coord, nToTrack, ((EDRIFT *)eptr->p_elem)->length);
+          break;
+        case T_KQUAD:
+        case T_KSEXT:
+          nLeft = multipole_tracking2(coord, nToTrack, eptr, 0.0, P_central, NULL, last_z, maxamp, NULL,
+                                      &apertureData, NULL, -1);
+          break;
+        case T_CSBEND: {
+          CSBEND *cs = (CSBEND *)eptr->p_elem;
+          cs->edgeFlags = determine_bend_flags(eptr, cs->edge_effects[cs->e1Index], cs->edge_effects[cs->e2Index]);
+          nLeft = track_through_csbend(coord, nToTrack, cs, 0.0, P_central, NULL, last_z, NULL, "b2e", maxamp,
+                                       NULL, &apertureData, -1, eptr);
+          break;
+        }
+        case T_CSRCSBEND: {
+          CSRCSBEND *cs = (CSRCSBEND *)eptr->p_elem;
+          cs->edgeFlags = determine_bend_flags(eptr, cs->edge_effects[cs->e1Index], cs->edge_effects[cs->e2Index]);
+          nLeft = track_through_csbendCSR(coord, nToTrack, cs, 0.0, P_central, NULL, last_z, z, charge, "b2e",
+                                          maxamp, NULL, &apertureData, eptr);
+          if (wake_out && csrWake.valid && csrWake.dGamma) {
+            for (j = 0; j < csrWake.bins && wake_count < wake_cap; j++)
+              wake_out[wake_count++] = csrWake.dGamma[j];
+          }
+          break;
+        }
+        case T_CSRDRIFT:
+          nLeft = track_through_driftCSR(coord, nToTrack, (CSRDRIFT *)eptr->p_elem, P_central, NULL, last_z,
+                                         revolution_length, charge, "b2e");
+          break;
+        default:
+          bombElegant("element type not supported by the reference driver", NULL);
+        }
+      }
+      if (!(classFlags & NO_APERTURE)) {
+        if (x_max || y_max) {
+          if (!elliptical)
+            nLeft = limit_amplitudes(coord, x_max, y_max, nLeft, NULL, z, P_central, eptr->type == T_DRIF,
+                                     maxampOpenCode, eptr);
+          else
+            nLeft = elimit_amplitudes(coord, x_max, y_max, nLeft, NULL, z, P_central, eptr->type == T_DRIF,
+                                      maxampOpenCode, maxampExponent, maxampYExponent, eptr);
+        }
+      }
+      nLeft = limit_amplitudes(coord, DBL_MAX, DBL_MAX, nLeft, NULL, z, P_central, 0, 0, eptr);
+      if (nLeft != nToTrack)
+        record_lost(coord, nLeft, nToTrack, i_pass);
+      nToTrack = nLeft;
+      eptr = eptr->succ;
+    }
+    *effort += nLeft;
+  }
+
+  for (i = 0; i < np; i++)
+    for (j = 0; j < 8; j++)
+      rows_out[i * 8 + j] = coord[i][j];
+  *n_left = nToTrack;
+  if (wake_written)
+    *wake_written = wake_count;
+  b2e_ref_trap_armed = 0;
+  free_czarray_2d((void **)coord, np ? np : 1, totalPropertiesPerParticle);
+  return status;
+}
+
+/* Report element-class flags so tests can check aperture bookkeeping. */
+unsigned long b2e_ref_type_flags(const char *type_name) {
+  long type = lookup_type(type_name);
+  (void)compute_offsets;
+  return type < 0 ? 0 : entity_description[type].flags;
+}
