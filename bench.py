@@ -1,0 +1,339 @@
+"""Throughput benchmark: particle-turns/s of FP64 ring tracking.
+
+Workload (one GPU): the batched error ensemble -- 512 instances of the 8-cell
+3 GeV FODO ring with seeded quadrupole offsets and quadrupole/sextupole
+strength errors, 500-4000 particles per instance (~1.15 M particles), tracked
+in one fused launch per step.  A step is ``--turns-per-step`` passes (100 by
+default) continuing the same run; ``--steps`` steps are timed after
+``--warmup`` untimed ones.
+
+- value: particle-turns/s with particles resident in HBM (b2e_track),
+  timed with CUDA events on the engine's stream, L2 flushed before each step.
+- e2e: the same metric through the C ABI with host buffers (b2e_track_host:
+  pinned-host -> device copy, tracking of a fresh run, device -> host copy,
+  all inside the timed region).
+- roofline: FP64 pipe; algorithmic FP64 operations per particle-turn
+  (counted for this lattice, see elegant_b200/flops.py) over the measured
+  FP64 DGEMM rate of this GPU.
+- cpu_baseline / --impl reference: elegant's own C tracking code
+  (oracle/_ref, compiled from the reference sources) on the host cores.
+
+Multi-GPU (torchrun): every rank tracks its own full ensemble (different
+seed): weak scaling, no data-path collective; time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-turns/s (FP64)"
+UNIT = "particle-turns/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--turns-per-step", type=int, default=100)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thr = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thr = threading.Thread(target=self._run, daemon=True)
+        self._thr.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thr:
+            self._thr.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------ CPU oracle ----
+def _ref_worker(args):
+    """Track a slice of ensemble instances with the reference's C code (libm)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from reforacle import RefOracle
+    from elegant_b200 import workloads as w
+    from elegant_b200.lattice import Element, Lattice
+
+    inst_list, n_instances, turns, seed, max_particles = args
+    lat, beam, offsets, overrides = w.ensemble(n_instances=n_instances, seed=seed)
+    oracle = RefOracle("libm")
+    effort = 0.0
+    t0 = time.perf_counter()
+    for i in inst_list:
+        els = []
+        for j, e in enumerate(lat.elements):
+            params = dict(e.params)
+            for (ie, name, vals) in overrides:
+                if ie == j:
+                    params[name] = float(vals[i])
+            els.append(Element(e.name, e.type, params))
+        sl = slice(offsets[i], min(offsets[i + 1], offsets[i] + max_particles))
+        _, _, eff, _ = oracle.track(Lattice(els), beam.coords[sl], beam.ids[sl], w.ring_p_central(), turns)
+        effort += eff
+    return effort, time.perf_counter() - t0
+
+
+def cpu_reference_rate(n_instances: int, seed: int, target_seconds: float, cores: int):
+    """Particle-turns/s of the reference C code on `cores` host processes over a
+    bounded sample: `cores` instances, each capped at a particle count sized
+    so one process runs for about `target_seconds`."""
+    rate_per_core = 1.6e4  # calibration guess, refined by the measurement itself
+    turns = 20
+    max_particles = max(50, int(target_seconds * rate_per_core / turns))
+    insts = [[i] for i in range(cores)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_ref_worker, [(il, n_instances, turns, seed, max_particles) for il in insts])
+    wall = time.perf_counter() - t0
+    effort = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return effort / busy, {"cores": cores, "turns": turns, "particles_per_instance_cap": max_particles,
+                           "instances": cores, "effort": effort, "busy_s": busy, "wall_s": wall}
+
+
+# ------------------------------------------------------------------ main ----
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from elegant_b200 import Tracker, workloads as w
+    from elegant_b200.flops import flops_per_particle_turn
+
+    seed = 2024 + 1000 * rank
+    lat, beam, offsets, overrides = w.ensemble(n_instances=args.instances, seed=seed)
+    n = beam.n
+    tracker = Tracker(lat, w.ring_p_central(), args.turns_per_step, device=local_rank)
+    tracker.load_ensemble(offsets, overrides)
+    stream = torch.cuda.ExternalStream(tracker.stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # ---- device-resident run: upload once, then continue the run step by step
+    tracker.upload(beam)
+    for _ in range(args.warmup):
+        tracker.continue_tracking()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = tracker.launches
+    step_ms = []
+    effort_total = 0.0
+    with ClockSampler(local_rank) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            effort_total += tracker.continue_tracking()
+            ev1.record(stream)
+            ev1.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+    torch.cuda.synchronize()
+    launches = tracker.launches - launches0
+    t_total = sum(step_ms) / 1e3
+    if dist:
+        tt = torch.tensor([t_total, effort_total], dtype=torch.float64, device="cuda")
+        tmax = tt.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+        t_job, effort_job = float(tmax[0]), float(tt[1])
+    else:
+        t_job, effort_job = t_total, effort_total
+    value = effort_job / t_job
+
+    # ---- roofline: FP64 operations per particle-turn over measured DGEMM rate
+    fpt = flops_per_particle_turn(lat)
+    achieved_tflops = effort_total * fpt / t_total / 1e12
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.mm(a, a)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.mm(a, a)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    fp64_peak = 2 * 8192 ** 3 / best / 1e12
+    del a
+
+    # ---- e2e: host buffers through the C ABI, fresh run per step
+    e2e = None
+    if not args.no_e2e:
+        pinned = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(6)]
+        ids = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        lp = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        le = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        src = torch.from_numpy(beam.coords)
+        src_ids = torch.from_numpy(beam.ids)
+
+        def e2e_step():
+            for c in range(6):
+                pinned[c].copy_(src[:, c])
+            ids.copy_(src_ids)
+            return tracker.track_host_pointers([p.data_ptr() for p in pinned], ids.data_ptr(), n, lp.data_ptr(),
+                                               le.data_ptr())
+
+        e2e_step()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e2e_ms = []
+        e2e_eff = 0.0
+        for _ in range(max(1, min(args.steps, 5))):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, eff = e2e_step()
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_eff += eff
+        t_e2e = sum(e2e_ms) / 1e3
+        if dist:
+            tt = torch.tensor([t_e2e, e2e_eff], dtype=torch.float64, device="cuda")
+            tmax = tt.clone()
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+            dist.all_reduce(tt, op=dist.ReduceOp.SUM)
+            t_e2e, e2e_eff = float(tmax[0]), float(tt[1])
+        e2e = {"value": e2e_eff / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(n * (6 * 8 + 8)),
+               "d2h_bytes_per_step": int(n * (6 * 8 + 8 + 4 + 4)), "steps": len(e2e_ms),
+               "ms_per_step": sum(e2e_ms) / len(e2e_ms), "timing": "host wall clock around the blocking C-ABI call"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        rate, info = cpu_reference_rate(args.instances, 2024, args.cpu_seconds, cores)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+               "sample": f"elegant's own C tracking (oracle/_ref, glibc libm), {info['instances']} ensemble "
+                         f"instances x <= {info['particles_per_instance_cap']} particles x {info['turns']} turns, "
+                         f"one process per core; busy {info['busy_s']:.1f} s"}
+
+    if dist:
+        dist.barrier()
+    tracker.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_job * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched error ensemble of the 8-cell FODO ring (config 2)",
+                       "instances_per_gpu": args.instances, "particles_per_gpu": n,
+                       "turns_per_step": args.turns_per_step, "lattice_elements": len(lat),
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved_tflops / fp64_peak, "traffic": None,
+                         "flops_per_particle_turn": fpt,
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.mm float64), best of 3"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    steps = []
+    effort_total = 0.0
+    for _ in range(args.warmup):
+        cpu_reference_rate(args.instances, 2024, min(2.0, args.cpu_seconds), cores)
+    t_sum = 0.0
+    info = None
+    for _ in range(args.steps):
+        rate, info = cpu_reference_rate(args.instances, 2024, args.cpu_seconds / 2, cores)
+        effort_total += info["effort"]
+        t_sum += info["busy_s"]
+        steps.append(info["busy_s"] * 1e3)
+    value = effort_total / t_sum
+    sample = (f"elegant's own C tracking (oracle/_ref, glibc libm) on {cores} host processes; each step "
+              f"{info['instances']} instances x <= {info['particles_per_instance_cap']} particles x "
+              f"{info['turns']} turns of the ensemble ring")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sum(steps) / len(steps), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched error ensemble of the 8-cell FODO ring (config 2)",
+                   "instances_per_gpu": args.instances},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+if __name__ == "__main__":
+    main()

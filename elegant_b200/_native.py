@@ -1,0 +1,104 @@
+"""ctypes binding of the engine's C ABI (include/elegant_b200.h).
+
+The library is loaded from the package directory.  There is no CPU fallback:
+if the library or a CUDA device is missing, calls raise ``EngineError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libelegant_b200.so")
+
+B2E_OK = 0
+ERRORS = {
+    -1: "invalid argument",
+    -2: "unsupported lattice",
+    -3: "CUDA error",
+    -4: "device out of memory",
+    -5: "call out of order",
+    -6: "device wait timed out",
+    -7: "device fault flag",
+}
+
+# element type codes (include/elegant_b200.h)
+DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT = range(1, 12)
+MAX_PARAMS = 40
+
+EXPORTED = [
+    "b2e_create", "b2e_destroy", "b2e_last_error", "b2e_version", "b2e_load_lattice",
+    "b2e_upload_particles", "b2e_track", "b2e_download", "b2e_track_host", "b2e_track_device",
+    "b2e_load_ensemble", "b2e_ensemble_history", "b2e_csr_wakes", "b2e_stream",
+    "b2e_kernel_launches",
+]
+
+
+class Element(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("reserved", ctypes.c_int32), ("name", ctypes.c_char * 32),
+                ("p", ctypes.c_double * MAX_PARAMS)]
+
+
+class RunOptions(ctypes.Structure):
+    _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_int32), ("default_order", ctypes.c_int32),
+                ("coord_limit", ctypes.c_double), ("slope_limit", ctypes.c_double),
+                ("passes_per_launch", ctypes.c_int32), ("threads_per_block", ctypes.c_int32)]
+
+
+class Override(ctypes.Structure):
+    _fields_ = [("element", ctypes.c_int32), ("slot", ctypes.c_int32), ("values", ctypes.POINTER(ctypes.c_double))]
+
+
+class EngineError(RuntimeError):
+    """A C-ABI call returned a nonzero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load the engine library (built by ``elegant_b200.build``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise EngineError(-5, f"{p} is missing; run `python -m elegant_b200.build`")
+    lib = ctypes.CDLL(p)
+    vp, c_int, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64
+    dpp = ctypes.POINTER(ctypes.c_void_p)
+    sig = {
+        "b2e_create": (c_int, [ctypes.POINTER(vp), c_int]),
+        "b2e_destroy": (c_int, [vp]),
+        "b2e_last_error": (ctypes.c_char_p, [vp]),
+        "b2e_version": (c_int, []),
+        "b2e_load_lattice": (c_int, [vp, ctypes.POINTER(Element), ctypes.c_int32, ctypes.POINTER(RunOptions)]),
+        "b2e_upload_particles": (c_int, [vp, dpp, vp, i64]),
+        "b2e_track": (c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
+        "b2e_download": (c_int, [vp, dpp, vp, vp, vp, ctypes.POINTER(i64)]),
+        "b2e_track_host": (c_int, [vp, dpp, vp, i64, vp, vp, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_double)]),
+        "b2e_track_device": (c_int, [vp, dpp, vp, i64, vp, vp, ctypes.POINTER(ctypes.c_double)]),
+        "b2e_load_ensemble": (c_int, [vp, ctypes.c_int32, vp, ctypes.POINTER(Override), ctypes.c_int32]),
+        "b2e_ensemble_history": (c_int, [vp, vp, vp, vp, vp, vp]),
+        "b2e_csr_wakes": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
+        "b2e_stream": (vp, [vp]),
+        "b2e_kernel_launches": (i64, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def pointer_array(ptrs) -> ctypes.Array:
+    arr = (ctypes.c_void_p * len(ptrs))()
+    for i, p in enumerate(ptrs):
+        arr[i] = p
+    return arr

@@ -1,0 +1,556 @@
+/*
+ * C-ABI implementation (include/elegant_b200.h): context, device buffers and
+ * the pass/element orchestration that replaces do_tracking's loop
+ * (do_tracking.c:488-2640) for the supported subset.
+ *
+ * Orchestration of one b2e_track call:
+ *   pass 0 is cut before every RFCA whose fiducial is not yet known; between
+ *   the pieces a one-thread-per-instance kernel forms the Kahan mean arrival
+ *   time (findFiducialTime, simple_rfca.c:62-262) on the particles that reach
+ *   the cavity; everything after the last fiducial runs as fused multi-pass
+ *   launches (passes_per_launch passes each, all by default).
+ *   CSR elements (CSRCSBEND/CSRDRIFT) are collective and are executed by the
+ *   CSR driver (b2e_csr.cu) between ring launches.
+ */
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include "b2e_lattice.h"
+#include "b2e_csr.h"
+#include "b2e_kernels.h"
+
+
+
+using namespace b2e;
+
+static const int kTileThreads = 128;
+
+template <typename T> struct DevBuf {
+  T *ptr = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap && ptr)
+      return cudaSuccess;
+    if (ptr)
+      cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    bytes = (bytes + 255) & ~(size_t)255;
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e == cudaSuccess)
+      cap = bytes / sizeof(T);
+    return e;
+  }
+  void release() {
+    if (ptr)
+      cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+struct b2e_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  /* lattice */
+  std::vector<b2e_element> base;
+  b2e_run_options opt{};
+  bool lattice_loaded = false;
+  CompiledLattice lat;            /* instance 0 / base */
+  int n_inst = 1;
+  std::vector<int64_t> inst_offsets{0, 0};
+  std::vector<DevElem> elems_all; /* [n_inst][n_elems] */
+  std::vector<DevAperture> aps_all;
+  DevBuf<DevElem> d_elems;
+  DevBuf<DevAperture> d_aps;
+  DevBuf<DevRfState> d_rf;
+  DevBuf<DevTile> d_tiles;
+  DevBuf<int64_t> d_inst_offsets;
+  std::vector<DevTile> tiles;
+  /* particles */
+  int64_t n = 0;
+  DevBuf<double> d_cols[6];
+  DevBuf<int64_t> d_ids;
+  DevBuf<int32_t> d_lost_pass, d_lost_elem;
+  DevBuf<unsigned int> d_flag;
+  DevBuf<unsigned long long> d_counters;
+  bool particles_loaded = false;
+  /* external (device) particle pointers for b2e_track_device */
+  DevParticles ext{};
+  bool use_ext = false;
+  CsrState csr;
+  int pass_counter = 0; /* next pass to track in the current run */
+  int64_t launches = 0; /* kernels launched by this context */
+};
+
+static int fail(b2e_ctx *ctx, int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx)
+    ctx->err = buf;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                                     \
+  do {                                                                                                           \
+    cudaError_t e_ = (call);                                                                                     \
+    if (e_ != cudaSuccess)                                                                                       \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? B2E_ERR_NOMEM : B2E_ERR_CUDA, "%s: %s (%s:%d)", #call, \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                                                   \
+  } while (0)
+
+extern "C" int b2e_version(void) { return 1; }
+
+extern "C" int b2e_create(b2e_ctx **out, int device) {
+  if (!out)
+    return B2E_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= 0)
+    return B2E_ERR_CUDA;
+  if (device < 0 || device >= ndev)
+    return B2E_ERR_ARG;
+  b2e_ctx *ctx = new b2e_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return B2E_ERR_CUDA;
+  }
+  *out = ctx;
+  return B2E_OK;
+}
+
+extern "C" int b2e_destroy(b2e_ctx *ctx) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->d_elems.release();
+  ctx->d_aps.release();
+  ctx->d_rf.release();
+  ctx->d_tiles.release();
+  ctx->d_inst_offsets.release();
+  for (auto &c : ctx->d_cols)
+    c.release();
+  ctx->d_ids.release();
+  ctx->d_lost_pass.release();
+  ctx->d_lost_elem.release();
+  ctx->d_flag.release();
+  ctx->d_counters.release();
+  csr_release(ctx->csr);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return B2E_OK;
+}
+
+extern "C" const char *b2e_last_error(const b2e_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" void *b2e_stream(b2e_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int64_t b2e_kernel_launches(const b2e_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+/* Rebuild the tile table for the current instance partition. */
+static void build_tiles(b2e_ctx *ctx) {
+  ctx->tiles.clear();
+  for (int i = 0; i < ctx->n_inst; i++) {
+    for (int64_t s = ctx->inst_offsets[i]; s < ctx->inst_offsets[i + 1]; s += kTileThreads) {
+      DevTile t;
+      t.start = s;
+      t.count = (int32_t)std::min<int64_t>(kTileThreads, ctx->inst_offsets[i + 1] - s);
+      t.inst = i;
+      ctx->tiles.push_back(t);
+    }
+  }
+}
+
+static int upload_lattice_tables(b2e_ctx *ctx) {
+  CUDA_TRY(ctx, ctx->d_elems.ensure(ctx->elems_all.size()));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_elems.ptr, ctx->elems_all.data(), sizeof(DevElem) * ctx->elems_all.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, ctx->d_aps.ensure(std::max<size_t>(ctx->aps_all.size(), 1)));
+  if (!ctx->aps_all.empty())
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_aps.ptr, ctx->aps_all.data(), sizeof(DevAperture) * ctx->aps_all.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, ctx->d_rf.ensure(std::max<size_t>((size_t)ctx->n_inst * ctx->lat.n_rf, 1)));
+  CUDA_TRY(ctx, ctx->d_inst_offsets.ensure(ctx->inst_offsets.size()));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_inst_offsets.ptr, ctx->inst_offsets.data(),
+                                sizeof(int64_t) * ctx->inst_offsets.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, ctx->d_tiles.ensure(std::max<size_t>(ctx->tiles.size(), 1)));
+  if (!ctx->tiles.empty())
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_tiles.ptr, ctx->tiles.data(), sizeof(DevTile) * ctx->tiles.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return B2E_OK;
+}
+
+extern "C" int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32_t n_elements,
+                                const b2e_run_options *options) {
+  if (!ctx || !elements || n_elements <= 0 || !options)
+    return fail(ctx, B2E_ERR_ARG, "b2e_load_lattice: null argument or empty lattice");
+  if (options->p_central <= 0)
+    return fail(ctx, B2E_ERR_ARG, "b2e_load_lattice: p_central must be positive");
+  if (options->n_passes < 0)
+    return fail(ctx, B2E_ERR_ARG, "b2e_load_lattice: n_passes must be >= 0");
+  cudaSetDevice(ctx->device);
+  ctx->opt = *options;
+  if (ctx->opt.default_order <= 0)
+    ctx->opt.default_order = 2;
+  if (ctx->opt.coord_limit <= 0)
+    ctx->opt.coord_limit = 10;
+  if (ctx->opt.slope_limit <= 0)
+    ctx->opt.slope_limit = 1;
+  std::string e = compile_lattice(elements, n_elements, ctx->opt, ctx->lat);
+  if (!e.empty())
+    return fail(ctx, B2E_ERR_LATTICE, "%s", e.c_str());
+  ctx->base.assign(elements, elements + n_elements);
+  ctx->n_inst = 1;
+  ctx->inst_offsets = {0, ctx->n};
+  ctx->elems_all = ctx->lat.elems;
+  ctx->aps_all = ctx->lat.aps;
+  build_tiles(ctx);
+  ctx->lattice_loaded = true;
+  int rc = csr_configure(ctx->csr, ctx->base.data(), n_elements, ctx->lat, ctx->opt, ctx->err);
+  if (rc)
+    return rc;
+  return upload_lattice_tables(ctx);
+}
+
+extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_t *offsets,
+                                 const b2e_override *overrides, int32_t n_overrides) {
+  if (!ctx || n_instances <= 0 || !offsets || (n_overrides > 0 && !overrides))
+    return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: bad arguments");
+  if (!ctx->lattice_loaded)
+    return fail(ctx, B2E_ERR_STATE, "b2e_load_ensemble: load a lattice first");
+  if (!ctx->lat.csr_elements.empty())
+    return fail(ctx, B2E_ERR_LATTICE, "b2e_load_ensemble: CSR elements are not supported in ring ensembles");
+  for (int i = 0; i < n_instances; i++)
+    if (offsets[i + 1] < offsets[i] || offsets[0] != 0)
+      return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: offsets must start at 0 and be nondecreasing");
+  const int ne = (int)ctx->base.size();
+  for (int k = 0; k < n_overrides; k++)
+    if (overrides[k].element < 0 || overrides[k].element >= ne || overrides[k].slot < 0 ||
+        overrides[k].slot >= B2E_MAX_PARAMS || !overrides[k].values)
+      return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: override %d out of range", k);
+  ctx->n_inst = n_instances;
+  ctx->inst_offsets.assign(offsets, offsets + n_instances + 1);
+  ctx->elems_all.clear();
+  ctx->aps_all.clear();
+  std::vector<b2e_element> inst(ctx->base);
+  CompiledLattice cl;
+  for (int i = 0; i < n_instances; i++) {
+    inst = ctx->base;
+    for (int k = 0; k < n_overrides; k++)
+      inst[overrides[k].element].p[overrides[k].slot] = overrides[k].values[i];
+    std::string e = compile_lattice(inst.data(), ne, ctx->opt, cl);
+    if (!e.empty())
+      return fail(ctx, B2E_ERR_LATTICE, "instance %d: %s", i, e.c_str());
+    ctx->elems_all.insert(ctx->elems_all.end(), cl.elems.begin(), cl.elems.end());
+    ctx->aps_all.insert(ctx->aps_all.end(), cl.aps.begin(), cl.aps.end());
+  }
+  build_tiles(ctx);
+  return upload_lattice_tables(ctx);
+}
+
+static int ensure_particle_buffers(b2e_ctx *ctx, int64_t n) {
+  for (auto &c : ctx->d_cols)
+    CUDA_TRY(ctx, c.ensure((size_t)n));
+  CUDA_TRY(ctx, ctx->d_ids.ensure((size_t)n));
+  CUDA_TRY(ctx, ctx->d_lost_pass.ensure((size_t)n));
+  CUDA_TRY(ctx, ctx->d_lost_elem.ensure((size_t)n));
+  CUDA_TRY(ctx, ctx->d_flag.ensure(1));
+  CUDA_TRY(ctx, ctx->d_counters.ensure(2));
+  return B2E_OK;
+}
+
+extern "C" int b2e_upload_particles(b2e_ctx *ctx, const double *const columns[6], const int64_t *ids, int64_t n) {
+  if (!ctx || n < 0 || (n > 0 && (!columns || !ids)))
+    return fail(ctx, B2E_ERR_ARG, "b2e_upload_particles: bad arguments");
+  for (int c = 0; c < 6 && n > 0; c++)
+    if (!columns[c])
+      return fail(ctx, B2E_ERR_ARG, "b2e_upload_particles: column %d is null", c);
+  cudaSetDevice(ctx->device);
+  int rc = ensure_particle_buffers(ctx, n);
+  if (rc)
+    return rc;
+  if (n > 0) {
+    for (int c = 0; c < 6; c++)
+      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_cols[c].ptr, columns[c], sizeof(double) * n, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_ids.ptr, ids, sizeof(int64_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_lost_pass.ptr, 0xff, sizeof(int32_t) * n, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_lost_elem.ptr, 0xff, sizeof(int32_t) * n, ctx->stream));
+  }
+  ctx->n = n;
+  ctx->particles_loaded = true;
+  ctx->use_ext = false;
+  ctx->pass_counter = 0;
+  if (ctx->n_inst == 1) {
+    ctx->inst_offsets = {0, n};
+    build_tiles(ctx);
+    return upload_lattice_tables(ctx);
+  }
+  if (ctx->inst_offsets.back() != n)
+    return fail(ctx, B2E_ERR_ARG, "b2e_upload_particles: ensemble offsets cover %lld particles, got %lld",
+                (long long)ctx->inst_offsets.back(), (long long)n);
+  return B2E_OK;
+}
+
+static DevParticles particle_view(b2e_ctx *ctx) {
+  if (ctx->use_ext)
+    return ctx->ext;
+  DevParticles P;
+  P.x = ctx->d_cols[0].ptr;
+  P.xp = ctx->d_cols[1].ptr;
+  P.y = ctx->d_cols[2].ptr;
+  P.yp = ctx->d_cols[3].ptr;
+  P.s = ctx->d_cols[4].ptr;
+  P.dp = ctx->d_cols[5].ptr;
+  P.lost_pass = ctx->d_lost_pass.ptr;
+  P.lost_elem = ctx->d_lost_elem.ptr;
+  return P;
+}
+
+/* Track element range [(pb, eb), (pe, ee)) with ring launches, splitting at CSR elements. */
+static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
+  const int ne = (int)ctx->lat.elems.size();
+  RingLaunch L;
+  L.P = particle_view(ctx);
+  L.tiles = ctx->d_tiles.ptr;
+  L.elems = ctx->d_elems.ptr;
+  L.aps = ctx->d_aps.ptr;
+  L.rf = ctx->d_rf.ptr;
+  L.n_elems = ne;
+  L.n_aps = (int)ctx->lat.aps.size();
+  L.n_rf = ctx->lat.n_rf;
+  L.g.p_central = ctx->opt.p_central;
+  L.g.coord_limit = ctx->opt.coord_limit;
+  L.g.slope_limit = ctx->opt.slope_limit;
+  L.error_flag = ctx->d_flag.ptr;
+  size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
+  bool staged = smem <= 200 * 1024;
+  int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
+  int p = pb, e = eb;
+  while (p < pe || (p == pe && e < ee)) {
+    /* end of this launch: at most ppl passes, never past (pe, ee) */
+    int lp = p + ppl - 1 < pe ? p + ppl - 1 : pe;
+    int le = lp == pe ? ee : ne;
+    if (lp > p && le == 0) { /* (lp, 0) is the same point as (lp-1, ne) */
+      lp -= 1;
+      le = ne;
+    }
+    L.pass_begin = p;
+    L.elem_begin = e;
+    L.pass_end = lp;
+    L.elem_end = le;
+    CUDA_TRY(ctx, launch_ring(L, (int)ctx->tiles.size(), staged, staged ? smem : 0, ctx->stream));
+    ctx->launches += ctx->tiles.empty() ? 0 : 1;
+    if (le >= ne) {
+      p = lp + 1;
+      e = 0;
+    } else {
+      p = lp;
+      e = le;
+    }
+  }
+  return B2E_OK;
+}
+
+static int track_impl(b2e_ctx *ctx, double *effort) {
+  const int ne = (int)ctx->lat.elems.size();
+  const int p0 = ctx->pass_counter;
+  const int npass = p0 + ctx->opt.n_passes; /* one past the last pass of this call */
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag.ptr, 0, sizeof(unsigned int), ctx->stream));
+  if (p0 == 0) {
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_rf.ptr, 0, sizeof(DevRfState) * std::max(1, ctx->n_inst * ctx->lat.n_rf),
+                                  ctx->stream));
+    csr_reset(ctx->csr);
+  }
+  /* stop points: every RFCA on pass 0 (fiducial), every CSR element on every pass */
+  int p = p0, e = 0;
+  size_t next_rf = 0;
+  while (p < npass) {
+    int stop_e = ne, stop_kind = 0; /* 1 = RFCA fiducial, 2 = CSR element */
+    for (int ie = e; ie < ne; ie++) {
+      if (p == 0 && next_rf < ctx->lat.rf_elements.size() && ctx->lat.rf_elements[next_rf] == ie) {
+        stop_e = ie;
+        stop_kind = 1;
+        break;
+      }
+      if (ctx->lat.elems[ie].kind == K_CSRCSBEND || ctx->lat.elems[ie].kind == K_CSRDRIFT) {
+        stop_e = ie;
+        stop_kind = 2;
+        break;
+      }
+    }
+    if (stop_kind == 0) {
+      /* nothing collective ahead on this pass; if the lattice has no CSR
+       * elements, run all remaining passes in fused launches */
+      int last_pass = ctx->lat.csr_elements.empty() ? npass - 1 : p;
+      int rc = run_ring_range(ctx, p, e, last_pass, ne);
+      if (rc)
+        return rc;
+      p = last_pass + 1;
+      e = 0;
+      continue;
+    }
+    if (stop_e > e) {
+      int rc = run_ring_range(ctx, p, e, p, stop_e);
+      if (rc)
+        return rc;
+    }
+    if (stop_kind == 1) {
+      ctx->launches++;
+      CUDA_TRY(ctx, launch_fiducial(particle_view(ctx), ctx->d_inst_offsets.ptr, ctx->n_inst, ctx->d_elems.ptr, ne,
+                                    stop_e, ctx->d_rf.ptr, ctx->lat.n_rf, ctx->opt.p_central, ctx->stream));
+      next_rf++;
+      /* the RFCA itself is tracked by the next ring launch */
+      int rc = run_ring_range(ctx, p, stop_e, p, stop_e + 1);
+      if (rc)
+        return rc;
+    } else {
+      int rc = csr_track_element(ctx->csr, particle_view(ctx), ctx->n, stop_e, p, ctx->stream, ctx->err);
+      if (rc)
+        return rc;
+    }
+    e = stop_e + 1;
+    if (e >= ne) {
+      p++;
+      e = 0;
+    }
+  }
+  ctx->pass_counter = npass;
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  ctx->launches++;
+  CUDA_TRY(ctx, launch_effort(particle_view(ctx).lost_pass, ctx->n, p0, npass, ctx->d_counters.ptr,
+                              ctx->d_counters.ptr + 1, ctx->stream));
+  unsigned long long counters[2];
+  unsigned int flag = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(counters, ctx->d_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flag.ptr, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (flag)
+    return fail(ctx, B2E_ERR_DEVICE, "device reported error flag 0x%x (RFCA fiducial missing)", flag);
+  if (effort)
+    *effort = (double)counters[0];
+  return B2E_OK;
+}
+
+extern "C" int b2e_track(b2e_ctx *ctx, double *effort) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  if (!ctx->lattice_loaded || !ctx->particles_loaded)
+    return fail(ctx, B2E_ERR_STATE, "b2e_track: load a lattice and particles first");
+  cudaSetDevice(ctx->device);
+  ctx->use_ext = false;
+  return track_impl(ctx, effort);
+}
+
+extern "C" int b2e_download(b2e_ctx *ctx, double *const columns[6], int64_t *ids, int32_t *lost_pass,
+                            int32_t *lost_element, int64_t *n_left) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  if (!ctx->particles_loaded)
+    return fail(ctx, B2E_ERR_STATE, "b2e_download: no particles");
+  cudaSetDevice(ctx->device);
+  const int64_t n = ctx->n;
+  if (n > 0) {
+    for (int c = 0; c < 6; c++)
+      if (columns && columns[c])
+        CUDA_TRY(ctx, cudaMemcpyAsync(columns[c], ctx->d_cols[c].ptr, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    if (ids)
+      CUDA_TRY(ctx, cudaMemcpyAsync(ids, ctx->d_ids.ptr, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (lost_pass)
+      CUDA_TRY(ctx, cudaMemcpyAsync(lost_pass, ctx->d_lost_pass.ptr, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    if (lost_element)
+      CUDA_TRY(ctx, cudaMemcpyAsync(lost_element, ctx->d_lost_elem.ptr, sizeof(int32_t) * n,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (n_left) {
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    ctx->launches++;
+    CUDA_TRY(ctx, launch_effort(ctx->d_lost_pass.ptr, n, 0, 0, ctx->d_counters.ptr, ctx->d_counters.ptr + 1,
+                                ctx->stream));
+    unsigned long long counters[2];
+    CUDA_TRY(ctx, cudaMemcpyAsync(counters, ctx->d_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *n_left = (int64_t)counters[1];
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return B2E_OK;
+}
+
+extern "C" int b2e_track_host(b2e_ctx *ctx, double *const columns[6], int64_t *ids, int64_t n, int32_t *lost_pass,
+                              int32_t *lost_element, int64_t *n_left, double *effort) {
+  int rc = b2e_upload_particles(ctx, (const double *const *)columns, ids, n);
+  if (rc)
+    return rc;
+  rc = b2e_track(ctx, effort);
+  if (rc)
+    return rc;
+  return b2e_download(ctx, columns, ids, lost_pass, lost_element, n_left);
+}
+
+extern "C" int b2e_track_device(b2e_ctx *ctx, double *const dev_columns[6], const int64_t *dev_ids, int64_t n,
+                                int32_t *dev_lost_pass, int32_t *dev_lost_element, double *effort) {
+  (void)dev_ids;
+  if (!ctx || !dev_columns || !dev_lost_pass || !dev_lost_element || n < 0)
+    return fail(ctx, B2E_ERR_ARG, "b2e_track_device: bad arguments");
+  if (!ctx->lattice_loaded)
+    return fail(ctx, B2E_ERR_STATE, "b2e_track_device: load a lattice first");
+  cudaSetDevice(ctx->device);
+  int rc = ensure_particle_buffers(ctx, 1);
+  if (rc)
+    return rc;
+  if (ctx->n_inst == 1) {
+    ctx->inst_offsets = {0, n};
+    build_tiles(ctx);
+    rc = upload_lattice_tables(ctx);
+    if (rc)
+      return rc;
+  } else if (ctx->inst_offsets.back() != n)
+    return fail(ctx, B2E_ERR_ARG, "b2e_track_device: ensemble offsets do not cover n particles");
+  ctx->ext.x = dev_columns[0];
+  ctx->ext.xp = dev_columns[1];
+  ctx->ext.y = dev_columns[2];
+  ctx->ext.yp = dev_columns[3];
+  ctx->ext.s = dev_columns[4];
+  ctx->ext.dp = dev_columns[5];
+  ctx->ext.lost_pass = dev_lost_pass;
+  ctx->ext.lost_elem = dev_lost_element;
+  ctx->use_ext = true;
+  ctx->n = n;
+  ctx->pass_counter = 0; /* caller-owned buffers: every call is a new run */
+  rc = track_impl(ctx, effort);
+  ctx->use_ext = false;
+  ctx->particles_loaded = false;
+  return rc;
+}
+
+extern "C" int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *cy, double *ex,
+                                    double *ey) {
+  (void)survivors;
+  (void)cx;
+  (void)cy;
+  (void)ex;
+  (void)ey;
+  return fail(ctx, B2E_ERR_STATE, "b2e_ensemble_history: not available");
+}
+
+extern "C" int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written) {
+  if (!ctx || !written)
+    return B2E_ERR_ARG;
+  return csr_copy_wakes(ctx->csr, wakes, capacity, written, ctx->err);
+}

@@ -1,0 +1,437 @@
+/*
+ * Per-particle element maps on the device.  Each function follows the
+ * reference routine's floating-point operation order (cited per function),
+ * because the goal is bit-identical results against the CPU oracle built
+ * with the same elementary functions (b2e_math.h).  The file is compiled
+ * with --fmad=false: no multiply-add contraction except the explicit fma()
+ * inside b2e_math.h.
+ *
+ * All functions return 0 while the particle survives, or a nonzero loss code.
+ */
+#ifndef B2E_ELEMENTS_CUH
+#define B2E_ELEMENTS_CUH
+#include "b2e_engine.h"
+#include "b2e_math.h"
+
+#define B2E_C_MKS 2.99792458e8
+#define B2E_PI 3.141592653589793238462643383279502884
+
+enum { LOSS_NONE = 0, LOSS_APERTURE = 1, LOSS_LIMIT = 2, LOSS_SLOPE = 3, LOSS_NAN = 4, LOSS_ENERGY = 5 };
+
+struct Part {
+  double x, xp, y, yp, s, dp;
+};
+
+__device__ __forceinline__ double b2e_ipow(double x, int n) {
+  /* integer power by repeated multiplication (the toolkit's ipow) */
+  double r;
+  int i;
+  if (n == 0)
+    return 1.0;
+  r = x;
+  for (i = 1; i < n; i++)
+    r *= x;
+  return r;
+}
+
+/* checkMultAperture (multipole.c:1786-1832) for a MAXAMP-derived aperture:
+ * returns true when (x, y) is inside. */
+__device__ __forceinline__ bool mult_aperture_ok(double xIn, double yIn, const DevAperture *ap, const DevElem &e) {
+  double x, y;
+  if (!ap)
+    return true;
+  x = xIn - 0.0; /* xCen = 0 without aperture files */
+  y = yIn - 0.0;
+  if (e.flags & EF_REVERSE_TILT) {
+    double x0 = x, y0 = y;
+    x = x0 * e.rev_cos + y0 * e.rev_sin;
+    y = -x0 * e.rev_sin + y0 * e.rev_cos;
+  }
+  if (ap->elliptical == 0 || ap->x_max <= 0 || ap->y_max <= 0) {
+    if ((ap->x_max > 0 && fabs(x) > ap->x_max) || (ap->y_max > 0 && fabs(y) > ap->y_max))
+      return false;
+  } else {
+    double xa = x / ap->x_max, yb = y / ap->y_max;
+    if ((b2e_ipow(xa, ap->xe) + b2e_ipow(yb, ap->ye)) >= 1)
+      return false;
+  }
+  return true;
+}
+
+/* ---- DRIF: second-order drift matrix through track_particles ---------
+ * drift_matrix (compute_matrices.c:391-412) has C[4]=L, R[0][1]=R[2][3]=L,
+ * T[4][1][1]=T[4][3][3]=L/2; the order-2 contraction (matrix.c:390-419)
+ * sums j = 5..0, so s picks up the yp^2 term before the xp^2 term. */
+__device__ __forceinline__ void drif_o2(Part &p, const DevElem &e) {
+  const double L = e.c[DR_L], LH = e.c[DR_LH];
+  double xn = L * p.xp + p.x;
+  double yn = L * p.yp + p.y;
+  double sn = (L + p.s) + (LH * p.yp) * p.yp;
+  sn = sn + (LH * p.xp) * p.xp;
+  p.x = xn;
+  p.y = yn;
+  p.s = sn;
+}
+
+__device__ __forceinline__ void drif_o1(Part &p, const DevElem &e) {
+  const double L = e.c[DR_L];
+  p.x = L * p.xp + p.x;
+  p.y = L * p.yp + p.y;
+  p.s = L + p.s;
+}
+
+/* ---- EDRIFT: exactDrift (csbend.c:3767-3790) ---- */
+__device__ __forceinline__ void edrift(Part &p, double L) {
+  p.x = p.x + p.xp * L;
+  p.y = p.y + p.yp * L;
+  p.s = p.s + L * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+}
+
+/* convertMomentaToSlopes (multipole.h:261-280, expandHamiltonian = 0) */
+__device__ __forceinline__ bool momenta_to_slopes(double &xp, double &yp, double qx, double qy, double dp) {
+  double denom = ((1 + dp) * (1 + dp) - qx * qx) - qy * qy;
+  if (denom <= 0)
+    return false;
+  denom = sqrt(denom);
+  xp = qx / denom;
+  yp = qy / denom;
+  return true;
+}
+
+/* offsetBeamCoordinatesForMisalignment (malign_mat.c:172-182) */
+__device__ __forceinline__ void offset_misalign(Part &p, double dx, double dy, double dz) {
+  p.s = p.s + dz * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+  p.x = (p.x - dx) + dz * p.xp;
+  p.y = (p.y - dy) + dz * p.yp;
+}
+
+/* rotateBeamCoordinatesForMisalignment (tilt_matrices.c:156-183), cos/sin precomputed */
+__device__ __forceinline__ void rotate_misalign(Part &p, double ca, double sa) {
+  double x = p.x, xp = p.xp, y = p.y, yp = p.yp;
+  p.x = x * ca + y * sa;
+  p.y = -x * sa + y * ca;
+  p.xp = xp * ca + yp * sa;
+  p.yp = -xp * sa + yp * ca;
+}
+
+/* ---- KQUAD / KSEXT: multipole_tracking2 (multipole.c:693-1117) with
+ * integrate_kick_multipole_ordn (multipole.c:1122-1410).  The reference
+ * always runs its radiation bookkeeping block (isr_coef is negated, not
+ * zeroed, when ISR is off, multipole.c:781-784), which divides and
+ * re-multiplies the canonical momenta by (1+delta) after each kick; that
+ * round trip is reproduced because it can move the last bit. */
+__device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g) {
+  const double *c = e.c;
+  const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = (int)c[KM_NSUB];
+  const double dx = c[KM_DX], dy = c[KM_DY];
+  double x, xp, y, yp, s, dp, qx, qy, denom;
+  int i_kick, step;
+
+  /* entrance misalignment, offsetParticlesForMisalignment mode 0 face 1 (malign_mat.c:491-497) */
+  if (e.flags & EF_ENTRANCE_OFFSET)
+    offset_misalign(p, dx, dy, c[KM_DZ]);
+  if (e.flags & EF_ENTRANCE_ROTATE)
+    rotate_misalign(p, c[KM_COS_TILT], c[KM_SIN_TILT]);
+
+  x = p.x;
+  xp = p.xp;
+  y = p.y;
+  yp = p.yp;
+  s = 0;
+  dp = p.dp;
+  if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp))
+    return LOSS_NAN;
+  if (fabs(x) > g.coord_limit || fabs(y) > g.coord_limit || fabs(xp) > g.slope_limit || fabs(yp) > g.slope_limit)
+    return LOSS_LIMIT;
+  /* convertSlopesToMomenta (multipole.h:250-259) */
+  denom = sqrt((1 + xp * xp) + yp * yp);
+  qx = ((1 + dp) * xp) / denom;
+  qy = ((1 + dp) * yp) / denom;
+  if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+    return LOSS_SLOPE;
+
+  for (i_kick = 0; i_kick < nSlices; i_kick++) {
+    if (!mult_aperture_ok(x + dx, y + dy, ap, e)) {
+      p.x = x;
+      p.y = y;
+      return LOSS_APERTURE;
+    }
+    for (step = 0; step < nSub; step++) {
+      const double dsh = c[KM_DSH0 + step];
+      const double kick = c[KM_KICK0 + step];
+      double sumFx, sumFy;
+      x = x + xp * dsh;
+      y = y + yp * dsh;
+      s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
+      if (step == nSub - 1) /* kickFrac[last] == 0 ends the slice */
+        break;
+      /* apply_canonical_multipole_kicks (multipole.h:213-245): coefficients
+       * (x+iy)^n/n! with signs; order 1: Fx=y, Fy=x; order 2: Fx=x*y,
+       * Fy=x^2/2-y^2/2, each accumulated from 0 in the reference's order. */
+      if (order == 1) {
+        sumFx = (1.0 * 1.0) * y;
+        sumFy = (1.0 * x) * 1.0;
+      } else {
+        double x2 = (1.0 * x) * x, y2 = (1.0 * y) * y;
+        sumFx = (1.0 * x) * y;
+        sumFy = (0.5 * x2) * 1.0;
+        sumFy = sumFy + (-0.5 * 1.0) * y2;
+      }
+      qx = qx - kick * sumFy;
+      qy = qy + kick * sumFx;
+      if (e.flags & (EF_QUAD_ORDER2 | EF_SKEW_ORDER2)) {
+        /* KSEXT K1/J1 terms: quadrupole order, normal then skew (multipole.c:1272-1275) */
+        if (e.flags & EF_QUAD_ORDER2) {
+          const double k1 = c[KM_KICK1_0 + step];
+          qx = qx - k1 * ((1.0 * x) * 1.0);
+          qy = qy + k1 * ((1.0 * 1.0) * y);
+        }
+        if (e.flags & EF_SKEW_ORDER2) {
+          const double j1 = c[KM_SKEW0 + step];
+          /* skew: swap(Fx, Fy), Fx = -Fx */
+          double fx = -((1.0 * x) * 1.0), fy = (1.0 * 1.0) * y;
+          qx = qx - j1 * fy;
+          qy = qy + j1 * fx;
+        }
+      }
+      if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+        return LOSS_SLOPE;
+      if (e.flags & EF_RADBLOCK) {
+        qx = qx / (1 + dp);
+        qy = qy / (1 + dp);
+        qx = qx * (1 + dp);
+        qy = qy * (1 + dp);
+        if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+          return LOSS_SLOPE;
+      }
+    }
+  }
+  if (!mult_aperture_ok(x + dx, y + dy, ap, e)) {
+    p.x = x;
+    p.y = y;
+    return LOSS_APERTURE;
+  }
+  if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+    return LOSS_SLOPE;
+  p.x = x;
+  p.xp = xp;
+  p.y = y;
+  p.yp = yp;
+  p.s = p.s + s;
+  p.dp = dp;
+  if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp))
+    return LOSS_NAN;
+  if (fabs(x) > g.coord_limit || fabs(y) > g.coord_limit || fabs(xp) > g.slope_limit || fabs(yp) > g.slope_limit)
+    return LOSS_LIMIT;
+  /* exit misalignment, face 2 (malign_mat.c:498-503) */
+  if (e.flags & EF_EXIT_MISALIGN) {
+    if (e.flags & EF_ENTRANCE_ROTATE)
+      rotate_misalign(p, c[KM_COS_TILT], -c[KM_SIN_TILT]);
+    if (e.flags & EF_ENTRANCE_OFFSET)
+      offset_misalign(p, -dx, -dy, -c[KM_DZ]);
+  }
+  return LOSS_NONE;
+}
+
+/* ---- CSBEND body: integrate_csbend_ordn (csbend.c:1434-1693) for the
+ * pure-dipole field (Fx = 0, Fy = 1, csbend.c:106-110).  Q = (X, QX, Y, QY,
+ * dist, DPoP).  `isr_block` reproduces the (QX/(1+d))*(1+d) round trip of
+ * the radiation block that the negated isrConstant always enables. */
+__device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y, double &QY, double &dist,
+                                                const double DPoP, const double *c, int nSlices, int nSub,
+                                                bool isr_block, const DevAperture *ap, const DevElem &e) {
+  const double rho0 = c[CB_RHO0], rho_actual = c[CB_RHO_ACTUAL];
+  int i, j;
+  dist = 0;
+  for (i = 0; i < nSlices; i++) {
+    if (!mult_aperture_ok(X, Y, ap, e))
+      return LOSS_APERTURE;
+    for (j = 0; j < nSub; j++) {
+      const double dsh = c[CB_DSH0 + j];
+      double f, sin_phi, phi, sine, cosi, tang, cos_phi, factor, arg;
+      f = (1 + DPoP) * (1 + DPoP) - QY * QY;
+      if (f <= 0)
+        return LOSS_SLOPE;
+      f = sqrt(f);
+      if (fabs(QX / f) > 1)
+        return LOSS_SLOPE;
+      sin_phi = QX / f;
+      phi = b2e_asin(sin_phi);
+      arg = dsh / rho0 + phi;
+      b2e_sincos(arg, &sine, &cosi);
+      if (cosi == 0)
+        return LOSS_SLOPE;
+      tang = sine / cosi;
+      cos_phi = b2e_cos(phi);
+      QX = f * sine;
+      factor = (((rho0 + X) * cos_phi) / f) * (tang - sin_phi / cos_phi);
+      Y = Y + QY * factor;
+      dist = dist + factor * (1 + DPoP);
+      f = cos_phi / cosi;
+      X = rho0 * (f - 1) + f * X;
+      if (j == nSub - 1) /* kickFrac[last] == 0 ends the slice */
+        break;
+      {
+        const double ds = c[CB_DS0 + j];
+        /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
+        QX = QX + ((((-ds) * (1 + X / rho0)) * 1.0) / rho_actual);
+        QY = QY + ((((ds) * (1 + X / rho0)) * 0.0) / rho_actual);
+        if (isr_block) {
+          QX = QX / (1 + DPoP);
+          QY = QY / (1 + DPoP);
+          QX = QX * (1 + DPoP);
+          QY = QY * (1 + DPoP);
+        }
+      }
+    }
+  }
+  if (!mult_aperture_ok(X, Y, ap, e))
+    return LOSS_APERTURE;
+  return LOSS_NONE;
+}
+
+/* ---- CSBEND: track_through_csbend (csbend.c:665-1409), malignMethod 0,
+ * edge method 1 at edge order 1, no synchrotron radiation. */
+__device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g) {
+  const double *c = e.c;
+  const double ct = c[CB_COS_TT], st = c[CB_SIN_TT];
+  const int nSlices = (int)c[CB_NSLICES], nSub = (int)c[CB_NSUB];
+  double x, y, xp, yp, s, dp, dp0, Q0, Q1, Q2, Q3, Q4, f, rho;
+  int lost;
+
+  /* element offsets and tilt (csbend.c:1108-1118) */
+  p.s = p.s + c[CB_DZI] * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+  p.x = (p.x + c[CB_DXI]) + c[CB_DZI] * p.xp;
+  p.y = (p.y + c[CB_DYI]) + c[CB_DZI] * p.yp;
+  x = p.x * ct + p.y * st;
+  y = -p.x * st + p.y * ct;
+  xp = p.xp * ct + p.yp * st;
+  yp = -p.xp * st + p.yp * ct;
+  s = p.s;
+  dp = dp0 = p.dp;
+
+  if (e.flags & EF_EDGE1) {
+    double delta_xp;
+    rho = (1 + dp) * c[CB_RHO_ACTUAL];
+    delta_xp = (c[CB_TAN_E1] / rho) * x;
+    xp = xp + delta_xp;
+    yp = yp - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * y;
+  }
+
+  /* convertToDipoleCanonicalCoordinates (csbend.c:1411-1419) */
+  f = (1 + dp) / sqrt((1 + xp * xp) + yp * yp);
+  Q0 = x;
+  Q1 = xp * f;
+  Q2 = y;
+  Q3 = yp * f;
+
+  lost = csbend_integrate(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e);
+
+  /* convertFromDipoleCanonicalCoordinates (csbend.c:1421-1429) */
+  f = 1 / sqrt(((1 + dp) * (1 + dp) - Q1 * Q1) - Q3 * Q3);
+  Q1 = Q1 * f;
+  Q3 = Q3 * f;
+  if (lost) {
+    p.x = Q0;
+    p.xp = Q1;
+    p.y = Q2;
+    p.yp = Q3;
+    return lost;
+  }
+
+  if (e.flags & EF_RADBLOCK) {
+    /* time-of-flight velocity fix (csbend.c:1259-1271), dp unchanged here */
+    double p0 = g.p_central * (1 + dp0), beta0 = p0 / sqrt(p0 * p0 + 1);
+    double p1 = g.p_central * (1 + dp), beta1 = p1 / sqrt(p1 * p1 + 1);
+    s = (beta1 * s) / beta0 + Q4;
+  } else
+    s = s + Q4;
+  x = Q0;
+  xp = Q1;
+  y = Q2;
+  yp = Q3;
+
+  if (e.flags & EF_EDGE2) {
+    double delta_xp;
+    rho = (1 + dp) * c[CB_RHO_ACTUAL];
+    delta_xp = (c[CB_TAN_E2] / rho) * x;
+    xp = xp + delta_xp;
+    yp = yp - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + dp)) / rho) * y;
+  }
+
+  /* back to the lab frame (csbend.c:1379-1388) */
+  p.x = (x * ct - y * st) + c[CB_ET0 + 0];
+  p.y = (x * st + y * ct) + c[CB_ET0 + 2];
+  p.xp = (xp * ct - yp * st) + c[CB_ET0 + 1];
+  p.yp = (xp * st + yp * ct) + c[CB_ET0 + 3];
+  p.s = s + c[CB_ET0 + 4];
+  p.dp = dp;
+  p.x = p.x + (c[CB_DXF] + c[CB_DZF] * p.xp);
+  p.y = p.y + (c[CB_DYF] + c[CB_DZF] * p.yp);
+  p.s = p.s + c[CB_DZF] * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+  return LOSS_NONE;
+}
+
+/* ---- RFCA, zero length, single kick: trackRfCavityWithWakes
+ * (simple_rfca.c:295-985) with add_to_particle_energy (:987-1006) and the
+ * final removeInvalidParticles sweep (limit_amplitudes.c:274-315). */
+__device__ __forceinline__ int rfca(Part &p, const DevElem &e, const DevRfState &rs, const DevGlobals &g) {
+  const double *c = e.c;
+  const double Po = g.p_central;
+  p.x = p.x - c[RF_DX];
+  p.y = p.y - c[RF_DY];
+  if (p.dp != -1) {
+    double P, gamma, beta_i, t, dgamma, gamma1, P1, Pz, Pz1, PRatio;
+    P = Po * (1 + p.dp);
+    gamma = sqrt(P * P + 1);
+    beta_i = P / gamma;
+    t = (p.s + 0.0) / (B2E_C_MKS * beta_i) - 0.0;
+    dgamma = (c[RF_VOLT] * b2e_sin(c[RF_OMEGA] * t + rs.phase)) * 1.0;
+    /* add_to_particle_energy */
+    gamma1 = gamma + dgamma;
+    if (gamma1 <= 1)
+      gamma1 = 1 + 1e-7;
+    P1 = sqrt(gamma1 * gamma1 - 1);
+    p.dp = (P1 - Po) / Po;
+    p.s = ((t * B2E_C_MKS) * P1) / gamma1;
+    Pz = P / sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+    Pz1 = sqrt((Pz * Pz + gamma1 * gamma1) - gamma * gamma);
+    PRatio = Pz / Pz1;
+    p.xp = p.xp * PRatio;
+    p.yp = p.yp * PRatio;
+    if (gamma + dgamma <= 1)
+      p.dp = -1;
+  }
+  p.x = p.x + c[RF_DX];
+  p.y = p.y + c[RF_DY];
+  if (isnan(p.x) || isnan(p.xp) || isnan(p.y) || isnan(p.yp) || isnan(p.s) || isnan(p.dp) || p.dp <= -1)
+    return LOSS_ENERGY;
+  return LOSS_NONE;
+}
+
+/* ---- apertures after each element (do_tracking.c:2455-2475) ----------
+ * mode 1: limit_amplitudes (limit_amplitudes.c:193-272), rectangular;
+ * mode 2: elimit_amplitudes (limit_amplitudes.c:472-600), super-elliptical.
+ * The host resolves elegant's fallbacks (elliptical with a zero half-axis
+ * falls back to rectangular; all-nonpositive half-axes check nothing). */
+__device__ __forceinline__ bool maxamp_ok(const Part &p, const DevAperture &a) {
+  if (a.mode == 1) {
+    bool out = (a.x_max > 0 && fabs(p.x) > a.x_max) || (a.y_max > 0 && fabs(p.y) > a.y_max);
+    if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))
+      out = true;
+    return !out;
+  }
+  if (a.mode == 2) {
+    if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))
+      return false;
+    return !((b2e_ipow(p.x, a.xe) / a.a2 + b2e_ipow(p.y, a.ye) / a.b2) > 1);
+  }
+  return true;
+}
+
+__device__ __forceinline__ bool finite_xy(const Part &p) {
+  /* limit_amplitudes(DBL_MAX, DBL_MAX): only inf/nan in x or y remove a particle */
+  return !(isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y));
+}
+
+#endif

@@ -1,0 +1,150 @@
+/*
+ * Internal data layout of the tracking engine (host and device).
+ *
+ * HBM layout: particles are six FP64 columns (x, xp, y, yp, s, delta), one
+ * int64 ID column and two int32 loss columns, each contiguous and 256-byte
+ * aligned, so a warp's 32 consecutive particles are one 256-byte transaction
+ * per column.  Batched ensembles store instance i's particles contiguously
+ * in [offset[i], offset[i+1]); the launch tiles each instance separately so
+ * a thread block never mixes instances.
+ *
+ * The lattice is "compiled" on the host into DevElem records: every constant
+ * the reference computes once per element call (KnL/nSlices*kickFrac,
+ * rho0, rho_actual, edge tangents, misalignment sines ...) is evaluated
+ * there, with the same expressions and the same elementary functions the
+ * reference uses, so the device only runs the per-particle arithmetic.  A
+ * block stages its instance's records in shared memory once per launch.
+ */
+#ifndef B2E_ENGINE_H
+#define B2E_ENGINE_H
+#include <stdint.h>
+#include "../../include/elegant_b200.h"
+
+#define B2E_NC 40 /* constants per compiled element */
+
+/* Compiled element kinds (device dispatch) */
+enum {
+  K_NONE = 0, /* MARK, CHARGE: no particle action */
+  K_DRIF_O1,  /* first-order drift matrix */
+  K_DRIF_O2,  /* second-order drift matrix (default_order 2) */
+  K_EDRIFT,
+  K_KMULT,    /* KQUAD / KSEXT, 4th-order (or 2nd) kick integrator */
+  K_CSBEND,
+  K_RFCA,
+  K_MAXAMP,
+  K_CSRCSBEND, /* collective: handled by the CSR driver, never in the ring kernel */
+  K_CSRDRIFT
+};
+
+/* Flags */
+#define EF_ENTRANCE_OFFSET 0x1  /* KMULT: dx||dy||dz at entrance */
+#define EF_ENTRANCE_ROTATE 0x2  /* KMULT: tilt at entrance */
+#define EF_EXIT_MISALIGN 0x4    /* KMULT: exit transform needed */
+#define EF_EDGE1 0x8            /* CSBEND: entrance edge (order 1, method 1) */
+#define EF_EDGE2 0x10           /* CSBEND: exit edge */
+#define EF_EXTRAPOLATE 0x20     /* aperture loss z-extrapolation (DRIF) */
+#define EF_NO_APERTURE 0x40     /* element class has NO_APERTURE */
+#define EF_RADBLOCK 0x80        /* the reference's radiation bookkeeping block runs (ISR coefficient nonzero) */
+#define EF_SKEW_ORDER2 0x100    /* KSEXT J1 term present */
+#define EF_QUAD_ORDER2 0x200    /* KSEXT K1 term present */
+#define EF_REVERSE_TILT 0x400   /* nonzero reverse tilt in the internal aperture check */
+
+/* KMULT constant slots */
+#define KM_ORDER 0       /* 1 quad, 2 sext */
+#define KM_NSLICES 1
+#define KM_NSUB 2        /* substeps per slice (4 for order-4 integration) */
+#define KM_DSH0 3        /* drift*driftFrac[j], j = 0..7 -> 3..10 */
+#define KM_KICK0 11      /* KnL/nSlices*kickFrac[j], j = 0..7 -> 11..18 (0 terminates) */
+#define KM_KICK1_0 19    /* secondary K1 term per substep, 19..25 (KSEXT K1) */
+#define KM_DX 27
+#define KM_DY 28
+#define KM_DZ 29
+#define KM_COS_TILT 30
+#define KM_SIN_TILT 31
+#define KM_REV_COS 32   /* reverse tilt cos/sin for the aperture check */
+#define KM_REV_SIN 33
+#define KM_SKEW0 34     /* J1 kick per substep 34..39 (first 6 substeps) */
+
+/* CSBEND constant slots */
+#define CB_RHO0 0
+#define CB_RHO_ACTUAL 1
+#define CB_NSLICES 2
+#define CB_NSUB 3
+#define CB_DSH0 4       /* s*driftFrac[j], 4..11 */
+#define CB_DS0 12       /* s*kickFrac[j], 12..19 (0 terminates) */
+#define CB_TAN_E1 20
+#define CB_E1 21
+#define CB_PSI1 22
+#define CB_TAN_E2 23
+#define CB_E2 24
+#define CB_PSI2 25
+#define CB_COS_TT 26
+#define CB_SIN_TT 27
+#define CB_DXI 28
+#define CB_DYI 29
+#define CB_DZI 30
+#define CB_DXF 31
+#define CB_DYF 32
+#define CB_DZF 33
+#define CB_ET0 34       /* dcoord_etilt[0..4] -> 34..38 */
+#define CB_REV_COS 39   /* reverse tilt cos/sin share slots with etilt? no: stored in aux */
+
+/* RFCA constant slots */
+#define RF_VOLT 0       /* volt/(1e6*mc^2[MV]*sign)/nKicks */
+#define RF_OMEGA 1
+#define RF_PHASE_DEG_RAD 2 /* rfca->phase*PI/180.0 */
+#define RF_DX 3
+#define RF_DY 4
+#define RF_T_REFERENCE 5
+#define RF_SOFFSET 6    /* length/2 used by the fiducial sum */
+#define RF_SLOT 7       /* index into the per-instance RF state table */
+
+/* DRIF / EDRIFT slots */
+#define DR_L 0
+#define DR_LH 1         /* L/2, the T[4][1][1] coefficient */
+
+typedef struct {
+  int32_t kind;
+  int32_t flags;
+  int32_t ap_pass0;   /* aperture record active during/after this element on pass 0 (-1: none) */
+  int32_t ap_later;   /* same, on later passes */
+  double z_start;     /* do_tracking last_z */
+  double z_end;       /* do_tracking z after the element */
+  double rev_cos, rev_sin; /* reverse tilt for internal aperture checks */
+  double c[B2E_NC];
+} DevElem;
+
+typedef struct {
+  double x_max, y_max;
+  double a2, b2;        /* ipow(x_max, xe), ipow(y_max, ye) */
+  int32_t elliptical, xe, ye;
+  int32_t mode; /* check after the element: 0 none, 1 rectangular, 2 elliptical */
+} DevAperture;
+
+/* Per RFCA per instance: fiducial time and phase (phase_reference.c state). */
+typedef struct {
+  double t0;      /* -phase_fiducial/omega */
+  double phase;   /* phase_fiducial + PHASE*PI/180 */
+  int32_t set, pad;
+} DevRfState;
+
+/* Launch description of one tile: a block tracks particles [start, start+count) of instance inst. */
+typedef struct {
+  int64_t start;
+  int32_t count;
+  int32_t inst;
+} DevTile;
+
+typedef struct {
+  double *x, *xp, *y, *yp, *s, *dp;
+  int32_t *lost_pass;
+  int32_t *lost_elem;
+} DevParticles;
+
+typedef struct {
+  double p_central;
+  double coord_limit;
+  double slope_limit;
+} DevGlobals;
+
+#endif

@@ -1,0 +1,33 @@
+/*
+ * Launch interfaces of the tracking kernels (b2e_ring.cu) used by the host
+ * orchestration (b2e_capi.cu).
+ */
+#ifndef B2E_KERNELS_H
+#define B2E_KERNELS_H
+#include <cuda_runtime.h>
+#include "b2e_engine.h"
+
+namespace b2e {
+
+struct RingLaunch {
+  DevParticles P;
+  const DevTile *tiles;
+  const DevElem *elems;     /* [n_inst][n_elems] */
+  const DevAperture *aps;   /* [n_inst][n_aps] */
+  const DevRfState *rf;     /* [n_inst][n_rf] */
+  int n_elems, n_aps, n_rf;
+  int pass_begin, elem_begin; /* first (pass, element) tracked */
+  int pass_end, elem_end;     /* last pass tracked, and one past its last element */
+  DevGlobals g;
+  unsigned int *error_flag;
+};
+
+cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream);
+cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
+                            int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
+                            cudaStream_t stream);
+cudaError_t launch_effort(const int32_t *lost_pass, int64_t n, int pass_begin, int pass_end, unsigned long long *effort,
+                          unsigned long long *survivors, cudaStream_t stream);
+
+} // namespace b2e
+#endif

@@ -1,0 +1,448 @@
+/*
+ * Lattice compilation on the host (see b2e_lattice.h).
+ */
+#include <math.h>
+#include <string.h>
+#include <string>
+#include "b2e_lattice.h"
+#include "b2e_math.h"
+
+namespace b2e {
+
+static const double kPI = 3.141592653589793238462643383279502884;
+static const double kME_MEV = 0.51099895000; /* electron rest energy, MeV (CODATA 2018) */
+static const double kBETA = 1.25992104989487316477; /* 2^(1/3), multipole.c:1119, csbend.c:1431 */
+
+/* Symplectic integrator step fractions: multipole.c:1140-1182, csbend.c:1453-1488. */
+static int integrator_fractions(int order, double *drift, double *kick) {
+  static const double d6[8] = {0.39225680523878,     0.5100434119184585, -0.47105338540975655, 0.0687531682525181,
+                               0.0687531682525181,   -0.47105338540975655, 0.5100434119184585, 0.39225680523878};
+  static const double k6[8] = {0.784513610477560, 0.235573213359357, -1.17767998417887, 1.3151863206839063,
+                               -1.17767998417887, 0.235573213359357, 0.784513610477560, 0};
+  int j;
+  switch (order) {
+  case 2:
+    drift[0] = drift[1] = 0.5;
+    kick[0] = 1.0;
+    kick[1] = 0.0;
+    return 2;
+  case 4:
+    drift[0] = 0.5 / (2 - kBETA);
+    drift[1] = (1 - kBETA) / (2 - kBETA) / 2;
+    drift[2] = (1 - kBETA) / (2 - kBETA) / 2;
+    drift[3] = 0.5 / (2 - kBETA);
+    kick[0] = 1. / (2 - kBETA);
+    kick[1] = -kBETA / (2 - kBETA);
+    kick[2] = 1 / (2 - kBETA);
+    kick[3] = 0;
+    return 4;
+  case 6:
+    for (j = 0; j < 8; j++) {
+      drift[j] = d6[j];
+      kick[j] = k6[j];
+    }
+    return 8;
+  default:
+    return 0;
+  }
+}
+
+static double ipow_host(double x, long n) {
+  double r = x;
+  long i;
+  if (n == 0)
+    return 1;
+  for (i = 1; i < n; i++)
+    r *= x;
+  return r;
+}
+
+/* rotateBeamCoordinatesForMisalignment's special angles (tilt_matrices.c:160-176) */
+static void rotation_cs(double angle, double *c, double *s) {
+  if (fabs(fabs(angle) - kPI) < 1e-12) {
+    *c = -1;
+    *s = 0;
+  } else if (fabs(angle - kPI / 2) < 1e-12) {
+    *c = 0;
+    *s = 1;
+  } else if (fabs(angle + kPI / 2) < 1e-12) {
+    *c = 0;
+    *s = -1;
+  } else {
+    *c = b2e_cos(angle);
+    *s = b2e_sin(angle);
+  }
+}
+
+void element_defaults(int type, double *p) {
+  for (int i = 0; i < B2E_MAX_PARAMS; i++)
+    p[i] = 0;
+  switch (type) {
+  case B2E_KQUAD:
+  case B2E_KSEXT:
+    p[B2E_KMULT_N_SLICES] = 1;          /* track_data.c:1234, :1130 */
+    p[B2E_KMULT_INTEGRATION_ORDER] = 4; /* :1253, :1153 */
+    break;
+  case B2E_CSBEND:
+  case B2E_CSRCSBEND:
+    p[B2E_BEND_FINT] = 0.5;             /* DEFAULT_FINT, track.h:1214 */
+    p[B2E_BEND_N_SLICES] = 4;           /* DEFAULT_N_SLICES, track.h:1229 */
+    p[B2E_BEND_INTEGRATION_ORDER] = 4;
+    p[B2E_BEND_EDGE1_EFFECTS] = 1;
+    p[B2E_BEND_EDGE2_EFFECTS] = 1;
+    p[B2E_BEND_EDGE_ORDER] = 1;
+    p[B2E_BEND_BIN_RANGE_FACTOR] = 1.2; /* csrcsbend_param, track_data.c:1982-2060 */
+    p[B2E_BEND_SG_ORDER] = 1;
+    p[B2E_BEND_TRAPAZOID_INTEGRATION] = 1;
+    p[B2E_BEND_CSR] = 1;
+    p[B2E_BEND_CLIP_NEGATIVE_BINS] = 1;
+    break;
+  case B2E_RFCA:
+    p[B2E_RFCA_FREQ] = 500e6;           /* track_data.c:580 */
+    p[B2E_RFCA_T_REFERENCE] = -1;
+    break;
+  case B2E_MAXAMP:
+    p[B2E_MAXAMP_EXPONENT] = 2;         /* track_data.c:990-997 */
+    break;
+  case B2E_CSRDRIFT:
+    p[B2E_CSRDRIFT_N_KICKS] = 1;
+    p[B2E_CSRDRIFT_CSR] = 1;
+    break;
+  default:
+    break;
+  }
+}
+
+static bool is_bend(int t) { return t == B2E_CSBEND || t == B2E_CSRCSBEND; }
+
+/* determine_bend_flags (bend_matrix.c:1342-1391): edges are skipped where an
+ * identically named bend of the same type follows/precedes (MARK between is
+ * transparent). */
+static void bend_edge_flags(const b2e_element *el, int n, int i, bool *edge1, bool *edge2) {
+  bool same_pre = false, same_post = false;
+  for (int j = i - 1; j >= 0; j--) {
+    if (el[j].type == el[i].type && strncmp(el[j].name, el[i].name, sizeof(el[i].name)) == 0) {
+      same_pre = true;
+      break;
+    }
+    if (el[j].type != B2E_MARK)
+      break;
+  }
+  for (int j = i + 1; j < n; j++) {
+    if (el[j].type == el[i].type && strncmp(el[j].name, el[i].name, sizeof(el[i].name)) == 0) {
+      same_post = true;
+      break;
+    }
+    if (el[j].type != B2E_MARK)
+      break;
+  }
+  *edge1 = el[i].p[B2E_BEND_EDGE1_EFFECTS] != 0 && !same_pre;
+  *edge2 = el[i].p[B2E_BEND_EDGE2_EFFECTS] != 0 && !same_post;
+}
+
+static std::string compile_kmult(const b2e_element &el, DevElem &d) {
+  const double *p = el.p;
+  double drift_frac[8], kick_frac[8];
+  const double L = p[B2E_KMULT_L];
+  int integ = (int)p[B2E_KMULT_INTEGRATION_ORDER];
+  long n_kicks = (long)p[B2E_KMULT_N_KICKS], nSlices = (long)p[B2E_KMULT_N_SLICES];
+  int nSub = integrator_fractions(integ, drift_frac, kick_frac);
+  double KnL, drift;
+  if (!nSub)
+    return "multipole INTEGRATION_ORDER must be 2, 4, or 6";
+  if (n_kicks <= 0) {
+    if (nSlices <= 0)
+      return "N_KICKS<=0 and N_SLICES<=0 in multipole tracking";
+  } else if (integ > 2) {
+    if ((nSlices = (long)ceil(n_kicks / (1.0 * integ))) < 1)
+      nSlices = 1;
+  } else
+    nSlices = n_kicks;
+  d.kind = K_KMULT;
+  d.c[KM_ORDER] = el.type == B2E_KQUAD ? 1 : 2;
+  d.c[KM_NSLICES] = (double)nSlices;
+  d.c[KM_NSUB] = nSub;
+  KnL = (p[B2E_KMULT_K] * L) * (1 + p[B2E_KMULT_FSE]);
+  drift = L / nSlices;
+  for (int j = 0; j < 8; j++) {
+    d.c[KM_DSH0 + j] = j < nSub ? drift * drift_frac[j] : 0;
+    d.c[KM_KICK0 + j] = j < nSub ? KnL / nSlices * kick_frac[j] : 0;
+  }
+  /* a zero KnL kick is skipped by the reference ("if (KnL[iOrder])"); here it
+   * subtracts an exact zero, which leaves the momenta unchanged */
+  if (el.type == B2E_KSEXT) {
+    if (p[B2E_KMULT_K1_OF_KSEXT] != 0) {
+      double K1L = p[B2E_KMULT_K1_OF_KSEXT] * L;
+      d.flags |= EF_QUAD_ORDER2;
+      for (int j = 0; j < 8; j++)
+        d.c[KM_KICK1_0 + j] = j < nSub ? K1L / nSlices * kick_frac[j] : 0;
+    }
+    if (p[B2E_KMULT_J1_OF_KSEXT] != 0) {
+      double J1L = p[B2E_KMULT_J1_OF_KSEXT] * L;
+      if (nSub > 6)
+        return "KSEXT J1 with INTEGRATION_ORDER=6 is not supported";
+      d.flags |= EF_SKEW_ORDER2;
+      for (int j = 0; j < 6; j++)
+        d.c[KM_SKEW0 + j] = j < nSub ? J1L / nSlices * kick_frac[j] : 0;
+    }
+  }
+  d.c[KM_DX] = p[B2E_KMULT_DX];
+  d.c[KM_DY] = p[B2E_KMULT_DY];
+  d.c[KM_DZ] = p[B2E_KMULT_DZ];
+  if (p[B2E_KMULT_DX] != 0 || p[B2E_KMULT_DY] != 0 || p[B2E_KMULT_DZ] != 0)
+    d.flags |= EF_ENTRANCE_OFFSET | EF_EXIT_MISALIGN;
+  if (p[B2E_KMULT_TILT] != 0) {
+    d.flags |= EF_ENTRANCE_ROTATE | EF_EXIT_MISALIGN;
+    rotation_cs(p[B2E_KMULT_TILT], &d.c[KM_COS_TILT], &d.c[KM_SIN_TILT]);
+    /* setupMultApertureData(-tilt): reverseTiltCS = cos(-tilt), sin(-tilt) */
+    d.flags |= EF_REVERSE_TILT;
+    d.rev_cos = b2e_cos(-p[B2E_KMULT_TILT]);
+    d.rev_sin = b2e_sin(-p[B2E_KMULT_TILT]);
+  }
+  /* isr_coef is nonzero (negated when ISR is off), so the radiation block
+   * runs whenever the slice drift is nonzero (multipole.c:1320) */
+  if (drift != 0)
+    d.flags |= EF_RADBLOCK;
+  return "";
+}
+
+static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, DevElem &d) {
+  const double *p = el.p;
+  double drift_frac[8], kick_frac[8];
+  const double length = p[B2E_BEND_L];
+  double angle, e1, e2, tilt, etilt, rho0, h, fse, rho_actual, Kg, psi1, psi2, ttilt, ct, st, s;
+  int integ = (int)p[B2E_BEND_INTEGRATION_ORDER], nSub, nSlices = (int)p[B2E_BEND_N_SLICES];
+  if (p[B2E_BEND_ANGLE] == 0) {
+    d.kind = K_EDRIFT;
+    d.c[DR_L] = length;
+    return "";
+  }
+  nSub = integrator_fractions(integ, drift_frac, kick_frac);
+  if (!nSub)
+    return "CSBEND integration_order is invalid--must be 2, 4, or 6";
+  if (nSlices < 1)
+    return "CSBEND N_SLICES must be >= 1";
+  if (p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0)
+    return "CSBEND with K1/K2 field terms is not supported by this engine";
+  if ((edge1 || edge2) && p[B2E_BEND_EDGE_ORDER] > 1)
+    return "CSBEND EDGE_ORDER>1 is not supported by this engine";
+  if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
+    return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
+  /* csbend.c:933-950: negative angle folded into a PI tilt */
+  if (p[B2E_BEND_ANGLE] < 0) {
+    angle = -p[B2E_BEND_ANGLE];
+    e1 = -p[B2E_BEND_E1];
+    e2 = -p[B2E_BEND_E2];
+    etilt = p[B2E_BEND_ETILT] * 1; /* etiltSign = 1 */
+    tilt = p[B2E_BEND_TILT] + kPI;
+    rho0 = length / angle;
+  } else {
+    angle = p[B2E_BEND_ANGLE];
+    e1 = p[B2E_BEND_E1];
+    e2 = p[B2E_BEND_E2];
+    etilt = p[B2E_BEND_ETILT] * 1;
+    tilt = p[B2E_BEND_TILT];
+    rho0 = length / angle;
+  }
+  if (fabs(rho0) > 1e6)
+    return "CSBEND with radius > 1e6 is not supported (use EDRIFT)";
+  if (etilt != 0)
+    return "CSBEND ETILT is not supported by this engine";
+  fse = p[B2E_BEND_FSE] + 0.0;
+  h = 1 / rho0;
+  if (fabs(fse + 1) < 1e-12)
+    fse = -1 + 1e-12;
+  rho_actual = 1 / ((1 + fse) * h);
+  /* fringe angles (csbend.c:985-991); FINT1/FINT2 default to FINT */
+  Kg = 2 * p[B2E_BEND_HGAP] * p[B2E_BEND_FINT] * (rho0 < 0 ? -1 : 1);
+  psi1 = Kg / fabs(rho_actual) / b2e_cos(e1) * (1 + b2e_sin(e1) * b2e_sin(e1));
+  psi2 = Kg / fabs(rho_actual) / b2e_cos(e2) * (1 + b2e_sin(e2) * b2e_sin(e2));
+  if (length < 0) {
+    psi1 *= -1;
+    psi2 *= -1;
+  }
+  /* total tilt (csbend.c:1051-1066) */
+  ttilt = tilt + etilt;
+  if (ttilt == 0) {
+    ct = 1;
+    st = 0;
+  } else if (fabs(fabs(ttilt) - kPI) < 1e-12) {
+    ct = -1;
+    st = 0;
+  } else if (fabs(ttilt - kPI / 2) < 1e-12) {
+    ct = 0;
+    st = 1;
+  } else if (fabs(ttilt + kPI / 2) < 1e-12) {
+    ct = 0;
+    st = -1;
+  } else {
+    ct = b2e_cos(ttilt);
+    st = b2e_sin(ttilt);
+  }
+  d.kind = el.type == B2E_CSBEND ? K_CSBEND : K_CSRCSBEND;
+  d.c[CB_RHO0] = rho0;
+  d.c[CB_RHO_ACTUAL] = rho_actual;
+  d.c[CB_NSLICES] = nSlices;
+  d.c[CB_NSUB] = nSub;
+  s = length / nSlices; /* integrate_csbend_ordn: s /= n */
+  if (el.type == B2E_CSRCSBEND)
+    s = (length / nSlices) / 1; /* track_through_csbendCSR integrates one slice of length/nSlices per kick */
+  for (int j = 0; j < 8; j++) {
+    d.c[CB_DSH0 + j] = j < nSub ? s * drift_frac[j] : 0;
+    d.c[CB_DS0 + j] = j < nSub ? s * kick_frac[j] : 0;
+  }
+  d.c[CB_TAN_E1] = b2e_tan(e1);
+  d.c[CB_E1] = e1;
+  d.c[CB_PSI1] = psi1;
+  d.c[CB_TAN_E2] = b2e_tan(e2);
+  d.c[CB_E2] = e2;
+  d.c[CB_PSI2] = psi2;
+  d.c[CB_COS_TT] = ct;
+  d.c[CB_SIN_TT] = st;
+  /* malignMethod 0 offsets (csbend.c:1070-1082) */
+  d.c[CB_DXI] = -p[B2E_BEND_DX];
+  d.c[CB_DZI] = p[B2E_BEND_DZ];
+  d.c[CB_DYI] = -p[B2E_BEND_DY];
+  d.c[CB_DXF] = p[B2E_BEND_DX] * b2e_cos(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * b2e_sin(p[B2E_BEND_ANGLE]);
+  d.c[CB_DZF] = p[B2E_BEND_DX] * b2e_sin(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * b2e_cos(p[B2E_BEND_ANGLE]);
+  d.c[CB_DYF] = p[B2E_BEND_DY];
+  for (int j = 0; j < 5; j++)
+    d.c[CB_ET0 + j] = 0; /* computeEtiltCentroidOffset with etilt = 0 */
+  if (edge1)
+    d.flags |= EF_EDGE1;
+  if (edge2)
+    d.flags |= EF_EDGE2;
+  if (-tilt != 0) {
+    d.flags |= EF_REVERSE_TILT;
+    d.rev_cos = b2e_cos(-tilt);
+    d.rev_sin = b2e_sin(-tilt);
+  }
+  /* isrConstant is nonzero for CSBEND (negated when ISR is off,
+   * csbend.c:962-965); CSRCSBEND sets it to 0 unless ISR is on (:2138-2142) */
+  if (el.type == B2E_CSBEND)
+    d.flags |= EF_RADBLOCK;
+  return "";
+}
+
+static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
+  const double *p = el.p;
+  if (p[B2E_RFCA_L] != 0)
+    return "RFCA with nonzero length is not supported by this engine";
+  if (p[B2E_RFCA_FREQ] == 0)
+    return "RFCA with zero frequency is not supported by this engine";
+  d.kind = K_RFCA;
+  /* volt = VOLT/(1e6*particleMassMV*particleRelSign)/nKicks, omega = PIx2*FREQ (simple_rfca.c:384-394) */
+  d.c[RF_VOLT] = p[B2E_RFCA_VOLT] / (1e6 * kME_MEV * 1) / 1;
+  d.c[RF_OMEGA] = (2 * kPI) * p[B2E_RFCA_FREQ];
+  d.c[RF_PHASE_DEG_RAD] = p[B2E_RFCA_PHASE] * kPI / 180.0;
+  d.c[RF_DX] = p[B2E_RFCA_DX];
+  d.c[RF_DY] = p[B2E_RFCA_DY];
+  d.c[RF_T_REFERENCE] = p[B2E_RFCA_T_REFERENCE];
+  d.c[RF_SOFFSET] = 0.0 / 2; /* length/2 with length 0 */
+  d.c[RF_SLOT] = slot;
+  return "";
+}
+
+std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options &opt, CompiledLattice &out) {
+  out = CompiledLattice();
+  out.elems.resize(n);
+  int last_ap = -1;
+  double z = 0;
+  for (int i = 0; i < n; i++) {
+    DevElem &d = out.elems[i];
+    memset(&d, 0, sizeof(d));
+    d.ap_pass0 = d.ap_later = -1;
+    std::string err;
+    const double *p = el[i].p;
+    d.z_start = z;
+    switch (el[i].type) {
+    case B2E_DRIF: {
+      int order = p[B2E_DRIF_ORDER] != 0 ? (int)p[B2E_DRIF_ORDER] : opt.default_order;
+      d.kind = order >= 2 ? K_DRIF_O2 : K_DRIF_O1;
+      d.c[DR_L] = p[B2E_DRIF_L];
+      d.c[DR_LH] = p[B2E_DRIF_L] / 2;
+      d.flags |= EF_EXTRAPOLATE;
+      z += p[B2E_DRIF_L];
+      break;
+    }
+    case B2E_EDRIFT:
+      d.kind = K_EDRIFT;
+      d.c[DR_L] = p[B2E_EDRIFT_L];
+      z += p[B2E_EDRIFT_L];
+      break;
+    case B2E_KQUAD:
+    case B2E_KSEXT:
+      err = compile_kmult(el[i], d);
+      z += p[B2E_KMULT_L];
+      break;
+    case B2E_CSBEND:
+    case B2E_CSRCSBEND: {
+      bool e1, e2;
+      bend_edge_flags(el, n, i, &e1, &e2);
+      err = compile_csbend(el[i], e1, e2, d);
+      if (el[i].type == B2E_CSRCSBEND && d.kind == K_CSRCSBEND)
+        out.csr_elements.push_back(i);
+      z += p[B2E_BEND_L];
+      break;
+    }
+    case B2E_RFCA:
+      err = compile_rfca(el[i], out.n_rf, d);
+      out.rf_elements.push_back(i);
+      out.n_rf++;
+      z += p[B2E_RFCA_L];
+      break;
+    case B2E_MAXAMP: {
+      DevAperture a;
+      memset(&a, 0, sizeof(a));
+      int xe = (int)p[B2E_MAXAMP_EXPONENT], ye = (int)p[B2E_MAXAMP_Y_EXPONENT];
+      a.x_max = p[B2E_MAXAMP_X_MAX];
+      a.y_max = p[B2E_MAXAMP_Y_MAX];
+      a.elliptical = p[B2E_MAXAMP_ELLIPTICAL] != 0;
+      a.xe = xe;
+      a.ye = ye ? ye : xe;
+      if (a.x_max != 0 || a.y_max != 0) {
+        if (!a.elliptical)
+          a.mode = (a.x_max < 0 && a.y_max < 0) ? 0 : 1;
+        else if (a.x_max <= 0 || a.y_max <= 0)
+          a.mode = (a.x_max > 0 || a.y_max > 0) ? 1 : 0;
+        else {
+          if (a.xe < 2 || a.xe % 2 || a.ye < 2 || a.ye % 2)
+            err = "MAXAMP exponent must be an even integer >= 2";
+          a.mode = 2;
+          a.a2 = ipow_host(a.x_max, a.xe);
+          a.b2 = ipow_host(a.y_max, a.ye);
+        }
+      }
+      last_ap = (int)out.aps.size();
+      out.aps.push_back(a);
+      d.kind = K_MAXAMP;
+      break;
+    }
+    case B2E_MARK:
+    case B2E_CHARGE:
+      d.kind = K_NONE;
+      d.flags |= EF_NO_APERTURE;
+      break;
+    case B2E_CSRDRIFT:
+      d.kind = K_CSRDRIFT;
+      d.c[0] = p[B2E_CSRDRIFT_L];
+      out.csr_elements.push_back(i);
+      z += p[B2E_CSRDRIFT_L];
+      break;
+    default:
+      err = "unsupported element type";
+    }
+    if (!err.empty())
+      return std::string("element ") + std::to_string(i) + " (" + std::string(el[i].name, strnlen(el[i].name, 32)) +
+             "): " + err;
+    d.ap_pass0 = last_ap;
+    d.z_end = z;
+  }
+  /* sticky MAXAMP carries over into later passes (do_tracking keeps x_max etc.) */
+  for (int i = 0; i < n; i++)
+    out.elems[i].ap_later = out.elems[i].ap_pass0 >= 0 ? out.elems[i].ap_pass0 : last_ap;
+  out.total_length = z;
+  return "";
+}
+
+} // namespace b2e

@@ -1,0 +1,200 @@
+/*
+ * FP64 elementary functions shared bit-for-bit by the CUDA kernels and the
+ * CPU oracles (compiled as __host__ __device__ by nvcc, as plain C by gcc).
+ *
+ * Why: the tracking path calls sin/cos/asin/tan in every CSBEND substep
+ * (csbend.c:1566-1574) and sin in RFCA (simple_rfca.c:560-573).  Library
+ * implementations on the host (glibc) and on the device differ by an ulp now
+ * and then, and over 1,000 turns those ulps grow.  With one implementation on
+ * both sides the GPU reproduces the CPU oracle bit-for-bit; the oracle built
+ * with glibc instead measures how far this implementation drifts from libm.
+ *
+ * Methods (all from the mathematics, coefficients derived here):
+ *  - sin/cos: Cody & Waite (1980) additive range reduction by pi/2 split into
+ *    three doubles (the first product is exact under fma), then the Taylor
+ *    series of sin and cos on |r| <= pi/4 truncated where the remainder is
+ *    below 2^-60 relative; 1 - r^2/2 is evaluated with the compensated
+ *    splitting used by Sun's fdlibm kernel cosine.
+ *  - asin: Taylor series  asin(x) = sum C(2n,n) x^(2n+1) / (4^n (2n+1))  on
+ *    |x| <= 1/2 (10 terms for |x| <= 1/8, 28 terms beyond), and
+ *    asin(x) = pi/2 - 2 asin(sqrt((1-x)/2)) for 1/2 < |x| <= 1.
+ *  - tan = sin/cos from the shared reduction.
+ *  - pow(x, 1/3.) (the CSR denominators, csbend.c:2575) is in b2e_csr_math.h.
+ * All polynomial evaluation uses explicit fma, so the result does not depend
+ * on the compiler's contraction setting.
+ */
+#ifndef B2E_MATH_H
+#define B2E_MATH_H
+
+#ifdef __CUDACC__
+#define B2E_HD __host__ __device__ __forceinline__
+#else
+#include <math.h>
+#define B2E_HD static inline
+#endif
+
+/* pi/2 = B2E_PIO2_1 + B2E_PIO2_2 + B2E_PIO2_3 (successive 53-bit pieces) */
+#define B2E_PIO2_1 0x1.921fb54442d18p+0
+#define B2E_PIO2_2 0x1.1a62633145c07p-54
+#define B2E_PIO2_3 (-0x1.f1976b7ed8fbcp-110)
+#define B2E_TWO_OVER_PI 0x1.45f306dc9c883p-1
+#define B2E_PIO4 0x1.921fb54442d18p-1
+
+B2E_HD double b2e_fma(double a, double b, double c) { return fma(a, b, c); }
+
+/* sin(r) for |r| <= pi/4: r + r^3 * sum_{n>=1} (-1)^n r^(2n-2) / (2n+1)!  (to r^19) */
+B2E_HD double b2e_sin_kernel(double r) {
+  double w = r * r, p;
+  p = -1.0 / 121645100408832000.0;          /* -1/19! */
+  p = b2e_fma(p, w, 1.0 / 355687428096000.0); /* 1/17! */
+  p = b2e_fma(p, w, -1.0 / 1307674368000.0);  /* -1/15! */
+  p = b2e_fma(p, w, 1.0 / 6227020800.0);      /* 1/13! */
+  p = b2e_fma(p, w, -1.0 / 39916800.0);       /* -1/11! */
+  p = b2e_fma(p, w, 1.0 / 362880.0);          /* 1/9! */
+  p = b2e_fma(p, w, -1.0 / 5040.0);           /* -1/7! */
+  p = b2e_fma(p, w, 1.0 / 120.0);             /* 1/5! */
+  p = b2e_fma(p, w, -1.0 / 6.0);              /* -1/3! */
+  return b2e_fma(r * w, p, r);
+}
+
+/* cos(r) for |r| <= pi/4: 1 - r^2/2 + r^4 * sum_{n>=0} (-1)^n r^(2n) / (2n+4)!  (to r^20) */
+B2E_HD double b2e_cos_kernel(double r) {
+  double w = r * r, q, hw, t;
+  q = 1.0 / 2432902008176640000.0;             /* 1/20! */
+  q = b2e_fma(q, w, -1.0 / 6402373705728000.0); /* -1/18! */
+  q = b2e_fma(q, w, 1.0 / 20922789888000.0);    /* 1/16! */
+  q = b2e_fma(q, w, -1.0 / 87178291200.0);      /* -1/14! */
+  q = b2e_fma(q, w, 1.0 / 479001600.0);         /* 1/12! */
+  q = b2e_fma(q, w, -1.0 / 3628800.0);          /* -1/10! */
+  q = b2e_fma(q, w, 1.0 / 40320.0);             /* 1/8! */
+  q = b2e_fma(q, w, -1.0 / 720.0);              /* -1/6! */
+  q = b2e_fma(q, w, 1.0 / 24.0);                /* 1/4! */
+  hw = 0.5 * w;
+  t = 1.0 - hw;
+  /* (1 - t) - hw recovers the rounding error of t exactly */
+  return t + (((1.0 - t) - hw) + (w * w) * q);
+}
+
+/* Reduce x to r in [-pi/4, pi/4] and the quadrant k mod 4. */
+B2E_HD double b2e_reduce_pio2(double x, int *quadrant) {
+  double k, r;
+  if (fabs(x) <= B2E_PIO4) {
+    *quadrant = 0;
+    return x;
+  }
+  k = rint(x * B2E_TWO_OVER_PI);
+  r = b2e_fma(-k, B2E_PIO2_1, x); /* exact */
+  r = b2e_fma(-k, B2E_PIO2_2, r);
+  r = b2e_fma(-k, B2E_PIO2_3, r);
+  *quadrant = (int)((long long)k & 3);
+  return r;
+}
+
+B2E_HD void b2e_sincos(double x, double *s, double *c) {
+  int q;
+  double r = b2e_reduce_pio2(x, &q), sr, cr;
+  sr = b2e_sin_kernel(r);
+  cr = b2e_cos_kernel(r);
+  switch (q) {
+  case 0:
+    *s = sr;
+    *c = cr;
+    break;
+  case 1:
+    *s = cr;
+    *c = -sr;
+    break;
+  case 2:
+    *s = -sr;
+    *c = -cr;
+    break;
+  default:
+    *s = -cr;
+    *c = sr;
+    break;
+  }
+  if (x != x) { /* NaN in, NaN out */
+    *s = x;
+    *c = x;
+  }
+}
+
+/* Single-result variants: same reduction and kernels as b2e_sincos, so each
+ * returns bit-for-bit the corresponding member of the pair. */
+B2E_HD double b2e_sin(double x) {
+  int q;
+  double r = b2e_reduce_pio2(x, &q), v;
+  if (x != x)
+    return x;
+  v = (q & 1) ? b2e_cos_kernel(r) : b2e_sin_kernel(r);
+  return (q & 2) ? -v : v;
+}
+
+B2E_HD double b2e_cos(double x) {
+  int q;
+  double r = b2e_reduce_pio2(x, &q), v;
+  if (x != x)
+    return x;
+  v = (q & 1) ? b2e_sin_kernel(r) : b2e_cos_kernel(r);
+  return (q == 1 || q == 2) ? -v : v;
+}
+
+B2E_HD double b2e_tan(double x) {
+  double s, c;
+  b2e_sincos(x, &s, &c);
+  return s / c;
+}
+
+/* asin(x) - x = x^3 * P(x^2) for |x| <= 1/8; coefficients C(2n,n)/((2n+1) 4^n), n = 1..10 */
+B2E_HD double b2e_asin_small(double x) {
+  double w = x * x, p;
+  p = (184756.0 / 21.0) * 0x1p-20;           /* n=10 */
+  p = b2e_fma(p, w, (48620.0 / 19.0) * 0x1p-18); /* n=9 */
+  p = b2e_fma(p, w, (12870.0 / 17.0) * 0x1p-16); /* n=8 */
+  p = b2e_fma(p, w, (3432.0 / 15.0) * 0x1p-14);  /* n=7 */
+  p = b2e_fma(p, w, (924.0 / 13.0) * 0x1p-12);   /* n=6 */
+  p = b2e_fma(p, w, (252.0 / 11.0) * 0x1p-10);   /* n=5 */
+  p = b2e_fma(p, w, (70.0 / 9.0) * 0x1p-8);     /* n=4 */
+  p = b2e_fma(p, w, (20.0 / 7.0) * 0x1p-6);     /* n=3 */
+  p = b2e_fma(p, w, (6.0 / 5.0) * 0x1p-4);       /* n=2 */
+  p = b2e_fma(p, w, (2.0 / 3.0) * 0x1p-2);       /* n=1 */
+  return b2e_fma(x * w, p, x);
+}
+
+/* Same series to n = 28 for 1/8 < |x| <= 1/2 (remainder < 2^-58 relative). */
+B2E_HD double b2e_asin_mid(double x) {
+  /* C(2n,n)/(2n+1) for n = 1..28; the 4^-n factor is applied by scaling w. */
+  const double c[28] = {
+    2.0 / 3.0, 6.0 / 5.0, 20.0 / 7.0, 70.0 / 9.0, 252.0 / 11.0, 924.0 / 13.0, 3432.0 / 15.0,
+    12870.0 / 17.0, 48620.0 / 19.0, 184756.0 / 21.0, 705432.0 / 23.0, 2704156.0 / 25.0,
+    10400600.0 / 27.0, 40116600.0 / 29.0, 155117520.0 / 31.0, 601080390.0 / 33.0,
+    2333606220.0 / 35.0, 9075135300.0 / 37.0, 35345263800.0 / 39.0, 137846528820.0 / 41.0,
+    538257874440.0 / 43.0, 2104098963720.0 / 45.0, 8233430727600.0 / 47.0,
+    32247603683100.0 / 49.0, 126410606437752.0 / 51.0, 495918532948104.0 / 53.0,
+    1946939425648112.0 / 55.0, 7648690600760440.0 / 57.0};
+  double w = 0.25 * x * x, p;
+  int n;
+  /* terms: c[n-1] * 4^-n * x^(2n) = c[n-1] * (x^2/4)^n */
+  p = c[27];
+  for (n = 26; n >= 0; n--)
+    p = b2e_fma(p, w, c[n]);
+  return b2e_fma(x * w, p, x);
+}
+
+B2E_HD double b2e_asin(double x) {
+  double a = fabs(x), r;
+  if (a <= 0.125)
+    return b2e_asin_small(x);
+  if (a <= 0.5)
+    return b2e_asin_mid(x);
+  if (a > 1.0 || x != x)
+    return (x - x) / (x - x); /* NaN */
+  {
+    double z = sqrt(0.5 * (1.0 - a)); /* 1 - a exact for a in [1/2, 1] */
+    double t = 2.0 * b2e_asin_mid(z);
+    r = (B2E_PIO2_1 - t) + B2E_PIO2_2;
+  }
+  return x < 0 ? -r : r;
+}
+
+#endif

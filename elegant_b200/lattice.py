@@ -1,0 +1,289 @@
+"""Lattice description for the tracking engine: elegant's element types,
+parameter names and defaults for the supported subset, plus a reader for the
+matching subset of elegant's ``.lte`` syntax.
+
+Parameter names and defaults follow the reference's tables (track_data.c):
+``drift_param`` :450, ``edrift_param`` :3174, ``kquad_param`` :1222,
+``ksext_param`` :1120, ``csbend_param`` :1893, ``csrcsbend_param`` :1982,
+``rfca_param`` :576, ``maxamp_param`` :990, ``charge_param`` :2488,
+``csrdrift_param`` :2543.  The .lte grammar handled here is the part of
+elegant's parser (get_beamline.c:117, mad_parse.c:886) that lattices of
+these element types use: ``NAME: TYPE, P=V, ...``, ``NAME: LINE=(...)`` with
+repetition ``n*X`` and reversal ``-X``, ``&`` continuation, ``!`` comments and
+``USE``.  Anything outside the subset raises ``LatticeError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+from dataclasses import dataclass, field
+
+from . import _native as nat
+
+
+class LatticeError(ValueError):
+    """The lattice uses an element type or parameter the engine does not support."""
+
+
+# elegant type name -> engine type code; aliases are elegant's synonyms
+TYPES = {
+    "DRIF": nat.DRIF, "DRIFT": nat.DRIF, "EDRIFT": nat.EDRIFT, "KQUAD": nat.KQUAD, "KSEXT": nat.KSEXT,
+    "CSBEND": nat.CSBEND, "RFCA": nat.RFCA, "MAXAMP": nat.MAXAMP, "MARK": nat.MARK, "MARKER": nat.MARK,
+    "CHARGE": nat.CHARGE, "CSRCSBEND": nat.CSRCSBEND, "CSRDRIFT": nat.CSRDRIFT,
+}
+TYPE_NAMES = {nat.DRIF: "DRIF", nat.EDRIFT: "EDRIFT", nat.KQUAD: "KQUAD", nat.KSEXT: "KSEXT",
+              nat.CSBEND: "CSBEND", nat.RFCA: "RFCA", nat.MAXAMP: "MAXAMP", nat.MARK: "MARK",
+              nat.CHARGE: "CHARGE", nat.CSRCSBEND: "CSRCSBEND", nat.CSRDRIFT: "CSRDRIFT"}
+
+_KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, "N_SLICES": 8,
+          "INTEGRATION_ORDER": 9}
+_BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "DY": 7, "DZ": 8, "FSE": 9,
+         "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
+         "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18}
+_CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=23, SGDERIV_HALFWIDTH=24,
+                SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29)
+
+# parameter name -> slot, per engine type
+SLOTS = {
+    nat.DRIF: {"L": 0, "ORDER": 1},
+    nat.EDRIFT: {"L": 0},
+    nat.KQUAD: dict(_KMULT, K1=1),
+    nat.KSEXT: dict(_KMULT, K2=1, K1=10, J1=11),
+    nat.CSBEND: _BEND,
+    nat.CSRCSBEND: _CSRBEND,
+    nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6},
+    nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "Y_EXPONENT": 4},
+    nat.MARK: {},
+    nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},
+    nat.CSRDRIFT: {"L": 0, "N_KICKS": 1, "DZ": 2, "CSR": 3, "USE_STUPAKOV": 4},
+}
+
+# defaults from the reference's parameter tables (only nonzero ones listed)
+DEFAULTS = {
+    nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4},
+    nat.KSEXT: {"N_SLICES": 1, "INTEGRATION_ORDER": 4},
+    nat.CSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
+                 "EDGE_ORDER": 1},
+    nat.CSRCSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
+                    "EDGE_ORDER": 1, "BIN_RANGE_FACTOR": 1.2, "SG_ORDER": 1, "TRAPAZOID_INTEGRATION": 1, "CSR": 1,
+                    "CLIP_NEGATIVE_BINS": 1},
+    nat.RFCA: {"FREQ": 500e6, "T_REFERENCE": -1},
+    nat.MAXAMP: {"EXPONENT": 2},
+    nat.CSRDRIFT: {"N_KICKS": 1, "CSR": 1},
+}
+
+LENGTH_TYPES = {nat.DRIF, nat.EDRIFT, nat.KQUAD, nat.KSEXT, nat.CSBEND, nat.RFCA, nat.CSRCSBEND, nat.CSRDRIFT}
+
+
+@dataclass
+class Element:
+    """One lattice element: elegant type name, element name and parameters."""
+
+    name: str
+    type: str
+    params: dict = field(default_factory=dict)
+
+    def __post_init__(self):
+        self.type = self.type.upper()
+        if self.type not in TYPES:
+            raise LatticeError(f"element type {self.type} is not supported by the engine")
+        code = TYPES[self.type]
+        self.type = TYPE_NAMES[code]
+        clean = {}
+        for k, v in self.params.items():
+            k = k.upper()
+            if k not in SLOTS[code]:
+                raise LatticeError(f"parameter {k} of {self.type} {self.name} is not supported by the engine")
+            if k == "N_KICKS" and code in (nat.CSBEND, nat.CSRCSBEND):
+                k = "N_SLICES"  # alias sharing storage (track_data.c:1925, :2006)
+            clean[k] = float(v)
+        self.params = clean
+
+    @property
+    def code(self) -> int:
+        return TYPES[self.type]
+
+    def get(self, key: str) -> float:
+        key = key.upper()
+        if key in self.params:
+            return self.params[key]
+        return float(DEFAULTS.get(self.code, {}).get(key, 0.0))
+
+    @property
+    def length(self) -> float:
+        return self.get("L") if self.code in LENGTH_TYPES else 0.0
+
+    def slots(self) -> list[float]:
+        p = [0.0] * nat.MAX_PARAMS
+        for k, v in DEFAULTS.get(self.code, {}).items():
+            p[SLOTS[self.code][k]] = float(v)
+        for k, v in self.params.items():
+            p[SLOTS[self.code][k]] = v
+        return p
+
+    def to_lte(self) -> str:
+        items = [f"{k}={v!r}" for k, v in self.params.items()]
+        return f"{self.name}: {self.type}" + ("".join(", " + i for i in items))
+
+
+class Lattice:
+    """An expanded beamline (list of Elements in tracking order)."""
+
+    def __init__(self, elements: list[Element]):
+        if not elements:
+            raise LatticeError("empty beamline")
+        self.elements = list(elements)
+
+    def __len__(self):
+        return len(self.elements)
+
+    @property
+    def total_length(self) -> float:
+        return sum(e.length for e in self.elements)
+
+    def index(self, name: str) -> list[int]:
+        return [i for i, e in enumerate(self.elements) if e.name == name]
+
+    def to_ctypes(self) -> ctypes.Array:
+        arr = (nat.Element * len(self.elements))()
+        for i, e in enumerate(self.elements):
+            arr[i].type = e.code
+            arr[i].name = e.name.encode()[:31]
+            for j, v in enumerate(e.slots()):
+                arr[i].p[j] = v
+        return arr
+
+    def to_lte(self, line_name: str = "RING") -> str:
+        """Write the expanded line as .lte text (one definition per element occurrence)."""
+        defs, seen, names = [], {}, []
+        for e in self.elements:
+            key = e.name
+            if key in seen and seen[key] != e.to_lte():
+                key = f"{e.name}_{len(seen)}"
+                e = Element(key, e.type, dict(e.params))
+            if key not in seen:
+                seen[key] = e.to_lte()
+                defs.append(seen[key])
+            names.append(key)
+        body = ",".join(names)
+        return "\n".join(defs) + f"\n{line_name}: LINE=({body})\nUSE,{line_name}\n"
+
+
+_TOKEN_NUM = re.compile(r"^[-+]?(\d+\.?\d*|\.\d+)([eEdD][-+]?\d+)?$")
+
+
+def _value(text: str) -> float:
+    t = text.strip().strip('"').strip()
+    if _TOKEN_NUM.match(t):
+        return float(t.replace("d", "e").replace("D", "e"))
+    # elegant accepts RPN expressions in quotes; the subset handled here is
+    # plain arithmetic on numbers and the constant pi
+    expr = t.replace("pi", "3.141592653589793").replace("PI", "3.141592653589793")
+    if re.fullmatch(r"[0-9eE.+\-*/() ]+", expr):
+        return float(eval(expr, {"__builtins__": {}}, {}))  # noqa: S307 - digits and operators only
+    raise LatticeError(f"cannot evaluate parameter value {text!r}")
+
+
+def _split_params(s: str) -> list[str]:
+    out, depth, cur, quote = [], 0, "", False
+    for ch in s:
+        if ch == '"':
+            quote = not quote
+        if ch == "(" and not quote:
+            depth += 1
+        if ch == ")" and not quote:
+            depth -= 1
+        if ch == "," and depth == 0 and not quote:
+            out.append(cur)
+            cur = ""
+        else:
+            cur += ch
+    if cur.strip():
+        out.append(cur)
+    return [x.strip() for x in out if x.strip()]
+
+
+def parse_lte(text: str, use: str | None = None) -> Lattice:
+    """Read the supported subset of elegant's .lte format and expand the used line."""
+    stmts, cur = [], ""
+    for raw in text.splitlines():
+        line = raw.split("!")[0].rstrip()
+        if not line.strip():
+            continue
+        if line.endswith("&"):
+            cur += line[:-1] + " "
+            continue
+        cur += line
+        stmts.append(cur.strip())
+        cur = ""
+    if cur.strip():
+        stmts.append(cur.strip())
+    elements: dict[str, Element] = {}
+    lines: dict[str, list[str]] = {}
+    last_line = None
+    for st in stmts:
+        up = st.upper()
+        if up.startswith("USE"):
+            use = use or _split_params(st.split(",", 1)[1] if "," in st else st.split(None, 1)[1])[0].upper()
+            continue
+        if up.startswith("RETURN"):
+            break
+        if ":" not in st:
+            raise LatticeError(f"cannot parse statement {st!r}")
+        name, rest = st.split(":", 1)
+        name = name.strip().strip('"').upper()
+        rest = rest.strip()
+        m = re.match(r"^LINE\s*=\s*\((.*)\)\s*$", rest, flags=re.I | re.S)
+        if m:
+            lines[name] = _split_params(m.group(1))
+            last_line = name
+            continue
+        parts = _split_params(rest)
+        etype = parts[0].upper()
+        params = {}
+        for p in parts[1:]:
+            if "=" not in p:
+                raise LatticeError(f"cannot parse parameter {p!r} of {name}")
+            k, v = p.split("=", 1)
+            params[k.strip().upper()] = _value(v)
+        if etype in elements:
+            base = elements[etype]
+            merged = dict(base.params)
+            merged.update(params)
+            elements[name] = Element(name, base.type, merged)
+        else:
+            elements[name] = Element(name, etype, params)
+
+    def expand(item: str, depth: int = 0) -> list[Element]:
+        if depth > 64:
+            raise LatticeError("beamline nesting too deep")
+        item = item.strip()
+        rep = 1
+        m = re.match(r"^(\d+)\s*\*\s*(.+)$", item)
+        if m:
+            rep, item = int(m.group(1)), m.group(2).strip()
+        reverse = item.startswith("-")
+        if reverse:
+            item = item[1:].strip()
+        if item.startswith("(") and item.endswith(")"):
+            seq = []
+            for sub in _split_params(item[1:-1]):
+                seq += expand(sub, depth + 1)
+        else:
+            key = item.upper()
+            if key in lines:
+                seq = []
+                for sub in lines[key]:
+                    seq += expand(sub, depth + 1)
+            elif key in elements:
+                seq = [elements[key]]
+            else:
+                raise LatticeError(f"undefined element or line {item}")
+        if reverse:
+            seq = seq[::-1]
+        return seq * rep
+
+    target = (use or last_line or "").upper()
+    if not target:
+        raise LatticeError("no beamline to use")
+    return Lattice(expand(target))

@@ -1,0 +1,183 @@
+"""Host-side mirror of elegant's tracking entry (&run_setup + &track ->
+do_tracking, do_tracking.c:144) for the supported element subset, calling
+the CUDA engine through its C ABI.
+
+    trk = Tracker(lattice, p_central, n_passes)
+    result = trk.track(beam)        # host buffers in, host buffers out
+
+Results keep the input particle order; ``lost_pass`` is -1 for survivors,
+else the pass on which the particle was lost (elegant's lossPass column).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as nat
+from .beam import Beam
+from .lattice import SLOTS, TYPES, Lattice
+
+
+@dataclass
+class TrackResult:
+    coords: np.ndarray       # (n, 6), input order
+    ids: np.ndarray          # (n,)
+    lost_pass: np.ndarray    # (n,) int32, -1 = survived
+    lost_element: np.ndarray  # (n,) int32, -1 = survived
+    n_left: int
+    effort: float            # particle-passes (do_tracking.c:2758-2764)
+
+    @property
+    def survived(self) -> np.ndarray:
+        return self.lost_pass < 0
+
+
+class Tracker:
+    """One engine context bound to a lattice and run options."""
+
+    def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
+                 passes_per_launch: int = 0):
+        self.lib = nat.load_library()
+        self.lattice = lattice
+        self._ctx = ctypes.c_void_p()
+        rc = self.lib.b2e_create(ctypes.byref(self._ctx), device)
+        if rc != nat.B2E_OK:
+            raise nat.EngineError(rc, "b2e_create failed (is a CUDA device visible?)")
+        self.options = nat.RunOptions(p_central=p_central, n_passes=n_passes, default_order=default_order,
+                                      coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
+                                      threads_per_block=0)
+        self._elems = lattice.to_ctypes()
+        self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
+        self.n_instances = 1
+
+    # -- helpers ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != nat.B2E_OK:
+            raise nat.EngineError(rc, self.lib.b2e_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self.lib.b2e_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- ensembles -------------------------------------------------------
+    def load_ensemble(self, offsets, overrides):
+        """offsets: n_instances+1 particle offsets; overrides: (element_index, PARAM, values)."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        n_inst = len(offsets) - 1
+        self._ov_values = []
+        arr = (nat.Override * max(len(overrides), 1))()
+        for k, (ie, name, values) in enumerate(overrides):
+            e = self.lattice.elements[ie]
+            slot = SLOTS[TYPES[e.type]][name.upper()]
+            v = np.ascontiguousarray(values, dtype=np.float64)
+            if v.shape != (n_inst,):
+                raise ValueError("override values must have one entry per instance")
+            self._ov_values.append(v)
+            arr[k].element = ie
+            arr[k].slot = slot
+            arr[k].values = v.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self._offsets = offsets
+        self._check(self.lib.b2e_load_ensemble(self._ctx, n_inst, offsets.ctypes.data_as(ctypes.c_void_p), arr,
+                                               len(overrides)))
+        self.n_instances = n_inst
+
+    # -- tracking --------------------------------------------------------
+    def track(self, beam: Beam) -> TrackResult:
+        """Upload, track all passes, download (b2e_track_host)."""
+        cols = [np.ascontiguousarray(beam.coords[:, i]) for i in range(6)]
+        ids = beam.ids.copy()
+        n = beam.n
+        lost_pass = np.empty(n, dtype=np.int32)
+        lost_elem = np.empty(n, dtype=np.int32)
+        n_left = ctypes.c_int64()
+        effort = ctypes.c_double()
+        ptrs = nat.pointer_array([c.ctypes.data for c in cols])
+        self._check(self.lib.b2e_track_host(self._ctx, ptrs, ids.ctypes.data, n, lost_pass.ctypes.data,
+                                            lost_elem.ctypes.data, ctypes.byref(n_left), ctypes.byref(effort)))
+        self._n = n
+        return TrackResult(np.stack(cols, axis=1), ids, lost_pass, lost_elem, int(n_left.value), effort.value)
+
+    def upload(self, beam: Beam):
+        """Copy a beam to the device (starts a new run at pass 0)."""
+        cols = [np.ascontiguousarray(beam.coords[:, i]) for i in range(6)]
+        self._n = beam.n
+        ptrs = nat.pointer_array([c.ctypes.data for c in cols])
+        self._check(self.lib.b2e_upload_particles(self._ctx, ptrs, beam.ids.ctypes.data, beam.n))
+
+    def continue_tracking(self) -> float:
+        """Track the resident particles for n_passes more passes; returns the effort."""
+        effort = ctypes.c_double()
+        self._check(self.lib.b2e_track(self._ctx, ctypes.byref(effort)))
+        return effort.value
+
+    def download(self) -> TrackResult:
+        n = self._n if hasattr(self, "_n") else 0
+        cols = [np.empty(n) for _ in range(6)]
+        ids = np.empty(n, dtype=np.int64)
+        lost_pass = np.empty(n, dtype=np.int32)
+        lost_elem = np.empty(n, dtype=np.int32)
+        n_left = ctypes.c_int64()
+        ptrs = nat.pointer_array([c.ctypes.data for c in cols])
+        self._check(self.lib.b2e_download(self._ctx, ptrs, ids.ctypes.data, lost_pass.ctypes.data,
+                                          lost_elem.ctypes.data, ctypes.byref(n_left)))
+        return TrackResult(np.stack(cols, axis=1), ids, lost_pass, lost_elem, int(n_left.value), float("nan"))
+
+    @property
+    def launches(self) -> int:
+        """Kernels launched by this context so far."""
+        return int(self.lib.b2e_kernel_launches(self._ctx))
+
+    def track_host_pointers(self, col_ptrs, ids_ptr: int, n: int, lost_pass_ptr: int, lost_elem_ptr: int):
+        """b2e_track_host on caller-owned (e.g. pinned) host buffers; returns (n_left, effort)."""
+        n_left = ctypes.c_int64()
+        effort = ctypes.c_double()
+        ptrs = nat.pointer_array(list(col_ptrs))
+        self._check(self.lib.b2e_track_host(self._ctx, ptrs, ids_ptr, n, lost_pass_ptr, lost_elem_ptr,
+                                            ctypes.byref(n_left), ctypes.byref(effort)))
+        self._n = n
+        return int(n_left.value), effort.value
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of this context (as an integer handle)."""
+        return self.lib.b2e_stream(self._ctx) or 0
+
+    def track_device(self, columns, lost_pass, lost_element) -> float:
+        """Track device-resident columns in place (six CUDA float64 tensors or raw
+        pointers, lost_pass/lost_element int32 initialised to -1).  Returns the effort."""
+        def ptr(t):
+            return t if isinstance(t, int) else t.data_ptr()
+        n = columns[0].numel() if hasattr(columns[0], "numel") else None
+        if n is None:
+            raise ValueError("pass tensors so the particle count is known")
+        effort = ctypes.c_double()
+        ptrs = nat.pointer_array([ptr(c) for c in columns])
+        self._check(self.lib.b2e_track_device(self._ctx, ptrs, None, n, ptr(lost_pass), ptr(lost_element),
+                                              ctypes.byref(effort)))
+        return effort.value
+
+    def csr_wakes(self, capacity: int) -> np.ndarray:
+        buf = np.empty(capacity, dtype=np.float64)
+        written = ctypes.c_int64()
+        self._check(self.lib.b2e_csr_wakes(self._ctx, buf.ctypes.data, capacity, ctypes.byref(written)))
+        return buf[: written.value]
+
+
+def track(lattice: Lattice, beam: Beam, p_central: float, n_passes: int, **kw) -> TrackResult:
+    with Tracker(lattice, p_central, n_passes, **kw) as t:
+        return t.track(beam)

@@ -1,0 +1,244 @@
+/*
+ * elegant_b200 -- C ABI of the B200 particle-tracking engine.
+ *
+ * The engine replaces, for one GPU, the per-element tracking calls that
+ * elegant's do_tracking() (do_tracking.c:144) makes for the hot-path element
+ * subset.  In the reference those calls are, per element and per pass:
+ *   track_particles (DRIF, matrix.c:294, called at do_tracking.c:1280)
+ *   exactDrift (EDRIFT, csbend.c:3767, do_tracking.c:1997)
+ *   multipole_tracking2 (KQUAD/KSEXT, multipole.c:693, do_tracking.c:2013, :2024)
+ *   track_through_csbend (CSBEND, csbend.c:665, do_tracking.c:1949)
+ *   simple_rf_cavity (RFCA, simple_rfca.c:264, do_tracking.c:1576)
+ *   track_through_csbendCSR (CSRCSBEND, csbend.c:1899, do_tracking.c:1977)
+ *   track_through_driftCSR (CSRDRIFT, csbend.c:3176, do_tracking.c:1984)
+ *   limit_amplitudes / elimit_amplitudes (apertures, limit_amplitudes.c:193,
+ *     :472, do_tracking.c:2459-2468)
+ * and the GPU hooks gpuElegant adds inside each of them
+ * (gpu_multipole_tracking2, gpu_track_through_csbend, ...; gpu_multipole.h,
+ * gpu_csbend.h, gpu_simple_rfca.h:11, gpu_limit_amplitudes.h:14,29).
+ * Here one call tracks a whole run (all passes, all elements) with the
+ * particles resident in HBM, so the host makes one call instead of
+ * elements x passes calls.
+ *
+ * Conventions
+ *  - Particles are structure-of-arrays FP64 columns x, xp, y, yp, s, delta
+ *    (elegant's coordinate order, track.h:81-86) plus an int64 particle ID.
+ *  - Every entry point returns B2E_OK (0) or a negative B2E_ERR_* code and
+ *    never exits the process; b2e_last_error() describes the last failure.
+ *  - A context owns one CUDA stream and the device buffers; use one context
+ *    per host thread.  No global state: the reference's file-static CSR
+ *    state (csrWake, csbend.h:27-63) is per context.
+ *  - Lattice parameters use elegant's element-parameter names; slots not
+ *    given take the defaults of elegant's parameter tables (track_data.c).
+ */
+#ifndef ELEGANT_B200_H
+#define ELEGANT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define B2E_OK 0
+#define B2E_ERR_ARG (-1)      /* invalid argument (null pointer, bad size) */
+#define B2E_ERR_LATTICE (-2)  /* unsupported element or parameter value */
+#define B2E_ERR_CUDA (-3)     /* CUDA runtime error */
+#define B2E_ERR_NOMEM (-4)    /* device allocation failed */
+#define B2E_ERR_STATE (-5)    /* call out of order (e.g. track before upload) */
+#define B2E_ERR_TIMEOUT (-6)  /* a bounded device wait gave up */
+#define B2E_ERR_DEVICE (-7)   /* the device reported a numerical fault flag */
+
+/* ---- element types (names follow elegant's entity_name table) -------- */
+#define B2E_DRIF 1
+#define B2E_EDRIFT 2
+#define B2E_KQUAD 3
+#define B2E_KSEXT 4
+#define B2E_CSBEND 5
+#define B2E_RFCA 6
+#define B2E_MAXAMP 7
+#define B2E_MARK 8
+#define B2E_CHARGE 9
+#define B2E_CSRCSBEND 10
+#define B2E_CSRDRIFT 11
+
+#define B2E_MAX_PARAMS 40
+
+/* Parameter slot indices, per element type.  Slot names are elegant's
+ * parameter names (track_data.c tables cited per type). */
+/* DRIF  (drift_param, track_data.c:450) */
+#define B2E_DRIF_L 0
+#define B2E_DRIF_ORDER 1
+/* EDRIFT (edrift_param, track_data.c:3174) */
+#define B2E_EDRIFT_L 0
+/* KQUAD (kquad_param, track_data.c:1222) and KSEXT (ksext_param, :1120) share slots */
+#define B2E_KMULT_L 0
+#define B2E_KMULT_K 1 /* K1 for KQUAD, K2 for KSEXT */
+#define B2E_KMULT_TILT 2
+#define B2E_KMULT_DX 3
+#define B2E_KMULT_DY 4
+#define B2E_KMULT_DZ 5
+#define B2E_KMULT_FSE 6
+#define B2E_KMULT_N_KICKS 7
+#define B2E_KMULT_N_SLICES 8
+#define B2E_KMULT_INTEGRATION_ORDER 9
+#define B2E_KMULT_K1_OF_KSEXT 10 /* KSEXT K1 (quadrupole error term) */
+#define B2E_KMULT_J1_OF_KSEXT 11 /* KSEXT J1 (skew quadrupole error term) */
+/* CSBEND (csbend_param, track_data.c:1893) and CSRCSBEND (csrcsbend_param, :1982) */
+#define B2E_BEND_L 0
+#define B2E_BEND_ANGLE 1
+#define B2E_BEND_E1 2
+#define B2E_BEND_E2 3
+#define B2E_BEND_TILT 4
+#define B2E_BEND_ETILT 5
+#define B2E_BEND_DX 6
+#define B2E_BEND_DY 7
+#define B2E_BEND_DZ 8
+#define B2E_BEND_FSE 9
+#define B2E_BEND_HGAP 10
+#define B2E_BEND_FINT 11
+#define B2E_BEND_N_SLICES 12 /* N_KICKS is an alias (track_data.c:1925, :2006) */
+#define B2E_BEND_INTEGRATION_ORDER 13
+#define B2E_BEND_EDGE1_EFFECTS 14
+#define B2E_BEND_EDGE2_EFFECTS 15
+#define B2E_BEND_EDGE_ORDER 16
+#define B2E_BEND_K1 17
+#define B2E_BEND_K2 18
+/* CSRCSBEND-only slots */
+#define B2E_BEND_BINS 20
+#define B2E_BEND_BIN_RANGE_FACTOR 21
+#define B2E_BEND_SG_HALFWIDTH 22
+#define B2E_BEND_SG_ORDER 23
+#define B2E_BEND_SGDERIV_HALFWIDTH 24
+#define B2E_BEND_SGDERIV_ORDER 25
+#define B2E_BEND_TRAPAZOID_INTEGRATION 26
+#define B2E_BEND_STEADY_STATE 27
+#define B2E_BEND_CSR 28
+#define B2E_BEND_CLIP_NEGATIVE_BINS 29
+/* RFCA (rfca_param, track_data.c:576) */
+#define B2E_RFCA_L 0
+#define B2E_RFCA_VOLT 1
+#define B2E_RFCA_PHASE 2
+#define B2E_RFCA_FREQ 3
+#define B2E_RFCA_DX 4
+#define B2E_RFCA_DY 5
+#define B2E_RFCA_T_REFERENCE 6
+/* MAXAMP (maxamp_param, track_data.c:990) */
+#define B2E_MAXAMP_X_MAX 0
+#define B2E_MAXAMP_Y_MAX 1
+#define B2E_MAXAMP_ELLIPTICAL 2
+#define B2E_MAXAMP_EXPONENT 3
+#define B2E_MAXAMP_Y_EXPONENT 4
+/* CHARGE (charge_param, track_data.c:2488) */
+#define B2E_CHARGE_TOTAL 0
+#define B2E_CHARGE_PER_PARTICLE 1
+/* CSRDRIFT (csrdrift_param, track_data.c:2543) */
+#define B2E_CSRDRIFT_L 0
+#define B2E_CSRDRIFT_N_KICKS 1
+#define B2E_CSRDRIFT_DZ 2
+#define B2E_CSRDRIFT_CSR 3
+#define B2E_CSRDRIFT_USE_STUPAKOV 4
+
+typedef struct {
+  int32_t type;             /* B2E_DRIF ... */
+  int32_t reserved;
+  char name[32];            /* element name; adjacent bends with equal names share edges */
+  double p[B2E_MAX_PARAMS]; /* parameter slots, see indices above */
+} b2e_element;
+
+/* Per-instance parameter overrides for batched ensembles: instance i
+ * replaces slot `slot` of element `element` with values[i]. */
+typedef struct {
+  int32_t element;
+  int32_t slot;
+  const double *values; /* n_instances values (host memory) */
+} b2e_override;
+
+/* Run options (elegant &run_setup / &track subset). */
+typedef struct {
+  double p_central;        /* reference momentum beta*gamma (run_setup p_central) */
+  int32_t n_passes;        /* &track n_passes */
+  int32_t default_order;   /* run_setup default_order for DRIF (2) */
+  double coord_limit;      /* global_settings coord_limit (10 m) */
+  double slope_limit;      /* global_settings slope_limit (1) */
+  int32_t passes_per_launch; /* 0 = all passes of a step in one launch */
+  int32_t threads_per_block; /* 0 = engine default */
+} b2e_run_options;
+
+typedef struct b2e_ctx b2e_ctx;
+
+/* ---- lifecycle --------------------------------------------------------- */
+int b2e_create(b2e_ctx **ctx, int device);
+int b2e_destroy(b2e_ctx *ctx);
+const char *b2e_last_error(const b2e_ctx *ctx);
+int b2e_version(void);
+
+/* ---- lattice ----------------------------------------------------------- */
+/* Replaces the parsed element list that do_tracking walks (ELEMENT_LIST,
+ * track.h:290-344) with a flat array.  Parameters are validated here. */
+int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32_t n_elements,
+                     const b2e_run_options *options);
+
+/* ---- particles (host buffers) ----------------------------------------- */
+/* Uploads n particles as columns x, xp, y, yp, s, delta (host pointers) and
+ * their IDs.  Replaces the host->device copy that gpuElegant performs on
+ * residency change (gpu_base.cu setElementGpuData). */
+int b2e_upload_particles(b2e_ctx *ctx, const double *const columns[6], const int64_t *ids, int64_t n);
+
+/* Tracks the resident particles for options->n_passes more passes
+ * (elegant's do_tracking pass loop, do_tracking.c:488).  The first call after
+ * b2e_upload_particles starts at pass 0; later calls continue the same run
+ * (pass numbers, RFCA fiducials and loss records carry over).  *effort
+ * receives the sum over this call's passes of the survivors at the end of
+ * each pass (do_tracking.c:2758-2764). */
+int b2e_track(b2e_ctx *ctx, double *effort);
+
+/* The CUDA stream (cudaStream_t) all of the context's work is queued on. */
+void *b2e_stream(b2e_ctx *ctx);
+
+/* Number of kernels this context has launched so far (instrumentation). */
+int64_t b2e_kernel_launches(const b2e_ctx *ctx);
+
+/* Downloads survivors and losses.  Columns receive all n particles in upload
+ * order; lost_pass[i] is -1 for survivors or the pass on which particle i
+ * was lost (elegant's lossPass column, track.h:89, do_tracking.c:4584);
+ * lost_element[i] is the index of the element where it was lost (or -1). */
+int b2e_download(b2e_ctx *ctx, double *const columns[6], int64_t *ids, int32_t *lost_pass,
+                 int32_t *lost_element, int64_t *n_left);
+
+/* One call for the whole drop-in path with host buffers: upload, track,
+ * download.  This is what a host program linked in place of the per-element
+ * calls invokes. */
+int b2e_track_host(b2e_ctx *ctx, double *const columns[6], int64_t *ids, int64_t n, int32_t *lost_pass,
+                   int32_t *lost_element, int64_t *n_left, double *effort);
+
+/* ---- device-resident variant (no host copies) ------------------------- */
+/* Columns are device pointers owned by the caller, tracked in place. */
+int b2e_track_device(b2e_ctx *ctx, double *const dev_columns[6], const int64_t *dev_ids, int64_t n,
+                     int32_t *dev_lost_pass, int32_t *dev_lost_element, double *effort);
+
+/* ---- batched ensembles ------------------------------------------------- */
+/* n_instances lattice copies; instance i owns particles
+ * [offsets[i], offsets[i+1]).  overrides apply per instance.  Each instance
+ * has its own RFCA fiducial.  Particles are host columns, as for
+ * b2e_upload_particles. */
+int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_t *offsets, const b2e_override *overrides,
+                      int32_t n_overrides);
+
+/* Per-instance diagnostics after each pass: survivors, centroids <x>, <y>,
+ * and rms emittances ex, ey (rms_emittance, final_props.c:844).  Buffers
+ * are host arrays of n_instances * n_passes values; any may be NULL. */
+int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *cy, double *ex, double *ey);
+
+/* ---- CSR (CSRCSBEND / CSRDRIFT) ---------------------------------------- */
+/* Wake arrays of every CSR kick of the last b2e_track call: for each
+ * CSRCSBEND kick, BINS values of dGamma (csbend.c:2673) in kick order. */
+int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,70 @@
+"""Test-side wrappers around the CPU oracles in oracle/.
+
+- ``RefOracle``: elegant's own hot-path C sources compiled through a shim
+  (oracle/_ref/libb2e_ref*.so, built by oracle/Makefile.ref), driven by
+  oracle/ref_driver.c.  ``math="libm"`` uses glibc's elementary functions like
+  the reference build; ``math="b2e"`` routes sin/cos/tan/asin to the shared
+  implementations of elegant_b200/csrc/b2e_math.h that the CUDA engine uses.
+- ``PortOracle``: the restatement in oracle/b2e_oracle.c (same math switch).
+
+Only tests, the graft smoke check and the benchmark's CPU-baseline leg use
+this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def lattice_spec(lattice) -> str:
+    """Element list in the driver's 'NAME:TYPE KEY=VALUE ...;' syntax."""
+    items = []
+    for e in lattice.elements:
+        kv = " ".join(f"{k}={v!r}" for k, v in e.params.items())
+        items.append(f"{e.name}:{e.type} {kv}".strip())
+    return ";".join(items)
+
+
+class RefOracle:
+    def __init__(self, math: str = "libm"):
+        name = "libb2e_ref.so" if math == "libm" else "libb2e_ref_b2emath.so"
+        path = os.path.join(REF_DIR, name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.b2e_ref_track.restype = ctypes.c_long
+        self.math = math
+
+    def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0):
+        """Returns (rows, n_left, effort, wakes); rows are the reference's final
+        particle array (x, xp, y, yp, s, delta, id, lossPass), survivors first."""
+        n = coords.shape[0]
+        rows = np.zeros((n, 7))
+        rows[:, :6] = coords
+        rows[:, 6] = ids
+        out = np.zeros((max(n, 1), 8))
+        nl = ctypes.c_long()
+        eff = ctypes.c_double()
+        err = ctypes.create_string_buffer(512)
+        ww = ctypes.c_long()
+        wakes = np.zeros(max(wake_capacity, 1))
+        rc = self.lib.b2e_ref_track(lattice_spec(lattice).encode(), ctypes.c_double(p_central),
+                                    rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.c_long(n_passes),
+                                    out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nl), ctypes.byref(eff),
+                                    wakes.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(wake_capacity),
+                                    ctypes.byref(ww), err, ctypes.c_long(512))
+        if rc != 0:
+            raise RuntimeError(f"reference oracle failed: {err.value.decode()}")
+        return out[:n], nl.value, eff.value, wakes[: ww.value]
+
+
+def by_id(rows):
+    """Sort reference rows by particle ID; returns (coords[n,6], ids, loss_pass)."""
+    order = np.argsort(rows[:, 6], kind="stable")
+    r = rows[order]
+    return r[:, :6], r[:, 6].astype(np.int64), r[:, 7].astype(np.int64)

@@ -1,0 +1,130 @@
+"""GPU parity of the fused ring kernel against the reference's own tracking
+code (oracle/_ref, built with the engine's elementary functions).
+
+Bar: bit-identical final coordinates for every surviving particle and an
+identical set of (particle ID, loss pass) for lost ones.
+"""
+import numpy as np
+import pytest
+
+from elegant_b200 import Element, Lattice, Tracker, workloads as w
+from elegant_b200.beam import Beam
+from reforacle import by_id
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_track(lat, beam, p, passes, **kw):
+    with Tracker(lat, p, passes, **kw) as t:
+        return t.track(beam)
+
+
+def assert_parity(res, rows, n_left):
+    ref_c, ref_ids, ref_loss = by_id(rows)
+    order = np.argsort(res.ids)
+    c, ids, lp = res.coords[order], res.ids[order], res.lost_pass[order]
+    assert np.array_equal(ids, ref_ids)
+    assert res.n_left == n_left
+    ref_lost = {(int(i), int(l)) for i, l in zip(ref_ids, ref_loss) if l >= 0}
+    gpu_lost = {(int(i), int(l)) for i, l in zip(ids, lp) if l >= 0}
+    assert gpu_lost == ref_lost
+    alive = lp < 0
+    diff = c[alive] != ref_c[alive]
+    assert not diff.any(), f"{diff.sum()} coordinates differ; max abs {np.abs(c[alive]-ref_c[alive]).max()}"
+
+
+def test_ring_bit_exact_100_turns(ref_b2e):
+    lat = w.fodo_ring()
+    beam = w.ring_beam(256, seed=11)
+    res = gpu_track(lat, beam, w.ring_p_central(), 100)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 100)
+    assert_parity(res, rows, nl)
+    assert res.effort == eff
+
+
+def test_ring_losses_match(ref_b2e):
+    """Large-amplitude and off-momentum particles hit the 20 mm aperture,
+    the slope limit and the sextupole dynamic aperture."""
+    lat = w.fodo_ring()
+    rng = np.random.default_rng(3)
+    n = 300
+    c = np.zeros((n, 6))
+    c[:, 0] = rng.uniform(-0.022, 0.022, n)
+    c[:, 1] = rng.uniform(-3e-3, 3e-3, n)
+    c[:, 2] = rng.uniform(-0.015, 0.015, n)
+    c[:, 3] = rng.uniform(-2e-3, 2e-3, n)
+    c[:, 4] = rng.normal(0, 5e-3, n)
+    c[:, 5] = rng.uniform(-0.03, 0.03, n)
+    beam = Beam(c, np.arange(1, n + 1))
+    res = gpu_track(lat, beam, w.ring_p_central(), 40)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 40)
+    assert nl < n, "test beam should lose particles"
+    assert_parity(res, rows, nl)
+
+
+def test_ring_misaligned_and_tilted(ref_b2e):
+    lat = w.fodo_ring()
+    els = []
+    for i, e in enumerate(lat.elements):
+        if e.type == "KQUAD":
+            e = Element(e.name, e.type, dict(e.params, DX=3e-4 * ((i % 3) - 1), DY=-2e-4, FSE=1e-3 * (i % 2)))
+        if e.type == "KSEXT" and i % 3 == 0:
+            e = Element(e.name, e.type, dict(e.params, TILT=0.01, DX=1e-4))
+        els.append(e)
+    lat2 = Lattice(els)
+    beam = w.ring_beam(128, seed=4)
+    res = gpu_track(lat2, beam, w.ring_p_central(), 30)
+    rows, nl, _, _ = ref_b2e.track(lat2, beam.coords, beam.ids, w.ring_p_central(), 30)
+    assert_parity(res, rows, nl)
+
+
+def test_continuation_equals_single_run():
+    lat = w.fodo_ring()
+    beam = w.ring_beam(200, seed=9)
+    one = gpu_track(lat, beam, w.ring_p_central(), 60)
+    with Tracker(lat, w.ring_p_central(), 30) as t:
+        t.track(beam)  # uploads and tracks passes 0..29
+        eff2 = t.continue_tracking()
+        two = t.download()
+    assert np.array_equal(one.coords, two.coords)
+    assert np.array_equal(one.lost_pass, two.lost_pass)
+
+
+def test_passes_per_launch_invariance():
+    lat = w.fodo_ring()
+    beam = w.ring_beam(200, seed=2)
+    a = gpu_track(lat, beam, w.ring_p_central(), 25)
+    b = gpu_track(lat, beam, w.ring_p_central(), 25, passes_per_launch=4)
+    assert np.array_equal(a.coords, b.coords)
+    assert np.array_equal(a.lost_pass, b.lost_pass)
+
+
+def test_empty_and_single_particle(ref_b2e):
+    lat = w.fodo_ring()
+    empty = Beam(np.zeros((0, 6)), np.zeros(0, dtype=np.int64))
+    res = gpu_track(lat, empty, w.ring_p_central(), 3)
+    assert res.n_left == 0 and res.effort == 0
+    one = w.ring_beam(1, seed=1)
+    res = gpu_track(lat, one, w.ring_p_central(), 20)
+    rows, nl, _, _ = ref_b2e.track(lat, one.coords, one.ids, w.ring_p_central(), 20)
+    assert_parity(res, rows, nl)
+
+
+def test_ensemble_matches_per_instance_reference(ref_b2e):
+    lat, beam, offsets, overrides = w.ensemble(n_instances=6, n_min=40, n_max=90, seed=5)
+    with Tracker(lat, w.ring_p_central(), 15) as t:
+        t.load_ensemble(offsets, overrides)
+        res = t.track(beam)
+    for i in range(6):
+        sl = slice(offsets[i], offsets[i + 1])
+        els = []
+        for j, e in enumerate(lat.elements):
+            params = dict(e.params)
+            for (ie, name, vals) in overrides:
+                if ie == j:
+                    params[name] = float(vals[i])
+            els.append(Element(e.name, e.type, params))
+        rows, nl, _, _ = ref_b2e.track(Lattice(els), beam.coords[sl], beam.ids[sl], w.ring_p_central(), 15)
+        sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
+                        int((res.lost_pass[sl] < 0).sum()), 0.0)
+        assert_parity(sub, rows, nl)
