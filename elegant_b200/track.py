@@ -98,8 +98,8 @@ class Tracker:
 
     # -- tracking --------------------------------------------------------
     def track(self, beam: Beam) -> TrackResult:
-        """Upload, track all passes, download (b2e_track_host)."""
-        cols = [np.ascontiguousarray(beam.coords[:, i]) for i in range(6)]
+        """Upload, track all passes, download (b2e_track_host).  The input beam is not modified."""
+        cols = [np.array(beam.coords[:, i], dtype=np.float64, copy=True) for i in range(6)]
         ids = beam.ids.copy()
         n = beam.n
         lost_pass = np.empty(n, dtype=np.int32)
@@ -114,7 +114,7 @@ class Tracker:
 
     def upload(self, beam: Beam):
         """Copy a beam to the device (starts a new run at pass 0)."""
-        cols = [np.ascontiguousarray(beam.coords[:, i]) for i in range(6)]
+        cols = [np.array(beam.coords[:, i], dtype=np.float64, copy=True) for i in range(6)]
         self._n = beam.n
         ptrs = nat.pointer_array([c.ctypes.data for c in cols])
         self._check(self.lib.b2e_upload_particles(self._ctx, ptrs, beam.ids.ctypes.data, beam.n))
