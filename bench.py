@@ -203,6 +203,7 @@ def main():
             step_ms.append(ev0.elapsed_time(ev1))
     torch.cuda.synchronize()
     launches = tracker.launches - launches0
+    variant, tune_ms = tracker.ring_tuning()
     t_total = sum(step_ms) / 1e3
     if dist:
         tt = torch.tensor([t_total, effort_total], dtype=torch.float64, device="cuda")
@@ -293,6 +294,7 @@ def main():
             "config": {"workload": "batched error ensemble of the 8-cell FODO ring (config 2)",
                        "instances_per_gpu": args.instances, "particles_per_gpu": n,
                        "turns_per_step": args.turns_per_step, "lattice_elements": len(lat),
+                       "ring_variant": variant, "autotune_ms_per_pass": [round(x, 3) for x in tune_ms],
                        "l2": "flushed (256 MiB write) before every timed step"},
             "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                          "frac": achieved_tflops / fp64_peak, "traffic": None,

@@ -30,7 +30,7 @@ EXPORTED = [
     "b2e_create", "b2e_destroy", "b2e_last_error", "b2e_version", "b2e_load_lattice",
     "b2e_upload_particles", "b2e_track", "b2e_download", "b2e_track_host", "b2e_track_device",
     "b2e_load_ensemble", "b2e_ensemble_history", "b2e_csr_wakes", "b2e_stream",
-    "b2e_kernel_launches",
+    "b2e_kernel_launches", "b2e_ring_tuning",
 ]
 
 
@@ -42,7 +42,7 @@ class Element(ctypes.Structure):
 class RunOptions(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_int32), ("default_order", ctypes.c_int32),
                 ("coord_limit", ctypes.c_double), ("slope_limit", ctypes.c_double),
-                ("passes_per_launch", ctypes.c_int32), ("threads_per_block", ctypes.c_int32)]
+                ("passes_per_launch", ctypes.c_int32), ("ring_variant", ctypes.c_int32)]
 
 
 class Override(ctypes.Structure):
@@ -92,6 +92,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
+    bind_extra(lib)
     if path is None:
         _lib = lib
     return lib
@@ -102,3 +103,9 @@ def pointer_array(ptrs) -> ctypes.Array:
     for i, p in enumerate(ptrs):
         arr[i] = p
     return arr
+
+
+def bind_extra(lib: ctypes.CDLL) -> None:
+    """Signatures of the instrumentation entry points."""
+    lib.b2e_ring_tuning.restype = ctypes.c_int
+    lib.b2e_ring_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]

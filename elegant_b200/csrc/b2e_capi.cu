@@ -87,6 +87,11 @@ struct b2e_ctx {
   CsrState csr;
   int pass_counter = 0; /* next pass to track in the current run */
   int64_t launches = 0; /* kernels launched by this context */
+  /* autotuning of the ring-kernel occupancy variant */
+  int tuned_variant = 0;
+  std::vector<float> tune_ms;
+  DevBuf<double> d_scratch;       /* 6 columns, for timing variants off the real state */
+  DevBuf<int32_t> d_scratch_loss; /* 2 columns */
 };
 
 static int fail(b2e_ctx *ctx, int code, const char *fmt, ...) {
@@ -158,6 +163,17 @@ extern "C" const char *b2e_last_error(const b2e_ctx *ctx) { return ctx ? ctx->er
 extern "C" void *b2e_stream(b2e_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 extern "C" int64_t b2e_kernel_launches(const b2e_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int b2e_ring_tuning(const b2e_ctx *ctx, int32_t *chosen, float *ms_per_variant) {
+  if (!ctx || !chosen)
+    return B2E_ERR_ARG;
+  *chosen = ctx->opt.ring_variant >= 1 && ctx->opt.ring_variant <= B2E_RING_VARIANTS ? ctx->opt.ring_variant
+                                                                                     : ctx->tuned_variant;
+  if (ms_per_variant)
+    for (int v = 0; v < B2E_RING_VARIANTS; v++)
+      ms_per_variant[v] = v < (int)ctx->tune_ms.size() ? ctx->tune_ms[v] : 0.f;
+  return B2E_OK;
+}
 
 /* Rebuild the tile table for the current instance partition. */
 static void build_tiles(b2e_ctx *ctx) {
@@ -320,6 +336,61 @@ static DevParticles particle_view(b2e_ctx *ctx) {
   return P;
 }
 
+/* Autotuner: time every ring-kernel variant on one pass of a scratch copy of
+ * the current particle state (so the real state is untouched) and keep the
+ * fastest.  The variants differ only in register allocation, never in
+ * arithmetic, so the choice cannot change results. */
+static int autotune_ring(b2e_ctx *ctx, const RingLaunch &Lreal, bool staged, size_t smem, int p, int e) {
+  const int64_t n = ctx->n;
+  const int ne = Lreal.n_elems;
+  CUDA_TRY(ctx, ctx->d_scratch.ensure((size_t)n * 6));
+  CUDA_TRY(ctx, ctx->d_scratch_loss.ensure((size_t)n * 2));
+  RingLaunch L = Lreal;
+  double *cols[6] = {Lreal.P.x, Lreal.P.xp, Lreal.P.y, Lreal.P.yp, Lreal.P.s, Lreal.P.dp};
+  L.P.x = ctx->d_scratch.ptr;
+  L.P.xp = L.P.x + n;
+  L.P.y = L.P.xp + n;
+  L.P.yp = L.P.y + n;
+  L.P.s = L.P.yp + n;
+  L.P.dp = L.P.s + n;
+  L.P.lost_pass = ctx->d_scratch_loss.ptr;
+  L.P.lost_elem = L.P.lost_pass + n;
+  /* one full pass starting at (p, e) */
+  L.pass_begin = p;
+  L.elem_begin = e;
+  L.pass_end = e == 0 ? p : p + 1;
+  L.elem_end = e == 0 ? ne : e;
+  cudaEvent_t ev0, ev1;
+  CUDA_TRY(ctx, cudaEventCreate(&ev0));
+  CUDA_TRY(ctx, cudaEventCreate(&ev1));
+  double *dst[6] = {L.P.x, L.P.xp, L.P.y, L.P.yp, L.P.s, L.P.dp};
+  float best = 1e30f;
+  int best_v = 1;
+  ctx->tune_ms.assign(B2E_RING_VARIANTS, 0.f);
+  for (int v = 1; v <= B2E_RING_VARIANTS; v++) {
+    for (int c = 0; c < 6; c++)
+      CUDA_TRY(ctx, cudaMemcpyAsync(dst[c], cols[c], sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(L.P.lost_pass, Lreal.P.lost_pass, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(ev0, ctx->stream));
+    CUDA_TRY(ctx, launch_ring(L, (int)ctx->tiles.size(), staged, staged ? smem : 0, ctx->stream, v));
+    CUDA_TRY(ctx, cudaEventRecord(ev1, ctx->stream));
+    CUDA_TRY(ctx, cudaEventSynchronize(ev1));
+    float ms = 0;
+    CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ev0, ev1));
+    ctx->tune_ms[v - 1] = ms;
+    if (ms < best) {
+      best = ms;
+      best_v = v;
+    }
+    ctx->launches++;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  ctx->tuned_variant = best_v;
+  return B2E_OK;
+}
+
 /* Track element range [(pb, eb), (pe, ee)) with ring launches, splitting at CSR elements. */
 static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   const int ne = (int)ctx->lat.elems.size();
@@ -339,6 +410,16 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
+  int variant = ctx->opt.ring_variant;
+  if (variant < 1 || variant > B2E_RING_VARIANTS) {
+    /* autotune once per context on a multi-pass range of a large enough beam */
+    if (!ctx->tuned_variant && pe > pb && ctx->n >= 16384) {
+      int rc = autotune_ring(ctx, L, staged, smem, pb, eb);
+      if (rc)
+        return rc;
+    }
+    variant = ctx->tuned_variant ? ctx->tuned_variant : 1;
+  }
   int p = pb, e = eb;
   while (p < pe || (p == pe && e < ee)) {
     /* end of this launch: at most ppl passes, never past (pe, ee) */
@@ -352,7 +433,7 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
     L.elem_begin = e;
     L.pass_end = lp;
     L.elem_end = le;
-    CUDA_TRY(ctx, launch_ring(L, (int)ctx->tiles.size(), staged, staged ? smem : 0, ctx->stream));
+    CUDA_TRY(ctx, launch_ring(L, (int)ctx->tiles.size(), staged, staged ? smem : 0, ctx->stream, variant));
     ctx->launches += ctx->tiles.empty() ? 0 : 1;
     if (le >= ne) {
       p = lp + 1;

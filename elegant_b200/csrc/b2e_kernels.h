@@ -22,7 +22,9 @@ struct RingLaunch {
   unsigned int *error_flag;
 };
 
-cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream);
+/* variant 1..B2E_RING_VARIANTS selects the occupancy target (see ring_kernel). */
+cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
+                        int variant);
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
                             cudaStream_t stream);

@@ -28,8 +28,12 @@ namespace b2e {
 
 
 
-template <bool STAGED>
-__global__ void __launch_bounds__(128) ring_kernel(RingLaunch L) {
+/* MINB is the occupancy target (blocks of 128 threads per SM) handed to the
+ * register allocator: 4 keeps every value in registers (~116 registers),
+ * 5/6/8 trade a few spills to L1 for more resident warps to hide FP64
+ * latency.  The arithmetic is identical in every variant. */
+template <bool STAGED, int MINB>
+__global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
   extern __shared__ __align__(16) unsigned char smem[];
   const DevTile tile = L.tiles[blockIdx.x];
   const DevElem *elems = L.elems + (size_t)tile.inst * L.n_elems;
@@ -196,19 +200,35 @@ __global__ void effort_kernel(const int32_t *lost_pass, int64_t n, int pass_begi
   }
 }
 
-cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream) {
-  if (n_tiles <= 0)
-    return cudaSuccess;
+template <int MINB>
+static cudaError_t launch_ring_v(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
+                                 cudaStream_t stream) {
   if (staged) {
-    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem_bytes);
     if (err != cudaSuccess)
       return err;
-    ring_kernel<true><<<n_tiles, 128, smem_bytes, stream>>>(L);
+    ring_kernel<true, MINB><<<n_tiles, 128, smem_bytes, stream>>>(L);
   } else {
-    ring_kernel<false><<<n_tiles, 128, 0, stream>>>(L);
+    ring_kernel<false, MINB><<<n_tiles, 128, 0, stream>>>(L);
   }
   return cudaGetLastError();
+}
+
+cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
+                        int variant) {
+  if (n_tiles <= 0)
+    return cudaSuccess;
+  switch (variant) {
+  case 2:
+    return launch_ring_v<5>(L, n_tiles, staged, smem_bytes, stream);
+  case 3:
+    return launch_ring_v<6>(L, n_tiles, staged, smem_bytes, stream);
+  case 4:
+    return launch_ring_v<8>(L, n_tiles, staged, smem_bytes, stream);
+  default:
+    return launch_ring_v<4>(L, n_tiles, staged, smem_bytes, stream);
+  }
 }
 
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,

@@ -38,7 +38,7 @@ class Tracker:
     """One engine context bound to a lattice and run options."""
 
     def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
-                 passes_per_launch: int = 0):
+                 passes_per_launch: int = 0, ring_variant: int = 0):
         self.lib = nat.load_library()
         self.lattice = lattice
         self._ctx = ctypes.c_void_p()
@@ -47,7 +47,7 @@ class Tracker:
             raise nat.EngineError(rc, "b2e_create failed (is a CUDA device visible?)")
         self.options = nat.RunOptions(p_central=p_central, n_passes=n_passes, default_order=default_order,
                                       coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
-                                      threads_per_block=0)
+                                      ring_variant=ring_variant)
         self._elems = lattice.to_ctypes()
         self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
         self.n_instances = 1
@@ -136,6 +136,13 @@ class Tracker:
         self._check(self.lib.b2e_download(self._ctx, ptrs, ids.ctypes.data, lost_pass.ctypes.data,
                                           lost_elem.ctypes.data, ctypes.byref(n_left)))
         return TrackResult(np.stack(cols, axis=1), ids, lost_pass, lost_elem, int(n_left.value), float("nan"))
+
+    def ring_tuning(self):
+        """(variant in use, per-variant ms of one pass) from the autotuner."""
+        chosen = ctypes.c_int32()
+        ms = (ctypes.c_float * 4)()
+        self._check(self.lib.b2e_ring_tuning(self._ctx, ctypes.byref(chosen), ms))
+        return int(chosen.value), [float(x) for x in ms]
 
     @property
     def launches(self) -> int:

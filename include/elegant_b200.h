@@ -65,6 +65,7 @@ extern "C" {
 #define B2E_CSRDRIFT 11
 
 #define B2E_MAX_PARAMS 40
+#define B2E_RING_VARIANTS 4
 
 /* Parameter slot indices, per element type.  Slot names are elegant's
  * parameter names (track_data.c tables cited per type). */
@@ -164,7 +165,8 @@ typedef struct {
   double coord_limit;      /* global_settings coord_limit (10 m) */
   double slope_limit;      /* global_settings slope_limit (1) */
   int32_t passes_per_launch; /* 0 = all passes of a step in one launch */
-  int32_t threads_per_block; /* 0 = engine default */
+  int32_t ring_variant;    /* ring-kernel occupancy variant: 0 = autotune on first use,
+                              1..B2E_RING_VARIANTS = fixed (all variants give identical results) */
 } b2e_run_options;
 
 typedef struct b2e_ctx b2e_ctx;
@@ -200,6 +202,10 @@ void *b2e_stream(b2e_ctx *ctx);
 
 /* Number of kernels this context has launched so far (instrumentation). */
 int64_t b2e_kernel_launches(const b2e_ctx *ctx);
+
+/* Ring-kernel autotuning result: the variant in use (0 = not tuned yet) and
+ * the time of one pass per variant in ms (B2E_RING_VARIANTS floats, may be NULL). */
+int b2e_ring_tuning(const b2e_ctx *ctx, int32_t *chosen, float *ms_per_variant);
 
 /* Downloads survivors and losses.  Columns receive all n particles in upload
  * order; lost_pass[i] is -1 for survivors or the pass on which particle i

@@ -128,3 +128,24 @@ def test_ensemble_matches_per_instance_reference(ref_b2e):
         sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
                         int((res.lost_pass[sl] < 0).sum()), 0.0)
         assert_parity(sub, rows, nl)
+
+
+def test_kernel_variants_identical():
+    """Every occupancy variant the autotuner may pick gives identical results."""
+    lat = w.fodo_ring()
+    beam = w.ring_beam(400, seed=21)
+    ref = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=1)
+    for v in (2, 3, 4):
+        r = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=v)
+        assert np.array_equal(r.coords, ref.coords)
+        assert np.array_equal(r.lost_pass, ref.lost_pass)
+
+
+def test_autotuner_picks_a_variant():
+    lat = w.fodo_ring()
+    beam = w.ring_beam(20000, seed=8)
+    with Tracker(lat, w.ring_p_central(), 3) as t:
+        t.track(beam)
+        chosen, ms = t.ring_tuning()
+    assert 1 <= chosen <= 4
+    assert all(m > 0 for m in ms)
