@@ -1,0 +1,922 @@
+/*
+ * CPU oracle: a plain-C restatement of elegant's particle-tracking hot path
+ * for the element subset of the CUDA engine (test infrastructure only; the
+ * product never calls this code).
+ *
+ * It follows the reference's own data layout and control flow: particles are
+ * rows of doubles (x, xp, y, yp, s, delta, id, lossPass), lost particles are
+ * swapped to the tail of the array as the reference does, and every
+ * floating-point expression keeps the reference's operation order, so with
+ * the same elementary functions it reproduces the reference bit for bit.
+ *
+ * Elementary functions: compiled with -DB2E_ORACLE_LIBM it calls glibc like
+ * the reference; otherwise sin/cos/tan/asin are the shared implementations of
+ * elegant_b200/csrc/b2e_math.h that the CUDA engine uses.
+ *
+ * Sources restated (file:line in the reference tree):
+ *   do_tracking        do_tracking.c:488-2640 (pass/element loop, z bookkeeping
+ *                      :1077-1084, sticky MAXAMP :1848-1858, aperture after
+ *                      each element :2455-2475, NaN sweep :2629, loss record
+ *                      :4584-4605, effort :2758-2764)
+ *   track_particles    matrix.c:294-469 (order-2 contraction :390-419)
+ *   drift_matrix       compute_matrices.c:391-412
+ *   exactDrift         csbend.c:3767-3790
+ *   multipole_tracking2 multipole.c:693-1117
+ *   integrate_kick_multipole_ordn multipole.c:1122-1410
+ *   apply_canonical_multipole_kicks, expansion_coefficients, fillPowerArray,
+ *   convertSlopesToMomenta/MomentaToSlopes multipole.h:173-280
+ *   checkMultAperture  multipole.c:1786-1832
+ *   offsetBeamCoordinatesForMisalignment malign_mat.c:172-182
+ *   offsetParticlesForMisalignment (mode 0) malign_mat.c:480-531
+ *   rotateBeamCoordinatesForMisalignment tilt_matrices.c:156-183
+ *   track_through_csbend csbend.c:665-1409; integrate_csbend_ordn csbend.c:1434-1693
+ *   convert{To,From}DipoleCanonicalCoordinates csbend.c:1411-1429
+ *   computeCSBENDFields (pure dipole fast path) csbend.c:101-110
+ *   trackRfCavityWithWakes simple_rfca.c:295-985; findFiducialTime :62-262;
+ *   add_to_particle_energy :987-1006; KahanPlus kahan.c:28-35
+ *   limit_amplitudes / removeInvalidParticles / elimit_amplitudes
+ *                      limit_amplitudes.c:193-315, :472-600
+ *   swapParticles      elegant.c:2663-2670; beta_from_delta do_tracking.c:95
+ */
+#include <math.h>
+#include <float.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "../include/elegant_b200.h"
+
+#ifdef B2E_ORACLE_LIBM
+#define M_SIN(x) sin(x)
+#define M_COS(x) cos(x)
+#define M_TAN(x) tan(x)
+#define M_ASIN(x) asin(x)
+#else
+#include "../elegant_b200/csrc/b2e_math.h"
+#define M_SIN(x) b2e_sin(x)
+#define M_COS(x) b2e_cos(x)
+#define M_TAN(x) b2e_tan(x)
+#define M_ASIN(x) b2e_asin(x)
+#endif
+
+#define NPROP 8 /* x, xp, y, yp, s, delta, id, lossPass */
+#define C_MKS 2.99792458e8
+#define ME_MEV 0.51099895000
+#define ME_MKS 9.1093837015e-31
+#define E_MKS 1.602176634e-19
+#define RE_MKS 2.8179403262e-15
+#define PI_ 3.141592653589793238462643383279502884
+#define BETA_ 1.25992104989487316477
+#define SQR(x) ((x) * (x))
+
+static double coord_limit = 10, slope_limit = 1;
+
+/* ---- small helpers ------------------------------------------------------ */
+static void swap_rows(double *a, double *b) {
+  double t[NPROP];
+  if (a == b)
+    return;
+  memcpy(t, a, sizeof(t));
+  memcpy(a, b, sizeof(t));
+  memcpy(b, t, sizeof(t));
+}
+
+static double ipow_(double x, long n) {
+  double r = x;
+  long i;
+  if (n == 0)
+    return 1;
+  for (i = 1; i < n; i++)
+    r *= x;
+  return r;
+}
+
+static int fractions(int order, double *df, double *kf) {
+  static const double d6[8] = {0.39225680523878,   0.5100434119184585,   -0.47105338540975655, 0.0687531682525181,
+                               0.0687531682525181, -0.47105338540975655, 0.5100434119184585,   0.39225680523878};
+  static const double k6[8] = {0.784513610477560,  0.235573213359357, -1.17767998417887, 1.3151863206839063,
+                               -1.17767998417887, 0.235573213359357, 0.784513610477560, 0};
+  int j;
+  if (order == 2) {
+    df[0] = df[1] = 0.5;
+    kf[0] = 1.0;
+    kf[1] = 0.0;
+    return 2;
+  }
+  if (order == 4) {
+    df[0] = 0.5 / (2 - BETA_);
+    df[1] = (1 - BETA_) / (2 - BETA_) / 2;
+    df[2] = (1 - BETA_) / (2 - BETA_) / 2;
+    df[3] = 0.5 / (2 - BETA_);
+    kf[0] = 1. / (2 - BETA_);
+    kf[1] = -BETA_ / (2 - BETA_);
+    kf[2] = 1 / (2 - BETA_);
+    kf[3] = 0;
+    return 4;
+  }
+  if (order == 6) {
+    for (j = 0; j < 8; j++) {
+      df[j] = d6[j];
+      kf[j] = k6[j];
+    }
+    return 8;
+  }
+  return 0;
+}
+
+/* ---- apertures ---------------------------------------------------------- */
+typedef struct {
+  int present; /* a MAXAMP has been seen */
+  double x_max, y_max;
+  long elliptical, exponent, y_exponent;
+} MaxAmp;
+
+typedef struct {
+  double xMax, yMax, reverseTilt, rc, rs;
+  long elliptical, xe, ye;
+} MultAp;
+
+static void setup_mult_ap(MultAp *a, double reverseTilt, const MaxAmp *m) {
+  a->reverseTilt = reverseTilt;
+  a->rc = M_COS(reverseTilt);
+  a->rs = M_SIN(reverseTilt);
+  a->xMax = a->yMax = 0;
+  a->elliptical = 0;
+  a->xe = a->ye = 2;
+  if (m && m->present) {
+    a->xMax = m->x_max;
+    a->yMax = m->y_max;
+    a->elliptical = m->elliptical;
+    a->xe = a->ye = m->exponent;
+    if (m->y_exponent)
+      a->ye = m->y_exponent;
+  }
+}
+
+static int mult_ap_ok(double xIn, double yIn, const MultAp *a) {
+  double x = xIn - 0.0, y = yIn - 0.0;
+  if (a->reverseTilt) {
+    double x0 = x, y0 = y;
+    x = x0 * a->rc + y0 * a->rs;
+    y = -x0 * a->rs + y0 * a->rc;
+  }
+  if (a->elliptical == 0 || a->xMax <= 0 || a->yMax <= 0) {
+    if ((a->xMax > 0 && fabs(x) > a->xMax) || (a->yMax > 0 && fabs(y) > a->yMax))
+      return 0;
+  } else {
+    double xa = x / a->xMax, yb = y / a->yMax;
+    if ((ipow_(xa, a->xe) + ipow_(yb, a->ye)) >= 1)
+      return 0;
+  }
+  return 1;
+}
+
+static long limit_amps(double **c, double xmax, double ymax, long np, double z, double Po, int extrap) {
+  long ip, itop = np - 1;
+  if (xmax < 0 && ymax < 0)
+    return np;
+  for (ip = 0; ip < np; ip++) {
+    double *part = c[ip], dz = 0;
+    long is_out = 0;
+    if (xmax > 0 && fabs(part[0]) > xmax)
+      is_out += 1;
+    if (ymax > 0 && fabs(part[2]) > ymax)
+      is_out += 2;
+    if (isinf(part[0]) || isinf(part[2]) || isnan(part[0]) || isnan(part[2]))
+      is_out += 4;
+    if (is_out && !(is_out & 4) && extrap) {
+      double dzx = -DBL_MAX, dzy = -DBL_MAX;
+      if (is_out & 1 && part[1] != 0)
+        dzx = (part[0] - (part[1] < 0 ? -1 : 1) * xmax) / part[1];
+      if (is_out & 2 && part[3] != 0)
+        dzy = (part[2] - (part[3] < 0 ? -1 : 1) * ymax) / part[3];
+      dz = dzx > dzy ? -dzx : -dzy;
+      if (dz == -DBL_MAX)
+        dz = 0;
+    }
+    if (is_out) {
+      if (ip != itop)
+        swap_rows(c[ip], c[itop]);
+      c[itop][0] += dz * c[itop][1];
+      c[itop][2] += dz * c[itop][3];
+      c[itop][4] = z + dz;
+      c[itop][5] = Po * (1 + c[itop][5]);
+      --itop;
+      --ip;
+      np--;
+    }
+  }
+  return np;
+}
+
+static long elimit_amps(double **c, double xmax, double ymax, long np, double z, double Po, int extrap, long xe,
+                        long ye) {
+  long ip, itop = np - 1;
+  double a2, b2;
+  if (!ye)
+    ye = xe;
+  if (xmax <= 0 || ymax <= 0) {
+    if (xmax > 0 || ymax > 0)
+      return limit_amps(c, xmax, ymax, np, z, Po, extrap);
+    return np;
+  }
+  a2 = ipow_(xmax, xe);
+  b2 = ipow_(ymax, ye);
+  for (ip = 0; ip < np; ip++) {
+    double *part = c[ip], dz = 0;
+    if (isinf(part[0]) || isinf(part[2]) || isnan(part[0]) || isnan(part[2])) {
+      swap_rows(c[ip], c[itop]);
+      c[itop][4] = z;
+      c[itop][5] = sqrt(SQR(Po * (1 + c[itop][5])) + 1);
+      --itop;
+      --ip;
+      np--;
+      continue;
+    }
+    if (!((ipow_(part[0], xe) / a2 + ipow_(part[2], ye) / b2) > 1))
+      continue;
+    if (extrap && xe == 2 && ye == 2) {
+      double c0 = SQR(part[0]) / a2 + SQR(part[2]) / b2 - 1;
+      double c1 = 2 * (part[0] * part[1] / a2 + part[2] * part[3] / b2);
+      double c2 = SQR(part[1]) / a2 + SQR(part[3]) / b2;
+      double det = SQR(c1) - 4 * c0 * c2;
+      if (z > 0 && c2 && det >= 0) {
+        if ((dz = (-c1 + sqrt(det)) / (2 * c2)) > 0)
+          dz = (-c1 - sqrt(det)) / (2 * c2);
+        if ((z + dz) < 0)
+          dz = -z;
+        part[0] += dz * part[1];
+        part[2] += dz * part[3];
+      }
+    }
+    swap_rows(c[ip], c[itop]);
+    c[itop][4] = z + dz;
+    c[itop][5] = sqrt(SQR(Po * (1 + c[itop][5])) + 1);
+    --itop;
+    --ip;
+    np--;
+  }
+  return np;
+}
+
+/* ---- DRIF: order-2 contraction of the drift matrix ------------------------ */
+static void drift_track(double **c, long np, double L, int order) {
+  /* C/R/T of drift_matrix; T stored lower-triangular T[i][j][k], k <= j */
+  double C[6] = {0, 0, 0, 0, L, 0}, R[6][6], T[6][6][6];
+  long ip, i, j, k;
+  memset(R, 0, sizeof(R));
+  memset(T, 0, sizeof(T));
+  for (i = 0; i < 6; i++)
+    R[i][i] = 1;
+  R[0][1] = R[2][3] = L;
+  if (order > 1)
+    T[4][1][1] = T[4][3][3] = L / 2;
+  for (ip = np - 1; ip >= 0; ip--) {
+    double *ini = c[ip], tmp[6];
+    for (i = 5; i >= 0; i--) {
+      double sum = C[i];
+      if (order >= 2) {
+        for (j = 5; j >= 0; j--) {
+          double cj = ini[j];
+          if (cj) {
+            double sum1 = R[i][j];
+            for (k = j; k >= 0; k--)
+              sum1 += T[i][j][k] * ini[k];
+            sum += sum1 * cj;
+          }
+        }
+      } else {
+        for (j = 5; j >= 0; j--)
+          sum += R[i][j] * ini[j];
+      }
+      tmp[i] = sum;
+    }
+    for (i = 5; i >= 0; i--)
+      ini[i] = tmp[i];
+  }
+}
+
+static void exact_drift(double **c, long np, double L) {
+  long i;
+  for (i = 0; i < np; i++) {
+    double *x = c[i];
+    x[0] += x[1] * L;
+    x[2] += x[3] * L;
+    x[4] += L * sqrt(1 + SQR(x[1]) + SQR(x[3]));
+  }
+}
+
+/* ---- misalignment ----------------------------------------------------------- */
+static void offset_beam(double **c, long np, double dx, double dy, double dz) {
+  long ip;
+  for (ip = np - 1; ip >= 0; ip--) {
+    double *p = c[ip];
+    p[4] += dz * sqrt(1 + SQR(p[1]) + SQR(p[3]));
+    p[0] = p[0] - dx + dz * p[1];
+    p[2] = p[2] - dy + dz * p[3];
+  }
+}
+
+static void rotate_beam(double **c, long np, double angle) {
+  double ca, sa;
+  long i;
+  if (!angle || fabs(fabs(angle) - 2 * PI_) < 1e-12)
+    return;
+  if (fabs(fabs(angle) - PI_) < 1e-12) {
+    ca = -1;
+    sa = 0;
+  } else if (fabs(angle - PI_ / 2) < 1e-12) {
+    ca = 0;
+    sa = 1;
+  } else if (fabs(angle + PI_ / 2) < 1e-12) {
+    ca = 0;
+    sa = -1;
+  } else {
+    ca = M_COS(angle);
+    sa = M_SIN(angle);
+  }
+  for (i = 0; i < np; i++) {
+    double *p = c[i], x = p[0], xp = p[1], y = p[2], yp = p[3];
+    p[0] = x * ca + y * sa;
+    p[2] = -x * sa + y * ca;
+    p[1] = xp * ca + yp * sa;
+    p[3] = -xp * sa + yp * ca;
+  }
+}
+
+/* ---- KQUAD / KSEXT ---------------------------------------------------------- */
+static int m2s(double *xp, double *yp, double qx, double qy, double dp) {
+  double d = SQR(1 + dp) - SQR(qx) - SQR(qy);
+  if (d <= 0)
+    return 0;
+  d = sqrt(d);
+  *xp = qx / d;
+  *yp = qy / d;
+  return 1;
+}
+
+static void canonical_kick(double *qx, double *qy, double x, double y, long order, double KnL, int skew) {
+  /* apply_canonical_multipole_kicks with expansion coefficients of (x+iy)^n/n! */
+  double xpow[4], ypow[4], coef[4], sFx = 0, sFy = 0, fi = 1, fni;
+  long i, m;
+  xpow[0] = ypow[0] = 1;
+  for (i = 1; i <= order; i++) {
+    xpow[i] = xpow[i - 1] * x;
+    ypow[i] = ypow[i - 1] * y;
+  }
+  for (i = 0; i <= order; i++) {
+    fi = 1;
+    for (m = 2; m <= i; m++)
+      fi *= m;
+    fni = 1;
+    for (m = 2; m <= order - i; m++)
+      fni *= m;
+    coef[i] = (((i / 2) & 1) ? -1.0 : 1.0) / (fi * fni);
+  }
+  for (i = 1; i <= order; i += 2)
+    sFx += coef[i] * xpow[order - i] * ypow[i];
+  for (i = 0; i <= order; i += 2)
+    sFy += coef[i] * xpow[order - i] * ypow[i];
+  if (skew) {
+    double t = sFx;
+    sFx = sFy;
+    sFy = t;
+    sFx = -sFx;
+  }
+  *qx -= KnL * sFy;
+  *qy += KnL * sFx;
+}
+
+static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma) {
+  const double *p = e->p;
+  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt;
+  long order[3] = {0, 0, 0}, nSlices, n_kicks, ip, itop;
+  int skew[3] = {0, 0, 0}, integ, nSub, radblock;
+  MultAp ap;
+  double dzLoss = 0;
+  drift = p[B2E_KMULT_L];
+  integ = (int)p[B2E_KMULT_INTEGRATION_ORDER];
+  nSlices = (long)p[B2E_KMULT_N_SLICES];
+  n_kicks = (long)p[B2E_KMULT_N_KICKS];
+  dx = p[B2E_KMULT_DX];
+  dy = p[B2E_KMULT_DY];
+  dz = p[B2E_KMULT_DZ];
+  tilt = p[B2E_KMULT_TILT];
+  if (e->type == B2E_KQUAD) {
+    order[0] = 1;
+    KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
+  } else {
+    order[0] = 2;
+    KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
+    if (p[B2E_KMULT_K1_OF_KSEXT]) {
+      KnL[1] = p[B2E_KMULT_K1_OF_KSEXT] * drift;
+      order[1] = 1;
+    }
+    if (p[B2E_KMULT_J1_OF_KSEXT]) {
+      KnL[2] = p[B2E_KMULT_J1_OF_KSEXT] * drift;
+      order[2] = 1;
+      skew[2] = 1;
+    }
+  }
+  nSub = fractions(integ, df, kf);
+  if (n_kicks > 0) {
+    if (integ > 2) {
+      if ((nSlices = (long)ceil(n_kicks / (1.0 * integ))) < 1)
+        nSlices = 1;
+    } else
+      nSlices = n_kicks;
+  }
+  setup_mult_ap(&ap, -tilt, ma);
+  /* entrance misalignment, mode 0 face 1 */
+  if (dx || dy || dz)
+    offset_beam(c, np, dx, dy, dz);
+  if (tilt)
+    rotate_beam(c, np, tilt);
+  radblock = 1; /* isr_coef is nonzero (negated) when ISR is off */
+  itop = np - 1;
+  for (ip = 0; ip <= itop; ip++) {
+    double *coord = c[ip], x, xp, y, yp, s, dpv, qx, qy, denom, dr;
+    long i_kick, step, io;
+    int lost = 0;
+    dr = drift / nSlices;
+    x = coord[0];
+    xp = coord[1];
+    y = coord[2];
+    yp = coord[3];
+    s = 0;
+    dpv = coord[5];
+    if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp))
+      lost = 1;
+    else if (fabs(x) > coord_limit || fabs(y) > coord_limit || fabs(xp) > slope_limit || fabs(yp) > slope_limit)
+      lost = 1;
+    if (!lost) {
+      denom = sqrt(1 + SQR(xp) + SQR(yp));
+      qx = (1 + dpv) * xp / denom;
+      qy = (1 + dpv) * yp / denom;
+      if (!m2s(&xp, &yp, qx, qy, dpv))
+        lost = 1;
+    }
+    if (!lost) {
+      dzLoss = 0;
+      for (i_kick = 0; i_kick < nSlices && !lost; i_kick++) {
+        if (!mult_ap_ok(x + dx, y + dy, &ap)) {
+          coord[0] = x;
+          coord[2] = y;
+          lost = 1;
+          break;
+        }
+        for (step = 0; step < nSub; step++) {
+          if (dr) {
+            double dsh = dr * df[step];
+            x += xp * dsh;
+            y += yp * dsh;
+            s += dsh * sqrt(1 + SQR(xp) + SQR(yp));
+            dzLoss += dsh;
+          }
+          if (!kf[step])
+            break;
+          for (io = 0; io < 3; io++)
+            if (KnL[io])
+              canonical_kick(&qx, &qy, x, y, order[io], KnL[io] / nSlices * kf[step], skew[io]);
+          if (!m2s(&xp, &yp, qx, qy, dpv)) {
+            lost = 1;
+            break;
+          }
+          if (radblock && dr) {
+            qx /= (1 + dpv);
+            qy /= (1 + dpv);
+            qx *= (1 + dpv);
+            qy *= (1 + dpv);
+            if (!m2s(&xp, &yp, qx, qy, dpv)) {
+              lost = 1;
+              break;
+            }
+          }
+        }
+      }
+      if (!lost && !mult_ap_ok(x + dx, y + dy, &ap)) {
+        coord[0] = x;
+        coord[2] = y;
+        lost = 1;
+      }
+      if (!lost && !m2s(&xp, &yp, qx, qy, dpv))
+        lost = 1;
+      if (!lost) {
+        coord[0] = x;
+        coord[1] = xp;
+        coord[2] = y;
+        coord[3] = yp;
+        coord[4] += s;
+        coord[5] = dpv;
+        if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > coord_limit || fabs(y) > coord_limit ||
+            fabs(xp) > slope_limit || fabs(yp) > slope_limit)
+          lost = 1;
+      }
+    }
+    if (lost) {
+      swap_rows(c[ip], c[itop]);
+      c[itop][4] = z_start + dzLoss;
+      c[itop][5] = Po * (1 + c[itop][5]);
+      itop--;
+      ip--;
+    }
+  }
+  /* exit misalignment, face 2, applied to all np rows like the reference */
+  if (dx || dy || dz || tilt) {
+    if (tilt)
+      rotate_beam(c, np, -tilt);
+    if (dx || dy || dz)
+      offset_beam(c, np, -dx, -dy, -dz);
+  }
+  return itop + 1;
+}
+
+/* ---- CSBEND ------------------------------------------------------------- */
+static int csbend_integrate(double *Qf, const double *Qi, double s, long n, double rho0, double rho_actual,
+                            const MultAp *ap, int integ, int isr_block, double *dz_lost) {
+  double df[8], kf[8];
+  int nSub = fractions(integ, df, kf), i, j;
+  double dist = 0;
+  memcpy(Qf, Qi, sizeof(double) * 6);
+  s /= n;
+  *dz_lost = 0;
+  for (i = 0; i < n; i++) {
+    if (!mult_ap_ok(Qf[0], Qf[2], ap))
+      return 0;
+    for (j = 0; j < nSub; j++) {
+      double dsh = s * df[j], f, sin_phi, phi, sine, cosi, tang, cos_phi, factor, ds;
+      f = SQR(1 + Qf[5]) - SQR(Qf[3]);
+      if (f <= 0)
+        return 0;
+      f = sqrt(f);
+      if (fabs(Qf[1] / f) > 1)
+        return 0;
+      sin_phi = Qf[1] / f;
+      phi = M_ASIN(sin_phi);
+      sine = M_SIN(dsh / rho0 + phi);
+      cosi = M_COS(dsh / rho0 + phi);
+      if (cosi == 0)
+        return 0;
+      tang = sine / cosi;
+      cos_phi = M_COS(phi);
+      Qf[1] = f * sine;
+      factor = (rho0 + Qf[0]) * cos_phi / f * (tang - sin_phi / cos_phi);
+      Qf[2] += Qf[3] * factor;
+      dist += factor * (1 + Qf[5]);
+      *dz_lost += dsh;
+      f = cos_phi / cosi;
+      Qf[0] = rho0 * (f - 1) + f * Qf[0];
+      if (kf[j] == 0)
+        break;
+      ds = s * kf[j];
+      /* pure dipole: Fx = 0, Fy = 1 */
+      Qf[1] += -ds * (1 + Qf[0] / rho0) * 1.0 / rho_actual;
+      Qf[3] += ds * (1 + Qf[0] / rho0) * 0.0 / rho_actual;
+      if (isr_block) {
+        Qf[1] /= (1 + Qf[5]);
+        Qf[3] /= (1 + Qf[5]);
+        Qf[1] *= (1 + Qf[5]);
+        Qf[3] *= (1 + Qf[5]);
+      }
+    }
+  }
+  *dz_lost = n * s;
+  if (!mult_ap_ok(Qf[0], Qf[2], ap))
+    return 0;
+  Qf[4] += dist;
+  return 1;
+}
+
+static int same_bend(const b2e_element *a, const b2e_element *b) {
+  return a->type == b->type && strncmp(a->name, b->name, sizeof(a->name)) == 0;
+}
+
+static long csbend_track(double **c, long np, const b2e_element *el, int idx, const b2e_element *all, int n_all,
+                         double Po, double z_start, const MaxAmp *ma) {
+  const double *p = el->p;
+  double angle, e1, e2, tilt, rho0, rho_actual, fse, h, psi1, psi2, Kg1, Kg2, ttilt, ct, st;
+  double dxi, dyi, dzi, dxf, dyf, dzf, length = p[B2E_BEND_L];
+  int edge1 = 0, edge2 = 0, j, integ = (int)p[B2E_BEND_INTEGRATION_ORDER];
+  long nSlices = (long)p[B2E_BEND_N_SLICES], ip, itop;
+  MultAp ap;
+  if (p[B2E_BEND_ANGLE] == 0) {
+    exact_drift(c, np, length);
+    return np;
+  }
+  /* determine_bend_flags (bend_matrix.c:1342-1391) */
+  {
+    int pre = 0, post = 0;
+    for (j = idx - 1; j >= 0; j--) {
+      if (same_bend(&all[j], el)) {
+        pre = 1;
+        break;
+      }
+      if (all[j].type != B2E_MARK)
+        break;
+    }
+    for (j = idx + 1; j < n_all; j++) {
+      if (same_bend(&all[j], el)) {
+        post = 1;
+        break;
+      }
+      if (all[j].type != B2E_MARK)
+        break;
+    }
+    edge1 = p[B2E_BEND_EDGE1_EFFECTS] && !pre;
+    edge2 = p[B2E_BEND_EDGE2_EFFECTS] && !post;
+  }
+  rho0 = length / p[B2E_BEND_ANGLE];
+  if (p[B2E_BEND_ANGLE] < 0) {
+    angle = -p[B2E_BEND_ANGLE];
+    e1 = -p[B2E_BEND_E1];
+    e2 = -p[B2E_BEND_E2];
+    tilt = p[B2E_BEND_TILT] + PI_;
+    rho0 = length / angle;
+  } else {
+    angle = p[B2E_BEND_ANGLE];
+    e1 = p[B2E_BEND_E1];
+    e2 = p[B2E_BEND_E2];
+    tilt = p[B2E_BEND_TILT];
+    rho0 = length / angle;
+  }
+  setup_mult_ap(&ap, -tilt, ma);
+  fse = p[B2E_BEND_FSE] + 0.0;
+  h = 1 / rho0;
+  if (fabs(fse + 1) < 1e-12)
+    fse = -1 + 1e-12;
+  rho_actual = 1 / ((1 + fse) * h);
+  Kg1 = Kg2 = 2 * p[B2E_BEND_HGAP] * p[B2E_BEND_FINT] * (rho0 < 0 ? -1 : 1);
+  psi1 = Kg1 / fabs(rho_actual) / M_COS(e1) * (1 + SQR(M_SIN(e1)));
+  psi2 = Kg2 / fabs(rho_actual) / M_COS(e2) * (1 + SQR(M_SIN(e2)));
+  if (length < 0) {
+    psi1 *= -1;
+    psi2 *= -1;
+  }
+  ttilt = tilt + p[B2E_BEND_ETILT];
+  if (ttilt == 0) {
+    ct = 1;
+    st = 0;
+  } else if (fabs(fabs(ttilt) - PI_) < 1e-12) {
+    ct = -1;
+    st = 0;
+  } else if (fabs(ttilt - PI_ / 2) < 1e-12) {
+    ct = 0;
+    st = 1;
+  } else if (fabs(ttilt + PI_ / 2) < 1e-12) {
+    ct = 0;
+    st = -1;
+  } else {
+    ct = M_COS(ttilt);
+    st = M_SIN(ttilt);
+  }
+  dxi = -p[B2E_BEND_DX];
+  dzi = p[B2E_BEND_DZ];
+  dyi = -p[B2E_BEND_DY];
+  dxf = p[B2E_BEND_DX] * M_COS(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * M_SIN(p[B2E_BEND_ANGLE]);
+  dzf = p[B2E_BEND_DX] * M_SIN(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * M_COS(p[B2E_BEND_ANGLE]);
+  dyf = p[B2E_BEND_DY];
+  itop = np - 1;
+  for (ip = 0; ip <= itop; ip++) {
+    double *coord = c[ip], x, y, xp, yp, s, dp, dp0, Qi[6], Qf[6], rho, f, dz_lost;
+    int lost;
+    coord[4] += dzi * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+    coord[0] = coord[0] + dxi + dzi * coord[1];
+    coord[2] = coord[2] + dyi + dzi * coord[3];
+    x = coord[0] * ct + coord[2] * st;
+    y = -coord[0] * st + coord[2] * ct;
+    xp = coord[1] * ct + coord[3] * st;
+    yp = -coord[1] * st + coord[3] * ct;
+    s = coord[4];
+    dp = dp0 = coord[5];
+    if (edge1) {
+      rho = (1 + dp) * rho_actual;
+      xp += M_TAN(e1) / rho * x;
+      yp -= M_TAN(e1 - psi1 / (1 + dp)) / rho * y;
+    }
+    Qi[0] = x;
+    Qi[1] = xp;
+    Qi[2] = y;
+    Qi[3] = yp;
+    Qi[4] = 0;
+    Qi[5] = dp;
+    f = (1 + Qi[5]) / sqrt(1 + SQR(Qi[1]) + SQR(Qi[3]));
+    Qi[1] *= f;
+    Qi[3] *= f;
+    lost = !csbend_integrate(Qf, Qi, length, nSlices, rho0, rho_actual, &ap, integ, 1, &dz_lost);
+    f = 1 / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
+    Qf[1] *= f;
+    Qf[3] *= f;
+    if (lost) {
+      /* the reference converts back to lab coordinates (convertFromCSBendCoords)
+       * before recording; only the loss bookkeeping is reproduced here */
+      memcpy(coord, Qf, sizeof(double) * 4);
+      swap_rows(c[ip], c[itop]);
+      c[itop][4] = z_start + dz_lost;
+      c[itop][5] = Po * (1 + c[itop][5]);
+      itop--;
+      ip--;
+      continue;
+    }
+    {
+      double p0 = Po * (1 + dp0), beta0 = p0 / sqrt(SQR(p0) + 1);
+      double p1 = Po * (1 + Qf[5]), beta1 = p1 / sqrt(SQR(p1) + 1);
+      s = beta1 * s / beta0 + Qf[4];
+    }
+    x = Qf[0];
+    xp = Qf[1];
+    y = Qf[2];
+    yp = Qf[3];
+    dp = Qf[5];
+    if (edge2) {
+      rho = (1 + dp) * rho_actual;
+      xp += M_TAN(e2) / rho * x;
+      yp -= M_TAN(e2 - psi2 / (1 + dp)) / rho * y;
+    }
+    coord[0] = x * ct - y * st + 0.0;
+    coord[2] = x * st + y * ct + 0.0;
+    coord[1] = xp * ct - yp * st + 0.0;
+    coord[3] = xp * st + yp * ct + 0.0;
+    coord[4] = s + 0.0;
+    coord[5] = dp;
+    coord[0] += dxf + dzf * coord[1];
+    coord[2] += dyf + dzf * coord[3];
+    coord[4] += dzf * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+  }
+  return itop + 1;
+}
+
+/* ---- RFCA (zero length, TMEAN fiducial) ---------------------------------- */
+typedef struct {
+  int seen;
+  double phase_fiducial;
+} RfState;
+
+static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, double Po) {
+  const double *p = e->p;
+  double omega = (2 * PI_) * p[B2E_RFCA_FREQ];
+  double volt = p[B2E_RFCA_VOLT] / (1e6 * ME_MEV * 1) / 1;
+  double phase, t0;
+  long ip, itop;
+  if (np <= 0)
+    return np;
+  if (!rs->seen) {
+    if (p[B2E_RFCA_T_REFERENCE] != -1)
+      t0 = p[B2E_RFCA_T_REFERENCE];
+    else {
+      double tsum = 0, error = 0;
+      for (ip = 0; ip < np; ip++) {
+        double pp = Po * (1 + c[ip][5]);
+        double b = (c[ip][4] + 0.0 / 2) / (C_MKS * (pp / sqrt(pp * pp + 1)));
+        double Y = b + error, sum = tsum + Y;
+        error = Y - (sum - tsum);
+        tsum = sum;
+      }
+      t0 = tsum / np;
+    }
+    rs->phase_fiducial = -omega * t0;
+    rs->seen = 1;
+  }
+  phase = rs->phase_fiducial;
+  phase += p[B2E_RFCA_PHASE] * PI_ / 180.0;
+  for (ip = 0; ip < np; ip++) {
+    c[ip][0] -= p[B2E_RFCA_DX];
+    c[ip][2] -= p[B2E_RFCA_DY];
+  }
+  for (ip = 0; ip < np; ip++) {
+    double *coord = c[ip], P, gamma, beta_i, t, dgamma, gamma1, P1, Pz, Pz1;
+    if (coord[5] == -1)
+      continue;
+    P = Po * (1 + coord[5]);
+    beta_i = P / (gamma = sqrt(SQR(P) + 1));
+    t = (coord[4] + 0) / (C_MKS * beta_i) - 0;
+    dgamma = volt * M_SIN(omega * (t - 0 - 0 * 0.0) + phase) * 1;
+    /* add_to_particle_energy */
+    P = Po * (1 + coord[5]);
+    gamma1 = (gamma = sqrt(P * P + 1)) + dgamma;
+    if (gamma1 <= 1)
+      gamma1 = 1 + 1e-7;
+    P1 = sqrt(gamma1 * gamma1 - 1);
+    coord[5] = (P1 - Po) / Po;
+    coord[4] = t * C_MKS * P1 / gamma1;
+    Pz = P / sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+    Pz1 = sqrt(Pz * Pz + gamma1 * gamma1 - gamma * gamma);
+    coord[1] *= Pz / Pz1;
+    coord[3] *= Pz / Pz1;
+    if ((gamma1 = gamma + dgamma) <= 1)
+      coord[5] = -1;
+  }
+  itop = np - 1;
+  for (ip = 0; ip < np; ip++) {
+    c[ip][0] += p[B2E_RFCA_DX];
+    c[ip][2] += p[B2E_RFCA_DY];
+  }
+  /* removeInvalidParticles */
+  for (ip = 0; ip <= itop; ip++) {
+    double *part = c[ip];
+    int ic, out = 0;
+    for (ic = 0; ic < 6; ic++)
+      if (isnan(part[ic]))
+        out = 1;
+    if (part[5] <= -1)
+      out = 1;
+    if (out) {
+      swap_rows(c[ip], c[itop]);
+      c[itop][5] = Po * (1 + c[itop][5]);
+      itop--;
+      ip--;
+    }
+  }
+  return itop + 1;
+}
+
+/* ---- do_tracking restated ------------------------------------------------ */
+/* rows: np x 8 (x, xp, y, yp, s, delta, id, lossPass); lossPass must be -1 on
+ * input.  Returns survivors; rows are left in the reference's array order. */
+long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_passes, int default_order,
+                      double *rows, long np, double *effort) {
+  double **c = malloc(sizeof(double *) * (np ? np : 1));
+  long i, nToTrack = np, nLeft;
+  int pass, k;
+  MaxAmp ma;
+  RfState *rf = calloc(n_el ? n_el : 1, sizeof(RfState));
+  memset(&ma, 0, sizeof(ma));
+  for (i = 0; i < np; i++)
+    c[i] = rows + i * NPROP;
+  *effort = 0;
+  for (pass = 0; pass < n_passes; pass++) {
+    double z = 0, last_z = 0;
+    long start = nToTrack;
+    for (k = 0; k < n_el && nToTrack; k++) {
+      const b2e_element *e = &el[k];
+      const double *p = e->p;
+      int no_aperture = (e->type == B2E_MARK || e->type == B2E_CHARGE);
+      double L = 0;
+      switch (e->type) {
+      case B2E_DRIF:
+      case B2E_EDRIFT:
+      case B2E_KQUAD:
+      case B2E_KSEXT:
+      case B2E_CSBEND:
+      case B2E_RFCA:
+        L = p[0];
+        break;
+      default:
+        break;
+      }
+      last_z = z;
+      z += L;
+      nLeft = nToTrack;
+      if (start) {
+        switch (e->type) {
+        case B2E_DRIF:
+          drift_track(c, nToTrack, L, p[B2E_DRIF_ORDER] ? (int)p[B2E_DRIF_ORDER] : default_order);
+          break;
+        case B2E_EDRIFT:
+          exact_drift(c, nToTrack, L);
+          break;
+        case B2E_KQUAD:
+        case B2E_KSEXT:
+          nLeft = kmult_track(c, nToTrack, e, p_central, last_z, &ma);
+          break;
+        case B2E_CSBEND:
+          nLeft = csbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, &ma);
+          break;
+        case B2E_RFCA:
+          nLeft = rfca_track(c, nToTrack, e, &rf[k], p_central);
+          break;
+        case B2E_MAXAMP:
+          ma.present = 1;
+          ma.x_max = p[B2E_MAXAMP_X_MAX];
+          ma.y_max = p[B2E_MAXAMP_Y_MAX];
+          ma.elliptical = (long)p[B2E_MAXAMP_ELLIPTICAL];
+          ma.exponent = (long)p[B2E_MAXAMP_EXPONENT];
+          ma.y_exponent = (long)p[B2E_MAXAMP_Y_EXPONENT];
+          break;
+        default:
+          break;
+        }
+      }
+      if (!no_aperture && ma.present && (ma.x_max || ma.y_max)) {
+        if (!ma.elliptical)
+          nLeft = limit_amps(c, ma.x_max, ma.y_max, nLeft, z, p_central, e->type == B2E_DRIF);
+        else
+          nLeft = elimit_amps(c, ma.x_max, ma.y_max, nLeft, z, p_central, e->type == B2E_DRIF, ma.exponent,
+                              ma.y_exponent);
+      }
+      nLeft = limit_amps(c, DBL_MAX, DBL_MAX, nLeft, z, p_central, 0);
+      for (i = nLeft; i < nToTrack; i++)
+        c[i][7] = pass;
+      nToTrack = nLeft;
+    }
+    *effort += nToTrack;
+  }
+  free(rf);
+  free(c);
+  return nToTrack;
+}
+
+/* Elementary functions as this build sees them (for the maths tests). */
+double b2e_oracle_sin(double x) { return M_SIN(x); }
+double b2e_oracle_cos(double x) { return M_COS(x); }
+double b2e_oracle_tan(double x) { return M_TAN(x); }
+double b2e_oracle_asin(double x) { return M_ASIN(x); }

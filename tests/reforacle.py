@@ -68,3 +68,34 @@ def by_id(rows):
     order = np.argsort(rows[:, 6], kind="stable")
     r = rows[order]
     return r[:, :6], r[:, 6].astype(np.int64), r[:, 7].astype(np.int64)
+
+
+class PortOracle:
+    """The C restatement in oracle/b2e_oracle.c (oracle/_build)."""
+
+    def __init__(self, math: str = "b2e"):
+        name = "libb2e_oracle.so" if math == "b2e" else "libb2e_oracle_libm.so"
+        path = os.path.join(ROOT, "oracle", "_build", name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.b2e_oracle_track.restype = ctypes.c_long
+        for f in ("sin", "cos", "tan", "asin"):
+            fn = getattr(self.lib, f"b2e_oracle_{f}")
+            fn.restype = ctypes.c_double
+            fn.argtypes = [ctypes.c_double]
+        self.math = math
+
+    def track(self, lattice, coords, ids, p_central, n_passes, default_order=2):
+        """Returns (rows, n_left, effort) like RefOracle.track."""
+        n = coords.shape[0]
+        rows = np.zeros((max(n, 1), 8))
+        rows[:n, :6] = coords
+        rows[:n, 6] = ids
+        rows[:n, 7] = -1
+        elems = lattice.to_ctypes()
+        eff = ctypes.c_double()
+        nl = self.lib.b2e_oracle_track(elems, ctypes.c_int(len(lattice)), ctypes.c_double(p_central),
+                                       ctypes.c_int(n_passes), ctypes.c_int(default_order),
+                                       rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.byref(eff))
+        return rows[:n], nl, eff.value
