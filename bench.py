@@ -51,7 +51,46 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-csr", action="store_true")
+    ap.add_argument("--csr-particles", type=int, default=1_000_000)
     return ap.parse_args()
+
+
+def csr_section(args, device, flush):
+    """Secondary figure: CSR pass time on the single-pass chicane (config 1:
+    1 GeV, 1 nC, 1e6 particles, 4 CSRCSBEND x 20 kicks, BINS=600,
+    SG_HALFWIDTH=2, CSRDRIFT 5/1/5 m).  A run is the whole chicane; the CSR
+    pass time is its device time divided by the 80 dipole kicks (each kick =
+    slice integration + binning + smoothing + wake + kick)."""
+    import torch
+
+    from elegant_b200 import Tracker, workloads as w
+
+    lat = w.chicane()
+    beam = w.chicane_beam(args.csr_particles, seed=777)
+    p0 = 1000 / 0.51099895
+    tr = Tracker(lat, p0, 1, device=device)
+    stream = torch.cuda.ExternalStream(tr.stream)
+    times = []
+    for it in range(3 + 3):
+        tr.upload(beam)
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tr.continue_tracking()
+        e1.record(stream)
+        e1.synchronize()
+        if it >= 3:
+            times.append(e0.elapsed_time(e1))
+    kicks = sum(int(e.get("N_SLICES")) for e in lat.elements if e.type == "CSRCSBEND")
+    ms = sum(times) / len(times)
+    tr.close()
+    return {"workload": "bunch-compressor chicane with CSR (config 1)", "particles": beam.n, "dipole_kicks": kicks,
+            "run_ms": ms, "csr_pass_ms_per_kick": ms / kicks,
+            "particle_kicks_per_s": beam.n * kicks / (ms / 1e3),
+            "timing": "CUDA events on the engine stream; includes CSRDRIFT kicks and the one host sync per CSR element"}
 
 
 # ---------------------------------------------------------------- clocks ----
@@ -274,6 +313,8 @@ def main():
                "d2h_bytes_per_step": int(n * (6 * 8 + 8 + 4 + 4)), "steps": len(e2e_ms),
                "ms_per_step": sum(e2e_ms) / len(e2e_ms), "timing": "host wall clock around the blocking C-ABI call"}
 
+    csr = None if args.no_csr else csr_section(args, local_rank, flush)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -301,6 +342,7 @@ def main():
                          "flops_per_particle_turn": fpt,
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.mm float64), best of 3"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
+            "csr": csr,
         }
         print(json.dumps(line))
     if dist:

@@ -446,6 +446,18 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   return B2E_OK;
 }
 
+static int count_alive(b2e_ctx *ctx, int64_t *n_alive) {
+  unsigned long long counters[2];
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  CUDA_TRY(ctx, launch_effort(particle_view(ctx).lost_pass, ctx->n, 0, 0, ctx->d_counters.ptr,
+                              ctx->d_counters.ptr + 1, ctx->stream));
+  ctx->launches++;
+  CUDA_TRY(ctx, cudaMemcpyAsync(counters, ctx->d_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *n_alive = (int64_t)counters[1];
+  return B2E_OK;
+}
+
 static int track_impl(b2e_ctx *ctx, double *effort) {
   const int ne = (int)ctx->lat.elems.size();
   const int p0 = ctx->pass_counter;
@@ -455,6 +467,15 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_rf.ptr, 0, sizeof(DevRfState) * std::max(1, ctx->n_inst * ctx->lat.n_rf),
                                   ctx->stream));
     csr_reset(ctx->csr);
+    /* CHARGE (do_tracking.c:1324-1360): macro-particle charge = TOTAL / particles at start */
+    ctx->csr.macro_charge = 0;
+    for (const b2e_element &el : ctx->base)
+      if (el.type == B2E_CHARGE) {
+        if (ctx->n)
+          ctx->csr.macro_charge = el.p[B2E_CHARGE_TOTAL] / ctx->n;
+        if (el.p[B2E_CHARGE_PER_PARTICLE])
+          ctx->csr.macro_charge = el.p[B2E_CHARGE_PER_PARTICLE];
+      }
   }
   /* stop points: every RFCA on pass 0 (fiducial), every CSR element on every pass */
   int p = p0, e = 0;
@@ -499,9 +520,20 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       if (rc)
         return rc;
     } else {
-      int rc = csr_track_element(ctx->csr, particle_view(ctx), ctx->n, stop_e, p, ctx->stream, ctx->err);
+      /* the collective step needs the number of particles alive at its entrance
+       * (n_part > 1 decides whether CSR is computed at all, csbend.c:1987) */
+      int64_t n_alive = 0;
+      int rc = count_alive(ctx, &n_alive);
       if (rc)
         return rc;
+      rc = csr_track_element(ctx->csr, ctx->d_elems.ptr, ctx->lat.elems[stop_e], particle_view(ctx), ctx->n, n_alive,
+                             stop_e, p, ctx->stream, ctx->err, &ctx->launches);
+      if (rc)
+        return rc;
+      const int iap = p == 0 ? ctx->lat.elems[stop_e].ap_pass0 : ctx->lat.elems[stop_e].ap_later;
+      CUDA_TRY(ctx, launch_post_element_sweep(particle_view(ctx), ctx->n, iap >= 0 ? ctx->d_aps.ptr + iap : nullptr,
+                                              p, stop_e, ctx->stream));
+      ctx->launches++;
     }
     e = stop_e + 1;
     if (e >= ne) {

@@ -1,48 +1,785 @@
 /*
- * CSR driver: placeholder until the collective kernels land; lattices with
- * CSR elements are rejected at load time.
+ * CSR step on the device: CSRCSBEND (track_through_csbendCSR, csbend.c:1899-3044)
+ * and CSRDRIFT mode 0 (track_through_driftCSR, csbend.c:3176-3533).
+ * See b2e_csr.h for the kernel pipeline.  Every floating-point expression
+ * keeps the reference's operation order; histogram counts are integers and
+ * min/max are exact, so the pipeline reproduces the CPU oracle bit for bit
+ * regardless of thread scheduling.
  */
+#include <math.h>
+#include <string.h>
+#include <algorithm>
 #include "b2e_csr.h"
+#include "b2e_elements.cuh"
+#include "b2e_sg.h"
 
 namespace b2e {
 
+static const double kPI = 3.141592653589793238462643383279502884;
+static const double kC = 2.99792458e8;
+static const double kE = 1.602176634e-19;
+static const double kME = 9.1093837015e-31;
+
+struct CsrDevState {
+  unsigned long long ct_min_key, ct_max_key; /* order-preserving keys of min/max c*t */
+  double ctLower, ctUpper, dct;              /* binning of the current kick */
+  double s0, dctBin;                         /* csrWake.s0, csrWake.dctBin */
+  long long nBinned;
+  double dGamma[B2E_CSR_MAX_BINS];           /* csrWake.dGamma: last dipole wake */
+};
+
+__device__ __forceinline__ unsigned long long key_of(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double value_of(unsigned long long k) {
+  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+/* binParticleCoordinate's range expansion (csbend.c:3079-3094) */
+__device__ __forceinline__ void expand_range(double *lower, double *upper, double factor) {
+  if (factor > 1) {
+    double center = (*lower + *upper) / 2, range = (*upper - *lower) * factor;
+    *lower = center - range / 2;
+    *upper = center + range / 2;
+  }
+}
+
+__device__ __forceinline__ void block_minmax(double v, bool valid, CsrDevState *st) {
+  unsigned long long kmin = valid ? key_of(v) : ~0ull, kmax = valid ? key_of(v) : 0ull;
+  for (int off = 16; off > 0; off >>= 1) {
+    kmin = min(kmin, __shfl_down_sync(0xffffffffu, kmin, off));
+    kmax = max(kmax, __shfl_down_sync(0xffffffffu, kmax, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (kmin != ~0ull)
+      atomicMin(&st->ct_min_key, kmin);
+    if (kmax != 0ull)
+      atomicMax(&st->ct_max_key, kmax);
+  }
+}
+
+/* CSR energy kick from the previous kick's wake (csbend.c:2692-2711) */
+__device__ __forceinline__ double csr_kick(double CT, double X, double DP, const CsrDevState *st, int nBins,
+                                           double Po, double rho0) {
+  double f = (CT - st->ctLower) / st->dct;
+  long long iBin = (long long)f;
+  f -= iBin;
+  if (iBin >= 0 && iBin < nBins - 1)
+    DP += ((1 - f) * st->dGamma[iBin] + f * st->dGamma[iBin + 1]) / Po * (1 + X / rho0);
+  return DP;
+}
+
+/* entrance: offsets, tilt, c*t = s/beta, entrance edge (csbend.c:2286-2377) */
+__global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const DevElem *ep, double Po) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  const DevElem &e = *ep;
+  const double *c = e.c;
+  const double ct = c[CB_COS_TT], st = c[CB_SIN_TT];
+  double x = P.x[i], xp = P.xp[i], y = P.y[i], yp = P.yp[i], s = P.s[i], dp = P.dp[i];
+  double X, Y, XP, YP, p0, b0, rho;
+  s = s + c[CB_DZI] * sqrt((1 + xp * xp) + yp * yp);
+  x = (x + c[CB_DXI]) + c[CB_DZI] * xp;
+  y = (y + c[CB_DYI]) + c[CB_DZI] * yp;
+  X = x * ct + y * st;
+  Y = -x * st + y * ct;
+  XP = xp * ct + yp * st;
+  YP = -xp * st + yp * ct;
+  p0 = Po * (1 + dp);
+  b0 = p0 / sqrt(p0 * p0 + 1);
+  s = s / b0;
+  if (e.flags & EF_EDGE1) {
+    rho = (1 + dp) * c[CB_RHO_ACTUAL];
+    XP = XP + (c[CB_TAN_E1] / rho) * X;
+    YP = YP - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * Y;
+  }
+  P.x[i] = X;
+  P.xp[i] = XP;
+  P.y[i] = Y;
+  P.yp[i] = YP;
+  P.s[i] = s;
+  beta0[i] = b0;
+}
+
+/* one kick: optional wake kick of the previous kick, one integrator slice,
+ * c*t update, min/max of c*t (csbend.c:2385-2450, :3066-3076) */
+__global__ void csr_slice_kernel(DevParticles P, int64_t n, const double *beta0, const DevElem *ep,
+                                 const DevAperture *ap, CsrDevState *st, int apply_kick, int nBins, double Po,
+                                 int pass, int elem_index) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool alive = i < n && P.lost_pass[i] < 0;
+  double CT = 0;
+  if (alive) {
+    const DevElem &e = *ep;
+    const double *c = e.c;
+    double X = P.x[i], XP = P.xp[i], Y = P.y[i], YP = P.yp[i], DP = P.dp[i], f, Q1, Q3, Q4;
+    CT = P.s[i];
+    if (apply_kick)
+      DP = csr_kick(CT, X, DP, st, nBins, Po, c[CB_RHO0]);
+    f = (1 + DP) / sqrt((1 + XP * XP) + YP * YP);
+    Q1 = XP * f;
+    Q3 = YP * f;
+    int lost = csbend_integrate(X, Q1, Y, Q3, Q4, DP, c, 1, (int)c[CB_NSUB], false, ap, e);
+    f = 1 / sqrt(((1 + DP) * (1 + DP) - Q1 * Q1) - Q3 * Q3);
+    Q1 = Q1 * f;
+    Q3 = Q3 * f;
+    P.x[i] = X;
+    P.xp[i] = Q1;
+    P.y[i] = Y;
+    P.yp[i] = Q3;
+    P.dp[i] = DP;
+    if (lost) {
+      P.lost_pass[i] = pass;
+      P.lost_elem[i] = elem_index;
+      alive = false;
+    } else {
+      CT = CT + Q4 / beta0[i];
+      P.s[i] = CT;
+    }
+  }
+  block_minmax(CT, alive, st);
+}
+
+/* histogram of c*t with the range of binParticleCoordinate (csbend.c:3047-3113):
+ * shared-memory integer counts aggregated per warp, then added to global counts. */
+__global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrDevState *st, unsigned int *counts, int nBins,
+                                double factor) {
+  extern __shared__ unsigned int scount[];
+  double lower = value_of(st->ct_min_key), upper = value_of(st->ct_max_key), dct;
+  expand_range(&lower, &upper, factor);
+  dct = (upper - lower) / nBins;
+  for (int b = threadIdx.x; b < nBins; b += blockDim.x)
+    scount[b] = 0;
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->ctLower = lower;
+    st->ctUpper = upper;
+    st->dct = dct;
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - threadIdx.x < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int bin = -1;
+    if (i < n && P.lost_pass[i] < 0) {
+      long long b = (long long)((P.s[i] - lower) / dct);
+      if (b >= 0 && b <= nBins - 1)
+        bin = (int)b;
+    }
+    /* warp aggregation: one shared-memory atomic per distinct bin per warp */
+    unsigned int peers = __match_any_sync(0xffffffffu, bin);
+    int leader = __ffs(peers) - 1;
+    if (bin >= 0 && (int)(threadIdx.x & 31) == leader)
+      atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < nBins; b += blockDim.x)
+    if (scount[b])
+      atomicAdd(&counts[b], scount[b]);
+}
+
+struct WakeArgs {
+  int nBins, sgHalf, sgdHalf, trapz, steady, correct;
+  const double *sg_w, *sgd_w; /* [nBins][B2E_SG_MAX_WIDTH] */
+  const int *sg_lo, *sg_n, *sgd_lo, *sgd_n;
+  double slippage, slippage13, c1, c2, csr_constant;
+  double *wakelog; /* nBins values for this kick, or null */
+};
+
+/* Savitzky-Golay pass with precomputed per-bin weights (b2e_sg.h convention);
+ * lo/wn point into an interleaved (start, width) table, stride 2 per bin. */
+__device__ void sg_apply(const double *in, double *out, int nBins, const double *w, const int *lo, const int *wn) {
+  for (int b = threadIdx.x; b < nBins; b += blockDim.x) {
+    double s = 0;
+    const double *wb = w + (size_t)b * B2E_SG_MAX_WIDTH;
+    const int start = lo[2 * b], width = wn[2 * b];
+    for (int k = 0; k < width; k++)
+      s += wb[k] * in[start + k];
+    out[b] = s;
+  }
+}
+
+/* wake of one kick (csbend.c:2566-2673): one CTA */
+__global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, WakeArgs a) {
+  extern __shared__ double sm[];
+  const int nb = a.nBins;
+  double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb, *tmp = sm + 3 * nb;
+  __shared__ long long nBinned;
+  __shared__ int skip;
+  const double dct = st->dct;
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int b = 0; b < nb; b++)
+      s += counts[b];
+    nBinned = s;
+    st->nBinned = s;
+    skip = 0;
+  }
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    hist[b] = (double)counts[b];
+  __syncthreads();
+  if (a.sgHalf > 0) {
+    sg_apply(hist, tmp, nb, a.sg_w, a.sg_lo, a.sg_n);
+    __syncthreads();
+    /* correctDistribution (csbend.c:4705-4721): sequential sum as the reference */
+    if (threadIdx.x == 0) {
+      double sum = 0;
+      for (int b = 0; b < nb; b++) {
+        if (tmp[b] < 0)
+          tmp[b] = 0;
+        sum += tmp[b];
+      }
+      if (!sum)
+        skip = 1;
+      else
+        deriv[0] = (1.0 * nBinned) / sum; /* factor, parked in deriv[0] */
+    }
+    __syncthreads();
+    const double factor = deriv[0];
+    const int sk = skip;
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+      hist[b] = sk ? tmp[b] : tmp[b] * factor;
+    __syncthreads();
+  }
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    denom[b] = b2e_pow13(dct * b);
+    hist[b] = hist[b] / dct;
+    deriv[b] = hist[b];
+  }
+  __syncthreads();
+  sg_apply(deriv, tmp, nb, a.sgd_w, a.sgd_lo, a.sgd_n);
+  __syncthreads();
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+    deriv[b] = tmp[b];
+  __syncthreads();
+  /* bins of slippage; clamped to [0, nb] so indexing stays in bounds for a
+   * degenerate bin size (the comparisons below give the same result) */
+  long long diS = (long long)(a.slippage / dct), diS4 = (long long)(4 * a.slippage / dct);
+  diS = diS < 0 ? 0 : (diS > nb ? nb : diS);
+  diS4 = diS4 < 0 ? 0 : (diS4 > nb ? nb : diS4);
+  if (!(dct > 0)) {
+    for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+      st->dGamma[ib] = 0;
+      if (a.wakelog)
+        a.wakelog[ib] = 0;
+    }
+    return;
+  }
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double T1 = 0, T2 = 0, term1 = 0, term2 = 0;
+    long long count, j;
+    if (a.csr_constant) {
+      if (a.steady) {
+        if (!a.trapz) {
+          for (j = ib + 1; j < nb; j++)
+            T1 += deriv[j] / denom[j - ib];
+        } else {
+          if ((j = ib + 1) < nb)
+            term1 = deriv[j] / denom[j - ib];
+          for (count = 0, j = ib + 1; j < nb; j++, count++)
+            T1 += (term2 = deriv[j] / denom[j - ib]);
+          if ((ib + 1) < nb)
+            T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
+          if (count > 1)
+            T1 -= (term1 + term2) / 2;
+        }
+      } else {
+        if (!a.trapz) {
+          for (j = ib + 1; j <= (ib + diS) && j < nb; j++)
+            T1 += deriv[j] / denom[j - ib];
+        } else {
+          if ((j = ib + 1) < nb && j <= (ib + diS))
+            term1 = deriv[j] / denom[j - ib] / 2;
+          for (count = 0, j = ib + 1; j <= (ib + diS) && j < nb; count++, j++)
+            T1 += (term2 = deriv[j] / denom[j - ib]);
+          if (diS > 0 && (ib + 1) < nb)
+            T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
+          if (count > 1)
+            T1 -= (term1 + term2) / 2;
+        }
+        if ((ib + diS) < nb)
+          T2 += hist[ib + diS];
+        if ((ib + diS4) < nb)
+          T2 -= hist[ib + diS4];
+      }
+      T1 *= a.c1;
+      T2 *= a.c2;
+    }
+    double dg = T1 + T2;
+    st->dGamma[ib] = dg;
+    if (a.wakelog)
+      a.wakelog[ib] = dg;
+  }
+}
+
+/* after the last kick: its wake kick and the min/max for the exit binning */
+__global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrDevState *st, int apply_kick, int nBins, double Po,
+                                     double rho0) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool alive = i < n && P.lost_pass[i] < 0;
+  double CT = 0;
+  if (alive) {
+    CT = P.s[i];
+    if (apply_kick)
+      P.dp[i] = csr_kick(CT, P.x[i], P.dp[i], st, nBins, Po, rho0);
+  }
+  block_minmax(CT, alive, st);
+}
+
+/* exit: c*t -> s at the final velocity, exit edge, back to the lab frame
+ * (csbend.c:2810-2955); csrWake.s0 from the exit binning's lower edge. */
+__global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, CsrDevState *st, double factor,
+                                int do_bin, double Po, int pass, int elem_index) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const DevElem &e = *ep;
+  const double *c = e.c;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double lower = 0, upper = 0;
+    st->dctBin = do_bin ? st->dct : 0;
+    if (do_bin) {
+      lower = value_of(st->ct_min_key);
+      upper = value_of(st->ct_max_key);
+      expand_range(&lower, &upper, factor);
+    }
+    st->s0 = lower + c[CB_DZF];
+  }
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  const double ct = c[CB_COS_TT], sn = c[CB_SIN_TT];
+  double X = P.x[i], XP = P.xp[i], Y = P.y[i], YP = P.yp[i], CT = P.s[i], DP = P.dp[i];
+  double p1 = Po * (1 + DP), beta1 = p1 / sqrt(p1 * p1 + 1), s, x, y, xp, yp, rho;
+  s = CT * beta1;
+  if (p1 <= 0) {
+    P.lost_pass[i] = pass;
+    P.lost_elem[i] = elem_index;
+    return;
+  }
+  if (e.flags & EF_EDGE2) {
+    rho = (1 + DP) * c[CB_RHO_ACTUAL];
+    XP = XP + (c[CB_TAN_E2] / rho) * X;
+    YP = YP - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + DP)) / rho) * Y;
+  }
+  x = (X * ct - Y * sn) + c[CB_ET0 + 0];
+  y = (X * sn + Y * ct) + c[CB_ET0 + 2];
+  xp = (XP * ct - YP * sn) + c[CB_ET0 + 1];
+  yp = (XP * sn + YP * ct) + c[CB_ET0 + 3];
+  x = x + (c[CB_DXF] + c[CB_DZF] * xp);
+  y = y + (c[CB_DYF] + c[CB_DZF] * yp);
+  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + c[CB_ET0 + 4]);
+  P.x[i] = x;
+  P.xp[i] = xp;
+  P.y[i] = y;
+  P.yp[i] = yp;
+  P.s[i] = s;
+}
+
+/* CSRDRIFT mode 0, one kick (csbend.c:3415-3502) */
+__global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, const CsrDevState *st, double dz, double s0_incr,
+                                      double factor, int apply, int nBins, double Po) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  double x = P.x[i], xp = P.xp[i], y = P.y[i], yp = P.yp[i], s = P.s[i], dp = P.dp[i], p, beta;
+  x = x + xp * dz;
+  y = y + yp * dz;
+  p = Po * (1 + dp);
+  beta = p / sqrt(p * p + 1);
+  s = (s + dz * sqrt((1 + xp * xp) + yp * yp)) / beta;
+  if (apply) {
+    const double ct0 = st->s0 + s0_incr;
+    double f = (s - ct0) / st->dctBin;
+    long long iBin = (long long)f;
+    f -= iBin;
+    if (iBin >= 0 && iBin < nBins - 1)
+      dp = dp + ((1 - f) * st->dGamma[iBin] + f * st->dGamma[iBin + 1]) / Po * factor;
+  }
+  p = (1 + dp) * Po;
+  beta = p / sqrt(p * p + 1);
+  P.x[i] = x;
+  P.y[i] = y;
+  P.s[i] = beta * s;
+  P.dp[i] = dp;
+}
+
+__global__ void csr_s0_add_kernel(CsrDevState *st, double incr) { st->s0 = st->s0 + incr; }
+
+/* do_tracking's sweeps after a collective element (do_tracking.c:2455-2475,
+ * :2629): MAXAMP aperture if one is active, then inf/NaN in x or y. */
+__global__ void post_element_sweep_kernel(DevParticles P, int64_t n, const DevAperture *ap, int pass, int elem_index) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  Part p;
+  p.x = P.x[i];
+  p.y = P.y[i];
+  bool lost = false;
+  if (ap && ap->mode) {
+    p.xp = P.xp[i];
+    p.yp = P.yp[i];
+    lost = !maxamp_ok(p, *ap);
+  }
+  if (!lost && !finite_xy(p))
+    lost = true;
+  if (lost) {
+    P.lost_pass[i] = pass;
+    P.lost_elem[i] = elem_index;
+  }
+}
+
+cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const DevAperture *ap, int pass, int elem,
+                                      cudaStream_t stream) {
+  const int grid = (int)std::max<int64_t>(1, (n + 255) / 256);
+  post_element_sweep_kernel<<<grid, 256, 0, stream>>>(P, n, ap, pass, elem);
+  return cudaGetLastError();
+}
+
+__global__ void edrift_kernel(DevParticles P, int64_t n, double L) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  double xp = P.xp[i], yp = P.yp[i];
+  P.x[i] = P.x[i] + xp * L;
+  P.y[i] = P.y[i] + yp * L;
+  P.s[i] = P.s[i] + L * sqrt((1 + xp * xp) + yp * yp);
+}
+
+/* ------------------------------------------------------------------ host -- */
+
+static int grid_for(int64_t n) { return (int)std::max<int64_t>(1, (n + 255) / 256); }
+
 int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLattice &lat, const b2e_run_options &opt,
                   std::string &err) {
-  (void)el;
-  (void)n;
-  (void)opt;
-  st.elements = lat.csr_elements;
+  csr_release(st);
+  st.elems.clear();
+  st.p_central = opt.p_central;
   st.enabled = !lat.csr_elements.empty();
-  if (st.enabled) {
-    err = "CSRCSBEND/CSRDRIFT are not available in this build";
-    return B2E_ERR_LATTICE;
+  if (!st.enabled)
+    return B2E_OK;
+  std::vector<double> sgw;
+  std::vector<int> sgi;
+  st.sg_offset.clear();
+  for (int idx : lat.csr_elements) {
+    const b2e_element &e = el[idx];
+    const DevElem &d = lat.elems[idx];
+    CsrElem ce;
+    ce.index = idx;
+    ce.kind = d.kind;
+    if (d.kind == K_CSRCSBEND) {
+      const double *p = e.p;
+      ce.bins = (int)p[B2E_BEND_BINS];
+      if (ce.bins < 2) {
+        err = "Less than 2 bins for CSR!";
+        return B2E_ERR_LATTICE;
+      }
+      if (ce.bins > B2E_CSR_MAX_BINS) {
+        err = "CSRCSBEND BINS above the engine maximum (4096)";
+        return B2E_ERR_LATTICE;
+      }
+      ce.nSlices = (int)d.c[CB_NSLICES];
+      ce.nSub = (int)d.c[CB_NSUB];
+      ce.sgHalf = (int)p[B2E_BEND_SG_HALFWIDTH];
+      ce.sgOrder = (int)p[B2E_BEND_SG_ORDER];
+      ce.sgdHalf = (int)p[B2E_BEND_SGDERIV_HALFWIDTH];
+      ce.sgdOrder = (int)p[B2E_BEND_SGDERIV_ORDER];
+      /* csbend.c:2042-2050 */
+      if (ce.sgdHalf <= 0)
+        ce.sgdHalf = ce.sgHalf;
+      if (ce.sgdHalf <= 0)
+        ce.sgdHalf = 1;
+      if (ce.sgdOrder <= 0)
+        ce.sgdOrder = ce.sgOrder;
+      if (ce.sgdOrder <= 0)
+        ce.sgdOrder = 1;
+      if (2 * std::max(ce.sgHalf, ce.sgdHalf) + 1 > B2E_SG_MAX_WIDTH) {
+        err = "Savitzky-Golay half-width too large";
+        return B2E_ERR_LATTICE;
+      }
+      ce.trapz = p[B2E_BEND_TRAPAZOID_INTEGRATION] != 0;
+      ce.steady = p[B2E_BEND_STEADY_STATE] != 0;
+      ce.csr = p[B2E_BEND_CSR] != 0;
+      ce.angle = fabs(p[B2E_BEND_ANGLE]);
+      ce.length = p[B2E_BEND_L];
+      ce.rho0 = d.c[CB_RHO0];
+      ce.binRangeFactor = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
+      ce.dzf = d.c[CB_DZF];
+      ce.z_end = d.z_end;
+      ce.same_bend_precedes = idx > 0 && el[idx - 1].type == B2E_CSRCSBEND &&
+                              strncmp(el[idx - 1].name, e.name, sizeof(e.name)) == 0;
+      /* per-bin Savitzky-Golay weights for smoothing (order sgOrder, derivative 0)
+       * and for the derivative (order sgdOrder, derivative 1) */
+      st.sg_offset.push_back(sgw.size());
+      for (int pass = 0; pass < 2; pass++) {
+        int half = pass == 0 ? ce.sgHalf : ce.sgdHalf, order = pass == 0 ? ce.sgOrder : ce.sgdOrder;
+        for (int b = 0; b < ce.bins; b++) {
+          double w[B2E_SG_MAX_WIDTH] = {0};
+          long width;
+          long lo = b2e_sg_window(b, ce.bins, half, half, &width);
+          long ord = order < width - 1 ? order : width - 1;
+          if (pass == 0 && half <= 0) {
+            width = 1;
+            lo = b;
+            w[0] = 1;
+          } else if ((pass == 1 && 1 > ord) || b2e_sg_weights(w, width, lo - b, ord, pass)) {
+            width = 0; /* derivative of a constant fit: zero */
+          }
+          for (int k = 0; k < B2E_SG_MAX_WIDTH; k++)
+            sgw.push_back(w[k]);
+          sgi.push_back((int)lo);
+          sgi.push_back((int)width);
+        }
+      }
+    } else {
+      const double *p = e.p;
+      if (p[B2E_CSRDRIFT_USE_STUPAKOV] != 0) {
+        err = "CSRDRIFT USE_STUPAKOV=1 is not available in this build";
+        return B2E_ERR_LATTICE;
+      }
+      ce.drift_length = p[B2E_CSRDRIFT_L];
+      ce.drift_dz = p[B2E_CSRDRIFT_DZ];
+      ce.drift_kicks = (int)p[B2E_CSRDRIFT_N_KICKS];
+      ce.drift_csr = p[B2E_CSRDRIFT_CSR] != 0;
+      ce.z_start = d.z_start;
+      st.sg_offset.push_back(sgw.size());
+    }
+    st.elems.push_back(ce);
   }
+  if (cudaMalloc(&st.d_state, sizeof(CsrDevState)) != cudaSuccess ||
+      cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS) != cudaSuccess) {
+    err = "CSR state allocation failed";
+    return B2E_ERR_NOMEM;
+  }
+  cudaMemset(st.d_state, 0, sizeof(CsrDevState));
+  if (!sgw.empty()) {
+    if (cudaMalloc(&st.d_sg, sizeof(double) * sgw.size()) != cudaSuccess ||
+        cudaMalloc(&st.d_sg_idx, sizeof(int) * sgi.size()) != cudaSuccess) {
+      err = "CSR weight allocation failed";
+      return B2E_ERR_NOMEM;
+    }
+    cudaMemcpy(st.d_sg, sgw.data(), sizeof(double) * sgw.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(st.d_sg_idx, sgi.data(), sizeof(int) * sgi.size(), cudaMemcpyHostToDevice);
+  }
+  /* the index array runs parallel to the weights: 2 ints per bin row */
   return B2E_OK;
 }
 
-void csr_reset(CsrState &st) { st.wakes_host.clear(); }
+void csr_reset(CsrState &st) {
+  st.wakes_host.clear();
+  st.wake_values = 0;
+  st.accumulated_angle = 0;
+  st.wake_valid = false;
+}
 
-int csr_track_element(CsrState &st, const DevParticles &P, int64_t n, int elem, int pass, cudaStream_t stream,
-                      std::string &err) {
-  (void)st;
-  (void)P;
-  (void)n;
-  (void)elem;
-  (void)pass;
-  (void)stream;
-  err = "CSR elements are not available in this build";
-  return B2E_ERR_LATTICE;
+static int ensure_wakelog(CsrState &st, int64_t values) {
+  if (values <= st.wakelog_cap)
+    return B2E_OK;
+  double *p = nullptr;
+  if (cudaMalloc(&p, sizeof(double) * values) != cudaSuccess)
+    return B2E_ERR_NOMEM;
+  if (st.d_wakelog) {
+    if (st.wake_values)
+      cudaMemcpy(p, st.d_wakelog, sizeof(double) * st.wake_values, cudaMemcpyDeviceToDevice);
+    cudaFree(st.d_wakelog);
+  }
+  st.d_wakelog = p;
+  st.wakelog_cap = values;
+  return B2E_OK;
+}
+
+#define CSR_CUDA(call)                                                                                           \
+  do {                                                                                                           \
+    cudaError_t e_ = (call);                                                                                     \
+    if (e_ != cudaSuccess) {                                                                                     \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);                                                  \
+      return B2E_ERR_CUDA;                                                                                       \
+    }                                                                                                            \
+  } while (0)
+
+int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
+                      int64_t n_alive, int elem, int pass, cudaStream_t stream, std::string &err, int64_t *launches) {
+  size_t k = 0;
+  while (k < st.elems.size() && st.elems[k].index != elem)
+    k++;
+  if (k == st.elems.size()) {
+    err = "CSR element not configured";
+    return B2E_ERR_STATE;
+  }
+  const CsrElem &ce = st.elems[k];
+  CsrDevState *dst = (CsrDevState *)st.d_state;
+  const double Po = st.p_central;
+  const int g = grid_for(n);
+  if (ce.kind == K_CSRDRIFT) {
+    /* track_through_driftCSR (csbend.c:3176-3533), mode 0 */
+    if (n_alive <= 1 || !st.wake_valid || !ce.drift_csr) {
+      edrift_kernel<<<g, 256, 0, stream>>>(P, n, ce.drift_length);
+      (*launches)++;
+      CSR_CUDA(cudaGetLastError());
+      return B2E_OK;
+    }
+    double zStart = ce.z_start;
+    int nKicks;
+    if (ce.drift_dz > 0) {
+      if ((nKicks = (int)(ce.drift_length / ce.drift_dz)) < 1)
+        nKicks = 1;
+    } else
+      nKicks = ce.drift_kicks;
+    if (nKicks <= 0) {
+      err = "nKicks=0 in CSR drift.";
+      return B2E_ERR_LATTICE;
+    }
+    double dz0 = ce.drift_length / nKicks, dz = dz0 / 2;
+    double dzFirst = zStart - st.zLast;
+    const int nb = st.elems[0].bins; /* csrWake.bins: bins of the last CSRCSBEND */
+    int lastBins = 0;
+    for (size_t j = 0; j < st.elems.size(); j++)
+      if (st.elems[j].kind == K_CSRCSBEND && st.elems[j].index < elem)
+        lastBins = st.elems[j].bins;
+    (void)nb;
+    for (int iKick = 0; iKick < nKicks; iKick++) {
+      if (iKick == 1)
+        dz = dz0;
+      double incr = dz + dzFirst;
+      double factor = (dz0 + dzFirst) / st.ds0;
+      csr_drift_kick_kernel<<<g, 256, 0, stream>>>(P, n, dst, dz, incr, factor, 1, lastBins, Po);
+      csr_s0_add_kernel<<<1, 1, 0, stream>>>(dst, incr);
+      (*launches) += 2;
+      CSR_CUDA(cudaGetLastError());
+      dzFirst = 0;
+    }
+    dz = dz0 / 2;
+    edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz);
+    csr_s0_add_kernel<<<1, 1, 0, stream>>>(dst, dz);
+    (*launches) += 2;
+    CSR_CUDA(cudaGetLastError());
+    st.zLast = zStart + ce.drift_length;
+    return B2E_OK;
+  }
+
+  /* ---- CSRCSBEND ---- */
+  const DevElem *d_e = d_elems + elem;
+  const bool more_than_one = n_alive > 1;
+  if (!ce.same_bend_precedes)
+    st.accumulated_angle = 0;
+  st.wake_valid = false;
+  if (st.beta0_cap < n) {
+    if (st.d_beta0)
+      cudaFree(st.d_beta0);
+    if (cudaMalloc(&st.d_beta0, sizeof(double) * std::max<int64_t>(n, 1)) != cudaSuccess) {
+      err = "CSR beta0 allocation failed";
+      return B2E_ERR_NOMEM;
+    }
+    st.beta0_cap = n;
+  }
+  if (ensure_wakelog(st, st.wake_values + (int64_t)ce.nSlices * ce.bins)) {
+    err = "CSR wake log allocation failed";
+    return B2E_ERR_NOMEM;
+  }
+  st.ds0 = ce.length / ce.nSlices;
+  st.zLast = st.z0 = ce.z_end;
+  /* CSRConstant (csbend.c:2378-2381) */
+  const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
+  double csr_constant = 0;
+  if (ce.csr && more_than_one)
+    csr_constant = 2 * st.macro_charge * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
+  const double c1 = csr_constant * ce.length / ce.nSlices;
+  const double *sgw = st.d_sg + st.sg_offset[k];
+  const int *sgi = st.d_sg_idx + st.sg_offset[k] / B2E_SG_MAX_WIDTH * 2;
+
+  csr_entry_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, Po);
+  (*launches)++;
+  CSR_CUDA(cudaGetLastError());
+  double phiBend = st.accumulated_angle;
+  for (int kick = 0; kick < ce.nSlices; kick++) {
+    CSR_CUDA(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), stream));
+    CSR_CUDA(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), stream));
+    csr_slice_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, nullptr, dst, kick > 0 && csr_constant != 0,
+                                            ce.bins, Po, pass, elem);
+    (*launches)++;
+    CSR_CUDA(cudaGetLastError());
+    if (!more_than_one)
+      continue;
+    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins, stream));
+    int hb = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 1023) / 1024));
+    csr_hist_kernel<<<hb, 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, dst, st.d_counts, ce.bins,
+                                                                         ce.binRangeFactor);
+    (*launches)++;
+    CSR_CUDA(cudaGetLastError());
+    phiBend += ce.angle / ce.nSlices;
+    double slippage = fabs(ce.rho0 * (phiBend * phiBend * phiBend) / 24.0);
+    WakeArgs a;
+    a.nBins = ce.bins;
+    a.sgHalf = ce.sgHalf;
+    a.sgdHalf = ce.sgdHalf;
+    a.trapz = ce.trapz;
+    a.steady = ce.steady;
+    a.correct = ce.sgHalf > 0;
+    a.sg_w = sgw;
+    a.sgd_w = sgw + (size_t)ce.bins * B2E_SG_MAX_WIDTH;
+    a.sg_lo = sgi;
+    a.sg_n = sgi + 1;
+    a.sgd_lo = sgi + 2 * ce.bins;
+    a.sgd_n = sgi + 2 * ce.bins + 1;
+    a.slippage = slippage;
+    a.slippage13 = b2e_pow(slippage, 1. / 3.);
+    a.c1 = c1;
+    a.c2 = -csr_constant * ce.length / ce.nSlices / a.slippage13;
+    a.csr_constant = csr_constant;
+    a.wakelog = st.d_wakelog + st.wake_values;
+    size_t smem = sizeof(double) * 4 * ce.bins;
+    CSR_CUDA(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    csr_wake_kernel<<<1, 1024, smem, stream>>>(dst, st.d_counts, a);
+    (*launches)++;
+    CSR_CUDA(cudaGetLastError());
+    st.wake_values += ce.bins;
+  }
+  CSR_CUDA(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), stream));
+  CSR_CUDA(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), stream));
+  csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, dst, more_than_one && csr_constant != 0, ce.bins, Po, ce.rho0);
+  csr_exit_kernel<<<g, 256, 0, stream>>>(P, n, d_e, dst, ce.binRangeFactor, more_than_one, Po, pass, elem);
+  (*launches) += 2;
+  CSR_CUDA(cudaGetLastError());
+  if (more_than_one)
+    st.wake_valid = true;
+  st.accumulated_angle += ce.angle;
+  return B2E_OK;
 }
 
 int csr_copy_wakes(CsrState &st, double *wakes, int64_t capacity, int64_t *written, std::string &err) {
-  (void)err;
-  int64_t k = 0;
-  for (; k < (int64_t)st.wakes_host.size() && k < capacity; k++)
-    wakes[k] = st.wakes_host[k];
-  *written = k;
+  int64_t n = std::min<int64_t>(st.wake_values, capacity);
+  if (n > 0 && wakes) {
+    cudaError_t e = cudaMemcpy(wakes, st.d_wakelog, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      err = cudaGetErrorString(e);
+      return B2E_ERR_CUDA;
+    }
+  }
+  *written = wakes ? n : st.wake_values;
   return B2E_OK;
 }
 
-void csr_release(CsrState &st) { st.wakes_host.clear(); }
+void csr_release(CsrState &st) {
+  if (st.d_beta0)
+    cudaFree(st.d_beta0);
+  if (st.d_state)
+    cudaFree(st.d_state);
+  if (st.d_counts)
+    cudaFree(st.d_counts);
+  if (st.d_sg)
+    cudaFree(st.d_sg);
+  if (st.d_sg_idx)
+    cudaFree(st.d_sg_idx);
+  if (st.d_wakelog)
+    cudaFree(st.d_wakelog);
+  st.d_beta0 = nullptr;
+  st.d_state = nullptr;
+  st.d_counts = nullptr;
+  st.d_sg = nullptr;
+  st.d_sg_idx = nullptr;
+  st.d_wakelog = nullptr;
+  st.beta0_cap = 0;
+  st.wakelog_cap = 0;
+  st.wake_values = 0;
+}
 
 } // namespace b2e

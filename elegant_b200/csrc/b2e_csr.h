@@ -1,5 +1,16 @@
 /*
  * Collective CSR step (CSRCSBEND / CSRDRIFT) driver interface.
+ *
+ * Per CSRCSBEND kick the device runs, with no host round trip:
+ *   slice   -- (previous kick's wake kick) + one integrator slice per particle
+ *              + block min/max of c*t, folded into global order-preserving
+ *              integer atomics (exact, order independent);
+ *   bin     -- warp-aggregated shared-memory histogram of c*t (integer counts,
+ *              exact) reduced into global counts;
+ *   wake    -- one CTA: Savitzky-Golay smoothing, distribution correction,
+ *              derivative, transient/steady T1/T2 integrals -> dGamma.
+ * gpuElegant instead copies every histogram to the host and the wake back
+ * (gpu_csbend.cu:3080-3140, :2689-2691).
  */
 #ifndef B2E_CSR_H
 #define B2E_CSR_H
@@ -11,19 +22,53 @@
 
 namespace b2e {
 
+#define B2E_CSR_MAX_BINS 4096
+
+/* Host description of one CSR element. */
+struct CsrElem {
+  int index = -1;   /* lattice index */
+  int kind = 0;     /* K_CSRCSBEND / K_CSRDRIFT */
+  /* CSRCSBEND */
+  int bins = 0, nSlices = 0, nSub = 0, sgHalf = 0, sgOrder = 1, sgdHalf = 1, sgdOrder = 1;
+  int trapz = 1, steady = 0, csr = 1, same_bend_precedes = 0, bin_once = 0;
+  double angle = 0, length = 0, rho0 = 0, binRangeFactor = 1.2, dzf = 0, z_end = 0;
+  std::vector<int> sg_lo, sg_w_n, sgd_lo, sgd_w_n;   /* per bin window start and width */
+  std::vector<double> sg_w, sgd_w;                    /* per bin weights, B2E_SG_MAX_WIDTH each */
+  /* CSRDRIFT */
+  double drift_length = 0, drift_dz = 0, z_start = 0;
+  int drift_kicks = 1, drift_csr = 1;
+};
+
 struct CsrState {
   bool enabled = false;
-  std::vector<int> elements;
-  std::vector<double> wakes_host;
-  void *impl = nullptr; /* device buffers, owned by b2e_csr.cu */
+  std::vector<CsrElem> elems;
+  std::vector<double> wakes_host; /* filled on demand from the device log */
+  int64_t wake_values = 0;        /* values written to the device log in this run */
+  double macro_charge = 0;        /* CHARGE TOTAL / particles at pass start */
+  double p_central = 0;
+  double accumulated_angle = 0;
+  /* device buffers */
+  double *d_beta0 = nullptr;
+  int64_t beta0_cap = 0;
+  void *d_state = nullptr;        /* CsrDevState */
+  unsigned int *d_counts = nullptr;
+  double *d_sg = nullptr;         /* weights of all elements, uploaded once */
+  int *d_sg_idx = nullptr;
+  std::vector<size_t> sg_offset;  /* per element: offset into d_sg / d_sg_idx */
+  double *d_wakelog = nullptr;
+  int64_t wakelog_cap = 0;
+  bool wake_valid = false;        /* csrWake.valid */
+  double ds0 = 0, zLast = 0, z0 = 0;
 };
 
 int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLattice &lat, const b2e_run_options &opt,
                   std::string &err);
 void csr_reset(CsrState &st);
-int csr_track_element(CsrState &st, const DevParticles &P, int64_t n, int elem, int pass, cudaStream_t stream,
-                      std::string &err);
+int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
+                      int64_t n_alive, int elem, int pass, cudaStream_t stream, std::string &err, int64_t *launches);
 int csr_copy_wakes(CsrState &st, double *wakes, int64_t capacity, int64_t *written, std::string &err);
+cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const DevAperture *ap, int pass, int elem,
+                                      cudaStream_t stream);
 void csr_release(CsrState &st);
 
 } // namespace b2e

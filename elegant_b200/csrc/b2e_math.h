@@ -181,6 +181,58 @@ B2E_HD double b2e_asin_mid(double x) {
   return b2e_fma(x * w, p, x);
 }
 
+/* ln(x) to ~1e-8 relative, for the tiny exponent correction in b2e_pow13:
+ * x = m 2^e, ln m = 2 atanh(s), s = (m-1)/(m+1), series to s^13. */
+B2E_HD double b2e_log_coarse(double x) {
+  int e;
+  double m = frexp(x, &e), s, w, p;
+  s = (m - 1.0) / (m + 1.0);
+  w = s * s;
+  p = b2e_fma(w, 1.0 / 13.0, 1.0 / 11.0);
+  p = b2e_fma(p, w, 1.0 / 9.0);
+  p = b2e_fma(p, w, 1.0 / 7.0);
+  p = b2e_fma(p, w, 1.0 / 5.0);
+  p = b2e_fma(p, w, 1.0 / 3.0);
+  p = b2e_fma(p, w, 1.0);
+  return e * 0x1.62e42fefa39efp-1 + 2.0 * s * p; /* ln 2 */
+}
+
+/* pow(x, 1./3.): C's pow with the double nearest 1/3, as the CSR code calls
+ * it (csbend.c:2379, :2575, :2590).  The cube root is computed to double-
+ * double accuracy by Newton iteration with an exact fma residual; the
+ * exponent's own rounding, 1/3 - 1./3. = 2^-54/3, enters as the factor
+ * (1 - 2^-54/3 ln x).  One final rounding, so the result is the correctly
+ * rounded value except in exceedingly rare near-tie cases. */
+B2E_HD double b2e_pow13(double x) {
+  int e, q, r;
+  double m, y, p_hi, p_lo, t_hi, t_lo, res, c, corr;
+  if (x != x || x < 0)
+    return (x - x) / (x - x);
+  if (x == 0 || x > 1.7976931348623157e308)
+    return x;
+  m = frexp(x, &e); /* x = m 2^e, m in [1/2, 1) */
+  q = e >= 0 ? e / 3 : -((2 - e) / 3);
+  r = e - 3 * q; /* 0, 1, 2 */
+  m = ldexp(m, r); /* in [1/2, 4) */
+  y = 0.65 + 0.25 * m - 0.0185 * m * m; /* within 6% on [1/2, 4) */
+  for (int i = 0; i < 6; i++)
+    y = y - (y * y * y - m) / (3.0 * y * y);
+  /* residual m - y^3 with y^3 as an unevaluated sum */
+  p_hi = y * y;
+  p_lo = b2e_fma(y, y, -p_hi);
+  t_hi = p_hi * y;
+  t_lo = b2e_fma(p_hi, y, -t_hi) + p_lo * y;
+  res = (m - t_hi) - t_lo;
+  c = res / (3.0 * y * y);
+  corr = -(0x1p-54 / 3.0) * b2e_log_coarse(x);
+  return ldexp(y + (c + y * corr), q);
+}
+
+/* pow(x, y) with the 1/3 exponent routed to b2e_pow13 (all other exponents
+ * only occur in host-side setup, where the library pow is used as in the
+ * reference). */
+B2E_HD double b2e_pow(double x, double y) { return y == 1.0 / 3.0 ? b2e_pow13(x) : pow(x, y); }
+
 B2E_HD double b2e_asin(double x) {
   double a = fabs(x), r;
   if (a <= 0.125)

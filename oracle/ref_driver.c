@@ -32,6 +32,7 @@ extern jmp_buf b2e_ref_trap;
 extern int b2e_ref_trap_armed;
 extern char b2e_ref_errmsg[512];
 extern long b2e_ref_warning_count;
+void b2e_ref_capture_reset(void);
 
 typedef struct {
   const char *name;
@@ -215,6 +216,7 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
     offsets_done = 1;
   }
   memset(&apertureData, 0, sizeof(apertureData));
+  b2e_ref_capture_reset();
   b2e_ref_errmsg[0] = 0;
   sizeOfParticle = totalPropertiesPerParticle * sizeof(double);
   particleMass = me_mks;

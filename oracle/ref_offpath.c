@@ -21,34 +21,21 @@ long isMaster = 1, isSlave = 1, notSinglePart = 0;
 OFFPATH(INTERPOLATE)
 OFFPATH(SDDS_CheckColumn)
 OFFPATH(SDDS_CheckParameter)
-OFFPATH(SDDS_DefineColumn)
-OFFPATH(SDDS_DefineParameter)
-OFFPATH(SDDS_DefineSimpleColumn)
-OFFPATH(SDDS_DefineSimpleParameter)
-OFFPATH(SDDS_DoFSync)
 OFFPATH(SDDS_GetColumnInDoubles)
 OFFPATH(SDDS_GetColumnInLong)
 OFFPATH(SDDS_GetParameterAsDouble)
 OFFPATH(SDDS_GetParameterAsLong)
 OFFPATH(SDDS_InitializeInputFromSearchPath)
-OFFPATH(SDDS_InitializeOutputElegant)
 OFFPATH(SDDS_PrintErrors)
 OFFPATH(SDDS_ReadPage)
 OFFPATH(SDDS_RowCount)
-OFFPATH(SDDS_SetColumn)
 OFFPATH(SDDS_SetError)
-OFFPATH(SDDS_SetParameters)
 OFFPATH(SDDS_SetRowValues)
-OFFPATH(SDDS_StartPage)
 OFFPATH(SDDS_Terminate)
 OFFPATH(SDDS_UpdatePage)
-OFFPATH(SDDS_WriteLayout)
-OFFPATH(SDDS_WritePage)
 OFFPATH(addLSCKick)
 OFFPATH(bend_matrix)
 OFFPATH(binaryArraySearch)
-OFFPATH(bitsSet)
-OFFPATH(compose_filename)
 OFFPATH(concat_matrices)
 OFFPATH(convertLocalCoordinatesToGlobal)
 OFFPATH(copy_matrices1)

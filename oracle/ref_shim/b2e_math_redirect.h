@@ -14,4 +14,5 @@
 #define cos(x) b2e_cos(x)
 #define tan(x) b2e_tan(x)
 #define asin(x) b2e_asin(x)
+#define pow(x, y) b2e_pow(x, y)
 #endif

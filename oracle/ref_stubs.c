@@ -219,3 +219,13 @@ long determine_bend_flags(ELEMENT_LIST *elem, long edge1_effects, long edge2_eff
   bend_flags |= BEND_EDGE_DETERMINED;
   return bend_flags;
 }
+
+/* Number of set bits in a word (mdblib bitsSet; used by CSRDRIFT mode checks). */
+long bitsSet(unsigned long data) {
+  long n = 0;
+  while (data) {
+    n += (long)(data & 1UL);
+    data >>= 1;
+  }
+  return n;
+}

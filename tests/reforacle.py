@@ -40,9 +40,11 @@ class RefOracle:
         self.lib.b2e_ref_track.restype = ctypes.c_long
         self.math = math
 
-    def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0):
+    def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0, capture_wakes=False):
         """Returns (rows, n_left, effort, wakes); rows are the reference's final
-        particle array (x, xp, y, yp, s, delta, id, lossPass), survivors first."""
+        particle array (x, xp, y, yp, s, delta, id, lossPass), survivors first.
+        With capture_wakes, every CSRCSBEND writes its per-kick DeltaGamma through
+        the reference's own OUTPUT_FILE path (captured in memory), returned as wakes."""
         n = coords.shape[0]
         rows = np.zeros((n, 7))
         rows[:, :6] = coords
@@ -53,13 +55,22 @@ class RefOracle:
         err = ctypes.create_string_buffer(512)
         ww = ctypes.c_long()
         wakes = np.zeros(max(wake_capacity, 1))
-        rc = self.lib.b2e_ref_track(lattice_spec(lattice).encode(), ctypes.c_double(p_central),
+        spec = lattice_spec(lattice)
+        if capture_wakes:
+            spec = spec.replace(":CSRCSBEND", ":CSRCSBEND OUTPUT_FILE=capture")
+        rc = self.lib.b2e_ref_track(spec.encode(), ctypes.c_double(p_central),
                                     rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.c_long(n_passes),
                                     out.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nl), ctypes.byref(eff),
                                     wakes.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(wake_capacity),
                                     ctypes.byref(ww), err, ctypes.c_long(512))
         if rc != 0:
             raise RuntimeError(f"reference oracle failed: {err.value.decode()}")
+        if capture_wakes:
+            self.lib.b2e_ref_capture_get.restype = ctypes.c_long
+            k = self.lib.b2e_ref_capture_get(0, None, ctypes.c_long(0))
+            buf = np.zeros(max(k, 1))
+            self.lib.b2e_ref_capture_get(0, buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(k))
+            return out[:n], nl.value, eff.value, buf[:k]
         return out[:n], nl.value, eff.value, wakes[: ww.value]
 
 
