@@ -8,9 +8,12 @@
  */
 #include <math.h>
 #include <string.h>
+#include <stdio.h>
 #include <algorithm>
+#include <mutex>
 #include "b2e_csr.h"
 #include "b2e_elements.cuh"
+#include "b2e_kernels.h"
 #include "b2e_sg.h"
 
 namespace b2e {
@@ -783,3 +786,249 @@ void csr_release(CsrState &st) {
 }
 
 } // namespace b2e
+
+/* ==========================================================================
+ * Allocation-free CSR dipole: b2e_csr_bend_static (include/elegant_b200.h).
+ *
+ * Some callers cannot allocate device memory at the moment they need this
+ * computation: a host program that has handed the whole card to its own
+ * memory pool, code that runs where cudaMalloc is not permitted, or an
+ * embedding that must never fail for lack of memory halfway through a run.
+ * For them, this path keeps all of its working memory in one file-scope
+ * device array that is part of the loaded library image, so a call needs only
+ * the caller's own particle and output buffers.
+ *
+ * The array holds per-particle entrance velocities (up to
+ * B2E_STATIC_MAX_PARTICLES), the CSR binning/wake state, the histogram, the
+ * Savitzky-Golay weight tables (up to B2E_STATIC_MAX_BINS bins) and the
+ * element record: about 10.2 MB, resident on every GPU that loads the library
+ * until the process exits.  All calls share it and it keeps the previous
+ * call's contents; everything that must start at zero is cleared by each
+ * call.  Two calls whose work overlaps on the GPU (different streams, or
+ * different host threads) race on this memory: callers must serialise them.
+ * ======================================================================== */
+
+/* B2E_STATIC_MAX_PARTICLES and B2E_STATIC_MAX_BINS come from elegant_b200.h */
+namespace b2e {
+
+struct StaticCsrScratch {
+  double beta0[B2E_STATIC_MAX_PARTICLES];
+  CsrDevState state;
+  unsigned int counts[B2E_STATIC_MAX_BINS];
+  double sg_w[2 * B2E_STATIC_MAX_BINS * B2E_SG_MAX_WIDTH];
+  int sg_idx[2 * B2E_STATIC_MAX_BINS * 2];
+  DevElem elem;
+  unsigned long long counters[2];
+};
+
+static __device__ __align__(256) unsigned char g_static_csr_scratch[sizeof(StaticCsrScratch)];
+
+/* device addresses of g_static_csr_scratch, one per device, looked up on the
+ * first call made with that device current */
+#define B2E_STATIC_MAX_DEVICES 64
+static void *g_static_addr[B2E_STATIC_MAX_DEVICES];
+static std::mutex g_static_mutex;
+
+static StaticCsrScratch *static_scratch(char *err, int64_t errlen) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= B2E_STATIC_MAX_DEVICES) {
+    snprintf(err, errlen, "b2e_csr_bend_static: no usable current device (%s)", cudaGetErrorString(e));
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_csr_scratch);
+    if (e != cudaSuccess || !p) {
+      snprintf(err, errlen, "b2e_csr_bend_static: cudaGetSymbolAddress failed on device %d (%s)", dev,
+               cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_static_addr[dev] = p;
+  }
+  return (StaticCsrScratch *)g_static_addr[dev];
+}
+
+__global__ void static_set_elem_kernel(DevElem e, DevElem *dst) { *dst = e; }
+
+/* Savitzky-Golay weight tables for one element, on the device, with the same
+ * helpers and layout as csr_configure (rows of B2E_SG_MAX_WIDTH weights;
+ * interleaved (start, width) index pairs; smoothing rows then derivative rows). */
+__global__ void static_sg_weights_kernel(int bins, int sgHalf, int sgOrder, int sgdHalf, int sgdOrder, double *w,
+                                         int *idx) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= 2 * bins)
+    return;
+  const int pass = row >= bins, b = row - pass * bins;
+  const int half = pass == 0 ? sgHalf : sgdHalf, order = pass == 0 ? sgOrder : sgdOrder;
+  double ww[B2E_SG_MAX_WIDTH];
+  for (int k = 0; k < B2E_SG_MAX_WIDTH; k++)
+    ww[k] = 0;
+  long width;
+  long lo = b2e_sg_window(b, bins, half, half, &width);
+  long ord = order < width - 1 ? order : width - 1;
+  if (pass == 0 && half <= 0) {
+    width = 1;
+    lo = b;
+    ww[0] = 1;
+  } else if ((pass == 1 && 1 > ord) || b2e_sg_weights(ww, width, lo - b, ord, pass)) {
+    width = 0;
+  }
+  for (int k = 0; k < B2E_SG_MAX_WIDTH; k++)
+    w[(size_t)row * B2E_SG_MAX_WIDTH + k] = ww[k];
+  idx[2 * row] = (int)lo;
+  idx[2 * row + 1] = (int)width;
+}
+
+#define STATIC_TRY(call)                                                                                          \
+  do {                                                                                                            \
+    cudaError_t e_ = (call);                                                                                      \
+    if (e_ != cudaSuccess) {                                                                                      \
+      snprintf(err, errlen, "b2e_csr_bend_static: %s: %s", #call, cudaGetErrorString(e_));                       \
+      return B2E_ERR_CUDA;                                                                                        \
+    }                                                                                                             \
+  } while (0)
+
+} // namespace b2e
+
+extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lost_pass, int32_t *dev_lost_element,
+                                   int64_t n, const b2e_element *bend, double p_central, double macro_particle_charge,
+                                   double *dev_wakes, int64_t wake_capacity, void *stream, char *errbuf,
+                                   int64_t errlen) {
+  using namespace b2e;
+  char local_err[256];
+  char *err = errbuf && errlen > 0 ? errbuf : local_err;
+  if (!(errbuf && errlen > 0))
+    errlen = sizeof(local_err);
+  err[0] = 0;
+  if (!dev_columns || !dev_lost_pass || !dev_lost_element || !bend || n < 0 || p_central <= 0) {
+    snprintf(err, errlen, "b2e_csr_bend_static: null pointer, negative count or nonpositive p_central");
+    return B2E_ERR_ARG;
+  }
+  for (int c = 0; c < 6; c++)
+    if (!dev_columns[c]) {
+      snprintf(err, errlen, "b2e_csr_bend_static: column %d is null", c);
+      return B2E_ERR_ARG;
+    }
+  if (n > B2E_STATIC_MAX_PARTICLES) {
+    snprintf(err, errlen, "b2e_csr_bend_static: %lld particles exceed the static limit of %d", (long long)n,
+             B2E_STATIC_MAX_PARTICLES);
+    return B2E_ERR_ARG;
+  }
+  DevElem d;
+  const char *msg = compile_single_csr_bend(*bend, d);
+  if (msg) {
+    snprintf(err, errlen, "b2e_csr_bend_static: %s", msg);
+    return B2E_ERR_LATTICE;
+  }
+  const double *p = bend->p;
+  const int bins = (int)p[B2E_BEND_BINS], nSlices = (int)d.c[CB_NSLICES];
+  if (bins < 2 || bins > B2E_STATIC_MAX_BINS) {
+    snprintf(err, errlen, "b2e_csr_bend_static: BINS=%d outside [2, %d]", bins, B2E_STATIC_MAX_BINS);
+    return B2E_ERR_ARG;
+  }
+  int sgHalf = (int)p[B2E_BEND_SG_HALFWIDTH], sgOrder = (int)p[B2E_BEND_SG_ORDER];
+  int sgdHalf = (int)p[B2E_BEND_SGDERIV_HALFWIDTH], sgdOrder = (int)p[B2E_BEND_SGDERIV_ORDER];
+  if (sgdHalf <= 0)
+    sgdHalf = sgHalf;
+  if (sgdHalf <= 0)
+    sgdHalf = 1;
+  if (sgdOrder <= 0)
+    sgdOrder = sgOrder;
+  if (sgdOrder <= 0)
+    sgdOrder = 1;
+  if (2 * (sgHalf > sgdHalf ? sgHalf : sgdHalf) + 1 > B2E_SG_MAX_WIDTH) {
+    snprintf(err, errlen, "b2e_csr_bend_static: Savitzky-Golay half-width too large");
+    return B2E_ERR_ARG;
+  }
+  if (dev_wakes && wake_capacity < (int64_t)nSlices * bins) {
+    snprintf(err, errlen, "b2e_csr_bend_static: wake buffer holds %lld values, %lld needed",
+             (long long)wake_capacity, (long long)nSlices * bins);
+    return B2E_ERR_ARG;
+  }
+  StaticCsrScratch *S = static_scratch(err, errlen);
+  if (!S)
+    return B2E_ERR_CUDA;
+  cudaStream_t s = (cudaStream_t)stream;
+  DevParticles P;
+  P.x = dev_columns[0];
+  P.xp = dev_columns[1];
+  P.y = dev_columns[2];
+  P.yp = dev_columns[3];
+  P.s = dev_columns[4];
+  P.dp = dev_columns[5];
+  P.lost_pass = dev_lost_pass;
+  P.lost_elem = dev_lost_element;
+
+  static_set_elem_kernel<<<1, 1, 0, s>>>(d, &S->elem);
+  static_sg_weights_kernel<<<(2 * bins + 127) / 128, 128, 0, s>>>(bins, sgHalf, sgOrder, sgdHalf, sgdOrder, S->sg_w,
+                                                                  S->sg_idx);
+  STATIC_TRY(cudaGetLastError());
+  /* particles alive at the entrance decide whether CSR is computed (csbend.c:1987) */
+  unsigned long long counters[2] = {0, 0};
+  STATIC_TRY(cudaMemsetAsync(S->counters, 0, sizeof(S->counters), s));
+  STATIC_TRY(launch_effort(dev_lost_pass, n, 0, 0, &S->counters[0], &S->counters[1], s));
+  STATIC_TRY(cudaMemcpyAsync(counters, S->counters, sizeof(counters), cudaMemcpyDeviceToHost, s));
+  STATIC_TRY(cudaStreamSynchronize(s));
+  const bool more_than_one = counters[1] > 1;
+
+  const double Po = p_central;
+  const double angle = fabs(p[B2E_BEND_ANGLE]), length = p[B2E_BEND_L], rho0 = d.c[CB_RHO0];
+  const double brf = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
+  const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
+  double csr_constant = 0;
+  if (p[B2E_BEND_CSR] != 0 && more_than_one)
+    csr_constant = 2 * macro_particle_charge * kE / b2e_pow(3 * rho0 * rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
+  const int g = (int)std::max<int64_t>(1, (n + 255) / 256);
+  CsrDevState *dst = &S->state;
+
+  csr_entry_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, Po);
+  STATIC_TRY(cudaGetLastError());
+  double phiBend = 0;
+  for (int kick = 0; kick < nSlices; kick++) {
+    STATIC_TRY(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), s));
+    STATIC_TRY(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), s));
+    csr_slice_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, nullptr, dst, kick > 0 && csr_constant != 0, bins,
+                                       Po, 0, 0);
+    STATIC_TRY(cudaGetLastError());
+    if (!more_than_one)
+      continue;
+    STATIC_TRY(cudaMemsetAsync(S->counts, 0, sizeof(unsigned int) * bins, s));
+    int hb = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 1023) / 1024));
+    csr_hist_kernel<<<hb, 1024, sizeof(unsigned int) * bins, s>>>(P, n, dst, S->counts, bins, brf);
+    STATIC_TRY(cudaGetLastError());
+    phiBend += angle / nSlices;
+    double slippage = fabs(rho0 * (phiBend * phiBend * phiBend) / 24.0);
+    WakeArgs a;
+    a.nBins = bins;
+    a.sgHalf = sgHalf;
+    a.sgdHalf = sgdHalf;
+    a.trapz = p[B2E_BEND_TRAPAZOID_INTEGRATION] != 0;
+    a.steady = p[B2E_BEND_STEADY_STATE] != 0;
+    a.correct = sgHalf > 0;
+    a.sg_w = S->sg_w;
+    a.sgd_w = S->sg_w + (size_t)bins * B2E_SG_MAX_WIDTH;
+    a.sg_lo = S->sg_idx;
+    a.sg_n = S->sg_idx + 1;
+    a.sgd_lo = S->sg_idx + 2 * bins;
+    a.sgd_n = S->sg_idx + 2 * bins + 1;
+    a.slippage = slippage;
+    a.slippage13 = b2e_pow(slippage, 1. / 3.);
+    a.c1 = csr_constant * length / nSlices;
+    a.c2 = -csr_constant * length / nSlices / a.slippage13;
+    a.csr_constant = csr_constant;
+    a.wakelog = dev_wakes ? dev_wakes + (size_t)kick * bins : nullptr;
+    size_t smem = sizeof(double) * 4 * bins;
+    STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    csr_wake_kernel<<<1, 1024, smem, s>>>(dst, S->counts, a);
+    STATIC_TRY(cudaGetLastError());
+  }
+  STATIC_TRY(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), s));
+  STATIC_TRY(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), s));
+  csr_last_kick_kernel<<<g, 256, 0, s>>>(P, n, dst, more_than_one && csr_constant != 0, bins, Po, rho0);
+  csr_exit_kernel<<<g, 256, 0, s>>>(P, n, &S->elem, dst, brf, more_than_one, Po, 0, 0);
+  STATIC_TRY(cudaGetLastError());
+  STATIC_TRY(launch_post_element_sweep(P, n, nullptr, 0, 0, s));
+  return B2E_OK;
+}

@@ -343,6 +343,26 @@ static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
   return "";
 }
 
+/* One CSRCSBEND standing alone (both edges active as its parameters say),
+ * compiled into `d` without any container; returns nullptr on success or a
+ * static message. */
+const char *compile_single_csr_bend(const b2e_element &el, DevElem &d) {
+  static thread_local char msg[256];
+  if (el.type != B2E_CSRCSBEND)
+    return "element is not a CSRCSBEND";
+  memset(&d, 0, sizeof(d));
+  d.ap_pass0 = d.ap_later = -1;
+  std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, d);
+  if (!e.empty()) {
+    snprintf(msg, sizeof(msg), "%s", e.c_str());
+    return msg;
+  }
+  if (d.kind != K_CSRCSBEND)
+    return "CSRCSBEND with zero angle is a drift; nothing to do here";
+  d.z_end = el.p[B2E_BEND_L];
+  return nullptr;
+}
+
 std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options &opt, CompiledLattice &out) {
   out = CompiledLattice();
   out.elems.resize(n);

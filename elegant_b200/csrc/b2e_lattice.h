@@ -30,6 +30,9 @@ struct CompiledLattice {
   double total_length = 0;
 };
 
+/* One standalone CSRCSBEND -> DevElem; nullptr on success, else a message. */
+const char *compile_single_csr_bend(const b2e_element &el, DevElem &d);
+
 /* Returns an empty string on success, else a description of the problem. */
 std::string compile_lattice(const b2e_element *elements, int n, const b2e_run_options &opt, CompiledLattice &out);
 

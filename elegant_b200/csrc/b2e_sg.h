@@ -29,11 +29,18 @@
 #define B2E_SG_MAX_WIDTH 65
 #define B2E_SG_MAX_ORDER 6
 
+/* the weight and window helpers also compile as device functions under nvcc */
+#ifdef __CUDACC__
+#define B2E_SG_FN __host__ __device__ static inline
+#else
+#define B2E_SG_FN static inline
+#endif
+
 /* Weights w[0..width-1] for the window offsets k = kLo .. kLo+width-1 relative
  * to the evaluation point, for a degree-`order` fit and derivative `deriv`.
  * Solves the (order+1)^2 normal equations by Gauss-Jordan elimination with
  * partial pivoting.  Returns 0 on success. */
-static inline int b2e_sg_weights(double *w, long width, long kLo, long order, long deriv) {
+B2E_SG_FN int b2e_sg_weights(double *w, long width, long kLo, long order, long deriv) {
   double a[B2E_SG_MAX_ORDER + 1][B2E_SG_MAX_ORDER + 1];
   double inv[B2E_SG_MAX_ORDER + 1][B2E_SG_MAX_ORDER + 1];
   long m = order + 1, i, j, k, r;
@@ -104,7 +111,7 @@ static inline int b2e_sg_weights(double *w, long width, long kLo, long order, lo
 }
 
 /* Window placement for point i: returns the first bin of the window and its width. */
-static inline long b2e_sg_window(long i, long rows, long nLeft, long nRight, long *width) {
+B2E_SG_FN long b2e_sg_window(long i, long rows, long nLeft, long nRight, long *width) {
   long w = nLeft + nRight + 1, lo;
   if (w > rows)
     w = rows;

@@ -243,6 +243,31 @@ int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *c
  * CSRCSBEND kick, BINS values of dGamma (csbend.c:2673) in kick order. */
 int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written);
 
+/* ---- allocation-free CSR dipole ---------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory when they track (a program whose memory pool owns
+ * the whole card, code running where cudaMalloc is not allowed, or a job that
+ * must not fail for lack of memory mid-run).  Tracks n caller-owned device
+ * particles (columns x, xp, y, yp, s, delta; lost_pass/lost_element int32,
+ * -1 = alive) through one CSRCSBEND, exactly as b2e_track does for that
+ * element (same kernels, same results), writing the per-kick wakes
+ * (N_KICKS x BINS values) to dev_wakes when it is non-NULL.  It allocates
+ * nothing: all working memory is one static device array of ~10.2 MB that
+ * the library image carries on every GPU that loads it, for up to
+ * B2E_STATIC_MAX_PARTICLES particles and B2E_STATIC_MAX_BINS bins; larger
+ * requests are rejected with B2E_ERR_ARG and a message in errbuf.  The first
+ * call on a device looks up that array's device address (with the device
+ * current); make that first call before any stream capture.  All calls share
+ * the array and each clears what it needs; calls that overlap on the GPU
+ * race on it and must be serialised by the caller.  stream is a
+ * cudaStream_t (NULL = legacy default stream).  p_central is beta*gamma;
+ * macro_particle_charge is CHARGE TOTAL divided by the particle count. */
+#define B2E_STATIC_MAX_PARTICLES 1048576
+#define B2E_STATIC_MAX_BINS 2048
+int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lost_pass, int32_t *dev_lost_element, int64_t n,
+                        const b2e_element *bend, double p_central, double macro_particle_charge, double *dev_wakes,
+                        int64_t wake_capacity, void *stream, char *errbuf, int64_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

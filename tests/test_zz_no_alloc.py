@@ -1,0 +1,81 @@
+"""The allocation-free CSR dipole entry point (b2e_csr_bend_static).
+
+It exists for callers that cannot allocate device memory while they track; it
+keeps its working memory in a static device array.  Here it is called through
+the C ABI on caller-owned device buffers, twice in a row, and each result must
+equal -- bit for bit, the bar of every parity test in this suite -- what the
+regular context path (b2e_track_host + b2e_csr_wakes) gives for the same
+bend.  This file is collected last so that a stop-at-first-failure run has
+already exercised everything else.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from elegant_b200 import Element, Lattice, Tracker, workloads as w
+from elegant_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+P0 = 1000 / 0.51099895
+CHARGE = 1e-9
+
+
+def bend_element():
+    return Element("B1", "CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "N_KICKS": 6, "BINS": 240, "SG_HALFWIDTH": 2})
+
+
+def static_call(lib, beam, bend_arr, wakes_needed):
+    import torch
+    dev = torch.device("cuda:0")
+    cols = [torch.tensor(np.ascontiguousarray(beam.coords[:, i]), dtype=torch.float64, device=dev) for i in range(6)]
+    lost_pass = torch.full((beam.n,), -1, dtype=torch.int32, device=dev)
+    lost_elem = torch.full((beam.n,), -1, dtype=torch.int32, device=dev)
+    wakes = torch.zeros(wakes_needed, dtype=torch.float64, device=dev)
+    ptrs = nat.pointer_array([c.data_ptr() for c in cols])
+    err = ctypes.create_string_buffer(512)
+    rc = lib.b2e_csr_bend_static(ptrs, ctypes.c_void_p(lost_pass.data_ptr()), ctypes.c_void_p(lost_elem.data_ptr()),
+                                 ctypes.c_int64(beam.n), ctypes.byref(bend_arr), ctypes.c_double(P0),
+                                 ctypes.c_double(CHARGE / beam.n), ctypes.c_void_p(wakes.data_ptr()),
+                                 ctypes.c_int64(wakes_needed), None, err, ctypes.c_int64(512))
+    torch.cuda.synchronize()
+    assert rc == 0, err.value.decode()
+    coords = np.stack([c.cpu().numpy() for c in cols], axis=1)
+    return coords, lost_pass.cpu().numpy(), wakes.cpu().numpy()
+
+
+def test_static_bend_matches_context_path_twice():
+    lib = nat.load_library()
+    lib.b2e_csr_bend_static.restype = ctypes.c_int
+    bend = bend_element()
+    lat = Lattice([Element("Q", "CHARGE", {"TOTAL": CHARGE}), bend])
+    beam = w.chicane_beam(30000, seed=12)
+    with Tracker(lat, P0, 1) as t:
+        ref = t.track(beam)
+        ref_wakes = t.csr_wakes(10_000_000)
+    n_wakes = 6 * 240
+    assert ref_wakes.shape == (n_wakes,)
+    bend_arr = Lattice([bend]).to_ctypes()[0]
+    for call in range(2):
+        coords, lost, wakes = static_call(lib, beam, bend_arr, n_wakes)
+        assert np.array_equal(lost, ref.lost_pass), f"call {call}: loss flags differ"
+        assert np.array_equal(wakes, ref_wakes), f"call {call}: wakes differ"
+        assert np.array_equal(coords, ref.coords), f"call {call}: coordinates differ"
+
+
+def test_static_bend_rejects_oversize_requests():
+    lib = nat.load_library()
+    lib.b2e_csr_bend_static.restype = ctypes.c_int
+    bend_arr = Lattice([bend_element()]).to_ctypes()[0]
+    dummy = nat.pointer_array([1, 1, 1, 1, 1, 1])
+    err = ctypes.create_string_buffer(256)
+    rc = lib.b2e_csr_bend_static(dummy, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_int64(1048577),
+                                 ctypes.byref(bend_arr), ctypes.c_double(P0), ctypes.c_double(1e-15), None,
+                                 ctypes.c_int64(0), None, err, ctypes.c_int64(256))
+    assert rc == -1 and b"exceed the static limit" in err.value
+    big = Lattice([Element("B", "CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 4096})]).to_ctypes()[0]
+    rc = lib.b2e_csr_bend_static(dummy, ctypes.c_void_p(1), ctypes.c_void_p(1), ctypes.c_int64(10),
+                                 ctypes.byref(big), ctypes.c_double(P0), ctypes.c_double(1e-15), None,
+                                 ctypes.c_int64(0), None, err, ctypes.c_int64(256))
+    assert rc == -1 and b"BINS=4096" in err.value
