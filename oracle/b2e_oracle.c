@@ -829,17 +829,449 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
   return itop + 1;
 }
 
+/* ---- CSR: CSRCSBEND and CSRDRIFT (mode 0) -------------------------------- */
+#ifdef B2E_ORACLE_LIBM
+#define M_POW13(x) pow(x, 1. / 3.)
+#else
+#define M_POW13(x) b2e_pow13(x)
+#endif
+#include "../elegant_b200/csrc/b2e_sg.h"
+
+/* the reference's file-static CSR state (csbend.h:27-63, csbend.c:1932) */
+typedef struct {
+  int valid, bins;
+  double *dGamma, dctBin, s0, ds0, zLast, z0;
+  double accumulatedAngle;
+  double macroParticleCharge;
+  double *wakes; /* per-kick dGamma log for the tests */
+  long n_wakes, cap_wakes;
+} CsrWake;
+
+/* binParticleCoordinate (csbend.c:3047-3113) on column `ic` of rows c[0..np) */
+static long bin_coordinate(double *hist, long bins, double *lower, double *upper, double *dct, double factor,
+                           double **c, long np, int ic) {
+  long ip, ib, nb = 0;
+  *upper = -(*lower = DBL_MAX);
+  for (ip = 0; ip < np; ip++) {
+    double v = c[ip][ic];
+    if (v < *lower)
+      *lower = v;
+    if (v > *upper)
+      *upper = v;
+  }
+  if (factor > 1) {
+    double center = (*lower + *upper) / 2, range = (*upper - *lower) * factor;
+    *lower = center - range / 2;
+    *upper = center + range / 2;
+  }
+  *dct = (*upper - *lower) / bins;
+  for (ib = 0; ib < bins; ib++)
+    hist[ib] = 0;
+  for (ip = 0; ip < np; ip++) {
+    ib = (long)((c[ip][ic] - *lower) / (*dct));
+    if (ib < 0 || ib > bins - 1)
+      continue;
+    hist[ib] += 1;
+    nb++;
+  }
+  return nb;
+}
+
+static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx, const b2e_element *all, int n_all,
+                            double Po, double z_start, double z_end, const MaxAmp *ma, CsrWake *cw) {
+  const double *p = el->p;
+  const double length = p[B2E_BEND_L];
+  long nBins = (long)p[B2E_BEND_BINS], nSlices = (long)p[B2E_BEND_N_SLICES], ip, itop, kick, iBin;
+  int integ = (int)p[B2E_BEND_INTEGRATION_ORDER], edge1, edge2, j;
+  long sgHalf = (long)p[B2E_BEND_SG_HALFWIDTH], sgOrder = (long)p[B2E_BEND_SG_ORDER];
+  long sgdHalf = (long)p[B2E_BEND_SGDERIV_HALFWIDTH], sgdOrder = (long)p[B2E_BEND_SGDERIV_ORDER];
+  double angle, e1, e2, tilt, rho0, rho_actual, fse, h, psi1, psi2, Kg, ttilt, ct, st;
+  double dxi, dyi, dzi, dxf, dyf, dzf, CSRConstant, phiBend, ctLower = 0, ctUpper = 0, dct = 0;
+  double brf = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
+  double *beta0, *ctHist, *ctHistDeriv, *denom, *T1, *T2;
+  int more_than_one = np > 1, same_pre = 0;
+  MultAp ap;
+  long nBinned = 0;
+  if (p[B2E_BEND_ANGLE] == 0) {
+    exact_drift(c, np, length);
+    return np;
+  }
+  /* edge flags and SAME_BEND_PRECEDES (determine_bend_flags) */
+  {
+    int pre = 0, post = 0;
+    for (j = idx - 1; j >= 0; j--) {
+      if (same_bend(&all[j], el)) {
+        pre = 1;
+        break;
+      }
+      if (all[j].type != B2E_MARK)
+        break;
+    }
+    for (j = idx + 1; j < n_all; j++) {
+      if (same_bend(&all[j], el)) {
+        post = 1;
+        break;
+      }
+      if (all[j].type != B2E_MARK)
+        break;
+    }
+    edge1 = p[B2E_BEND_EDGE1_EFFECTS] && !pre;
+    edge2 = p[B2E_BEND_EDGE2_EFFECTS] && !post;
+    same_pre = pre;
+  }
+  if (!same_pre)
+    cw->accumulatedAngle = 0;
+  cw->valid = 0;
+  if (sgdHalf <= 0)
+    sgdHalf = sgHalf;
+  if (sgdHalf <= 0)
+    sgdHalf = 1;
+  if (sgdOrder <= 0)
+    sgdOrder = sgOrder;
+  if (sgdOrder <= 0)
+    sgdOrder = 1;
+  rho0 = length / p[B2E_BEND_ANGLE];
+  if (p[B2E_BEND_ANGLE] < 0) {
+    angle = -p[B2E_BEND_ANGLE];
+    e1 = -p[B2E_BEND_E1];
+    e2 = -p[B2E_BEND_E2];
+    tilt = p[B2E_BEND_TILT] + PI_;
+    rho0 = length / angle;
+  } else {
+    angle = p[B2E_BEND_ANGLE];
+    e1 = p[B2E_BEND_E1];
+    e2 = p[B2E_BEND_E2];
+    tilt = p[B2E_BEND_TILT];
+    rho0 = length / angle;
+  }
+  setup_mult_ap(&ap, -tilt, ma);
+  h = 1 / rho0;
+  fse = p[B2E_BEND_FSE];
+  rho_actual = fse > -1 ? 1 / ((1 + fse) * h) : 1e16 / h;
+  Kg = 2 * p[B2E_BEND_HGAP] * p[B2E_BEND_FINT];
+  psi1 = Kg / rho_actual / M_COS(e1) * (1 + SQR(M_SIN(e1)));
+  psi2 = Kg / rho_actual / M_COS(e2) * (1 + SQR(M_SIN(e2)));
+  if (length < 0) {
+    psi1 *= -1;
+    psi2 *= -1;
+  }
+  ttilt = tilt + p[B2E_BEND_ETILT];
+  if (ttilt == 0) {
+    ct = 1;
+    st = 0;
+  } else if (fabs(fabs(ttilt) - PI_) < 1e-12) {
+    ct = -1;
+    st = 0;
+  } else if (fabs(ttilt - PI_ / 2) < 1e-12) {
+    ct = 0;
+    st = 1;
+  } else if (fabs(ttilt + PI_ / 2) < 1e-12) {
+    ct = 0;
+    st = -1;
+  } else {
+    ct = M_COS(ttilt);
+    st = M_SIN(ttilt);
+  }
+  dxi = -p[B2E_BEND_DX];
+  dzi = p[B2E_BEND_DZ];
+  dyi = -p[B2E_BEND_DY];
+  dxf = p[B2E_BEND_DX] * M_COS(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * M_SIN(p[B2E_BEND_ANGLE]);
+  dzf = p[B2E_BEND_DX] * M_SIN(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * M_COS(p[B2E_BEND_ANGLE]);
+  dyf = p[B2E_BEND_DY];
+  beta0 = malloc(sizeof(double) * (np ? np : 1));
+  ctHist = calloc(nBins, sizeof(double));
+  ctHistDeriv = calloc(nBins, sizeof(double));
+  denom = calloc(nBins, sizeof(double));
+  T1 = calloc(nBins, sizeof(double));
+  T2 = calloc(nBins, sizeof(double));
+  free(cw->dGamma);
+  cw->dGamma = calloc(nBins, sizeof(double));
+  cw->bins = nBins;
+  cw->ds0 = length / nSlices;
+  cw->zLast = cw->z0 = z_end;
+  /* entrance (csbend.c:2286-2377) */
+  for (ip = 0; ip < np; ip++) {
+    double *x = c[ip], X, Y, XP, YP, p0, rho;
+    x[4] += dzi * sqrt(1 + SQR(x[1]) + SQR(x[3]));
+    x[0] = x[0] + dxi + dzi * x[1];
+    x[2] = x[2] + dyi + dzi * x[3];
+    X = x[0] * ct + x[2] * st;
+    Y = -x[0] * st + x[2] * ct;
+    x[0] = X;
+    x[2] = Y;
+    XP = x[1] * ct + x[3] * st;
+    YP = -x[1] * st + x[3] * ct;
+    x[1] = XP;
+    x[3] = YP;
+    p0 = Po * (1 + x[5]);
+    beta0[ip] = p0 / sqrt(p0 * p0 + 1);
+    x[4] /= beta0[ip];
+    if (edge1) {
+      rho = (1 + x[5]) * rho_actual;
+      x[1] += M_TAN(e1) / rho * x[0];
+      x[3] -= M_TAN(e1 - psi1 / (1 + x[5])) / rho * x[2];
+    }
+  }
+  CSRConstant = 0;
+  if (p[B2E_BEND_CSR] && more_than_one) {
+    double eps0 = 1 / ((4 * PI_ * 1e-7) * C_MKS * C_MKS);
+    CSRConstant = 2 * cw->macroParticleCharge * E_MKS / M_POW13(3 * rho0 * rho0) / (4 * PI_ * eps0 * ME_MKS * SQR(C_MKS));
+  }
+  phiBend = cw->accumulatedAngle;
+  itop = np - 1;
+  for (kick = 0; kick < nSlices; kick++) {
+    for (ip = 0; ip <= itop; ip++) {
+      double *x = c[ip], Qi[6], Qf[6], f, dz_lost;
+      int lost;
+      Qi[0] = x[0];
+      Qi[1] = x[1];
+      Qi[2] = x[2];
+      Qi[3] = x[3];
+      Qi[4] = 0;
+      Qi[5] = x[5];
+      f = (1 + Qi[5]) / sqrt(1 + SQR(Qi[1]) + SQR(Qi[3]));
+      Qi[1] *= f;
+      Qi[3] *= f;
+      lost = !csbend_integrate(Qf, Qi, length / nSlices, 1, rho0, rho_actual, &ap, integ, 0, &dz_lost);
+      f = 1 / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
+      Qf[1] *= f;
+      Qf[3] *= f;
+      x[0] = Qf[0];
+      x[1] = Qf[1];
+      x[2] = Qf[2];
+      x[3] = Qf[3];
+      x[5] = Qf[5];
+      if (lost) {
+        /* the reference swaps the rows but not beta0[] (csbend.c:2417-2437),
+         * so the row moved into slot ip continues with the lost particle's
+         * beta0; kept as is */
+        swap_rows(c[ip], c[itop]);
+        c[itop][4] = z_start + dz_lost;
+        c[itop][5] = Po * (1 + c[itop][5]);
+        itop--;
+        ip--;
+      } else
+        x[4] += Qf[4] / beta0[ip];
+    }
+    np = itop + 1;
+    if (more_than_one) {
+      long diS, diS4, ib;
+      ctLower = ctUpper = dct = 0;
+      nBinned = bin_coordinate(ctHist, nBins, &ctLower, &ctUpper, &dct, brf, c, np, 4);
+      if (sgHalf > 0) {
+        double sum = 0, factor;
+        b2e_sg_apply_host(ctHist, nBins, sgOrder, sgHalf, sgHalf, 0);
+        /* correctDistribution (csbend.c:4705-4721) */
+        for (ib = 0; ib < nBins; ib++) {
+          if (ctHist[ib] < 0)
+            ctHist[ib] = 0;
+          sum += ctHist[ib];
+        }
+        if (sum) {
+          factor = 1.0 * nBinned / sum;
+          for (ib = 0; ib < nBins; ib++)
+            ctHist[ib] *= factor;
+        }
+      }
+      for (ib = 0; ib < nBins; ib++) {
+        denom[ib] = M_POW13(dct * ib);
+        ctHistDeriv[ib] = (ctHist[ib] /= dct);
+      }
+      b2e_sg_apply_host(ctHistDeriv, nBins, sgdOrder, sgdHalf, sgdHalf, 1);
+      phiBend += angle / nSlices;
+      {
+        double slip = fabs(rho0 * (phiBend * phiBend * phiBend) / 24.0), slip13 = M_POW13(slip);
+        diS = (long)(slip / dct);
+        diS4 = (long)(4 * slip / dct);
+        for (ib = 0; ib < nBins; ib++) {
+          double term1 = 0, term2 = 0;
+          long count, jb;
+          T1[ib] = T2[ib] = 0;
+          if (CSRConstant) {
+            if (p[B2E_BEND_STEADY_STATE]) {
+              if (!p[B2E_BEND_TRAPAZOID_INTEGRATION]) {
+                for (jb = ib + 1; jb < nBins; jb++)
+                  T1[ib] += ctHistDeriv[jb] / denom[jb - ib];
+              } else {
+                if ((jb = ib + 1) < nBins)
+                  term1 = ctHistDeriv[jb] / denom[jb - ib];
+                for (count = 0, jb = ib + 1; jb < nBins; jb++, count++)
+                  T1[ib] += (term2 = ctHistDeriv[jb] / denom[jb - ib]);
+                if ((ib + 1) < nBins)
+                  T1[ib] += 0.3 * SQR(denom[1]) * (2 * ctHistDeriv[ib + 1] + 3 * ctHistDeriv[ib]) / dct;
+                if (count > 1)
+                  T1[ib] -= (term1 + term2) / 2;
+              }
+            } else {
+              if (!p[B2E_BEND_TRAPAZOID_INTEGRATION]) {
+                for (jb = ib + 1; jb <= (ib + diS) && jb < nBins; jb++)
+                  T1[ib] += ctHistDeriv[jb] / denom[jb - ib];
+              } else {
+                if ((jb = ib + 1) < nBins && jb <= (ib + diS))
+                  term1 = ctHistDeriv[jb] / denom[jb - ib] / 2;
+                for (count = 0, jb = ib + 1; jb <= (ib + diS) && jb < nBins; count++, jb++)
+                  T1[ib] += (term2 = ctHistDeriv[jb] / denom[jb - ib]);
+                if (diS > 0 && (ib + 1) < nBins)
+                  T1[ib] += 0.3 * SQR(denom[1]) * (2 * ctHistDeriv[ib + 1] + 3 * ctHistDeriv[ib]) / dct;
+                if (count > 1)
+                  T1[ib] -= (term1 + term2) / 2;
+              }
+              if ((ib + diS) < nBins)
+                T2[ib] += ctHist[ib + diS];
+              if ((ib + diS4) < nBins)
+                T2[ib] -= ctHist[ib + diS4];
+            }
+            T1[ib] *= CSRConstant * length / nSlices;
+            T2[ib] *= -CSRConstant * length / nSlices / slip13;
+          }
+          cw->dGamma[ib] = T1[ib] + T2[ib];
+        }
+      }
+      if (cw->wakes) {
+        if (cw->n_wakes + nBins > cw->cap_wakes) {
+          cw->cap_wakes = 2 * (cw->n_wakes + nBins);
+          cw->wakes = realloc(cw->wakes, sizeof(double) * cw->cap_wakes);
+        }
+        memcpy(cw->wakes + cw->n_wakes, cw->dGamma, sizeof(double) * nBins);
+        cw->n_wakes += nBins;
+      }
+      if (CSRConstant) {
+        for (ip = 0; ip < np; ip++) {
+          double *x = c[ip], f;
+          iBin = (long)(f = (x[4] - ctLower) / dct);
+          f -= iBin;
+          if (iBin >= 0 && iBin < nBins - 1)
+            x[5] += ((1 - f) * cw->dGamma[iBin] + f * cw->dGamma[iBin + 1]) / Po * (1 + x[0] / rho0);
+        }
+      }
+    }
+  }
+  /* exit (csbend.c:2810-2955) */
+  if (more_than_one) {
+    cw->dctBin = dct;
+    ctLower = ctUpper = dct = 0;
+    bin_coordinate(ctHist, nBins, &ctLower, &ctUpper, &dct, brf, c, np, 4);
+    cw->s0 = ctLower + dzf;
+  } else {
+    ctLower = ctUpper = dct = 0;
+    cw->dctBin = dct;
+    cw->s0 = ctLower + dzf;
+  }
+  itop = np - 1;
+  for (ip = 0; ip <= itop; ip++) {
+    double *x = c[ip], p1, beta1, X, Y, XP, YP, rho;
+    p1 = Po * (1 + x[5]);
+    beta1 = p1 / sqrt(SQR(p1) + 1);
+    x[4] = x[4] * beta1;
+    if (p1 <= 0) {
+      swap_rows(c[ip], c[itop]);
+      c[itop][5] = Po * (1 + c[itop][5]);
+      itop--;
+      ip--;
+      continue;
+    }
+    if (edge2) {
+      rho = (1 + x[5]) * rho_actual;
+      x[1] += M_TAN(e2) / rho * x[0];
+      x[3] -= M_TAN(e2 - psi2 / (1 + x[5])) / rho * x[2];
+    }
+    X = x[0] * ct - x[2] * st + 0.0;
+    Y = x[0] * st + x[2] * ct + 0.0;
+    XP = x[1] * ct - x[3] * st + 0.0;
+    YP = x[1] * st + x[3] * ct + 0.0;
+    x[0] = X;
+    x[2] = Y;
+    x[1] = XP;
+    x[3] = YP;
+    x[0] += dxf + dzf * x[1];
+    x[2] += dyf + dzf * x[3];
+    x[4] += dzf * sqrt(1 + SQR(x[1]) + SQR(x[3])) + 0.0;
+  }
+  if (more_than_one)
+    cw->valid = 1;
+  cw->accumulatedAngle += fabs(angle);
+  free(beta0);
+  free(ctHist);
+  free(ctHistDeriv);
+  free(denom);
+  free(T1);
+  free(T2);
+  return itop + 1;
+}
+
+static long csrdrift_track(double **c, long np, const b2e_element *el, double Po, double zStart, CsrWake *cw) {
+  const double *p = el->p;
+  double length = p[B2E_CSRDRIFT_L], dz, dz0, dzFirst, ct0 = 0, factor, dct;
+  long nKicks, iKick, ip, nBins1;
+  if (np <= 1 || !cw->valid || !p[B2E_CSRDRIFT_CSR]) {
+    exact_drift(c, np, length);
+    return np;
+  }
+  nBins1 = cw->bins - 1;
+  dct = cw->dctBin;
+  if (p[B2E_CSRDRIFT_DZ] > 0) {
+    if ((nKicks = (long)(length / p[B2E_CSRDRIFT_DZ])) < 1)
+      nKicks = 1;
+  } else
+    nKicks = (long)p[B2E_CSRDRIFT_N_KICKS];
+  dz = (dz0 = length / nKicks) / 2;
+  dzFirst = zStart - cw->zLast;
+  for (iKick = 0; iKick < nKicks; iKick++) {
+    if (iKick == 1)
+      dz = dz0;
+    for (ip = 0; ip < np; ip++) {
+      double *x = c[ip], pp, beta;
+      x[0] += x[1] * dz;
+      x[2] += x[3] * dz;
+      pp = Po * (1 + x[5]);
+      beta = pp / sqrt(pp * pp + 1);
+      x[4] = (x[4] + dz * sqrt(1 + SQR(x[1]) + SQR(x[3]))) / beta;
+    }
+    cw->s0 += dz + dzFirst;
+    ct0 = cw->s0;
+    factor = (dz0 + dzFirst) / cw->ds0;
+    dzFirst = 0;
+    for (ip = 0; ip < np; ip++) {
+      double *x = c[ip], f, pp, beta;
+      long iBin = (long)(f = (x[4] - ct0) / dct);
+      f -= iBin;
+      if (iBin >= 0 && iBin < nBins1)
+        x[5] += ((1 - f) * cw->dGamma[iBin] + f * cw->dGamma[iBin + 1]) / Po * factor;
+      pp = (1 + x[5]) * Po;
+      beta = pp / sqrt(pp * pp + 1);
+      x[4] = beta * x[4];
+    }
+  }
+  dz = dz0 / 2;
+  for (ip = 0; ip < np; ip++) {
+    double *x = c[ip];
+    x[0] += x[1] * dz;
+    x[2] += x[3] * dz;
+    x[4] += dz * sqrt(1 + SQR(x[1]) + SQR(x[3]));
+  }
+  cw->zLast = zStart + length;
+  cw->s0 += dz;
+  return np;
+}
+
 /* ---- do_tracking restated ------------------------------------------------ */
 /* rows: np x 8 (x, xp, y, yp, s, delta, id, lossPass); lossPass must be -1 on
- * input.  Returns survivors; rows are left in the reference's array order. */
-long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_passes, int default_order,
-                      double *rows, long np, double *effort) {
+ * input.  Returns survivors; rows are left in the reference's array order.
+ * wakes (optional): every CSRCSBEND kick's dGamma, in order. */
+long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int n_passes, int default_order,
+                          double *rows, long np, double *effort, double *wakes, long wake_cap, long *n_wakes) {
   double **c = malloc(sizeof(double *) * (np ? np : 1));
   long i, nToTrack = np, nLeft;
   int pass, k;
   MaxAmp ma;
+  CsrWake cw;
   RfState *rf = calloc(n_el ? n_el : 1, sizeof(RfState));
   memset(&ma, 0, sizeof(ma));
+  memset(&cw, 0, sizeof(cw));
+  if (wakes) {
+    cw.cap_wakes = 1024;
+    cw.wakes = malloc(sizeof(double) * cw.cap_wakes);
+  }
   for (i = 0; i < np; i++)
     c[i] = rows + i * NPROP;
   *effort = 0;
@@ -858,6 +1290,8 @@ long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_p
       case B2E_KSEXT:
       case B2E_CSBEND:
       case B2E_RFCA:
+      case B2E_CSRCSBEND:
+      case B2E_CSRDRIFT:
         L = p[0];
         break;
       default:
@@ -892,6 +1326,20 @@ long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_p
           ma.exponent = (long)p[B2E_MAXAMP_EXPONENT];
           ma.y_exponent = (long)p[B2E_MAXAMP_Y_EXPONENT];
           break;
+        case B2E_CHARGE:
+          /* do_tracking.c:1324-1360: charge per macro-particle on the first pass */
+          if (pass == 0) {
+            cw.macroParticleCharge = np ? p[B2E_CHARGE_TOTAL] / np : 0;
+            if (p[B2E_CHARGE_PER_PARTICLE])
+              cw.macroParticleCharge = p[B2E_CHARGE_PER_PARTICLE];
+          }
+          break;
+        case B2E_CSRCSBEND:
+          nLeft = csrcsbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, z, &ma, &cw);
+          break;
+        case B2E_CSRDRIFT:
+          nLeft = csrdrift_track(c, nToTrack, e, p_central, last_z, &cw);
+          break;
         default:
           break;
         }
@@ -910,9 +1358,20 @@ long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_p
     }
     *effort += nToTrack;
   }
+  if (n_wakes)
+    *n_wakes = cw.n_wakes;
+  if (wakes && cw.wakes)
+    memcpy(wakes, cw.wakes, sizeof(double) * (cw.n_wakes < wake_cap ? cw.n_wakes : wake_cap));
+  free(cw.wakes);
+  free(cw.dGamma);
   free(rf);
   free(c);
   return nToTrack;
+}
+
+long b2e_oracle_track(const b2e_element *el, int n_el, double p_central, int n_passes, int default_order,
+                      double *rows, long np, double *effort) {
+  return b2e_oracle_track_csr(el, n_el, p_central, n_passes, default_order, rows, np, effort, NULL, 0, NULL);
 }
 
 /* Elementary functions as this build sees them (for the maths tests). */

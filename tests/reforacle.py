@@ -97,8 +97,9 @@ class PortOracle:
             fn.argtypes = [ctypes.c_double]
         self.math = math
 
-    def track(self, lattice, coords, ids, p_central, n_passes, default_order=2):
-        """Returns (rows, n_left, effort) like RefOracle.track."""
+    def track(self, lattice, coords, ids, p_central, n_passes, default_order=2, capture_wakes=False):
+        """Returns (rows, n_left, effort) like RefOracle.track, plus the per-kick
+        CSR wakes as a fourth item when capture_wakes is set."""
         n = coords.shape[0]
         rows = np.zeros((max(n, 1), 8))
         rows[:n, :6] = coords
@@ -106,7 +107,15 @@ class PortOracle:
         rows[:n, 7] = -1
         elems = lattice.to_ctypes()
         eff = ctypes.c_double()
-        nl = self.lib.b2e_oracle_track(elems, ctypes.c_int(len(lattice)), ctypes.c_double(p_central),
-                                       ctypes.c_int(n_passes), ctypes.c_int(default_order),
-                                       rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.byref(eff))
+        self.lib.b2e_oracle_track_csr.restype = ctypes.c_long
+        cap = 4_000_000 if capture_wakes else 0
+        wakes = np.zeros(max(cap, 1))
+        nw = ctypes.c_long()
+        nl = self.lib.b2e_oracle_track_csr(elems, ctypes.c_int(len(lattice)), ctypes.c_double(p_central),
+                                           ctypes.c_int(n_passes), ctypes.c_int(default_order),
+                                           rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.byref(eff),
+                                           wakes.ctypes.data_as(ctypes.c_void_p) if capture_wakes else None,
+                                           ctypes.c_long(cap), ctypes.byref(nw))
+        if capture_wakes:
+            return rows[:n], nl, eff.value, wakes[: nw.value]
         return rows[:n], nl, eff.value

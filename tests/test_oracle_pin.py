@@ -93,3 +93,30 @@ def test_shared_math_within_one_ulp_envelope_after_200_turns():
     envelope = _rel(a[0], c[0])
     diff = _rel(a[0], b[0])
     assert (diff <= 20 * envelope + 1e-15).all(), (diff, envelope)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("variant", ["default", "steady_plain", "no_sg"])
+def test_port_reproduces_reference_csr(math, variant):
+    """CSRCSBEND + CSRDRIFT: the restatement reproduces the reference's final
+    rows and every per-kick wake (captured through the reference's own
+    OUTPUT_FILE writer) bit for bit."""
+    from elegant_b200 import Element, Lattice
+    lat = w.chicane(bins=120, n_kicks=4, sg_halfwidth=0 if variant == "no_sg" else 2)
+    if variant == "steady_plain":
+        els = []
+        for i, e in enumerate(lat.elements):
+            if e.type == "CSRCSBEND":
+                e = Element(e.name, e.type, dict(e.params, **({"STEADY_STATE": 1} if i % 2 else
+                                                              {"TRAPAZOID_INTEGRATION": 0})))
+            if e.type == "CSRDRIFT":
+                e = Element(e.name, e.type, dict(e.params, N_KICKS=3))
+            els.append(e)
+        lat = Lattice(els)
+    beam = w.chicane_beam(6000, seed=11)
+    p0 = 1000 / 0.51099895
+    r1, n1, e1, w1 = RefOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    r2, n2, e2, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    assert n1 == n2 and w1.size == w2.size > 0
+    assert np.array_equal(w1, w2)
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
