@@ -52,12 +52,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-csr", action="store_true")
+    ap.add_argument("--no-history", action="store_true", help="do not record the per-instance pass history")
+    ap.add_argument("--ring-variant", type=int, default=0, help="0 = autotune, else a fixed ring-kernel variant")
     ap.add_argument("--csr-particles", type=int, default=1_000_000)
     return ap.parse_args()
 
 
 def csr_section(args, device, flush):
-    """Secondary figure: CSR pass time on the single-pass chicane (config 1:
+    """Secondary figure: CSR pass time on the single-pass chicane (
     1 GeV, 1 nC, 1e6 particles, 4 CSRCSBEND x 20 kicks, BINS=600,
     SG_HALFWIDTH=2, CSRDRIFT 5/1/5 m).  A run is the whole chicane; the CSR
     pass time is its device time divided by the 80 dipole kicks (each kick =
@@ -87,7 +89,7 @@ def csr_section(args, device, flush):
     kicks = sum(int(e.get("N_SLICES")) for e in lat.elements if e.type == "CSRCSBEND")
     ms = sum(times) / len(times)
     tr.close()
-    return {"workload": "bunch-compressor chicane with CSR (config 1)", "particles": beam.n, "dipole_kicks": kicks,
+    return {"workload": "bunch-compressor chicane with CSR, 1 GeV, 1 nC", "particles": beam.n, "dipole_kicks": kicks,
             "run_ms": ms, "csr_pass_ms_per_kick": ms / kicks,
             "particle_kicks_per_s": beam.n * kicks / (ms / 1e3),
             "timing": "CUDA events on the engine stream; includes CSRDRIFT kicks and the one host sync per CSR element"}
@@ -214,7 +216,8 @@ def main():
     seed = 2024 + 1000 * rank
     lat, beam, offsets, overrides = w.ensemble(n_instances=args.instances, seed=seed)
     n = beam.n
-    tracker = Tracker(lat, w.ring_p_central(), args.turns_per_step, device=local_rank)
+    tracker = Tracker(lat, w.ring_p_central(), args.turns_per_step, device=local_rank,
+                      record_history=not args.no_history, ring_variant=args.ring_variant)
     tracker.load_ensemble(offsets, overrides)
     stream = torch.cuda.ExternalStream(tracker.stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -243,6 +246,14 @@ def main():
     torch.cuda.synchronize()
     launches = tracker.launches - launches0
     variant, tune_ms = tracker.ring_tuning()
+    history = None
+    if not args.no_history:
+        h = tracker.history()
+        history = {"recorded": "per instance and pass: survivors, <x>, <y>, rms emittances",
+                   "passes": int(h["ex"].shape[1]),
+                   "final_survival": float(h["survivors"][:, -1].sum() / n),
+                   "final_ex_median_m": float(np.median(h["ex"][:, -1])),
+                   "final_ey_median_m": float(np.median(h["ey"][:, -1]))}
     t_total = sum(step_ms) / 1e3
     if dist:
         tt = torch.tensor([t_total, effort_total], dtype=torch.float64, device="cuda")
@@ -332,8 +343,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_job * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched error ensemble of the 8-cell FODO ring (config 2)",
+            "config": {"workload": "batched error ensemble of the 8-cell FODO ring",
                        "instances_per_gpu": args.instances, "particles_per_gpu": n,
+                       "history": history,
                        "turns_per_step": args.turns_per_step, "lattice_elements": len(lat),
                        "ring_variant": variant, "autotune_ms_per_pass": [round(x, 3) for x in tune_ms],
                        "l2": "flushed (256 MiB write) before every timed step"},
@@ -372,7 +384,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": sum(steps) / len(steps), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "batched error ensemble of the 8-cell FODO ring (config 2)",
+        "config": {"workload": "batched error ensemble of the 8-cell FODO ring",
                    "instances_per_gpu": args.instances},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

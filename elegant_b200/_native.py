@@ -25,12 +25,13 @@ ERRORS = {
 # element type codes (include/elegant_b200.h)
 DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT = range(1, 12)
 MAX_PARAMS = 40
+RING_VARIANTS = 12
 
 EXPORTED = [
     "b2e_create", "b2e_destroy", "b2e_last_error", "b2e_version", "b2e_load_lattice",
     "b2e_upload_particles", "b2e_track", "b2e_download", "b2e_track_host", "b2e_track_device",
     "b2e_load_ensemble", "b2e_ensemble_history", "b2e_csr_wakes", "b2e_stream",
-    "b2e_kernel_launches", "b2e_ring_tuning",
+    "b2e_kernel_launches", "b2e_ring_tuning", "b2e_history_passes", "b2e_csr_bend_static",
 ]
 
 
@@ -42,7 +43,8 @@ class Element(ctypes.Structure):
 class RunOptions(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_int32), ("default_order", ctypes.c_int32),
                 ("coord_limit", ctypes.c_double), ("slope_limit", ctypes.c_double),
-                ("passes_per_launch", ctypes.c_int32), ("ring_variant", ctypes.c_int32)]
+                ("passes_per_launch", ctypes.c_int32), ("ring_variant", ctypes.c_int32),
+                ("record_history", ctypes.c_int32)]
 
 
 class Override(ctypes.Structure):
@@ -87,6 +89,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_csr_wakes": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
         "b2e_stream": (vp, [vp]),
         "b2e_kernel_launches": (i64, [vp]),
+        "b2e_history_passes": (i64, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

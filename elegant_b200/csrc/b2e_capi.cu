@@ -92,6 +92,13 @@ struct b2e_ctx {
   std::vector<float> tune_ms;
   DevBuf<double> d_scratch;       /* 6 columns, for timing variants off the real state */
   DevBuf<int32_t> d_scratch_loss; /* 2 columns */
+  /* ensemble history */
+  std::vector<int> tile_first;     /* first tile of each instance, n_inst + 1 entries */
+  DevBuf<int> d_tile_first;
+  DevBuf<double> d_hist_partials;  /* [n_tiles][passes of the call][11] */
+  DevBuf<double> d_hist_out;       /* [n_inst][passes of the call][5] */
+  std::vector<double> history;     /* [pass][inst][5]: survivors, <x>, <y>, ex, ey */
+  int hist_pass0 = 0, hist_passes = 0;
 };
 
 static int fail(b2e_ctx *ctx, int code, const char *fmt, ...) {
@@ -178,6 +185,7 @@ extern "C" int b2e_ring_tuning(const b2e_ctx *ctx, int32_t *chosen, float *ms_pe
 /* Rebuild the tile table for the current instance partition. */
 static void build_tiles(b2e_ctx *ctx) {
   ctx->tiles.clear();
+  ctx->tile_first.assign(1, 0);
   for (int i = 0; i < ctx->n_inst; i++) {
     for (int64_t s = ctx->inst_offsets[i]; s < ctx->inst_offsets[i + 1]; s += kTileThreads) {
       DevTile t;
@@ -186,6 +194,7 @@ static void build_tiles(b2e_ctx *ctx) {
       t.inst = i;
       ctx->tiles.push_back(t);
     }
+    ctx->tile_first.push_back((int)ctx->tiles.size());
   }
 }
 
@@ -201,6 +210,9 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
   CUDA_TRY(ctx, ctx->d_inst_offsets.ensure(ctx->inst_offsets.size()));
   CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_inst_offsets.ptr, ctx->inst_offsets.data(),
                                 sizeof(int64_t) * ctx->inst_offsets.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CUDA_TRY(ctx, ctx->d_tile_first.ensure(ctx->tile_first.size()));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_tile_first.ptr, ctx->tile_first.data(), sizeof(int) * ctx->tile_first.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(ctx, ctx->d_tiles.ensure(std::max<size_t>(ctx->tiles.size(), 1)));
   if (!ctx->tiles.empty())
     CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_tiles.ptr, ctx->tiles.data(), sizeof(DevTile) * ctx->tiles.size(),
@@ -338,8 +350,10 @@ static DevParticles particle_view(b2e_ctx *ctx) {
 
 /* Autotuner: time every ring-kernel variant on one pass of a scratch copy of
  * the current particle state (so the real state is untouched) and keep the
- * fastest.  The variants differ only in register allocation, never in
- * arithmetic, so the choice cannot change results. */
+ * fastest.  The variants differ only in register allocation and in how often
+ * a block's warps are brought back in step, never in arithmetic, so the
+ * choice cannot change results.  With history recording the timed pass
+ * records too (into slots the real launch overwrites). */
 static int autotune_ring(b2e_ctx *ctx, const RingLaunch &Lreal, bool staged, size_t smem, int p, int e) {
   const int64_t n = ctx->n;
   const int ne = Lreal.n_elems;
@@ -407,6 +421,9 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.g.coord_limit = ctx->opt.coord_limit;
   L.g.slope_limit = ctx->opt.slope_limit;
   L.error_flag = ctx->d_flag.ptr;
+  L.hist = ctx->opt.record_history && !ctx->use_ext ? ctx->d_hist_partials.ptr : nullptr;
+  L.hist_pass0 = ctx->hist_pass0;
+  L.hist_passes = ctx->hist_passes;
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
@@ -463,6 +480,20 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
   const int p0 = ctx->pass_counter;
   const int npass = p0 + ctx->opt.n_passes; /* one past the last pass of this call */
   CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_flag.ptr, 0, sizeof(unsigned int), ctx->stream));
+  const bool record = ctx->opt.record_history && !ctx->use_ext && ctx->opt.n_passes > 0;
+  if (p0 == 0)
+    ctx->history.clear();
+  if (record) {
+    if (!ctx->lat.csr_elements.empty())
+      return fail(ctx, B2E_ERR_LATTICE, "history recording is not available with CSR elements");
+    ctx->hist_pass0 = p0;
+    ctx->hist_passes = ctx->opt.n_passes;
+    CUDA_TRY(ctx, ctx->d_hist_partials.ensure(std::max<size_t>(ctx->tiles.size(), 1) * ctx->hist_passes * 11));
+    CUDA_TRY(ctx, ctx->d_hist_out.ensure((size_t)ctx->n_inst * ctx->hist_passes * 5));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_hist_partials.ptr, 0,
+                                  sizeof(double) * std::max<size_t>(ctx->tiles.size(), 1) * ctx->hist_passes * 11,
+                                  ctx->stream));
+  }
   if (p0 == 0) {
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_rf.ptr, 0, sizeof(DevRfState) * std::max(1, ctx->n_inst * ctx->lat.n_rf),
                                   ctx->stream));
@@ -542,6 +573,22 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     }
   }
   ctx->pass_counter = npass;
+  if (record) {
+    CUDA_TRY(ctx, launch_history_merge(ctx->d_hist_partials.ptr, ctx->hist_passes, ctx->d_tile_first.ptr,
+                                       ctx->n_inst, ctx->d_hist_out.ptr, ctx->stream));
+    ctx->launches++;
+    std::vector<double> h((size_t)ctx->n_inst * ctx->hist_passes * 5);
+    CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), ctx->d_hist_out.ptr, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    /* [inst][pass][5] -> append as [pass][inst][5] */
+    const size_t base = ctx->history.size();
+    ctx->history.resize(base + h.size());
+    for (int j = 0; j < ctx->hist_passes; j++)
+      for (int i = 0; i < ctx->n_inst; i++)
+        for (int k = 0; k < 5; k++)
+          ctx->history[base + ((size_t)j * ctx->n_inst + i) * 5 + k] = h[((size_t)i * ctx->hist_passes + j) * 5 + k];
+  }
   CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 2 * sizeof(unsigned long long), ctx->stream));
   ctx->launches++;
   CUDA_TRY(ctx, launch_effort(particle_view(ctx).lost_pass, ctx->n, p0, npass, ctx->d_counters.ptr,
@@ -654,12 +701,31 @@ extern "C" int b2e_track_device(b2e_ctx *ctx, double *const dev_columns[6], cons
 
 extern "C" int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *cy, double *ex,
                                     double *ey) {
-  (void)survivors;
-  (void)cx;
-  (void)cy;
-  (void)ex;
-  (void)ey;
-  return fail(ctx, B2E_ERR_STATE, "b2e_ensemble_history: not available");
+  if (!ctx)
+    return B2E_ERR_ARG;
+  if (!ctx->opt.record_history)
+    return fail(ctx, B2E_ERR_STATE, "b2e_ensemble_history: run options did not request record_history");
+  const size_t n_inst = (size_t)ctx->n_inst, n_pass = ctx->history.size() / (n_inst * 5);
+  for (size_t i = 0; i < n_inst; i++)
+    for (size_t j = 0; j < n_pass; j++) {
+      const double *h = &ctx->history[(j * n_inst + i) * 5];
+      const size_t o = i * n_pass + j;
+      if (survivors)
+        survivors[o] = (int64_t)h[0];
+      if (cx)
+        cx[o] = h[1];
+      if (cy)
+        cy[o] = h[2];
+      if (ex)
+        ex[o] = h[3];
+      if (ey)
+        ey[o] = h[4];
+    }
+  return B2E_OK;
+}
+
+extern "C" int64_t b2e_history_passes(const b2e_ctx *ctx) {
+  return ctx && ctx->n_inst > 0 ? (int64_t)(ctx->history.size() / ((size_t)ctx->n_inst * 5)) : -1;
 }
 
 extern "C" int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written) {

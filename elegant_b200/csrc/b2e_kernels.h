@@ -20,14 +20,20 @@ struct RingLaunch {
   int pass_end, elem_end;     /* last pass tracked, and one past its last element */
   DevGlobals g;
   unsigned int *error_flag;
+  double *hist;    /* per (tile, pass) moments [n_tiles][hist_passes][11], or null */
+  int hist_pass0;  /* absolute pass of hist's first slot */
+  int hist_passes;
 };
 
-/* variant 1..B2E_RING_VARIANTS selects the occupancy target (see ring_kernel). */
+/* variant 1..B2E_RING_VARIANTS selects the occupancy target and the barrier
+ * level of the ring kernel (see launch_ring in b2e_ring.cu). */
 cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
                         int variant);
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
                             cudaStream_t stream);
+cudaError_t launch_history_merge(const double *partials, int hist_passes, const int *tile_first, int n_inst,
+                                 double *out, cudaStream_t stream);
 cudaError_t launch_effort(const int32_t *lost_pass, int64_t n, int pass_begin, int pass_end, unsigned long long *effort,
                           unsigned long long *survivors, cudaStream_t stream);
 

@@ -28,12 +28,60 @@ namespace b2e {
 
 
 
+/* Per-pass beam moments of one tile, for the ensemble history: count, means
+ * of x, xp, y, yp, then sums of squared deviations (x, xp, xx', y, yp, yy')
+ * about the tile means -- two block reductions in a fixed order, so the
+ * result does not depend on scheduling.  Every thread of the block calls it. */
+__device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *out) {
+  __shared__ double red[4][12];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v[5] = {alive ? 1.0 : 0.0, alive ? p.x : 0.0, alive ? p.xp : 0.0, alive ? p.y : 0.0, alive ? p.yp : 0.0};
+  for (int k = 0; k < 5; k++)
+    for (int off = 16; off > 0; off >>= 1)
+      v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+  if (lane == 0)
+    for (int k = 0; k < 5; k++)
+      red[warp][k] = v[k];
+  __syncthreads();
+  double tot[5];
+  for (int k = 0; k < 5; k++)
+    tot[k] = ((red[0][k] + red[1][k]) + red[2][k]) + red[3][k];
+  const double n = tot[0];
+  double m[4];
+  for (int k = 0; k < 4; k++)
+    m[k] = n > 0 ? tot[k + 1] / n : 0.0;
+  const double dx = p.x - m[0], dxp = p.xp - m[1], dy = p.y - m[2], dyp = p.yp - m[3];
+  double q[6] = {alive ? dx * dx : 0.0,  alive ? dxp * dxp : 0.0, alive ? dx * dxp : 0.0,
+                 alive ? dy * dy : 0.0,  alive ? dyp * dyp : 0.0, alive ? dy * dyp : 0.0};
+  for (int k = 0; k < 6; k++)
+    for (int off = 16; off > 0; off >>= 1)
+      q[k] += __shfl_down_sync(0xffffffffu, q[k], off);
+  if (lane == 0)
+    for (int k = 0; k < 6; k++)
+      red[warp][5 + k] = q[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[0] = n;
+    for (int k = 0; k < 4; k++)
+      out[1 + k] = m[k];
+    for (int k = 0; k < 6; k++)
+      out[5 + k] = ((red[0][5 + k] + red[1][5 + k]) + red[2][5 + k]) + red[3][5 + k];
+  }
+  __syncthreads();
+}
+
 /* MINB is the occupancy target (blocks of 128 threads per SM) handed to the
- * register allocator: 4 keeps every value in registers (~116 registers),
+ * register allocator: 4 keeps every value in registers (~118 registers),
  * 5/6/8 trade a few spills to L1 for more resident warps to hide FP64
- * latency.  The arithmetic is identical in every variant. */
-template <bool STAGED, int MINB>
+ * latency.  SYNC sets how often the four warps of a block are brought back
+ * in step: 0 never, 1 after every pass, 2 after every element; warps that
+ * stay on the same element share its instruction stream and its shared-
+ * memory record.  The arithmetic is identical in every variant.  HIST records
+ * the per-pass tile moments (it needs SYNC >= 1); when SYNC >= 1 every thread
+ * stays in the pass loop until the whole tile is lost. */
+template <bool STAGED, int MINB, int SYNC, bool HIST>
 __global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
+  static_assert(!HIST || SYNC >= 1, "history needs the per-pass barrier");
   extern __shared__ __align__(16) unsigned char smem[];
   const DevTile tile = L.tiles[blockIdx.x];
   const DevElem *elems = L.elems + (size_t)tile.inst * L.n_elems;
@@ -57,25 +105,40 @@ __global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
     aps = sa;
   }
 
-  if ((int)threadIdx.x >= tile.count)
-    return;
   const int64_t ip = tile.start + threadIdx.x;
-  if (L.P.lost_pass[ip] >= 0)
+  const bool tracked = (int)threadIdx.x < tile.count && L.P.lost_pass[ip] < 0;
+  if (SYNC == 0 && !tracked)
     return;
 
-  Part p;
-  p.x = L.P.x[ip];
-  p.xp = L.P.xp[ip];
-  p.y = L.P.y[ip];
-  p.yp = L.P.yp[ip];
-  p.s = L.P.s[ip];
-  p.dp = L.P.dp[ip];
+  Part p = {0, 0, 0, 0, 0, 0};
+  if (tracked) {
+    p.x = L.P.x[ip];
+    p.xp = L.P.xp[ip];
+    p.y = L.P.y[ip];
+    p.yp = L.P.yp[ip];
+    p.s = L.P.s[ip];
+    p.dp = L.P.dp[ip];
+  }
 
   int lost = LOSS_NONE, lost_pass = -1, lost_elem = -1;
-  for (int pass = L.pass_begin; pass <= L.pass_end && !lost; pass++) {
+  bool active = tracked;
+  for (int pass = L.pass_begin; pass <= L.pass_end; pass++) {
+    if (SYNC == 0) {
+      if (!active)
+        break;
+    } else if (!__syncthreads_or(active)) {
+      break; /* the whole tile is lost (history slots stay zero: no survivors) */
+    }
     const int e0 = pass == L.pass_begin ? L.elem_begin : 0;
     const int e1 = pass == L.pass_end ? L.elem_end : L.n_elems;
     for (int ie = e0; ie < e1; ie++) {
+      if (SYNC == 2)
+        __syncthreads();
+      if (!active) {
+        if (SYNC == 2)
+          continue;
+        break;
+      }
       const DevElem &e = elems[ie];
       const int iap = pass == 0 ? e.ap_pass0 : e.ap_later;
       const DevAperture *ap = iap >= 0 ? &aps[iap] : nullptr;
@@ -115,11 +178,15 @@ __global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
       if (lost) {
         lost_pass = pass;
         lost_elem = ie;
-        break;
+        active = false;
       }
     }
+    if (HIST && e1 == L.n_elems && pass >= L.hist_pass0)
+      tile_moments(p, active, L.hist + ((size_t)blockIdx.x * L.hist_passes + (pass - L.hist_pass0)) * 11);
   }
 
+  if (!tracked)
+    return;
   L.P.x[ip] = p.x;
   L.P.xp[ip] = p.xp;
   L.P.y[ip] = p.y;
@@ -130,6 +197,63 @@ __global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
     L.P.lost_pass[ip] = lost_pass;
     L.P.lost_elem[ip] = lost_elem;
   }
+}
+
+/* Ensemble history: merge the tiles of each instance, pass by pass, in tile
+ * order with the pairwise update of Chan, Golub & LeVeque (1979) for means
+ * and co-moments; rms emittance as rms_emittance (final_props.c:844-880):
+ * sqrt(Sxx Sx'x' - Sxx'^2)/n.  out[inst][pass][5] = survivors, <x>, <y>,
+ * emittance x, emittance y. */
+__global__ void history_merge_kernel(const double *partials, int hist_passes, const int *tile_first, int n_inst,
+                                     double *out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_inst * hist_passes)
+    return;
+  const int inst = idx / hist_passes, j = idx - inst * hist_passes;
+  double n = 0, m[4] = {0, 0, 0, 0}, S[6] = {0, 0, 0, 0, 0, 0};
+  for (int t = tile_first[inst]; t < tile_first[inst + 1]; t++) {
+    const double *b = partials + ((size_t)t * hist_passes + j) * 11;
+    const double nb = b[0];
+    if (nb == 0)
+      continue;
+    if (n == 0) {
+      n = nb;
+      for (int k = 0; k < 4; k++)
+        m[k] = b[1 + k];
+      for (int k = 0; k < 6; k++)
+        S[k] = b[5 + k];
+      continue;
+    }
+    const double N = n + nb, w = n * nb / N;
+    double d[4];
+    for (int k = 0; k < 4; k++)
+      d[k] = b[1 + k] - m[k];
+    S[0] += b[5] + d[0] * d[0] * w;
+    S[1] += b[6] + d[1] * d[1] * w;
+    S[2] += b[7] + d[0] * d[1] * w;
+    S[3] += b[8] + d[2] * d[2] * w;
+    S[4] += b[9] + d[3] * d[3] * w;
+    S[5] += b[10] + d[2] * d[3] * w;
+    for (int k = 0; k < 4; k++)
+      m[k] += d[k] * nb / N;
+    n = N;
+  }
+  double *o = out + (size_t)idx * 5;
+  o[0] = n;
+  o[1] = m[0];
+  o[2] = m[2];
+  double ex = S[0] * S[1] - S[2] * S[2], ey = S[3] * S[4] - S[5] * S[5];
+  o[3] = n > 0 ? (ex > 0 ? sqrt(ex) : 0) / n : 0;
+  o[4] = n > 0 ? (ey > 0 ? sqrt(ey) : 0) / n : 0;
+}
+
+cudaError_t launch_history_merge(const double *partials, int hist_passes, const int *tile_first, int n_inst,
+                                 double *out, cudaStream_t stream) {
+  const int total = n_inst * hist_passes;
+  if (total <= 0)
+    return cudaSuccess;
+  history_merge_kernel<<<(total + 127) / 128, 128, 0, stream>>>(partials, hist_passes, tile_first, n_inst, out);
+  return cudaGetLastError();
 }
 
 /* RFCA fiducial time, TMEAN mode (findFiducialTime, simple_rfca.c:177-230):
@@ -200,34 +324,56 @@ __global__ void effort_kernel(const int32_t *lost_pass, int64_t n, int pass_begi
   }
 }
 
-template <int MINB>
+template <int MINB, int SYNC, bool HIST>
 static cudaError_t launch_ring_v(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
                                  cudaStream_t stream) {
   if (staged) {
-    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem_bytes);
+    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB, SYNC, HIST>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
     if (err != cudaSuccess)
       return err;
-    ring_kernel<true, MINB><<<n_tiles, 128, smem_bytes, stream>>>(L);
+    ring_kernel<true, MINB, SYNC, HIST><<<n_tiles, 128, smem_bytes, stream>>>(L);
   } else {
-    ring_kernel<false, MINB><<<n_tiles, 128, 0, stream>>>(L);
+    ring_kernel<false, MINB, SYNC, HIST><<<n_tiles, 128, 0, stream>>>(L);
   }
   return cudaGetLastError();
 }
 
+template <int SYNC, bool HIST>
+static cudaError_t launch_ring_s(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
+                                 cudaStream_t stream, int minb_index) {
+  switch (minb_index) {
+  case 1:
+    return launch_ring_v<5, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+  case 2:
+    return launch_ring_v<6, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+  case 3:
+    return launch_ring_v<8, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+  default:
+    return launch_ring_v<4, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+  }
+}
+
+/* variant 1..12: occupancy target MINB = {4, 5, 6, 8}[(variant-1) % 4],
+ * barrier level SYNC = (variant-1) / 4.  With history the barrier level is
+ * at least 1. */
 cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
                         int variant) {
   if (n_tiles <= 0)
     return cudaSuccess;
-  switch (variant) {
+  if (variant < 1 || variant > B2E_RING_VARIANTS)
+    variant = 1;
+  const int minb_index = (variant - 1) % 4, sync = (variant - 1) / 4;
+  if (L.hist)
+    return sync == 2 ? launch_ring_s<2, true>(L, n_tiles, staged, smem_bytes, stream, minb_index)
+                     : launch_ring_s<1, true>(L, n_tiles, staged, smem_bytes, stream, minb_index);
+  switch (sync) {
+  case 1:
+    return launch_ring_s<1, false>(L, n_tiles, staged, smem_bytes, stream, minb_index);
   case 2:
-    return launch_ring_v<5>(L, n_tiles, staged, smem_bytes, stream);
-  case 3:
-    return launch_ring_v<6>(L, n_tiles, staged, smem_bytes, stream);
-  case 4:
-    return launch_ring_v<8>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_s<2, false>(L, n_tiles, staged, smem_bytes, stream, minb_index);
   default:
-    return launch_ring_v<4>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_s<0, false>(L, n_tiles, staged, smem_bytes, stream, minb_index);
   }
 }
 

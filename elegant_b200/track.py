@@ -38,7 +38,7 @@ class Tracker:
     """One engine context bound to a lattice and run options."""
 
     def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
-                 passes_per_launch: int = 0, ring_variant: int = 0):
+                 passes_per_launch: int = 0, ring_variant: int = 0, record_history: bool = False):
         self.lib = nat.load_library()
         self.lattice = lattice
         self._ctx = ctypes.c_void_p()
@@ -47,7 +47,7 @@ class Tracker:
             raise nat.EngineError(rc, "b2e_create failed (is a CUDA device visible?)")
         self.options = nat.RunOptions(p_central=p_central, n_passes=n_passes, default_order=default_order,
                                       coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
-                                      ring_variant=ring_variant)
+                                      ring_variant=ring_variant, record_history=int(record_history))
         self._elems = lattice.to_ctypes()
         self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
         self.n_instances = 1
@@ -140,7 +140,7 @@ class Tracker:
     def ring_tuning(self):
         """(variant in use, per-variant ms of one pass) from the autotuner."""
         chosen = ctypes.c_int32()
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * nat.RING_VARIANTS)()
         self._check(self.lib.b2e_ring_tuning(self._ctx, ctypes.byref(chosen), ms))
         return int(chosen.value), [float(x) for x in ms]
 
@@ -177,6 +177,18 @@ class Tracker:
         self._check(self.lib.b2e_track_device(self._ctx, ptrs, None, n, ptr(lost_pass), ptr(lost_element),
                                               ctypes.byref(effort)))
         return effort.value
+
+    def history(self) -> dict:
+        """Per-instance, per-pass survivors, centroids and rms emittances of the
+        run so far: arrays of shape (n_instances, n_passes)."""
+        n_pass = int(self.lib.b2e_history_passes(self._ctx))
+        shape = (self.n_instances, max(n_pass, 0))
+        out = {"survivors": np.zeros(shape, dtype=np.int64)}
+        for k in ("cx", "cy", "ex", "ey"):
+            out[k] = np.zeros(shape, dtype=np.float64)
+        self._check(self.lib.b2e_ensemble_history(self._ctx, *(out[k].ctypes.data for k in
+                                                                ("survivors", "cx", "cy", "ex", "ey"))))
+        return out
 
     def csr_wakes(self, capacity: int) -> np.ndarray:
         buf = np.empty(capacity, dtype=np.float64)

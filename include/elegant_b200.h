@@ -65,7 +65,7 @@ extern "C" {
 #define B2E_CSRDRIFT 11
 
 #define B2E_MAX_PARAMS 40
-#define B2E_RING_VARIANTS 4
+#define B2E_RING_VARIANTS 12
 
 /* Parameter slot indices, per element type.  Slot names are elegant's
  * parameter names (track_data.c tables cited per type). */
@@ -165,8 +165,11 @@ typedef struct {
   double coord_limit;      /* global_settings coord_limit (10 m) */
   double slope_limit;      /* global_settings slope_limit (1) */
   int32_t passes_per_launch; /* 0 = all passes of a step in one launch */
-  int32_t ring_variant;    /* ring-kernel occupancy variant: 0 = autotune on first use,
-                              1..B2E_RING_VARIANTS = fixed (all variants give identical results) */
+  int32_t ring_variant;    /* ring-kernel variant (occupancy target x warp barrier level):
+                              0 = autotune on first use, 1..B2E_RING_VARIANTS = fixed
+                              (all variants give identical results) */
+  int32_t record_history;  /* nonzero: keep per-instance, per-pass survivors, centroids and
+                              rms emittances (b2e_ensemble_history) */
 } b2e_run_options;
 
 typedef struct b2e_ctx b2e_ctx;
@@ -234,9 +237,14 @@ int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_t *offsets,
                       int32_t n_overrides);
 
 /* Per-instance diagnostics after each pass: survivors, centroids <x>, <y>,
- * and rms emittances ex, ey (rms_emittance, final_props.c:844).  Buffers
- * are host arrays of n_instances * n_passes values; any may be NULL. */
+ * and rms emittances ex, ey (rms_emittance, final_props.c:844).  Requires
+ * record_history in the run options and a lattice without CSR elements.
+ * Buffers are host arrays of n_instances * b2e_history_passes() values,
+ * instance-major; any may be NULL.  The record covers every pass tracked
+ * since the last b2e_upload_particles (b2e_track continuations append). */
 int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *cy, double *ex, double *ey);
+/* Passes recorded so far, or -1 for a null context. */
+int64_t b2e_history_passes(const b2e_ctx *ctx);
 
 /* ---- CSR (CSRCSBEND / CSRDRIFT) ---------------------------------------- */
 /* Wake arrays of every CSR kick of the last b2e_track call: for each

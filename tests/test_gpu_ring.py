@@ -130,15 +130,31 @@ def test_ensemble_matches_per_instance_reference(ref_b2e):
         assert_parity(sub, rows, nl)
 
 
-def test_kernel_variants_identical():
-    """Every occupancy variant the autotuner may pick gives identical results."""
+def _lossy_beam(n, seed):
+    rng = np.random.default_rng(seed)
+    c = np.zeros((n, 6))
+    c[:, 0] = rng.uniform(-0.022, 0.022, n)
+    c[:, 1] = rng.uniform(-3e-3, 3e-3, n)
+    c[:, 2] = rng.uniform(-0.015, 0.015, n)
+    c[:, 3] = rng.uniform(-2e-3, 2e-3, n)
+    c[:, 4] = rng.normal(0, 5e-3, n)
+    c[:, 5] = rng.uniform(-0.03, 0.03, n)
+    return Beam(c, np.arange(1, n + 1))
+
+
+@pytest.mark.parametrize("history", [False, True])
+def test_kernel_variants_identical(history):
+    """Every variant the autotuner may pick (occupancy target x warp barrier
+    level) gives identical coordinates and losses, with and without history."""
     lat = w.fodo_ring()
-    beam = w.ring_beam(400, seed=21)
+    beam = _lossy_beam(700, seed=21)
     ref = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=1)
-    for v in (2, 3, 4):
-        r = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=v)
-        assert np.array_equal(r.coords, ref.coords)
-        assert np.array_equal(r.lost_pass, ref.lost_pass)
+    assert (ref.lost_pass >= 0).any() and (ref.lost_pass < 0).any()
+    for v in range(1, 13):
+        r = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=v, record_history=history)
+        assert np.array_equal(r.coords, ref.coords), v
+        assert np.array_equal(r.lost_pass, ref.lost_pass), v
+        assert np.array_equal(r.lost_element, ref.lost_element), v
 
 
 def test_autotuner_picks_a_variant():
@@ -147,5 +163,59 @@ def test_autotuner_picks_a_variant():
     with Tracker(lat, w.ring_p_central(), 3) as t:
         t.track(beam)
         chosen, ms = t.ring_tuning()
-    assert 1 <= chosen <= 4
-    assert all(m > 0 for m in ms)
+    assert 1 <= chosen <= 12
+    assert len(ms) == 12 and all(m > 0 for m in ms)
+
+
+def _moments(coords, alive):
+    """Survivors, centroids and rms emittances as rms_emittance
+    (final_props.c:844-880) forms them: sqrt(<dx^2><dx'^2> - <dx dx'>^2)."""
+    c = coords[alive]
+    n = len(c)
+    if n == 0:
+        return n, 0.0, 0.0, 0.0, 0.0
+    m = c[:, :4].mean(axis=0)
+    d = c[:, :4] - m
+    ex = np.sqrt(max((d[:, 0] ** 2).mean() * (d[:, 1] ** 2).mean() - (d[:, 0] * d[:, 1]).mean() ** 2, 0.0))
+    ey = np.sqrt(max((d[:, 2] ** 2).mean() * (d[:, 3] ** 2).mean() - (d[:, 2] * d[:, 3]).mean() ** 2, 0.0))
+    return n, m[0], m[2], ex, ey
+
+
+def test_ensemble_history_matches_per_pass_moments():
+    """The per-pass history equals the moments of the coordinates downloaded
+    after each pass, per instance; recording it leaves the tracking unchanged."""
+    lat, beam, offsets, overrides = w.ensemble(n_instances=5, n_min=150, n_max=400, seed=9)
+    # instance 2 gets a large-amplitude beam so that it loses particles
+    lossy = _lossy_beam(int(offsets[3] - offsets[2]), seed=4)
+    beam.coords[offsets[2]:offsets[3]] = lossy.coords
+    passes = 6
+    with Tracker(lat, w.ring_p_central(), passes, record_history=True) as t:
+        t.load_ensemble(offsets, overrides)
+        res = t.track(beam)
+        hist = t.history()
+    assert hist["ex"].shape == (5, passes)
+    with Tracker(lat, w.ring_p_central(), passes) as t:
+        t.load_ensemble(offsets, overrides)
+        plain = t.track(beam)
+    assert np.array_equal(res.coords, plain.coords)
+    assert np.array_equal(res.lost_pass, plain.lost_pass)
+
+    with Tracker(lat, w.ring_p_central(), 1, record_history=True) as t:
+        t.load_ensemble(offsets, overrides)
+        t.upload(beam)
+        expected = np.zeros((5, passes, 5))
+        for j in range(passes):
+            t.continue_tracking()
+            r = t.download()
+            order = np.argsort(r.ids)
+            coords, lost = r.coords[order], r.lost_pass[order]
+            for i in range(5):
+                sl = slice(offsets[i], offsets[i + 1])
+                expected[i, j] = _moments(coords[sl], lost[sl] < 0)
+        stepped = t.history()
+    assert (expected[2, :, 0] < expected[2, 0, 0]).any() or expected[2, 0, 0] < offsets[3] - offsets[2]
+    for h in (hist, stepped):
+        assert np.array_equal(h["survivors"], expected[:, :, 0].astype(np.int64))
+        for k, col in (("cx", 1), ("cy", 2), ("ex", 3), ("ey", 4)):
+            np.testing.assert_allclose(h[k], expected[:, :, col], rtol=1e-10, atol=1e-18)
+    assert np.array_equal(stepped["ex"], hist["ex"])
