@@ -8,6 +8,7 @@ Usage: ``python -m elegant_b200.build`` (or ``build()`` from Python).
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -19,9 +20,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libelegant_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-SOURCES = ["b2e_ring.cu", "b2e_csr.cu", "b2e_lattice.cu", "b2e_capi.cu"]
+SOURCES = ["b2e_ring.cu", "b2e_csr.cu", "b2e_lattice.cu", "b2e_capi.cu", "b2e_tmap.cu", "b2e_wakenet.cu"]
 HEADERS = ["b2e_engine.h", "b2e_elements.cuh", "b2e_math.h", "b2e_kernels.h", "b2e_lattice.h",
-           "b2e_csr.h", "b2e_sg.h"]
+           "b2e_csr.h", "b2e_sg.h", "b2e_umma.cuh", "b2e_tmap.h"]
 
 # --fmad=false: no implicit multiply-add contraction, so every product and sum
 # rounds exactly where the reference's C expression rounds; the explicit fma()
@@ -49,7 +50,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     nvcc = nvcc_path()
     os.makedirs(BUILD_DIR, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "elegant_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
@@ -59,7 +60,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
+    # translation units compile independently
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), jobs)):
+            if r.returncode != 0:
+                sys.stderr.write((r.stdout or "") + (r.stderr or ""))
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB, objs):
         cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-cudart", "static", "-o", LIB, *objs]
         if verbose:

@@ -203,20 +203,26 @@ __device__ void sg_apply(const double *in, double *out, int nBins, const double 
   }
 }
 
-/* wake of one kick (csbend.c:2566-2673): one CTA */
-__global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, WakeArgs a) {
-  extern __shared__ double sm[];
+/* Wake of one kick (csbend.c:2566-2673) on one CTA, from a histogram of
+ * counts (unsigned counts in tracking, real-valued counts for batched
+ * profiles).  sm holds 4*nBins doubles.  Writes dgamma[nBins], the wake log
+ * when a.wakelog is set, the binned total when nbinned_out is set, and the
+ * smoothed density (per unit ct) and its derivative when hist_out/deriv_out
+ * are set. */
+template <typename CountT, typename SumT>
+__device__ void wake_body(const CountT *counts, const WakeArgs &a, const double dct, double *sm, double *dgamma,
+                          SumT *nbinned_out, double *hist_out, double *deriv_out) {
   const int nb = a.nBins;
   double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb, *tmp = sm + 3 * nb;
-  __shared__ long long nBinned;
+  __shared__ double nBinnedD;
   __shared__ int skip;
-  const double dct = st->dct;
   if (threadIdx.x == 0) {
-    long long s = 0;
+    SumT s = 0;
     for (int b = 0; b < nb; b++)
       s += counts[b];
-    nBinned = s;
-    st->nBinned = s;
+    nBinnedD = 1.0 * s;
+    if (nbinned_out)
+      *nbinned_out = s;
     skip = 0;
   }
   for (int b = threadIdx.x; b < nb; b += blockDim.x)
@@ -236,7 +242,7 @@ __global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, Wak
       if (!sum)
         skip = 1;
       else
-        deriv[0] = (1.0 * nBinned) / sum; /* factor, parked in deriv[0] */
+        deriv[0] = nBinnedD / sum; /* factor, parked in deriv[0] */
     }
     __syncthreads();
     const double factor = deriv[0];
@@ -254,8 +260,13 @@ __global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, Wak
   __syncthreads();
   sg_apply(deriv, tmp, nb, a.sgd_w, a.sgd_lo, a.sgd_n);
   __syncthreads();
-  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     deriv[b] = tmp[b];
+    if (hist_out)
+      hist_out[b] = hist[b];
+    if (deriv_out)
+      deriv_out[b] = tmp[b];
+  }
   __syncthreads();
   /* bins of slippage; clamped to [0, nb] so indexing stays in bounds for a
    * degenerate bin size (the comparisons below give the same result) */
@@ -264,7 +275,7 @@ __global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, Wak
   diS4 = diS4 < 0 ? 0 : (diS4 > nb ? nb : diS4);
   if (!(dct > 0)) {
     for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
-      st->dGamma[ib] = 0;
+      dgamma[ib] = 0;
       if (a.wakelog)
         a.wakelog[ib] = 0;
     }
@@ -311,10 +322,34 @@ __global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, Wak
       T2 *= a.c2;
     }
     double dg = T1 + T2;
-    st->dGamma[ib] = dg;
+    dgamma[ib] = dg;
     if (a.wakelog)
       a.wakelog[ib] = dg;
   }
+}
+
+/* wake of one kick of a tracked bunch */
+__global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, WakeArgs a) {
+  extern __shared__ double sm[];
+  wake_body<unsigned int, long long>(counts, a, st->dct, sm, st->dGamma, &st->nBinned, nullptr, nullptr);
+}
+
+/* Batched wake integral of many profiles in bin units (dct = 1), one CTA per
+ * profile: out = T1 (c1 = 1, no T2 term) for the profile's slippage in bins;
+ * hist_out/deriv_out receive the smoothed density and its derivative. */
+__global__ void wake_batch_kernel(const double *counts, const double *slippage_bins, WakeArgs a, double *t1_out,
+                                  double *hist_out, double *deriv_out) {
+  extern __shared__ double sm[];
+  const size_t off = (size_t)blockIdx.x * a.nBins;
+  WakeArgs w = a;
+  w.slippage = slippage_bins[blockIdx.x];
+  w.slippage13 = 1;
+  w.c1 = 1;
+  w.c2 = 0;
+  w.csr_constant = 1;
+  w.wakelog = nullptr;
+  wake_body<double, double>(counts + off, w, 1.0, sm, t1_out + off, (double *)nullptr, hist_out + off,
+                            deriv_out + off);
 }
 
 /* after the last kick: its wake kick and the min/max for the exit binning */
@@ -1031,4 +1066,70 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   STATIC_TRY(cudaGetLastError());
   STATIC_TRY(launch_post_element_sweep(P, n, nullptr, 0, 0, s));
   return B2E_OK;
+}
+
+/* Batched wake integral for the wake-network data set: n_profiles histograms
+ * of `bins` real-valued counts, each with its own slippage in bins. */
+using b2e::WakeArgs;
+using b2e::static_sg_weights_kernel;
+using b2e::wake_batch_kernel;
+extern "C" int b2e_csr_wake_batch(const double *dev_counts, const double *dev_slippage_bins, int32_t n_profiles,
+                                  int32_t bins, int32_t sg_halfwidth, int32_t sg_order, int32_t sgd_halfwidth,
+                                  int32_t sgd_order, int32_t trapezoid, int32_t steady, double *dev_t1,
+                                  double *dev_density, double *dev_derivative, void *stream) {
+  if (!dev_counts || !dev_slippage_bins || !dev_t1 || !dev_density || !dev_derivative || n_profiles < 0 ||
+      bins < 2 || bins > B2E_CSR_MAX_BINS)
+    return B2E_ERR_ARG;
+  if (sgd_halfwidth <= 0)
+    sgd_halfwidth = sg_halfwidth;
+  if (sgd_halfwidth <= 0)
+    sgd_halfwidth = 1;
+  if (sgd_order <= 0)
+    sgd_order = sg_order;
+  if (sgd_order <= 0)
+    sgd_order = 1;
+  if (2 * std::max(sg_halfwidth, sgd_halfwidth) + 1 > B2E_SG_MAX_WIDTH)
+    return B2E_ERR_ARG;
+  if (n_profiles == 0)
+    return B2E_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *w = nullptr;
+  int *idx = nullptr;
+  if (cudaMallocAsync((void **)&w, sizeof(double) * 2 * bins * B2E_SG_MAX_WIDTH, s) != cudaSuccess)
+    return B2E_ERR_NOMEM;
+  if (cudaMallocAsync((void **)&idx, sizeof(int) * 4 * bins, s) != cudaSuccess) {
+    cudaFreeAsync(w, s);
+    return B2E_ERR_NOMEM;
+  }
+  static_sg_weights_kernel<<<(2 * bins + 127) / 128, 128, 0, s>>>(bins, sg_halfwidth, sg_order, sgd_halfwidth,
+                                                                  sgd_order, w, idx);
+  WakeArgs a;
+  a.nBins = bins;
+  a.sgHalf = sg_halfwidth;
+  a.sgdHalf = sgd_halfwidth;
+  a.trapz = trapezoid != 0;
+  a.steady = steady != 0;
+  a.correct = sg_halfwidth > 0;
+  a.sg_w = w;
+  a.sgd_w = w + (size_t)bins * B2E_SG_MAX_WIDTH;
+  a.sg_lo = idx;
+  a.sg_n = idx + 1;
+  a.sgd_lo = idx + 2 * bins;
+  a.sgd_n = idx + 2 * bins + 1;
+  a.slippage = 0;
+  a.slippage13 = 1;
+  a.c1 = 1;
+  a.c2 = 0;
+  a.csr_constant = 1;
+  a.wakelog = nullptr;
+  const size_t smem = sizeof(double) * 4 * bins;
+  cudaError_t e = cudaFuncSetAttribute(wake_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    wake_batch_kernel<<<n_profiles, 512, smem, s>>>(dev_counts, dev_slippage_bins, a, dev_t1, dev_density,
+                                                    dev_derivative);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(w, s);
+  cudaFreeAsync(idx, s);
+  return e == cudaSuccess ? B2E_OK : B2E_ERR_CUDA;
 }

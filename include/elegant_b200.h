@@ -251,6 +251,59 @@ int64_t b2e_history_passes(const b2e_ctx *ctx);
  * CSRCSBEND kick, BINS values of dGamma (csbend.c:2673) in kick order. */
 int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written);
 
+/* ---- batched wake integral (wake-network data) ------------------------
+ * For each of n_profiles histograms (dev_counts: [n_profiles][bins] real
+ * counts, bin width 1) the CSRCSBEND wake pipeline of one kick
+ * (csbend.c:2566-2673: Savitzky-Golay smoothing, correctDistribution,
+ * derivative filter, transient or steady-state integral) with the slippage
+ * dev_slippage_bins[p] in bins.  Outputs, all [n_profiles][bins] FP64:
+ * dev_t1 = the integral term T1 alone (CSR constant 1, no T2 term),
+ * dev_density = the smoothed density, dev_derivative = its derivative.  The
+ * wake of a kick with bin width dct is then
+ *   CSRConstant * L / N_KICKS * dct^(-4/3) * (T1 - (hist[i+diS] - hist[i+diS4]) / s^(1/3)).
+ * No counterpart in the reference (it evaluates one wake per kick). */
+int b2e_csr_wake_batch(const double *dev_counts, const double *dev_slippage_bins, int32_t n_profiles, int32_t bins,
+                       int32_t sg_halfwidth, int32_t sg_order, int32_t sgd_halfwidth, int32_t sgd_order,
+                       int32_t trapezoid, int32_t steady, double *dev_t1, double *dev_density, double *dev_derivative,
+                       void *stream);
+
+/* ---- wake network (learned CSR wake integral) --------------------------
+ * A 6-layer 1-D convolutional network (64 channels, 5 taps, per-layer
+ * dilations, GELU) that maps a binned profile -- smoothed density, its
+ * derivative and a slippage code, [n][3][bins] FP32 on the device -- to the
+ * wake integral T1 of b2e_csr_wake_batch, [n][bins] FP32, in the scaled units
+ * the caller trains it in.  BF16 weights and activations, FP32 accumulation
+ * on the tensor cores; the optimiser is Adam on FP32 master weights.
+ * Parameters are a flat FP32 array of b2e_wakenet_param_count() values:
+ * weights [layer][tap][out][in] (6 x 5 x 64 x 64), then biases [layer][64].
+ * The reference has no learned component; this is an addition. */
+typedef struct b2e_wakenet b2e_wakenet;
+int b2e_wakenet_create(b2e_wakenet **out, int32_t bins, int32_t max_batch, const int32_t *dilations, int32_t device);
+int b2e_wakenet_destroy(b2e_wakenet *net);
+const char *b2e_wakenet_last_error(const b2e_wakenet *net);
+int64_t b2e_wakenet_param_count(void);
+/* Replaces the parameters (and resets the optimiser state). */
+int b2e_wakenet_set_params(b2e_wakenet *net, const float *host_params);
+/* Copies parameters and/or the last gradients (either may be NULL). */
+int b2e_wakenet_get_params(b2e_wakenet *net, float *host_params, float *host_grads);
+/* Inference: dev_out[n][bins] from dev_inputs[n][3][bins]. */
+int b2e_wakenet_forward(b2e_wakenet *net, const float *dev_inputs, int32_t n, float *dev_out, void *stream);
+/* Forward + backward of the mean squared error against dev_targets[n][bins];
+ * gradients are kept for b2e_wakenet_get_params; *loss (host, may be NULL). */
+int b2e_wakenet_gradients(b2e_wakenet *net, const float *dev_inputs, const float *dev_targets, int32_t n,
+                          double *loss, void *stream);
+/* One Adam step (learning rate lr) on one batch; *loss as above (NULL skips
+ * the host synchronisation). */
+int b2e_wakenet_train_step(b2e_wakenet *net, const float *dev_inputs, const float *dev_targets, int32_t n, float lr,
+                           double *loss, void *stream);
+
+/* ---- tensor-core self-test ---------------------------------------------
+ * Runs one UMMA tile on device buffers to check the operand layouts the wake
+ * network uses.  mode 0: D[128][64] = A[128][64] . B[64][64]^T; mode 1:
+ * D[m][n] = sum_k A[m/64][k][m%64] * B[k][n] with A [2][128][64], B [128][64].
+ * A, B: BF16 row-major; D: FP32.  No counterpart in the reference. */
+int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b, float *dev_d, void *stream);
+
 /* ---- allocation-free CSR dipole ---------------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory when they track (a program whose memory pool owns

@@ -1379,3 +1379,91 @@ double b2e_oracle_sin(double x) { return M_SIN(x); }
 double b2e_oracle_cos(double x) { return M_COS(x); }
 double b2e_oracle_tan(double x) { return M_TAN(x); }
 double b2e_oracle_asin(double x) { return M_ASIN(x); }
+
+/* Wake integral of one histogram in bin units (dct = 1) with the CSR
+ * constant, length and kick count folded to 1 and no T2 term: the T1 part of
+ * the CSRCSBEND kick wake above (csbend.c:2566-2673), for the wake network's
+ * data set.  counts are real-valued; their sum plays nBinned. */
+void b2e_oracle_wake_t1(const double *counts, long nBins, double slippage_bins, int sgHalf, int sgOrder, int sgdHalf,
+                        int sgdOrder, int trapz, int steady, double *T1, double *hist_out, double *deriv_out) {
+  double *ctHist = malloc(sizeof(double) * nBins), *ctHistDeriv = malloc(sizeof(double) * nBins),
+         *denom = malloc(sizeof(double) * nBins);
+  double nBinned = 0, dct = 1;
+  long ib, jb, diS;
+  if (sgdHalf <= 0)
+    sgdHalf = sgHalf;
+  if (sgdHalf <= 0)
+    sgdHalf = 1;
+  if (sgdOrder <= 0)
+    sgdOrder = sgOrder;
+  if (sgdOrder <= 0)
+    sgdOrder = 1;
+  for (ib = 0; ib < nBins; ib++) {
+    ctHist[ib] = counts[ib];
+    nBinned += counts[ib];
+  }
+  if (sgHalf > 0) {
+    double sum = 0, factor;
+    b2e_sg_apply_host(ctHist, nBins, sgOrder, sgHalf, sgHalf, 0);
+    for (ib = 0; ib < nBins; ib++) {
+      if (ctHist[ib] < 0)
+        ctHist[ib] = 0;
+      sum += ctHist[ib];
+    }
+    if (sum) {
+      factor = 1.0 * nBinned / sum;
+      for (ib = 0; ib < nBins; ib++)
+        ctHist[ib] *= factor;
+    }
+  }
+  for (ib = 0; ib < nBins; ib++) {
+    denom[ib] = M_POW13(dct * ib);
+    ctHistDeriv[ib] = (ctHist[ib] /= dct);
+  }
+  b2e_sg_apply_host(ctHistDeriv, nBins, sgdOrder, sgdHalf, sgdHalf, 1);
+  diS = (long)(slippage_bins / dct);
+  for (ib = 0; ib < nBins; ib++) {
+    double term1 = 0, term2 = 0;
+    long count;
+    T1[ib] = 0;
+    if (steady) {
+      if (!trapz) {
+        for (jb = ib + 1; jb < nBins; jb++)
+          T1[ib] += ctHistDeriv[jb] / denom[jb - ib];
+      } else {
+        if ((jb = ib + 1) < nBins)
+          term1 = ctHistDeriv[jb] / denom[jb - ib];
+        for (count = 0, jb = ib + 1; jb < nBins; jb++, count++)
+          T1[ib] += (term2 = ctHistDeriv[jb] / denom[jb - ib]);
+        if ((ib + 1) < nBins)
+          T1[ib] += 0.3 * SQR(denom[1]) * (2 * ctHistDeriv[ib + 1] + 3 * ctHistDeriv[ib]) / dct;
+        if (count > 1)
+          T1[ib] -= (term1 + term2) / 2;
+      }
+    } else {
+      if (!trapz) {
+        for (jb = ib + 1; jb <= (ib + diS) && jb < nBins; jb++)
+          T1[ib] += ctHistDeriv[jb] / denom[jb - ib];
+      } else {
+        if ((jb = ib + 1) < nBins && jb <= (ib + diS))
+          term1 = ctHistDeriv[jb] / denom[jb - ib] / 2;
+        for (count = 0, jb = ib + 1; jb <= (ib + diS) && jb < nBins; count++, jb++)
+          T1[ib] += (term2 = ctHistDeriv[jb] / denom[jb - ib]);
+        if (diS > 0 && (ib + 1) < nBins)
+          T1[ib] += 0.3 * SQR(denom[1]) * (2 * ctHistDeriv[ib + 1] + 3 * ctHistDeriv[ib]) / dct;
+        if (count > 1)
+          T1[ib] -= (term1 + term2) / 2;
+      }
+    }
+    T1[ib] *= 1.0;
+  }
+  for (ib = 0; ib < nBins; ib++) {
+    if (hist_out)
+      hist_out[ib] = ctHist[ib];
+    if (deriv_out)
+      deriv_out[ib] = ctHistDeriv[ib];
+  }
+  free(ctHist);
+  free(ctHistDeriv);
+  free(denom);
+}

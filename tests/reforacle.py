@@ -97,6 +97,20 @@ class PortOracle:
             fn.argtypes = [ctypes.c_double]
         self.math = math
 
+    def wake_t1(self, counts, slippage_bins, sg_half=0, sg_order=1, sgd_half=0, sgd_order=0, trapz=True,
+                steady=False):
+        """T1 wake integral of one histogram in bin units: (t1, density, derivative)."""
+        c = np.ascontiguousarray(counts, dtype=np.float64)
+        nb = c.size
+        t1, h, d = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        dp = ctypes.POINTER(ctypes.c_double)
+        f = self.lib.b2e_oracle_wake_t1
+        f.restype = None
+        f.argtypes = [dp, ctypes.c_long, ctypes.c_double] + [ctypes.c_int] * 6 + [dp, dp, dp]
+        f(c.ctypes.data_as(dp), nb, float(slippage_bins), sg_half, sg_order, sgd_half, sgd_order, int(trapz),
+          int(steady), t1.ctypes.data_as(dp), h.ctypes.data_as(dp), d.ctypes.data_as(dp))
+        return t1, h, d
+
     def track(self, lattice, coords, ids, p_central, n_passes, default_order=2, capture_wakes=False):
         """Returns (rows, n_left, effort) like RefOracle.track, plus the per-kick
         CSR wakes as a fourth item when capture_wakes is set."""

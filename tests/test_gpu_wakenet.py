@@ -1,0 +1,148 @@
+"""Tensor-core (tcgen05/UMMA) kernels of the wake network on the GPU."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from elegant_b200 import _native as nat
+    lib = nat.load_library()
+    lib.b2e_umma_selftest.restype = ctypes.c_int
+    lib.b2e_umma_selftest.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+    return lib
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_umma_operand_layouts(mode):
+    import torch
+    lib = _lib()
+    g = torch.Generator().manual_seed(3 + mode)
+    if mode == 0:
+        a = torch.randn(128, 64, generator=g).to(torch.bfloat16)
+        b = torch.randn(64, 64, generator=g).to(torch.bfloat16)
+        ref = a.double() @ b.double().T
+    else:
+        a = torch.randn(2, 128, 64, generator=g).to(torch.bfloat16)
+        b = torch.randn(128, 64, generator=g).to(torch.bfloat16)
+        at = torch.cat([a[0].double().T, a[1].double().T], dim=0)  # [128 m][128 k]
+        ref = at @ b.double()
+    da, db = a.cuda(), b.cuda()
+    d = torch.full((128, 64), float("nan"), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.b2e_umma_selftest(mode, da.data_ptr(), db.data_ptr(), d.data_ptr(), stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    out = d.cpu().double()
+    err = (out - ref).abs().max().item()
+    assert err < 1e-3 * ref.abs().max().item(), err
+
+
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def _profiles(n, nb, seed):
+    rng = np.random.default_rng(seed)
+    i = np.arange(nb)
+    out = np.zeros((n, nb))
+    for p in range(n):
+        for _ in range(rng.integers(1, 5)):
+            c, s, w = rng.uniform(0.2, 0.8) * nb, rng.uniform(0.01, 0.1) * nb, rng.uniform(0.2, 1)
+            out[p] += w * np.exp(-0.5 * ((i - c) / s) ** 2)
+        out[p] *= 1e5 / out[p].sum()
+        out[p] += rng.normal(0, 1, nb) * np.sqrt(out[p] + 1)
+        out[p] = np.maximum(out[p], 0)
+    return out
+
+
+@pytest.mark.parametrize("sg,trapz,steady", [(2, True, False), (0, True, False), (3, False, False), (2, True, True)])
+def test_wake_batch_matches_oracle_bit_exact(sg, trapz, steady):
+    import torch
+    from elegant_b200.wakenet import library
+    from reforacle import PortOracle
+    lib, o = library(), PortOracle("b2e")
+    nb, n = 600, 6
+    counts = _profiles(n, nb, seed=sg + 7 * trapz)
+    slip = np.array([0.3, 1.0, 2.7, 35.5, 400.0, 5000.0])
+    dc, ds = torch.tensor(counts, device="cuda"), torch.tensor(slip, device="cuda")
+    t1, h, d = (torch.empty((n, nb), dtype=torch.float64, device="cuda") for _ in range(3))
+    rc = lib.b2e_csr_wake_batch(dc.data_ptr(), ds.data_ptr(), n, nb, sg, 1, 0, 0, int(trapz), int(steady),
+                                t1.data_ptr(), h.data_ptr(), d.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    for p in range(n):
+        rt1, rh, rd = o.wake_t1(counts[p], slip[p], sg_half=sg, sg_order=1, trapz=trapz, steady=steady)
+        assert np.array_equal(h[p].cpu().numpy(), rh)
+        assert np.array_equal(d[p].cpu().numpy(), rd)
+        assert np.array_equal(t1[p].cpu().numpy(), rt1), p
+
+
+def _net_case(seed, n=3, L=256):
+    import wakenet_oracle as wo
+    rng = np.random.default_rng(seed)
+    params = wo.init_params(seed, out_scale=1.0)
+    params[wo.LAYERS * wo.WSIZE:] = rng.normal(0, 0.05, wo.LAYERS * wo.CH).astype(np.float32)
+    params[wo.LAYERS * wo.WSIZE + 5 * 64 + 1:] = 0  # output channels 1..63 are not live
+    inputs = rng.normal(0, 1, (n, 3, L)).astype(np.float32)
+    targets = rng.normal(0, 1, (n, L)).astype(np.float32)
+    return params, inputs, targets
+
+
+def test_wakenet_forward_matches_oracle():
+    import torch
+    import wakenet_oracle as wo
+    from elegant_b200.wakenet import WakeNet
+    params, inputs, _ = _net_case(1)
+    with WakeNet(bins=256, max_batch=4) as net:
+        net.set_params(params)
+        y = net.forward(torch.tensor(inputs, device="cuda")).cpu().numpy().astype(np.float64)
+    ref, _ = wo.forward(params, inputs, net.dilations)
+    rel = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    assert rel < 1e-2, rel
+
+
+def test_wakenet_gradients_match_oracle():
+    import torch
+    import wakenet_oracle as wo
+    from elegant_b200.wakenet import WakeNet
+    params, inputs, targets = _net_case(2)
+    with WakeNet(bins=256, max_batch=4) as net:
+        net.set_params(params)
+        loss = net.gradients(torch.tensor(inputs, device="cuda"), torch.tensor(targets, device="cuda"))
+        g = net.grads().astype(np.float64)
+    ref_loss, ref = wo.loss_and_gradients(params, inputs, targets, net.dilations)
+    assert abs(loss - ref_loss) < 1e-2 * ref_loss
+    for l in range(wo.LAYERS):
+        sl = slice(l * wo.WSIZE, (l + 1) * wo.WSIZE)
+        a, b = g[sl], ref[sl]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel < 3e-2, (l, rel)
+    gb, rb = g[wo.LAYERS * wo.WSIZE:], ref[wo.LAYERS * wo.WSIZE:]
+    assert np.linalg.norm(gb - rb) / np.linalg.norm(rb) < 3e-2
+
+
+def test_wakenet_training_reduces_loss():
+    import torch
+    import wakenet_oracle as wo
+    from elegant_b200.wakenet import WakeNet
+    rng = np.random.default_rng(4)
+    L, n = 256, 8
+    x = rng.normal(0, 1, (n, 3, L)).astype(np.float32)
+    # a fixed linear target: a smoothed, shifted copy of channel 1
+    k = np.exp(-0.5 * (np.arange(-8, 9) / 3.0) ** 2)
+    tgt = np.stack([np.convolve(x[p, 1], k / k.sum(), mode="same") for p in range(n)]).astype(np.float32)
+    with WakeNet(bins=L, max_batch=n) as net:
+        net.set_params(wo.init_params(3))
+        xi, ti = torch.tensor(x, device="cuda"), torch.tensor(tgt, device="cuda")
+        first = net.train_step(xi, ti, 1e-3, want_loss=True)
+        for _ in range(150):
+            net.train_step(xi, ti, 1e-3)
+        last = net.train_step(xi, ti, 1e-3, want_loss=True)
+    assert last < 0.2 * first, (first, last)
