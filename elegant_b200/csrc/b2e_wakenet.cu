@@ -11,8 +11,8 @@
  * by the TMA unit.
  *
  * Layers: 6 convolutions of 64 channels, 5 taps, dilations set per layer,
- * GELU between them.  The input has 3 live channels (density, derivative,
- * slippage code) and the output 1 live channel; both are carried in 64-wide
+ * GELU between them.  The input has 4 live channels (density, derivative,
+ * slippage code, density shifted by the slippage) and the output 1 live channel; both are carried in 64-wide
  * tensors with zero channels, so every layer runs the same kernels.
  */
 #include <cuda_bf16.h>
@@ -501,15 +501,15 @@ extern "C" int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b,
 /* ======================================================== network context */
 namespace b2e {
 
-/* inputs [n][3][L] FP32 -> X0 [n][L][64] BF16 (channels 3..63 zero) */
+/* inputs [n][WN_IN][L] FP32 -> X0 [n][L][64] BF16 (channels WN_IN..63 zero) */
 __global__ void wn_pack_kernel(const float *in, int L, int64_t rows, __nv_bfloat16 *x0) {
   const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (r >= rows)
     return;
   const int64_t p = r / L, i = r - p * L;
-  const float *src = in + p * 3 * L + i;
+  const float *src = in + p * WN_IN * L + i;
   uint4 *dst = reinterpret_cast<uint4 *>(x0 + r * 64);
-  dst[0] = make_uint4(pack_bf16(src[0], src[L]), pack_bf16(src[2 * L], 0.f), 0u, 0u);
+  dst[0] = make_uint4(pack_bf16(src[0], src[L]), pack_bf16(src[2 * L], src[3 * L]), 0u, 0u);
   for (int c = 1; c < 8; c++)
     dst[c] = make_uint4(0u, 0u, 0u, 0u);
 }

@@ -14,7 +14,7 @@ namespace b2e {
 constexpr int WN_LAYERS = 6;
 constexpr int WN_CH = 64;
 constexpr int WN_TAPS = 5;
-constexpr int WN_IN = 3;                                   /* density, derivative, slippage code */
+constexpr int WN_IN = 4; /* density, derivative, slippage code, density shifted by the slippage */
 constexpr int WN_WSIZE = WN_TAPS * WN_CH * WN_CH;          /* weights of one layer */
 constexpr int WN_NPARAM = WN_LAYERS * (WN_WSIZE + WN_CH);  /* weights then biases */
 constexpr int WN_STAGES = 4;                               /* operand stages of the conv kernel */

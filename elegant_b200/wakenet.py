@@ -14,7 +14,26 @@ from . import _native as nat
 
 DILATIONS = (1, 3, 9, 27, 81, 243)
 LAYERS, CH, TAPS = 6, 64, 5
+IN_CH = 4  # density, derivative, slippage code, density shifted by the slippage
 WSIZE = TAPS * CH * CH
+
+
+def init_params(seed: int, out_scale: float = 0.1) -> np.ndarray:
+    """He-style initialisation of the flat parameter array: weights
+    N(0, 2/fan_in) with fan_in counted over live input channels (3 for the
+    first layer: IN_CH); only output channel 0 of the last layer live, scaled by
+    out_scale; biases zero."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = np.zeros((LAYERS, TAPS, CH, CH))
+    for l in range(LAYERS):
+        std = np.sqrt(2.0 / (TAPS * (IN_CH if l == 0 else CH)))
+        if l == 0:
+            w[l, :, :, :IN_CH] = rng.normal(0, std, (TAPS, CH, IN_CH))
+        elif l == LAYERS - 1:
+            w[l, :, 0, :] = rng.normal(0, std * out_scale, (TAPS, CH))
+        else:
+            w[l] = rng.normal(0, std, (TAPS, CH, CH))
+    return np.concatenate([w.ravel(), np.zeros(LAYERS * CH)]).astype(np.float32)
 
 
 def _bind(lib):
@@ -104,10 +123,10 @@ class WakeNet:
         return (stream or torch.cuda.current_stream()).cuda_stream
 
     def forward(self, inputs, out=None, stream=None):
-        """inputs: float32 CUDA tensor [n][3][bins] -> [n][bins]."""
+        """inputs: float32 CUDA tensor [n][IN_CH][bins] -> [n][bins]."""
         import torch
         n = inputs.shape[0]
-        assert inputs.is_contiguous() and inputs.dtype == torch.float32 and inputs.shape[1:] == (3, self.bins)
+        assert inputs.is_contiguous() and inputs.dtype == torch.float32 and inputs.shape[1:] == (IN_CH, self.bins)
         if out is None:
             out = torch.empty((n, self.bins), dtype=torch.float32, device=inputs.device)
         for s in range(0, n, self.max_batch):

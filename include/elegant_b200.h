@@ -270,7 +270,8 @@ int b2e_csr_wake_batch(const double *dev_counts, const double *dev_slippage_bins
 /* ---- wake network (learned CSR wake integral) --------------------------
  * A 6-layer 1-D convolutional network (64 channels, 5 taps, per-layer
  * dilations, GELU) that maps a binned profile -- smoothed density, its
- * derivative and a slippage code, [n][3][bins] FP32 on the device -- to the
+ * derivative, a slippage code and the density shifted by the slippage,
+ * [n][4][bins] FP32 on the device -- to the
  * wake integral T1 of b2e_csr_wake_batch, [n][bins] FP32, in the scaled units
  * the caller trains it in.  BF16 weights and activations, FP32 accumulation
  * on the tensor cores; the optimiser is Adam on FP32 master weights.
@@ -286,7 +287,7 @@ int64_t b2e_wakenet_param_count(void);
 int b2e_wakenet_set_params(b2e_wakenet *net, const float *host_params);
 /* Copies parameters and/or the last gradients (either may be NULL). */
 int b2e_wakenet_get_params(b2e_wakenet *net, float *host_params, float *host_grads);
-/* Inference: dev_out[n][bins] from dev_inputs[n][3][bins]. */
+/* Inference: dev_out[n][bins] from dev_inputs[n][4][bins]. */
 int b2e_wakenet_forward(b2e_wakenet *net, const float *dev_inputs, int32_t n, float *dev_out, void *stream);
 /* Forward + backward of the mean squared error against dev_targets[n][bins];
  * gradients are kept for b2e_wakenet_get_params; *loss (host, may be NULL). */

@@ -74,10 +74,10 @@ def conv_t(g, w, d):
 
 
 def pack(inputs: np.ndarray, use_bf16: bool) -> np.ndarray:
-    """inputs [n][3][L] -> [n][L][64] with channels 3..63 zero."""
-    n, _, L = inputs.shape
+    """inputs [n][c][L] -> [n][L][64] with channels c..63 zero."""
+    n, c, L = inputs.shape
     x = np.zeros((n, L, CH))
-    x[:, :, :3] = np.transpose(inputs, (0, 2, 1))
+    x[:, :, :c] = np.transpose(inputs, (0, 2, 1))
     return bf16(x) if use_bf16 else x
 
 
@@ -118,21 +118,3 @@ def loss_and_gradients(params, inputs, targets, dilations, use_bf16=True):
             g = da * gelu_grad(zs[l - 1])
             dz = bf16(g) if use_bf16 else g
     return loss, np.concatenate([gw.ravel(), gb.ravel()])
-
-
-def init_params(seed: int, out_scale: float = 0.1) -> np.ndarray:
-    """He-style initialisation: weights N(0, 2/fan_in) with fan_in counted over
-    live input channels (3 for the first layer); output layer scaled by
-    out_scale and only output channel 0 live; biases zero."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    w = np.zeros((LAYERS, TAPS, CH, CH))
-    for l in range(LAYERS):
-        fan_in = TAPS * (3 if l == 0 else CH)
-        std = np.sqrt(2.0 / fan_in)
-        if l == 0:
-            w[l, :, :, :3] = rng.normal(0, std, (TAPS, CH, 3))
-        elif l == LAYERS - 1:
-            w[l, :, 0, :] = rng.normal(0, std * out_scale, (TAPS, CH))
-        else:
-            w[l] = rng.normal(0, std, (TAPS, CH, CH))
-    return np.concatenate([w.ravel(), np.zeros(LAYERS * CH)]).astype(np.float32)

@@ -86,11 +86,12 @@ def test_wake_batch_matches_oracle_bit_exact(sg, trapz, steady):
 
 def _net_case(seed, n=3, L=256):
     import wakenet_oracle as wo
+    from elegant_b200.wakenet import init_params
     rng = np.random.default_rng(seed)
-    params = wo.init_params(seed, out_scale=1.0)
+    params = init_params(seed, out_scale=1.0)
     params[wo.LAYERS * wo.WSIZE:] = rng.normal(0, 0.05, wo.LAYERS * wo.CH).astype(np.float32)
     params[wo.LAYERS * wo.WSIZE + 5 * 64 + 1:] = 0  # output channels 1..63 are not live
-    inputs = rng.normal(0, 1, (n, 3, L)).astype(np.float32)
+    inputs = rng.normal(0, 1, (n, 4, L)).astype(np.float32)
     targets = rng.normal(0, 1, (n, L)).astype(np.float32)
     return params, inputs, targets
 
@@ -98,6 +99,7 @@ def _net_case(seed, n=3, L=256):
 def test_wakenet_forward_matches_oracle():
     import torch
     import wakenet_oracle as wo
+    from elegant_b200.wakenet import init_params
     from elegant_b200.wakenet import WakeNet
     params, inputs, _ = _net_case(1)
     with WakeNet(bins=256, max_batch=4) as net:
@@ -111,6 +113,7 @@ def test_wakenet_forward_matches_oracle():
 def test_wakenet_gradients_match_oracle():
     import torch
     import wakenet_oracle as wo
+    from elegant_b200.wakenet import init_params
     from elegant_b200.wakenet import WakeNet
     params, inputs, targets = _net_case(2)
     with WakeNet(bins=256, max_batch=4) as net:
@@ -131,15 +134,16 @@ def test_wakenet_gradients_match_oracle():
 def test_wakenet_training_reduces_loss():
     import torch
     import wakenet_oracle as wo
+    from elegant_b200.wakenet import init_params
     from elegant_b200.wakenet import WakeNet
     rng = np.random.default_rng(4)
     L, n = 256, 8
-    x = rng.normal(0, 1, (n, 3, L)).astype(np.float32)
+    x = rng.normal(0, 1, (n, 4, L)).astype(np.float32)
     # a fixed linear target: a smoothed, shifted copy of channel 1
     k = np.exp(-0.5 * (np.arange(-8, 9) / 3.0) ** 2)
     tgt = np.stack([np.convolve(x[p, 1], k / k.sum(), mode="same") for p in range(n)]).astype(np.float32)
     with WakeNet(bins=L, max_batch=n) as net:
-        net.set_params(wo.init_params(3))
+        net.set_params(init_params(3))
         xi, ti = torch.tensor(x, device="cuda"), torch.tensor(tgt, device="cuda")
         first = net.train_step(xi, ti, 1e-3, want_loss=True)
         for _ in range(150):

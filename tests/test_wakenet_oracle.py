@@ -9,6 +9,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import wakenet_oracle as wo  # noqa: E402
+from elegant_b200.wakenet import init_params  # noqa: E402
 
 
 def test_bf16_rounding_matches_torch():
@@ -21,9 +22,9 @@ def test_bf16_rounding_matches_torch():
 def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(5)
     dil = (1, 2, 3, 1, 2, 1)
-    params = wo.init_params(11, out_scale=1.0).astype(np.float64)
+    params = init_params(11, out_scale=1.0).astype(np.float64)
     params[wo.LAYERS * wo.WSIZE:] = rng.normal(0, 0.1, wo.LAYERS * wo.CH)
-    inputs = rng.normal(0, 1, (2, 3, 24))
+    inputs = rng.normal(0, 1, (2, 4, 24))
     targets = rng.normal(0, 1, (2, 24))
     loss, g = wo.loss_and_gradients(params, inputs, targets, dil, use_bf16=False)
     w_idx = [l * wo.WSIZE + (t * 64 + co) * 64 + ci for l, t, co, ci in
