@@ -259,8 +259,6 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: bad arguments");
   if (!ctx->lattice_loaded)
     return fail(ctx, B2E_ERR_STATE, "b2e_load_ensemble: load a lattice first");
-  if (!ctx->lat.csr_elements.empty())
-    return fail(ctx, B2E_ERR_LATTICE, "b2e_load_ensemble: CSR elements are not supported in ring ensembles");
   for (int i = 0; i < n_instances; i++)
     if (offsets[i + 1] < offsets[i] || offsets[0] != 0)
       return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: offsets must start at 0 and be nondecreasing");
@@ -269,6 +267,12 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     if (overrides[k].element < 0 || overrides[k].element >= ne || overrides[k].slot < 0 ||
         overrides[k].slot >= B2E_MAX_PARAMS || !overrides[k].values)
       return fail(ctx, B2E_ERR_ARG, "b2e_load_ensemble: override %d out of range", k);
+  for (int k = 0; k < n_overrides; k++) {
+    const int t = ctx->base[overrides[k].element].type;
+    if (t == B2E_CSRCSBEND || t == B2E_CSRDRIFT)
+      return fail(ctx, B2E_ERR_LATTICE,
+                  "b2e_load_ensemble: CSR elements are shared by all bunches and take no per-instance overrides");
+  }
   ctx->n_inst = n_instances;
   ctx->inst_offsets.assign(offsets, offsets + n_instances + 1);
   ctx->elems_all.clear();
@@ -286,7 +290,12 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     ctx->aps_all.insert(ctx->aps_all.end(), cl.aps.begin(), cl.aps.end());
   }
   build_tiles(ctx);
-  return upload_lattice_tables(ctx);
+  int rc = upload_lattice_tables(ctx);
+  if (rc)
+    return rc;
+  if (ctx->csr.enabled && csr_set_bunches(ctx->csr, n_instances, ctx->d_inst_offsets.ptr, ctx->err))
+    return B2E_ERR_NOMEM;
+  return B2E_OK;
 }
 
 static int ensure_particle_buffers(b2e_ctx *ctx, int64_t n) {
@@ -497,16 +506,24 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
   if (p0 == 0) {
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_rf.ptr, 0, sizeof(DevRfState) * std::max(1, ctx->n_inst * ctx->lat.n_rf),
                                   ctx->stream));
+    if (ctx->csr.enabled && ctx->csr.n_bunches != ctx->n_inst &&
+        csr_set_bunches(ctx->csr, ctx->n_inst, ctx->d_inst_offsets.ptr, ctx->err))
+      return B2E_ERR_NOMEM;
     csr_reset(ctx->csr);
-    /* CHARGE (do_tracking.c:1324-1360): macro-particle charge = TOTAL / particles at start */
-    ctx->csr.macro_charge = 0;
-    for (const b2e_element &el : ctx->base)
-      if (el.type == B2E_CHARGE) {
-        if (ctx->n)
-          ctx->csr.macro_charge = el.p[B2E_CHARGE_TOTAL] / ctx->n;
-        if (el.p[B2E_CHARGE_PER_PARTICLE])
-          ctx->csr.macro_charge = el.p[B2E_CHARGE_PER_PARTICLE];
-      }
+    /* CHARGE (do_tracking.c:1324-1360): macro-particle charge = TOTAL / particles
+     * at start; in an ensemble every instance is a bunch of charge TOTAL */
+    for (int b = 0; ctx->csr.enabled && b < ctx->csr.n_bunches; b++) {
+      const int64_t nb = ctx->csr.n_bunches == 1 ? ctx->n : ctx->inst_offsets[b + 1] - ctx->inst_offsets[b];
+      double q = 0;
+      for (const b2e_element &el : ctx->base)
+        if (el.type == B2E_CHARGE) {
+          if (nb)
+            q = el.p[B2E_CHARGE_TOTAL] / nb;
+          if (el.p[B2E_CHARGE_PER_PARTICLE])
+            q = el.p[B2E_CHARGE_PER_PARTICLE];
+        }
+      ctx->csr.macro_charge[b] = q;
+    }
   }
   /* stop points: every RFCA on pass 0 (fiducial), every CSR element on every pass */
   int p = p0, e = 0;
@@ -553,11 +570,13 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     } else {
       /* the collective step needs the number of particles alive at its entrance
        * (n_part > 1 decides whether CSR is computed at all, csbend.c:1987) */
-      int64_t n_alive = 0;
-      int rc = count_alive(ctx, &n_alive);
+      std::vector<int64_t> alive;
+      ctx->csr.d_offsets = ctx->d_inst_offsets.ptr;
+      int rc = csr_count_alive(ctx->csr, particle_view(ctx).lost_pass, ctx->n, alive, ctx->stream, ctx->err);
       if (rc)
         return rc;
-      rc = csr_track_element(ctx->csr, ctx->d_elems.ptr, ctx->lat.elems[stop_e], particle_view(ctx), ctx->n, n_alive,
+      ctx->launches++;
+      rc = csr_track_element(ctx->csr, ctx->d_elems.ptr, ctx->lat.elems[stop_e], particle_view(ctx), ctx->n, alive,
                              stop_e, p, ctx->stream, ctx->err, &ctx->launches);
       if (rc)
         return rc;

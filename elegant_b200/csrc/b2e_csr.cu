@@ -31,6 +31,34 @@ struct CsrDevState {
   double dGamma[B2E_CSR_MAX_BINS];           /* csrWake.dGamma: last dipole wake */
 };
 
+/* Per-bunch view for the CSR kernels.  Bunches are contiguous particle ranges
+ * [offs[b], offs[b+1]); each has its own binning and wake state, its own
+ * CSRConstant (zero when the bunch has at most one particle at the element
+ * entrance) and, in CSRDRIFT, its own choice between wake kicks and the exact
+ * drift.  A single bunch is n = 1 (offs is then not read). */
+struct CsrBunches {
+  const int64_t *offs;
+  int n;
+  CsrDevState *st;
+  const double *csr_const;
+  const unsigned char *active; /* more than one particle alive at the element entrance */
+  const unsigned char *mode;   /* CSRDRIFT: 1 = wake kicks, 0 = exact drift */
+};
+
+__device__ __forceinline__ int bunch_of(int64_t i, const CsrBunches &B) {
+  if (B.n <= 1)
+    return 0;
+  int lo = 0, hi = B.n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (B.offs[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ unsigned long long key_of(double v) {
   unsigned long long b = (unsigned long long)__double_as_longlong(v);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
@@ -60,6 +88,18 @@ __device__ __forceinline__ void block_minmax(double v, bool valid, CsrDevState *
       atomicMin(&st->ct_min_key, kmin);
     if (kmax != 0ull)
       atomicMax(&st->ct_max_key, kmax);
+  }
+}
+
+/* min/max of c*t per bunch: a warp whose lanes all belong to one bunch
+ * reduces first; a warp that straddles bunches updates lane by lane. */
+__device__ __forceinline__ void bunch_minmax(double v, bool valid, int b, const CsrBunches &B) {
+  const int b0 = __shfl_sync(0xffffffffu, b, 0);
+  if (__all_sync(0xffffffffu, b == b0)) {
+    block_minmax(v, valid, B.st + b0);
+  } else if (valid) {
+    atomicMin(&B.st[b].ct_min_key, key_of(v));
+    atomicMax(&B.st[b].ct_max_key, key_of(v));
   }
 }
 
@@ -110,10 +150,13 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
 /* one kick: optional wake kick of the previous kick, one integrator slice,
  * c*t update, min/max of c*t (csbend.c:2385-2450, :3066-3076) */
 __global__ void csr_slice_kernel(DevParticles P, int64_t n, const double *beta0, const DevElem *ep,
-                                 const DevAperture *ap, CsrDevState *st, int apply_kick, int nBins, double Po,
+                                 const DevAperture *ap, CsrBunches B, int after_first_kick, int nBins, double Po,
                                  int pass, int elem_index) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool alive = i < n && P.lost_pass[i] < 0;
+  const int b = i < n ? bunch_of(i, B) : B.n - 1;
+  const CsrDevState *st = B.st + b;
+  const int apply_kick = after_first_kick && B.csr_const[b] != 0;
   double CT = 0;
   if (alive) {
     const DevElem &e = *ep;
@@ -143,14 +186,20 @@ __global__ void csr_slice_kernel(DevParticles P, int64_t n, const double *beta0,
       P.s[i] = CT;
     }
   }
-  block_minmax(CT, alive, st);
+  bunch_minmax(CT, alive, b, B);
 }
 
 /* histogram of c*t with the range of binParticleCoordinate (csbend.c:3047-3113):
  * shared-memory integer counts aggregated per warp, then added to global counts. */
-__global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrDevState *st, unsigned int *counts, int nBins,
+__global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigned int *counts_all, int nBins,
                                 double factor) {
   extern __shared__ unsigned int scount[];
+  const int bunch = blockIdx.y;
+  if (!B.active[bunch])
+    return;
+  CsrDevState *st = B.st + bunch;
+  unsigned int *counts = counts_all + (size_t)bunch * nBins;
+  const int64_t first = B.n <= 1 ? 0 : B.offs[bunch], end = B.n <= 1 ? n : B.offs[bunch + 1];
   double lower = value_of(st->ct_min_key), upper = value_of(st->ct_max_key), dct;
   expand_range(&lower, &upper, factor);
   dct = (upper - lower) / nBins;
@@ -162,10 +211,10 @@ __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrDevState *st, unsi
     st->ctUpper = upper;
     st->dct = dct;
   }
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - threadIdx.x < n;
+  for (int64_t i = first + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - threadIdx.x < end;
        i += (int64_t)gridDim.x * blockDim.x) {
     int bin = -1;
-    if (i < n && P.lost_pass[i] < 0) {
+    if (i < end && P.lost_pass[i] < 0) {
       long long b = (long long)((P.s[i] - lower) / dct);
       if (b >= 0 && b <= nBins - 1)
         bin = (int)b;
@@ -187,7 +236,8 @@ struct WakeArgs {
   const double *sg_w, *sgd_w; /* [nBins][B2E_SG_MAX_WIDTH] */
   const int *sg_lo, *sg_n, *sgd_lo, *sgd_n;
   double slippage, slippage13, c1, c2, csr_constant;
-  double *wakelog; /* nBins values for this kick, or null */
+  double length, nSlices;   /* element length and kicks: c1 and c2 of each bunch */
+  double *wakelog;          /* nBins values per bunch for this kick, or null */
 };
 
 /* Savitzky-Golay pass with precomputed per-bin weights (b2e_sg.h convention);
@@ -328,10 +378,22 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
   }
 }
 
-/* wake of one kick of a tracked bunch */
-__global__ void csr_wake_kernel(CsrDevState *st, const unsigned int *counts, WakeArgs a) {
+/* wake of one kick, one CTA per bunch; c1 and c2 from the bunch's CSRConstant
+ * in the host expression's order (csbend.c:2664-2667) */
+__global__ void csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a) {
   extern __shared__ double sm[];
-  wake_body<unsigned int, long long>(counts, a, st->dct, sm, st->dGamma, &st->nBinned, nullptr, nullptr);
+  const int bunch = blockIdx.x;
+  if (!B.active[bunch])
+    return;
+  CsrDevState *st = B.st + bunch;
+  WakeArgs w = a;
+  const double csr_constant = B.csr_const[bunch];
+  w.csr_constant = csr_constant;
+  w.c1 = csr_constant * a.length / a.nSlices;
+  w.c2 = -csr_constant * a.length / a.nSlices / a.slippage13;
+  w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
+  wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, st->dct, sm, st->dGamma, &st->nBinned,
+                                     nullptr, nullptr);
 }
 
 /* Batched wake integral of many profiles in bin units (dct = 1), one CTA per
@@ -353,36 +415,39 @@ __global__ void wake_batch_kernel(const double *counts, const double *slippage_b
 }
 
 /* after the last kick: its wake kick and the min/max for the exit binning */
-__global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrDevState *st, int apply_kick, int nBins, double Po,
-                                     double rho0) {
+__global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrBunches B, int nBins, double Po, double rho0) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool alive = i < n && P.lost_pass[i] < 0;
+  const int b = i < n ? bunch_of(i, B) : B.n - 1;
   double CT = 0;
   if (alive) {
     CT = P.s[i];
-    if (apply_kick)
-      P.dp[i] = csr_kick(CT, P.x[i], P.dp[i], st, nBins, Po, rho0);
+    if (B.active[b] && B.csr_const[b] != 0)
+      P.dp[i] = csr_kick(CT, P.x[i], P.dp[i], B.st + b, nBins, Po, rho0);
   }
-  block_minmax(CT, alive, st);
+  bunch_minmax(CT, alive, b, B);
 }
 
 /* exit: c*t -> s at the final velocity, exit edge, back to the lab frame
  * (csbend.c:2810-2955); csrWake.s0 from the exit binning's lower edge. */
-__global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, CsrDevState *st, double factor,
-                                int do_bin, double Po, int pass, int elem_index) {
+__global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, CsrBunches B, double factor, double Po,
+                                int pass, int elem_index) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const DevElem &e = *ep;
   const double *c = e.c;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    double lower = 0, upper = 0;
-    st->dctBin = do_bin ? st->dct : 0;
-    if (do_bin) {
-      lower = value_of(st->ct_min_key);
-      upper = value_of(st->ct_max_key);
-      expand_range(&lower, &upper, factor);
+  if (blockIdx.x == 0)
+    for (int b = threadIdx.x; b < B.n; b += blockDim.x) {
+      CsrDevState *st = B.st + b;
+      const int do_bin = B.active[b];
+      double lower = 0, upper = 0;
+      st->dctBin = do_bin ? st->dct : 0;
+      if (do_bin) {
+        lower = value_of(st->ct_min_key);
+        upper = value_of(st->ct_max_key);
+        expand_range(&lower, &upper, factor);
+      }
+      st->s0 = lower + c[CB_DZF];
     }
-    st->s0 = lower + c[CB_DZF];
-  }
   if (i >= n || P.lost_pass[i] >= 0)
     return;
   const double ct = c[CB_COS_TT], sn = c[CB_SIN_TT];
@@ -414,11 +479,15 @@ __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, Cs
 }
 
 /* CSRDRIFT mode 0, one kick (csbend.c:3415-3502) */
-__global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, const CsrDevState *st, double dz, double s0_incr,
+__global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, CsrBunches B, double dz, double s0_incr,
                                       double factor, int apply, int nBins, double Po) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
     return;
+  const int b = bunch_of(i, B);
+  if (!B.mode[b])
+    return;
+  const CsrDevState *st = B.st + b;
   double x = P.x[i], xp = P.xp[i], y = P.y[i], yp = P.yp[i], s = P.s[i], dp = P.dp[i], p, beta;
   x = x + xp * dz;
   y = y + yp * dz;
@@ -441,7 +510,19 @@ __global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, const CsrDevSta
   P.dp[i] = dp;
 }
 
-__global__ void csr_s0_add_kernel(CsrDevState *st, double incr) { st->s0 = st->s0 + incr; }
+/* empty min/max keys of every bunch before a binning pass */
+__global__ void csr_reset_keys_kernel(CsrBunches B) {
+  for (int b = threadIdx.x; b < B.n; b += blockDim.x) {
+    B.st[b].ct_min_key = ~0ull;
+    B.st[b].ct_max_key = 0ull;
+  }
+}
+
+__global__ void csr_s0_add_kernel(CsrBunches B, double incr) {
+  for (int b = threadIdx.x; b < B.n; b += blockDim.x)
+    if (B.mode[b])
+      B.st[b].s0 = B.st[b].s0 + incr;
+}
 
 /* do_tracking's sweeps after a collective element (do_tracking.c:2455-2475,
  * :2629): MAXAMP aperture if one is active, then inf/NaN in x or y. */
@@ -473,9 +554,13 @@ cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const De
   return cudaGetLastError();
 }
 
-__global__ void edrift_kernel(DevParticles P, int64_t n, double L) {
+/* exact drift of the particles of the bunches whose CSRDRIFT mode is `mode`
+ * (every particle when the mode table is null) */
+__global__ void edrift_kernel(DevParticles P, int64_t n, double L, CsrBunches B, int mode) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  if (B.mode && B.mode[bunch_of(i, B)] != mode)
     return;
   double xp = P.xp[i], yp = P.yp[i];
   P.x[i] = P.x[i] + xp * L;
@@ -583,12 +668,8 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
     }
     st.elems.push_back(ce);
   }
-  if (cudaMalloc(&st.d_state, sizeof(CsrDevState)) != cudaSuccess ||
-      cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS) != cudaSuccess) {
-    err = "CSR state allocation failed";
+  if (csr_set_bunches(st, 1, nullptr, err))
     return B2E_ERR_NOMEM;
-  }
-  cudaMemset(st.d_state, 0, sizeof(CsrDevState));
   if (!sgw.empty()) {
     if (cudaMalloc(&st.d_sg, sizeof(double) * sgw.size()) != cudaSuccess ||
         cudaMalloc(&st.d_sg_idx, sizeof(int) * sgi.size()) != cudaSuccess) {
@@ -602,11 +683,85 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
   return B2E_OK;
 }
 
+int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::string &err) {
+  if (n_bunches < 1 || (n_bunches > 1 && !d_offsets)) {
+    err = "CSR: bad bunch layout";
+    return B2E_ERR_ARG;
+  }
+  if (st.d_state)
+    cudaFree(st.d_state);
+  if (st.d_counts)
+    cudaFree(st.d_counts);
+  if (st.d_csr_const)
+    cudaFree(st.d_csr_const);
+  if (st.d_flags)
+    cudaFree(st.d_flags);
+  if (st.d_alive)
+    cudaFree(st.d_alive);
+  st.d_state = nullptr;
+  st.d_counts = nullptr;
+  st.d_csr_const = nullptr;
+  st.d_flags = nullptr;
+  st.d_alive = nullptr;
+  st.n_bunches = n_bunches;
+  st.d_offsets = d_offsets;
+  st.wake_valid.assign(n_bunches, 0);
+  st.macro_charge.assign(n_bunches, 0.0);
+  if (cudaMalloc(&st.d_state, sizeof(CsrDevState) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_csr_const, sizeof(double) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_flags, 2 * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
+    err = "CSR state allocation failed";
+    return B2E_ERR_NOMEM;
+  }
+  cudaMemset(st.d_state, 0, sizeof(CsrDevState) * n_bunches);
+  cudaMemset(st.d_csr_const, 0, sizeof(double) * n_bunches);
+  cudaMemset(st.d_flags, 0, 2 * n_bunches);
+  return B2E_OK;
+}
+
+/* alive particles per bunch: blockIdx.y is the bunch */
+__global__ void alive_per_bunch_kernel(const int32_t *lost_pass, int64_t n, const int64_t *offs, int nb,
+                                       unsigned long long *alive) {
+  const int b = blockIdx.y;
+  const int64_t first = nb <= 1 ? 0 : offs[b], end = nb <= 1 ? n : offs[b + 1];
+  unsigned long long c = 0;
+  for (int64_t i = first + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
+       i += (int64_t)gridDim.x * blockDim.x)
+    c += lost_pass[i] < 0;
+  for (int off = 16; off > 0; off >>= 1)
+    c += __shfl_down_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c)
+    atomicAdd(&alive[b], c);
+}
+
+int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vector<int64_t> &alive, cudaStream_t stream,
+                    std::string &err) {
+  const int nb = st.n_bunches;
+  std::vector<unsigned long long> h(nb);
+  if (cudaMemsetAsync(st.d_alive, 0, sizeof(unsigned long long) * nb, stream) != cudaSuccess) {
+    err = "CSR: alive count failed";
+    return B2E_ERR_CUDA;
+  }
+  const int gx = (int)std::min<int64_t>(std::max(1, 148 * 4 / nb), std::max<int64_t>(1, (n / nb + 255) / 256));
+  alive_per_bunch_kernel<<<dim3(gx, nb), 256, 0, stream>>>(lost_pass, n, st.d_offsets, nb, st.d_alive);
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(h.data(), st.d_alive, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    err = "CSR: alive count failed";
+    return B2E_ERR_CUDA;
+  }
+  alive.assign(h.begin(), h.end());
+  return B2E_OK;
+}
+
 void csr_reset(CsrState &st) {
   st.wakes_host.clear();
   st.wake_values = 0;
   st.accumulated_angle = 0;
-  st.wake_valid = false;
+  st.wake_valid.assign(st.n_bunches, 0);
 }
 
 static int ensure_wakelog(CsrState &st, int64_t values) {
@@ -635,7 +790,8 @@ static int ensure_wakelog(CsrState &st, int64_t values) {
   } while (0)
 
 int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
-                      int64_t n_alive, int elem, int pass, cudaStream_t stream, std::string &err, int64_t *launches) {
+                      const std::vector<int64_t> &alive, int elem, int pass, cudaStream_t stream, std::string &err,
+                      int64_t *launches) {
   size_t k = 0;
   while (k < st.elems.size() && st.elems[k].index != elem)
     k++;
@@ -643,17 +799,47 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     err = "CSR element not configured";
     return B2E_ERR_STATE;
   }
+  if ((int)alive.size() != st.n_bunches) {
+    err = "CSR: per-bunch alive counts do not match the bunch layout";
+    return B2E_ERR_STATE;
+  }
   const CsrElem &ce = st.elems[k];
-  CsrDevState *dst = (CsrDevState *)st.d_state;
+  const int nbunch = st.n_bunches;
+  CsrBunches B;
+  B.offs = st.d_offsets;
+  B.n = nbunch;
+  B.st = (CsrDevState *)st.d_state;
+  B.csr_const = st.d_csr_const;
+  B.active = st.d_flags;
+  B.mode = st.d_flags + nbunch;
   const double Po = st.p_central;
   const int g = grid_for(n);
+  std::vector<unsigned char> flags(2 * nbunch, 0);
   if (ce.kind == K_CSRDRIFT) {
-    /* track_through_driftCSR (csbend.c:3176-3533), mode 0 */
-    if (n_alive <= 1 || !st.wake_valid || !ce.drift_csr) {
-      edrift_kernel<<<g, 256, 0, stream>>>(P, n, ce.drift_length);
+    /* track_through_driftCSR (csbend.c:3176-3533), mode 0: bunches with a
+     * valid dipole wake and more than one particle get wake kicks, the others
+     * an exact drift (csbend.c:3196-3212) */
+    bool any = false;
+    for (int b = 0; b < nbunch; b++) {
+      flags[nbunch + b] = alive[b] > 1 && st.wake_valid[b] && ce.drift_csr;
+      any = any || flags[nbunch + b];
+    }
+    if (!any) {
+      CsrBunches all = B;
+      all.mode = nullptr;
+      edrift_kernel<<<g, 256, 0, stream>>>(P, n, ce.drift_length, all, 0);
       (*launches)++;
       CSR_CUDA(cudaGetLastError());
       return B2E_OK;
+    }
+    CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
+    bool some_plain = false;
+    for (int b = 0; b < nbunch; b++)
+      some_plain = some_plain || !flags[nbunch + b];
+    if (some_plain) {
+      edrift_kernel<<<g, 256, 0, stream>>>(P, n, ce.drift_length, B, 0);
+      (*launches)++;
+      CSR_CUDA(cudaGetLastError());
     }
     double zStart = ce.z_start;
     int nKicks;
@@ -668,26 +854,24 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     }
     double dz0 = ce.drift_length / nKicks, dz = dz0 / 2;
     double dzFirst = zStart - st.zLast;
-    const int nb = st.elems[0].bins; /* csrWake.bins: bins of the last CSRCSBEND */
-    int lastBins = 0;
+    int lastBins = 0; /* csrWake.bins: bins of the last CSRCSBEND */
     for (size_t j = 0; j < st.elems.size(); j++)
       if (st.elems[j].kind == K_CSRCSBEND && st.elems[j].index < elem)
         lastBins = st.elems[j].bins;
-    (void)nb;
     for (int iKick = 0; iKick < nKicks; iKick++) {
       if (iKick == 1)
         dz = dz0;
       double incr = dz + dzFirst;
       double factor = (dz0 + dzFirst) / st.ds0;
-      csr_drift_kick_kernel<<<g, 256, 0, stream>>>(P, n, dst, dz, incr, factor, 1, lastBins, Po);
-      csr_s0_add_kernel<<<1, 1, 0, stream>>>(dst, incr);
+      csr_drift_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, dz, incr, factor, 1, lastBins, Po);
+      csr_s0_add_kernel<<<1, 32, 0, stream>>>(B, incr);
       (*launches) += 2;
       CSR_CUDA(cudaGetLastError());
       dzFirst = 0;
     }
     dz = dz0 / 2;
-    edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz);
-    csr_s0_add_kernel<<<1, 1, 0, stream>>>(dst, dz);
+    edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz, B, 1);
+    csr_s0_add_kernel<<<1, 32, 0, stream>>>(B, dz);
     (*launches) += 2;
     CSR_CUDA(cudaGetLastError());
     st.zLast = zStart + ce.drift_length;
@@ -696,10 +880,14 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
 
   /* ---- CSRCSBEND ---- */
   const DevElem *d_e = d_elems + elem;
-  const bool more_than_one = n_alive > 1;
+  bool any_active = false;
+  for (int b = 0; b < nbunch; b++) {
+    flags[b] = alive[b] > 1; /* csbend.c:1987 */
+    any_active = any_active || flags[b];
+  }
   if (!ce.same_bend_precedes)
     st.accumulated_angle = 0;
-  st.wake_valid = false;
+  st.wake_valid.assign(nbunch, 0);
   if (st.beta0_cap < n) {
     if (st.d_beta0)
       cudaFree(st.d_beta0);
@@ -709,38 +897,44 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     }
     st.beta0_cap = n;
   }
-  if (ensure_wakelog(st, st.wake_values + (int64_t)ce.nSlices * ce.bins)) {
+  if (ensure_wakelog(st, st.wake_values + (int64_t)ce.nSlices * ce.bins * nbunch)) {
     err = "CSR wake log allocation failed";
     return B2E_ERR_NOMEM;
   }
   st.ds0 = ce.length / ce.nSlices;
   st.zLast = st.z0 = ce.z_end;
-  /* CSRConstant (csbend.c:2378-2381) */
+  /* CSRConstant (csbend.c:2378-2381), per bunch */
   const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
-  double csr_constant = 0;
-  if (ce.csr && more_than_one)
-    csr_constant = 2 * st.macro_charge * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
-  const double c1 = csr_constant * ce.length / ce.nSlices;
+  std::vector<double> csr_constant(nbunch, 0.0);
+  for (int b = 0; b < nbunch; b++)
+    if (ce.csr && flags[b])
+      csr_constant[b] = 2 * st.macro_charge[b] * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) /
+                        (4 * kPI * eps0 * kME * (kC * kC));
+  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), sizeof(double) * nbunch, cudaMemcpyHostToDevice,
+                           stream));
+  CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
   const double *sgw = st.d_sg + st.sg_offset[k];
   const int *sgi = st.d_sg_idx + st.sg_offset[k] / B2E_SG_MAX_WIDTH * 2;
+  const size_t wake_smem = sizeof(double) * 4 * ce.bins;
+  CSR_CUDA(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wake_smem));
 
   csr_entry_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, Po);
   (*launches)++;
   CSR_CUDA(cudaGetLastError());
   double phiBend = st.accumulated_angle;
   for (int kick = 0; kick < ce.nSlices; kick++) {
-    CSR_CUDA(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), stream));
-    CSR_CUDA(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), stream));
-    csr_slice_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, nullptr, dst, kick > 0 && csr_constant != 0,
-                                            ce.bins, Po, pass, elem);
+    csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
+    (*launches)++;
+    csr_slice_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, nullptr, B, kick > 0, ce.bins, Po, pass, elem);
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
-    if (!more_than_one)
+    if (!any_active)
       continue;
-    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins, stream));
-    int hb = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 1023) / 1024));
-    csr_hist_kernel<<<hb, 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, dst, st.d_counts, ce.bins,
-                                                                         ce.binRangeFactor);
+    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
+    int64_t per = (n + nbunch - 1) / nbunch;
+    int hb = (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 4 / nbunch), std::max<int64_t>(1, (per + 1023) / 1024));
+    csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, B, st.d_counts, ce.bins,
+                                                                                       ce.binRangeFactor);
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
     phiBend += ce.angle / ce.nSlices;
@@ -760,25 +954,23 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     a.sgd_n = sgi + 2 * ce.bins + 1;
     a.slippage = slippage;
     a.slippage13 = b2e_pow(slippage, 1. / 3.);
-    a.c1 = c1;
-    a.c2 = -csr_constant * ce.length / ce.nSlices / a.slippage13;
-    a.csr_constant = csr_constant;
+    a.length = ce.length;
+    a.nSlices = ce.nSlices;
+    a.c1 = a.c2 = a.csr_constant = 0; /* per bunch in the kernel */
     a.wakelog = st.d_wakelog + st.wake_values;
-    size_t smem = sizeof(double) * 4 * ce.bins;
-    CSR_CUDA(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    csr_wake_kernel<<<1, 1024, smem, stream>>>(dst, st.d_counts, a);
+    csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a);
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
-    st.wake_values += ce.bins;
+    st.wake_values += (int64_t)ce.bins * nbunch;
   }
-  CSR_CUDA(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), stream));
-  CSR_CUDA(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), stream));
-  csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, dst, more_than_one && csr_constant != 0, ce.bins, Po, ce.rho0);
-  csr_exit_kernel<<<g, 256, 0, stream>>>(P, n, d_e, dst, ce.binRangeFactor, more_than_one, Po, pass, elem);
+  csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
+  (*launches)++;
+  csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, ce.bins, Po, ce.rho0);
+  csr_exit_kernel<<<g, 256, 0, stream>>>(P, n, d_e, B, ce.binRangeFactor, Po, pass, elem);
   (*launches) += 2;
   CSR_CUDA(cudaGetLastError());
-  if (more_than_one)
-    st.wake_valid = true;
+  for (int b = 0; b < nbunch; b++)
+    st.wake_valid[b] = flags[b];
   st.accumulated_angle += ce.angle;
   return B2E_OK;
 }
@@ -803,6 +995,15 @@ void csr_release(CsrState &st) {
     cudaFree(st.d_state);
   if (st.d_counts)
     cudaFree(st.d_counts);
+  if (st.d_csr_const)
+    cudaFree(st.d_csr_const);
+  if (st.d_flags)
+    cudaFree(st.d_flags);
+  if (st.d_alive)
+    cudaFree(st.d_alive);
+  st.d_csr_const = nullptr;
+  st.d_flags = nullptr;
+  st.d_alive = nullptr;
   if (st.d_sg)
     cudaFree(st.d_sg);
   if (st.d_sg_idx)
@@ -854,6 +1055,8 @@ struct StaticCsrScratch {
   int sg_idx[2 * B2E_STATIC_MAX_BINS * 2];
   DevElem elem;
   unsigned long long counters[2];
+  double csr_const;       /* the one bunch's CSRConstant */
+  unsigned char flags[2]; /* active, CSRDRIFT mode */
 };
 
 static __device__ __align__(256) unsigned char g_static_csr_scratch[sizeof(StaticCsrScratch)];
@@ -890,6 +1093,12 @@ __global__ void static_set_elem_kernel(DevElem e, DevElem *dst) { *dst = e; }
 /* Savitzky-Golay weight tables for one element, on the device, with the same
  * helpers and layout as csr_configure (rows of B2E_SG_MAX_WIDTH weights;
  * interleaved (start, width) index pairs; smoothing rows then derivative rows). */
+__global__ void static_set_bunch_kernel(StaticCsrScratch *S, double csr_constant, int active) {
+  S->csr_const = csr_constant;
+  S->flags[0] = (unsigned char)active;
+  S->flags[1] = 0;
+}
+
 __global__ void static_sg_weights_kernel(int bins, int sgHalf, int sgOrder, int sgdHalf, int sgdOrder, double *w,
                                          int *idx) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1017,21 +1226,27 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     csr_constant = 2 * macro_particle_charge * kE / b2e_pow(3 * rho0 * rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
   const int g = (int)std::max<int64_t>(1, (n + 255) / 256);
   CsrDevState *dst = &S->state;
+  static_set_bunch_kernel<<<1, 1, 0, s>>>(S, csr_constant, more_than_one);
+  CsrBunches B;
+  B.offs = nullptr;
+  B.n = 1;
+  B.st = dst;
+  B.csr_const = &S->csr_const;
+  B.active = &S->flags[0];
+  B.mode = &S->flags[1];
 
   csr_entry_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, Po);
   STATIC_TRY(cudaGetLastError());
   double phiBend = 0;
   for (int kick = 0; kick < nSlices; kick++) {
-    STATIC_TRY(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), s));
-    STATIC_TRY(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), s));
-    csr_slice_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, nullptr, dst, kick > 0 && csr_constant != 0, bins,
-                                       Po, 0, 0);
+    csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);
+    csr_slice_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, nullptr, B, kick > 0, bins, Po, 0, 0);
     STATIC_TRY(cudaGetLastError());
     if (!more_than_one)
       continue;
     STATIC_TRY(cudaMemsetAsync(S->counts, 0, sizeof(unsigned int) * bins, s));
     int hb = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 1023) / 1024));
-    csr_hist_kernel<<<hb, 1024, sizeof(unsigned int) * bins, s>>>(P, n, dst, S->counts, bins, brf);
+    csr_hist_kernel<<<dim3(hb, 1), 1024, sizeof(unsigned int) * bins, s>>>(P, n, B, S->counts, bins, brf);
     STATIC_TRY(cudaGetLastError());
     phiBend += angle / nSlices;
     double slippage = fabs(rho0 * (phiBend * phiBend * phiBend) / 24.0);
@@ -1050,19 +1265,18 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     a.sgd_n = S->sg_idx + 2 * bins + 1;
     a.slippage = slippage;
     a.slippage13 = b2e_pow(slippage, 1. / 3.);
-    a.c1 = csr_constant * length / nSlices;
-    a.c2 = -csr_constant * length / nSlices / a.slippage13;
-    a.csr_constant = csr_constant;
+    a.length = length;
+    a.nSlices = nSlices;
+    a.c1 = a.c2 = a.csr_constant = 0; /* formed in the kernel from B.csr_const */
     a.wakelog = dev_wakes ? dev_wakes + (size_t)kick * bins : nullptr;
     size_t smem = sizeof(double) * 4 * bins;
     STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    csr_wake_kernel<<<1, 1024, smem, s>>>(dst, S->counts, a);
+    csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a);
     STATIC_TRY(cudaGetLastError());
   }
-  STATIC_TRY(cudaMemsetAsync(&dst->ct_min_key, 0xff, sizeof(unsigned long long), s));
-  STATIC_TRY(cudaMemsetAsync(&dst->ct_max_key, 0x00, sizeof(unsigned long long), s));
-  csr_last_kick_kernel<<<g, 256, 0, s>>>(P, n, dst, more_than_one && csr_constant != 0, bins, Po, rho0);
-  csr_exit_kernel<<<g, 256, 0, s>>>(P, n, &S->elem, dst, brf, more_than_one, Po, 0, 0);
+  csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);
+  csr_last_kick_kernel<<<g, 256, 0, s>>>(P, n, B, bins, Po, rho0);
+  csr_exit_kernel<<<g, 256, 0, s>>>(P, n, &S->elem, B, brf, Po, 0, 0);
   STATIC_TRY(cudaGetLastError());
   STATIC_TRY(launch_post_element_sweep(P, n, nullptr, 0, 0, s));
   return B2E_OK;

@@ -44,28 +44,42 @@ struct CsrState {
   std::vector<CsrElem> elems;
   std::vector<double> wakes_host; /* filled on demand from the device log */
   int64_t wake_values = 0;        /* values written to the device log in this run */
-  double macro_charge = 0;        /* CHARGE TOTAL / particles at pass start */
+  std::vector<double> macro_charge; /* per bunch: CHARGE TOTAL / its particles at pass start */
   double p_central = 0;
   double accumulated_angle = 0;
+  /* bunches: contiguous particle ranges, each with its own CSR state */
+  int n_bunches = 1;
+  const int64_t *d_offsets = nullptr; /* [n_bunches + 1], owned by the caller */
+  std::vector<unsigned char> wake_valid; /* per bunch: csrWake.valid */
   /* device buffers */
   double *d_beta0 = nullptr;
   int64_t beta0_cap = 0;
-  void *d_state = nullptr;        /* CsrDevState */
-  unsigned int *d_counts = nullptr;
+  void *d_state = nullptr;        /* CsrDevState[n_bunches] */
+  unsigned int *d_counts = nullptr; /* [n_bunches][B2E_CSR_MAX_BINS] */
+  double *d_csr_const = nullptr;  /* [n_bunches] */
+  unsigned char *d_flags = nullptr; /* [2][n_bunches]: active, CSRDRIFT mode */
+  unsigned long long *d_alive = nullptr; /* [n_bunches] */
   double *d_sg = nullptr;         /* weights of all elements, uploaded once */
   int *d_sg_idx = nullptr;
   std::vector<size_t> sg_offset;  /* per element: offset into d_sg / d_sg_idx */
   double *d_wakelog = nullptr;
   int64_t wakelog_cap = 0;
-  bool wake_valid = false;        /* csrWake.valid */
   double ds0 = 0, zLast = 0, z0 = 0;
 };
 
 int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLattice &lat, const b2e_run_options &opt,
                   std::string &err);
 void csr_reset(CsrState &st);
+/* Bunch layout for the CSR step (n_bunches contiguous ranges; offsets on the
+ * device, owned by the caller); allocates the per-bunch state. */
+int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::string &err);
+/* particles alive (lost_pass < 0), per bunch */
+int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vector<int64_t> &alive, cudaStream_t stream,
+                    std::string &err);
+/* alive: particles alive at the element entrance, per bunch */
 int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
-                      int64_t n_alive, int elem, int pass, cudaStream_t stream, std::string &err, int64_t *launches);
+                      const std::vector<int64_t> &alive, int elem, int pass, cudaStream_t stream, std::string &err,
+                      int64_t *launches);
 int csr_copy_wakes(CsrState &st, double *wakes, int64_t capacity, int64_t *written, std::string &err);
 cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const DevAperture *ap, int pass, int elem,
                                       cudaStream_t stream);

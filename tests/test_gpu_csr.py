@@ -63,3 +63,45 @@ def test_chicane_without_charge_is_plain_tracking(ref_b2e):
     lat = w.chicane(bins=100, n_kicks=3, charge=0.0)
     beam = w.chicane_beam(5000, seed=2)
     check(*run_both(ref_b2e, lat, beam))
+
+
+def _bunch_train(sizes, chirps, seed):
+    from elegant_b200.beam import Beam
+    parts, next_id = [], 1
+    for k, (n, h) in enumerate(zip(sizes, chirps)):
+        b = w.chicane_beam(n, seed=seed + k, chirp=h)
+        parts.append(Beam(b.coords, np.arange(next_id, next_id + n)))
+        next_id += n
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    return Beam(np.concatenate([p.coords for p in parts]), np.concatenate([p.ids for p in parts])), offsets
+
+
+@pytest.mark.parametrize("drift_kicks", [1, 3])
+def test_bunch_train_matches_single_bunches(ref_b2e, drift_kicks):
+    """Bunches tracked together, each with its own histogram, wake and macro
+    charge, give every bunch the reference's single-bunch result bit for bit
+    (one bunch holds a single particle: no CSR for it)."""
+    lat = w.chicane(bins=120, n_kicks=4)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, N_KICKS=drift_kicks)) if e.type == "CSRDRIFT" else e
+                   for e in lat.elements])
+    sizes, chirps = [3000, 1, 7000, 4500], [-10.0, -8.0, -15.0, -5.0]
+    beam, offsets = _bunch_train(sizes, chirps, seed=50)
+    with Tracker(lat, P0, 1) as t:
+        t.load_ensemble(offsets, [])
+        res = t.track(beam)
+        wakes = t.csr_wakes(10_000_000)
+    nb = len(sizes)
+    wakes = wakes.reshape(-1, nb, 120)
+    for b in range(nb):
+        sl = slice(offsets[b], offsets[b + 1])
+        rows, nl, _, ref_wakes = ref_b2e.track(lat, beam.coords[sl], beam.ids[sl], P0, 1, capture_wakes=True)
+        sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
+                        int((res.lost_pass[sl] < 0).sum()), 0.0)
+        ref_c, ref_ids, ref_loss = by_id(rows)
+        order = np.argsort(sub.ids)
+        assert sub.n_left == nl
+        assert np.array_equal(sub.ids[order], ref_ids)
+        alive = ref_loss < 0
+        assert np.array_equal(sub.coords[order][alive], ref_c[alive]), b
+        if sizes[b] > 1:
+            assert np.array_equal(wakes[:, b, :].ravel(), ref_wakes), b
