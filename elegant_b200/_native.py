@@ -90,6 +90,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_stream": (vp, [vp]),
         "b2e_kernel_launches": (i64, [vp]),
         "b2e_history_passes": (i64, [vp]),
+        "b2e_set_csr_surrogate": (c_int, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
+        "b2e_csr_surrogate_stats": (c_int, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp, i64,
+                                            ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -22,6 +22,7 @@
 #include "b2e_lattice.h"
 #include "b2e_csr.h"
 #include "b2e_kernels.h"
+#include "b2e_wakenet.h"
 
 
 
@@ -751,4 +752,43 @@ extern "C" int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int6
   if (!ctx || !written)
     return B2E_ERR_ARG;
   return csr_copy_wakes(ctx->csr, wakes, capacity, written, ctx->err);
+}
+
+extern "C" int b2e_set_csr_surrogate(b2e_ctx *ctx, b2e_wakenet *net, const double feature_scales[3], double tolerance,
+                                     int32_t gate_stride) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  if (net && (!feature_scales || !(tolerance >= 0) || gate_stride < 1))
+    return fail(ctx, B2E_ERR_ARG, "b2e_set_csr_surrogate: scales, a tolerance >= 0 and a stride >= 1 are required");
+  if (net && wakenet_bins(net) < 128)
+    return fail(ctx, B2E_ERR_ARG, "b2e_set_csr_surrogate: not a wake network");
+  ctx->csr.net = net;
+  if (net) {
+    ctx->csr.sc_dens = (float)feature_scales[0];
+    ctx->csr.sc_deriv = (float)feature_scales[1];
+    ctx->csr.sc_target = (float)feature_scales[2];
+    ctx->csr.gate_tol = tolerance;
+    ctx->csr.gate_stride = gate_stride;
+  }
+  return B2E_OK;
+}
+
+extern "C" int b2e_csr_surrogate_stats(b2e_ctx *ctx, int64_t *evaluations, int64_t *fallbacks, double *gate_errors,
+                                       int64_t capacity, int64_t *written) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  unsigned long long c[2] = {0, 0};
+  cudaSetDevice(ctx->device);
+  if (ctx->csr.d_sur_counts)
+    CUDA_TRY(ctx, cudaMemcpy(c, ctx->csr.d_sur_counts, sizeof(c), cudaMemcpyDeviceToHost));
+  if (evaluations)
+    *evaluations = (int64_t)c[0];
+  if (fallbacks)
+    *fallbacks = (int64_t)c[1];
+  const int64_t n = std::min<int64_t>(capacity, ctx->csr.gate_values);
+  if (gate_errors && n > 0)
+    CUDA_TRY(ctx, cudaMemcpy(gate_errors, ctx->csr.d_gate_log, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  if (written)
+    *written = gate_errors ? std::max<int64_t>(n, 0) : ctx->csr.gate_values;
+  return B2E_OK;
 }

@@ -15,6 +15,7 @@
 #include "b2e_elements.cuh"
 #include "b2e_kernels.h"
 #include "b2e_sg.h"
+#include "b2e_wakenet.h"
 
 namespace b2e {
 
@@ -253,15 +254,12 @@ __device__ void sg_apply(const double *in, double *out, int nBins, const double 
   }
 }
 
-/* Wake of one kick (csbend.c:2566-2673) on one CTA, from a histogram of
- * counts (unsigned counts in tracking, real-valued counts for batched
- * profiles).  sm holds 4*nBins doubles.  Writes dgamma[nBins], the wake log
- * when a.wakelog is set, the binned total when nbinned_out is set, and the
- * smoothed density (per unit ct) and its derivative when hist_out/deriv_out
- * are set. */
+/* Filters of one kick's wake (csbend.c:2566-2591) on one CTA: Savitzky-Golay
+ * smoothing of the counts, correctDistribution, density per unit ct, its
+ * derivative filter and the (dct*b)^(1/3) denominators.  Leaves hist = sm,
+ * deriv = sm + nBins, denom = sm + 2 nBins (tmp = sm + 3 nBins is scratch). */
 template <typename CountT, typename SumT>
-__device__ void wake_body(const CountT *counts, const WakeArgs &a, const double dct, double *sm, double *dgamma,
-                          SumT *nbinned_out, double *hist_out, double *deriv_out) {
+__device__ void wake_filters(const CountT *counts, const WakeArgs &a, const double dct, double *sm, SumT *nbinned_out) {
   const int nb = a.nBins;
   double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb, *tmp = sm + 3 * nb;
   __shared__ double nBinnedD;
@@ -310,19 +308,84 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
   __syncthreads();
   sg_apply(deriv, tmp, nb, a.sgd_w, a.sgd_lo, a.sgd_n);
   __syncthreads();
-  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
     deriv[b] = tmp[b];
+  __syncthreads();
+}
+
+/* bins of slippage; clamped to [0, nb] so indexing stays in bounds for a
+ * degenerate bin size (the comparisons below give the same result) */
+__device__ __forceinline__ void slippage_bins(const WakeArgs &a, double dct, long long *diS, long long *diS4) {
+  long long d = (long long)(a.slippage / dct), d4 = (long long)(4 * a.slippage / dct);
+  *diS = d < 0 ? 0 : (d > a.nBins ? a.nBins : d);
+  *diS4 = d4 < 0 ? 0 : (d4 > a.nBins ? a.nBins : d4);
+}
+
+/* T1 (integral) and T2 (slippage boundary) of bin ib before the c1/c2 factors
+ * (csbend.c:2623-2662) */
+__device__ __forceinline__ void wake_terms(int ib, const WakeArgs &a, const double dct, const double *hist,
+                                           const double *deriv, const double *denom, long long diS, long long diS4,
+                                           double *T1out, double *T2out) {
+  const int nb = a.nBins;
+  double T1 = 0, T2 = 0, term1 = 0, term2 = 0;
+  long long count, j;
+  if (a.steady) {
+    if (!a.trapz) {
+      for (j = ib + 1; j < nb; j++)
+        T1 += deriv[j] / denom[j - ib];
+    } else {
+      if ((j = ib + 1) < nb)
+        term1 = deriv[j] / denom[j - ib];
+      for (count = 0, j = ib + 1; j < nb; j++, count++)
+        T1 += (term2 = deriv[j] / denom[j - ib]);
+      if ((ib + 1) < nb)
+        T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
+      if (count > 1)
+        T1 -= (term1 + term2) / 2;
+    }
+  } else {
+    if (!a.trapz) {
+      for (j = ib + 1; j <= (ib + diS) && j < nb; j++)
+        T1 += deriv[j] / denom[j - ib];
+    } else {
+      if ((j = ib + 1) < nb && j <= (ib + diS))
+        term1 = deriv[j] / denom[j - ib] / 2;
+      for (count = 0, j = ib + 1; j <= (ib + diS) && j < nb; count++, j++)
+        T1 += (term2 = deriv[j] / denom[j - ib]);
+      if (diS > 0 && (ib + 1) < nb)
+        T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
+      if (count > 1)
+        T1 -= (term1 + term2) / 2;
+    }
+    if ((ib + diS) < nb)
+      T2 += hist[ib + diS];
+    if ((ib + diS4) < nb)
+      T2 -= hist[ib + diS4];
+  }
+  *T1out = T1;
+  *T2out = T2;
+}
+
+/* Wake of one kick (csbend.c:2566-2673) on one CTA, from a histogram of
+ * counts (unsigned counts in tracking, real-valued counts for batched
+ * profiles).  sm holds 4*nBins doubles.  Writes dgamma[nBins], the wake log
+ * when a.wakelog is set, the binned total when nbinned_out is set, and the
+ * smoothed density (per unit ct) and its derivative when hist_out/deriv_out
+ * are set. */
+template <typename CountT, typename SumT>
+__device__ void wake_body(const CountT *counts, const WakeArgs &a, const double dct, double *sm, double *dgamma,
+                          SumT *nbinned_out, double *hist_out, double *deriv_out) {
+  const int nb = a.nBins;
+  wake_filters<CountT, SumT>(counts, a, dct, sm, nbinned_out);
+  const double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     if (hist_out)
       hist_out[b] = hist[b];
     if (deriv_out)
-      deriv_out[b] = tmp[b];
+      deriv_out[b] = deriv[b];
   }
-  __syncthreads();
-  /* bins of slippage; clamped to [0, nb] so indexing stays in bounds for a
-   * degenerate bin size (the comparisons below give the same result) */
-  long long diS = (long long)(a.slippage / dct), diS4 = (long long)(4 * a.slippage / dct);
-  diS = diS < 0 ? 0 : (diS > nb ? nb : diS);
-  diS4 = diS4 < 0 ? 0 : (diS4 > nb ? nb : diS4);
+  long long diS, diS4;
+  slippage_bins(a, dct, &diS, &diS4);
   if (!(dct > 0)) {
     for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
       dgamma[ib] = 0;
@@ -332,42 +395,9 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
     return;
   }
   for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
-    double T1 = 0, T2 = 0, term1 = 0, term2 = 0;
-    long long count, j;
+    double T1 = 0, T2 = 0;
     if (a.csr_constant) {
-      if (a.steady) {
-        if (!a.trapz) {
-          for (j = ib + 1; j < nb; j++)
-            T1 += deriv[j] / denom[j - ib];
-        } else {
-          if ((j = ib + 1) < nb)
-            term1 = deriv[j] / denom[j - ib];
-          for (count = 0, j = ib + 1; j < nb; j++, count++)
-            T1 += (term2 = deriv[j] / denom[j - ib]);
-          if ((ib + 1) < nb)
-            T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
-          if (count > 1)
-            T1 -= (term1 + term2) / 2;
-        }
-      } else {
-        if (!a.trapz) {
-          for (j = ib + 1; j <= (ib + diS) && j < nb; j++)
-            T1 += deriv[j] / denom[j - ib];
-        } else {
-          if ((j = ib + 1) < nb && j <= (ib + diS))
-            term1 = deriv[j] / denom[j - ib] / 2;
-          for (count = 0, j = ib + 1; j <= (ib + diS) && j < nb; count++, j++)
-            T1 += (term2 = deriv[j] / denom[j - ib]);
-          if (diS > 0 && (ib + 1) < nb)
-            T1 += 0.3 * (denom[1] * denom[1]) * (2 * deriv[ib + 1] + 3 * deriv[ib]) / dct;
-          if (count > 1)
-            T1 -= (term1 + term2) / 2;
-        }
-        if ((ib + diS) < nb)
-          T2 += hist[ib + diS];
-        if ((ib + diS4) < nb)
-          T2 -= hist[ib + diS4];
-      }
+      wake_terms(ib, a, dct, hist, deriv, denom, diS, diS4, &T1, &T2);
       T1 *= a.c1;
       T2 *= a.c2;
     }
@@ -394,6 +424,154 @@ __global__ void csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, Wa
   w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
   wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, st->dct, sm, st->dGamma, &st->nBinned,
                                      nullptr, nullptr);
+}
+
+/* deterministic sum over the CTA (blockDim.x a power of two, red >= blockDim.x doubles) */
+__device__ double block_sum(double v, double *red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+/* Learned wake, step 1 (one CTA per bunch): the kick's filters, then the
+ * network inputs in bin units -- density and derivative normalised to unit
+ * sum and by k = 1/rms(derivative) over the network's L bins, the slippage
+ * code log2(diS)/log2(L), and the density at bin i + diS -- padded with zeros
+ * to L bins.  The tables (density, derivative, denominators) and the
+ * per-bunch scalars (sum, k, dct) are kept for step 3. */
+__global__ void __launch_bounds__(1024, 1) csr_sur_filter_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a, int L, float sc_dens,
+                                      float sc_deriv, double *tab, double *scal, float *inputs) {
+  extern __shared__ double sm[];
+  const int b = blockIdx.x, nb = a.nBins;
+  float *in = inputs + (size_t)b * 4 * L;
+  if (!B.active[b]) {
+    for (int i = threadIdx.x; i < 4 * L; i += blockDim.x)
+      in[i] = 0.f;
+    return;
+  }
+  CsrDevState *st = B.st + b;
+  const double dct = st->dct;
+  wake_filters<unsigned int, long long>(counts_all + (size_t)b * nb, a, dct, sm, &st->nBinned);
+  const double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb;
+  double *red = sm + 3 * nb;
+  double *t = tab + (size_t)b * 3 * B2E_CSR_MAX_BINS;
+  double part = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    t[i] = hist[i];
+    t[B2E_CSR_MAX_BINS + i] = deriv[i];
+    t[2 * B2E_CSR_MAX_BINS + i] = denom[i];
+    part += hist[i] * dct;
+  }
+  const double total = block_sum(part, red);
+  part = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    const double d = deriv[i] * dct / total;
+    part += d * d;
+  }
+  const double k = 1.0 / sqrt(block_sum(part, red) / L);
+  long long diS, diS4;
+  slippage_bins(a, dct, &diS, &diS4);
+  const float code = (float)(log2((double)(diS < 1 ? 1 : (diS > L ? L : diS))) / log2((double)L));
+  const double fd = k / total * sc_dens, fg = k / total * sc_deriv;
+  const int dsh = (int)(diS < 1 ? 1 : diS);
+  for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    in[i] = i < nb ? (float)(hist[i] * dct * fd) : 0.f;
+    in[L + i] = i < nb ? (float)(deriv[i] * dct * fg) : 0.f;
+    in[2 * L + i] = code;
+    in[3 * L + i] = i + dsh < nb ? (float)(hist[i + dsh] * dct * fd) : 0.f;
+  }
+  if (threadIdx.x == 0) {
+    scal[b * 4 + 0] = total;
+    scal[b * 4 + 1] = k;
+    scal[b * 4 + 2] = dct;
+  }
+}
+
+/* Learned wake, step 3 (one CTA per bunch): the network's T1 (bin units) to
+ * the kick's T1 (times dct^(-4/3)), the gate -- the plain T1 and T2 at every
+ * stride-th bin from `start`, relative rms error of the wake c1 T1 + c2 T2
+ * there -- and the kick's dGamma: the learned T1 with the exact T2, or, when
+ * the error exceeds tol, the plain wake exactly as csr_wake_kernel forms it. */
+__global__ void __launch_bounds__(1024, 1) csr_sur_combine_kernel(CsrBunches B, WakeArgs a, const double *tab, const double *scal, const float *y,
+                                       int L, float sc_target, double tol, int stride, int start, double *gate_log,
+                                       unsigned long long *counters) {
+  extern __shared__ double sm[];
+  const int b = blockIdx.x, nb = a.nBins;
+  if (!B.active[b])
+    return;
+  CsrDevState *st = B.st + b;
+  double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb, *red = sm + 3 * nb;
+  const double *t = tab + (size_t)b * 3 * B2E_CSR_MAX_BINS;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    hist[i] = t[i];
+    deriv[i] = t[B2E_CSR_MAX_BINS + i];
+    denom[i] = t[2 * B2E_CSR_MAX_BINS + i];
+  }
+  __syncthreads();
+  const double csr_constant = B.csr_const[b];
+  const double c1 = csr_constant * a.length / a.nSlices;
+  const double c2 = -csr_constant * a.length / a.nSlices / a.slippage13;
+  const double total = scal[b * 4 + 0], k = scal[b * 4 + 1], dct = scal[b * 4 + 2];
+  double *wl = a.wakelog ? a.wakelog + (size_t)b * nb : nullptr;
+  if (!(dct > 0) || !csr_constant) {
+    for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+      st->dGamma[ib] = 0;
+      if (wl)
+        wl[ib] = 0;
+    }
+    return;
+  }
+  long long diS, diS4;
+  slippage_bins(a, dct, &diS, &diS4);
+  const double unit = 1.0 / dct / b2e_pow13(dct); /* dct^(-4/3) */
+  const float *yb = y + (size_t)b * L;
+  /* gate */
+  double e2 = 0, w2 = 0;
+  if (diS > 0)
+    for (int ib = start + threadIdx.x * stride; ib < nb; ib += blockDim.x * stride) {
+      double T1p, T2;
+      wake_terms(ib, a, dct, hist, deriv, denom, diS, diS4, &T1p, &T2);
+      const double T1s = (double)yb[ib] / sc_target / k * total * unit;
+      const double d = (T1s - T1p) * c1, wp = T1p * c1 + T2 * c2;
+      e2 += d * d;
+      w2 += wp * wp;
+    }
+  e2 = block_sum(e2, red);
+  w2 = block_sum(w2, red);
+  const double err = diS > 0 ? (w2 > 0 ? sqrt(e2 / w2) : (e2 > 0 ? INFINITY : 0.0)) : 0.0;
+  const bool plain = !(err <= tol);
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double T1, T2;
+    if (plain) {
+      wake_terms(ib, a, dct, hist, deriv, denom, diS, diS4, &T1, &T2);
+    } else {
+      T1 = diS > 0 ? (double)yb[ib] / sc_target / k * total * unit : 0.0;
+      T2 = 0;
+      if ((ib + diS) < nb)
+        T2 += hist[ib + diS];
+      if ((ib + diS4) < nb)
+        T2 -= hist[ib + diS4];
+    }
+    T1 *= c1;
+    T2 *= c2;
+    const double dg = T1 + T2;
+    st->dGamma[ib] = dg;
+    if (wl)
+      wl[ib] = dg;
+  }
+  if (threadIdx.x == 0) {
+    gate_log[b] = err;
+    atomicAdd(&counters[0], 1ull);
+    if (plain)
+      atomicAdd(&counters[1], 1ull);
+  }
 }
 
 /* Batched wake integral of many profiles in bin units (dct = 1), one CTA per
@@ -760,6 +938,9 @@ int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vect
 void csr_reset(CsrState &st) {
   st.wakes_host.clear();
   st.wake_values = 0;
+  st.gate_values = 0;
+  if (st.d_sur_counts)
+    cudaMemset(st.d_sur_counts, 0, 2 * sizeof(unsigned long long));
   st.accumulated_angle = 0;
   st.wake_valid.assign(st.n_bunches, 0);
 }
@@ -788,6 +969,50 @@ static int ensure_wakelog(CsrState &st, int64_t values) {
       return B2E_ERR_CUDA;                                                                                       \
     }                                                                                                            \
   } while (0)
+
+static int ensure_surrogate_buffers(CsrState &st, int64_t gate_values, std::string &err) {
+  const int nb = st.n_bunches, L = wakenet_bins(st.net);
+  if (st.sur_cap_bunches < nb) {
+    cudaFree(st.d_sur_in);
+    cudaFree(st.d_sur_out);
+    cudaFree(st.d_sur_tab);
+    cudaFree(st.d_sur_scal);
+    st.d_sur_in = st.d_sur_out = nullptr;
+    st.d_sur_tab = st.d_sur_scal = nullptr;
+    st.sur_cap_bunches = 0;
+    if (cudaMalloc(&st.d_sur_in, sizeof(float) * 4 * L * nb) != cudaSuccess ||
+        cudaMalloc(&st.d_sur_out, sizeof(float) * L * nb) != cudaSuccess ||
+        cudaMalloc(&st.d_sur_tab, sizeof(double) * 3 * B2E_CSR_MAX_BINS * nb) != cudaSuccess ||
+        cudaMalloc(&st.d_sur_scal, sizeof(double) * 4 * nb) != cudaSuccess) {
+      err = "CSR: wake network buffers";
+      return B2E_ERR_NOMEM;
+    }
+    st.sur_cap_bunches = nb;
+  }
+  if (!st.d_sur_counts) {
+    if (cudaMalloc(&st.d_sur_counts, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+      err = "CSR: wake network buffers";
+      return B2E_ERR_NOMEM;
+    }
+    cudaMemset(st.d_sur_counts, 0, 2 * sizeof(unsigned long long));
+  }
+  if (st.gate_values + gate_values > st.gate_cap) {
+    const int64_t cap = std::max<int64_t>(2 * st.gate_cap, st.gate_values + gate_values);
+    double *p = nullptr;
+    if (cudaMalloc(&p, sizeof(double) * cap) != cudaSuccess) {
+      err = "CSR: gate log";
+      return B2E_ERR_NOMEM;
+    }
+    if (st.d_gate_log) {
+      if (st.gate_values)
+        cudaMemcpy(p, st.d_gate_log, sizeof(double) * st.gate_values, cudaMemcpyDeviceToDevice);
+      cudaFree(st.d_gate_log);
+    }
+    st.d_gate_log = p;
+    st.gate_cap = cap;
+  }
+  return B2E_OK;
+}
 
 int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
                       const std::vector<int64_t> &alive, int elem, int pass, cudaStream_t stream, std::string &err,
@@ -917,6 +1142,21 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   const int *sgi = st.d_sg_idx + st.sg_offset[k] / B2E_SG_MAX_WIDTH * 2;
   const size_t wake_smem = sizeof(double) * 4 * ce.bins;
   CSR_CUDA(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wake_smem));
+  /* learned wake: trained on the transient integral with trapezoid rule (the
+   * CSRCSBEND defaults); other settings, or a bunch train larger than the
+   * network's batch, use the plain integral */
+  const bool use_net = st.net && any_active && !ce.steady && ce.trapz && ce.bins <= wakenet_bins(st.net) &&
+                       nbunch <= wakenet_max_batch(st.net);
+  const size_t sur_smem = sizeof(double) * (3 * ce.bins + 1024);
+  if (use_net) {
+    int rc = ensure_surrogate_buffers(st, (int64_t)ce.nSlices * nbunch, err);
+    if (rc)
+      return rc;
+    CSR_CUDA(cudaFuncSetAttribute(csr_sur_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)std::max(sur_smem, sizeof(double) * (4 * ce.bins + 1024))));
+    CSR_CUDA(cudaFuncSetAttribute(csr_sur_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sur_smem));
+  }
 
   csr_entry_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, Po);
   (*launches)++;
@@ -958,9 +1198,28 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     a.nSlices = ce.nSlices;
     a.c1 = a.c2 = a.csr_constant = 0; /* per bunch in the kernel */
     a.wakelog = st.d_wakelog + st.wake_values;
-    csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a);
-    (*launches)++;
-    CSR_CUDA(cudaGetLastError());
+    if (use_net) {
+      const int L = wakenet_bins(st.net);
+      csr_sur_filter_kernel<<<nbunch, 1024, std::max(sur_smem, sizeof(double) * 4 * ce.bins), stream>>>(B, st.d_counts, a, L, st.sc_dens, st.sc_deriv,
+                                                                st.d_sur_tab, st.d_sur_scal, st.d_sur_in);
+      CSR_CUDA(cudaGetLastError());
+      int rc = wakenet_infer(st.net, st.d_sur_in, nbunch, st.d_sur_out, stream);
+      if (rc) {
+        err = "CSR: wake network inference failed";
+        return rc;
+      }
+      csr_sur_combine_kernel<<<nbunch, 1024, sur_smem, stream>>>(B, a, st.d_sur_tab, st.d_sur_scal, st.d_sur_out, L,
+                                                                 st.sc_target, st.gate_tol, st.gate_stride,
+                                                                 kick % st.gate_stride, st.d_gate_log + st.gate_values,
+                                                                 st.d_sur_counts);
+      CSR_CUDA(cudaGetLastError());
+      st.gate_values += nbunch;
+      (*launches) += 3 + 7; /* filter, pack + 6 convolutions, combine */
+    } else {
+      csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a);
+      (*launches)++;
+      CSR_CUDA(cudaGetLastError());
+    }
     st.wake_values += (int64_t)ce.bins * nbunch;
   }
   csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
@@ -972,6 +1231,10 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   for (int b = 0; b < nbunch; b++)
     st.wake_valid[b] = flags[b];
   st.accumulated_angle += ce.angle;
+  if (use_net && wakenet_take_status(st.net, stream)) {
+    err = "CSR: a bounded wait in the wake network gave up";
+    return B2E_ERR_TIMEOUT;
+  }
   return B2E_OK;
 }
 
@@ -1004,6 +1267,14 @@ void csr_release(CsrState &st) {
   st.d_csr_const = nullptr;
   st.d_flags = nullptr;
   st.d_alive = nullptr;
+  void *sur[] = {st.d_sur_in, st.d_sur_out, st.d_sur_tab, st.d_sur_scal, st.d_gate_log, st.d_sur_counts};
+  for (void *q : sur)
+    if (q)
+      cudaFree(q);
+  st.d_sur_in = st.d_sur_out = nullptr;
+  st.d_sur_tab = st.d_sur_scal = st.d_gate_log = nullptr;
+  st.d_sur_counts = nullptr;
+  st.sur_cap_bunches = st.gate_cap = st.gate_values = 0;
   if (st.d_sg)
     cudaFree(st.d_sg);
   if (st.d_sg_idx)

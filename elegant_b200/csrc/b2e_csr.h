@@ -65,6 +65,21 @@ struct CsrState {
   double *d_wakelog = nullptr;
   int64_t wakelog_cap = 0;
   double ds0 = 0, zLast = 0, z0 = 0;
+  /* learned wake integral (optional): a trained wake network replaces the T1
+   * integral of CSRCSBEND kicks, checked on every kick against the plain
+   * integral at every gate_stride-th bin; above gate_tol relative rms error
+   * of the wake the kick falls back to the plain wake */
+  b2e_wakenet *net = nullptr;
+  float sc_dens = 1, sc_deriv = 1, sc_target = 1;
+  double gate_tol = 0.01;
+  int gate_stride = 16;
+  float *d_sur_in = nullptr, *d_sur_out = nullptr; /* [n_bunches][4][L], [n_bunches][L] */
+  double *d_sur_tab = nullptr;                     /* [n_bunches][3][B2E_CSR_MAX_BINS] */
+  double *d_sur_scal = nullptr;                    /* [n_bunches][4] */
+  int64_t sur_cap_bunches = 0;
+  double *d_gate_log = nullptr;                    /* one relative error per (kick, bunch) */
+  int64_t gate_cap = 0, gate_values = 0;
+  unsigned long long *d_sur_counts = nullptr;      /* evaluations, fallbacks */
 };
 
 int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLattice &lat, const b2e_run_options &opt,

@@ -647,8 +647,9 @@ cudaError_t refresh_weights(b2e_wakenet *n, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-/* forward pass of n_prof profiles; keeps the pre-activations when train */
-int forward(b2e_wakenet *n, const float *inputs, int n_prof, bool train, cudaStream_t s) {
+/* forward pass of n_prof profiles; keeps the pre-activations when train;
+ * the output goes to y_out (the network's own buffer when null) */
+int forward(b2e_wakenet *n, const float *inputs, int n_prof, bool train, cudaStream_t s, float *y_out = nullptr) {
   const int64_t rows = (int64_t)n_prof * n->L;
   wn_pack_kernel<<<(int)((rows + 255) / 256), 256, 0, s>>>(inputs, n->L, rows, n->x0);
   WN_TRY(n, cudaGetLastError());
@@ -668,7 +669,7 @@ int forward(b2e_wakenet *n, const float *inputs, int n_prof, bool train, cudaStr
       a.a_out = n->act[l];
       WN_TRY(n, launch_conv(EPI_HIDDEN, tin, n->t_wk[l], a, grid, s));
     } else {
-      a.y_out = n->y;
+      a.y_out = y_out ? y_out : n->y;
       WN_TRY(n, launch_conv(EPI_OUTPUT, tin, n->t_wk[l], a, grid, s));
     }
   }
@@ -734,6 +735,25 @@ int check_status(b2e_wakenet *n, cudaStream_t s) {
 }
 
 } // namespace
+
+namespace b2e {
+int wakenet_infer(b2e_wakenet *net, const float *dev_inputs, int n_prof, float *dev_out, cudaStream_t s) {
+  if (!net || n_prof < 0 || n_prof > net->max_batch)
+    return B2E_ERR_ARG;
+  return n_prof ? forward(net, dev_inputs, n_prof, false, s, dev_out) : B2E_OK;
+}
+int wakenet_bins(const b2e_wakenet *net) { return net ? net->L : 0; }
+int wakenet_max_batch(const b2e_wakenet *net) { return net ? net->max_batch : 0; }
+unsigned int wakenet_take_status(b2e_wakenet *net, cudaStream_t s) {
+  unsigned int st = 0;
+  if (cudaMemcpyAsync(&st, net->status, sizeof(st), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return ~0u;
+  if (st)
+    cudaMemsetAsync(net->status, 0, sizeof(unsigned int), s);
+  return st;
+}
+} // namespace b2e
 
 extern "C" int b2e_wakenet_create(b2e_wakenet **out, int32_t bins, int32_t max_batch, const int32_t *dilations,
                                   int32_t device) {

@@ -8,6 +8,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "elegant_b200.h"
 
 namespace b2e {
 
@@ -39,6 +40,15 @@ struct WgradArgs {
   float *partial; /* [gridDim.x][5][64 ci][64 co] */
   unsigned int *status;
 };
+
+/* Inference on device buffers without a host synchronisation (the status
+ * word is read by wakenet_take_status).  B2E_ERR_ARG if the batch or the bin
+ * count does not fit the network. */
+int wakenet_infer(b2e_wakenet *net, const float *dev_inputs, int n_prof, float *dev_out, cudaStream_t s);
+int wakenet_bins(const b2e_wakenet *net);
+int wakenet_max_batch(const b2e_wakenet *net);
+/* status word of the network's kernels (nonzero: a bounded wait gave up), then cleared */
+unsigned int wakenet_take_status(b2e_wakenet *net, cudaStream_t s);
 
 cudaError_t launch_conv(int epi, const CUtensorMap &t_in, const CUtensorMap &t_w, const ConvArgs &a, int grid,
                         cudaStream_t s);

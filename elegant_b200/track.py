@@ -190,6 +190,28 @@ class Tracker:
                                                                 ("survivors", "cx", "cy", "ex", "ey"))))
         return out
 
+    def set_csr_surrogate(self, surrogate, tolerance: float = 0.01, gate_stride: int = 16):
+        """Use a trained wake surrogate (elegant_b200.wake_surrogate.WakeSurrogate)
+        for the CSRCSBEND wake integral, gated by the plain integral on every
+        gate_stride-th bin with fallback above `tolerance`; None switches back."""
+        if surrogate is None:
+            self._check(self.lib.b2e_set_csr_surrogate(self._ctx, None, None, 0.0, 1))
+            self._surrogate = None
+            return
+        f = surrogate.features
+        sc = (ctypes.c_double * 3)(f.dens_scale, f.deriv_scale, f.target_scale)
+        self._check(self.lib.b2e_set_csr_surrogate(self._ctx, surrogate.net._h, sc, tolerance, gate_stride))
+        self._surrogate = surrogate  # keeps the network alive while bound
+
+    def csr_surrogate_stats(self) -> dict:
+        ev, fb, wr = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.b2e_csr_surrogate_stats(self._ctx, ctypes.byref(ev), ctypes.byref(fb), None, 0,
+                                                     ctypes.byref(wr)))
+        errs = np.zeros(max(wr.value, 1))
+        self._check(self.lib.b2e_csr_surrogate_stats(self._ctx, ctypes.byref(ev), ctypes.byref(fb),
+                                                     errs.ctypes.data, wr.value, ctypes.byref(wr)))
+        return {"evaluations": ev.value, "fallbacks": fb.value, "gate_errors": errs[: wr.value]}
+
     def csr_wakes(self, capacity: int) -> np.ndarray:
         buf = np.empty(capacity, dtype=np.float64)
         written = ctypes.c_int64()

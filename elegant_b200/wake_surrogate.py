@@ -41,7 +41,9 @@ MM = 1e-3
 def sample_profile_params(n: int, seed: int):
     """Gaussian mixtures (1-4 components), sigma 0.2-2 mm, centres within
     +-3 mm, Dirichlet(1) weights; bend radius 5-50 m; particle count
-    log-uniform 0.5M-4M; slippage (in bins) log-uniform in [1, 2 * bins]."""
+    log-uniform 0.5M-4M; slippage (in bins) log-uniform in [1, 2 * bins];
+    binning window widened by a factor 1.2-2.2 (tracking bins a bunch on its
+    own extent, and a histogram of fewer bins than the network's is padded)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     k = rng.integers(1, 5, size=n)
     sig = rng.uniform(0.2, 2.0, size=(n, 4)) * MM
@@ -52,14 +54,14 @@ def sample_profile_params(n: int, seed: int):
     rho = rng.uniform(5.0, 50.0, size=n)
     npart = np.exp(rng.uniform(np.log(5e5), np.log(4e6), size=n))
     slip_u = rng.uniform(0, 1, size=n)
-    return dict(k=k, sigma=sig, centre=cen, weight=w, rho=rho, n_particles=npart, slip_u=slip_u)
+    widen = rng.uniform(1.2, 2.2, size=n)
+    return dict(k=k, sigma=sig, centre=cen, weight=w, rho=rho, n_particles=npart, slip_u=slip_u, widen=widen)
 
 
-def make_histograms(params: dict, bins: int, seed: int, device="cuda", range_factor: float = 1.2,
-                    chunk: int = 16384):
+def make_histograms(params: dict, bins: int, seed: int, device="cuda", chunk: int = 16384):
     """Bin-integrated mixture densities on each profile's own window (the
-    +-4.5 sigma extent of its components, widened by range_factor as the
-    tracking binning is), times the particle count, plus Gaussian shot noise
+    +-4.5 sigma extent of its components, widened by the profile's factor),
+    times the particle count, plus Gaussian shot noise
     of variance = count.  Returns (counts [n][bins] float64, slippage in bins,
     bin width in m).  Works in chunks of `chunk` profiles, each with its own
     seeded noise stream."""
@@ -75,7 +77,8 @@ def make_histograms(params: dict, bins: int, seed: int, device="cuda", range_fac
         live = w > 0
         lo = torch.where(live, cen - 4.5 * sig, torch.full_like(cen, 1e9)).min(dim=1).values
         hi = torch.where(live, cen + 4.5 * sig, torch.full_like(cen, -1e9)).max(dim=1).values
-        mid, half = (lo + hi) / 2, (hi - lo) / 2 * range_factor
+        widen = torch.tensor(params["widen"][c0:c1], dtype=torch.float64, device=device)
+        mid, half = (lo + hi) / 2, (hi - lo) / 2 * widen
         lo = mid - half
         dct = 2 * half / bins
         edges = lo[:, None] + dct[:, None] * ar

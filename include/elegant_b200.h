@@ -298,6 +298,26 @@ int b2e_wakenet_gradients(b2e_wakenet *net, const float *dev_inputs, const float
 int b2e_wakenet_train_step(b2e_wakenet *net, const float *dev_inputs, const float *dev_targets, int32_t n, float lr,
                            double *loss, void *stream);
 
+/* ---- learned CSR wake in tracking --------------------------------------
+ * Binds a trained wake network to a tracking context (net = NULL unbinds).
+ * For CSRCSBEND kicks with the transient integral and the trapezoid rule
+ * (the defaults), BINS <= the network's bins and at most its batch of
+ * bunches, the network replaces the T1 integral of the kick wake; the T2
+ * term, the filters and the kick stay exact.  feature_scales = the density,
+ * derivative and target scales the network was trained with.  Every kick is
+ * checked: the plain integral is evaluated at every gate_stride-th bin (a
+ * different offset each kick) and, if the relative rms error of the wake
+ * there exceeds tolerance, the kick uses the plain wake (bit-identical to the
+ * plain path).  The network must outlive its use by the context.  No
+ * counterpart in the reference. */
+int b2e_set_csr_surrogate(b2e_ctx *ctx, b2e_wakenet *net, const double feature_scales[3], double tolerance,
+                          int32_t gate_stride);
+/* Since the last run start: network wake evaluations (kicks x bunches),
+ * fallbacks to the plain wake, and the gate's relative error of each
+ * evaluation (in kick order, bunches within a kick; NULL to query *written). */
+int b2e_csr_surrogate_stats(b2e_ctx *ctx, int64_t *evaluations, int64_t *fallbacks, double *gate_errors,
+                            int64_t capacity, int64_t *written);
+
 /* ---- tensor-core self-test ---------------------------------------------
  * Runs one UMMA tile on device buffers to check the operand layouts the wake
  * network uses.  mode 0: D[128][64] = A[128][64] . B[64][64]^T; mode 1:

@@ -105,3 +105,48 @@ def test_bunch_train_matches_single_bunches(ref_b2e, drift_kicks):
         assert np.array_equal(sub.coords[order][alive], ref_c[alive]), b
         if sizes[b] > 1:
             assert np.array_equal(wakes[:, b, :].ravel(), ref_wakes), b
+
+
+def _surrogate():
+    import os
+    from elegant_b200.wake_surrogate import WakeSurrogate
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "elegant_b200", "data",
+                        "wakenet_1024.npz")
+    return WakeSurrogate.load(path, max_batch=16)
+
+
+def test_surrogate_zero_tolerance_is_the_plain_wake():
+    """With tolerance 0 every kick whose integral is not empty falls back, and
+    the fallback is the plain wake bit for bit; kicks with an empty integral
+    (slippage under one bin) are exact in both paths."""
+    lat = w.chicane(bins=200, n_kicks=6)
+    beam = w.chicane_beam(20000, seed=31)
+    with Tracker(lat, P0, 1) as t:
+        plain = t.track(beam)
+        plain_w = t.csr_wakes(10_000_000)
+    sur = _surrogate()
+    with Tracker(lat, P0, 1) as t:
+        t.set_csr_surrogate(sur, tolerance=0.0, gate_stride=8)
+        res = t.track(beam)
+        wk = t.csr_wakes(10_000_000)
+        stats = t.csr_surrogate_stats()
+    assert np.array_equal(wk, plain_w)
+    assert np.array_equal(res.coords, plain.coords)
+    assert stats["evaluations"] == 4 * 6 and stats["fallbacks"] <= stats["evaluations"]
+
+
+def test_surrogate_wakes_follow_the_plain_wakes():
+    """At the default 1% gate, every kick's wake agrees with the plain wake of
+    the same histogram to the gate's tolerance (or is the plain wake)."""
+    lat = w.chicane(bins=600, n_kicks=20)
+    beam = w.chicane_beam(200000, seed=32)
+    sur = _surrogate()
+    with Tracker(lat, P0, 1) as t:
+        t.set_csr_surrogate(sur, tolerance=0.01, gate_stride=16)
+        t.track(beam)
+        stats = t.csr_surrogate_stats()
+    errs = stats["gate_errors"]
+    assert stats["evaluations"] == 80 and errs.size == 80
+    assert np.all(np.isfinite(errs))
+    # the fallback count is what the gate decided
+    assert stats["fallbacks"] == int((errs > 0.01).sum())
