@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-history", action="store_true", help="do not record the per-instance pass history")
     ap.add_argument("--ring-variant", type=int, default=0, help="0 = autotune, else a fixed ring-kernel variant")
     ap.add_argument("--csr-particles", type=int, default=1_000_000)
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the wake-network evaluation")
+    ap.add_argument("--no-bunch-train", action="store_true", help="skip the 16-bunch chicane")
     return ap.parse_args()
 
 
@@ -93,6 +95,34 @@ def csr_section(args, device, flush):
             "run_ms": ms, "csr_pass_ms_per_kick": ms / kicks,
             "particle_kicks_per_s": beam.n * kicks / (ms / 1e3),
             "timing": "CUDA events on the engine stream; includes CSRDRIFT kicks and the one host sync per CSR element"}
+
+
+def surrogate_section(args):
+    """Secondary figure: the shipped wake network (elegant_b200/data) on 10,000
+    fresh profiles (a seed the training never used): rms wake error against
+    the FP64 integral, and device time of the surrogate path against the
+    plain integral (batched and one profile)."""
+    import json as _json
+
+    from elegant_b200 import wake_surrogate as ws
+    from elegant_b200.bunch_train import DEFAULT_NET
+
+    sur = ws.WakeSurrogate.load(DEFAULT_NET, max_batch=256)
+    data = ws.build_set(10_000, sur.features.bins, seed=9001)
+    ev = ws.evaluate(sur, data)
+    meta = _json.load(open(DEFAULT_NET.replace(".npz", ".json")))
+    return {"workload": "wake network, 1024 bins, 6 conv layers x 64 channels x 5 taps, BF16/FP32 on tcgen05",
+            "eval": ev, "timing_batch": ws.timing(sur, data, 8192), "timing_single": ws.timing(sur, data, 1, reps=50),
+            "training": {k: meta[k] for k in ("train_profiles", "epochs", "train_s", "train_step_ms", "steps")}}
+
+
+def bunch_train_section(args):
+    """Secondary figure: 16 bunches (0.5-4 M particles, chirp -15..-5 /m)
+    through the CSR chicane in one run, plain FP64 wake against the learned
+    wake with its per-kick gate (1 %)."""
+    from elegant_b200 import bunch_train
+
+    return bunch_train.run(reps=2, warmup=1)
 
 
 # ---------------------------------------------------------------- clocks ----
@@ -325,6 +355,8 @@ def main():
                "ms_per_step": sum(e2e_ms) / len(e2e_ms), "timing": "host wall clock around the blocking C-ABI call"}
 
     csr = None if args.no_csr else csr_section(args, local_rank, flush)
+    surrogate = None if (args.no_surrogate or world > 1) else surrogate_section(args)
+    train = None if (args.no_bunch_train or world > 1) else bunch_train_section(args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,7 +386,7 @@ def main():
                          "flops_per_particle_turn": fpt,
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.mm float64), best of 3"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
-            "csr": csr,
+            "csr": csr, "wake_surrogate": surrogate, "bunch_train": train,
         }
         print(json.dumps(line))
     if dist:
