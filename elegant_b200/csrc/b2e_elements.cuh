@@ -275,7 +275,14 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
         const double ds = c[CB_DS0 + j];
         /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
         QX = QX + ((((-ds) * (1 + X / rho0)) * 1.0) / rho_actual);
-        QY = QY + ((((ds) * (1 + X / rho0)) * 0.0) / rho_actual);
+        {
+          /* (t * Fx) / rho_actual with Fx = 0 is a signed zero (NaN for a
+           * non-finite t): the sign of t * 0.0 flipped by rho_actual's, which
+           * is finite and nonzero in a bend -- the same value without the
+           * division */
+          const double z = ((ds) * (1 + X / rho0)) * 0.0;
+          QY = QY + (rho_actual < 0 ? -z : z);
+        }
         if (isr_block) {
           QX = QX / (1 + DPoP);
           QY = QY / (1 + DPoP);

@@ -13,10 +13,11 @@
  *  - sin/cos: Cody & Waite (1980) additive range reduction by pi/2 split into
  *    three doubles (the first product is exact under fma), then the Taylor
  *    series of sin and cos on |r| <= pi/4 truncated where the remainder is
- *    below 2^-60 relative; 1 - r^2/2 is evaluated with the compensated
+ *    below 2^-60 relative -- on |r| <= 2^-4 that is four terms of each
+ *    series, beyond it ten; 1 - r^2/2 is evaluated with the compensated
  *    splitting used by Sun's fdlibm kernel cosine.
  *  - asin: Taylor series  asin(x) = sum C(2n,n) x^(2n+1) / (4^n (2n+1))  on
- *    |x| <= 1/2 (10 terms for |x| <= 1/8, 28 terms beyond), and
+ *    |x| <= 1/2 (4 terms for |x| <= 2^-6, 10 for |x| <= 1/8, 28 beyond), and
  *    asin(x) = pi/2 - 2 asin(sqrt((1-x)/2)) for 1/2 < |x| <= 1.
  *  - tan = sin/cos from the shared reduction.
  *  - pow(x, 1/3.) (the CSR denominators, csbend.c:2575) is in b2e_csr_math.h.
@@ -75,6 +76,31 @@ B2E_HD double b2e_cos_kernel(double r) {
   return t + (((1.0 - t) - hw) + (w * w) * q);
 }
 
+/* The same series truncated for |r| <= 2^-4, where the first dropped term is
+ * below 2^-60 relative: sin to r^9 (next: r^10/11! < 2.3e-20), cos to r^8
+ * (next: r^10/10! < 2.6e-19). */
+B2E_HD double b2e_sin_kernel_small(double r) {
+  double w = r * r, p;
+  p = 1.0 / 362880.0;                /* 1/9! */
+  p = b2e_fma(p, w, -1.0 / 5040.0);  /* -1/7! */
+  p = b2e_fma(p, w, 1.0 / 120.0);    /* 1/5! */
+  p = b2e_fma(p, w, -1.0 / 6.0);     /* -1/3! */
+  return b2e_fma(r * w, p, r);
+}
+
+B2E_HD double b2e_cos_kernel_small(double r) {
+  double w = r * r, q, hw, t;
+  q = 1.0 / 40320.0;               /* 1/8! */
+  q = b2e_fma(q, w, -1.0 / 720.0); /* -1/6! */
+  q = b2e_fma(q, w, 1.0 / 24.0);   /* 1/4! */
+  hw = 0.5 * w;
+  t = 1.0 - hw;
+  return t + (((1.0 - t) - hw) + (w * w) * q);
+}
+
+B2E_HD double b2e_sin_r(double r) { return fabs(r) <= 0x1p-4 ? b2e_sin_kernel_small(r) : b2e_sin_kernel(r); }
+B2E_HD double b2e_cos_r(double r) { return fabs(r) <= 0x1p-4 ? b2e_cos_kernel_small(r) : b2e_cos_kernel(r); }
+
 /* Reduce x to r in [-pi/4, pi/4] and the quadrant k mod 4. */
 B2E_HD double b2e_reduce_pio2(double x, int *quadrant) {
   double k, r;
@@ -93,8 +119,8 @@ B2E_HD double b2e_reduce_pio2(double x, int *quadrant) {
 B2E_HD void b2e_sincos(double x, double *s, double *c) {
   int q;
   double r = b2e_reduce_pio2(x, &q), sr, cr;
-  sr = b2e_sin_kernel(r);
-  cr = b2e_cos_kernel(r);
+  sr = b2e_sin_r(r);
+  cr = b2e_cos_r(r);
   switch (q) {
   case 0:
     *s = sr;
@@ -126,7 +152,7 @@ B2E_HD double b2e_sin(double x) {
   double r = b2e_reduce_pio2(x, &q), v;
   if (x != x)
     return x;
-  v = (q & 1) ? b2e_cos_kernel(r) : b2e_sin_kernel(r);
+  v = (q & 1) ? b2e_cos_r(r) : b2e_sin_r(r);
   return (q & 2) ? -v : v;
 }
 
@@ -135,7 +161,7 @@ B2E_HD double b2e_cos(double x) {
   double r = b2e_reduce_pio2(x, &q), v;
   if (x != x)
     return x;
-  v = (q & 1) ? b2e_sin_kernel(r) : b2e_cos_kernel(r);
+  v = (q & 1) ? b2e_sin_r(r) : b2e_cos_r(r);
   return (q == 1 || q == 2) ? -v : v;
 }
 
@@ -143,6 +169,17 @@ B2E_HD double b2e_tan(double x) {
   double s, c;
   b2e_sincos(x, &s, &c);
   return s / c;
+}
+
+/* asin(x) - x = x^3 * P(x^2) for |x| <= 2^-6 to n = 4 (next term below
+ * 2^-60 relative: 0.0224 x^10 < 2e-20) */
+B2E_HD double b2e_asin_tiny(double x) {
+  double w = x * x, p;
+  p = (70.0 / 9.0) * 0x1p-8;                 /* n=4 */
+  p = b2e_fma(p, w, (20.0 / 7.0) * 0x1p-6);  /* n=3 */
+  p = b2e_fma(p, w, (6.0 / 5.0) * 0x1p-4);   /* n=2 */
+  p = b2e_fma(p, w, (2.0 / 3.0) * 0x1p-2);   /* n=1 */
+  return b2e_fma(x * w, p, x);
 }
 
 /* asin(x) - x = x^3 * P(x^2) for |x| <= 1/8; coefficients C(2n,n)/((2n+1) 4^n), n = 1..10 */
@@ -235,6 +272,8 @@ B2E_HD double b2e_pow(double x, double y) { return y == 1.0 / 3.0 ? b2e_pow13(x)
 
 B2E_HD double b2e_asin(double x) {
   double a = fabs(x), r;
+  if (a <= 0x1p-6)
+    return b2e_asin_tiny(x);
   if (a <= 0.125)
     return b2e_asin_small(x);
   if (a <= 0.5)

@@ -18,7 +18,9 @@ def ulp_error(got, exact):
 
 @pytest.mark.parametrize("fn,lo,hi,bound", [
     ("sin", -0.8, 0.8, 1.0), ("cos", -0.8, 0.8, 1.0), ("sin", -1e6, 1e6, 1.5), ("cos", -50.0, 50.0, 1.5),
-    ("asin", -0.125, 0.125, 0.6), ("asin", -0.5, 0.5, 0.7), ("asin", -1.0, 1.0, 2.5), ("tan", -0.7, 0.7, 2.0)])
+    ("asin", -0.125, 0.125, 0.6), ("asin", -0.5, 0.5, 0.7), ("asin", -1.0, 1.0, 2.5), ("tan", -0.7, 0.7, 2.0),
+    ("sin", -0.0625, 0.0625, 0.6), ("cos", -0.0625, 0.0625, 0.6), ("asin", -0.015625, 0.015625, 0.6),
+    ("sin", 0.0625, 0.07, 0.6), ("cos", 0.0625, 0.07, 0.6), ("asin", 0.015625, 0.02, 0.6)])
 def test_ulp_error(fn, lo, hi, bound):
     o = PortOracle("b2e")
     f = getattr(o.lib, f"b2e_oracle_{fn}")
