@@ -42,6 +42,20 @@ def test_ring_bit_exact_100_turns(ref_b2e):
     assert res.effort == eff
 
 
+def test_ring_bit_exact_1000_turns(ref_b2e):
+    """The single-ring workload's 1,000 turns: every survivor coordinate
+    bit-identical to the reference's own tracking (shared elementary
+    functions) and the same (ID, loss turn) set, on a sample of its beam."""
+    lat = w.fodo_ring()
+    full = w.ring_beam(10000, seed=12345)
+    idx = np.linspace(0, 9999, 160).astype(int)
+    beam = Beam(full.coords[idx], full.ids[idx])
+    res = gpu_track(lat, beam, w.ring_p_central(), 1000)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 1000)
+    assert_parity(res, rows, nl)
+    assert res.effort == eff
+
+
 def test_ring_losses_match(ref_b2e):
     """Large-amplitude and off-momentum particles hit the 20 mm aperture,
     the slope limit and the sextupole dynamic aperture."""
