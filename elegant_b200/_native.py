@@ -25,7 +25,7 @@ ERRORS = {
 # element type codes (include/elegant_b200.h)
 DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT = range(1, 12)
 MAX_PARAMS = 40
-RING_VARIANTS = 12
+RING_VARIANTS = 17
 
 EXPORTED = [
     "b2e_create", "b2e_destroy", "b2e_last_error", "b2e_version", "b2e_load_lattice",

@@ -427,6 +427,7 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.n_elems = ne;
   L.n_aps = (int)ctx->lat.aps.size();
   L.n_rf = ctx->lat.n_rf;
+  L.n_tiles = (int)ctx->tiles.size();
   L.g.p_central = ctx->opt.p_central;
   L.g.coord_limit = ctx->opt.coord_limit;
   L.g.slope_limit = ctx->opt.slope_limit;

@@ -16,6 +16,7 @@ struct RingLaunch {
   const DevAperture *aps;   /* [n_inst][n_aps] */
   const DevRfState *rf;     /* [n_inst][n_rf] */
   int n_elems, n_aps, n_rf;
+  int n_tiles;
   int pass_begin, elem_begin; /* first (pass, element) tracked */
   int pass_end, elem_end;     /* last pass tracked, and one past its last element */
   DevGlobals g;

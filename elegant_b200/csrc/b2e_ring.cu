@@ -30,11 +30,14 @@ namespace b2e {
 
 /* Per-pass beam moments of one tile, for the ensemble history: count, means
  * of x, xp, y, yp, then sums of squared deviations (x, xp, xx', y, yp, yy')
- * about the tile means -- two block reductions in a fixed order, so the
- * result does not depend on scheduling.  Every thread of the block calls it. */
+ * about the tile means -- two reductions over the tile's four warps in a
+ * fixed order, so the result does not depend on scheduling.  Every thread of
+ * the block calls it; the 128-thread group g of the block reduces its own
+ * tile and writes it to out (when out is not null). */
 __device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *out) {
-  __shared__ double red[4][12];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double red_all[8][4][12];
+  const int lane = threadIdx.x & 31, warp = (threadIdx.x >> 5) & 3;
+  double(*red)[12] = red_all[threadIdx.x >> 7];
   double v[5] = {alive ? 1.0 : 0.0, alive ? p.x : 0.0, alive ? p.xp : 0.0, alive ? p.y : 0.0, alive ? p.yp : 0.0};
   for (int k = 0; k < 5; k++)
     for (int off = 16; off > 0; off >>= 1)
@@ -60,7 +63,7 @@ __device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *
     for (int k = 0; k < 6; k++)
       red[warp][5 + k] = q[k];
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if ((threadIdx.x & 127) == 0 && out) {
     out[0] = n;
     for (int k = 0; k < 4; k++)
       out[1 + k] = m[k];
@@ -79,34 +82,43 @@ __device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *
  * memory record.  The arithmetic is identical in every variant.  HIST records
  * the per-pass tile moments (it needs SYNC >= 1); when SYNC >= 1 every thread
  * stays in the pass loop until the whole tile is lost. */
-template <bool STAGED, int MINB, int SYNC, bool HIST>
-__global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
+template <bool STAGED, int MINB, int SYNC, bool HIST, int TPB>
+__global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
   static_assert(!HIST || SYNC >= 1, "history needs the per-pass barrier");
+  static_assert(TPB == 1 || ((TPB == 2 || TPB == 4 || TPB == 8) && SYNC >= 1), "tiles of a block run in step");
   extern __shared__ __align__(16) unsigned char smem[];
-  const DevTile tile = L.tiles[blockIdx.x];
+  /* TPB tiles per block, 128 threads each; a missing second tile (odd tile
+   * count) leaves its threads idle but inside the barriers */
+  const int group = TPB == 1 ? 0 : (int)(threadIdx.x >> 7), lt = threadIdx.x & 127;
+  (void)group;
+  const int tidx = blockIdx.x * TPB + group;
+  DevTile tile = {0, 0, 0};
+  if (tidx < L.n_tiles)
+    tile = L.tiles[tidx];
   const DevElem *elems = L.elems + (size_t)tile.inst * L.n_elems;
   const DevAperture *aps = L.aps + (size_t)tile.inst * L.n_aps;
   const DevRfState *rf = L.rf + (size_t)tile.inst * L.n_rf;
 
   if (STAGED) {
-    /* stage this instance's element and aperture records in shared memory */
-    DevElem *se = reinterpret_cast<DevElem *>(smem);
-    DevAperture *sa = reinterpret_cast<DevAperture *>(smem + sizeof(DevElem) * L.n_elems);
+    /* stage this tile's instance's element and aperture records in shared memory */
+    const size_t stage = sizeof(DevElem) * L.n_elems + sizeof(DevAperture) * L.n_aps;
+    DevElem *se = reinterpret_cast<DevElem *>(smem + group * stage);
+    DevAperture *sa = reinterpret_cast<DevAperture *>(smem + group * stage + sizeof(DevElem) * L.n_elems);
     const int nw_e = (int)(sizeof(DevElem) * L.n_elems / 8), nw_a = (int)(sizeof(DevAperture) * L.n_aps / 8);
     const double *src_e = reinterpret_cast<const double *>(elems);
     const double *src_a = reinterpret_cast<const double *>(aps);
     double *dst_e = reinterpret_cast<double *>(se), *dst_a = reinterpret_cast<double *>(sa);
-    for (int i = threadIdx.x; i < nw_e; i += blockDim.x)
+    for (int i = lt; i < nw_e; i += 128)
       dst_e[i] = src_e[i];
-    for (int i = threadIdx.x; i < nw_a; i += blockDim.x)
+    for (int i = lt; i < nw_a; i += 128)
       dst_a[i] = src_a[i];
     __syncthreads();
     elems = se;
     aps = sa;
   }
 
-  const int64_t ip = tile.start + threadIdx.x;
-  const bool tracked = (int)threadIdx.x < tile.count && L.P.lost_pass[ip] < 0;
+  const int64_t ip = tile.start + lt;
+  const bool tracked = lt < tile.count && L.P.lost_pass[ip] < 0;
   if (SYNC == 0 && !tracked)
     return;
 
@@ -182,7 +194,8 @@ __global__ void __launch_bounds__(128, MINB) ring_kernel(RingLaunch L) {
       }
     }
     if (HIST && e1 == L.n_elems && pass >= L.hist_pass0)
-      tile_moments(p, active, L.hist + ((size_t)blockIdx.x * L.hist_passes + (pass - L.hist_pass0)) * 11);
+      tile_moments(p, active,
+                   tidx < L.n_tiles ? L.hist + ((size_t)tidx * L.hist_passes + (pass - L.hist_pass0)) * 11 : nullptr);
   }
 
   if (!tracked)
@@ -324,17 +337,21 @@ __global__ void effort_kernel(const int32_t *lost_pass, int64_t n, int pass_begi
   }
 }
 
-template <int MINB, int SYNC, bool HIST>
+template <int MINB, int SYNC, bool HIST, int TPB>
 static cudaError_t launch_ring_v(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
                                  cudaStream_t stream) {
+  const int grid = (n_tiles + TPB - 1) / TPB;
+  if (staged && smem_bytes * TPB > 200 * 1024)
+    staged = false; /* two instances' records do not fit: read them from global memory */
   if (staged) {
-    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB, SYNC, HIST>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    const size_t bytes = smem_bytes * TPB;
+    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB, SYNC, HIST, TPB>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess)
       return err;
-    ring_kernel<true, MINB, SYNC, HIST><<<n_tiles, 128, smem_bytes, stream>>>(L);
+    ring_kernel<true, MINB, SYNC, HIST, TPB><<<grid, 128 * TPB, bytes, stream>>>(L);
   } else {
-    ring_kernel<false, MINB, SYNC, HIST><<<n_tiles, 128, 0, stream>>>(L);
+    ring_kernel<false, MINB, SYNC, HIST, TPB><<<grid, 128 * TPB, 0, stream>>>(L);
   }
   return cudaGetLastError();
 }
@@ -344,25 +361,48 @@ static cudaError_t launch_ring_s(const RingLaunch &L, int n_tiles, bool staged, 
                                  cudaStream_t stream, int minb_index) {
   switch (minb_index) {
   case 1:
-    return launch_ring_v<5, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_v<5, SYNC, HIST, 1>(L, n_tiles, staged, smem_bytes, stream);
   case 2:
-    return launch_ring_v<6, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_v<6, SYNC, HIST, 1>(L, n_tiles, staged, smem_bytes, stream);
   case 3:
-    return launch_ring_v<8, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_v<8, SYNC, HIST, 1>(L, n_tiles, staged, smem_bytes, stream);
   default:
-    return launch_ring_v<4, SYNC, HIST>(L, n_tiles, staged, smem_bytes, stream);
+    return launch_ring_v<4, SYNC, HIST, 1>(L, n_tiles, staged, smem_bytes, stream);
   }
 }
 
-/* variant 1..12: occupancy target MINB = {4, 5, 6, 8}[(variant-1) % 4],
- * barrier level SYNC = (variant-1) / 4.  With history the barrier level is
- * at least 1. */
+template <bool HIST>
+static cudaError_t launch_ring_group(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
+                                     cudaStream_t stream, int index) {
+  switch (index) {
+  case 1:
+    return launch_ring_v<3, 2, HIST, 2>(L, n_tiles, staged, smem_bytes, stream);
+  case 2:
+    return launch_ring_v<4, 2, HIST, 2>(L, n_tiles, staged, smem_bytes, stream);
+  case 3:
+    return launch_ring_v<2, 2, HIST, 4>(L, n_tiles, staged, smem_bytes, stream);
+  case 4:
+    return launch_ring_v<1, 2, HIST, 8>(L, n_tiles, staged, smem_bytes, stream);
+  default:
+    return launch_ring_v<2, 2, HIST, 2>(L, n_tiles, staged, smem_bytes, stream);
+  }
+}
+
+/* variant 1..12: one 128-particle tile per block, occupancy target MINB =
+ * {4, 5, 6, 8}[(variant-1) % 4] blocks per SM, barrier level SYNC =
+ * (variant-1) / 4 (with history at least 1).  Variants 13..17 keep several
+ * tiles of a block in step with a barrier after every element: two tiles per
+ * 256-thread block at {2, 3, 4} blocks per SM, four tiles per 512-thread
+ * block at 2, eight tiles per 1024-thread block at 1. */
 cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
                         int variant) {
   if (n_tiles <= 0)
     return cudaSuccess;
   if (variant < 1 || variant > B2E_RING_VARIANTS)
     variant = 1;
+  if (variant > 12)
+    return L.hist ? launch_ring_group<true>(L, n_tiles, staged, smem_bytes, stream, variant - 13)
+                  : launch_ring_group<false>(L, n_tiles, staged, smem_bytes, stream, variant - 13);
   const int minb_index = (variant - 1) % 4, sync = (variant - 1) / 4;
   if (L.hist)
     return sync == 2 ? launch_ring_s<2, true>(L, n_tiles, staged, smem_bytes, stream, minb_index)

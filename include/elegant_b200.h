@@ -65,7 +65,7 @@ extern "C" {
 #define B2E_CSRDRIFT 11
 
 #define B2E_MAX_PARAMS 40
-#define B2E_RING_VARIANTS 12
+#define B2E_RING_VARIANTS 17
 
 /* Parameter slot indices, per element type.  Slot names are elegant's
  * parameter names (track_data.c tables cited per type). */

@@ -164,7 +164,7 @@ def test_kernel_variants_identical(history):
     beam = _lossy_beam(700, seed=21)
     ref = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=1)
     assert (ref.lost_pass >= 0).any() and (ref.lost_pass < 0).any()
-    for v in range(1, 13):
+    for v in range(1, 18):
         r = gpu_track(lat, beam, w.ring_p_central(), 12, ring_variant=v, record_history=history)
         assert np.array_equal(r.coords, ref.coords), v
         assert np.array_equal(r.lost_pass, ref.lost_pass), v
@@ -177,8 +177,8 @@ def test_autotuner_picks_a_variant():
     with Tracker(lat, w.ring_p_central(), 3) as t:
         t.track(beam)
         chosen, ms = t.ring_tuning()
-    assert 1 <= chosen <= 12
-    assert len(ms) == 12 and all(m > 0 for m in ms)
+    assert 1 <= chosen <= 17
+    assert len(ms) == 17 and all(m > 0 for m in ms)
 
 
 def _moments(coords, alive):
