@@ -51,6 +51,11 @@ class Override(ctypes.Structure):
     _fields_ = [("element", ctypes.c_int32), ("slot", ctypes.c_int32), ("values", ctypes.POINTER(ctypes.c_double))]
 
 
+# int (*)(void *user, int32_t op, void *dev_buf, int64_t count, void *stream)
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+                             ctypes.c_void_p)
+
+
 class EngineError(RuntimeError):
     """A C-ABI call returned a nonzero status."""
 
@@ -90,6 +95,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_stream": (vp, [vp]),
         "b2e_kernel_launches": (i64, [vp]),
         "b2e_history_passes": (i64, [vp]),
+        "b2e_set_csr_reducer": (c_int, [vp, vp, vp]),
         "b2e_set_csr_surrogate": (c_int, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
         "b2e_csr_surrogate_stats": (c_int, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp, i64,
                                             ctypes.POINTER(i64)]),

@@ -514,8 +514,13 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     csr_reset(ctx->csr);
     /* CHARGE (do_tracking.c:1324-1360): macro-particle charge = TOTAL / particles
      * at start; in an ensemble every instance is a bunch of charge TOTAL */
+    std::vector<int64_t> sizes(ctx->csr.n_bunches);
+    for (int b = 0; ctx->csr.enabled && b < ctx->csr.n_bunches; b++)
+      sizes[b] = ctx->csr.n_bunches == 1 ? ctx->n : ctx->inst_offsets[b + 1] - ctx->inst_offsets[b];
+    if (ctx->csr.enabled && csr_reduce_counts(ctx->csr, sizes, ctx->stream, ctx->err))
+      return B2E_ERR_CUDA;
     for (int b = 0; ctx->csr.enabled && b < ctx->csr.n_bunches; b++) {
-      const int64_t nb = ctx->csr.n_bunches == 1 ? ctx->n : ctx->inst_offsets[b + 1] - ctx->inst_offsets[b];
+      const int64_t nb = sizes[b];
       double q = 0;
       for (const b2e_element &el : ctx->base)
         if (el.type == B2E_CHARGE) {
@@ -791,5 +796,13 @@ extern "C" int b2e_csr_surrogate_stats(b2e_ctx *ctx, int64_t *evaluations, int64
     CUDA_TRY(ctx, cudaMemcpy(gate_errors, ctx->csr.d_gate_log, sizeof(double) * n, cudaMemcpyDeviceToHost));
   if (written)
     *written = gate_errors ? std::max<int64_t>(n, 0) : ctx->csr.gate_values;
+  return B2E_OK;
+}
+
+extern "C" int b2e_set_csr_reducer(b2e_ctx *ctx, b2e_reduce_fn fn, void *user) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  ctx->csr.reducer = fn;
+  ctx->csr.reducer_user = fn ? user : nullptr;
   return B2E_OK;
 }

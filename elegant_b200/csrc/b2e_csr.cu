@@ -696,6 +696,21 @@ __global__ void csr_reset_keys_kernel(CsrBunches B) {
   }
 }
 
+/* min/max keys of every bunch to a contiguous [2][n] buffer and back, around
+ * an all-rank reduction */
+__global__ void csr_keys_gather_kernel(CsrBunches B, unsigned long long *keys) {
+  for (int b = threadIdx.x; b < B.n; b += blockDim.x) {
+    keys[b] = B.st[b].ct_min_key;
+    keys[B.n + b] = B.st[b].ct_max_key;
+  }
+}
+__global__ void csr_keys_scatter_kernel(CsrBunches B, const unsigned long long *keys) {
+  for (int b = threadIdx.x; b < B.n; b += blockDim.x) {
+    B.st[b].ct_min_key = keys[b];
+    B.st[b].ct_max_key = keys[B.n + b];
+  }
+}
+
 __global__ void csr_s0_add_kernel(CsrBunches B, double incr) {
   for (int b = threadIdx.x; b < B.n; b += blockDim.x)
     if (B.mode[b])
@@ -876,6 +891,9 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
     cudaFree(st.d_flags);
   if (st.d_alive)
     cudaFree(st.d_alive);
+  if (st.d_keys)
+    cudaFree(st.d_keys);
+  st.d_keys = nullptr;
   st.d_state = nullptr;
   st.d_counts = nullptr;
   st.d_csr_const = nullptr;
@@ -889,7 +907,8 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
       cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_csr_const, sizeof(double) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_flags, 2 * n_bunches) != cudaSuccess ||
-      cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
+      cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_keys, 2 * sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
     err = "CSR state allocation failed";
     return B2E_ERR_NOMEM;
   }
@@ -924,6 +943,10 @@ int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vect
   }
   const int gx = (int)std::min<int64_t>(std::max(1, 148 * 4 / nb), std::max<int64_t>(1, (n / nb + 255) / 256));
   alive_per_bunch_kernel<<<dim3(gx, nb), 256, 0, stream>>>(lost_pass, n, st.d_offsets, nb, st.d_alive);
+  if (st.reducer && st.reducer(st.reducer_user, B2E_REDUCE_SUM_U64, st.d_alive, nb, stream)) {
+    err = "CSR: the all-rank reduction of alive counts failed";
+    return B2E_ERR_CUDA;
+  }
   if (cudaGetLastError() != cudaSuccess ||
       cudaMemcpyAsync(h.data(), st.d_alive, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stream) !=
           cudaSuccess ||
@@ -933,6 +956,39 @@ int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vect
   }
   alive.assign(h.begin(), h.end());
   return B2E_OK;
+}
+
+int csr_reduce_counts(CsrState &st, std::vector<int64_t> &counts, cudaStream_t stream, std::string &err) {
+  if (!st.reducer)
+    return B2E_OK;
+  const int nb = (int)counts.size();
+  std::vector<unsigned long long> h(counts.begin(), counts.end());
+  if (nb > st.n_bunches || cudaMemcpyAsync(st.d_alive, h.data(), sizeof(unsigned long long) * nb,
+                                           cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+      st.reducer(st.reducer_user, B2E_REDUCE_SUM_U64, st.d_alive, nb, stream) ||
+      cudaMemcpyAsync(h.data(), st.d_alive, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    err = "CSR: the all-rank reduction of bunch sizes failed";
+    return B2E_ERR_CUDA;
+  }
+  counts.assign(h.begin(), h.end());
+  return B2E_OK;
+}
+
+/* all-rank min/max of every bunch's c*t keys (no-op without a reducer) */
+static int reduce_keys(CsrState &st, const CsrBunches &B, cudaStream_t stream, std::string &err, int64_t *launches) {
+  if (!st.reducer)
+    return B2E_OK;
+  csr_keys_gather_kernel<<<1, 32, 0, stream>>>(B, st.d_keys);
+  if (st.reducer(st.reducer_user, B2E_REDUCE_MIN_U64, st.d_keys, B.n, stream) ||
+      st.reducer(st.reducer_user, B2E_REDUCE_MAX_U64, st.d_keys + B.n, B.n, stream)) {
+    err = "CSR: the all-rank reduction of the c*t range failed";
+    return B2E_ERR_CUDA;
+  }
+  csr_keys_scatter_kernel<<<1, 32, 0, stream>>>(B, st.d_keys);
+  (*launches) += 2;
+  return cudaGetLastError() == cudaSuccess ? B2E_OK : B2E_ERR_CUDA;
 }
 
 void csr_reset(CsrState &st) {
@@ -1170,6 +1226,9 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     CSR_CUDA(cudaGetLastError());
     if (!any_active)
       continue;
+    int rrc = reduce_keys(st, B, stream, err, launches);
+    if (rrc)
+      return rrc;
     CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
     int64_t per = (n + nbunch - 1) / nbunch;
     int hb = (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 4 / nbunch), std::max<int64_t>(1, (per + 1023) / 1024));
@@ -1177,6 +1236,10 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
                                                                                        ce.binRangeFactor);
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
+    if (st.reducer && st.reducer(st.reducer_user, B2E_REDUCE_SUM_U32, st.d_counts, (int64_t)ce.bins * nbunch, stream)) {
+      err = "CSR: the all-rank reduction of the histogram failed";
+      return B2E_ERR_CUDA;
+    }
     phiBend += ce.angle / ce.nSlices;
     double slippage = fabs(ce.rho0 * (phiBend * phiBend * phiBend) / 24.0);
     WakeArgs a;
@@ -1225,6 +1288,12 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
   (*launches)++;
   csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, ce.bins, Po, ce.rho0);
+  CSR_CUDA(cudaGetLastError());
+  if (any_active) {
+    int rrc = reduce_keys(st, B, stream, err, launches);
+    if (rrc)
+      return rrc;
+  }
   csr_exit_kernel<<<g, 256, 0, stream>>>(P, n, d_e, B, ce.binRangeFactor, Po, pass, elem);
   (*launches) += 2;
   CSR_CUDA(cudaGetLastError());
@@ -1264,6 +1333,9 @@ void csr_release(CsrState &st) {
     cudaFree(st.d_flags);
   if (st.d_alive)
     cudaFree(st.d_alive);
+  if (st.d_keys)
+    cudaFree(st.d_keys);
+  st.d_keys = nullptr;
   st.d_csr_const = nullptr;
   st.d_flags = nullptr;
   st.d_alive = nullptr;

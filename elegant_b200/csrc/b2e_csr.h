@@ -59,6 +59,10 @@ struct CsrState {
   double *d_csr_const = nullptr;  /* [n_bunches] */
   unsigned char *d_flags = nullptr; /* [2][n_bunches]: active, CSRDRIFT mode */
   unsigned long long *d_alive = nullptr; /* [n_bunches] */
+  /* optional all-rank reduction (a bunch spread over several GPUs) */
+  b2e_reduce_fn reducer = nullptr;
+  void *reducer_user = nullptr;
+  unsigned long long *d_keys = nullptr; /* [2][n_bunches]: gathered min, max keys */
   double *d_sg = nullptr;         /* weights of all elements, uploaded once */
   int *d_sg_idx = nullptr;
   std::vector<size_t> sg_offset;  /* per element: offset into d_sg / d_sg_idx */
@@ -88,6 +92,8 @@ void csr_reset(CsrState &st);
 /* Bunch layout for the CSR step (n_bunches contiguous ranges; offsets on the
  * device, owned by the caller); allocates the per-bunch state. */
 int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::string &err);
+/* all-rank sums of per-bunch counts (identity without a reducer) */
+int csr_reduce_counts(CsrState &st, std::vector<int64_t> &counts, cudaStream_t stream, std::string &err);
 /* particles alive (lost_pass < 0), per bunch */
 int csr_count_alive(CsrState &st, const int32_t *lost_pass, int64_t n, std::vector<int64_t> &alive, cudaStream_t stream,
                     std::string &err);

@@ -190,6 +190,24 @@ class Tracker:
                                                                 ("survivors", "cx", "cy", "ex", "ey"))))
         return out
 
+    def set_csr_reducer(self, fn):
+        """Spread bunches over several ranks: fn(op, device_ptr, count, stream)
+        all-reduces an engine buffer in place (see elegant_b200.parallel);
+        None for single-GPU bunches."""
+        if fn is None:
+            self._reducer = None
+            self._check(self.lib.b2e_set_csr_reducer(self._ctx, None, None))
+            return
+
+        def cb(user, op, ptr, count, stream):
+            try:
+                return int(fn(int(op), int(ptr or 0), int(count), int(stream or 0)) or 0)
+            except Exception:  # an exception must not cross into C
+                return -1
+
+        self._reducer = nat.REDUCE_FN(cb)  # kept alive while registered
+        self._check(self.lib.b2e_set_csr_reducer(self._ctx, self._reducer, None))
+
     def set_csr_surrogate(self, surrogate, tolerance: float = 0.01, gate_stride: int = 16):
         """Use a trained wake surrogate (elegant_b200.wake_surrogate.WakeSurrogate)
         for the CSRCSBEND wake integral, gated by the plain integral on every

@@ -298,6 +298,26 @@ int b2e_wakenet_gradients(b2e_wakenet *net, const float *dev_inputs, const float
 int b2e_wakenet_train_step(b2e_wakenet *net, const float *dev_inputs, const float *dev_targets, int32_t n, float lr,
                            double *loss, void *stream);
 
+/* ---- CSR with a bunch spread over several GPUs -------------------------
+ * Each rank holds part of every bunch (same bunch layout on every rank).  At
+ * the reference's exchange points (csbend.c:2532-2550, findGlobalMinMax.c)
+ * the engine calls `fn` on device buffers of its own stream: the min/max of
+ * c*t per bunch (B2E_REDUCE_MIN_U64 / MAX_U64 on order-preserving keys), the
+ * histogram counts per bunch (B2E_REDUCE_SUM_U32, bunch-major), and the
+ * particle counts per bunch (B2E_REDUCE_SUM_U64: alive at an element, and at
+ * the start of a run for the macro-particle charge).  The callback must leave
+ * the all-rank result in the buffer before later work on `stream` reads it
+ * (for example an NCCL all-reduce enqueued on that stream) and return 0.
+ * Every rank then bins, smooths and integrates the same global histogram, so
+ * each particle receives the kick it would receive on one GPU.  fn = NULL
+ * switches back to single-GPU bunches. */
+#define B2E_REDUCE_MIN_U64 0
+#define B2E_REDUCE_MAX_U64 1
+#define B2E_REDUCE_SUM_U32 2
+#define B2E_REDUCE_SUM_U64 3
+typedef int (*b2e_reduce_fn)(void *user, int32_t op, void *dev_buf, int64_t count, void *stream);
+int b2e_set_csr_reducer(b2e_ctx *ctx, b2e_reduce_fn fn, void *user);
+
 /* ---- learned CSR wake in tracking --------------------------------------
  * Binds a trained wake network to a tracking context (net = NULL unbinds).
  * For CSRCSBEND kicks with the transient integral and the trapezoid rule

@@ -150,3 +150,100 @@ def test_surrogate_wakes_follow_the_plain_wakes():
     assert np.all(np.isfinite(errs))
     # the fallback count is what the gate decided
     assert stats["fallbacks"] == int((errs > 0.01).sum())
+
+
+class _HostExchange:
+    """Two tracking contexts in two host threads on one GPU, each holding half
+    of every bunch, exchanging through host memory at the engine's CSR
+    reduction points (a stand-in for NCCL between GPUs: no kernel waits on
+    another; the host threads meet at a barrier with a timeout)."""
+
+    def __init__(self, n):
+        import threading
+        self.n = n
+        self.barrier = threading.Barrier(n, timeout=120)
+        self.slots = [None] * n
+
+    def reducer(self, rank):
+        import torch
+        from elegant_b200.parallel import DeviceBuffer, REDUCE_MAX_U64, REDUCE_MIN_U64, REDUCE_SUM_U32
+
+        def fn(op, ptr, count, stream):
+            s = torch.cuda.ExternalStream(stream)
+            t = torch.as_tensor(DeviceBuffer(ptr, count, "<i4" if op == REDUCE_SUM_U32 else "<i8"), device="cuda")
+            with torch.cuda.stream(s):
+                host = t.cpu().numpy().copy()
+            self.slots[rank] = host
+            self.barrier.wait()
+            vals = np.stack(self.slots)
+            if op == REDUCE_MIN_U64:
+                out = vals.view(np.uint64).min(axis=0).view(np.int64)
+            elif op == REDUCE_MAX_U64:
+                out = vals.view(np.uint64).max(axis=0).view(np.int64)
+            else:
+                out = vals.sum(axis=0).astype(vals.dtype)
+            self.barrier.wait()
+            with torch.cuda.stream(s):
+                t.copy_(torch.from_numpy(out))
+            s.synchronize()
+            return 0
+        return fn
+
+
+@pytest.mark.parametrize("train", [False, True])
+def test_bunches_split_over_two_ranks_match_one(train):
+    """Every bunch's particles split between two ranks, each rank's engine
+    reducing min/max, histograms and counts with the other: the union of the
+    two runs equals the one-rank run bit for bit, and both ranks log the same
+    per-kick wakes."""
+    import threading
+    lat = w.chicane(bins=120, n_kicks=4)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, N_KICKS=2)) if e.type == "CSRDRIFT" else e
+                   for e in lat.elements])
+    sizes = [6000, 9000] if train else [12000]
+    beam, offsets = _bunch_train(sizes, [-10.0, -14.0][:len(sizes)], seed=70)
+    with Tracker(lat, P0, 1) as t:
+        if train:
+            t.load_ensemble(offsets, [])
+        full = t.track(beam)
+        full_w = t.csr_wakes(10_000_000)
+    parts = []
+    for r in range(2):
+        idx = np.concatenate([np.arange(offsets[b] + r, offsets[b + 1], 2) for b in range(len(sizes))])
+        loc = np.concatenate([[0], np.cumsum([len(range(offsets[b] + r, offsets[b + 1], 2))
+                                              for b in range(len(sizes))])]).astype(np.int64)
+        parts.append((idx, loc))
+    ex = _HostExchange(2)
+    results, errors = [None, None], []
+
+    def run(r):
+        try:
+            from elegant_b200.beam import Beam
+            idx, loc = parts[r]
+            with Tracker(lat, P0, 1) as t:
+                if train:
+                    t.load_ensemble(loc, [])
+                t.set_csr_reducer(ex.reducer(r))
+                res = t.track(Beam(beam.coords[idx], beam.ids[idx]))
+                results[r] = (res, t.csr_wakes(10_000_000))
+        except Exception as e:  # reported below
+            errors.append(e)
+            ex.barrier.abort()
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(2)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join(timeout=300)
+    assert not errors, errors
+    for r in range(2):
+        assert np.array_equal(results[r][1], full_w)
+    order = np.argsort(full.ids)
+    ids = np.concatenate([results[r][0].ids for r in range(2)])
+    coords = np.concatenate([results[r][0].coords for r in range(2)])
+    lost = np.concatenate([results[r][0].lost_pass for r in range(2)])
+    o2 = np.argsort(ids)
+    assert np.array_equal(ids[o2], full.ids[order])
+    assert np.array_equal(lost[o2], full.lost_pass[order])
+    alive = full.lost_pass[order] < 0
+    assert np.array_equal(coords[o2][alive], full.coords[order][alive])

@@ -100,3 +100,39 @@ def test_two_rank_gloo_sharded_run(tmp_path):
         work += eff
     assert total == work
     assert np.array_equal(rows, np.concatenate(expect))
+
+
+def _keys_worker(rank, world, port, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from elegant_b200.parallel import (REDUCE_MAX_U64, REDUCE_MIN_U64, REDUCE_SUM_U32, REDUCE_SUM_U64,
+                                       allreduce_keys_and_counts)
+    # order-preserving keys: values with the top bit set compare above the others
+    keys = np.array([[0x8000000000000005, 0x7FFFFFFFFFFFFFF0, 3], [0x8000000000000001, 0xFFFFFFFFFFFFFFFF, 9]],
+                    dtype=np.uint64)[rank]
+    t = torch.from_numpy(keys.view(np.int64).copy())
+    allreduce_keys_and_counts(t, REDUCE_MIN_U64, dist)
+    mn = t.numpy().view(np.uint64).tolist()
+    t = torch.from_numpy(keys.view(np.int64).copy())
+    allreduce_keys_and_counts(t, REDUCE_MAX_U64, dist)
+    mx = t.numpy().view(np.uint64).tolist()
+    c32 = torch.tensor([rank + 1, 10 * rank, 7], dtype=torch.int32)
+    allreduce_keys_and_counts(c32, REDUCE_SUM_U32, dist)
+    c64 = torch.tensor([2 ** 40 + rank], dtype=torch.int64)
+    allreduce_keys_and_counts(c64, REDUCE_SUM_U64, dist)
+    np.save(os.path.join(out_dir, f"keys{rank}.npy"), np.array([mn, mx], dtype=np.uint64))
+    np.save(os.path.join(out_dir, f"counts{rank}.npy"), np.concatenate([c32.numpy(), c64.numpy()]).astype(np.int64))
+    dist.destroy_process_group()
+
+
+def test_csr_exchange_reductions_two_ranks(tmp_path):
+    """The CSR exchange (a bunch spread over two ranks): unsigned min/max of
+    order-preserving c*t keys and sums of histogram and particle counts."""
+    port = _free_port()
+    mp.start_processes(_keys_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn")
+    for r in range(2):
+        k = np.load(tmp_path / f"keys{r}.npy")
+        assert k[0].tolist() == [0x8000000000000001, 0x7FFFFFFFFFFFFFF0, 3]
+        assert k[1].tolist() == [0x8000000000000005, 0xFFFFFFFFFFFFFFFF, 9]
+        c = np.load(tmp_path / f"counts{r}.npy")
+        assert c.tolist() == [3, 10, 14, 2 ** 41 + 1]
