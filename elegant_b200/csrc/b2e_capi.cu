@@ -100,6 +100,11 @@ struct b2e_ctx {
   DevBuf<double> d_hist_out;       /* [n_inst][passes of the call][5] */
   std::vector<double> history;     /* [pass][inst][5]: survivors, <x>, <y>, ex, ey */
   int hist_pass0 = 0, hist_passes = 0;
+  /* lost-particle compaction: second set of particle buffers, survivors per instance */
+  DevBuf<double> d_cmp_cols[6];
+  DevBuf<int64_t> d_cmp_ids;
+  DevBuf<int32_t> d_cmp_lost_pass, d_cmp_lost_elem;
+  DevBuf<int> d_alive_inst;
 };
 
 static int fail(b2e_ctx *ctx, int code, const char *fmt, ...) {
@@ -160,6 +165,12 @@ extern "C" int b2e_destroy(b2e_ctx *ctx) {
   ctx->d_lost_elem.release();
   ctx->d_flag.release();
   ctx->d_counters.release();
+  for (auto &c : ctx->d_cmp_cols)
+    c.release();
+  ctx->d_cmp_ids.release();
+  ctx->d_cmp_lost_pass.release();
+  ctx->d_cmp_lost_elem.release();
+  ctx->d_alive_inst.release();
   csr_release(ctx->csr);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -183,20 +194,30 @@ extern "C" int b2e_ring_tuning(const b2e_ctx *ctx, int32_t *chosen, float *ms_pe
   return B2E_OK;
 }
 
-/* Rebuild the tile table for the current instance partition. */
-static void build_tiles(b2e_ctx *ctx) {
+/* Rebuild the tile table for the current instance partition (every particle
+ * of instance i, or its first alive[i] after a compaction). */
+static void build_tiles(b2e_ctx *ctx, const int *alive = nullptr) {
   ctx->tiles.clear();
   ctx->tile_first.assign(1, 0);
   for (int i = 0; i < ctx->n_inst; i++) {
-    for (int64_t s = ctx->inst_offsets[i]; s < ctx->inst_offsets[i + 1]; s += kTileThreads) {
+    const int64_t end = alive ? ctx->inst_offsets[i] + alive[i] : ctx->inst_offsets[i + 1];
+    for (int64_t s = ctx->inst_offsets[i]; s < end; s += kTileThreads) {
       DevTile t;
       t.start = s;
-      t.count = (int32_t)std::min<int64_t>(kTileThreads, ctx->inst_offsets[i + 1] - s);
+      t.count = (int32_t)std::min<int64_t>(kTileThreads, end - s);
       t.inst = i;
       ctx->tiles.push_back(t);
     }
     ctx->tile_first.push_back((int)ctx->tiles.size());
   }
+}
+
+static int upload_tiles(b2e_ctx *ctx) {
+  CUDA_TRY(ctx, ctx->d_tiles.ensure(std::max<size_t>(ctx->tiles.size(), 1)));
+  if (!ctx->tiles.empty())
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_tiles.ptr, ctx->tiles.data(), sizeof(DevTile) * ctx->tiles.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  return B2E_OK;
 }
 
 static int upload_lattice_tables(b2e_ctx *ctx) {
@@ -340,7 +361,8 @@ extern "C" int b2e_upload_particles(b2e_ctx *ctx, const double *const columns[6]
   if (ctx->inst_offsets.back() != n)
     return fail(ctx, B2E_ERR_ARG, "b2e_upload_particles: ensemble offsets cover %lld particles, got %lld",
                 (long long)ctx->inst_offsets.back(), (long long)n);
-  return B2E_OK;
+  build_tiles(ctx); /* a compaction of the previous run may have shortened the tiles */
+  return upload_tiles(ctx);
 }
 
 static DevParticles particle_view(b2e_ctx *ctx) {
@@ -415,6 +437,42 @@ static int autotune_ring(b2e_ctx *ctx, const RingLaunch &Lreal, bool staged, siz
   return B2E_OK;
 }
 
+/* Lost-particle compaction between launches: survivors of every instance to
+ * the front of its range (rows reordered, IDs with them), tiles rebuilt over
+ * the survivors only. */
+static int compact_particles(b2e_ctx *ctx) {
+  const size_t n = (size_t)ctx->n;
+  for (auto &c : ctx->d_cmp_cols)
+    CUDA_TRY(ctx, c.ensure(n));
+  CUDA_TRY(ctx, ctx->d_cmp_ids.ensure(n));
+  CUDA_TRY(ctx, ctx->d_cmp_lost_pass.ensure(n));
+  CUDA_TRY(ctx, ctx->d_cmp_lost_elem.ensure(n));
+  CUDA_TRY(ctx, ctx->d_alive_inst.ensure((size_t)ctx->n_inst));
+  DevParticles dst;
+  dst.x = ctx->d_cmp_cols[0].ptr;
+  dst.xp = ctx->d_cmp_cols[1].ptr;
+  dst.y = ctx->d_cmp_cols[2].ptr;
+  dst.yp = ctx->d_cmp_cols[3].ptr;
+  dst.s = ctx->d_cmp_cols[4].ptr;
+  dst.dp = ctx->d_cmp_cols[5].ptr;
+  dst.lost_pass = ctx->d_cmp_lost_pass.ptr;
+  dst.lost_elem = ctx->d_cmp_lost_elem.ptr;
+  CUDA_TRY(ctx, launch_compact(particle_view(ctx), ctx->d_ids.ptr, dst, ctx->d_cmp_ids.ptr, ctx->d_inst_offsets.ptr,
+                               ctx->n_inst, ctx->d_alive_inst.ptr, ctx->stream));
+  ctx->launches++;
+  std::vector<int> alive(ctx->n_inst);
+  CUDA_TRY(ctx, cudaMemcpyAsync(alive.data(), ctx->d_alive_inst.ptr, sizeof(int) * ctx->n_inst, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int c = 0; c < 6; c++)
+    std::swap(ctx->d_cols[c], ctx->d_cmp_cols[c]);
+  std::swap(ctx->d_ids, ctx->d_cmp_ids);
+  std::swap(ctx->d_lost_pass, ctx->d_cmp_lost_pass);
+  std::swap(ctx->d_lost_elem, ctx->d_cmp_lost_elem);
+  build_tiles(ctx, alive.data());
+  return upload_tiles(ctx);
+}
+
 /* Track element range [(pb, eb), (pe, ee)) with ring launches, splitting at CSR elements. */
 static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   const int ne = (int)ctx->lat.elems.size();
@@ -438,6 +496,9 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
+  const bool compact = ctx->opt.compact_every > 0 && !ctx->use_ext && !L.hist;
+  if (compact)
+    ppl = std::min(ppl, ctx->opt.compact_every);
   int variant = ctx->opt.ring_variant;
   if (variant < 1 || variant > B2E_RING_VARIANTS) {
     /* autotune once per context on a multi-pass range of a large enough beam */
@@ -456,6 +517,14 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
     if (lp > p && le == 0) { /* (lp, 0) is the same point as (lp-1, ne) */
       lp -= 1;
       le = ne;
+    }
+    if (compact && e == 0 && p >= 1 && p > pb) {
+      int rc = compact_particles(ctx);
+      if (rc)
+        return rc;
+      L.P = particle_view(ctx);
+      L.tiles = ctx->d_tiles.ptr;
+      L.n_tiles = (int)ctx->tiles.size();
     }
     L.pass_begin = p;
     L.elem_begin = e;

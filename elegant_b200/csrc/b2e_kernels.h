@@ -30,6 +30,10 @@ struct RingLaunch {
  * level of the ring kernel (see launch_ring in b2e_ring.cu). */
 cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes, cudaStream_t stream,
                         int variant);
+/* survivors of every instance moved to the front of its range (src -> dst);
+ * alive_out[inst] = survivors */
+cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticles dst, int64_t *ids_dst,
+                           const int64_t *offs, int n_inst, int *alive_out, cudaStream_t stream);
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
                             cudaStream_t stream);

@@ -417,6 +417,75 @@ cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t sm
   }
 }
 
+/* Stable partition of every instance's particles: survivors first, in their
+ * order, lost particles after them (last to first).  One block per instance
+ * walks its range in chunks of blockDim particles; a warp ballot gives each
+ * particle its rank among its warp's survivors (or losses) and a scan over
+ * the block's warp totals the chunk offsets (lost-particle compaction with
+ * warp ballots and prefix sums). */
+__global__ void compact_kernel(DevParticles src, const int64_t *ids_src, DevParticles dst, int64_t *ids_dst,
+                               const int64_t *offs, int *alive_out) {
+  __shared__ int warp_alive[32], warp_dead[32];
+  __shared__ int base_alive, base_dead;
+  const int inst = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int64_t first = offs[inst], end = offs[inst + 1];
+  if (threadIdx.x == 0) {
+    base_alive = 0;
+    base_dead = 0;
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  for (int64_t c = first; c < end; c += blockDim.x) {
+    const int64_t i = c + threadIdx.x;
+    const bool valid = i < end;
+    const bool alive = valid && src.lost_pass[i] < 0;
+    const unsigned ba = __ballot_sync(0xffffffffu, alive), bd = __ballot_sync(0xffffffffu, valid && !alive);
+    if (lane == 0) {
+      warp_alive[warp] = __popc(ba);
+      warp_dead[warp] = __popc(bd);
+    }
+    __syncthreads();
+    int pa = 0, pd = 0, ta = 0, td = 0;
+    for (int w = 0; w < nw; w++) {
+      if (w < warp) {
+        pa += warp_alive[w];
+        pd += warp_dead[w];
+      }
+      ta += warp_alive[w];
+      td += warp_dead[w];
+    }
+    if (valid) {
+      const int64_t d = alive ? first + base_alive + pa + __popc(ba & below)
+                              : end - 1 - (base_dead + pd + __popc(bd & below));
+      dst.x[d] = src.x[i];
+      dst.xp[d] = src.xp[i];
+      dst.y[d] = src.y[i];
+      dst.yp[d] = src.yp[i];
+      dst.s[d] = src.s[i];
+      dst.dp[d] = src.dp[i];
+      dst.lost_pass[d] = src.lost_pass[i];
+      dst.lost_elem[d] = src.lost_elem[i];
+      ids_dst[d] = ids_src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      base_alive += ta;
+      base_dead += td;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    alive_out[inst] = base_alive;
+}
+
+cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticles dst, int64_t *ids_dst,
+                           const int64_t *offs, int n_inst, int *alive_out, cudaStream_t stream) {
+  if (n_inst <= 0)
+    return cudaSuccess;
+  compact_kernel<<<n_inst, 1024, 0, stream>>>(src, ids_src, dst, ids_dst, offs, alive_out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
                             cudaStream_t stream) {

@@ -38,7 +38,8 @@ class Tracker:
     """One engine context bound to a lattice and run options."""
 
     def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
-                 passes_per_launch: int = 0, ring_variant: int = 0, record_history: bool = False):
+                 passes_per_launch: int = 0, ring_variant: int = 0, record_history: bool = False,
+                 compact_every: int = 0):
         self.lib = nat.load_library()
         self.lattice = lattice
         self._ctx = ctypes.c_void_p()
@@ -47,7 +48,8 @@ class Tracker:
             raise nat.EngineError(rc, "b2e_create failed (is a CUDA device visible?)")
         self.options = nat.RunOptions(p_central=p_central, n_passes=n_passes, default_order=default_order,
                                       coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
-                                      ring_variant=ring_variant, record_history=int(record_history))
+                                      ring_variant=ring_variant, record_history=int(record_history),
+                                      compact_every=compact_every)
         self._elems = lattice.to_ctypes()
         self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
         self.n_instances = 1

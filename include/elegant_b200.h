@@ -170,6 +170,10 @@ typedef struct {
                               (all variants give identical results) */
   int32_t record_history;  /* nonzero: keep per-instance, per-pass survivors, centroids and
                               rms emittances (b2e_ensemble_history) */
+  int32_t compact_every;   /* > 0: every this many passes (after pass 0), move each instance's
+                              surviving particles to the front of its range and launch only
+                              them; the order of rows changes, IDs travel with them.  Not with
+                              record_history or device-owned columns. */
 } b2e_run_options;
 
 typedef struct b2e_ctx b2e_ctx;

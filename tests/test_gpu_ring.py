@@ -233,3 +233,35 @@ def test_ensemble_history_matches_per_pass_moments():
         for k, col in (("cx", 1), ("cy", 2), ("ex", 3), ("ey", 4)):
             np.testing.assert_allclose(h[k], expected[:, :, col], rtol=1e-10, atol=1e-18)
     assert np.array_equal(stepped["ex"], hist["ex"])
+
+
+@pytest.mark.parametrize("ensemble", [False, True])
+def test_compaction_gives_the_same_particles(ensemble):
+    """Moving each instance's survivors to the front every few passes (rows
+    reordered, launches over survivors only) changes no particle's result."""
+    if ensemble:
+        lat, beam, offsets, overrides = w.ensemble(n_instances=4, n_min=200, n_max=500, seed=12)
+        lossy = _lossy_beam(int(offsets[2] - offsets[1]), seed=6)
+        beam.coords[offsets[1]:offsets[2]] = lossy.coords
+    else:
+        lat, beam = w.fodo_ring(), _lossy_beam(900, seed=17)
+
+    def run(**kw):
+        with Tracker(lat, w.ring_p_central(), 30, **kw) as t:
+            if ensemble:
+                t.load_ensemble(offsets, overrides)
+            return t.track(beam)
+
+    plain, comp = run(), run(compact_every=3)
+    assert (plain.lost_pass >= 0).sum() > 50
+    assert comp.effort == plain.effort and comp.n_left == plain.n_left
+    o1, o2 = np.argsort(plain.ids), np.argsort(comp.ids)
+    assert np.array_equal(plain.ids[o1], comp.ids[o2])
+    assert np.array_equal(plain.lost_pass[o1], comp.lost_pass[o2])
+    assert np.array_equal(plain.lost_element[o1], comp.lost_element[o2])
+    alive = plain.lost_pass[o1] < 0
+    assert np.array_equal(plain.coords[o1][alive], comp.coords[o2][alive])
+    if ensemble:  # every particle stays inside its own instance's range
+        for i in range(4):
+            sl = slice(offsets[i], offsets[i + 1])
+            assert set(comp.ids[sl]) == set(beam.ids[sl])
