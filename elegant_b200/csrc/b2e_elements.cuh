@@ -62,7 +62,19 @@ __device__ __forceinline__ bool mult_aperture_ok(double xIn, double yIn, const D
  * drift_matrix (compute_matrices.c:391-412) has C[4]=L, R[0][1]=R[2][3]=L,
  * T[4][1][1]=T[4][3][3]=L/2; the order-2 contraction (matrix.c:390-419)
  * sums j = 5..0, so s picks up the yp^2 term before the xp^2 term. */
+/* track_particles (matrix.c:294-469) forms every output as a sum over all
+ * six inputs, so a non-finite coordinate anywhere (0 * NaN, 0 * inf) makes the
+ * outputs non-finite and the particle is lost after the element; with finite
+ * inputs the zero matrix entries add nothing and only the terms below remain. */
+__device__ __forceinline__ bool matrix_inputs_finite(const Part &p) {
+  return isfinite(p.x) && isfinite(p.xp) && isfinite(p.y) && isfinite(p.yp) && isfinite(p.s) && isfinite(p.dp);
+}
+
 __device__ __forceinline__ void drif_o2(Part &p, const DevElem &e) {
+  if (!matrix_inputs_finite(p)) {
+    p.x = p.y = NAN;
+    return;
+  }
   const double L = e.c[DR_L], LH = e.c[DR_LH];
   double xn = L * p.xp + p.x;
   double yn = L * p.yp + p.y;
@@ -74,6 +86,10 @@ __device__ __forceinline__ void drif_o2(Part &p, const DevElem &e) {
 }
 
 __device__ __forceinline__ void drif_o1(Part &p, const DevElem &e) {
+  if (!matrix_inputs_finite(p)) {
+    p.x = p.y = NAN;
+    return;
+  }
   const double L = e.c[DR_L];
   p.x = L * p.xp + p.x;
   p.y = L * p.yp + p.y;

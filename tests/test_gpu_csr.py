@@ -247,3 +247,10 @@ def test_bunches_split_over_two_ranks_match_one(train):
     assert np.array_equal(lost[o2], full.lost_pass[order])
     alive = full.lost_pass[order] < 0
     assert np.array_equal(coords[o2][alive], full.coords[order][alive])
+
+
+@pytest.mark.parametrize("bins", [2, 4096])
+def test_chicane_extreme_bin_counts(ref_b2e, bins):
+    lat = w.chicane(bins=bins, n_kicks=3)
+    beam = w.chicane_beam(30000, seed=bins)
+    check(*run_both(ref_b2e, lat, beam))

@@ -265,3 +265,57 @@ def test_compaction_gives_the_same_particles(ensemble):
         for i in range(4):
             sl = slice(offsets[i], offsets[i + 1])
             assert set(comp.ids[sl]) == set(beam.ids[sl])
+
+
+def test_non_finite_inputs_are_lost_like_the_reference(ref_b2e):
+    """NaN and infinite starting coordinates: the same particles lost at the
+    same turn as in the reference, the rest untouched."""
+    lat = w.fodo_ring()
+    beam = w.ring_beam(64, seed=3)
+    c = beam.coords.copy()
+    c[3, 0] = np.nan
+    c[10, 1] = np.inf
+    c[17, 2] = -np.inf
+    c[25, 5] = np.nan
+    c[40, 4] = np.nan
+    b = Beam(c, beam.ids)
+    res = gpu_track(lat, b, w.ring_p_central(), 5)
+    rows, nl, eff, _ = ref_b2e.track(lat, b.coords, b.ids, w.ring_p_central(), 5)
+    assert_parity(res, rows, nl)
+
+
+def test_ragged_ensemble_with_an_empty_instance(ref_b2e):
+    lat, beam, offsets, overrides = w.ensemble(n_instances=4, n_min=3, n_max=140, seed=8)
+    sizes = np.diff(offsets)
+    sizes[1] = 0
+    keep = np.concatenate([np.arange(offsets[i], offsets[i] + sizes[i]) for i in range(4)]).astype(int)
+    beam = Beam(beam.coords[keep], beam.ids[keep])
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    with Tracker(lat, w.ring_p_central(), 8) as t:
+        t.load_ensemble(offsets, overrides)
+        res = t.track(beam)
+    for i in (0, 2, 3):
+        sl = slice(offsets[i], offsets[i + 1])
+        els = []
+        for j, e in enumerate(lat.elements):
+            params = dict(e.params)
+            for (ie, name, vals) in overrides:
+                if ie == j:
+                    params[name] = float(vals[i])
+            els.append(Element(e.name, e.type, params))
+        rows, nl, _, _ = ref_b2e.track(Lattice(els), beam.coords[sl], beam.ids[sl], w.ring_p_central(), 8)
+        sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
+                        int((res.lost_pass[sl] < 0).sum()), 0.0)
+        assert_parity(sub, rows, nl)
+
+
+def test_lattice_too_large_for_shared_memory(ref_b2e):
+    """650 elements do not fit the shared-memory staging: the kernel reads the
+    element records from global memory, with the same results."""
+    cell = [e for e in w.fodo_ring().elements]
+    lat = Lattice([Element(f"{e.name}_{k}", e.type, dict(e.params)) for k in range(10) for e in cell])
+    assert len(lat) > 600
+    beam = w.ring_beam(48, seed=5)
+    res = gpu_track(lat, beam, w.ring_p_central(), 2)
+    rows, nl, _, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 2)
+    assert_parity(res, rows, nl)
