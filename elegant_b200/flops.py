@@ -4,8 +4,10 @@ Counted from the element maps as the reference writes them (multipole.c,
 csbend.c, simple_rfca.c, matrix.c, limit_amplitudes.c): every +, -, *, /,
 sqrt counts 1, an fma counts 2, comparisons and sign flips count 0.  The
 elementary functions count the operations of their implementations in
-elegant_b200/csrc/b2e_math.h (asin on |x| <= 1/8: 24; sin or cos kernel on
-|x| <= pi/4: 22 / 27; a pi/2 reduction: 7).  Division and sqrt are one
+elegant_b200/csrc/b2e_math.h (asin on |x| <= 2^-6: 10, on |x| <= 1/8: 24;
+sin or cos kernel on |x| <= 2^-4: 10 / 13, on |x| <= pi/4: 22 / 27; a pi/2
+reduction: 7).  A bend's substep angle decides which sin/cos kernel its
+drift takes; its sin(phi) = p_x / p is taken to be below 2^-6 (stored beams).  Division and sqrt are one
 operation here although the FP64 pipe executes each as a short Newton
 sequence, so the achieved fraction of the DGEMM peak understates pipe
 occupancy; the ncu pipe counters in profiles/ give that directly.
@@ -14,9 +16,14 @@ from __future__ import annotations
 
 from .lattice import Lattice
 
+ASIN_TINY = 10
 ASIN_SMALL = 24
 SIN_KERNEL = 22
 COS_KERNEL = 27
+SIN_SMALL = 10
+COS_SMALL = 13
+# largest |drift fraction| of the kick integrators: order 2, 4 (Forest-Ruth), 6 (taken as 1)
+MAX_DRIFT_FRAC = {2: 0.5, 4: 1.0 / (2.0 * (2.0 - 2.0 ** (1.0 / 3.0))), 6: 1.0}
 REDUCTION = 7
 TAN = REDUCTION + SIN_KERNEL + COS_KERNEL + 1
 
@@ -55,7 +62,10 @@ def element_flops(e, has_aperture: bool) -> int:
         integ = int(e.get("INTEGRATION_ORDER"))
         nsub = _nsub(integ)
         n_slices = int(e.get("N_SLICES"))
-        drift = 4 + 1 + 2 + ASIN_SMALL + 2 + SIN_KERNEL + COS_KERNEL + 1 + COS_KERNEL + 1 + 6 + 2 + 3 + 1 + 4
+        angle = abs(float(e.get("ANGLE"))) / max(n_slices, 1) * MAX_DRIFT_FRAC.get(integ, 1.0)
+        small = angle + 0.01 <= 2.0 ** -4  # substep angle plus a particle angle within the short kernels
+        sn, cs = (SIN_SMALL, COS_SMALL) if small else (SIN_KERNEL, COS_KERNEL)
+        drift = 4 + 1 + 2 + ASIN_TINY + 2 + sn + cs + 1 + cs + 1 + 6 + 2 + 3 + 1 + 4
         kick = 10 + 4
         per_slice = (5 if has_aperture else 0) + nsub * drift + (nsub - 1) * kick
         edges = (8 + TAN) * ((e.get("EDGE1_EFFECTS") != 0) + (e.get("EDGE2_EFFECTS") != 0))
