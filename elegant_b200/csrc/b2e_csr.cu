@@ -41,7 +41,7 @@ struct CsrBunches {
   const int64_t *offs;
   int n;
   CsrDevState *st;
-  const double *csr_const;
+  const double *csr_const; /* [2][n]: CSRConstant, then the IGF wake factor */
   const unsigned char *active; /* more than one particle alive at the element entrance */
   const unsigned char *mode;   /* CSRDRIFT: 1 = wake kicks, 0 = exact drift */
 };
@@ -239,6 +239,9 @@ struct WakeArgs {
   double slippage, slippage13, c1, c2, csr_constant;
   double length, nSlices;   /* element length and kicks: c1 and c2 of each bunch */
   double *wakelog;          /* nBins values per bunch for this kick, or null */
+  /* integrated Green's function (csbend.c:2593-2621, :2676-2680) */
+  int igf;
+  double gamma2, gamma3, rho0, const1, q4pe, igf_factor;
 };
 
 /* Savitzky-Golay pass with precomputed per-bin weights (b2e_sg.h convention);
@@ -366,6 +369,55 @@ __device__ __forceinline__ void wake_terms(int ib, const WakeArgs &a, const doub
   *T2out = T2;
 }
 
+/* Steady-state wake by the integrated Green's function (csbend.c:2593-2621,
+ * :2676-2680, convolveArrays1 :5484-5491): chi(z) per bin, its second
+ * difference, the one-sided convolution with the density (per-bin serial
+ * sums in the reference's order), times -q_macro/(m c^2) L/N_KICKS.  chik and
+ * grnk are nBins scratch arrays in shared memory. */
+__device__ void igf_wake(const WakeArgs &a, const double dct, const double *hist, double *chik, double *grnk,
+                         double *dgamma) {
+  const int nb = a.nBins;
+  const double frac = 9.0 / 16.0;
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    const double z = ib * dct;
+    const double xmu = 3.0 * a.gamma3 * z / (2.0 * a.rho0);
+    const double aa = sqrt(xmu * xmu + 1.0);
+    const double b = aa + xmu;
+    double chi;
+    if (xmu < 1e-3) {
+      const double x2 = xmu * xmu, x3 = xmu * xmu * xmu;
+      chi = frac * a.const1 + 0.50 * x2 - (7.0 / 54.0) * (x2 * x2) + (140.0 / 2187.0) * (x3 * x3);
+    } else {
+      const double b13 = b2e_pow13(b), b23 = b2e_pow23(b), b43 = b2e_pow43(b);
+      const double q = (1 - b23) / xmu;
+      chi = frac * (3.0 * (-2.0 * xmu * b13 + b23 + b43) + b2e_log((q * q) / (1 + b23 + b43)));
+    }
+    chik[ib] = chi;
+  }
+  __syncthreads();
+  const double const2 = (16.0 / 27.0) * a.q4pe / (a.gamma2 * dct);
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double g;
+    if (ib == 0)
+      g = const2 * (chik[1] - chik[0]);
+    else if (ib < nb - 1)
+      g = const2 * (chik[ib + 1] - 2.0 * chik[ib] + chik[ib - 1]);
+    else
+      g = 0;
+    grnk[ib] = g;
+  }
+  __syncthreads();
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double out = 0;
+    for (int ib1 = ib; ib1 < nb; ib1++)
+      out += hist[ib1] * grnk[ib1 - ib];
+    const double dg = out * a.igf_factor;
+    dgamma[ib] = dg;
+    if (a.wakelog)
+      a.wakelog[ib] = dg;
+  }
+}
+
 /* Wake of one kick (csbend.c:2566-2673) on one CTA, from a histogram of
  * counts (unsigned counts in tracking, real-valued counts for batched
  * profiles).  sm holds 4*nBins doubles.  Writes dgamma[nBins], the wake log
@@ -392,6 +444,10 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
       if (a.wakelog)
         a.wakelog[ib] = 0;
     }
+    return;
+  }
+  if (a.igf) {
+    igf_wake(a, dct, hist, sm + 3 * nb, sm + 2 * nb, dgamma);
     return;
   }
   for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
@@ -421,6 +477,7 @@ __global__ void csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, Wa
   w.csr_constant = csr_constant;
   w.c1 = csr_constant * a.length / a.nSlices;
   w.c2 = -csr_constant * a.length / a.nSlices / a.slippage13;
+  w.igf_factor = B.csr_const[B.n + bunch];
   w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
   wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, st->dct, sm, st->dGamma, &st->nBinned,
                                      nullptr, nullptr);
@@ -814,6 +871,11 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
       }
       ce.trapz = p[B2E_BEND_TRAPAZOID_INTEGRATION] != 0;
       ce.steady = p[B2E_BEND_STEADY_STATE] != 0;
+      ce.igf = p[B2E_BEND_IGF] != 0;
+      if (ce.igf && !ce.steady) {
+        err = "Must have STEADY_STATE=1 when IGF=1"; /* csbend.c:2598 */
+        return B2E_ERR_LATTICE;
+      }
       ce.csr = p[B2E_BEND_CSR] != 0;
       ce.angle = fabs(p[B2E_BEND_ANGLE]);
       ce.length = p[B2E_BEND_L];
@@ -905,7 +967,7 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
   st.macro_charge.assign(n_bunches, 0.0);
   if (cudaMalloc(&st.d_state, sizeof(CsrDevState) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS * n_bunches) != cudaSuccess ||
-      cudaMalloc(&st.d_csr_const, sizeof(double) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_csr_const, 2 * sizeof(double) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_flags, 2 * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_keys, 2 * sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
@@ -913,7 +975,7 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
     return B2E_ERR_NOMEM;
   }
   cudaMemset(st.d_state, 0, sizeof(CsrDevState) * n_bunches);
-  cudaMemset(st.d_csr_const, 0, sizeof(double) * n_bunches);
+  cudaMemset(st.d_csr_const, 0, 2 * sizeof(double) * n_bunches);
   cudaMemset(st.d_flags, 0, 2 * n_bunches);
   return B2E_OK;
 }
@@ -1186,12 +1248,15 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   st.zLast = st.z0 = ce.z_end;
   /* CSRConstant (csbend.c:2378-2381), per bunch */
   const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
-  std::vector<double> csr_constant(nbunch, 0.0);
-  for (int b = 0; b < nbunch; b++)
+  std::vector<double> csr_constant(2 * nbunch, 0.0);
+  for (int b = 0; b < nbunch; b++) {
     if (ce.csr && flags[b])
       csr_constant[b] = 2 * st.macro_charge[b] * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) /
                         (4 * kPI * eps0 * kME * (kC * kC));
-  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), sizeof(double) * nbunch, cudaMemcpyHostToDevice,
+    /* the IGF wake's factor (csbend.c:2678-2679) */
+    csr_constant[nbunch + b] = -st.macro_charge[b] / (kME * (kC * kC)) * ce.length / ce.nSlices;
+  }
+  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), 2 * sizeof(double) * nbunch, cudaMemcpyHostToDevice,
                            stream));
   CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
   const double *sgw = st.d_sg + st.sg_offset[k];
@@ -1261,6 +1326,18 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     a.nSlices = ce.nSlices;
     a.c1 = a.c2 = a.csr_constant = 0; /* per bunch in the kernel */
     a.wakelog = st.d_wakelog + st.wake_values;
+    a.igf = ce.igf;
+    {
+      /* gamma^2, gamma^3 and the IGF constants as the reference forms them
+       * (csbend.c:1981-1982, :2604, :2617) */
+      const double gamma2 = Po * Po + 1;
+      a.gamma2 = gamma2;
+      a.gamma3 = b2e_pow(gamma2, 3. / 2);
+      a.rho0 = ce.rho0;
+      a.const1 = 6.0 - b2e_log(27.0 / 4.0);
+      a.q4pe = kE / (4 * kPI * eps0);
+      a.igf_factor = 0;
+    }
     if (use_net) {
       const int L = wakenet_bins(st.net);
       csr_sur_filter_kernel<<<nbunch, 1024, std::max(sur_smem, sizeof(double) * 4 * ce.bins), stream>>>(B, st.d_counts, a, L, st.sc_dens, st.sc_deriv,
@@ -1398,7 +1475,7 @@ struct StaticCsrScratch {
   int sg_idx[2 * B2E_STATIC_MAX_BINS * 2];
   DevElem elem;
   unsigned long long counters[2];
-  double csr_const;       /* the one bunch's CSRConstant */
+  double csr_const[2];    /* the one bunch's CSRConstant and IGF wake factor */
   unsigned char flags[2]; /* active, CSRDRIFT mode */
 };
 
@@ -1436,8 +1513,9 @@ __global__ void static_set_elem_kernel(DevElem e, DevElem *dst) { *dst = e; }
 /* Savitzky-Golay weight tables for one element, on the device, with the same
  * helpers and layout as csr_configure (rows of B2E_SG_MAX_WIDTH weights;
  * interleaved (start, width) index pairs; smoothing rows then derivative rows). */
-__global__ void static_set_bunch_kernel(StaticCsrScratch *S, double csr_constant, int active) {
-  S->csr_const = csr_constant;
+__global__ void static_set_bunch_kernel(StaticCsrScratch *S, double csr_constant, double igf_factor, int active) {
+  S->csr_const[0] = csr_constant;
+  S->csr_const[1] = igf_factor;
   S->flags[0] = (unsigned char)active;
   S->flags[1] = 0;
 }
@@ -1569,12 +1647,17 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     csr_constant = 2 * macro_particle_charge * kE / b2e_pow(3 * rho0 * rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
   const int g = (int)std::max<int64_t>(1, (n + 255) / 256);
   CsrDevState *dst = &S->state;
-  static_set_bunch_kernel<<<1, 1, 0, s>>>(S, csr_constant, more_than_one);
+  if (p[B2E_BEND_IGF] != 0 && p[B2E_BEND_STEADY_STATE] == 0) {
+    snprintf(err, errlen, "b2e_csr_bend_static: Must have STEADY_STATE=1 when IGF=1");
+    return B2E_ERR_LATTICE;
+  }
+  static_set_bunch_kernel<<<1, 1, 0, s>>>(S, csr_constant,
+                                          -macro_particle_charge / (kME * (kC * kC)) * length / nSlices, more_than_one);
   CsrBunches B;
   B.offs = nullptr;
   B.n = 1;
   B.st = dst;
-  B.csr_const = &S->csr_const;
+  B.csr_const = S->csr_const;
   B.active = &S->flags[0];
   B.mode = &S->flags[1];
 
@@ -1612,6 +1695,13 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     a.nSlices = nSlices;
     a.c1 = a.c2 = a.csr_constant = 0; /* formed in the kernel from B.csr_const */
     a.wakelog = dev_wakes ? dev_wakes + (size_t)kick * bins : nullptr;
+    a.igf = p[B2E_BEND_IGF] != 0;
+    a.gamma2 = Po * Po + 1;
+    a.gamma3 = b2e_pow(a.gamma2, 3. / 2);
+    a.rho0 = rho0;
+    a.const1 = 6.0 - b2e_log(27.0 / 4.0);
+    a.q4pe = kE / (4 * kPI * eps0);
+    a.igf_factor = 0;
     size_t smem = sizeof(double) * 4 * bins;
     STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a);
@@ -1679,6 +1769,9 @@ extern "C" int b2e_csr_wake_batch(const double *dev_counts, const double *dev_sl
   a.c2 = 0;
   a.csr_constant = 1;
   a.wakelog = nullptr;
+  a.length = a.nSlices = 1;
+  a.igf = 0;
+  a.gamma2 = a.gamma3 = a.rho0 = a.const1 = a.q4pe = a.igf_factor = 0;
   const size_t smem = sizeof(double) * 4 * bins;
   cudaError_t e = cudaFuncSetAttribute(wake_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {

@@ -30,7 +30,7 @@ struct CsrElem {
   int kind = 0;     /* K_CSRCSBEND / K_CSRDRIFT */
   /* CSRCSBEND */
   int bins = 0, nSlices = 0, nSub = 0, sgHalf = 0, sgOrder = 1, sgdHalf = 1, sgdOrder = 1;
-  int trapz = 1, steady = 0, csr = 1, same_bend_precedes = 0, bin_once = 0;
+  int trapz = 1, steady = 0, csr = 1, same_bend_precedes = 0, bin_once = 0, igf = 0;
   double angle = 0, length = 0, rho0 = 0, binRangeFactor = 1.2, dzf = 0, z_end = 0;
   std::vector<int> sg_lo, sg_w_n, sgd_lo, sgd_w_n;   /* per bin window start and width */
   std::vector<double> sg_w, sgd_w;                    /* per bin weights, B2E_SG_MAX_WIDTH each */
@@ -56,7 +56,7 @@ struct CsrState {
   int64_t beta0_cap = 0;
   void *d_state = nullptr;        /* CsrDevState[n_bunches] */
   unsigned int *d_counts = nullptr; /* [n_bunches][B2E_CSR_MAX_BINS] */
-  double *d_csr_const = nullptr;  /* [n_bunches] */
+  double *d_csr_const = nullptr;  /* [2][n_bunches]: CSRConstant, IGF wake factor */
   unsigned char *d_flags = nullptr; /* [2][n_bunches]: active, CSRDRIFT mode */
   unsigned long long *d_alive = nullptr; /* [n_bunches] */
   /* optional all-rank reduction (a bunch spread over several GPUs) */

@@ -20,7 +20,15 @@
  *    |x| <= 1/2 (4 terms for |x| <= 2^-6, 10 for |x| <= 1/8, 28 beyond), and
  *    asin(x) = pi/2 - 2 asin(sqrt((1-x)/2)) for 1/2 < |x| <= 1.
  *  - tan = sin/cos from the shared reduction.
- *  - pow(x, 1/3.) (the CSR denominators, csbend.c:2575) is in b2e_csr_math.h.
+ *  - pow(x, y) for the exponents the CSR code evaluates per bin (1./3, 2./3,
+ *    4./3, 2): a double-double cube root by Newton iteration, squared or
+ *    multiplied by x in double-double, times the correction for the
+ *    exponent's own rounding (y - p/3 = -(p/3) 2^-54: the factor
+ *    1 - (p/3) 2^-54 ln x).
+ *  - log: ln(1 + f) = f - (f^2/2 - s (f^2/2 + R(s^2))), s = f/(2 + f), with
+ *    f = m - 1 exact for m in [1/sqrt2, sqrt2) and R the Taylor series of
+ *    2 atanh(s) - 2 s (12 terms, |s| <= 0.1716), plus e ln2 with ln2 split
+ *    into a 42-bit head (exact product) and a tail.
  * All polynomial evaluation uses explicit fma, so the result does not depend
  * on the compiler's contraction setting.
  */
@@ -234,19 +242,11 @@ B2E_HD double b2e_log_coarse(double x) {
   return e * 0x1.62e42fefa39efp-1 + 2.0 * s * p; /* ln 2 */
 }
 
-/* pow(x, 1./3.): C's pow with the double nearest 1/3, as the CSR code calls
- * it (csbend.c:2379, :2575, :2590).  The cube root is computed to double-
- * double accuracy by Newton iteration with an exact fma residual; the
- * exponent's own rounding, 1/3 - 1./3. = 2^-54/3, enters as the factor
- * (1 - 2^-54/3 ln x).  One final rounding, so the result is the correctly
- * rounded value except in exceedingly rare near-tie cases. */
-B2E_HD double b2e_pow13(double x) {
+/* Cube root of x to double-double accuracy: x = m 2^(3q), m in [1/2, 4),
+ * cbrt(m) = y + c.  Returns y, sets *c, *m and *q. */
+B2E_HD double b2e_cbrt_dd(double x, double *c, double *mout, int *qout) {
   int e, q, r;
-  double m, y, p_hi, p_lo, t_hi, t_lo, res, c, corr;
-  if (x != x || x < 0)
-    return (x - x) / (x - x);
-  if (x == 0 || x > 1.7976931348623157e308)
-    return x;
+  double m, y, p_hi, p_lo, t_hi, t_lo, res;
   m = frexp(x, &e); /* x = m 2^e, m in [1/2, 1) */
   q = e >= 0 ? e / 3 : -((2 - e) / 3);
   r = e - 3 * q; /* 0, 1, 2 */
@@ -260,15 +260,121 @@ B2E_HD double b2e_pow13(double x) {
   t_hi = p_hi * y;
   t_lo = b2e_fma(p_hi, y, -t_hi) + p_lo * y;
   res = (m - t_hi) - t_lo;
-  c = res / (3.0 * y * y);
+  *c = res / (3.0 * y * y);
+  *mout = m;
+  *qout = q;
+  return y;
+}
+
+/* pow(x, 1./3.): C's pow with the double nearest 1/3, as the CSR code calls
+ * it (csbend.c:2379, :2575, :2590).  The cube root is computed to double-
+ * double accuracy by Newton iteration with an exact fma residual; the
+ * exponent's own rounding, 1/3 - 1./3. = 2^-54/3, enters as the factor
+ * (1 - 2^-54/3 ln x).  One final rounding, so the result is the correctly
+ * rounded value except in exceedingly rare near-tie cases. */
+B2E_HD double b2e_pow13(double x) {
+  int q;
+  double m, c, y, corr;
+  if (x != x || x < 0)
+    return (x - x) / (x - x);
+  if (x == 0 || x > 1.7976931348623157e308)
+    return x;
+  y = b2e_cbrt_dd(x, &c, &m, &q);
   corr = -(0x1p-54 / 3.0) * b2e_log_coarse(x);
   return ldexp(y + (c + y * corr), q);
 }
 
-/* pow(x, y) with the 1/3 exponent routed to b2e_pow13 (all other exponents
- * only occur in host-side setup, where the library pow is used as in the
- * reference). */
-B2E_HD double b2e_pow(double x, double y) { return y == 1.0 / 3.0 ? b2e_pow13(x) : pow(x, y); }
+/* pow(x, 2./3.) = (y + c)^2 2^(2q) (1 - (2/3) 2^-54 ln x), for x > 0 */
+B2E_HD double b2e_pow23(double x) {
+  int q;
+  double m, c, y, hi, lo, corr;
+  if (x != x || x < 0)
+    return (x - x) / (x - x);
+  if (x == 0 || x > 1.7976931348623157e308)
+    return x;
+  y = b2e_cbrt_dd(x, &c, &m, &q);
+  hi = y * y;
+  lo = b2e_fma(y, y, -hi) + 2.0 * y * c;
+  corr = -(0x1p-54 * (2.0 / 3.0)) * b2e_log_coarse(x);
+  return ldexp(hi + (lo + hi * corr), 2 * q);
+}
+
+/* pow(x, 4./3.) = m (y + c) 2^(4q) (1 - (4/3) 2^-54 ln x), for x > 0 */
+B2E_HD double b2e_pow43(double x) {
+  int q;
+  double m, c, y, hi, lo, corr;
+  if (x != x || x < 0)
+    return (x - x) / (x - x);
+  if (x == 0 || x > 1.7976931348623157e308)
+    return x;
+  y = b2e_cbrt_dd(x, &c, &m, &q);
+  hi = m * y;
+  lo = b2e_fma(m, y, -hi) + m * c;
+  corr = -(0x1p-54 * (4.0 / 3.0)) * b2e_log_coarse(x);
+  return ldexp(hi + (lo + hi * corr), 4 * q);
+}
+
+/* pow(x, y) for the exponents evaluated per bin (1./3, 2./3, 4./3, 2); any
+ * other exponent only occurs in host-side setup, where the library pow is
+ * used as in the reference. */
+B2E_HD double b2e_pow(double x, double y) {
+  if (y == 1.0 / 3.0)
+    return b2e_pow13(x);
+  if (y == 2.0 / 3.0)
+    return b2e_pow23(x);
+  if (y == 4.0 / 3.0)
+    return b2e_pow43(x);
+  if (y == 2.0)
+    return x * x;
+  return pow(x, y);
+}
+
+/* natural logarithm (see the header comment); x <= 0, inf and NaN as C's log */
+#define B2E_LN2_HI 0x1.62e42fefa3800p-1 /* ln 2 to 42 bits: e * B2E_LN2_HI is exact */
+#define B2E_LN2_LO 0x1.ef35793c76730p-45
+B2E_HD double b2e_log(double x) {
+  int e;
+  double m, f, s, z, R, hfsq, lg;
+  if (x != x)
+    return x;
+  if (x < 0)
+    return (x - x) / (x - x);
+  if (x == 0)
+    return -1.0 / 0.0;
+  if (x > 1.7976931348623157e308)
+    return x;
+  m = frexp(x, &e); /* handles subnormal x */
+  if (m < 0.70710678118654752440) {
+    m = 2.0 * m;
+    e -= 1;
+  }
+  f = m - 1.0; /* exact */
+  s = f / (2.0 + f);
+  z = s * s;
+  /* R = 2 z/3 + 2 z^2/5 + ... + 2 z^12/25 */
+  R = 2.0 / 25.0;
+  R = b2e_fma(R, z, 2.0 / 23.0);
+  R = b2e_fma(R, z, 2.0 / 21.0);
+  R = b2e_fma(R, z, 2.0 / 19.0);
+  R = b2e_fma(R, z, 2.0 / 17.0);
+  R = b2e_fma(R, z, 2.0 / 15.0);
+  R = b2e_fma(R, z, 2.0 / 13.0);
+  R = b2e_fma(R, z, 2.0 / 11.0);
+  R = b2e_fma(R, z, 2.0 / 9.0);
+  R = b2e_fma(R, z, 2.0 / 7.0);
+  R = b2e_fma(R, z, 2.0 / 5.0);
+  R = b2e_fma(R, z, 2.0 / 3.0);
+  R = R * z;
+  hfsq = 0.5 * f * f;
+  lg = hfsq - s * (hfsq + R); /* ln(1 + f) = f - lg */
+  {
+    /* (e ln2_hi + f) as an exact two-sum (Knuth), then the small terms, so the
+     * cancellation of e ln2 against f costs no extra rounding */
+    const double a = e * B2E_LN2_HI, sum = a + f, bb = sum - a;
+    const double err = (a - (sum - bb)) + (f - bb);
+    return sum + (err + (e * B2E_LN2_LO - lg));
+  }
+}
 
 B2E_HD double b2e_asin(double x) {
   double a = fabs(x), r;

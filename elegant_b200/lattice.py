@@ -41,7 +41,7 @@ _BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "
          "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
          "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18}
 _CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=23, SGDERIV_HALFWIDTH=24,
-                SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29)
+                SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29, IGF=30)
 
 # parameter name -> slot, per engine type
 SLOTS = {

@@ -118,6 +118,7 @@ extern "C" {
 #define B2E_BEND_STEADY_STATE 27
 #define B2E_BEND_CSR 28
 #define B2E_BEND_CLIP_NEGATIVE_BINS 29
+#define B2E_BEND_IGF 30 /* integrated Green's function, steady state only (csbend.c:2593-2621) */
 /* RFCA (rfca_param, track_data.c:576) */
 #define B2E_RFCA_L 0
 #define B2E_RFCA_VOLT 1

@@ -51,12 +51,16 @@
 #define M_COS(x) cos(x)
 #define M_TAN(x) tan(x)
 #define M_ASIN(x) asin(x)
+#define M_LOG(x) log(x)
+#define M_POW(x, y) pow(x, y)
 #else
 #include "../elegant_b200/csrc/b2e_math.h"
 #define M_SIN(x) b2e_sin(x)
 #define M_COS(x) b2e_cos(x)
 #define M_TAN(x) b2e_tan(x)
 #define M_ASIN(x) b2e_asin(x)
+#define M_LOG(x) b2e_log(x)
+#define M_POW(x, y) b2e_pow(x, y)
 #endif
 
 #define NPROP 8 /* x, xp, y, yp, s, delta, id, lossPass */
@@ -1081,6 +1085,36 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
       phiBend += angle / nSlices;
       {
         double slip = fabs(rho0 * (phiBend * phiBend * phiBend) / 24.0), slip13 = M_POW13(slip);
+        if (p[B2E_BEND_IGF]) {
+          /* integrated Green's function (csbend.c:2593-2621), convolveArrays1
+           * (:5484-5491) and the wake factor (:2676-2680) */
+          double gamma2 = Po * Po + 1, gamma3 = M_POW(gamma2, 3. / 2), frac = 9.0 / 16.0;
+          double const1 = 6.0 - M_LOG(27.0 / 4.0), const2, eps0 = 1 / ((4 * PI_ * 1e-7) * C_MKS * C_MKS);
+          double *chik = T1, *grnk = T2;
+          for (ib = 0; ib < nBins; ib++) {
+            double z = ib * dct, xmu = 3.0 * gamma3 * z / (2.0 * rho0), a = sqrt(xmu * xmu + 1.0), b = a + xmu;
+            if (xmu < 1e-3)
+              chik[ib] = frac * const1 + 0.50 * (xmu * xmu) - (7.0 / 54.0) * ((xmu * xmu) * (xmu * xmu)) +
+                         (140.0 / 2187.0) * ((xmu * xmu * xmu) * (xmu * xmu * xmu));
+            else
+              chik[ib] = frac * (3.0 * (-2.0 * xmu * M_POW(b, 1.0 / 3.0) + M_POW(b, 2.0 / 3.0) + M_POW(b, 4.0 / 3.0)) +
+                                 M_LOG(M_POW((1 - M_POW(b, 2.0 / 3.0)) / xmu, 2) /
+                                       (1 + M_POW(b, 2.0 / 3.0) + M_POW(b, 4.0 / 3.0))));
+          }
+          const2 = (16.0 / 27.0) * (E_MKS / (4 * PI_ * eps0)) / (gamma2 * dct);
+          grnk[0] = const2 * (chik[1] - chik[0]);
+          for (ib = 1; ib < nBins - 1; ib++)
+            grnk[ib] = const2 * (chik[ib + 1] - 2.0 * chik[ib] + chik[ib - 1]);
+          grnk[nBins - 1] = 0;
+          for (ib = 0; ib < nBins; ib++) {
+            long ib1;
+            double out = 0;
+            for (ib1 = ib; ib1 < nBins; ib1++)
+              out += ctHist[ib1] * grnk[ib1 - ib];
+            cw->dGamma[ib] = out * (-cw->macroParticleCharge / (ME_MKS * SQR(C_MKS)) * length / nSlices);
+          }
+          diS = diS4 = 0;
+        } else {
         diS = (long)(slip / dct);
         diS4 = (long)(4 * slip / dct);
         for (ib = 0; ib < nBins; ib++) {
@@ -1125,6 +1159,7 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
             T2[ib] *= -CSRConstant * length / nSlices / slip13;
           }
           cw->dGamma[ib] = T1[ib] + T2[ib];
+        }
         }
       }
       if (cw->wakes) {
@@ -1379,6 +1414,8 @@ double b2e_oracle_sin(double x) { return M_SIN(x); }
 double b2e_oracle_cos(double x) { return M_COS(x); }
 double b2e_oracle_tan(double x) { return M_TAN(x); }
 double b2e_oracle_asin(double x) { return M_ASIN(x); }
+double b2e_oracle_log(double x) { return M_LOG(x); }
+double b2e_oracle_pow(double x, double y) { return M_POW(x, y); }
 
 /* Wake integral of one histogram in bin units (dct = 1) with the CSR
  * constant, length and kick count folded to 1 and no T2 term: the T1 part of

@@ -15,4 +15,5 @@
 #define tan(x) b2e_tan(x)
 #define asin(x) b2e_asin(x)
 #define pow(x, y) b2e_pow(x, y)
+#define log(x) b2e_log(x)
 #endif

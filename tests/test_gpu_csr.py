@@ -254,3 +254,15 @@ def test_chicane_extreme_bin_counts(ref_b2e, bins):
     lat = w.chicane(bins=bins, n_kicks=3)
     beam = w.chicane_beam(30000, seed=bins)
     check(*run_both(ref_b2e, lat, beam))
+
+
+@pytest.mark.parametrize("bins,kicks", [(150, 4), (600, 6)])
+def test_chicane_igf_bit_exact(ref_b2e, bins, kicks):
+    """Steady-state CSR by the integrated Green's function (IGF=1): the
+    device's chi/Green's-function tables, convolution and kicks equal the
+    reference's bit for bit, per-kick wakes included."""
+    lat = w.chicane(bins=bins, n_kicks=kicks)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, STEADY_STATE=1, IGF=1)) if e.type == "CSRCSBEND" else e
+                   for e in lat.elements])
+    beam = w.chicane_beam(25000, seed=bins + 1)
+    check(*run_both(ref_b2e, lat, beam))

@@ -40,3 +40,30 @@ def test_symmetry_and_special_values():
         assert o.b2e_oracle_asin(-min(x, 1.0)) == -o.b2e_oracle_asin(min(x, 1.0))
     assert o.b2e_oracle_sin(0.0) == 0.0 and o.b2e_oracle_cos(0.0) == 1.0 and o.b2e_oracle_tan(0.0) == 0.0
     assert math.isnan(o.b2e_oracle_asin(1.5)) and math.isnan(o.b2e_oracle_sin(float("nan")))
+
+
+@pytest.mark.parametrize("lo,hi", [(1e-3, 10.0), (0.5, 2.0), (1e-300, 1e300), (0.99, 1.01)])
+def test_log_ulp_error(lo, hi):
+    o = PortOracle("b2e")
+    import ctypes
+    f = o.lib.b2e_oracle_log
+    f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double]
+    rng = np.random.default_rng(7)
+    xs = np.exp(rng.uniform(np.log(lo), np.log(hi), 3000))
+    worst = max(ulp_error(f(float(x)), mp.log(mp.mpf(float(x)))) for x in xs)
+    assert worst <= 0.75, worst
+    assert f(1.0) == 0.0 and math.isinf(f(0.0)) and math.isnan(f(-1.0))
+
+
+@pytest.mark.parametrize("y", [1.0 / 3.0, 2.0 / 3.0, 4.0 / 3.0, 2.0])
+def test_pow_exponents_ulp_error(y):
+    """pow for the exponents the CSR code evaluates per bin, against the
+    exact value of x to the double nearest p/3 (not p/3 itself)."""
+    o = PortOracle("b2e")
+    import ctypes
+    f = o.lib.b2e_oracle_pow
+    f.restype, f.argtypes = ctypes.c_double, [ctypes.c_double, ctypes.c_double]
+    rng = np.random.default_rng(8)
+    xs = np.exp(rng.uniform(np.log(1e-12), np.log(1e6), 3000))
+    worst = max(ulp_error(f(float(x), y), mp.power(mp.mpf(float(x)), mp.mpf(y))) for x in xs)
+    assert worst <= 0.51, worst

@@ -96,7 +96,7 @@ def test_shared_math_within_one_ulp_envelope_after_200_turns():
 
 
 @pytest.mark.parametrize("math", ["libm", "b2e"])
-@pytest.mark.parametrize("variant", ["default", "steady_plain", "no_sg"])
+@pytest.mark.parametrize("variant", ["default", "steady_plain", "no_sg", "igf"])
 def test_port_reproduces_reference_csr(math, variant):
     """CSRCSBEND + CSRDRIFT: the restatement reproduces the reference's final
     rows and every per-kick wake (captured through the reference's own
@@ -113,6 +113,9 @@ def test_port_reproduces_reference_csr(math, variant):
                 e = Element(e.name, e.type, dict(e.params, N_KICKS=3))
             els.append(e)
         lat = Lattice(els)
+    if variant == "igf":
+        lat = Lattice([Element(e.name, e.type, dict(e.params, STEADY_STATE=1, IGF=1)) if e.type == "CSRCSBEND" else e
+                       for e in lat.elements])
     beam = w.chicane_beam(6000, seed=11)
     p0 = 1000 / 0.51099895
     r1, n1, e1, w1 = RefOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
@@ -120,3 +123,18 @@ def test_port_reproduces_reference_csr(math, variant):
     assert n1 == n2 and w1.size == w2.size > 0
     assert np.array_equal(w1, w2)
     assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+
+
+def test_igf_shared_math_close_to_libm():
+    """The IGF wake through the shared pow/log against glibc's: final
+    coordinates of the chicane within 1e-10 relative."""
+    from elegant_b200 import Element, Lattice
+    lat = w.chicane(bins=120, n_kicks=4)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, STEADY_STATE=1, IGF=1)) if e.type == "CSRCSBEND" else e
+                   for e in lat.elements])
+    beam = w.chicane_beam(6000, seed=12)
+    p0 = 1000 / 0.51099895
+    a = by_id(RefOracle("libm").track(lat, beam.coords, beam.ids, p0, 1)[0])
+    b = by_id(RefOracle("b2e").track(lat, beam.coords, beam.ids, p0, 1)[0])
+    assert np.array_equal(a[2], b[2])
+    assert _rel(a[0], b[0]).max() <= 1e-10
