@@ -150,7 +150,9 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
 
 /* one kick: optional wake kick of the previous kick, one integrator slice,
  * c*t update, min/max of c*t (csbend.c:2385-2450, :3066-3076) */
-__global__ void csr_slice_kernel(DevParticles P, int64_t n, const double *beta0, const DevElem *ep,
+/* 64 registers (4 blocks of 256 per SM): twice the resident warps of the
+ * unconstrained build, the FP64 chains' latency being what limits it */
+__global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64_t n, const double *beta0, const DevElem *ep,
                                  const DevAperture *ap, CsrBunches B, int after_first_kick, int nBins, double Po,
                                  int pass, int elem_index) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
