@@ -266,3 +266,39 @@ def test_chicane_igf_bit_exact(ref_b2e, bins, kicks):
                    for e in lat.elements])
     beam = w.chicane_beam(25000, seed=bins + 1)
     check(*run_both(ref_b2e, lat, beam))
+
+
+def test_torch_nccl_reducer_single_rank_is_identity():
+    """The NCCL reducer (torch.distributed on the engine's stream) in a one-rank
+    job: every exchange is an identity, so results equal the plain run bit
+    for bit -- the plumbing (device-buffer views, stream ordering, the uint64
+    key mapping) is exercised on the GPU."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+    from elegant_b200.parallel import torch_csr_reducer
+
+    lat = w.chicane(bins=150, n_kicks=4)
+    beam, offsets = _bunch_train([8000, 5000], [-10.0, -12.0], seed=80)
+    with Tracker(lat, P0, 1) as t:
+        t.load_ensemble(offsets, [])
+        ref = t.track(beam)
+        ref_w = t.csr_wakes(10_000_000)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        with Tracker(lat, P0, 1) as t:
+            t.load_ensemble(offsets, [])
+            t.set_csr_reducer(torch_csr_reducer(dist))
+            res = t.track(beam)
+            wk = t.csr_wakes(10_000_000)
+    finally:
+        dist.destroy_process_group()
+    assert np.array_equal(wk, ref_w)
+    assert np.array_equal(res.coords, ref.coords)
+    assert np.array_equal(res.lost_pass, ref.lost_pass)
