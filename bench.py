@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-turns/s (FP64)"
+# dram__bytes_read.sum + dram__bytes_write.sum of one ring_kernel launch on the
+# 512-instance ensemble (71.16 MB + 22.74 MB; the capture in profiles/)
+RING_TRAFFIC_BYTES = 93_907_712
 UNIT = "particle-turns/s"
 
 
@@ -412,7 +415,10 @@ def main():
                        "ring_variant": variant, "autotune_ms_per_pass": [round(x, 3) for x in tune_ms],
                        "l2": "flushed (256 MiB write) before every timed step"},
             "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": achieved_tflops / fp64_peak, "traffic": None,
+                         "frac": achieved_tflops / fp64_peak, "traffic": RING_TRAFFIC_BYTES,
+                         "traffic_note": "DRAM read+write bytes of one ring launch (ncu, full-size ensemble: "
+                                         "profiles/ring_kernel_ensemble.md); the coordinates once per launch",
+                         "algorithmic_bytes_per_launch": int(n * 96),
                          "flops_per_particle_turn": fpt,
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.mm float64), best of 3"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
