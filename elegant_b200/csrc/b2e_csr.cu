@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <mutex>
 #include "b2e_csr.h"
+#include "b2e_roots.h"
 #include "b2e_elements.cuh"
 #include "b2e_kernels.h"
 #include "b2e_sg.h"
@@ -30,6 +31,7 @@ struct CsrDevState {
   double s0, dctBin;                         /* csrWake.s0, csrWake.dctBin */
   long long nBinned;
   double dGamma[B2E_CSR_MAX_BINS];           /* csrWake.dGamma: last dipole wake */
+  double phi_last;                           /* SolveForPhiStupakov's start value */
 };
 
 /* Per-bunch view for the CSR kernels.  Bunches are contiguous particle ranges
@@ -41,7 +43,7 @@ struct CsrBunches {
   const int64_t *offs;
   int n;
   CsrDevState *st;
-  const double *csr_const; /* [2][n]: CSRConstant, then the IGF wake factor */
+  const double *csr_const; /* [3][n]: CSRConstant, the IGF wake factor, GSConstant */
   const unsigned char *active; /* more than one particle alive at the element entrance */
   const unsigned char *mode;   /* CSRDRIFT: 1 = wake kicks, 0 = exact drift */
 };
@@ -747,6 +749,168 @@ __global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, CsrBunches B, d
   P.dp[i] = dp;
 }
 
+/* ---- CSRDRIFT, Stupakov mode (csbend.c:3803-4159) ---------------------- */
+
+/* phi_last starts at -1, the value SolveForPhiStupakov's static holds before
+ * its first call (csbend.c:4177) */
+__global__ void csr_init_state_kernel(CsrDevState *st, int n) {
+  for (int b = threadIdx.x; b < n; b += blockDim.x)
+    st[b].phi_last = -1;
+}
+
+/* one kick's drift: the particles move back by dz_back first (only on the
+ * first kick when the drift does not start where the last CSR element ended,
+ * csbend.c:3835-3848), then forward by dz; c*t = s/beta; min/max of c*t per
+ * bunch (csbend.c:3876-3893) */
+__global__ void stupakov_drift_kernel(DevParticles P, int64_t n, CsrBunches B, double dz_back, double dz, double Po) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int b = i < n ? bunch_of(i, B) : B.n - 1;
+  const bool mine = i < n && P.lost_pass[i] < 0 && B.mode[b];
+  double ct = 0;
+  if (mine) {
+    double x = P.x[i], xp = P.xp[i], y = P.y[i], yp = P.yp[i], s = P.s[i];
+    if (dz_back != 0) {
+      x = x - dz_back * xp;
+      y = y - dz_back * yp;
+      s = s - dz_back * sqrt((1 + xp * xp) + yp * yp);
+    }
+    x = x + xp * dz;
+    y = y + yp * dz;
+    const double p = Po * (1 + P.dp[i]), beta = p / sqrt(p * p + 1);
+    ct = (s + dz * sqrt((1 + xp * xp) + yp * yp)) / beta;
+    P.x[i] = x;
+    P.y[i] = y;
+    P.s[i] = ct;
+  }
+  bunch_minmax(ct, mine, b, B);
+}
+
+/* fn of SolveForPhiStupakov (csbend.c:4163-4165) */
+struct StupakovFn {
+  double x, x4;
+  __device__ double operator()(double phi) const { return phi * phi * phi * (phi + x4) / (phi + x); }
+};
+
+/* SolveForPhiStupakov (csbend.c:4169-4202); *phi_last carries the start
+ * value from one solve to the next */
+__device__ double stupakov_phi(double x, double ds, double phim, double *phi_last) {
+  if (ds < 0)
+    return -1;
+  if (ds == 0)
+    return 0;
+  ds *= 24;
+  StupakovFn fn;
+  fn.x = x;
+  fn.x4 = 4 * x;
+  if (*phi_last == -1)
+    *phi_last = phim / 2;
+  if (fabs(ds - fn(phim)) < ds / 1e4) {
+    *phi_last = phim;
+    return phim;
+  }
+  double phi = b2e_zero_newton(fn, ds, *phi_last, phim / 1000, 3, ds / 1e4);
+  if (phi < 0 || phi > phim || fabs(ds - fn(phi)) > ds / 1e4)
+    phi = b2e_zero_interp(fn, ds, 0, phim * 1.01, phim / 100, ds / 1e4);
+  if (phi < 0 || phi > phim)
+    return -1;
+  *phi_last = phi;
+  return phi;
+}
+
+/* per-kick scalars, formed on the host as the reference writes them */
+struct StupakovArgs {
+  double x;      /* zTravel / rho */
+  double dsMax;  /* rho/24 theta^3 (theta + 4x)/(theta + x) */
+  double dsC;    /* rho/6 theta^2 (theta + 3x), case C */
+  double theta, rho, dz0;
+  int trapz;
+};
+
+/* bins of a distance, clamped to [0, nb] (the comparisons against nb give
+ * the reference's result; a negative distance does not occur behind a dipole) */
+__device__ __forceinline__ long long clamp_bins(double d, int nb) {
+  if (!(d > 0))
+    return 0;
+  return d >= (double)nb ? nb : (long long)d;
+}
+
+/* wake of one Stupakov kick, one CTA per bunch (csbend.c:3950-4054): the
+ * histogram filters of the last dipole, phi solutions (serial, each starting
+ * from the previous one), then per bin case C, case D's boundary term and its
+ * integral in the reference's order, times -4/rho GSConstant dz0.  Shared
+ * memory: 4 nBins doubles for the filters, nBins for phi. */
+__global__ void __launch_bounds__(1024, 1) stupakov_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a, StupakovArgs sa) {
+  extern __shared__ double sm[];
+  const int bunch = blockIdx.x;
+  if (!B.mode[bunch])
+    return;
+  CsrDevState *st = B.st + bunch;
+  const int nb = a.nBins;
+  const double dct = st->dct;
+  wake_filters<unsigned int, unsigned long long>(counts_all + (size_t)bunch * nb, a, dct, sm, nullptr);
+  const double *hist = sm, *deriv = sm + nb;
+  double *phi = sm + 4 * nb;
+  if (!(dct > 0)) {
+    for (int ib = threadIdx.x; ib < nb; ib += blockDim.x)
+      st->dGamma[ib] = 0;
+    return;
+  }
+  if (threadIdx.x == 0) {
+    double last = st->phi_last;
+    for (int ib = 0; ib < nb; ib++) {
+      phi[ib] = -1;
+      if (ib * dct > sa.dsMax)
+        break;
+      phi[ib] = stupakov_phi(sa.x, ib * dct / sa.rho, sa.theta, &last);
+    }
+    st->phi_last = last;
+  }
+  __syncthreads();
+  const long long diC = clamp_bins(sa.dsC / dct, nb), diD = clamp_bins(sa.dsMax / dct, nb);
+  const double fC = -1 / (sa.theta + 2 * sa.x), factor = -4 / sa.rho * B.csr_const[2 * B.n + bunch] * sa.dz0;
+  for (int ib = threadIdx.x; ib < nb; ib += blockDim.x) {
+    double g = ib + diC < nb ? fC * hist[ib + diC] : 0, term1 = 0, term2 = 0;
+    if (ib + diD < nb)
+      g = g + hist[ib + diD] / (sa.theta + 2 * sa.x);
+    int count = 0;
+    for (int j = ib; j < nb; j++) {
+      const double p = phi[j - ib];
+      if (!(p >= 0))
+        break;
+      if (p > 0) {
+        term2 = deriv[j] / (p + 2 * sa.x);
+        g = g - term2;
+        if (count == 0)
+          term1 = term2;
+        count++;
+      }
+    }
+    if (count > 1 && sa.trapz)
+      g = g + (term1 + term2) / 2;
+    st->dGamma[ib] = g * factor;
+  }
+}
+
+/* kick from the wake and c*t back to s at the new velocity (csbend.c:4078-4096) */
+__global__ void stupakov_kick_kernel(DevParticles P, int64_t n, CsrBunches B, int nBins, double Po) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  const int b = bunch_of(i, B);
+  if (!B.mode[b])
+    return;
+  const CsrDevState *st = B.st + b;
+  const double ct = P.s[i];
+  double dp = P.dp[i], f = (ct - st->ctLower) / st->dct;
+  const long long iBin = (long long)f;
+  f -= iBin;
+  if (iBin >= 0 && iBin < nBins - 1)
+    dp = dp + ((1 - f) * st->dGamma[iBin] + f * st->dGamma[iBin + 1]) / Po;
+  const double p = (1 + dp) * Po, beta = p / sqrt(p * p + 1);
+  P.dp[i] = dp;
+  P.s[i] = beta * ct;
+}
+
 /* empty min/max keys of every bunch before a binning pass */
 __global__ void csr_reset_keys_kernel(CsrBunches B) {
   for (int b = threadIdx.x; b < B.n; b += blockDim.x) {
@@ -885,8 +1049,17 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
       ce.binRangeFactor = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
       ce.dzf = d.c[CB_DZF];
       ce.z_end = d.z_end;
-      ce.same_bend_precedes = idx > 0 && el[idx - 1].type == B2E_CSRCSBEND &&
-                              strncmp(el[idx - 1].name, e.name, sizeof(e.name)) == 0;
+      /* SAME_BEND_PRECEDES of determine_bend_flags (bend_matrix.c:1342-1363):
+       * MARKs in between are transparent */
+      ce.same_bend_precedes = 0;
+      for (int j = idx - 1; j >= 0; j--) {
+        if (el[j].type == B2E_CSRCSBEND && strncmp(el[j].name, e.name, sizeof(e.name)) == 0) {
+          ce.same_bend_precedes = 1;
+          break;
+        }
+        if (el[j].type != B2E_MARK)
+          break;
+      }
       /* per-bin Savitzky-Golay weights for smoothing (order sgOrder, derivative 0)
        * and for the derivative (order sgdOrder, derivative 1) */
       st.sg_offset.push_back(sgw.size());
@@ -912,10 +1085,7 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
       }
     } else {
       const double *p = e.p;
-      if (p[B2E_CSRDRIFT_USE_STUPAKOV] != 0) {
-        err = "CSRDRIFT USE_STUPAKOV=1 is not available in this build";
-        return B2E_ERR_LATTICE;
-      }
+      ce.stupakov = p[B2E_CSRDRIFT_USE_STUPAKOV] != 0;
       ce.drift_length = p[B2E_CSRDRIFT_L];
       ce.drift_dz = p[B2E_CSRDRIFT_DZ];
       ce.drift_kicks = (int)p[B2E_CSRDRIFT_N_KICKS];
@@ -925,6 +1095,27 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
     }
     st.elems.push_back(ce);
   }
+  /* one CSRDRIFT mode behind each dipole (csbend.c:3259-3263 stops the run
+   * otherwise); the line is read cyclically, as drifts ahead of the first
+   * dipole follow the last one on the next pass */
+  {
+    const int ne = (int)st.elems.size();
+    int mode = -1;
+    for (int k = 0; k < 2 * ne; k++) {
+      const CsrElem &c = st.elems[k % ne];
+      if (c.kind == K_CSRCSBEND)
+        mode = -1;
+      else if (c.drift_csr) {
+        if (mode >= 0 && mode != c.stupakov) {
+          err = "CSRDRIFT mode changed between dipoles. Pick one mode following each dipole.";
+          return B2E_ERR_LATTICE;
+        }
+        mode = c.stupakov;
+      }
+    }
+  }
+  st.revolution_length = lat.total_length;
+  st.last_bend = -1;
   if (csr_set_bunches(st, 1, nullptr, err))
     return B2E_ERR_NOMEM;
   if (!sgw.empty()) {
@@ -969,7 +1160,7 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
   st.macro_charge.assign(n_bunches, 0.0);
   if (cudaMalloc(&st.d_state, sizeof(CsrDevState) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS * n_bunches) != cudaSuccess ||
-      cudaMalloc(&st.d_csr_const, 2 * sizeof(double) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_csr_const, 3 * sizeof(double) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_flags, 2 * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_keys, 2 * sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
@@ -977,8 +1168,13 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
     return B2E_ERR_NOMEM;
   }
   cudaMemset(st.d_state, 0, sizeof(CsrDevState) * n_bunches);
-  cudaMemset(st.d_csr_const, 0, 2 * sizeof(double) * n_bunches);
+  cudaMemset(st.d_csr_const, 0, 3 * sizeof(double) * n_bunches);
   cudaMemset(st.d_flags, 0, 2 * n_bunches);
+  csr_init_state_kernel<<<1, 256>>>((CsrDevState *)st.d_state, n_bunches);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    err = "CSR state initialisation failed";
+    return B2E_ERR_CUDA;
+  }
   return B2E_OK;
 }
 
@@ -1063,6 +1259,7 @@ void csr_reset(CsrState &st) {
     cudaMemset(st.d_sur_counts, 0, 2 * sizeof(unsigned long long));
   st.accumulated_angle = 0;
   st.wake_valid.assign(st.n_bunches, 0);
+  st.last_bend = -1;
 }
 
 static int ensure_wakelog(CsrState &st, int64_t values) {
@@ -1134,6 +1331,97 @@ static int ensure_surrogate_buffers(CsrState &st, int64_t gate_values, std::stri
   return B2E_OK;
 }
 
+/* CSRDRIFT with USE_STUPAKOV=1 (track_through_driftCSR_Stupakov,
+ * csbend.c:3803-4159) for the bunches whose mode flag is set; the others have
+ * had their exact drift.  Per kick: drift and c*t with the min/max keys, the
+ * histogram of the last dipole's bin count and range factor, the wake (one
+ * CTA per bunch), the kick; then the closing half drift. */
+static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, const DevParticles &P, int64_t n,
+                          double zStart, cudaStream_t stream, std::string &err, int64_t *launches) {
+  if (st.last_bend < 0) {
+    err = "CSRDRIFT: no dipole wake to follow";
+    return B2E_ERR_STATE;
+  }
+  const CsrElem &bend = st.elems[st.last_bend];
+  const int nb = bend.bins, nbunch = B.n, g = grid_for(n);
+  const double Po = st.p_central, rho = st.last_rho, theta = st.last_theta;
+  double length = ce.drift_length, dz_back = 0;
+  if (zStart != st.zLast) {
+    length += (dz_back = zStart - st.zLast);
+    zStart = st.zLast;
+  }
+  long nKicks;
+  if (ce.drift_dz > 0) {
+    if ((nKicks = (long)(length / ce.drift_dz + 0.5)) < 1)
+      nKicks = 1;
+  } else
+    nKicks = ce.drift_kicks;
+  if (nKicks <= 0) {
+    err = "nKicks=0 in CSR drift.";
+    return B2E_ERR_LATTICE;
+  }
+  const double dz0 = length / nKicks;
+  double dz = dz0 / 2, zTravel = zStart - st.z0;
+  const double *sgw = st.d_sg + st.sg_offset[st.last_bend];
+  const int *sgi = st.d_sg_idx + st.sg_offset[st.last_bend] / B2E_SG_MAX_WIDTH * 2;
+  WakeArgs a = {};
+  a.nBins = nb;
+  a.sgHalf = bend.sgHalf;
+  a.sgdHalf = bend.sgdHalf;
+  a.trapz = bend.trapz;
+  a.correct = bend.sgHalf > 0;
+  a.sg_w = sgw;
+  a.sgd_w = sgw + (size_t)nb * B2E_SG_MAX_WIDTH;
+  a.sg_lo = sgi;
+  a.sg_n = sgi + 1;
+  a.sgd_lo = sgi + 2 * nb;
+  a.sgd_n = sgi + 2 * nb + 1;
+  const size_t smem = sizeof(double) * 5 * nb;
+  CSR_CUDA(cudaFuncSetAttribute(stupakov_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CsrBunches H = B; /* the histogram bins the bunches in this mode */
+  H.active = B.mode;
+  for (long iKick = 0; iKick < nKicks; iKick++) {
+    if (iKick == 1)
+      dz = dz0;
+    zTravel += dz;
+    StupakovArgs sa;
+    sa.x = zTravel / rho;
+    sa.dsMax = rho / 24 * b2e_pow(theta, 3) * (theta + 4 * sa.x) / (theta + sa.x);
+    sa.dsC = rho / 6 * (theta * theta) * (theta + 3 * sa.x);
+    sa.theta = theta;
+    sa.rho = rho;
+    sa.dz0 = dz0;
+    sa.trapz = bend.trapz;
+    csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
+    stupakov_drift_kernel<<<g, 256, 0, stream>>>(P, n, B, iKick == 0 ? dz_back : 0.0, dz, Po);
+    (*launches) += 2;
+    CSR_CUDA(cudaGetLastError());
+    int rrc = reduce_keys(st, B, stream, err, launches);
+    if (rrc)
+      return rrc;
+    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * nb * nbunch, stream));
+    const int64_t per = (n + nbunch - 1) / nbunch;
+    const int hb = (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 4 / nbunch), std::max<int64_t>(1, (per + 1023) / 1024));
+    csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * nb, stream>>>(P, n, H, st.d_counts, nb,
+                                                                                  bend.binRangeFactor);
+    (*launches)++;
+    CSR_CUDA(cudaGetLastError());
+    if (st.reducer && st.reducer(st.reducer_user, B2E_REDUCE_SUM_U32, st.d_counts, (int64_t)nb * nbunch, stream)) {
+      err = "CSR: the all-rank reduction of the histogram failed";
+      return B2E_ERR_CUDA;
+    }
+    stupakov_wake_kernel<<<nbunch, 1024, smem, stream>>>(B, st.d_counts, a, sa);
+    stupakov_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, nb, Po);
+    (*launches) += 2;
+    CSR_CUDA(cudaGetLastError());
+  }
+  edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz0 / 2, B, 1);
+  (*launches)++;
+  CSR_CUDA(cudaGetLastError());
+  st.zLast = zStart + length;
+  return B2E_OK;
+}
+
 int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_elem, const DevParticles &P, int64_t n,
                       const std::vector<int64_t> &alive, int elem, int pass, cudaStream_t stream, std::string &err,
                       int64_t *launches) {
@@ -1187,6 +1475,11 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       CSR_CUDA(cudaGetLastError());
     }
     double zStart = ce.z_start;
+    /* a drift behind the previous pass's dipole (csbend.c:3251-3255) */
+    for (int guard = 0; zStart + 1e-12 < st.zLast && st.revolution_length > 0 && guard < (1 << 20); guard++)
+      zStart += st.revolution_length;
+    if (ce.stupakov)
+      return stupakov_drift(st, ce, B, P, n, zStart, stream, err, launches);
     int nKicks;
     if (ce.drift_dz > 0) {
       if ((nKicks = (int)(ce.drift_length / ce.drift_dz)) < 1)
@@ -1199,10 +1492,9 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     }
     double dz0 = ce.drift_length / nKicks, dz = dz0 / 2;
     double dzFirst = zStart - st.zLast;
-    int lastBins = 0; /* csrWake.bins: bins of the last CSRCSBEND */
-    for (size_t j = 0; j < st.elems.size(); j++)
-      if (st.elems[j].kind == K_CSRCSBEND && st.elems[j].index < elem)
-        lastBins = st.elems[j].bins;
+    /* csrWake.bins: bins of the last CSRCSBEND tracked (on a later pass,
+     * possibly one further down the line) */
+    const int lastBins = st.last_bend >= 0 ? st.elems[st.last_bend].bins : 0;
     for (int iKick = 0; iKick < nKicks; iKick++) {
       if (iKick == 1)
         dz = dz0;
@@ -1250,15 +1542,17 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   st.zLast = st.z0 = ce.z_end;
   /* CSRConstant (csbend.c:2378-2381), per bunch */
   const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
-  std::vector<double> csr_constant(2 * nbunch, 0.0);
+  std::vector<double> csr_constant(3 * nbunch, 0.0);
   for (int b = 0; b < nbunch; b++) {
     if (ce.csr && flags[b])
       csr_constant[b] = 2 * st.macro_charge[b] * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) /
                         (4 * kPI * eps0 * kME * (kC * kC));
     /* the IGF wake's factor (csbend.c:2678-2679) */
     csr_constant[nbunch + b] = -st.macro_charge[b] / (kME * (kC * kC)) * ce.length / ce.nSlices;
+    /* GSConstant for a Stupakov CSRDRIFT (csbend.c:2999) */
+    csr_constant[2 * nbunch + b] = csr_constant[b] * b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) / 2;
   }
-  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), 2 * sizeof(double) * nbunch, cudaMemcpyHostToDevice,
+  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), 3 * sizeof(double) * nbunch, cudaMemcpyHostToDevice,
                            stream));
   CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
   const double *sgw = st.d_sg + st.sg_offset[k];
@@ -1378,6 +1672,10 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   CSR_CUDA(cudaGetLastError());
   for (int b = 0; b < nbunch; b++)
     st.wake_valid[b] = flags[b];
+  /* csrWake.rho, csrWake.bendingAngle (csbend.c:2992-2993) */
+  st.last_bend = (int)k;
+  st.last_rho = h_elem.c[CB_RHO_ACTUAL];
+  st.last_theta = ce.same_bend_precedes ? fabs(phiBend) : ce.angle;
   st.accumulated_angle += ce.angle;
   if (use_net && wakenet_take_status(st.net, stream)) {
     err = "CSR: a bounded wait in the wake network gave up";

@@ -36,7 +36,7 @@ struct CsrElem {
   std::vector<double> sg_w, sgd_w;                    /* per bin weights, B2E_SG_MAX_WIDTH each */
   /* CSRDRIFT */
   double drift_length = 0, drift_dz = 0, z_start = 0;
-  int drift_kicks = 1, drift_csr = 1;
+  int drift_kicks = 1, drift_csr = 1, stupakov = 0;
 };
 
 struct CsrState {
@@ -56,7 +56,7 @@ struct CsrState {
   int64_t beta0_cap = 0;
   void *d_state = nullptr;        /* CsrDevState[n_bunches] */
   unsigned int *d_counts = nullptr; /* [n_bunches][B2E_CSR_MAX_BINS] */
-  double *d_csr_const = nullptr;  /* [2][n_bunches]: CSRConstant, IGF wake factor */
+  double *d_csr_const = nullptr;  /* [3][n_bunches]: CSRConstant, IGF wake factor, GSConstant */
   unsigned char *d_flags = nullptr; /* [2][n_bunches]: active, CSRDRIFT mode */
   unsigned long long *d_alive = nullptr; /* [n_bunches] */
   /* optional all-rank reduction (a bunch spread over several GPUs) */
@@ -69,6 +69,13 @@ struct CsrState {
   double *d_wakelog = nullptr;
   int64_t wakelog_cap = 0;
   double ds0 = 0, zLast = 0, z0 = 0;
+  double revolution_length = 0;   /* added to a CSRDRIFT's start behind the last dipole */
+  /* what the last CSRCSBEND leaves for a Stupakov CSRDRIFT (csbend.c:2991-3003):
+   * its entry in elems (bins, SG tables, range factor, trapezoid rule), the
+   * actual bending radius and the bending angle; GSConstant is per bunch in
+   * d_csr_const[2][b] */
+  int last_bend = -1;
+  double last_rho = 0, last_theta = 0;
   /* learned wake integral (optional): a trained wake network replaces the T1
    * integral of CSRCSBEND kicks, checked on every kick against the plain
    * integral at every gate_stride-th bin; above gate_tol relative rms error

@@ -111,16 +111,23 @@ def ensemble(n_instances: int = 512, seed: int = 2024, n_min: int = 500, n_max: 
 CHICANE_P_MEV = 1000.0
 
 
-def chicane(bins: int = 600, n_kicks: int = 20, sg_halfwidth: int = 2, charge: float = 1e-9) -> Lattice:
+def chicane(bins: int = 600, n_kicks: int = 20, sg_halfwidth: int = 2, charge: float = 1e-9,
+            stupakov: bool = False, drift: dict | None = None) -> Lattice:
+    """Four-dipole chicane with CSR (CSRCSBEND L=0.5 m, angle +-0.05, CSRDRIFT
+    5/1/5 m).  stupakov: CSRDRIFT USE_STUPAKOV=1 instead of mode 0; drift:
+    extra CSRDRIFT parameters (N_KICKS, DZ, CSR)."""
     b = {"L": 0.5, "N_KICKS": n_kicks, "BINS": bins, "SG_HALFWIDTH": sg_halfwidth}
+    d = dict(drift or {})
+    if stupakov:
+        d["USE_STUPAKOV"] = 1
     return Lattice([
         Element("Q", "CHARGE", {"TOTAL": charge}),
         Element("B1", "CSRCSBEND", dict(b, ANGLE=0.05)),
-        Element("D1", "CSRDRIFT", {"L": 5.0}),
+        Element("D1", "CSRDRIFT", dict(d, L=5.0)),
         Element("B2", "CSRCSBEND", dict(b, ANGLE=-0.05)),
-        Element("D2", "CSRDRIFT", {"L": 1.0}),
+        Element("D2", "CSRDRIFT", dict(d, L=1.0)),
         Element("B3", "CSRCSBEND", dict(b, ANGLE=-0.05)),
-        Element("D3", "CSRDRIFT", {"L": 5.0}),
+        Element("D3", "CSRDRIFT", dict(d, L=5.0)),
         Element("B4", "CSRCSBEND", dict(b, ANGLE=0.05)),
     ])
 

@@ -833,13 +833,14 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
   return itop + 1;
 }
 
-/* ---- CSR: CSRCSBEND and CSRDRIFT (mode 0) -------------------------------- */
+/* ---- CSR: CSRCSBEND and CSRDRIFT (mode 0 and Stupakov) -------------------- */
 #ifdef B2E_ORACLE_LIBM
 #define M_POW13(x) pow(x, 1. / 3.)
 #else
 #define M_POW13(x) b2e_pow13(x)
 #endif
 #include "../elegant_b200/csrc/b2e_sg.h"
+#include "../elegant_b200/csrc/b2e_roots.h"
 
 /* the reference's file-static CSR state (csbend.h:27-63, csbend.c:1932) */
 typedef struct {
@@ -849,6 +850,13 @@ typedef struct {
   double macroParticleCharge;
   double *wakes; /* per-kick dGamma log for the tests */
   long n_wakes, cap_wakes;
+  /* what the last dipole leaves for a Stupakov CSRDRIFT (csbend.c:2991-3003) */
+  double rho, bendingAngle, GSConstant, binRangeFactor;
+  long sgHalf, sgOrder, sgdHalf, sgdOrder;
+  int trapz;
+  int lastMode;       /* 0 none yet, 1 mode 0, 2 Stupakov (csbend.c:3243-3264) */
+  double phiLast;     /* SolveForPhiStupakov's static start value (csbend.c:4177) */
+  double revolutionLength;
 } CsrWake;
 
 /* binParticleCoordinate (csbend.c:3047-3113) on column `ic` of rows c[0..np) */
@@ -926,6 +934,7 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   if (!same_pre)
     cw->accumulatedAngle = 0;
   cw->valid = 0;
+  cw->lastMode = 0; /* reset_driftCSR (csbend.c:3539-3548) */
   if (sgdHalf <= 0)
     sgdHalf = sgHalf;
   if (sgdHalf <= 0)
@@ -1222,8 +1231,18 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
     x[2] += dyf + dzf * x[3];
     x[4] += dzf * sqrt(1 + SQR(x[1]) + SQR(x[3])) + 0.0;
   }
-  if (more_than_one)
+  if (more_than_one) {
     cw->valid = 1;
+    cw->rho = rho_actual;
+    cw->bendingAngle = same_pre ? fabs(phiBend) : fabs(angle);
+    cw->GSConstant = CSRConstant * M_POW13(3 * rho0 * rho0) / 2;
+    cw->binRangeFactor = p[B2E_BEND_BIN_RANGE_FACTOR];
+    cw->sgHalf = sgHalf;
+    cw->sgOrder = sgOrder;
+    cw->sgdHalf = sgdHalf;
+    cw->sgdOrder = sgdOrder;
+    cw->trapz = p[B2E_BEND_TRAPAZOID_INTEGRATION] != 0;
+  }
   cw->accumulatedAngle += fabs(angle);
   free(beta0);
   free(ctHist);
@@ -1234,14 +1253,181 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   return itop + 1;
 }
 
+/* SolveForPhiStupakov (csbend.c:4161-4202): phi with
+ * 24 ds = phi^3 (phi + 4x) / (phi + x); each solve starts from the last one */
+static double stup_x, stup_4x;
+static double stupakov_fn(double phi) { return phi * phi * phi * (phi + stup_4x) / (phi + stup_x); }
+
+static double stupakov_phi(double x, double ds, double phim, double *phiLast) {
+  double phi;
+  if (ds < 0)
+    return -1;
+  if (ds == 0)
+    return 0;
+  ds *= 24;
+  stup_x = x;
+  stup_4x = 4 * x;
+  if (*phiLast == -1)
+    *phiLast = phim / 2;
+  if (fabs(ds - stupakov_fn(phim)) < ds / 1e4) {
+    *phiLast = phim;
+    return phim;
+  }
+  phi = b2e_zero_newton(stupakov_fn, ds, *phiLast, phim / 1000, 3, ds / 1e4);
+  if (phi < 0 || phi > phim || fabs(ds - stupakov_fn(phi)) > ds / 1e4)
+    phi = b2e_zero_interp(stupakov_fn, ds, 0, phim * 1.01, phim / 100, ds / 1e4);
+  if (phi < 0 || phi > phim)
+    return -1;
+  *phiLast = phi;
+  return phi;
+}
+
+/* track_through_driftCSR_Stupakov (csbend.c:3803-4159) without LSC, output
+ * files or filters */
+static long csrdrift_stupakov(double **c, long np, const b2e_element *el, double Po, double zStart, CsrWake *cw) {
+  const double *p = el->p;
+  double length = p[B2E_CSRDRIFT_L], dz, dz0, dzFirst, zTravel, x, dsMax, ds, factor;
+  double ctLower, ctUpper, dct, *ctHist, *ctHistDeriv, *phiSoln, theta = cw->bendingAngle, rho = cw->rho;
+  long nKicks, iKick, ip, iBin, nBins = cw->bins, nBins1 = nBins - 1, nBinned, diBin;
+  if (zStart != cw->zLast) {
+    length += (dzFirst = zStart - cw->zLast);
+    for (ip = 0; ip < np; ip++) {
+      double *v = c[ip];
+      v[0] -= dzFirst * v[1];
+      v[2] -= dzFirst * v[3];
+      v[4] -= dzFirst * sqrt(1 + SQR(v[1]) + SQR(v[3]));
+    }
+    zStart = cw->zLast;
+  }
+  if (p[B2E_CSRDRIFT_DZ] > 0) {
+    if ((nKicks = (long)(length / p[B2E_CSRDRIFT_DZ] + 0.5)) < 1)
+      nKicks = 1;
+  } else
+    nKicks = (long)p[B2E_CSRDRIFT_N_KICKS];
+  dz = (dz0 = length / nKicks) / 2;
+  zTravel = zStart - cw->z0;
+  ctHist = calloc(nBins, sizeof(double));
+  ctHistDeriv = calloc(nBins, sizeof(double));
+  phiSoln = calloc(nBins, sizeof(double));
+  for (iKick = 0; iKick < nKicks; iKick++) {
+    if (iKick == 1)
+      dz = dz0;
+    zTravel += dz;
+    x = zTravel / rho;
+    dsMax = rho / 24 * M_POW(theta, 3) * (theta + 4 * x) / (theta + x);
+    for (ip = 0; ip < np; ip++) {
+      double *v = c[ip], pp, beta;
+      v[0] += v[1] * dz;
+      v[2] += v[3] * dz;
+      pp = Po * (1 + v[5]);
+      beta = pp / sqrt(pp * pp + 1);
+      v[4] = (v[4] + dz * sqrt(1 + SQR(v[1]) + SQR(v[3]))) / beta;
+    }
+    ctLower = ctUpper = dct = 0;
+    nBinned = bin_coordinate(ctHist, nBins, &ctLower, &ctUpper, &dct,
+                             cw->binRangeFactor < 1.1 ? 1.1 : cw->binRangeFactor, c, np, 4);
+    if (cw->sgHalf > 0) {
+      double sum = 0, f;
+      b2e_sg_apply_host(ctHist, nBins, cw->sgOrder, cw->sgHalf, cw->sgHalf, 0);
+      for (iBin = 0; iBin < nBins; iBin++) {
+        if (ctHist[iBin] < 0)
+          ctHist[iBin] = 0;
+        sum += ctHist[iBin];
+      }
+      if (sum) {
+        f = 1.0 * nBinned / sum;
+        for (iBin = 0; iBin < nBins; iBin++)
+          ctHist[iBin] *= f;
+      }
+    }
+    for (iBin = 0; iBin < nBins; iBin++)
+      ctHistDeriv[iBin] = (ctHist[iBin] /= dct);
+    b2e_sg_apply_host(ctHistDeriv, nBins, cw->sgdOrder, cw->sgdHalf, cw->sgdHalf, 1);
+    /* case C */
+    for (iBin = 0; iBin < nBins; iBin++) {
+      ds = rho / 6 * SQR(theta) * (theta + 3 * x);
+      diBin = (long)(ds / dct);
+      if (iBin + diBin < nBins)
+        cw->dGamma[iBin] = -1 / (theta + 2 * x) * ctHist[iBin + diBin];
+      else
+        cw->dGamma[iBin] = 0;
+    }
+    /* case D */
+    for (iBin = 0; iBin < nBins; iBin++) {
+      phiSoln[iBin] = -1;
+      if ((ds = iBin * dct) > dsMax)
+        break;
+      phiSoln[iBin] = stupakov_phi(x, iBin * dct / rho, theta, &cw->phiLast);
+    }
+    for (iBin = 0; iBin < nBins; iBin++) {
+      long jBin, first = 1, count = 0;
+      double term1 = 0, term2 = 0;
+      diBin = (long)(dsMax / dct);
+      if (iBin + diBin < nBins)
+        cw->dGamma[iBin] += ctHist[iBin + diBin] / (theta + 2 * x);
+      for (jBin = iBin; jBin < nBins; jBin++) {
+        double phi;
+        if ((phi = phiSoln[jBin - iBin]) >= 0) {
+          if (phi > 0) {
+            term2 = ctHistDeriv[jBin] / (phi + 2 * x);
+            cw->dGamma[iBin] -= term2;
+            if (first) {
+              term1 = term2;
+              first = 0;
+            }
+            count++;
+          }
+        } else
+          break;
+      }
+      if (count > 1 && cw->trapz)
+        cw->dGamma[iBin] += (term1 + term2) / 2;
+    }
+    factor = -4 / rho * cw->GSConstant * dz0;
+    for (iBin = 0; iBin < nBins; iBin++)
+      cw->dGamma[iBin] *= factor;
+    for (ip = 0; ip < np; ip++) {
+      double *v = c[ip], f, pp, beta;
+      iBin = (long)(f = (v[4] - ctLower) / dct);
+      f -= iBin;
+      if (iBin >= 0 && iBin < nBins1)
+        v[5] += ((1 - f) * cw->dGamma[iBin] + f * cw->dGamma[iBin + 1]) / Po;
+      pp = (1 + v[5]) * Po;
+      beta = pp / sqrt(pp * pp + 1);
+      v[4] = beta * v[4];
+    }
+  }
+  dz = dz0 / 2;
+  for (ip = 0; ip < np; ip++) {
+    double *v = c[ip];
+    v[0] += v[1] * dz;
+    v[2] += v[3] * dz;
+    v[4] += dz * sqrt(1 + SQR(v[1]) + SQR(v[3]));
+  }
+  cw->zLast = zStart + length;
+  free(ctHist);
+  free(ctHistDeriv);
+  free(phiSoln);
+  return np;
+}
+
 static long csrdrift_track(double **c, long np, const b2e_element *el, double Po, double zStart, CsrWake *cw) {
   const double *p = el->p;
   double length = p[B2E_CSRDRIFT_L], dz, dz0, dzFirst, ct0 = 0, factor, dct;
   long nKicks, iKick, ip, nBins1;
+  int mode = p[B2E_CSRDRIFT_USE_STUPAKOV] ? 2 : 1;
   if (np <= 1 || !cw->valid || !p[B2E_CSRDRIFT_CSR]) {
     exact_drift(c, np, length);
     return np;
   }
+  /* csbend.c:3243-3264 */
+  while ((zStart + 1e-12) < cw->zLast && cw->revolutionLength > 0)
+    zStart += cw->revolutionLength;
+  if (cw->lastMode && cw->lastMode != mode)
+    fprintf(stderr, "CSRDRIFT mode changed between dipoles (the reference stops here)\n");
+  cw->lastMode = mode;
+  if (mode == 2)
+    return csrdrift_stupakov(c, np, el, Po, zStart, cw);
   nBins1 = cw->bins - 1;
   dct = cw->dctBin;
   if (p[B2E_CSRDRIFT_DZ] > 0) {
@@ -1303,6 +1489,12 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
   RfState *rf = calloc(n_el ? n_el : 1, sizeof(RfState));
   memset(&ma, 0, sizeof(ma));
   memset(&cw, 0, sizeof(cw));
+  cw.phiLast = -1;
+  for (k = 0; k < n_el; k++)
+    if (el[k].type == B2E_DRIF || el[k].type == B2E_EDRIFT || el[k].type == B2E_KQUAD || el[k].type == B2E_KSEXT ||
+        el[k].type == B2E_CSBEND || el[k].type == B2E_RFCA || el[k].type == B2E_CSRCSBEND ||
+        el[k].type == B2E_CSRDRIFT)
+      cw.revolutionLength += el[k].p[0];
   if (wakes) {
     cw.cap_wakes = 1024;
     cw.wakes = malloc(sizeof(double) * cw.cap_wakes);
@@ -1503,4 +1695,10 @@ void b2e_oracle_wake_t1(const double *counts, long nBins, double slippage_bins, 
   free(ctHist);
   free(ctHistDeriv);
   free(denom);
+}
+
+/* SolveForPhiStupakov restated, for unit tests of the root finders;
+ * *phi_last is the carried start value (-1 before the first solve) */
+double b2e_oracle_stupakov_phi(double x, double ds, double phim, double *phi_last) {
+  return stupakov_phi(x, ds, phim, phi_last);
 }

@@ -2,14 +2,16 @@
  * Restated support routines that the reference's CSR path calls but that live
  * outside the compiled subset: final_props.c (rms_emittance, approximateBeamWidth)
  * and the SDDS toolkit's mdbmth (fill_double_array, index_min_max,
- * SavitzyGolaySmooth).  The Savitzky-Golay convention is the one this project
+ * SavitzyGolaySmooth, zeroNewton, zeroInterp).  The Savitzky-Golay convention is the one this project
  * defines for both the oracle and the CUDA path (b2e_sg.h); the toolkit's own
  * edge treatment is not in the reference tree, so CSR parity at that boundary
- * is against this shared definition.  Test infrastructure only.
+ * is against this shared definition; the same holds for the two root finders
+ * of SolveForPhiStupakov (b2e_roots.h).  Test infrastructure only.
  */
 #include "mdb.h"
 #include "track.h"
 #include "b2e_sg.h"
+#include "b2e_roots.h"
 
 #define ANALYSIS_BINS 10000 /* final_props.c:21 */
 
@@ -111,4 +113,14 @@ double approximateBeamWidth(double fraction, double **part, long nPart, long iCo
 
 long SavitzyGolaySmooth(double *data, long rows, long order, long nLeft, long nRight, long derivativeOrder) {
   return b2e_sg_apply_host(data, rows, order, nLeft, nRight, derivativeOrder);
+}
+
+/* mdbmth's root finders as SolveForPhiStupakov (csbend.c:4189-4195) calls
+ * them, on the shared definitions of b2e_roots.h */
+double zeroNewton(double (*fn)(double), double value, double x_i, double dx, long n_passes, double _zero) {
+  return b2e_zero_newton(fn, value, x_i, dx, n_passes, _zero);
+}
+
+double zeroInterp(double (*fn)(double), double value, double x_i, double x_f, double dx, double _zero) {
+  return b2e_zero_interp(fn, value, x_i, x_f, dx, _zero);
 }

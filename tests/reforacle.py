@@ -31,12 +31,27 @@ def lattice_spec(lattice) -> str:
 
 
 class RefOracle:
-    def __init__(self, math: str = "libm"):
+    def __init__(self, math: str = "libm", private: bool = False):
+        """private=True loads a fresh copy of the library, so that file-static
+        state of the reference (SolveForPhiStupakov's start value, which
+        carries over from one call to the next for the life of an elegant
+        process) starts as in a new process."""
         name = "libb2e_ref.so" if math == "libm" else "libb2e_ref_b2emath.so"
         path = os.path.join(REF_DIR, name)
         if not os.path.exists(path):
             raise FileNotFoundError(path)
-        self.lib = ctypes.CDLL(path)
+        if private:
+            import shutil
+            import tempfile
+            fd, tmp = tempfile.mkstemp(prefix="b2e_ref_", suffix=".so")
+            os.close(fd)
+            shutil.copyfile(path, tmp)
+            try:
+                self.lib = ctypes.CDLL(tmp)
+            finally:
+                os.unlink(tmp)  # the mapping stays valid
+        else:
+            self.lib = ctypes.CDLL(path)
         self.lib.b2e_ref_track.restype = ctypes.c_long
         self.math = math
 

@@ -94,3 +94,12 @@ def test_wakenet_rejects_bad_sizes():
         rc = net.lib.b2e_wakenet_forward(net._h, x.data_ptr(), 3, y.data_ptr(), None)
         assert rc == ERR_ARG  # above the network's maximum batch
         assert net.forward(x).shape == (3, 256)  # the binding splits the batch
+
+
+def test_csrdrift_mode_change_behind_one_dipole_is_rejected():
+    lat = w.chicane(bins=100, n_kicks=2)
+    els = [Element(e.name, e.type, dict(e.params, USE_STUPAKOV=1)) if e.name == "D3" else e for e in lat.elements]
+    els.insert(7, Element("D3B", "CSRDRIFT", {"L": 0.5}))
+    with pytest.raises(EngineError) as e:
+        Tracker(Lattice(els), P0, 1)
+    assert e.value.code == ERR_LATTICE and "mode" in str(e.value)

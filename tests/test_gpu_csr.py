@@ -302,3 +302,45 @@ def test_torch_nccl_reducer_single_rank_is_identity():
     assert np.array_equal(wk, ref_w)
     assert np.array_equal(res.coords, ref.coords)
     assert np.array_equal(res.lost_pass, ref.lost_pass)
+
+
+@pytest.mark.parametrize("case", ["default", "fine_bins_3kicks", "dz", "no_sg", "steady_plain", "gap", "gap_mode0",
+                                  "ring_2p", "ring_mode0_2p"])
+def test_csrdrift_modes_bit_exact(case):
+    """CSRDRIFT in Stupakov mode, a CSRDRIFT starting behind the dipole's
+    wake and one ahead of the first dipole on the second pass: final
+    coordinates and every dipole wake equal elegant's code (a fresh copy of
+    the library per run, as a new elegant process) bit for bit."""
+    from csr_cases import stupakov_cases
+    from reforacle import RefOracle
+    lat = stupakov_cases()[case]
+    passes = 2 if case.endswith("2p") else 1
+    beam = w.chicane_beam(20000, seed=31)
+    with Tracker(lat, P0, passes) as t:
+        res = t.track(beam)
+        wakes = t.csr_wakes(10_000_000)
+    rows, nl, _, ref_wakes = RefOracle("b2e", private=True).track(lat, beam.coords, beam.ids, P0, passes,
+                                                                  capture_wakes=True)
+    check(res, wakes, rows, nl, ref_wakes)
+
+
+def test_stupakov_bunch_train_matches_single_bunches():
+    """Bunches in Stupakov CSRDRIFTs: each bunch's own histogram, wake and
+    phi solutions (its own carried start value) reproduce a separate
+    reference run of that bunch bit for bit; the one-particle bunch drifts."""
+    from reforacle import RefOracle
+    lat = w.chicane(bins=300, n_kicks=4, stupakov=True, drift={"N_KICKS": 2})
+    sizes, chirps = [3000, 1, 7000, 4500], [-10.0, -8.0, -15.0, -5.0]
+    beam, offsets = _bunch_train(sizes, chirps, seed=51)
+    with Tracker(lat, P0, 1) as t:
+        t.load_ensemble(offsets, [])
+        res = t.track(beam)
+    for b in range(len(sizes)):
+        sl = slice(offsets[b], offsets[b + 1])
+        rows, nl, _, _ = RefOracle("b2e", private=True).track(lat, beam.coords[sl], beam.ids[sl], P0, 1)
+        ref_c, ref_ids, ref_loss = by_id(rows)
+        order = np.argsort(res.ids[sl])
+        assert int((res.lost_pass[sl] < 0).sum()) == nl
+        assert np.array_equal(res.ids[sl][order], ref_ids)
+        alive = ref_loss < 0
+        assert np.array_equal(res.coords[sl][order][alive], ref_c[alive]), b

@@ -138,3 +138,66 @@ def test_igf_shared_math_close_to_libm():
     b = by_id(RefOracle("b2e").track(lat, beam.coords, beam.ids, p0, 1)[0])
     assert np.array_equal(a[2], b[2])
     assert _rel(a[0], b[0]).max() <= 1e-10
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("case", ["default", "fine_bins_3kicks", "dz", "no_sg", "steady_plain", "gap", "gap_mode0",
+                                  "ring_2p", "ring_mode0_2p"])
+def test_port_reproduces_reference_csrdrift_modes(math, case):
+    """CSRDRIFT in Stupakov mode (phi solutions, cases C and D), a CSRDRIFT
+    that starts behind the dipole's wake, and one ahead of the first dipole
+    on a second pass: the restatement reproduces elegant's own code bit for
+    bit.  Each reference run loads a fresh copy of the library, so
+    SolveForPhiStupakov's carried start value begins as in a new process."""
+    from csr_cases import stupakov_cases
+    lat = stupakov_cases()[case]
+    passes = 2 if case.endswith("2p") else 1
+    beam = w.chicane_beam(5000, seed=21)
+    p0 = 1000 / 0.51099895
+    r1, n1, _, w1 = RefOracle(math, private=True).track(lat, beam.coords, beam.ids, p0, passes, capture_wakes=True)
+    r2, n2, _, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, passes, capture_wakes=True)
+    assert n1 == n2 and w1.size == w2.size > 0
+    assert np.array_equal(w1, w2)
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+
+
+def test_stupakov_drift_differs_from_mode_0():
+    """The Stupakov wake is a different model from the mode-0 propagated
+    dipole wake: the final momenta differ (by far more than rounding)."""
+    p0 = 1000 / 0.51099895
+    beam = w.chicane_beam(5000, seed=22)
+    a = by_id(RefOracle("b2e").track(w.chicane(bins=200, n_kicks=4), beam.coords, beam.ids, p0, 1)[0])[0]
+    b = by_id(RefOracle("b2e", private=True).track(w.chicane(bins=200, n_kicks=4, stupakov=True), beam.coords,
+                                                   beam.ids, p0, 1)[0])[0]
+    assert np.abs(a[:, 5] - b[:, 5]).max() > 1e-3 * np.abs(a[:, 5]).max()
+
+
+def test_stupakov_phi_solver():
+    """The root finders behind SolveForPhiStupakov: every solution satisfies
+    24 ds = phi^3 (phi + 4x)/(phi + x) to the reference's 1e-4 relative
+    tolerance, x = 0 gives the cube root, a start far from the root still
+    converges (the scanning fallback), and ds beyond phim has no solution."""
+    import ctypes
+    from reforacle import PortOracle as _P
+    lib = _P("b2e").lib
+    f = lib.b2e_oracle_stupakov_phi
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)]
+
+    def fn(p, x):
+        return p * p * p * (p + 4 * x) / (p + x)
+    for x in (0.0, 1e-3, 0.1, 0.5, 3.0):
+        last = ctypes.c_double(-1)
+        for ds in np.geomspace(1e-9, 4e-6, 25):
+            phi = f(x, ds, 0.05, ctypes.byref(last))
+            assert 0 < phi <= 0.05
+            assert abs(24 * ds - fn(phi, x)) <= 24 * ds / 1e4
+            if x == 0.0:
+                assert abs(phi - (24 * ds) ** (1 / 3)) < 1e-4 * phi
+    last = ctypes.c_double(1e-12)
+    phi = f(0.3, 1e-7, 0.05, ctypes.byref(last))
+    assert abs(24e-7 - fn(phi, 0.3)) <= 24e-7 / 1e4
+    last = ctypes.c_double(-1)
+    assert f(0.01, 1.0, 0.05, ctypes.byref(last)) == -1
+    assert f(0.01, 0.0, 0.05, ctypes.byref(last)) == 0
+    assert f(0.01, -1e-9, 0.05, ctypes.byref(last)) == -1
