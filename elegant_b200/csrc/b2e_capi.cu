@@ -243,6 +243,15 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
   return B2E_OK;
 }
 
+extern "C" int b2e_element_defaults(int32_t type, b2e_element *element) {
+  if (!element || type < B2E_DRIF || type > B2E_CSRDRIFT)
+    return B2E_ERR_ARG;
+  element->type = type;
+  element->reserved = 0;
+  b2e::element_defaults(type, element->p);
+  return B2E_OK;
+}
+
 extern "C" int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32_t n_elements,
                                 const b2e_run_options *options) {
   if (!ctx || !elements || n_elements <= 0 || !options)

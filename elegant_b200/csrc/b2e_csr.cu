@@ -13,6 +13,7 @@
 #include <mutex>
 #include "b2e_csr.h"
 #include "b2e_roots.h"
+#include "b2e_fft.h"
 #include "b2e_elements.cuh"
 #include "b2e_kernels.h"
 #include "b2e_sg.h"
@@ -246,7 +247,57 @@ struct WakeArgs {
   /* integrated Green's function (csbend.c:2593-2621, :2676-2680) */
   int igf;
   double gamma2, gamma3, rho0, const1, q4pe, igf_factor;
+  /* low/high-pass filters of the histogram (applyLHPassFilters): on when
+   * HIGH_FREQUENCY_CUTOFF0 > 0 or LOW_FREQUENCY_CUTOFF0 >= 0 */
+  int lh, clip;
+  double startHP, endHP, startLP, endLP;
 };
+
+/* applyLHPassFilters (csbend.c:4611-4703) on hist[0..nb) in one CTA with the
+ * transform of b2e_fft.h; scratch: ri = sm + nb (nb + 2 values), twiddles at
+ * sm + 2 nb + 2 and sm + 3 nb + 2 (the filters' arrays are not yet in use) */
+__device__ void lh_pass_filters(const WakeArgs &a, double *sm) {
+  const int nb = a.nBins, freq = nb / 2 + 1;
+  double *hist = sm, *ri = sm + nb, *tc = sm + 2 * nb + 2, *ts = sm + 3 * nb + 2;
+  __shared__ double orig_sum;
+  for (int t = threadIdx.x; t < nb; t += blockDim.x)
+    b2e_dft_twiddle(nb, t, &tc[t], &ts[t]);
+  __syncthreads();
+  for (int k = threadIdx.x; k < freq; k += blockDim.x)
+    b2e_rdft_pair(hist, nb, k, tc, ts, &ri[2 * k], &ri[2 * k + 1]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    b2e_lh_ramps(ri, freq, a.startHP, a.endHP, a.startLP, a.endLP);
+    double sum = 0;
+    for (int b = 0; b < nb; b++)
+      sum += hist[b];
+    orig_sum = sum;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nb; j += blockDim.x)
+    hist[j] = b2e_rdft_sample(ri, nb, j, tc, ts);
+  __syncthreads();
+  if (a.clip) {
+    /* correctDistribution (csbend.c:4705-4721) to the unfiltered sum */
+    __shared__ double factor;
+    __shared__ int skip;
+    if (threadIdx.x == 0) {
+      double sum = 0;
+      for (int b = 0; b < nb; b++) {
+        if (hist[b] < 0)
+          hist[b] = 0;
+        sum += hist[b];
+      }
+      skip = !sum;
+      factor = skip ? 1 : orig_sum / sum;
+    }
+    __syncthreads();
+    if (!skip)
+      for (int b = threadIdx.x; b < nb; b += blockDim.x)
+        hist[b] = hist[b] * factor;
+    __syncthreads();
+  }
+}
 
 /* Savitzky-Golay pass with precomputed per-bin weights (b2e_sg.h convention);
  * lo/wn point into an interleaved (start, width) table, stride 2 per bin. */
@@ -283,6 +334,8 @@ __device__ void wake_filters(const CountT *counts, const WakeArgs &a, const doub
   for (int b = threadIdx.x; b < nb; b += blockDim.x)
     hist[b] = (double)counts[b];
   __syncthreads();
+  if (a.lh)
+    lh_pass_filters(a, sm);
   if (a.sgHalf > 0) {
     sg_apply(hist, tmp, nb, a.sg_w, a.sg_lo, a.sg_n);
     __syncthreads();
@@ -424,7 +477,7 @@ __device__ void igf_wake(const WakeArgs &a, const double dct, const double *hist
 
 /* Wake of one kick (csbend.c:2566-2673) on one CTA, from a histogram of
  * counts (unsigned counts in tracking, real-valued counts for batched
- * profiles).  sm holds 4*nBins doubles.  Writes dgamma[nBins], the wake log
+ * profiles).  sm holds 4*nBins + 8 doubles.  Writes dgamma[nBins], the wake log
  * when a.wakelog is set, the binned total when nbinned_out is set, and the
  * smoothed density (per unit ct) and its derivative when hist_out/deriv_out
  * are set. */
@@ -470,7 +523,7 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
 
 /* wake of one kick, one CTA per bunch; c1 and c2 from the bunch's CSRConstant
  * in the host expression's order (csbend.c:2664-2667) */
-__global__ void csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a) {
+__global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a) {
   extern __shared__ double sm[];
   const int bunch = blockIdx.x;
   if (!B.active[bunch])
@@ -838,7 +891,7 @@ __device__ __forceinline__ long long clamp_bins(double d, int nb) {
  * histogram filters of the last dipole, phi solutions (serial, each starting
  * from the previous one), then per bin case C, case D's boundary term and its
  * integral in the reference's order, times -4/rho GSConstant dz0.  Shared
- * memory: 4 nBins doubles for the filters, nBins for phi. */
+ * memory: 4 nBins + 8 doubles for the filters, nBins for phi. */
 __global__ void __launch_bounds__(1024, 1) stupakov_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a, StupakovArgs sa) {
   extern __shared__ double sm[];
   const int bunch = blockIdx.x;
@@ -849,7 +902,7 @@ __global__ void __launch_bounds__(1024, 1) stupakov_wake_kernel(CsrBunches B, co
   const double dct = st->dct;
   wake_filters<unsigned int, unsigned long long>(counts_all + (size_t)bunch * nb, a, dct, sm, nullptr);
   const double *hist = sm, *deriv = sm + nb;
-  double *phi = sm + 4 * nb;
+  double *phi = sm + 4 * nb + 8;
   if (!(dct > 0)) {
     for (int ib = threadIdx.x; ib < nb; ib += blockDim.x)
       st->dGamma[ib] = 0;
@@ -1043,6 +1096,12 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
         return B2E_ERR_LATTICE;
       }
       ce.csr = p[B2E_BEND_CSR] != 0;
+      ce.lowCut0 = p[B2E_BEND_LOW_FREQUENCY_CUTOFF0];
+      ce.lowCut1 = p[B2E_BEND_LOW_FREQUENCY_CUTOFF1];
+      ce.highCut0 = p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0];
+      ce.highCut1 = p[B2E_BEND_HIGH_FREQUENCY_CUTOFF1];
+      ce.lh = ce.highCut0 > 0 || ce.lowCut0 >= 0;
+      ce.clip = p[B2E_BEND_CLIP_NEGATIVE_BINS] != 0;
       ce.angle = fabs(p[B2E_BEND_ANGLE]);
       ce.length = p[B2E_BEND_L];
       ce.rho0 = d.c[CB_RHO0];
@@ -1331,6 +1390,19 @@ static int ensure_surrogate_buffers(CsrState &st, int64_t gate_values, std::stri
   return B2E_OK;
 }
 
+/* the filter arguments of applyLHPassFilters as the dipole passes them: the
+ * low-frequency cutoffs are the high-pass ramp, the high-frequency cutoffs
+ * the low-pass ramp (csbend.c:2559-2562) */
+static void set_filter_args(WakeArgs &a, int lh, int clip, double lowCut0, double lowCut1, double highCut0,
+                            double highCut1) {
+  a.lh = lh;
+  a.clip = clip;
+  a.startHP = lowCut0;
+  a.endHP = lowCut1;
+  a.startLP = highCut0;
+  a.endLP = highCut1;
+}
+
 /* CSRDRIFT with USE_STUPAKOV=1 (track_through_driftCSR_Stupakov,
  * csbend.c:3803-4159) for the bunches whose mode flag is set; the others have
  * had their exact drift.  Per kick: drift and c*t with the min/max keys, the
@@ -1376,7 +1448,8 @@ static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, 
   a.sg_n = sgi + 1;
   a.sgd_lo = sgi + 2 * nb;
   a.sgd_n = sgi + 2 * nb + 1;
-  const size_t smem = sizeof(double) * 5 * nb;
+  set_filter_args(a, bend.lh, bend.clip, bend.lowCut0, bend.lowCut1, bend.highCut0, bend.highCut1);
+  const size_t smem = sizeof(double) * (5 * nb + 8);
   CSR_CUDA(cudaFuncSetAttribute(stupakov_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CsrBunches H = B; /* the histogram bins the bunches in this mode */
   H.active = B.mode;
@@ -1557,12 +1630,12 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
   const double *sgw = st.d_sg + st.sg_offset[k];
   const int *sgi = st.d_sg_idx + st.sg_offset[k] / B2E_SG_MAX_WIDTH * 2;
-  const size_t wake_smem = sizeof(double) * 4 * ce.bins;
+  const size_t wake_smem = sizeof(double) * (4 * ce.bins + 8);
   CSR_CUDA(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wake_smem));
   /* learned wake: trained on the transient integral with trapezoid rule (the
    * CSRCSBEND defaults); other settings, or a bunch train larger than the
    * network's batch, use the plain integral */
-  const bool use_net = st.net && any_active && !ce.steady && ce.trapz && ce.bins <= wakenet_bins(st.net) &&
+  const bool use_net = st.net && any_active && !ce.steady && ce.trapz && !ce.lh && ce.bins <= wakenet_bins(st.net) &&
                        nbunch <= wakenet_max_batch(st.net);
   const size_t sur_smem = sizeof(double) * (3 * ce.bins + 1024);
   if (use_net) {
@@ -1603,7 +1676,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     }
     phiBend += ce.angle / ce.nSlices;
     double slippage = fabs(ce.rho0 * (phiBend * phiBend * phiBend) / 24.0);
-    WakeArgs a;
+    WakeArgs a = {};
     a.nBins = ce.bins;
     a.sgHalf = ce.sgHalf;
     a.sgdHalf = ce.sgdHalf;
@@ -1623,6 +1696,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     a.c1 = a.c2 = a.csr_constant = 0; /* per bunch in the kernel */
     a.wakelog = st.d_wakelog + st.wake_values;
     a.igf = ce.igf;
+    set_filter_args(a, ce.lh, ce.clip, ce.lowCut0, ce.lowCut1, ce.highCut0, ce.highCut1);
     {
       /* gamma^2, gamma^3 and the IGF constants as the reference forms them
        * (csbend.c:1981-1982, :2604, :2617) */
@@ -1976,7 +2050,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     STATIC_TRY(cudaGetLastError());
     phiBend += angle / nSlices;
     double slippage = fabs(rho0 * (phiBend * phiBend * phiBend) / 24.0);
-    WakeArgs a;
+    WakeArgs a = {};
     a.nBins = bins;
     a.sgHalf = sgHalf;
     a.sgdHalf = sgdHalf;
@@ -1996,13 +2070,17 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     a.c1 = a.c2 = a.csr_constant = 0; /* formed in the kernel from B.csr_const */
     a.wakelog = dev_wakes ? dev_wakes + (size_t)kick * bins : nullptr;
     a.igf = p[B2E_BEND_IGF] != 0;
+    set_filter_args(a, p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0] > 0 || p[B2E_BEND_LOW_FREQUENCY_CUTOFF0] >= 0,
+                    p[B2E_BEND_CLIP_NEGATIVE_BINS] != 0, p[B2E_BEND_LOW_FREQUENCY_CUTOFF0],
+                    p[B2E_BEND_LOW_FREQUENCY_CUTOFF1], p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0],
+                    p[B2E_BEND_HIGH_FREQUENCY_CUTOFF1]);
     a.gamma2 = Po * Po + 1;
     a.gamma3 = b2e_pow(a.gamma2, 3. / 2);
     a.rho0 = rho0;
     a.const1 = 6.0 - b2e_log(27.0 / 4.0);
     a.q4pe = kE / (4 * kPI * eps0);
     a.igf_factor = 0;
-    size_t smem = sizeof(double) * 4 * bins;
+    size_t smem = sizeof(double) * (4 * bins + 8);
     STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a);
     STATIC_TRY(cudaGetLastError());
@@ -2050,7 +2128,7 @@ extern "C" int b2e_csr_wake_batch(const double *dev_counts, const double *dev_sl
   }
   static_sg_weights_kernel<<<(2 * bins + 127) / 128, 128, 0, s>>>(bins, sg_halfwidth, sg_order, sgd_halfwidth,
                                                                   sgd_order, w, idx);
-  WakeArgs a;
+  WakeArgs a = {};
   a.nBins = bins;
   a.sgHalf = sg_halfwidth;
   a.sgdHalf = sgd_halfwidth;

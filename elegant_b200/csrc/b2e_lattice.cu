@@ -91,11 +91,17 @@ void element_defaults(int type, double *p) {
     p[B2E_BEND_EDGE1_EFFECTS] = 1;
     p[B2E_BEND_EDGE2_EFFECTS] = 1;
     p[B2E_BEND_EDGE_ORDER] = 1;
-    p[B2E_BEND_BIN_RANGE_FACTOR] = 1.2; /* csrcsbend_param, track_data.c:1982-2060 */
-    p[B2E_BEND_SG_ORDER] = 1;
-    p[B2E_BEND_TRAPAZOID_INTEGRATION] = 1;
-    p[B2E_BEND_CSR] = 1;
-    p[B2E_BEND_CLIP_NEGATIVE_BINS] = 1;
+    if (type == B2E_CSRCSBEND) {
+      p[B2E_BEND_BIN_RANGE_FACTOR] = 1.2; /* csrcsbend_param, track_data.c:1982-2060 */
+      p[B2E_BEND_SG_ORDER] = 1;
+      p[B2E_BEND_TRAPAZOID_INTEGRATION] = 1;
+      p[B2E_BEND_CSR] = 1;
+      p[B2E_BEND_CLIP_NEGATIVE_BINS] = 1;
+      p[B2E_BEND_LOW_FREQUENCY_CUTOFF0] = -1; /* track_data.c:2046-2049 */
+      p[B2E_BEND_LOW_FREQUENCY_CUTOFF1] = -1;
+      p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0] = -1;
+      p[B2E_BEND_HIGH_FREQUENCY_CUTOFF1] = -1;
+    }
     break;
   case B2E_RFCA:
     p[B2E_RFCA_FREQ] = 500e6;           /* track_data.c:580 */

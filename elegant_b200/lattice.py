@@ -41,7 +41,9 @@ _BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "
          "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
          "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18}
 _CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=23, SGDERIV_HALFWIDTH=24,
-                SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29, IGF=30)
+                SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29, IGF=30,
+                LOW_FREQUENCY_CUTOFF0=31, LOW_FREQUENCY_CUTOFF1=32, HIGH_FREQUENCY_CUTOFF0=33,
+                HIGH_FREQUENCY_CUTOFF1=34)
 
 # parameter name -> slot, per engine type
 SLOTS = {
@@ -66,7 +68,8 @@ DEFAULTS = {
                  "EDGE_ORDER": 1},
     nat.CSRCSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
                     "EDGE_ORDER": 1, "BIN_RANGE_FACTOR": 1.2, "SG_ORDER": 1, "TRAPAZOID_INTEGRATION": 1, "CSR": 1,
-                    "CLIP_NEGATIVE_BINS": 1},
+                    "CLIP_NEGATIVE_BINS": 1, "LOW_FREQUENCY_CUTOFF0": -1, "LOW_FREQUENCY_CUTOFF1": -1,
+                    "HIGH_FREQUENCY_CUTOFF0": -1, "HIGH_FREQUENCY_CUTOFF1": -1},
     nat.RFCA: {"FREQ": 500e6, "T_REFERENCE": -1},
     nat.MAXAMP: {"EXPONENT": 2},
     nat.CSRDRIFT: {"N_KICKS": 1, "CSR": 1},

@@ -119,6 +119,14 @@ extern "C" {
 #define B2E_BEND_CSR 28
 #define B2E_BEND_CLIP_NEGATIVE_BINS 29
 #define B2E_BEND_IGF 30 /* integrated Green's function, steady state only (csbend.c:2593-2621) */
+/* CSRCSBEND histogram filters (applyLHPassFilters, csbend.c:2557-2562,
+ * :4611-4703), in units of the Nyquist frequency; elegant's defaults are -1
+ * (off): b2e_element_defaults sets them, a zero LOW_FREQUENCY_CUTOFF0 turns
+ * the filter path on */
+#define B2E_BEND_LOW_FREQUENCY_CUTOFF0 31
+#define B2E_BEND_LOW_FREQUENCY_CUTOFF1 32
+#define B2E_BEND_HIGH_FREQUENCY_CUTOFF0 33
+#define B2E_BEND_HIGH_FREQUENCY_CUTOFF1 34
 /* RFCA (rfca_param, track_data.c:576) */
 #define B2E_RFCA_L 0
 #define B2E_RFCA_VOLT 1
@@ -186,6 +194,12 @@ const char *b2e_last_error(const b2e_ctx *ctx);
 int b2e_version(void);
 
 /* ---- lattice ----------------------------------------------------------- */
+/* Fill *element with elegant's parameter defaults for `type` (the tables of
+ * track_data.c for the supported parameters; zero elsewhere) and set its
+ * type; the name is left as it is.  A caller sets the parameters it gives on
+ * top.  Returns B2E_ERR_ARG for an unknown type.  No device needed. */
+int b2e_element_defaults(int32_t type, b2e_element *element);
+
 /* Replaces the parsed element list that do_tracking walks (ELEMENT_LIST,
  * track.h:290-344) with a flat array.  Parameters are validated here. */
 int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32_t n_elements,

@@ -841,6 +841,7 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
 #endif
 #include "../elegant_b200/csrc/b2e_sg.h"
 #include "../elegant_b200/csrc/b2e_roots.h"
+#include "../elegant_b200/csrc/b2e_fft.h"
 
 /* the reference's file-static CSR state (csbend.h:27-63, csbend.c:1932) */
 typedef struct {
@@ -856,8 +857,47 @@ typedef struct {
   int trapz;
   int lastMode;       /* 0 none yet, 1 mode 0, 2 Stupakov (csbend.c:3243-3264) */
   double phiLast;     /* SolveForPhiStupakov's static start value (csbend.c:4177) */
+  double lowCut0, lowCut1, highCut0, highCut1; /* csrWake's filter cutoffs (csbend.c:2272-2276) */
+  int clip;
   double revolutionLength;
 } CsrWake;
+
+/* applyLHPassFilters (csbend.c:4611-4703) with the transform of b2e_fft.h;
+ * returns the number of bins clipped */
+static long lh_pass_filters(double *hist, long bins, double startHP, double endHP, double startLP, double endLP,
+                            int clip) {
+  double *ri = malloc(sizeof(double) * (bins + 2)), *c = malloc(sizeof(double) * bins);
+  double *s = malloc(sizeof(double) * bins), sum = 0, sum2, factor;
+  long i, nz = 0, freq = bins / 2 + 1;
+  for (i = 0; i < bins; i++)
+    b2e_dft_twiddle(bins, i, &c[i], &s[i]);
+  for (i = 0; i < freq; i++)
+    b2e_rdft_pair(hist, bins, i, c, s, &ri[2 * i], &ri[2 * i + 1]);
+  b2e_lh_ramps(ri, freq, startHP, endHP, startLP, endLP);
+  for (i = 0; i < bins; i++)
+    sum += hist[i];
+  for (i = 0; i < bins; i++)
+    hist[i] = b2e_rdft_sample(ri, bins, i, c, s);
+  if (clip) {
+    /* correctDistribution (csbend.c:4705-4721) */
+    for (i = 0, sum2 = 0; i < bins; i++) {
+      if (hist[i] < 0) {
+        nz++;
+        hist[i] = 0;
+      }
+      sum2 += hist[i];
+    }
+    if (sum2) {
+      factor = sum / sum2;
+      for (i = 0; i < bins; i++)
+        hist[i] *= factor;
+    }
+  }
+  free(ri);
+  free(c);
+  free(s);
+  return nz;
+}
 
 /* binParticleCoordinate (csbend.c:3047-3113) on column `ic` of rows c[0..np) */
 static long bin_coordinate(double *hist, long bins, double *lower, double *upper, double *dct, double factor,
@@ -1002,6 +1042,11 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   cw->bins = nBins;
   cw->ds0 = length / nSlices;
   cw->zLast = cw->z0 = z_end;
+  cw->highCut0 = p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0];
+  cw->highCut1 = p[B2E_BEND_HIGH_FREQUENCY_CUTOFF1];
+  cw->lowCut0 = p[B2E_BEND_LOW_FREQUENCY_CUTOFF0];
+  cw->lowCut1 = p[B2E_BEND_LOW_FREQUENCY_CUTOFF1];
+  cw->clip = p[B2E_BEND_CLIP_NEGATIVE_BINS] != 0;
   /* entrance (csbend.c:2286-2377) */
   for (ip = 0; ip < np; ip++) {
     double *x = c[ip], X, Y, XP, YP, p0, rho;
@@ -1071,6 +1116,10 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
       long diS, diS4, ib;
       ctLower = ctUpper = dct = 0;
       nBinned = bin_coordinate(ctHist, nBins, &ctLower, &ctUpper, &dct, brf, c, np, 4);
+      if (p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0] > 0 || p[B2E_BEND_LOW_FREQUENCY_CUTOFF0] >= 0)
+        lh_pass_filters(ctHist, nBins, p[B2E_BEND_LOW_FREQUENCY_CUTOFF0], p[B2E_BEND_LOW_FREQUENCY_CUTOFF1],
+                        p[B2E_BEND_HIGH_FREQUENCY_CUTOFF0], p[B2E_BEND_HIGH_FREQUENCY_CUTOFF1],
+                        p[B2E_BEND_CLIP_NEGATIVE_BINS] != 0);
       if (sgHalf > 0) {
         double sum = 0, factor;
         b2e_sg_apply_host(ctHist, nBins, sgOrder, sgHalf, sgHalf, 0);
@@ -1326,6 +1375,8 @@ static long csrdrift_stupakov(double **c, long np, const b2e_element *el, double
     ctLower = ctUpper = dct = 0;
     nBinned = bin_coordinate(ctHist, nBins, &ctLower, &ctUpper, &dct,
                              cw->binRangeFactor < 1.1 ? 1.1 : cw->binRangeFactor, c, np, 4);
+    if (cw->highCut0 > 0 || cw->lowCut0 >= 0)
+      lh_pass_filters(ctHist, nBins, cw->lowCut0, cw->lowCut1, cw->highCut0, cw->highCut1, cw->clip);
     if (cw->sgHalf > 0) {
       double sum = 0, f;
       b2e_sg_apply_host(ctHist, nBins, cw->sgOrder, cw->sgHalf, cw->sgHalf, 0);
@@ -1701,4 +1752,10 @@ void b2e_oracle_wake_t1(const double *counts, long nBins, double slippage_bins, 
  * *phi_last is the carried start value (-1 before the first solve) */
 double b2e_oracle_stupakov_phi(double x, double ds, double phim, double *phi_last) {
   return stupakov_phi(x, ds, phim, phi_last);
+}
+
+/* applyLHPassFilters restated, for unit tests of the transform */
+long b2e_oracle_lh_pass_filters(double *hist, long bins, double startHP, double endHP, double startLP, double endLP,
+                                int clip) {
+  return lh_pass_filters(hist, bins, startHP, endHP, startLP, endLP, clip);
 }

@@ -2,16 +2,18 @@
  * Restated support routines that the reference's CSR path calls but that live
  * outside the compiled subset: final_props.c (rms_emittance, approximateBeamWidth)
  * and the SDDS toolkit's mdbmth (fill_double_array, index_min_max,
- * SavitzyGolaySmooth, zeroNewton, zeroInterp).  The Savitzky-Golay convention is the one this project
+ * SavitzyGolaySmooth, zeroNewton, zeroInterp, realFFT2).  The Savitzky-Golay convention is the one this project
  * defines for both the oracle and the CUDA path (b2e_sg.h); the toolkit's own
  * edge treatment is not in the reference tree, so CSR parity at that boundary
  * is against this shared definition; the same holds for the two root finders
- * of SolveForPhiStupakov (b2e_roots.h).  Test infrastructure only.
+ * of SolveForPhiStupakov (b2e_roots.h) and the real transform behind
+ * applyLHPassFilters (b2e_fft.h).  Test infrastructure only.
  */
 #include "mdb.h"
 #include "track.h"
 #include "b2e_sg.h"
 #include "b2e_roots.h"
+#include "b2e_fft.h"
 
 #define ANALYSIS_BINS 10000 /* final_props.c:21 */
 
@@ -123,4 +125,33 @@ double zeroNewton(double (*fn)(double), double value, double x_i, double dx, lon
 
 double zeroInterp(double (*fn)(double), double value, double x_i, double x_f, double dx, double _zero) {
   return b2e_zero_interp(fn, value, x_i, x_f, dx, _zero);
+}
+
+/* realFFT2 as applyLHPassFilters (csbend.c:4631, :4687) calls it: forward
+ * (flags 0) from n real values to n/2 + 1 (re, im) pairs, or back
+ * (INVERSE_FFT), on the shared transform of b2e_fft.h; input and output may
+ * be the same array */
+long realFFT2(double *output, double *input, long n, unsigned long flags) {
+  double *c, *s, *in;
+  long i;
+  if (n < 1)
+    return 0;
+  c = malloc(sizeof(double) * n);
+  s = malloc(sizeof(double) * n);
+  in = malloc(sizeof(double) * (n + 2));
+  for (i = 0; i < n; i++)
+    b2e_dft_twiddle(n, i, &c[i], &s[i]);
+  if (flags & INVERSE_FFT) {
+    memcpy(in, input, sizeof(double) * (n + 2));
+    for (i = 0; i < n; i++)
+      output[i] = b2e_rdft_sample(in, n, i, c, s);
+  } else {
+    memcpy(in, input, sizeof(double) * n);
+    for (i = 0; i < n / 2 + 1; i++)
+      b2e_rdft_pair(in, n, i, c, s, &output[2 * i], &output[2 * i + 1]);
+  }
+  free(c);
+  free(s);
+  free(in);
+  return 1;
 }

@@ -62,7 +62,6 @@ OFFPATH(pointIsInsideContour)
 OFFPATH(pop_log)
 OFFPATH(push_log)
 OFFPATH(quadFringe)
-OFFPATH(realFFT2)
 OFFPATH(rpn)
 OFFPATH(rpn_clear)
 OFFPATH(simplexMin)

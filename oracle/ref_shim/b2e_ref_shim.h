@@ -151,6 +151,7 @@ char *cp_str(char **s, char *t);
 double interp(double *f, double *x, long n, double xo, long warnings, long order, long *returnCode);
 double zeroNewton(double (*fn)(double), double value, double x_i, double dx, long n_passes, double _zero);
 double zeroInterp(double (*fn)(double), double value, double x_i, double x_f, double dx, double _zero);
+long realFFT2(double *output, double *input, long n, unsigned long flags);
 int double_cmpasc(const void *a, const void *b);
 long binaryArraySearch(void *array, size_t elemSize, long nElems, void *key, int (*compare)(const void *, const void *), long bracket);
 long SavitzyGolaySmooth(double *data, long rows, long order, long nLeft, long nRight, long derivativeOrder);

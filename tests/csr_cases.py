@@ -40,3 +40,22 @@ def stupakov_cases():
         "ring_2p": leading_drift(w.chicane(bins=200, n_kicks=4, stupakov=True, drift={"N_KICKS": 2})),
         "ring_mode0_2p": leading_drift(w.chicane(bins=200, n_kicks=4, drift={"N_KICKS": 2})),
     }
+
+
+def _filtered(lat: Lattice, **kw) -> Lattice:
+    return Lattice([Element(e.name, e.type, dict(e.params, **kw)) if e.type == "CSRCSBEND" else e
+                    for e in lat.elements])
+
+
+def filter_cases():
+    """CSRCSBEND histogram filters (LOW/HIGH_FREQUENCY_CUTOFF0/1,
+    CLIP_NEGATIVE_BINS): name -> lattice."""
+    return {
+        "low_pass": _filtered(w.chicane(bins=200, n_kicks=4), HIGH_FREQUENCY_CUTOFF0=0.2, HIGH_FREQUENCY_CUTOFF1=0.4),
+        "high_pass": _filtered(w.chicane(bins=200, n_kicks=4), LOW_FREQUENCY_CUTOFF0=0.01, LOW_FREQUENCY_CUTOFF1=0.03),
+        "both_odd_bins": _filtered(w.chicane(bins=151, n_kicks=4), LOW_FREQUENCY_CUTOFF0=0.02,
+                                   HIGH_FREQUENCY_CUTOFF0=0.3, HIGH_FREQUENCY_CUTOFF1=0.5),
+        "round_trip_only": _filtered(w.chicane(bins=120, n_kicks=3), LOW_FREQUENCY_CUTOFF0=0.0),
+        "no_clip_stupakov": _filtered(w.chicane(bins=200, n_kicks=4, stupakov=True), HIGH_FREQUENCY_CUTOFF0=0.1,
+                                      CLIP_NEGATIVE_BINS=0),
+    }

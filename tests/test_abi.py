@@ -41,3 +41,25 @@ def test_version_and_null_handling():
     lib.b2e_last_error.restype = ctypes.c_char_p
     assert lib.b2e_last_error(None) == b"null context"
     assert lib.b2e_destroy(None) == -1
+
+
+def test_element_defaults_match_the_host_tables():
+    """b2e_element_defaults (no device needed) gives every supported type the
+    same defaults the Python layer writes, the reference's parameter-table
+    values; the CSR filter cutoffs default to -1 (off)."""
+    from elegant_b200 import _native as nat
+    from elegant_b200.lattice import DEFAULTS, SLOTS, TYPE_NAMES
+    lib = ctypes.CDLL(LIB)
+    for code in TYPE_NAMES:
+        el = nat.Element()
+        assert lib.b2e_element_defaults(code, ctypes.byref(el)) == 0
+        assert el.type == code
+        want = [0.0] * nat.MAX_PARAMS
+        for k, v in DEFAULTS.get(code, {}).items():
+            want[SLOTS[code][k]] = float(v)
+        assert list(el.p) == want, TYPE_NAMES[code]
+    el = nat.Element()
+    lib.b2e_element_defaults(nat.CSRCSBEND, ctypes.byref(el))
+    assert [el.p[i] for i in (31, 32, 33, 34)] == [-1.0] * 4
+    assert lib.b2e_element_defaults(99, ctypes.byref(el)) == -1
+    assert lib.b2e_element_defaults(nat.DRIF, None) == -1

@@ -344,3 +344,20 @@ def test_stupakov_bunch_train_matches_single_bunches():
         assert np.array_equal(res.ids[sl][order], ref_ids)
         alive = ref_loss < 0
         assert np.array_equal(res.coords[sl][order][alive], ref_c[alive]), b
+
+
+@pytest.mark.parametrize("case", ["low_pass", "high_pass", "both_odd_bins", "round_trip_only", "no_clip_stupakov"])
+def test_csr_histogram_filters_bit_exact(case):
+    """LOW/HIGH_FREQUENCY_CUTOFF filters of the histogram (one CTA per
+    bunch: twiddles, forward pairs, ramps, inverse, clipping) equal elegant's
+    applyLHPassFilters on the shared transform, bit for bit."""
+    from csr_cases import filter_cases
+    from reforacle import RefOracle
+    lat = filter_cases()[case]
+    beam = w.chicane_beam(20000, seed=32)
+    with Tracker(lat, P0, 1) as t:
+        res = t.track(beam)
+        wakes = t.csr_wakes(10_000_000)
+    rows, nl, _, ref_wakes = RefOracle("b2e", private=True).track(lat, beam.coords, beam.ids, P0, 1,
+                                                                  capture_wakes=True)
+    check(res, wakes, rows, nl, ref_wakes)

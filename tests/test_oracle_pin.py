@@ -201,3 +201,71 @@ def test_stupakov_phi_solver():
     assert f(0.01, 1.0, 0.05, ctypes.byref(last)) == -1
     assert f(0.01, 0.0, 0.05, ctypes.byref(last)) == 0
     assert f(0.01, -1e-9, 0.05, ctypes.byref(last)) == -1
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("case", ["low_pass", "high_pass", "both_odd_bins", "round_trip_only", "no_clip_stupakov"])
+def test_port_reproduces_reference_csr_filters(math, case):
+    """The histogram filters (applyLHPassFilters through the shared real
+    transform): restatement and elegant's own code agree bit for bit."""
+    from csr_cases import filter_cases
+    lat = filter_cases()[case]
+    beam = w.chicane_beam(5000, seed=23)
+    p0 = 1000 / 0.51099895
+    r1, n1, _, w1 = RefOracle(math, private=True).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    r2, n2, _, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    assert n1 == n2 and w1.size == w2.size > 0
+    assert np.array_equal(w1, w2)
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+
+
+def _numpy_lh(h, start_hp, end_hp, start_lp, end_lp, clip):
+    """applyLHPassFilters with numpy's FFT (an independent transform)."""
+    n = h.size
+    freq = n // 2 + 1
+    X = np.fft.rfft(h)
+    scale = np.ones(freq)
+    end_lp, end_hp = max(end_lp, start_lp), max(end_hp, start_hp)
+    if start_lp > 0:
+        i1 = min(max(int(start_lp * freq), 0), freq - 1)
+        i2 = min(max(int(end_lp * freq), 0), freq - 1)
+        d = 0 if i1 == i2 else 1.0 / (i2 - i1)
+        f = 1.0
+        for i in range(i1, i2 + 1):
+            scale[i] *= f
+            f = max(f - d, 0)
+        scale[i2 + 1:] = 0
+    if start_hp > 0:
+        i1 = min(max(int(start_hp * freq), 0), freq - 1)
+        i2 = min(max(int(end_hp * freq), 0), freq - 1)
+        d = 0 if i1 == i2 else 1.0 / (i2 - i1)
+        scale[:i1] = 0
+        f = 0.0
+        for i in range(i1, i2 + 1):
+            scale[i] *= f
+            f = min(f + d, 1)
+    y = np.fft.irfft(X * scale, n)
+    if clip:
+        y = np.where(y < 0, 0, y)
+        y *= h.sum() / y.sum()
+    return y
+
+
+@pytest.mark.parametrize("n", [8, 9, 120, 151, 600, 1024])
+@pytest.mark.parametrize("cut", [(-1, -1, 0.2, 0.4), (0.05, 0.1, -1, -1), (0.02, 0.02, 0.3, 0.6), (0.0, -1, -1, -1)])
+def test_histogram_filter_transform_against_numpy(n, cut):
+    """The project's real transform (b2e_fft.h, any n) and the filter ramps
+    agree with numpy's FFT to rounding, with and without clipping."""
+    import ctypes
+    lib = PortOracle("b2e").lib
+    f = lib.b2e_oracle_lh_pass_filters
+    f.restype = ctypes.c_long
+    f.argtypes = [ctypes.c_void_p, ctypes.c_long] + [ctypes.c_double] * 4 + [ctypes.c_int]
+    rng = np.random.default_rng(n)
+    x = np.arange(n)
+    h = np.round(50 * np.exp(-0.5 * ((x - n / 2) / (n / 8)) ** 2) + rng.poisson(5, n)).astype(float)
+    for clip in (0, 1):
+        ours = h.copy()
+        f(ours.ctypes.data, n, *cut, clip)
+        ref = _numpy_lh(h, *cut, clip)
+        assert np.allclose(ours, ref, rtol=1e-11, atol=1e-11 * h.max()), (clip, np.abs(ours - ref).max())

@@ -22,8 +22,9 @@ P0 = 1000 / 0.51099895
 CHARGE = 1e-9
 
 
-def bend_element():
-    return Element("B1", "CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "N_KICKS": 6, "BINS": 240, "SG_HALFWIDTH": 2})
+def bend_element(**extra):
+    return Element("B1", "CSRCSBEND", dict({"L": 0.5, "ANGLE": 0.05, "N_KICKS": 6, "BINS": 240, "SG_HALFWIDTH": 2},
+                                           **extra))
 
 
 def static_call(lib, beam, bend_arr, wakes_needed):
@@ -45,10 +46,11 @@ def static_call(lib, beam, bend_arr, wakes_needed):
     return coords, lost_pass.cpu().numpy(), wakes.cpu().numpy()
 
 
-def test_static_bend_matches_context_path_twice():
+@pytest.mark.parametrize("extra", [{}, {"HIGH_FREQUENCY_CUTOFF0": 0.2, "LOW_FREQUENCY_CUTOFF0": 0.02}])
+def test_static_bend_matches_context_path_twice(extra):
     lib = nat.load_library()
     lib.b2e_csr_bend_static.restype = ctypes.c_int
-    bend = bend_element()
+    bend = bend_element(**extra)
     lat = Lattice([Element("Q", "CHARGE", {"TOTAL": CHARGE}), bend])
     beam = w.chicane_beam(30000, seed=12)
     with Tracker(lat, P0, 1) as t:
