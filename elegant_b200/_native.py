@@ -44,7 +44,8 @@ class RunOptions(ctypes.Structure):
     _fields_ = [("p_central", ctypes.c_double), ("n_passes", ctypes.c_int32), ("default_order", ctypes.c_int32),
                 ("coord_limit", ctypes.c_double), ("slope_limit", ctypes.c_double),
                 ("passes_per_launch", ctypes.c_int32), ("ring_variant", ctypes.c_int32),
-                ("record_history", ctypes.c_int32), ("compact_every", ctypes.c_int32)]
+                ("record_history", ctypes.c_int32), ("compact_every", ctypes.c_int32),
+                ("sr_gaussian_limit", ctypes.c_double), ("isr_seed", ctypes.c_uint64)]
 
 
 class Override(ctypes.Structure):

@@ -85,6 +85,7 @@ struct b2e_ctx {
   /* external (device) particle pointers for b2e_track_device */
   DevParticles ext{};
   bool use_ext = false;
+  bool radiates = false; /* some element of some instance has SYNCH_RAD or ISR */
   CsrState csr;
   int pass_counter = 0; /* next pass to track in the current run */
   int64_t launches = 0; /* kernels launched by this context */
@@ -243,6 +244,13 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
   return B2E_OK;
 }
 
+static bool any_radiation(const std::vector<DevElem> &elems) {
+  for (const DevElem &d : elems)
+    if (d.flags & (EF_SR | EF_ISR))
+      return true;
+  return false;
+}
+
 extern "C" int b2e_element_defaults(int32_t type, b2e_element *element) {
   if (!element || type < B2E_DRIF || type > B2E_CSRDRIFT)
     return B2E_ERR_ARG;
@@ -276,6 +284,7 @@ extern "C" int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32
   ctx->inst_offsets = {0, ctx->n};
   ctx->elems_all = ctx->lat.elems;
   ctx->aps_all = ctx->lat.aps;
+  ctx->radiates = any_radiation(ctx->elems_all);
   build_tiles(ctx);
   ctx->lattice_loaded = true;
   int rc = csr_configure(ctx->csr, ctx->base.data(), n_elements, ctx->lat, ctx->opt, ctx->err);
@@ -320,6 +329,7 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     ctx->elems_all.insert(ctx->elems_all.end(), cl.elems.begin(), cl.elems.end());
     ctx->aps_all.insert(ctx->aps_all.end(), cl.aps.begin(), cl.aps.end());
   }
+  ctx->radiates = any_radiation(ctx->elems_all);
   build_tiles(ctx);
   int rc = upload_lattice_tables(ctx);
   if (rc)
@@ -502,6 +512,10 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.hist = ctx->opt.record_history && !ctx->use_ext ? ctx->d_hist_partials.ptr : nullptr;
   L.hist_pass0 = ctx->hist_pass0;
   L.hist_passes = ctx->hist_passes;
+  L.rad = ctx->radiates;
+  L.ids = ctx->use_ext ? nullptr : ctx->d_ids.ptr;
+  L.isr_seed = ctx->opt.isr_seed;
+  L.sr_limit = ctx->opt.sr_gaussian_limit == 0 ? 3.0 : ctx->opt.sr_gaussian_limit;
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
@@ -511,7 +525,7 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   int variant = ctx->opt.ring_variant;
   if (variant < 1 || variant > B2E_RING_VARIANTS) {
     /* autotune once per context on a multi-pass range of a large enough beam */
-    if (!ctx->tuned_variant && pe > pb && ctx->n >= 16384) {
+    if (!ctx->tuned_variant && pe > pb && ctx->n >= 16384 && !L.rad) {
       int rc = autotune_ring(ctx, L, staged, smem, pb, eb);
       if (rc)
         return rc;
@@ -532,6 +546,7 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
       if (rc)
         return rc;
       L.P = particle_view(ctx);
+      L.ids = ctx->d_ids.ptr; /* the IDs moved with the rows */
       L.tiles = ctx->d_tiles.ptr;
       L.n_tiles = (int)ctx->tiles.size();
     }

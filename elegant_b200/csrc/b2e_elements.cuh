@@ -10,6 +10,7 @@
  */
 #ifndef B2E_ELEMENTS_CUH
 #define B2E_ELEMENTS_CUH
+#include "b2e_rng.h"
 #include "b2e_engine.h"
 #include "b2e_math.h"
 
@@ -136,7 +137,46 @@ __device__ __forceinline__ void rotate_misalign(Part &p, double ca, double sa) {
  * zeroed, when ISR is off, multipole.c:781-784), which divides and
  * re-multiplies the canonical momenta by (1+delta) after each kick; that
  * round trip is reproduced because it can move the last bit. */
-__device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g) {
+/* where an ISR deviate comes from (b2e_rng.h): the particle and the place */
+struct RadSite {
+  int64_t id;
+  int32_t pass, elem;
+  uint64_t seed;
+  double limit;
+};
+
+/* radiation after a kick (multipole.c:1320-1349): the momenta scaled by
+ * 1/(1+delta), F2 from this substep's kick, the classical loss with
+ * SYNCH_RAD and a Gaussian ISR kick with ISR; xkick = ykick = 0 */
+__device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &dp, double dqx, double dqy,
+                                                double xp, double yp, const double *c, int step, int nSub,
+                                                unsigned flags, const RadSite &rs, int slice) {
+  const double drift = c[KM_DRIFT], kfrac = c[KM_KFRAC0 + step];
+  double deltaFactor, F2, dsFactor, dsISRFactor;
+  qx = qx / (1 + dp);
+  qy = qy / (1 + dp);
+  deltaFactor = (1 + dp) * (1 + dp);
+  dqx = dqx / kfrac;
+  dqy = dqy / kfrac;
+  {
+    const double a = dqx / drift - 0.0 / drift, b = dqy / drift + 0.0 / drift;
+    F2 = a * a + b * b;
+  }
+  dsFactor = sqrt((1 + xp * xp) + yp * yp);
+  dsISRFactor = (dsFactor * drift) / (nSub - 1);
+  dsFactor = dsFactor * (drift * kfrac);
+  if (flags & EF_SR)
+    dp = dp - ((c[KM_RAD] * deltaFactor) * F2) * dsFactor;
+  if (flags & EF_ISR)
+    dp = dp - (((c[KM_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISRFactor)) *
+                  b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, slice, step, rs.limit);
+  qx = qx * (1 + dp);
+  qy = qy * (1 + dp);
+}
+
+template <bool RAD>
+__device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g,
+                                     const RadSite &rs) {
   const double *c = e.c;
   const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = (int)c[KM_NSUB];
   const double dx = c[KM_DX], dy = c[KM_DY];
@@ -175,7 +215,7 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
     for (step = 0; step < nSub; step++) {
       const double dsh = c[KM_DSH0 + step];
       const double kick = c[KM_KICK0 + step];
-      double sumFx, sumFy;
+      double sumFx, sumFy, dqx = 0, dqy = 0;
       x = x + xp * dsh;
       y = y + yp * dsh;
       s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
@@ -195,12 +235,22 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
       }
       qx = qx - kick * sumFy;
       qy = qy + kick * sumFx;
+      if (RAD) {
+        /* delta_qx, delta_qy of apply_canonical_multipole_kicks (multipole.h:237-240) */
+        dqx = dqx - kick * sumFy;
+        dqy = dqy + kick * sumFx;
+      }
       if (e.flags & (EF_QUAD_ORDER2 | EF_SKEW_ORDER2)) {
         /* KSEXT K1/J1 terms: quadrupole order, normal then skew (multipole.c:1272-1275) */
         if (e.flags & EF_QUAD_ORDER2) {
           const double k1 = c[KM_KICK1_0 + step];
-          qx = qx - k1 * ((1.0 * x) * 1.0);
-          qy = qy + k1 * ((1.0 * 1.0) * y);
+          const double fy = (1.0 * x) * 1.0, fx = (1.0 * 1.0) * y;
+          qx = qx - k1 * fy;
+          qy = qy + k1 * fx;
+          if (RAD) {
+            dqx = dqx - k1 * fy;
+            dqy = dqy + k1 * fx;
+          }
         }
         if (e.flags & EF_SKEW_ORDER2) {
           const double j1 = c[KM_SKEW0 + step];
@@ -208,15 +258,23 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
           double fx = -((1.0 * x) * 1.0), fy = (1.0 * 1.0) * y;
           qx = qx - j1 * fy;
           qy = qy + j1 * fx;
+          if (RAD) {
+            dqx = dqx - j1 * fy;
+            dqy = dqy + j1 * fx;
+          }
         }
       }
       if (!momenta_to_slopes(xp, yp, qx, qy, dp))
         return LOSS_SLOPE;
       if (e.flags & EF_RADBLOCK) {
-        qx = qx / (1 + dp);
-        qy = qy / (1 + dp);
-        qx = qx * (1 + dp);
-        qy = qy * (1 + dp);
+        if (RAD && (e.flags & (EF_SR | EF_ISR))) {
+          kmult_radiation(qx, qy, dp, dqx, dqy, xp, yp, c, step, nSub, e.flags, rs, i_kick);
+        } else {
+          qx = qx / (1 + dp);
+          qy = qy / (1 + dp);
+          qx = qx * (1 + dp);
+          qy = qy * (1 + dp);
+        }
         if (!momenta_to_slopes(xp, yp, qx, qy, dp))
           return LOSS_SLOPE;
       }
@@ -233,7 +291,13 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
   p.xp = xp;
   p.y = y;
   p.yp = yp;
-  p.s = p.s + s;
+  if (RAD && (e.flags & EF_SR)) {
+    /* path length at the changed velocity (multipole.c:1391-1394) */
+    const double p0 = g.p_central * (1 + p.dp), beta0 = p0 / sqrt(p0 * p0 + 1);
+    const double p1 = g.p_central * (1 + dp), beta1 = p1 / sqrt(p1 * p1 + 1);
+    p.s = beta1 * (p.s / beta0 + (2 * s) / (beta0 + beta1));
+  } else
+    p.s = p.s + s;
   p.dp = dp;
   if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp))
     return LOSS_NAN;
@@ -253,9 +317,11 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
  * pure-dipole field (Fx = 0, Fy = 1, csbend.c:106-110).  Q = (X, QX, Y, QY,
  * dist, DPoP).  `isr_block` reproduces the (QX/(1+d))*(1+d) round trip of
  * the radiation block that the negated isrConstant always enables. */
+template <bool RAD>
 __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y, double &QY, double &dist,
-                                                const double DPoP, const double *c, int nSlices, int nSub,
-                                                bool isr_block, const DevAperture *ap, const DevElem &e) {
+                                                double &DPoP, const double *c, int nSlices, int nSub,
+                                                bool isr_block, const DevAperture *ap, const DevElem &e,
+                                                const RadSite &rs) {
   const double rho0 = c[CB_RHO0], rho_actual = c[CB_RHO_ACTUAL];
   int i, j;
   dist = 0;
@@ -299,7 +365,25 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
           const double z = ((ds) * (1 + X / rho0)) * 0.0;
           QY = QY + (rho_actual < 0 ? -z : z);
         }
-        if (isr_block) {
+        if (RAD && (e.flags & (EF_SR | EF_ISR))) {
+          /* radiation after the kick (csbend.c:1603-1622), Fx = 0, Fy = 1 */
+          const double a = 1 + X * c[CB_INV_RHO0];
+          const double f = a / sqrt(((1 + DPoP) * (1 + DPoP) - QX * QX) - QY * QY);
+          const double xp = QX * f, yp = QY * f;
+          const double dsFactor = sqrt((a * a + xp * xp) + yp * yp);
+          const double F2 = 0.0 * 0.0 + 1.0 * 1.0;
+          const double deltaFactor = (1 + DPoP) * (1 + DPoP);
+          const double dsISR = c[CB_SLICE] / (nSub - 1);
+          QX = QX / (1 + DPoP);
+          QY = QY / (1 + DPoP);
+          if (e.flags & EF_SR)
+            DPoP = DPoP - (((c[CB_RAD] * deltaFactor) * F2) * ds) * dsFactor;
+          if (e.flags & EF_ISR)
+            DPoP = DPoP - (((c[CB_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISR * dsFactor)) *
+                              b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, i, j, rs.limit);
+          QX = QX * (1 + DPoP);
+          QY = QY * (1 + DPoP);
+        } else if (isr_block) {
           QX = QX / (1 + DPoP);
           QY = QY / (1 + DPoP);
           QX = QX * (1 + DPoP);
@@ -315,7 +399,19 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
 
 /* ---- CSBEND: track_through_csbend (csbend.c:665-1409), malignMethod 0,
  * edge method 1 at edge order 1, no synchrotron radiation. */
-__device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g) {
+/* dp_prime * x * tan(e) of the radiation edge corrections (csbend.c:1211-1216,
+ * :1265-1276), Fx = 0, Fy = 1 */
+__device__ __forceinline__ double bend_edge_radiation(double x, double xp, double yp, double dp, double tan_e,
+                                                      const double *c) {
+  const double a = 1 + x / c[CB_RHO0];
+  const double dp_prime = ((-c[CB_RAD]) * (0.0 * 0.0 + 1.0 * 1.0)) * ((1 + dp) * (1 + dp)) *
+                          sqrt((a * a + xp * xp) + yp * yp);
+  return (dp_prime * x) * tan_e;
+}
+
+template <bool RAD>
+__device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g,
+                                      const RadSite &rs) {
   const double *c = e.c;
   const double ct = c[CB_COS_TT], st = c[CB_SIN_TT];
   const int nSlices = (int)c[CB_NSLICES], nSub = (int)c[CB_NSUB];
@@ -341,6 +437,10 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
     yp = yp - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * y;
   }
 
+  /* anticipate the radiation error of integrating the sector (csbend.c:1211-1216) */
+  if (RAD && (e.flags & EF_EDGE1) && (e.flags & EF_SR) && c[CB_E1] != 0)
+    dp = dp - bend_edge_radiation(x, xp, yp, dp, c[CB_TAN_E1], c);
+
   /* convertToDipoleCanonicalCoordinates (csbend.c:1411-1419) */
   f = (1 + dp) / sqrt((1 + xp * xp) + yp * yp);
   Q0 = x;
@@ -348,7 +448,7 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   Q2 = y;
   Q3 = yp * f;
 
-  lost = csbend_integrate(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e);
+  lost = csbend_integrate<RAD>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e, rs);
 
   /* convertFromDipoleCanonicalCoordinates (csbend.c:1421-1429) */
   f = 1 / sqrt(((1 + dp) * (1 + dp) - Q1 * Q1) - Q3 * Q3);
@@ -359,11 +459,16 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
     p.xp = Q1;
     p.y = Q2;
     p.yp = Q3;
+    if (RAD)
+      p.dp = dp;
     return lost;
   }
+  /* correct the radiation error of the sector at the exit (csbend.c:1265-1276) */
+  if (RAD && (e.flags & EF_EDGE2) && (e.flags & EF_SR) && c[CB_E2] != 0)
+    dp = dp - bend_edge_radiation(Q0, Q1, Q3, dp, c[CB_TAN_E2], c);
 
   if (e.flags & EF_RADBLOCK) {
-    /* time-of-flight velocity fix (csbend.c:1259-1271), dp unchanged here */
+    /* time-of-flight velocity fix (csbend.c:1278-1288) */
     double p0 = g.p_central * (1 + dp0), beta0 = p0 / sqrt(p0 * p0 + 1);
     double p1 = g.p_central * (1 + dp), beta1 = p1 / sqrt(p1 * p1 + 1);
     s = (beta1 * s) / beta0 + Q4;

@@ -20,7 +20,7 @@
 #include <stdint.h>
 #include "../../include/elegant_b200.h"
 
-#define B2E_NC 40 /* constants per compiled element */
+#define B2E_NC 52 /* constants per compiled element */
 
 /* Compiled element kinds (device dispatch) */
 enum {
@@ -48,6 +48,8 @@ enum {
 #define EF_SKEW_ORDER2 0x100    /* KSEXT J1 term present */
 #define EF_QUAD_ORDER2 0x200    /* KSEXT K1 term present */
 #define EF_REVERSE_TILT 0x400   /* nonzero reverse tilt in the internal aperture check */
+#define EF_SR 0x800             /* KMULT / CSBEND: classical synchrotron radiation (SYNCH_RAD) */
+#define EF_ISR 0x1000           /* KMULT / CSBEND: quantum excitation (ISR) */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -64,6 +66,10 @@ enum {
 #define KM_REV_COS 32   /* reverse tilt cos/sin for the aperture check */
 #define KM_REV_SIN 33
 #define KM_SKEW0 34     /* J1 kick per substep 34..39 (first 6 substeps) */
+#define KM_KFRAC0 40    /* kickFrac[j], j = 0..7 -> 40..47 (radiation) */
+#define KM_RAD 48       /* rad_coef (multipole.c:789) */
+#define KM_ISR 49       /* isr_coef, > 0 only when ISR is applied (:790-795) */
+#define KM_DRIFT 50     /* slice drift length (:1189) */
 
 /* CSBEND constant slots */
 #define CB_RHO0 0
@@ -87,7 +93,10 @@ enum {
 #define CB_DYF 32
 #define CB_DZF 33
 #define CB_ET0 34       /* dcoord_etilt[0..4] -> 34..38 */
-#define CB_REV_COS 39   /* reverse tilt cos/sin share slots with etilt? no: stored in aux */
+#define CB_RAD 40       /* rad_coef (csbend.c:967-970) */
+#define CB_ISR 41       /* isrConstant, > 0 only when ISR is applied (:972-975) */
+#define CB_SLICE 42     /* s = length / N_SLICES, for dsISR (:1614) */
+#define CB_INV_RHO0 43  /* 1. / rho0 (:1605) */
 
 /* RFCA constant slots */
 #define RF_VOLT 0       /* volt/(1e6*mc^2[MV]*sign)/nKicks */

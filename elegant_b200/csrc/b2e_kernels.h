@@ -24,6 +24,13 @@ struct RingLaunch {
   double *hist;    /* per (tile, pass) moments [n_tiles][hist_passes][11], or null */
   int hist_pass0;  /* absolute pass of hist's first slot */
   int hist_passes;
+  /* radiation (SYNCH_RAD / ISR elements present): the kernel with the
+   * radiation code; ISR deviates are addressed by particle ID (ids, or the
+   * row number + 1 without IDs), pass, element, slice and step */
+  int rad;
+  const int64_t *ids;
+  uint64_t isr_seed;
+  double sr_limit;
 };
 
 /* variant 1..B2E_RING_VARIANTS selects the occupancy target and the barrier

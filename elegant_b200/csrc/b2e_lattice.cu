@@ -5,6 +5,7 @@
 #include <string.h>
 #include <string>
 #include "b2e_lattice.h"
+#include "b2e_rng.h"
 #include "b2e_math.h"
 
 namespace b2e {
@@ -12,6 +13,25 @@ namespace b2e {
 static const double kPI = 3.141592653589793238462643383279502884;
 static const double kME_MEV = 0.51099895000; /* electron rest energy, MeV (CODATA 2018) */
 static const double kBETA = 1.25992104989487316477; /* 2^(1/3), multipole.c:1119, csbend.c:1431 */
+/* CODATA 2018, the values the oracle's reference build uses */
+static const double kC_MKS = 2.99792458e8, kE_MKS = 1.602176634e-19, kME_MKS = 9.1093837015e-31;
+static const double kRE_MKS = 2.8179403262e-15;
+
+/* the radiation coefficients' common factors, in the reference's expression
+ * order (multipole.c:789-790, csbend.c:967-972): epsilon_o = 1/(mu_o c^2),
+ * pow3/pow5 as repeated products */
+static double eps0_mks() { return 1 / ((4 * kPI * 1e-7) * kC_MKS * kC_MKS); }
+static double pow3_host(double x) { return (x * x) * x; }
+static double pow5_host(double x) { return ((x * x) * (x * x)) * x; }
+
+/* ISR options that the engine does not follow */
+static std::string check_radiation(const double *p, int slot_isr, int slot_isr1, long nSlices) {
+  if (p[slot_isr] != 0 && p[slot_isr1] == 0)
+    return "ISR=1 with ISR1PART=0 is not supported by this engine";
+  if (p[slot_isr] != 0 && nSlices > B2E_ISR_MAX_SLICES)
+    return "ISR with more than 256 slices per element is not supported by this engine";
+  return "";
+}
 
 /* Symplectic integrator step fractions: multipole.c:1140-1182, csbend.c:1453-1488. */
 static int integrator_fractions(int order, double *drift, double *kick) {
@@ -82,6 +102,7 @@ void element_defaults(int type, double *p) {
   case B2E_KSEXT:
     p[B2E_KMULT_N_SLICES] = 1;          /* track_data.c:1234, :1130 */
     p[B2E_KMULT_INTEGRATION_ORDER] = 4; /* :1253, :1153 */
+    p[B2E_KMULT_ISR1PART] = 1;          /* :1257, :1157 */
     break;
   case B2E_CSBEND:
   case B2E_CSRCSBEND:
@@ -91,6 +112,7 @@ void element_defaults(int type, double *p) {
     p[B2E_BEND_EDGE1_EFFECTS] = 1;
     p[B2E_BEND_EDGE2_EFFECTS] = 1;
     p[B2E_BEND_EDGE_ORDER] = 1;
+    p[B2E_BEND_ISR1PART] = 1;           /* track_data.c:1966, :2039 */
     if (type == B2E_CSRCSBEND) {
       p[B2E_BEND_BIN_RANGE_FACTOR] = 1.2; /* csrcsbend_param, track_data.c:1982-2060 */
       p[B2E_BEND_SG_ORDER] = 1;
@@ -146,7 +168,7 @@ static void bend_edge_flags(const b2e_element *el, int n, int i, bool *edge1, bo
   *edge2 = el[i].p[B2E_BEND_EDGE2_EFFECTS] != 0 && !same_post;
 }
 
-static std::string compile_kmult(const b2e_element &el, DevElem &d) {
+static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d) {
   const double *p = el.p;
   double drift_frac[8], kick_frac[8];
   const double L = p[B2E_KMULT_L];
@@ -205,14 +227,39 @@ static std::string compile_kmult(const b2e_element &el, DevElem &d) {
     d.rev_cos = b2e_cos(-p[B2E_KMULT_TILT]);
     d.rev_sin = b2e_sin(-p[B2E_KMULT_TILT]);
   }
-  /* isr_coef is nonzero (negated when ISR is off), so the radiation block
-   * runs whenever the slice drift is nonzero (multipole.c:1320) */
-  if (drift != 0)
-    d.flags |= EF_RADBLOCK;
+  /* radiation (multipole.c:788-800): rad_coef with SYNCH_RAD; isr_coef is
+   * always nonzero and negated when ISR is off, so the radiation block runs
+   * whenever the slice drift is nonzero (:1320); both are zeroed for a
+   * radiating element shorter than 1e-6 m */
+  {
+    std::string re = check_radiation(p, B2E_KMULT_ISR, B2E_KMULT_ISR1PART, nSlices);
+    if (!re.empty())
+      return re;
+    double rad_coef = 0, isr_coef;
+    const bool sr = p[B2E_KMULT_SYNCH_RAD] != 0, isr = p[B2E_KMULT_ISR] != 0;
+    if (sr)
+      rad_coef = (kE_MKS * kE_MKS) * pow3_host(Po) / (6 * kPI * eps0_mks() * (kC_MKS * kC_MKS) * kME_MKS);
+    isr_coef = kRE_MKS * sqrt(55.0 / (24 * sqrt(3)) * pow5_host(Po) * 137.0359895);
+    if (!isr)
+      isr_coef *= -1;
+    if (L < 1e-6 && (isr || sr))
+      rad_coef = isr_coef = 0;
+    d.c[KM_RAD] = rad_coef;
+    d.c[KM_ISR] = isr_coef;
+    d.c[KM_DRIFT] = drift;
+    for (int j = 0; j < 8; j++)
+      d.c[KM_KFRAC0 + j] = j < nSub ? kick_frac[j] : 0;
+    if ((rad_coef != 0 || isr_coef != 0) && drift != 0)
+      d.flags |= EF_RADBLOCK;
+    if (rad_coef != 0 && drift != 0)
+      d.flags |= EF_SR;
+    if (isr_coef > 0 && drift != 0)
+      d.flags |= EF_ISR;
+  }
   return "";
 }
 
-static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, DevElem &d) {
+static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, double Po, DevElem &d) {
   const double *p = el.p;
   double drift_frac[8], kick_frac[8];
   const double length = p[B2E_BEND_L];
@@ -324,9 +371,30 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     d.rev_sin = b2e_sin(-tilt);
   }
   /* isrConstant is nonzero for CSBEND (negated when ISR is off,
-   * csbend.c:962-965); CSRCSBEND sets it to 0 unless ISR is on (:2138-2142) */
-  if (el.type == B2E_CSBEND)
+   * csbend.c:972-975); CSRCSBEND sets it to 0 unless ISR is on (:2138-2142) */
+  if (el.type == B2E_CSBEND) {
+    std::string re = check_radiation(p, B2E_BEND_ISR, B2E_BEND_ISR1PART, nSlices);
+    if (!re.empty())
+      return re;
+    double rad_coef = 0, isr_const;
+    if (p[B2E_BEND_SYNCH_RAD] != 0)
+      rad_coef = (kE_MKS * kE_MKS) * pow3_host(Po) * ((1 + fse) * (1 + fse)) /
+                 (6 * kPI * eps0_mks() * (kC_MKS * kC_MKS) * kME_MKS * (rho0 * rho0));
+    isr_const = kRE_MKS * sqrt(55.0 / (24 * sqrt(3)) * pow5_host(Po) * 137.0359895 / pow3_host(fabs(rho_actual)));
+    if (p[B2E_BEND_ISR] == 0)
+      isr_const *= -1;
+    d.c[CB_RAD] = rad_coef;
+    d.c[CB_ISR] = isr_const;
+    d.c[CB_SLICE] = s;
+    d.c[CB_INV_RHO0] = 1. / rho0;
     d.flags |= EF_RADBLOCK;
+    if (rad_coef != 0)
+      d.flags |= EF_SR;
+    if (isr_const > 0)
+      d.flags |= EF_ISR;
+  } else if (p[B2E_BEND_SYNCH_RAD] != 0 || p[B2E_BEND_ISR] != 0) {
+    return "CSRCSBEND with SYNCH_RAD or ISR is not supported by this engine";
+  }
   return "";
 }
 
@@ -358,7 +426,7 @@ const char *compile_single_csr_bend(const b2e_element &el, DevElem &d) {
     return "element is not a CSRCSBEND";
   memset(&d, 0, sizeof(d));
   d.ap_pass0 = d.ap_later = -1;
-  std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, d);
+  std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, 0.0, d);
   if (!e.empty()) {
     snprintf(msg, sizeof(msg), "%s", e.c_str());
     return msg;
@@ -398,14 +466,14 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
       break;
     case B2E_KQUAD:
     case B2E_KSEXT:
-      err = compile_kmult(el[i], d);
+      err = compile_kmult(el[i], opt.p_central, d);
       z += p[B2E_KMULT_L];
       break;
     case B2E_CSBEND:
     case B2E_CSRCSBEND: {
       bool e1, e2;
       bend_edge_flags(el, n, i, &e1, &e2);
-      err = compile_csbend(el[i], e1, e2, d);
+      err = compile_csbend(el[i], e1, e2, opt.p_central, d);
       if (el[i].type == B2E_CSRCSBEND && d.kind == K_CSRCSBEND)
         out.csr_elements.push_back(i);
       z += p[B2E_BEND_L];

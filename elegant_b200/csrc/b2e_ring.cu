@@ -82,7 +82,7 @@ __device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *
  * memory record.  The arithmetic is identical in every variant.  HIST records
  * the per-pass tile moments (it needs SYNC >= 1); when SYNC >= 1 every thread
  * stays in the pass loop until the whole tile is lost. */
-template <bool STAGED, int MINB, int SYNC, bool HIST, int TPB>
+template <bool STAGED, int MINB, int SYNC, bool HIST, int TPB, bool RAD = false>
 __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
   static_assert(!HIST || SYNC >= 1, "history needs the per-pass barrier");
   static_assert(TPB == 1 || ((TPB == 2 || TPB == 4 || TPB == 8) && SYNC >= 1), "tiles of a block run in step");
@@ -134,6 +134,12 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
 
   int lost = LOSS_NONE, lost_pass = -1, lost_elem = -1;
   bool active = tracked;
+  RadSite rs = {0, 0, 0, 0, 0};
+  if (RAD) {
+    rs.id = tracked ? (L.ids ? L.ids[ip] : ip + 1) : 0;
+    rs.seed = L.isr_seed;
+    rs.limit = L.sr_limit;
+  }
   for (int pass = L.pass_begin; pass <= L.pass_end; pass++) {
     if (SYNC == 0) {
       if (!active)
@@ -165,10 +171,18 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
         edrift(p, e.c[DR_L]);
         break;
       case K_KMULT:
-        lost = kmult(p, e, ap, L.g);
+        if (RAD) {
+          rs.pass = pass;
+          rs.elem = ie;
+        }
+        lost = kmult<RAD>(p, e, ap, L.g, rs);
         break;
       case K_CSBEND:
-        lost = csbend(p, e, ap, L.g);
+        if (RAD) {
+          rs.pass = pass;
+          rs.elem = ie;
+        }
+        lost = csbend<RAD>(p, e, ap, L.g, rs);
         break;
       case K_RFCA: {
         const DevRfState rs = rf[(int)e.c[RF_SLOT]];
@@ -337,7 +351,7 @@ __global__ void effort_kernel(const int32_t *lost_pass, int64_t n, int pass_begi
   }
 }
 
-template <int MINB, int SYNC, bool HIST, int TPB>
+template <int MINB, int SYNC, bool HIST, int TPB, bool RAD = false>
 static cudaError_t launch_ring_v(const RingLaunch &L, int n_tiles, bool staged, size_t smem_bytes,
                                  cudaStream_t stream) {
   const int grid = (n_tiles + TPB - 1) / TPB;
@@ -345,13 +359,13 @@ static cudaError_t launch_ring_v(const RingLaunch &L, int n_tiles, bool staged, 
     staged = false; /* two instances' records do not fit: read them from global memory */
   if (staged) {
     const size_t bytes = smem_bytes * TPB;
-    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB, SYNC, HIST, TPB>,
+    cudaError_t err = cudaFuncSetAttribute(ring_kernel<true, MINB, SYNC, HIST, TPB, RAD>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (err != cudaSuccess)
       return err;
-    ring_kernel<true, MINB, SYNC, HIST, TPB><<<grid, 128 * TPB, bytes, stream>>>(L);
+    ring_kernel<true, MINB, SYNC, HIST, TPB, RAD><<<grid, 128 * TPB, bytes, stream>>>(L);
   } else {
-    ring_kernel<false, MINB, SYNC, HIST, TPB><<<grid, 128 * TPB, 0, stream>>>(L);
+    ring_kernel<false, MINB, SYNC, HIST, TPB, RAD><<<grid, 128 * TPB, 0, stream>>>(L);
   }
   return cudaGetLastError();
 }
@@ -398,6 +412,9 @@ cudaError_t launch_ring(const RingLaunch &L, int n_tiles, bool staged, size_t sm
                         int variant) {
   if (n_tiles <= 0)
     return cudaSuccess;
+  if (L.rad) /* radiating lattices: one configuration (two tiles per block, a barrier per element) */
+    return L.hist ? launch_ring_v<2, 2, true, 2, true>(L, n_tiles, staged, smem_bytes, stream)
+                  : launch_ring_v<2, 2, false, 2, true>(L, n_tiles, staged, smem_bytes, stream);
   if (variant < 1 || variant > B2E_RING_VARIANTS)
     variant = 1;
   if (variant > 12)

@@ -39,7 +39,7 @@ class Tracker:
 
     def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
                  passes_per_launch: int = 0, ring_variant: int = 0, record_history: bool = False,
-                 compact_every: int = 0):
+                 compact_every: int = 0, isr_seed: int = 0, sr_gaussian_limit: float = 3.0):
         self.lib = nat.load_library()
         self.lattice = lattice
         self._ctx = ctypes.c_void_p()
@@ -49,7 +49,8 @@ class Tracker:
         self.options = nat.RunOptions(p_central=p_central, n_passes=n_passes, default_order=default_order,
                                       coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
                                       ring_variant=ring_variant, record_history=int(record_history),
-                                      compact_every=compact_every)
+                                      compact_every=compact_every, sr_gaussian_limit=sr_gaussian_limit,
+                                      isr_seed=isr_seed)
         self._elems = lattice.to_ctypes()
         self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
         self.n_instances = 1

@@ -62,6 +62,32 @@ def fodo_ring(n_cells: int = 8, rf: bool = True, volt: float = 1e6, harmonic: in
     return Lattice(els)
 
 
+def radiating_ring(isr: bool = False, volt: float = 4e6, edge_angle: float = 0.0) -> Lattice:
+    """The FODO ring with SYNCH_RAD (and ISR) on its quadrupoles, sextupoles
+    and dipoles, and an RF cavity whose voltage and phase replace the energy
+    radiated per turn: U0 = C_gamma E^4 / rho (C_gamma = 8.8463e-5 m/GeV^3),
+    phase = 180 - asin(U0 / V) degrees (above transition).  edge_angle sets
+    E1 = E2 on the dipoles (edge focusing and the edge radiation terms)."""
+    base = fodo_ring(rf=False)
+    bend = next(e for e in base.elements if e.type == "CSBEND")
+    rho = bend.params["L"] / bend.params["ANGLE"]
+    e_gev = ring_p_central() * 0.51099895e-3
+    u0_mev = 8.8463e-5 * e_gev ** 4 / rho * 1e3
+    phase = 180.0 - math.degrees(math.asin(u0_mev / (volt / 1e6)))
+    extra = {"SYNCH_RAD": 1}
+    if isr:
+        extra["ISR"] = 1
+    els = []
+    for e in fodo_ring(volt=volt, phase=phase).elements:
+        if e.type in ("KQUAD", "KSEXT", "CSBEND"):
+            params = dict(e.params, **extra)
+            if e.type == "CSBEND" and edge_angle:
+                params.update(E1=edge_angle, E2=edge_angle)
+            e = Element(e.name, e.type, params)
+        els.append(e)
+    return Lattice(els)
+
+
 def ring_beam(n: int = 10000, seed: int = 12345, lattice: Lattice | None = None, first_id: int = 1) -> Beam:
     tw = periodic_twiss(lattice or fodo_ring(rf=False))
     return gaussian_beam(n, seed, 1e-9, 1e-9, tw.beta_x, tw.alpha_x, tw.beta_y, tw.alpha_y, 3e-3, 1e-3,

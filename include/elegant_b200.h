@@ -87,6 +87,9 @@ extern "C" {
 #define B2E_KMULT_INTEGRATION_ORDER 9
 #define B2E_KMULT_K1_OF_KSEXT 10 /* KSEXT K1 (quadrupole error term) */
 #define B2E_KMULT_J1_OF_KSEXT 11 /* KSEXT J1 (skew quadrupole error term) */
+#define B2E_KMULT_SYNCH_RAD 12    /* classical synchrotron radiation (multipole.c:1320-1349) */
+#define B2E_KMULT_ISR 13          /* incoherent synchrotron radiation (quantum excitation) */
+#define B2E_KMULT_ISR1PART 14     /* ISR also for a one-particle beam (default 1; 0 is not supported) */
 /* CSBEND (csbend_param, track_data.c:1893) and CSRCSBEND (csrcsbend_param, :1982) */
 #define B2E_BEND_L 0
 #define B2E_BEND_ANGLE 1
@@ -127,6 +130,10 @@ extern "C" {
 #define B2E_BEND_LOW_FREQUENCY_CUTOFF1 32
 #define B2E_BEND_HIGH_FREQUENCY_CUTOFF0 33
 #define B2E_BEND_HIGH_FREQUENCY_CUTOFF1 34
+/* CSBEND radiation (csbend.c:964-977, :1603-1622; edges :1211-1276); not on CSRCSBEND */
+#define B2E_BEND_SYNCH_RAD 35
+#define B2E_BEND_ISR 36
+#define B2E_BEND_ISR1PART 37
 /* RFCA (rfca_param, track_data.c:576) */
 #define B2E_RFCA_L 0
 #define B2E_RFCA_VOLT 1
@@ -183,6 +190,11 @@ typedef struct {
                               surviving particles to the front of its range and launch only
                               them; the order of rows changes, IDs travel with them.  Not with
                               record_history or device-owned columns. */
+  double sr_gaussian_limit; /* global_settings SR_gaussian_limit: ISR deviates beyond this many
+                               sigma are redrawn; 0 = elegant's default 3, < 0 = no cut */
+  uint64_t isr_seed;        /* seed of the ISR deviates, which are addressed by (particle ID,
+                               pass, element, slice, step): a run is reproducible and does not
+                               depend on launch shape or compaction */
 } b2e_run_options;
 
 typedef struct b2e_ctx b2e_ctx;

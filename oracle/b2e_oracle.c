@@ -348,6 +348,22 @@ static void rotate_beam(double **c, long np, double angle) {
   }
 }
 
+/* ---- synchrotron radiation ------------------------------------------------ */
+#include "../elegant_b200/csrc/b2e_rng.h"
+/* ISR deviates: the counter-based generator the engine uses, addressed by
+ * (seed; particle ID, pass, element, slice, step); the reference's own serial
+ * gauss_rn_lim(0, 1, srGaussianLimit, random_2) draws from the same
+ * truncated Gaussian in a different sequence */
+static uint64_t g_isr_seed = 0;
+static double g_sr_limit = 3.0;
+void b2e_oracle_set_isr(uint64_t seed, double limit) {
+  g_isr_seed = seed;
+  g_sr_limit = limit;
+}
+#define EPS0_MKS (1 / ((4 * PI_ * 1e-7) * C_MKS * C_MKS))
+#define POW3(x) ((x) * (x) * (x))
+#define POW5(x) (((x) * (x)) * ((x) * (x)) * (x))
+
 /* ---- KQUAD / KSEXT ---------------------------------------------------------- */
 static int m2s(double *xp, double *yp, double qx, double qy, double dp) {
   double d = SQR(1 + dp) - SQR(qx) - SQR(qy);
@@ -359,7 +375,8 @@ static int m2s(double *xp, double *yp, double qx, double qy, double dp) {
   return 1;
 }
 
-static void canonical_kick(double *qx, double *qy, double x, double y, long order, double KnL, int skew) {
+static void canonical_kick(double *qx, double *qy, double *dqx, double *dqy, double x, double y, long order,
+                           double KnL, int skew) {
   /* apply_canonical_multipole_kicks with expansion coefficients of (x+iy)^n/n! */
   double xpow[4], ypow[4], coef[4], sFx = 0, sFy = 0, fi = 1, fni;
   long i, m;
@@ -389,11 +406,14 @@ static void canonical_kick(double *qx, double *qy, double x, double y, long orde
   }
   *qx -= KnL * sFy;
   *qy += KnL * sFx;
+  *dqx -= KnL * sFy;
+  *dqy += KnL * sFx;
 }
 
-static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma) {
+static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma,
+                        int pass, int elem) {
   const double *p = e->p;
-  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt;
+  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt, rad_coef = 0, isr_coef;
   long order[3] = {0, 0, 0}, nSlices, n_kicks, ip, itop;
   int skew[3] = {0, 0, 0}, integ, nSub, radblock;
   MultAp ap;
@@ -436,13 +456,23 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
     offset_beam(c, np, dx, dy, dz);
   if (tilt)
     rotate_beam(c, np, tilt);
-  radblock = 1; /* isr_coef is nonzero (negated) when ISR is off */
+  /* multipole.c:788-800 */
+  if (p[B2E_KMULT_SYNCH_RAD])
+    rad_coef = SQR(E_MKS) * POW3(Po) / (6 * PI_ * EPS0_MKS * SQR(C_MKS) * ME_MKS);
+  isr_coef = RE_MKS * sqrt(55.0 / (24 * sqrt(3)) * POW5(Po) * 137.0359895);
+  if (!p[B2E_KMULT_ISR])
+    isr_coef *= -1;
+  if (drift < 1e-6 && (p[B2E_KMULT_ISR] || p[B2E_KMULT_SYNCH_RAD]))
+    rad_coef = isr_coef = 0;
+  radblock = rad_coef || isr_coef;
   itop = np - 1;
   for (ip = 0; ip <= itop; ip++) {
-    double *coord = c[ip], x, xp, y, yp, s, dpv, qx, qy, denom, dr;
+    double *coord = c[ip], x, xp, y, yp, s, dpv, qx, qy, denom, dr, beta0, pp;
     long i_kick, step, io;
     int lost = 0;
     dr = drift / nSlices;
+    pp = Po * (1 + coord[5]);
+    beta0 = pp / sqrt(SQR(pp) + 1);
     x = coord[0];
     xp = coord[1];
     y = coord[2];
@@ -479,21 +509,38 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
           }
           if (!kf[step])
             break;
-          for (io = 0; io < 3; io++)
-            if (KnL[io])
-              canonical_kick(&qx, &qy, x, y, order[io], KnL[io] / nSlices * kf[step], skew[io]);
-          if (!m2s(&xp, &yp, qx, qy, dpv)) {
-            lost = 1;
-            break;
-          }
-          if (radblock && dr) {
-            qx /= (1 + dpv);
-            qy /= (1 + dpv);
-            qx *= (1 + dpv);
-            qy *= (1 + dpv);
+          {
+            double dqx = 0, dqy = 0;
+            for (io = 0; io < 3; io++)
+              if (KnL[io])
+                canonical_kick(&qx, &qy, &dqx, &dqy, x, y, order[io], KnL[io] / nSlices * kf[step], skew[io]);
             if (!m2s(&xp, &yp, qx, qy, dpv)) {
               lost = 1;
               break;
+            }
+            if (radblock && dr) {
+              /* multipole.c:1320-1349, xkick = ykick = 0 */
+              double deltaFactor, F2, dsFactor, dsISRFactor;
+              qx /= (1 + dpv);
+              qy /= (1 + dpv);
+              deltaFactor = SQR(1 + dpv);
+              dqx /= kf[step];
+              dqy /= kf[step];
+              F2 = SQR(dqx / dr - 0.0 / dr) + SQR(dqy / dr + 0.0 / dr);
+              dsFactor = sqrt(1 + SQR(xp) + SQR(yp));
+              dsISRFactor = dsFactor * dr / (nSub - 1);
+              dsFactor *= dr * kf[step];
+              if (rad_coef)
+                dpv -= rad_coef * deltaFactor * F2 * dsFactor;
+              if (isr_coef > 0)
+                dpv -= isr_coef * deltaFactor * b2e_isr_pow34(F2) * sqrt(dsISRFactor) *
+                       b2e_isr_gauss(g_isr_seed, (int64_t)coord[6], pass, elem, (int)i_kick, (int)step, g_sr_limit);
+              qx *= (1 + dpv);
+              qy *= (1 + dpv);
+              if (!m2s(&xp, &yp, qx, qy, dpv)) {
+                lost = 1;
+                break;
+              }
             }
           }
         }
@@ -510,7 +557,11 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
         coord[1] = xp;
         coord[2] = y;
         coord[3] = yp;
-        coord[4] += s;
+        if (rad_coef) {
+          double p1 = Po * (1 + dpv), beta1 = p1 / sqrt(SQR(p1) + 1);
+          coord[4] = beta1 * (coord[4] / beta0 + 2 * s / (beta0 + beta1));
+        } else
+          coord[4] += s;
         coord[5] = dpv;
         if (isnan(x) || isnan(xp) || isnan(y) || isnan(yp) || fabs(x) > coord_limit || fabs(y) > coord_limit ||
             fabs(xp) > slope_limit || fabs(yp) > slope_limit)
@@ -536,8 +587,16 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
 }
 
 /* ---- CSBEND ------------------------------------------------------------- */
+/* radiation of one bend for csbend_integrate: rad_coef, isrConstant, and
+ * the address of the particle's ISR deviates */
+typedef struct {
+  double rad_coef, isr;
+  int64_t id;
+  int pass, elem;
+} BendRad;
+
 static int csbend_integrate(double *Qf, const double *Qi, double s, long n, double rho0, double rho_actual,
-                            const MultAp *ap, int integ, int isr_block, double *dz_lost) {
+                            const MultAp *ap, int integ, int isr_block, double *dz_lost, const BendRad *br) {
   double df[8], kf[8];
   int nSub = fractions(integ, df, kf), i, j;
   double dist = 0;
@@ -577,8 +636,20 @@ static int csbend_integrate(double *Qf, const double *Qi, double s, long n, doub
       Qf[1] += -ds * (1 + Qf[0] / rho0) * 1.0 / rho_actual;
       Qf[3] += ds * (1 + Qf[0] / rho0) * 0.0 / rho_actual;
       if (isr_block) {
+        /* csbend.c:1603-1622 with Fx = 0, Fy = 1 */
+        double f = (1 + Qf[0] * (1. / rho0)) / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
+        double xp = Qf[1] * f, yp = Qf[3] * f;
+        double dsFactor = sqrt(SQR(1 + Qf[0] * (1. / rho0)) + SQR(xp) + SQR(yp));
+        double F2 = SQR(0.0) + SQR(1.0);
+        double deltaFactor = SQR(1 + Qf[5]);
+        double dsISR = s / (nSub - 1);
         Qf[1] /= (1 + Qf[5]);
         Qf[3] /= (1 + Qf[5]);
+        if (br && br->rad_coef)
+          Qf[5] -= br->rad_coef * deltaFactor * F2 * ds * dsFactor;
+        if (br && br->isr > 0)
+          Qf[5] -= br->isr * deltaFactor * b2e_isr_pow34(F2) * sqrt(dsISR * dsFactor) *
+                   b2e_isr_gauss(g_isr_seed, br->id, br->pass, br->elem, i, j, g_sr_limit);
         Qf[1] *= (1 + Qf[5]);
         Qf[3] *= (1 + Qf[5]);
       }
@@ -596,9 +667,10 @@ static int same_bend(const b2e_element *a, const b2e_element *b) {
 }
 
 static long csbend_track(double **c, long np, const b2e_element *el, int idx, const b2e_element *all, int n_all,
-                         double Po, double z_start, const MaxAmp *ma) {
+                         double Po, double z_start, const MaxAmp *ma, int pass) {
   const double *p = el->p;
   double angle, e1, e2, tilt, rho0, rho_actual, fse, h, psi1, psi2, Kg1, Kg2, ttilt, ct, st;
+  BendRad br;
   double dxi, dyi, dzi, dxf, dyf, dzf, length = p[B2E_BEND_L];
   int edge1 = 0, edge2 = 0, j, integ = (int)p[B2E_BEND_INTEGRATION_ORDER];
   long nSlices = (long)p[B2E_BEND_N_SLICES], ip, itop;
@@ -679,10 +751,20 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   dxf = p[B2E_BEND_DX] * M_COS(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * M_SIN(p[B2E_BEND_ANGLE]);
   dzf = p[B2E_BEND_DX] * M_SIN(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * M_COS(p[B2E_BEND_ANGLE]);
   dyf = p[B2E_BEND_DY];
+  /* csbend.c:964-977 */
+  br.rad_coef = 0;
+  if (p[B2E_BEND_SYNCH_RAD])
+    br.rad_coef = SQR(E_MKS) * POW3(Po) * SQR(1 + fse) / (6 * PI_ * EPS0_MKS * SQR(C_MKS) * ME_MKS * SQR(rho0));
+  br.isr = RE_MKS * sqrt(55.0 / (24 * sqrt(3)) * POW5(Po) * 137.0359895 / POW3(fabs(rho_actual)));
+  if (!p[B2E_BEND_ISR])
+    br.isr *= -1;
+  br.pass = pass;
+  br.elem = idx;
   itop = np - 1;
   for (ip = 0; ip <= itop; ip++) {
     double *coord = c[ip], x, y, xp, yp, s, dp, dp0, Qi[6], Qf[6], rho, f, dz_lost;
     int lost;
+    br.id = (int64_t)coord[6];
     coord[4] += dzi * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
     coord[0] = coord[0] + dxi + dzi * coord[1];
     coord[2] = coord[2] + dyi + dzi * coord[3];
@@ -703,10 +785,16 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     Qi[3] = yp;
     Qi[4] = 0;
     Qi[5] = dp;
+    if (edge1 && e1 != 0 && br.rad_coef) {
+      /* csbend.c:1211-1216 */
+      double dp_prime = -br.rad_coef * (SQR(0.0) + SQR(1.0)) * SQR(1 + dp) *
+                        sqrt(SQR(1 + x / rho0) + SQR(xp) + SQR(yp));
+      Qi[5] -= dp_prime * x * M_TAN(e1);
+    }
     f = (1 + Qi[5]) / sqrt(1 + SQR(Qi[1]) + SQR(Qi[3]));
     Qi[1] *= f;
     Qi[3] *= f;
-    lost = !csbend_integrate(Qf, Qi, length, nSlices, rho0, rho_actual, &ap, integ, 1, &dz_lost);
+    lost = !csbend_integrate(Qf, Qi, length, nSlices, rho0, rho_actual, &ap, integ, 1, &dz_lost, &br);
     f = 1 / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
     Qf[1] *= f;
     Qf[3] *= f;
@@ -714,12 +802,19 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
       /* the reference converts back to lab coordinates (convertFromCSBendCoords)
        * before recording; only the loss bookkeeping is reproduced here */
       memcpy(coord, Qf, sizeof(double) * 4);
+      coord[5] = Qf[5];
       swap_rows(c[ip], c[itop]);
       c[itop][4] = z_start + dz_lost;
       c[itop][5] = Po * (1 + c[itop][5]);
       itop--;
       ip--;
       continue;
+    }
+    if (edge2 && e2 != 0 && br.rad_coef) {
+      /* csbend.c:1265-1276 */
+      double dp_prime = -br.rad_coef * (SQR(0.0) + SQR(1.0)) * SQR(1 + Qf[5]) *
+                        sqrt(SQR(1 + Qf[0] / rho0) + SQR(Qf[1]) + SQR(Qf[3]));
+      Qf[5] -= dp_prime * Qf[0] * M_TAN(e2);
     }
     {
       double p0 = Po * (1 + dp0), beta0 = p0 / sqrt(SQR(p0) + 1);
@@ -1090,7 +1185,7 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
       f = (1 + Qi[5]) / sqrt(1 + SQR(Qi[1]) + SQR(Qi[3]));
       Qi[1] *= f;
       Qi[3] *= f;
-      lost = !csbend_integrate(Qf, Qi, length / nSlices, 1, rho0, rho_actual, &ap, integ, 0, &dz_lost);
+      lost = !csbend_integrate(Qf, Qi, length / nSlices, 1, rho0, rho_actual, &ap, integ, 0, &dz_lost, NULL);
       f = 1 / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
       Qf[1] *= f;
       Qf[3] *= f;
@@ -1588,10 +1683,10 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
           break;
         case B2E_KQUAD:
         case B2E_KSEXT:
-          nLeft = kmult_track(c, nToTrack, e, p_central, last_z, &ma);
+          nLeft = kmult_track(c, nToTrack, e, p_central, last_z, &ma, pass, k);
           break;
         case B2E_CSBEND:
-          nLeft = csbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, &ma);
+          nLeft = csbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, &ma, pass);
           break;
         case B2E_RFCA:
           nLeft = rfca_track(c, nToTrack, e, &rf[k], p_central);
@@ -1759,3 +1854,6 @@ long b2e_oracle_lh_pass_filters(double *hist, long bins, double startHP, double 
                                 int clip) {
   return lh_pass_filters(hist, bins, startHP, endHP, startLP, endLP, clip);
 }
+
+/* Philox4x32-10 of b2e_rng.h, for its known-answer test */
+void b2e_oracle_philox(const uint32_t *ctr, const uint32_t *key, uint32_t *out) { b2e_philox4x32(ctr, key, out); }

@@ -173,13 +173,35 @@ int SDDS_CopyString(char **target, const char *source) {
   return 1;
 }
 
-/* Random numbers: only reached with ISR/scattering, which the subset excludes. */
+/* Random numbers, reached with ISR (gauss_rn_lim(0, 1, srGaussianLimit,
+ * random_2), multipole.c:1343, csbend.c:1619).  The toolkit's generators are
+ * not in the tree; these are this project's: random_2 a SplitMix64 stream
+ * (reseeded by a negative seed, as the toolkit's generators are), gauss_rn_lim
+ * Box-Muller on it with deviates beyond `limit` sigma (limit > 0) redrawn.
+ * The reference's ISR is therefore compared with the engine's in
+ * distribution, not draw by draw. */
+static uint64_t b2e_r2_state = 0x853c49e6748fea9bull;
+double random_2(long iseed) {
+  uint64_t z;
+  if (iseed < 0)
+    b2e_r2_state = (uint64_t)(-iseed) * 0x9E3779B97F4A7C15ull;
+  z = (b2e_r2_state += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
 double gauss_rn_lim(double mean, double sigma, double limit, double (*urandom)(long)) {
-  NOT_ON_PATH(gauss_rn_lim);
-  return 0;
+  int tries;
+  for (tries = 0; tries < 1000; tries++) {
+    double u1 = urandom(0), u2 = urandom(0);
+    double g = sqrt(-2.0 * log(u1)) * cos(2 * 3.141592653589793 * u2);
+    if (!(limit > 0) || fabs(g) <= limit)
+      return mean + sigma * g;
+  }
+  return mean;
 }
 double random_1(long iseed) { NOT_ON_PATH(random_1); return 0; }
-double random_2(long iseed) { NOT_ON_PATH(random_2); return 0; }
 double random_3(long iseed) { NOT_ON_PATH(random_3); return 0; }
 double random_4(long iseed) { NOT_ON_PATH(random_4); return 0; }
 double random_1_elegant(long iseed) { NOT_ON_PATH(random_1_elegant); return 0; }

@@ -111,6 +111,12 @@ class PortOracle:
             fn.restype = ctypes.c_double
             fn.argtypes = [ctypes.c_double]
         self.math = math
+        self.set_isr(0, 3.0)
+
+    def set_isr(self, seed: int, limit: float = 3.0):
+        """Seed and truncation of the ISR deviates (the engine's generator)."""
+        self.lib.b2e_oracle_set_isr.argtypes = [ctypes.c_uint64, ctypes.c_double]
+        self.lib.b2e_oracle_set_isr(ctypes.c_uint64(seed), ctypes.c_double(limit))
 
     def wake_t1(self, counts, slippage_bins, sg_half=0, sg_order=1, sgd_half=0, sgd_order=0, trapz=True,
                 steady=False):
