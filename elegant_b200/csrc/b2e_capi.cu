@@ -67,6 +67,8 @@ struct b2e_ctx {
   int n_inst = 1;
   std::vector<int64_t> inst_offsets{0, 0};
   std::vector<DevElem> elems_all; /* [n_inst][n_elems] */
+  std::vector<DevRad> rads_all;   /* [n_inst][n_elems] */
+  DevBuf<DevRad> d_rads;
   std::vector<DevAperture> aps_all;
   DevBuf<DevElem> d_elems;
   DevBuf<DevAperture> d_aps;
@@ -155,6 +157,7 @@ extern "C" int b2e_destroy(b2e_ctx *ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->d_elems.release();
+  ctx->d_rads.release();
   ctx->d_aps.release();
   ctx->d_rf.release();
   ctx->d_tiles.release();
@@ -222,6 +225,9 @@ static int upload_tiles(b2e_ctx *ctx) {
 }
 
 static int upload_lattice_tables(b2e_ctx *ctx) {
+  CUDA_TRY(ctx, ctx->d_rads.ensure(ctx->rads_all.size()));
+  CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_rads.ptr, ctx->rads_all.data(), sizeof(DevRad) * ctx->rads_all.size(),
+                                cudaMemcpyHostToDevice, ctx->stream));
   CUDA_TRY(ctx, ctx->d_elems.ensure(ctx->elems_all.size()));
   CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_elems.ptr, ctx->elems_all.data(), sizeof(DevElem) * ctx->elems_all.size(),
                                 cudaMemcpyHostToDevice, ctx->stream));
@@ -283,6 +289,7 @@ extern "C" int b2e_load_lattice(b2e_ctx *ctx, const b2e_element *elements, int32
   ctx->n_inst = 1;
   ctx->inst_offsets = {0, ctx->n};
   ctx->elems_all = ctx->lat.elems;
+  ctx->rads_all = ctx->lat.rads;
   ctx->aps_all = ctx->lat.aps;
   ctx->radiates = any_radiation(ctx->elems_all);
   build_tiles(ctx);
@@ -316,6 +323,7 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
   ctx->n_inst = n_instances;
   ctx->inst_offsets.assign(offsets, offsets + n_instances + 1);
   ctx->elems_all.clear();
+  ctx->rads_all.clear();
   ctx->aps_all.clear();
   std::vector<b2e_element> inst(ctx->base);
   CompiledLattice cl;
@@ -327,6 +335,7 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     if (!e.empty())
       return fail(ctx, B2E_ERR_LATTICE, "instance %d: %s", i, e.c_str());
     ctx->elems_all.insert(ctx->elems_all.end(), cl.elems.begin(), cl.elems.end());
+    ctx->rads_all.insert(ctx->rads_all.end(), cl.rads.begin(), cl.rads.end());
     ctx->aps_all.insert(ctx->aps_all.end(), cl.aps.begin(), cl.aps.end());
   }
   ctx->radiates = any_radiation(ctx->elems_all);
@@ -513,6 +522,7 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.hist_pass0 = ctx->hist_pass0;
   L.hist_passes = ctx->hist_passes;
   L.rad = ctx->radiates;
+  L.rads = ctx->d_rads.ptr;
   L.ids = ctx->use_ext ? nullptr : ctx->d_ids.ptr;
   L.isr_seed = ctx->opt.isr_seed;
   L.sr_limit = ctx->opt.sr_gaussian_limit == 0 ? 3.0 : ctx->opt.sr_gaussian_limit;

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
     f = (1 + DP) / sqrt((1 + XP * XP) + YP * YP);
     Q1 = XP * f;
     Q3 = YP * f;
-    const RadSite no_rad = {0, 0, 0, 0, 0};
+    const RadSite no_rad = {0, 0, 0, 0, 0, nullptr};
     int lost = csbend_integrate<false>(X, Q1, Y, Q3, Q4, DP, c, 1, (int)c[CB_NSUB], false, ap, e, no_rad);
     f = 1 / sqrt(((1 + DP) * (1 + DP) - Q1 * Q1) - Q3 * Q3);
     Q1 = Q1 * f;

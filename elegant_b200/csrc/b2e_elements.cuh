@@ -143,6 +143,7 @@ struct RadSite {
   int32_t pass, elem;
   uint64_t seed;
   double limit;
+  const double *rc; /* the element's radiation constants (DevRad) */
 };
 
 /* radiation after a kick (multipole.c:1320-1349): the momenta scaled by
@@ -151,7 +152,7 @@ struct RadSite {
 __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &dp, double dqx, double dqy,
                                                 double xp, double yp, const double *c, int step, int nSub,
                                                 unsigned flags, const RadSite &rs, int slice) {
-  const double drift = c[KM_DRIFT], kfrac = c[KM_KFRAC0 + step];
+  const double drift = rs.rc[RK_DRIFT], kfrac = rs.rc[RK_KFRAC0 + step];
   double deltaFactor, F2, dsFactor, dsISRFactor;
   qx = qx / (1 + dp);
   qy = qy / (1 + dp);
@@ -166,9 +167,9 @@ __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &
   dsISRFactor = (dsFactor * drift) / (nSub - 1);
   dsFactor = dsFactor * (drift * kfrac);
   if (flags & EF_SR)
-    dp = dp - ((c[KM_RAD] * deltaFactor) * F2) * dsFactor;
+    dp = dp - ((rs.rc[RK_RAD] * deltaFactor) * F2) * dsFactor;
   if (flags & EF_ISR)
-    dp = dp - (((c[KM_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISRFactor)) *
+    dp = dp - (((rs.rc[RK_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISRFactor)) *
                   b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, slice, step, rs.limit);
   qx = qx * (1 + dp);
   qy = qy * (1 + dp);
@@ -367,19 +368,19 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
         }
         if (RAD && (e.flags & (EF_SR | EF_ISR))) {
           /* radiation after the kick (csbend.c:1603-1622), Fx = 0, Fy = 1 */
-          const double a = 1 + X * c[CB_INV_RHO0];
+          const double a = 1 + X * rs.rc[RB_INV_RHO0];
           const double f = a / sqrt(((1 + DPoP) * (1 + DPoP) - QX * QX) - QY * QY);
           const double xp = QX * f, yp = QY * f;
           const double dsFactor = sqrt((a * a + xp * xp) + yp * yp);
           const double F2 = 0.0 * 0.0 + 1.0 * 1.0;
           const double deltaFactor = (1 + DPoP) * (1 + DPoP);
-          const double dsISR = c[CB_SLICE] / (nSub - 1);
+          const double dsISR = rs.rc[RB_SLICE] / (nSub - 1);
           QX = QX / (1 + DPoP);
           QY = QY / (1 + DPoP);
           if (e.flags & EF_SR)
-            DPoP = DPoP - (((c[CB_RAD] * deltaFactor) * F2) * ds) * dsFactor;
+            DPoP = DPoP - (((rs.rc[RB_RAD] * deltaFactor) * F2) * ds) * dsFactor;
           if (e.flags & EF_ISR)
-            DPoP = DPoP - (((c[CB_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISR * dsFactor)) *
+            DPoP = DPoP - (((rs.rc[RB_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISR * dsFactor)) *
                               b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, i, j, rs.limit);
           QX = QX * (1 + DPoP);
           QY = QY * (1 + DPoP);
@@ -402,9 +403,9 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
 /* dp_prime * x * tan(e) of the radiation edge corrections (csbend.c:1211-1216,
  * :1265-1276), Fx = 0, Fy = 1 */
 __device__ __forceinline__ double bend_edge_radiation(double x, double xp, double yp, double dp, double tan_e,
-                                                      const double *c) {
+                                                      const double *c, const double *rc) {
   const double a = 1 + x / c[CB_RHO0];
-  const double dp_prime = ((-c[CB_RAD]) * (0.0 * 0.0 + 1.0 * 1.0)) * ((1 + dp) * (1 + dp)) *
+  const double dp_prime = ((-rc[RB_RAD]) * (0.0 * 0.0 + 1.0 * 1.0)) * ((1 + dp) * (1 + dp)) *
                           sqrt((a * a + xp * xp) + yp * yp);
   return (dp_prime * x) * tan_e;
 }
@@ -439,7 +440,7 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
 
   /* anticipate the radiation error of integrating the sector (csbend.c:1211-1216) */
   if (RAD && (e.flags & EF_EDGE1) && (e.flags & EF_SR) && c[CB_E1] != 0)
-    dp = dp - bend_edge_radiation(x, xp, yp, dp, c[CB_TAN_E1], c);
+    dp = dp - bend_edge_radiation(x, xp, yp, dp, c[CB_TAN_E1], c, rs.rc);
 
   /* convertToDipoleCanonicalCoordinates (csbend.c:1411-1419) */
   f = (1 + dp) / sqrt((1 + xp * xp) + yp * yp);
@@ -465,7 +466,7 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   }
   /* correct the radiation error of the sector at the exit (csbend.c:1265-1276) */
   if (RAD && (e.flags & EF_EDGE2) && (e.flags & EF_SR) && c[CB_E2] != 0)
-    dp = dp - bend_edge_radiation(Q0, Q1, Q3, dp, c[CB_TAN_E2], c);
+    dp = dp - bend_edge_radiation(Q0, Q1, Q3, dp, c[CB_TAN_E2], c, rs.rc);
 
   if (e.flags & EF_RADBLOCK) {
     /* time-of-flight velocity fix (csbend.c:1278-1288) */

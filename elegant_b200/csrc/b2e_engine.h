@@ -20,7 +20,7 @@
 #include <stdint.h>
 #include "../../include/elegant_b200.h"
 
-#define B2E_NC 52 /* constants per compiled element */
+#define B2E_NC 40 /* constants per compiled element */
 
 /* Compiled element kinds (device dispatch) */
 enum {
@@ -66,10 +66,7 @@ enum {
 #define KM_REV_COS 32   /* reverse tilt cos/sin for the aperture check */
 #define KM_REV_SIN 33
 #define KM_SKEW0 34     /* J1 kick per substep 34..39 (first 6 substeps) */
-#define KM_KFRAC0 40    /* kickFrac[j], j = 0..7 -> 40..47 (radiation) */
-#define KM_RAD 48       /* rad_coef (multipole.c:789) */
-#define KM_ISR 49       /* isr_coef, > 0 only when ISR is applied (:790-795) */
-#define KM_DRIFT 50     /* slice drift length (:1189) */
+
 
 /* CSBEND constant slots */
 #define CB_RHO0 0
@@ -93,10 +90,20 @@ enum {
 #define CB_DYF 32
 #define CB_DZF 33
 #define CB_ET0 34       /* dcoord_etilt[0..4] -> 34..38 */
-#define CB_RAD 40       /* rad_coef (csbend.c:967-970) */
-#define CB_ISR 41       /* isrConstant, > 0 only when ISR is applied (:972-975) */
-#define CB_SLICE 42     /* s = length / N_SLICES, for dsISR (:1614) */
-#define CB_INV_RHO0 43  /* 1. / rho0 (:1605) */
+
+
+/* Radiation constants of a KMULT / CSBEND, in a table beside the element
+ * records ([instance][element] DevRad): only radiating lattices read them, so
+ * the records the ring kernel stages in shared memory stay small. */
+#define B2E_NRAD 12
+#define RK_KFRAC0 0     /* KMULT: kickFrac[j], j = 0..7 */
+#define RK_RAD 8        /* rad_coef (multipole.c:789) */
+#define RK_ISR 9        /* isr_coef, > 0 only when ISR is applied (:790-795) */
+#define RK_DRIFT 10     /* slice drift length (:1189) */
+#define RB_RAD 0        /* CSBEND: rad_coef (csbend.c:967-970) */
+#define RB_ISR 1        /* isrConstant, > 0 only when ISR is applied (:972-975) */
+#define RB_SLICE 2      /* s = length / N_SLICES, for dsISR (:1614) */
+#define RB_INV_RHO0 3   /* 1. / rho0 (:1605) */
 
 /* RFCA constant slots */
 #define RF_VOLT 0       /* volt/(1e6*mc^2[MV]*sign)/nKicks */
@@ -122,6 +129,10 @@ typedef struct {
   double rev_cos, rev_sin; /* reverse tilt for internal aperture checks */
   double c[B2E_NC];
 } DevElem;
+
+typedef struct {
+  double c[B2E_NRAD];
+} DevRad;
 
 typedef struct {
   double x_max, y_max;

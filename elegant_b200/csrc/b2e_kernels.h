@@ -28,6 +28,7 @@ struct RingLaunch {
    * radiation code; ISR deviates are addressed by particle ID (ids, or the
    * row number + 1 without IDs), pass, element, slice and step */
   int rad;
+  const DevRad *rads;       /* [n_inst][n_elems] */
   const int64_t *ids;
   uint64_t isr_seed;
   double sr_limit;

@@ -168,7 +168,7 @@ static void bend_edge_flags(const b2e_element *el, int n, int i, bool *edge1, bo
   *edge2 = el[i].p[B2E_BEND_EDGE2_EFFECTS] != 0 && !same_post;
 }
 
-static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d) {
+static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, DevRad &r) {
   const double *p = el.p;
   double drift_frac[8], kick_frac[8];
   const double L = p[B2E_KMULT_L];
@@ -244,11 +244,11 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d) {
       isr_coef *= -1;
     if (L < 1e-6 && (isr || sr))
       rad_coef = isr_coef = 0;
-    d.c[KM_RAD] = rad_coef;
-    d.c[KM_ISR] = isr_coef;
-    d.c[KM_DRIFT] = drift;
+    r.c[RK_RAD] = rad_coef;
+    r.c[RK_ISR] = isr_coef;
+    r.c[RK_DRIFT] = drift;
     for (int j = 0; j < 8; j++)
-      d.c[KM_KFRAC0 + j] = j < nSub ? kick_frac[j] : 0;
+      r.c[RK_KFRAC0 + j] = j < nSub ? kick_frac[j] : 0;
     if ((rad_coef != 0 || isr_coef != 0) && drift != 0)
       d.flags |= EF_RADBLOCK;
     if (rad_coef != 0 && drift != 0)
@@ -259,7 +259,8 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d) {
   return "";
 }
 
-static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, double Po, DevElem &d) {
+static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, double Po, DevElem &d,
+                                  DevRad &r) {
   const double *p = el.p;
   double drift_frac[8], kick_frac[8];
   const double length = p[B2E_BEND_L];
@@ -383,10 +384,10 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     isr_const = kRE_MKS * sqrt(55.0 / (24 * sqrt(3)) * pow5_host(Po) * 137.0359895 / pow3_host(fabs(rho_actual)));
     if (p[B2E_BEND_ISR] == 0)
       isr_const *= -1;
-    d.c[CB_RAD] = rad_coef;
-    d.c[CB_ISR] = isr_const;
-    d.c[CB_SLICE] = s;
-    d.c[CB_INV_RHO0] = 1. / rho0;
+    r.c[RB_RAD] = rad_coef;
+    r.c[RB_ISR] = isr_const;
+    r.c[RB_SLICE] = s;
+    r.c[RB_INV_RHO0] = 1. / rho0;
     d.flags |= EF_RADBLOCK;
     if (rad_coef != 0)
       d.flags |= EF_SR;
@@ -426,7 +427,9 @@ const char *compile_single_csr_bend(const b2e_element &el, DevElem &d) {
     return "element is not a CSRCSBEND";
   memset(&d, 0, sizeof(d));
   d.ap_pass0 = d.ap_later = -1;
-  std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, 0.0, d);
+  DevRad unused_rad;
+  std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, 0.0, d,
+                                 unused_rad);
   if (!e.empty()) {
     snprintf(msg, sizeof(msg), "%s", e.c_str());
     return msg;
@@ -440,6 +443,9 @@ const char *compile_single_csr_bend(const b2e_element &el, DevElem &d) {
 std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options &opt, CompiledLattice &out) {
   out = CompiledLattice();
   out.elems.resize(n);
+  out.rads.assign(n, DevRad());
+  for (DevRad &r : out.rads)
+    memset(&r, 0, sizeof(r));
   int last_ap = -1;
   double z = 0;
   for (int i = 0; i < n; i++) {
@@ -466,14 +472,14 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
       break;
     case B2E_KQUAD:
     case B2E_KSEXT:
-      err = compile_kmult(el[i], opt.p_central, d);
+      err = compile_kmult(el[i], opt.p_central, d, out.rads[i]);
       z += p[B2E_KMULT_L];
       break;
     case B2E_CSBEND:
     case B2E_CSRCSBEND: {
       bool e1, e2;
       bend_edge_flags(el, n, i, &e1, &e2);
-      err = compile_csbend(el[i], e1, e2, opt.p_central, d);
+      err = compile_csbend(el[i], e1, e2, opt.p_central, d, out.rads[i]);
       if (el[i].type == B2E_CSRCSBEND && d.kind == K_CSRCSBEND)
         out.csr_elements.push_back(i);
       z += p[B2E_BEND_L];

@@ -23,6 +23,7 @@ void element_defaults(int type, double *p);
 
 struct CompiledLattice {
   std::vector<DevElem> elems;
+  std::vector<DevRad> rads;        /* radiation constants, parallel to elems */
   std::vector<DevAperture> aps;
   std::vector<int> rf_elements;    /* element indices of RFCA, in lattice order */
   std::vector<int> csr_elements;   /* CSRCSBEND / CSRDRIFT indices */

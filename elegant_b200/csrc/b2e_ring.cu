@@ -134,7 +134,8 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
 
   int lost = LOSS_NONE, lost_pass = -1, lost_elem = -1;
   bool active = tracked;
-  RadSite rs = {0, 0, 0, 0, 0};
+  RadSite rs = {0, 0, 0, 0, 0, nullptr};
+  const DevRad *rads = RAD ? L.rads + (size_t)tile.inst * L.n_elems : nullptr;
   if (RAD) {
     rs.id = tracked ? (L.ids ? L.ids[ip] : ip + 1) : 0;
     rs.seed = L.isr_seed;
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
         if (RAD) {
           rs.pass = pass;
           rs.elem = ie;
+          rs.rc = rads[ie].c;
         }
         lost = kmult<RAD>(p, e, ap, L.g, rs);
         break;
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
         if (RAD) {
           rs.pass = pass;
           rs.elem = ie;
+          rs.rc = rads[ie].c;
         }
         lost = csbend<RAD>(p, e, ap, L.g, rs);
         break;
