@@ -23,7 +23,7 @@ ERRORS = {
 }
 
 # element type codes (include/elegant_b200.h)
-DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT = range(1, 12)
+DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT, MALIGN = range(1, 13)
 MAX_PARAMS = 40
 RING_VARIANTS = 17
 

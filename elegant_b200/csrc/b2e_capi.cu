@@ -258,7 +258,7 @@ static bool any_radiation(const std::vector<DevElem> &elems) {
 }
 
 extern "C" int b2e_element_defaults(int32_t type, b2e_element *element) {
-  if (!element || type < B2E_DRIF || type > B2E_CSRDRIFT)
+  if (!element || type < B2E_DRIF || type > B2E_MALIGN)
     return B2E_ERR_ARG;
   element->type = type;
   element->reserved = 0;

@@ -501,6 +501,38 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   return LOSS_NONE;
 }
 
+/* ---- MALIGN: offset_beam (do_tracking.c:3243-3300) for one particle ---- */
+__device__ __forceinline__ void malign(Part &p, const double *c, double p_central) {
+  double ds, pc, beta, t;
+  if (c[MA_DZ] != 0)
+    ds = c[MA_DZ] * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+  else
+    ds = 0;
+  p.x = p.x + (c[MA_DX] + c[MA_DZ] * p.xp);
+  p.xp = p.xp + c[MA_DXP];
+  p.y = p.y + (c[MA_DY] + c[MA_DZ] * p.yp);
+  p.yp = p.yp + c[MA_DYP];
+  p.s = p.s + ds;
+  if (c[MA_DT] != 0 || c[MA_DP] != 0 || c[MA_DE] != 0) {
+    double gamma;
+    pc = p_central * (1 + p.dp);
+    beta = pc / (gamma = sqrt(1 + pc * pc));
+    t = p.s / (beta * c[MA_C]) + c[MA_DT];
+    if (c[MA_DP] != 0) {
+      p.dp = p.dp + c[MA_DP];
+      pc = p_central * (1 + p.dp);
+      beta = pc / sqrt(1 + pc * pc);
+    }
+    if (c[MA_DE] != 0) {
+      gamma = gamma + c[MA_DE] * gamma;
+      pc = sqrt(gamma * gamma - 1);
+      beta = pc / gamma;
+      p.dp = (pc - p_central) / p_central;
+    }
+    p.s = (t * beta) * c[MA_C];
+  }
+}
+
 /* ---- RFCA, zero length, single kick: trackRfCavityWithWakes
  * (simple_rfca.c:295-985) with add_to_particle_energy (:987-1006) and the
  * final removeInvalidParticles sweep (limit_amplitudes.c:274-315). */

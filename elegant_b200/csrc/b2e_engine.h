@@ -33,7 +33,8 @@ enum {
   K_RFCA,
   K_MAXAMP,
   K_CSRCSBEND, /* collective: handled by the CSR driver, never in the ring kernel */
-  K_CSRDRIFT
+  K_CSRDRIFT,
+  K_MALIGN     /* offset_beam on one pass (or every pass) */
 };
 
 /* Flags */
@@ -114,6 +115,20 @@ enum {
 #define RF_T_REFERENCE 5
 #define RF_SOFFSET 6    /* length/2 used by the fiducial sum */
 #define RF_SLOT 7       /* index into the per-instance RF state table */
+
+/* MALIGN constant slots */
+#define MA_DX 0
+#define MA_DXP 1
+#define MA_DY 2
+#define MA_DYP 3
+#define MA_DZ 4
+#define MA_DT 5
+#define MA_DP 6
+#define MA_DE 7
+#define MA_ON_PASS 8    /* -1: every pass */
+#define MA_START_PID 9  /* -1: every particle */
+#define MA_END_PID 10
+#define MA_C 11         /* c_mks */
 
 /* DRIF / EDRIFT slots */
 #define DR_L 0

@@ -136,6 +136,11 @@ void element_defaults(int type, double *p) {
     p[B2E_CSRDRIFT_N_KICKS] = 1;
     p[B2E_CSRDRIFT_CSR] = 1;
     break;
+  case B2E_MALIGN:
+    p[B2E_MALIGN_ON_PASS] = -1;         /* track_data.c:935-938 */
+    p[B2E_MALIGN_START_PID] = -1;
+    p[B2E_MALIGN_END_PID] = -1;
+    break;
   default:
     break;
   }
@@ -529,6 +534,28 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
       out.csr_elements.push_back(i);
       z += p[B2E_CSRDRIFT_L];
       break;
+    case B2E_MALIGN: {
+      /* offset_beam's checks (do_tracking.c:3268-3271) */
+      const long s_pid = (long)p[B2E_MALIGN_START_PID], e_pid = (long)p[B2E_MALIGN_END_PID];
+      if (s_pid >= 0 && s_pid > e_pid)
+        err = "MALIGN START_PID greater than END_PID";
+      else if ((e_pid >= 0 && s_pid < 0) || (s_pid >= 0 && e_pid < 0))
+        err = "MALIGN START_PID and END_PID must both be set or both be -1";
+      d.kind = K_MALIGN;
+      d.c[MA_DX] = p[B2E_MALIGN_DX];
+      d.c[MA_DXP] = p[B2E_MALIGN_DXP];
+      d.c[MA_DY] = p[B2E_MALIGN_DY];
+      d.c[MA_DYP] = p[B2E_MALIGN_DYP];
+      d.c[MA_DZ] = p[B2E_MALIGN_DZ];
+      d.c[MA_DT] = p[B2E_MALIGN_DT];
+      d.c[MA_DP] = p[B2E_MALIGN_DP];
+      d.c[MA_DE] = p[B2E_MALIGN_DE];
+      d.c[MA_ON_PASS] = (double)(long)p[B2E_MALIGN_ON_PASS];
+      d.c[MA_START_PID] = (double)s_pid;
+      d.c[MA_END_PID] = (double)e_pid;
+      d.c[MA_C] = kC_MKS;
+      break;
+    }
     default:
       err = "unsupported element type";
     }

@@ -187,6 +187,20 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
         }
         lost = csbend<RAD>(p, e, ap, L.g, rs);
         break;
+      case K_MALIGN: {
+        const double *mc = e.c;
+        const int on_pass = (int)mc[MA_ON_PASS];
+        if (on_pass == -1 || on_pass == pass) {
+          bool hit = true;
+          if (mc[MA_START_PID] >= 0) {
+            const double id = (double)(L.ids ? L.ids[ip] : ip + 1);
+            hit = !(id < mc[MA_START_PID] || id > mc[MA_END_PID]);
+          }
+          if (hit)
+            malign(p, mc, L.g.p_central);
+        }
+        break;
+      }
       case K_RFCA: {
         const DevRfState rs = rf[(int)e.c[RF_SLOT]];
         if (!rs.set) {

@@ -29,11 +29,11 @@ class LatticeError(ValueError):
 TYPES = {
     "DRIF": nat.DRIF, "DRIFT": nat.DRIF, "EDRIFT": nat.EDRIFT, "KQUAD": nat.KQUAD, "KSEXT": nat.KSEXT,
     "CSBEND": nat.CSBEND, "RFCA": nat.RFCA, "MAXAMP": nat.MAXAMP, "MARK": nat.MARK, "MARKER": nat.MARK,
-    "CHARGE": nat.CHARGE, "CSRCSBEND": nat.CSRCSBEND, "CSRDRIFT": nat.CSRDRIFT,
+    "CHARGE": nat.CHARGE, "CSRCSBEND": nat.CSRCSBEND, "CSRDRIFT": nat.CSRDRIFT, "MALIGN": nat.MALIGN,
 }
 TYPE_NAMES = {nat.DRIF: "DRIF", nat.EDRIFT: "EDRIFT", nat.KQUAD: "KQUAD", nat.KSEXT: "KSEXT",
               nat.CSBEND: "CSBEND", nat.RFCA: "RFCA", nat.MAXAMP: "MAXAMP", nat.MARK: "MARK",
-              nat.CHARGE: "CHARGE", nat.CSRCSBEND: "CSRCSBEND", nat.CSRDRIFT: "CSRDRIFT"}
+              nat.CHARGE: "CHARGE", nat.CSRCSBEND: "CSRCSBEND", nat.CSRDRIFT: "CSRDRIFT", nat.MALIGN: "MALIGN"}
 
 _KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, "N_SLICES": 8,
           "INTEGRATION_ORDER": 9, "SYNCH_RAD": 12, "ISR": 13, "ISR1PART": 14}
@@ -58,6 +58,8 @@ SLOTS = {
     nat.MARK: {},
     nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},
     nat.CSRDRIFT: {"L": 0, "N_KICKS": 1, "DZ": 2, "CSR": 3, "USE_STUPAKOV": 4},
+    nat.MALIGN: {"DXP": 0, "DYP": 1, "DX": 2, "DY": 3, "DZ": 4, "DT": 5, "DP": 6, "DE": 7, "ON_PASS": 8,
+                 "START_PID": 9, "END_PID": 10},
 }
 
 # defaults from the reference's parameter tables (only nonzero ones listed)
@@ -73,6 +75,7 @@ DEFAULTS = {
     nat.RFCA: {"FREQ": 500e6, "T_REFERENCE": -1},
     nat.MAXAMP: {"EXPONENT": 2},
     nat.CSRDRIFT: {"N_KICKS": 1, "CSR": 1},
+    nat.MALIGN: {"ON_PASS": -1, "START_PID": -1, "END_PID": -1},
 }
 
 LENGTH_TYPES = {nat.DRIF, nat.EDRIFT, nat.KQUAD, nat.KSEXT, nat.CSBEND, nat.RFCA, nat.CSRCSBEND, nat.CSRDRIFT}

@@ -1,0 +1,211 @@
+"""Momentum-aperture search (elegant's &momentum_aperture, output_mode 0,
+momentumAperture.c:243-700) on the batched engine.
+
+The reference, for every selected element and each sign of the momentum
+offset, tracks one particle at a time: the particle starts on the design
+orbit (zero coordinates), and when it reaches the element after the selected
+one on pass 1 (pass 0 for a one-pass run) a tracking "wedge" offsets it by
+(x_initial, y_initial, delta) through offset_beam (momentumAperture.c:34-45).
+Each scan steps delta from its start by delta_step_size until a particle is
+lost; each of the `splits` refinements restarts steps_back steps behind the
+last survivor with a step split_step_divisor times smaller, up to the first
+loss (:540-657).  Every run is its own fiducial beam (fiducialize = 0:
+delete_phase_references before each run).
+
+Particle fates are independent, so each refinement level is one engine run
+holding every trial of every element and side at once: one ensemble instance
+per trial (so that each trial's RF phase reference comes from that particle
+alone, as in the reference), a MALIGN element after every selected element
+carrying the wedge (ON_PASS = the firing pass; per-instance overrides set DX,
+DY and DP on the trial's own element and leave the others at zero, where
+offset_beam changes nothing).  The deltas come from the same repeated
+additions, so the first loss of each scan, the last survivor before it and
+the next level's start are the reference's, bit for bit.
+
+Not built: fiducialize = 1, forbid_resonance_crossing (needs tunes from
+turn-by-turn data), output modes 1 and 2, include patterns with wildcards
+other than '*' and '?'.
+"""
+from __future__ import annotations
+
+import fnmatch
+import math
+
+import numpy as np
+
+from .beam import Beam
+from .lattice import Element, Lattice
+from .track import Tracker
+
+WEDGE = "MA_WEDGE"
+
+
+def wedge_lattice(lattice: Lattice, locations, fire_on_pass: int) -> tuple[Lattice, list[int]]:
+    """The lattice with a zero MALIGN wedge where each selected element's
+    wedge fires: before the element that follows it, or before the first
+    selected element for the line's last element (momentumAperture.c:517-518).
+    Returns it and the wedges' element indices, in the order of locations."""
+    last = len(lattice.elements) - 1
+    before = {}  # element index -> selected elements whose wedge goes just before it
+    for i in locations:
+        before.setdefault(i + 1 if i < last else locations[0], []).append(i)
+    els, at = [], {}
+    for i, e in enumerate(lattice.elements):
+        for src in before.get(i, []):
+            at[src] = len(els)
+            els.append(Element(f"{WEDGE}{src}", "MALIGN", {"ON_PASS": fire_on_pass}))
+        els.append(e)
+    return Lattice(els), [at[i] for i in locations]
+
+
+def select_elements(lattice: Lattice, s_start=0.0, s_end=math.inf, include_name_pattern=None,
+                    include_type_pattern=None, skip_elements=0, process_elements=2 ** 31 - 1):
+    """Element indices in the reference's order and selection
+    (momentumAperture.c:282-300): end position in [s_start, s_end), name and
+    type patterns, the first skip_elements matches skipped, at most
+    process_elements."""
+    out, z, skip = [], 0.0, skip_elements
+    for i, e in enumerate(lattice.elements):
+        z += e.length
+        if not (len(out) < process_elements and z < s_end):
+            break
+        if z >= s_start and (include_name_pattern is None or fnmatch.fnmatchcase(e.name, include_name_pattern)) and \
+                (include_type_pattern is None or fnmatch.fnmatchcase(e.type, include_type_pattern)):
+            if skip > 0:
+                skip -= 1
+                continue
+            out.append(i)
+    return out
+
+
+def scan_deltas(start: float, interval: float, limit: float) -> list[float]:
+    """The deltas one scan tries: start, start + interval, ... while
+    |delta| <= |limit| (repeated additions, momentumAperture.c:543-643)."""
+    out, d = [], start
+    while abs(d) <= abs(limit):
+        out.append(d)
+        d += interval
+        if len(out) > 10_000_000:
+            raise ValueError("momentum aperture scan does not end")
+    return out
+
+
+def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initial=1e-5, y_initial=1e-5,
+                      delta_negative_limit=-0.10, delta_positive_limit=0.10, delta_negative_start=0.0,
+                      delta_positive_start=0.0, delta_step_size=0.0025, splits=1, steps_back=1,
+                      split_step_divisor=10, s_start=0.0, s_end=math.inf, include_name_pattern=None,
+                      include_type_pattern=None, skip_elements=0, process_elements=2 ** 31 - 1,
+                      soft_failure=False, device=0, compact_every=0, track_trials=None):
+    """Returns one dict per selected element: name, type, s (its end),
+    index, and per side ('negative', 'positive'): delta (last survivor),
+    found (a loss was found), lost_on_pass, x_lost, y_lost, delta_lost
+    (the first lost trial's offset).  Also returns the number of
+    particle-turns tracked.  track_trials(lattice, offsets, overrides, beam,
+    p_central, n_passes) -> (lost_pass, coords at the end or at loss, effort),
+    rows in beam order, replaces the engine (used to check the batching
+    against a CPU tracker)."""
+    if delta_negative_limit >= 0 or delta_positive_limit <= 0 or delta_negative_start > 0 or \
+            delta_positive_start < 0 or delta_step_size <= 0 or splits < 0 or s_start >= s_end:
+        raise ValueError("momentum_aperture: invalid limits, starts, step, splits or s range "
+                         "(momentumAperture.c:80-101)")
+    locs = select_elements(lattice, s_start, s_end, include_name_pattern, include_type_pattern, skip_elements,
+                           process_elements)
+    if not locs:
+        raise ValueError("no elements found between s_start and s_end for momentum aperture computation")
+    fire = 0 if n_passes == 1 else 1
+    wl, wedges = wedge_lattice(lattice, locs, fire)
+    z_end = np.cumsum([e.length for e in lattice.elements])
+    limits = (delta_negative_limit, delta_positive_limit)
+    starts = (delta_negative_start, delta_positive_start)
+    # per (location, side) scan state, as in the reference's loop variables
+    st = []
+    for k, _ in enumerate(locs):
+        for side in (0, 1):
+            sign = -1 if side == 0 else 1
+            st.append({"k": k, "side": side, "sign": sign, "start": starts[side], "interval": delta_step_size * sign,
+                       "limit": limits[side], "lost": sign * 1.7976931348623157e308 / 2, "survived": 0.0,
+                       "survivor": False, "loser": False, "lost_on_pass": -1, "x_lost": 0.0, "y_lost": 0.0,
+                       "delta_lost_at": 0.0, "active": True})
+    effort = 0.0
+    for split in range(splits + 1):
+        trials = []  # (scan index, delta)
+        for j, s in enumerate(st):
+            if s["active"]:
+                trials += [(j, d) for d in scan_deltas(s["start"], s["interval"], s["limit"])]
+        if trials:
+            lost_pass, x_l, y_l, dpl, eff = _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial,
+                                                          y_initial, device, compact_every, track_trials)
+            effort += eff
+            done = set()
+            for t, (j, d) in enumerate(trials):
+                if j in done:
+                    continue
+                s = st[j]
+                if lost_pass[t] >= 0:
+                    s.update(lost_on_pass=int(lost_pass[t]), x_lost=float(x_l[t]), y_lost=float(y_l[t]),
+                             delta_lost_at=float(dpl[t]), loser=True)
+                    s["lost"] = d
+                    done.add(j)
+                else:
+                    s["survived"] = d
+                    s["survivor"] = True
+        for s in st:
+            if not s["active"]:
+                continue
+            stop = False
+            if split == 0:
+                if not s["survivor"]:
+                    if not soft_failure:
+                        raise RuntimeError(f"No survivor found for initial scan for element index {locs[s['k']]}")
+                    s["survived"], s["survivor"], stop = 0.0, True, True
+                if not s["loser"]:
+                    if not soft_failure:
+                        raise RuntimeError(f"No loss found for initial scan for element index {locs[s['k']]}")
+                    s["loser"], stop = True, True
+            s["start"] = s["survived"] - steps_back * s["interval"]
+            s["interval"] /= split_step_divisor
+            s["start"] += s["interval"]
+            s["limit"] = s["lost"]
+            if (s["start"] < 0 and s["sign"] == 1) or (s["start"] > 0 and s["sign"] == -1):
+                s["start"] = 0
+            if stop:
+                s["active"] = False
+    out = []
+    for k, i in enumerate(locs):
+        e = lattice.elements[i]
+        row = {"index": i, "name": e.name, "type": e.type, "s": float(z_end[i])}
+        for side, label in ((0, "negative"), (1, "positive")):
+            s = st[2 * k + side]
+            row[label] = {"delta": s["survived"], "found": s["loser"], "lost_on_pass": s["lost_on_pass"],
+                          "x_lost": s["x_lost"], "y_lost": s["y_lost"], "delta_lost": s["lost"]
+                          if s["loser"] and abs(s["lost"]) < 1e300 else None}
+        out.append(row)
+    return out, effort
+
+
+def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_initial, device, compact_every,
+                  track_trials=None):
+    """One engine run, one instance (one particle) per trial."""
+    n = len(trials)
+    coords = np.zeros((n, 6))
+    ids = np.arange(1, n + 1, dtype=np.int64)
+    offsets = np.arange(n + 1, dtype=np.int64)
+    overrides = []
+    for w_k, wi in enumerate(wedges):
+        dx = np.zeros(n)
+        dy = np.zeros(n)
+        dp = np.zeros(n)
+        for t, (j, d) in enumerate(trials):
+            if st[j]["k"] == w_k:
+                dx[t], dy[t], dp[t] = x_initial, y_initial, d
+        overrides += [(wi, "DX", dx), (wi, "DY", dy), (wi, "DP", dp)]
+    beam = Beam(coords, ids)
+    if track_trials is not None:
+        lost_pass, c, effort = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
+        return lost_pass, c[:, 0], c[:, 2], c[:, 5], effort
+    with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every) as t:
+        t.load_ensemble(offsets, overrides)
+        res = t.track(beam)
+    order = np.argsort(res.ids)
+    c = res.coords[order]
+    return res.lost_pass[order], c[:, 0], c[:, 2], c[:, 5], res.effort

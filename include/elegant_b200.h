@@ -63,6 +63,7 @@ extern "C" {
 #define B2E_CHARGE 9
 #define B2E_CSRCSBEND 10
 #define B2E_CSRDRIFT 11
+#define B2E_MALIGN 12
 
 #define B2E_MAX_PARAMS 40
 #define B2E_RING_VARIANTS 17
@@ -157,6 +158,19 @@ extern "C" {
 #define B2E_CSRDRIFT_DZ 2
 #define B2E_CSRDRIFT_CSR 3
 #define B2E_CSRDRIFT_USE_STUPAKOV 4
+/* MALIGN (malign_param, track_data.c:926-940; offset_beam, do_tracking.c:3243-3300;
+ * applied on pass ON_PASS, or every pass for -1, do_tracking.c:1818-1821) */
+#define B2E_MALIGN_DXP 0
+#define B2E_MALIGN_DYP 1
+#define B2E_MALIGN_DX 2
+#define B2E_MALIGN_DY 3
+#define B2E_MALIGN_DZ 4
+#define B2E_MALIGN_DT 5
+#define B2E_MALIGN_DP 6
+#define B2E_MALIGN_DE 7
+#define B2E_MALIGN_ON_PASS 8   /* default -1 */
+#define B2E_MALIGN_START_PID 9 /* default -1: every particle */
+#define B2E_MALIGN_END_PID 10  /* default -1 */
 
 typedef struct {
   int32_t type;             /* B2E_DRIF ... */

@@ -844,6 +844,43 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   return itop + 1;
 }
 
+/* ---- MALIGN: offset_beam (do_tracking.c:3243-3300) ----------------------- */
+static void malign_track(double **c, long np, const b2e_element *e, double Po) {
+  const double *p = e->p;
+  const double dx = p[B2E_MALIGN_DX], dxp = p[B2E_MALIGN_DXP], dy = p[B2E_MALIGN_DY], dyp = p[B2E_MALIGN_DYP];
+  const double dz = p[B2E_MALIGN_DZ], dt = p[B2E_MALIGN_DT], dp = p[B2E_MALIGN_DP], de = p[B2E_MALIGN_DE];
+  const long s_pid = (long)p[B2E_MALIGN_START_PID], e_pid = (long)p[B2E_MALIGN_END_PID];
+  long i;
+  for (i = np - 1; i >= 0; i--) {
+    double *v = c[i], ds, pc, beta, gamma, t;
+    if (!(s_pid == -1 && e_pid == -1) && (v[6] < s_pid || v[6] > e_pid))
+      continue;
+    ds = dz ? dz * sqrt(1 + SQR(v[1]) + SQR(v[3])) : 0;
+    v[0] += dx + dz * v[1];
+    v[1] += dxp;
+    v[2] += dy + dz * v[3];
+    v[3] += dyp;
+    v[4] += ds;
+    if (dt || dp || de) {
+      pc = Po * (1 + v[5]);
+      beta = pc / (gamma = sqrt(1 + pc * pc));
+      t = v[4] / (beta * C_MKS) + dt;
+      if (dp) {
+        v[5] += dp;
+        pc = Po * (1 + v[5]);
+        beta = pc / sqrt(1 + pc * pc);
+      }
+      if (de) {
+        gamma += de * gamma;
+        pc = sqrt(gamma * gamma - 1);
+        beta = pc / gamma;
+        v[5] = (pc - Po) / Po;
+      }
+      v[4] = t * beta * C_MKS;
+    }
+  }
+}
+
 /* ---- RFCA (zero length, TMEAN fiducial) ---------------------------------- */
 typedef struct {
   int seen;
@@ -1712,6 +1749,11 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
           break;
         case B2E_CSRDRIFT:
           nLeft = csrdrift_track(c, nToTrack, e, p_central, last_z, &cw);
+          break;
+        case B2E_MALIGN:
+          /* do_tracking.c:1818-1821 */
+          if ((long)p[B2E_MALIGN_ON_PASS] == -1 || (long)p[B2E_MALIGN_ON_PASS] == pass)
+            malign_track(c, nToTrack, e, p_central);
           break;
         default:
           break;

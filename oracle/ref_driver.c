@@ -43,7 +43,46 @@ static const B2E_REF_TYPE b2e_ref_types[] = {
   {"DRIF", T_DRIF}, {"DRIFT", T_DRIF}, {"EDRIFT", T_EDRIFT}, {"KQUAD", T_KQUAD},
   {"KSEXT", T_KSEXT}, {"CSBEND", T_CSBEND}, {"SBEN", T_CSBEND}, {"RFCA", T_RFCA},
   {"MAXAMP", T_MAXAMP}, {"MARK", T_MARK}, {"CHARGE", T_CHARGE},
-  {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {NULL, 0}};
+  {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {"MALIGN", T_MALIGN}, {NULL, 0}};
+
+/* offset_beam (do_tracking.c:3243-3300) restated: do_tracking.c is not part
+ * of the compiled subset */
+static void b2e_ref_offset_beam(double **coord, long nToTrack, MALIGN *offset, double P_central) {
+  long i_part, allParticles;
+  double *part, pc, beta, gamma, t, ds;
+  allParticles = (offset->startPID == -1) && (offset->endPID == -1);
+  for (i_part = nToTrack - 1; i_part >= 0; i_part--) {
+    part = coord[i_part];
+    if (!allParticles && (part[6] < offset->startPID || part[6] > offset->endPID))
+      continue;
+    if (offset->dz)
+      ds = offset->dz * sqrt(1 + sqr(part[1]) + sqr(part[3]));
+    else
+      ds = 0;
+    part[0] += offset->dx + offset->dz * part[1];
+    part[1] += offset->dxp;
+    part[2] += offset->dy + offset->dz * part[3];
+    part[3] += offset->dyp;
+    part[4] += ds;
+    if (offset->dt || offset->dp || offset->de) {
+      pc = P_central * (1 + part[5]);
+      beta = pc / (gamma = sqrt(1 + pc * pc));
+      t = part[4] / (beta * c_mks) + offset->dt;
+      if (offset->dp) {
+        part[5] += offset->dp;
+        pc = P_central * (1 + part[5]);
+        beta = pc / sqrt(1 + pc * pc);
+      }
+      if (offset->de) {
+        gamma += offset->de * gamma;
+        pc = sqrt(gamma * gamma - 1);
+        beta = pc / gamma;
+        part[5] = (pc - P_central) / P_central;
+      }
+      part[4] = t * beta * c_mks;
+    }
+  }
+}
 
 static long lookup_type(const char *name) {
   long i;
@@ -295,6 +334,11 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
           }
           break;
         case T_MARK:
+          break;
+        case T_MALIGN:
+          /* do_tracking.c:1818-1821 */
+          if (((MALIGN *)eptr->p_elem)->on_pass == -1 || ((MALIGN *)eptr->p_elem)->on_pass == i_pass)
+            b2e_ref_offset_beam(coord, nToTrack, (MALIGN *)eptr->p_elem, P_central);
           break;
         case T_MAXAMP:
           maxamp = (MAXAMP *)eptr->p_elem;
