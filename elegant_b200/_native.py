@@ -45,7 +45,8 @@ class RunOptions(ctypes.Structure):
                 ("coord_limit", ctypes.c_double), ("slope_limit", ctypes.c_double),
                 ("passes_per_launch", ctypes.c_int32), ("ring_variant", ctypes.c_int32),
                 ("record_history", ctypes.c_int32), ("compact_every", ctypes.c_int32),
-                ("sr_gaussian_limit", ctypes.c_double), ("isr_seed", ctypes.c_uint64)]
+                ("sr_gaussian_limit", ctypes.c_double), ("isr_seed", ctypes.c_uint64),
+                ("record_tbt", ctypes.c_int32), ("fiducial_particles", ctypes.c_int32)]
 
 
 class Override(ctypes.Structure):
@@ -100,6 +101,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_set_csr_surrogate": (c_int, [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
         "b2e_csr_surrogate_stats": (c_int, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp, i64,
                                             ctypes.POINTER(i64)]),
+        "b2e_tbt": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
+        "b2e_tbt_tunes": (c_int, [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, vp]),
+        "b2e_naff": (c_int, [vp, i64, ctypes.c_int32, vp, vp, vp, vp]),
+        "b2e_element_defaults": (c_int, [ctypes.c_int32, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

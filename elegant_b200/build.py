@@ -20,7 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libelegant_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-SOURCES = ["b2e_ring.cu", "b2e_csr.cu", "b2e_lattice.cu", "b2e_capi.cu", "b2e_tmap.cu", "b2e_wakenet.cu"]
+SOURCES = ["b2e_ring.cu", "b2e_csr.cu", "b2e_lattice.cu", "b2e_capi.cu", "b2e_tmap.cu", "b2e_wakenet.cu",
+           "b2e_naff.cu"]
 HEADERS = ["b2e_engine.h", "b2e_elements.cuh", "b2e_math.h", "b2e_kernels.h", "b2e_lattice.h",
            "b2e_csr.h", "b2e_sg.h", "b2e_umma.cuh", "b2e_tmap.h"]
 

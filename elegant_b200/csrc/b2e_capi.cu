@@ -103,6 +103,11 @@ struct b2e_ctx {
   DevBuf<double> d_hist_out;       /* [n_inst][passes of the call][5] */
   std::vector<double> history;     /* [pass][inst][5]: survivors, <x>, <y>, ex, ey */
   int hist_pass0 = 0, hist_passes = 0;
+  DevBuf<double> d_tbt;      /* [tbt_records][4][n] */
+  int tbt_records = 0;
+  int64_t tbt_rows = 0;
+  DevBuf<double> d_naff;     /* [4][3][n] NAFF results, then [4][n] tunes */
+  DevBuf<int> d_naff_bad;
   /* lost-particle compaction: second set of particle buffers, survivors per instance */
   DevBuf<double> d_cmp_cols[6];
   DevBuf<int64_t> d_cmp_ids;
@@ -158,6 +163,9 @@ extern "C" int b2e_destroy(b2e_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   ctx->d_elems.release();
   ctx->d_rads.release();
+  ctx->d_tbt.release();
+  ctx->d_naff.release();
+  ctx->d_naff_bad.release();
   ctx->d_aps.release();
   ctx->d_rf.release();
   ctx->d_tiles.release();
@@ -523,6 +531,10 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.hist_passes = ctx->hist_passes;
   L.rad = ctx->radiates;
   L.rads = ctx->d_rads.ptr;
+  L.tbt = ctx->opt.record_tbt && !ctx->use_ext && ctx->tbt_records > 0 ? ctx->d_tbt.ptr : nullptr;
+  L.tbt_pass0 = ctx->pass_counter;
+  L.tbt_records = ctx->tbt_records;
+  L.tbt_rows = ctx->n;
   L.ids = ctx->use_ext ? nullptr : ctx->d_ids.ptr;
   L.isr_seed = ctx->opt.isr_seed;
   L.sr_limit = ctx->opt.sr_gaussian_limit == 0 ? 3.0 : ctx->opt.sr_gaussian_limit;
@@ -597,6 +609,19 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
   const bool record = ctx->opt.record_history && !ctx->use_ext && ctx->opt.n_passes > 0;
   if (p0 == 0)
     ctx->history.clear();
+  ctx->tbt_records = 0;
+  if (ctx->opt.record_tbt && !ctx->use_ext) {
+    if (!ctx->lat.csr_elements.empty())
+      return fail(ctx, B2E_ERR_LATTICE, "turn-by-turn recording is not available with CSR elements");
+    if (ctx->opt.compact_every > 0)
+      return fail(ctx, B2E_ERR_ARG, "turn-by-turn recording keeps rows in place: no compact_every");
+    ctx->tbt_records = ctx->opt.n_passes + 1;
+    ctx->tbt_rows = ctx->n;
+    CUDA_TRY(ctx, ctx->d_tbt.ensure(std::max<size_t>((size_t)ctx->tbt_records * 4 * ctx->n, 1)));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_tbt.ptr, 0xff, sizeof(double) * (size_t)ctx->tbt_records * 4 * ctx->n,
+                                  ctx->stream)); /* NaN until written */
+    CUDA_TRY(ctx, launch_tbt_start(particle_view(ctx), ctx->n, ctx->d_tbt.ptr, ctx->stream));
+  }
   if (record) {
     if (!ctx->lat.csr_elements.empty())
       return fail(ctx, B2E_ERR_LATTICE, "history recording is not available with CSR elements");
@@ -671,7 +696,8 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     if (stop_kind == 1) {
       ctx->launches++;
       CUDA_TRY(ctx, launch_fiducial(particle_view(ctx), ctx->d_inst_offsets.ptr, ctx->n_inst, ctx->d_elems.ptr, ne,
-                                    stop_e, ctx->d_rf.ptr, ctx->lat.n_rf, ctx->opt.p_central, ctx->stream));
+                                    stop_e, ctx->d_rf.ptr, ctx->lat.n_rf, ctx->opt.p_central,
+                                    ctx->opt.fiducial_particles, ctx->stream));
       next_rf++;
       /* the RFCA itself is tracked by the next ring launch */
       int rc = run_ring_range(ctx, p, stop_e, p, stop_e + 1);
@@ -855,6 +881,66 @@ extern "C" int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx
 
 extern "C" int64_t b2e_history_passes(const b2e_ctx *ctx) {
   return ctx && ctx->n_inst > 0 ? (int64_t)(ctx->history.size() / ((size_t)ctx->n_inst * 5)) : -1;
+}
+
+extern "C" int b2e_tbt(b2e_ctx *ctx, double *host_out, int64_t capacity, int64_t *written) {
+  if (!ctx || !written || capacity < 0)
+    return B2E_ERR_ARG;
+  if (!ctx->opt.record_tbt || ctx->tbt_records <= 0)
+    return fail(ctx, B2E_ERR_STATE, "b2e_tbt: no turn-by-turn data (set record_tbt and track)");
+  const int64_t total = (int64_t)ctx->tbt_records * 4 * ctx->tbt_rows;
+  *written = total;
+  if (!host_out)
+    return B2E_OK;
+  if (capacity < total)
+    return fail(ctx, B2E_ERR_ARG, "b2e_tbt: %lld values needed, capacity %lld", (long long)total,
+                (long long)capacity);
+  CUDA_TRY(ctx, cudaMemcpyAsync(host_out, ctx->d_tbt.ptr, sizeof(double) * total, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return B2E_OK;
+}
+
+extern "C" int b2e_tbt_tunes(b2e_ctx *ctx, int32_t first_record, int32_t n_records, double *nux, double *nuy,
+                             double *ax, double *ay) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  if (!ctx->opt.record_tbt || ctx->tbt_records <= 0)
+    return fail(ctx, B2E_ERR_STATE, "b2e_tbt_tunes: no turn-by-turn data (set record_tbt and track)");
+  if (first_record < 0 || n_records < 4 || n_records > 8192 || first_record + n_records > ctx->tbt_records)
+    return fail(ctx, B2E_ERR_ARG, "b2e_tbt_tunes: window [%d, %d) outside 4..8192 records of the %d recorded",
+                first_record, first_record + n_records, ctx->tbt_records);
+  const int64_t rows = ctx->tbt_rows;
+  if (rows == 0)
+    return B2E_OK;
+  cudaSetDevice(ctx->device);
+  CUDA_TRY(ctx, ctx->d_naff.ensure((size_t)rows * 16));
+  CUDA_TRY(ctx, ctx->d_naff_bad.ensure((size_t)rows));
+  CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_naff_bad.ptr, 0, sizeof(int) * rows, ctx->stream));
+  double *scratch = ctx->d_naff.ptr, *nu = ctx->d_naff.ptr + (size_t)rows * 12;
+  CUDA_TRY(ctx, launch_tbt_tunes(ctx->d_tbt.ptr, rows, first_record, n_records, scratch, ctx->d_naff_bad.ptr, nu,
+                                 ctx->stream));
+  ctx->launches += 2;
+  double *outs[4] = {nux, nuy, ax, ay};
+  for (int k = 0; k < 4; k++)
+    if (outs[k])
+      CUDA_TRY(ctx, cudaMemcpyAsync(outs[k], nu + (size_t)k * rows, sizeof(double) * rows, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return B2E_OK;
+}
+
+extern "C" int b2e_naff(const double *dev_signals, int64_t n_signals, int32_t n_points, double *dev_frequency,
+                        double *dev_amplitude, double *dev_phase, void *stream) {
+  if (n_signals < 0 || n_points < 4 || n_points > 8192 || (n_signals > 0 && (!dev_signals || !dev_frequency ||
+                                                                             !dev_amplitude || !dev_phase)))
+    return B2E_ERR_ARG;
+  if (n_signals == 0)
+    return B2E_OK;
+  return launch_naff(dev_signals, n_signals, n_points, dev_frequency, dev_amplitude, dev_phase,
+                     (cudaStream_t)stream) == cudaSuccess
+             ? B2E_OK
+             : B2E_ERR_CUDA;
 }
 
 extern "C" int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written) {

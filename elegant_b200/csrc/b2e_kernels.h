@@ -32,6 +32,11 @@ struct RingLaunch {
   const int64_t *ids;
   uint64_t isr_seed;
   double sr_limit;
+  /* turn-by-turn record [records][4][tbt_rows]: after each full pass p,
+   * record p - tbt_pass0 + 1 < tbt_records gets x, x', y, y' of live rows */
+  double *tbt;
+  int tbt_pass0, tbt_records;
+  int64_t tbt_rows;
 };
 
 /* variant 1..B2E_RING_VARIANTS selects the occupancy target and the barrier
@@ -44,7 +49,17 @@ cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticle
                            const int64_t *offs, int n_inst, int *alive_out, cudaStream_t stream);
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
-                            cudaStream_t stream);
+                            int64_t max_rows, cudaStream_t stream);
+/* turn-by-turn record 0: x, x', y, y' of every row */
+cudaError_t launch_tbt_start(DevParticles P, int64_t n, double *tbt, cudaStream_t stream);
+/* NAFF (b2e_naff.cu): signals [n_signals][N] -> frequency, amplitude, phase */
+cudaError_t launch_naff(const double *sig, int64_t n_signals, int N, double *freq, double *amp, double *phase,
+                        cudaStream_t stream);
+/* tunes of records [first, first + N) of turn-by-turn data [records][4][rows]:
+ * scratch [4][3][rows], bad [rows] (zeroed by the caller), nu [4][rows] =
+ * nux, nuy, ax, ay */
+cudaError_t launch_tbt_tunes(const double *tbt, int64_t rows, int first, int N, double *scratch, int *bad,
+                             double *nu, cudaStream_t stream);
 cudaError_t launch_history_merge(const double *partials, int hist_passes, const int *tile_first, int n_inst,
                                  double *out, cudaStream_t stream);
 cudaError_t launch_effort(const int32_t *lost_pass, int64_t n, int pass_begin, int pass_end, unsigned long long *effort,

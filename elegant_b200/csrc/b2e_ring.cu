@@ -224,6 +224,16 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
         active = false;
       }
     }
+    if (L.tbt && active && e1 == L.n_elems) {
+      const int r = pass - L.tbt_pass0 + 1;
+      if (r >= 1 && r < L.tbt_records) {
+        double *o = L.tbt + (size_t)r * 4 * L.tbt_rows + ip;
+        o[0] = p.x;
+        o[L.tbt_rows] = p.xp;
+        o[2 * L.tbt_rows] = p.y;
+        o[3 * L.tbt_rows] = p.yp;
+      }
+    }
     if (HIST && e1 == L.n_elems && pass >= L.hist_pass0)
       tile_moments(p, active,
                    tidx < L.n_tiles ? L.hist + ((size_t)tidx * L.hist_passes + (pass - L.hist_pass0)) * 11 : nullptr);
@@ -308,7 +318,8 @@ cudaError_t launch_history_merge(const double *partials, int hist_passes, const 
  * upstream on that pass (elegant's swap-to-tail would otherwise reorder the
  * survivors). */
 __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
-                                   int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central) {
+                                   int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
+                                   int64_t max_rows) {
   const int inst = blockIdx.x * blockDim.x + threadIdx.x;
   if (inst >= n_inst)
     return;
@@ -318,7 +329,8 @@ __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, 
   DevRfState &rs = rf[(size_t)inst * n_rf + slot];
   double tsum = 0, error = 0;
   int64_t nsum = 0;
-  for (int64_t ip = inst_offsets[inst]; ip < inst_offsets[inst + 1]; ip++) {
+  const int64_t first = inst_offsets[inst], end = inst_offsets[inst + 1];
+  for (int64_t ip = first; ip < end && (max_rows <= 0 || ip - first < max_rows); ip++) {
     if (P.lost_pass[ip] >= 0)
       continue;
     double pp = p_central * (1 + P.dp[ip]);
@@ -522,10 +534,27 @@ cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticle
 
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
-                            cudaStream_t stream) {
+                            int64_t max_rows, cudaStream_t stream) {
   int tpb = 64, nb = (n_inst + tpb - 1) / tpb;
   rf_fiducial_kernel<<<nb, tpb, 0, stream>>>(P, inst_offsets, n_inst, elems, n_elems, elem_index, rf, n_rf,
-                                             p_central);
+                                             p_central, max_rows);
+  return cudaGetLastError();
+}
+
+__global__ void tbt_start_kernel(DevParticles P, int64_t n, double *tbt) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  const bool live = P.lost_pass[i] < 0;
+  tbt[i] = live ? P.x[i] : NAN;
+  tbt[n + i] = live ? P.xp[i] : NAN;
+  tbt[2 * n + i] = live ? P.y[i] : NAN;
+  tbt[3 * n + i] = live ? P.yp[i] : NAN;
+}
+
+cudaError_t launch_tbt_start(DevParticles P, int64_t n, double *tbt, cudaStream_t stream) {
+  if (n > 0)
+    tbt_start_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(P, n, tbt);
   return cudaGetLastError();
 }
 

@@ -39,7 +39,8 @@ class Tracker:
 
     def __init__(self, lattice: Lattice, p_central: float, n_passes: int, device: int = 0, default_order: int = 2,
                  passes_per_launch: int = 0, ring_variant: int = 0, record_history: bool = False,
-                 compact_every: int = 0, isr_seed: int = 0, sr_gaussian_limit: float = 3.0):
+                 compact_every: int = 0, isr_seed: int = 0, sr_gaussian_limit: float = 3.0,
+                 record_tbt: bool = False, fiducial_particles: int = 0):
         self.lib = nat.load_library()
         self.lattice = lattice
         self._ctx = ctypes.c_void_p()
@@ -50,7 +51,8 @@ class Tracker:
                                       coord_limit=10.0, slope_limit=1.0, passes_per_launch=passes_per_launch,
                                       ring_variant=ring_variant, record_history=int(record_history),
                                       compact_every=compact_every, sr_gaussian_limit=sr_gaussian_limit,
-                                      isr_seed=isr_seed)
+                                      isr_seed=isr_seed, record_tbt=int(record_tbt),
+                                      fiducial_particles=fiducial_particles)
         self._elems = lattice.to_ctypes()
         self._check(self.lib.b2e_load_lattice(self._ctx, self._elems, len(lattice), ctypes.byref(self.options)))
         self.n_instances = 1
@@ -191,6 +193,24 @@ class Tracker:
             out[k] = np.zeros(shape, dtype=np.float64)
         self._check(self.lib.b2e_ensemble_history(self._ctx, *(out[k].ctypes.data for k in
                                                                 ("survivors", "cx", "cy", "ex", "ey"))))
+        return out
+
+    def tbt(self) -> np.ndarray:
+        """Turn-by-turn x, x', y, y' of the last call with record_tbt:
+        array [records][4][n]; record 0 is the call's start."""
+        n = ctypes.c_int64()
+        self._check(self.lib.b2e_tbt(self._ctx, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, dtype=np.float64)
+        self._check(self.lib.b2e_tbt(self._ctx, out.ctypes.data, n.value, ctypes.byref(n)))
+        return out.reshape(-1, 4, self._n)
+
+    def tbt_tunes(self, first_record: int, n_records: int) -> dict:
+        """Tunes (NAFF + half-plane from the x/x' phases) of every row over
+        records [first_record, first_record + n_records); -1 where the
+        particle was lost before the window's end."""
+        out = {k: np.empty(self._n) for k in ("nux", "nuy", "ax", "ay")}
+        self._check(self.lib.b2e_tbt_tunes(self._ctx, first_record, n_records, *(out[k].ctypes.data for k in
+                                                                                 ("nux", "nuy", "ax", "ay"))))
         return out
 
     def set_csr_reducer(self, fn):

@@ -209,6 +209,12 @@ typedef struct {
   uint64_t isr_seed;        /* seed of the ISR deviates, which are addressed by (particle ID,
                                pass, element, slice, step): a run is reproducible and does not
                                depend on launch shape or compaction */
+  int32_t record_tbt;       /* nonzero: keep every particle's x, x', y, y' at the start of a
+                               call and after each of its passes (b2e_tbt, b2e_tbt_tunes).  Not
+                               with compact_every, CSR elements or device-owned columns. */
+  int32_t fiducial_particles; /* > 0: only the first this many rows of each instance set the
+                                 RF phase reference on pass 0 (elegant's separate fiducial
+                                 particle, e.g. frequencyMap.c:180-195); 0 = all particles */
 } b2e_run_options;
 
 typedef struct b2e_ctx b2e_ctx;
@@ -290,6 +296,35 @@ int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_t *offsets,
 int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx, double *cy, double *ex, double *ey);
 /* Passes recorded so far, or -1 for a null context. */
 int64_t b2e_history_passes(const b2e_ctx *ctx);
+
+/* ---- turn-by-turn data and tunes --------------------------------------- */
+/* Turn-by-turn coordinates of the last b2e_track / b2e_track_host call made
+ * with record_tbt: host array [records][4][n] (x, x', y, y'), record 0 the
+ * coordinates at the call's start, record j those after its j-th pass (rows
+ * in the uploaded order; a lost particle's records after its loss are NaN).
+ * *written = records * 4 * n; with host_out NULL only *written is set.
+ * Replaces the per-turn bookkeeping of computeTunesFromTracking
+ * (twiss.cc:3885-3925). */
+int b2e_tbt(b2e_ctx *ctx, double *host_out, int64_t capacity, int64_t *written);
+
+/* Tunes of every particle from records [first_record, first_record +
+ * n_records) of the turn-by-turn data, as computeTunesFromTracking does
+ * (twiss.cc:3942-4022): the strongest frequency of x, x', y and y' by NAFF
+ * (one frequency, Hann window, refined to 1e-12 of a turn by golden-section
+ * search; the toolkit's PerformNAFF is not in the reference tree, so the
+ * method is this library's), then adjustTuneHalfPlane (twiss.cc:4036-4046)
+ * from the phases of x and x' (y and y').  Host arrays of n values; a
+ * particle lost before the window's last record gets -1 in nux/nuy.  Runs
+ * on the device; needs 4 <= n_records <= 8192. */
+int b2e_tbt_tunes(b2e_ctx *ctx, int32_t first_record, int32_t n_records, double *nux, double *nuy, double *ax,
+                  double *ay);
+
+/* NAFF of n_signals device-resident signals of n_points each (signal s at
+ * dev_signals + s * n_points), the strongest frequency in [0, 0.5] cycles per
+ * sample with its amplitude and phase, written to device arrays of
+ * n_signals values; the same method as b2e_tbt_tunes. */
+int b2e_naff(const double *dev_signals, int64_t n_signals, int32_t n_points, double *dev_frequency,
+             double *dev_amplitude, double *dev_phase, void *stream);
 
 /* ---- CSR (CSRCSBEND / CSRDRIFT) ---------------------------------------- */
 /* Wake arrays of every CSR kick of the last b2e_track call: for each
