@@ -757,13 +757,13 @@ __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, Cs
     XP = XP + (c[CB_TAN_E2] / rho) * X;
     YP = YP - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + DP)) / rho) * Y;
   }
-  x = (X * ct - Y * sn) + c[CB_ET0 + 0];
-  y = (X * sn + Y * ct) + c[CB_ET0 + 2];
-  xp = (XP * ct - YP * sn) + c[CB_ET0 + 1];
-  yp = (XP * sn + YP * ct) + c[CB_ET0 + 3];
+  x = (X * ct - Y * sn) + 0.0;
+  y = (X * sn + Y * ct) + 0.0;
+  xp = (XP * ct - YP * sn) + 0.0;
+  yp = (XP * sn + YP * ct) + 0.0;
   x = x + (c[CB_DXF] + c[CB_DZF] * xp);
   y = y + (c[CB_DYF] + c[CB_DZF] * yp);
-  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + c[CB_ET0 + 4]);
+  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + 0.0);
   P.x[i] = x;
   P.xp[i] = xp;
   P.y[i] = y;

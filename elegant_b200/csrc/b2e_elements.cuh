@@ -131,6 +131,22 @@ __device__ __forceinline__ void rotate_misalign(Part &p, double ca, double sa) {
   p.yp = -xp * sa + yp * ca;
 }
 
+/* a/b correctly rounded from y = RN(1/b) computed once (Markstein, "Computation
+ * of elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+ * Dev. 34, 1990: with y within half an ulp of 1/b and q = RN(a y) within one
+ * ulp of a/b, the remainder r = a - b q is exact under FMA and RN(q + r y) is
+ * RN(a/b)).  An exact quotient (r = 0, signed zeros included) and a
+ * non-finite q are returned as they are.  For divisors fixed per element, away
+ * from overflow and the subnormal range; checked against division on the
+ * device by b2e_selftest_division. */
+__device__ __forceinline__ double div_rn_recip(double a, double b, double y) {
+  const double q = a * y;
+  const double r = fma(-q, b, a);
+  if (r == 0 || !isfinite(q))
+    return q;
+  return fma(r, y, q);
+}
+
 /* ---- KQUAD / KSEXT: multipole_tracking2 (multipole.c:693-1117) with
  * integrate_kick_multipole_ordn (multipole.c:1122-1410).  The reference
  * always runs its radiation bookkeeping block (isr_coef is negated, not
@@ -330,7 +346,7 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
     if (!mult_aperture_ok(X, Y, ap, e))
       return LOSS_APERTURE;
     for (j = 0; j < nSub; j++) {
-      const double dsh = c[CB_DSH0 + j];
+      const double dsh_rho0 = c[CB_DSH0 + j];
       double f, sin_phi, phi, sine, cosi, tang, cos_phi, factor, arg;
       f = (1 + DPoP) * (1 + DPoP) - QY * QY;
       if (f <= 0)
@@ -340,7 +356,7 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
         return LOSS_SLOPE;
       sin_phi = QX / f;
       phi = b2e_asin(sin_phi);
-      arg = dsh / rho0 + phi;
+      arg = dsh_rho0 + phi;
       b2e_sincos(arg, &sine, &cosi);
       if (cosi == 0)
         return LOSS_SLOPE;
@@ -357,13 +373,14 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
       {
         const double ds = c[CB_DS0 + j];
         /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
-        QX = QX + ((((-ds) * (1 + X / rho0)) * 1.0) / rho_actual);
+        const double x_rho0 = div_rn_recip(X, rho0, c[CB_INV_RHO0]);
+        QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * 1.0), rho_actual, c[CB_INV_RHO_ACTUAL]);
         {
           /* (t * Fx) / rho_actual with Fx = 0 is a signed zero (NaN for a
            * non-finite t): the sign of t * 0.0 flipped by rho_actual's, which
            * is finite and nonzero in a bend -- the same value without the
            * division */
-          const double z = ((ds) * (1 + X / rho0)) * 0.0;
+          const double z = ((ds) * (1 + x_rho0)) * 0.0;
           QY = QY + (rho_actual < 0 ? -z : z);
         }
         if (RAD && (e.flags & (EF_SR | EF_ISR))) {
@@ -489,11 +506,11 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   }
 
   /* back to the lab frame (csbend.c:1379-1388) */
-  p.x = (x * ct - y * st) + c[CB_ET0 + 0];
-  p.y = (x * st + y * ct) + c[CB_ET0 + 2];
-  p.xp = (xp * ct - yp * st) + c[CB_ET0 + 1];
-  p.yp = (xp * st + yp * ct) + c[CB_ET0 + 3];
-  p.s = s + c[CB_ET0 + 4];
+  p.x = (x * ct - y * st) + 0.0;
+  p.y = (x * st + y * ct) + 0.0;
+  p.xp = (xp * ct - yp * st) + 0.0;
+  p.yp = (xp * st + yp * ct) + 0.0;
+  p.s = s + 0.0;
   p.dp = dp;
   p.x = p.x + (c[CB_DXF] + c[CB_DZF] * p.xp);
   p.y = p.y + (c[CB_DYF] + c[CB_DZF] * p.yp);

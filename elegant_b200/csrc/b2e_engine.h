@@ -74,7 +74,7 @@ enum {
 #define CB_RHO_ACTUAL 1
 #define CB_NSLICES 2
 #define CB_NSUB 3
-#define CB_DSH0 4       /* s*driftFrac[j], 4..11 */
+#define CB_DSH0 4       /* (s*driftFrac[j])/rho0, 4..11: the drift angle of substep j */
 #define CB_DS0 12       /* s*kickFrac[j], 12..19 (0 terminates) */
 #define CB_TAN_E1 20
 #define CB_E1 21
@@ -90,7 +90,8 @@ enum {
 #define CB_DXF 31
 #define CB_DYF 32
 #define CB_DZF 33
-#define CB_ET0 34       /* dcoord_etilt[0..4] -> 34..38 */
+#define CB_INV_RHO0 34  /* RN(1/rho0), for X/rho0 by div_rn_recip */
+#define CB_INV_RHO_ACTUAL 35 /* RN(1/rho_actual) */
 
 
 /* Radiation constants of a KMULT / CSBEND, in a table beside the element

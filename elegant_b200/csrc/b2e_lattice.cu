@@ -347,7 +347,9 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
   if (el.type == B2E_CSRCSBEND)
     s = (length / nSlices) / 1; /* track_through_csbendCSR integrates one slice of length/nSlices per kick */
   for (int j = 0; j < 8; j++) {
-    d.c[CB_DSH0 + j] = j < nSub ? s * drift_frac[j] : 0;
+    /* the integrator uses the drift only as dsh/rho0 (csbend.c:1566): the
+     * same two roundings, done once */
+    d.c[CB_DSH0 + j] = j < nSub ? (s * drift_frac[j]) / rho0 : 0;
     d.c[CB_DS0 + j] = j < nSub ? s * kick_frac[j] : 0;
   }
   d.c[CB_TAN_E1] = b2e_tan(e1);
@@ -365,8 +367,9 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
   d.c[CB_DXF] = p[B2E_BEND_DX] * b2e_cos(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * b2e_sin(p[B2E_BEND_ANGLE]);
   d.c[CB_DZF] = p[B2E_BEND_DX] * b2e_sin(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * b2e_cos(p[B2E_BEND_ANGLE]);
   d.c[CB_DYF] = p[B2E_BEND_DY];
-  for (int j = 0; j < 5; j++)
-    d.c[CB_ET0 + j] = 0; /* computeEtiltCentroidOffset with etilt = 0 */
+  /* dcoord_etilt (computeEtiltCentroidOffset) is zero: ETILT is rejected above */
+  d.c[CB_INV_RHO0] = 1 / rho0;
+  d.c[CB_INV_RHO_ACTUAL] = 1 / rho_actual;
   if (edge1)
     d.flags |= EF_EDGE1;
   if (edge2)

@@ -570,3 +570,58 @@ cudaError_t launch_effort(const int32_t *lost_pass, int64_t n, int pass_begin, i
 }
 
 } // namespace b2e
+
+/* ---- division self-test (b2e_selftest_division) ------------------------- */
+namespace b2e {
+
+__global__ void division_selftest_kernel(const double *b, int nb, int64_t samples, uint64_t seed,
+                                         unsigned long long *mismatches) {
+  const int ib = blockIdx.y;
+  const double bv = b[ib], y = 1 / bv;
+  unsigned long long bad = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < samples; k += (int64_t)gridDim.x * blockDim.x) {
+    /* SplitMix64 of (seed, divisor, sample) -> sign, exponent, mantissa */
+    uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(k * nb + ib + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    const int ex = (int)((z >> 52) % 81) - 40;
+    const double m = 1.0 + (double)(z & ((1ull << 52) - 1)) * 0x1p-52;
+    const double a = ldexp((z >> 63) ? -m : m, ex);
+    const double q1 = a / bv, q2 = div_rn_recip(a, bv, y);
+    bad += __double_as_longlong(q1) != __double_as_longlong(q2);
+  }
+  for (int off = 16; off > 0; off >>= 1)
+    bad += __shfl_down_sync(0xffffffffu, bad, off);
+  if ((threadIdx.x & 31) == 0 && bad)
+    atomicAdd(mismatches, bad);
+}
+
+} // namespace b2e
+
+extern "C" int b2e_selftest_division(const double *host_b, int32_t n_b, int64_t samples, uint64_t seed,
+                                     int64_t *mismatches) {
+  using namespace b2e;
+  if (!host_b || n_b < 1 || n_b > 65535 || samples < 1 || !mismatches)
+    return B2E_ERR_ARG;
+  double *db = nullptr;
+  unsigned long long *dm = nullptr, hm = 0;
+  if (cudaMalloc(&db, sizeof(double) * n_b) != cudaSuccess)
+    return B2E_ERR_NOMEM;
+  if (cudaMalloc(&dm, sizeof(unsigned long long)) != cudaSuccess) {
+    cudaFree(db);
+    return B2E_ERR_NOMEM;
+  }
+  cudaMemcpy(db, host_b, sizeof(double) * n_b, cudaMemcpyHostToDevice);
+  cudaMemset(dm, 0, sizeof(unsigned long long));
+  division_selftest_kernel<<<dim3(148 * 4, n_b), 256>>>(db, n_b, samples, seed, dm);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&hm, dm, sizeof(hm), cudaMemcpyDeviceToHost);
+  cudaFree(db);
+  cudaFree(dm);
+  if (e != cudaSuccess)
+    return B2E_ERR_CUDA;
+  *mismatches = (int64_t)hm;
+  return B2E_OK;
+}

@@ -425,6 +425,14 @@ int b2e_csr_surrogate_stats(b2e_ctx *ctx, int64_t *evaluations, int64_t *fallbac
  * A, B: BF16 row-major; D: FP32.  No counterpart in the reference. */
 int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b, float *dev_d, void *stream);
 
+/* ---- division self-test -------------------------------------------------
+ * Compares, on the device, a / b with the engine's division by a stored
+ * reciprocal (Markstein's correction step) for every divisor in host_b and
+ * `samples` numerators each, drawn with magnitudes 2^-40..2^40 and both signs
+ * from `seed`; *mismatches = the pairs whose bits differ.  No counterpart in
+ * the reference. */
+int b2e_selftest_division(const double *host_b, int32_t n_b, int64_t samples, uint64_t seed, int64_t *mismatches);
+
 /* ---- allocation-free CSR dipole ---------------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory when they track (a program whose memory pool owns
