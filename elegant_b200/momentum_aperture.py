@@ -98,8 +98,9 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
                       soft_failure=False, device=0, compact_every=0, track_trials=None):
     """Returns one dict per selected element: name, type, s (its end),
     index, and per side ('negative', 'positive'): delta (last survivor),
-    found (a loss was found), lost_on_pass, x_lost, y_lost, delta_lost
-    (the first lost trial's offset).  Also returns the number of
+    found (a loss was found), lost_on_pass, x_lost, y_lost, s_lost (end of
+    the element of the loss), delta_when_lost (the particle's delta there),
+    delta_lost (the first lost trial's offset).  Also returns the number of
     particle-turns tracked.  track_trials(lattice, offsets, overrides, beam,
     p_central, n_passes) -> (lost_pass, coords at the end or at loss, effort),
     rows in beam order, replaces the engine (used to check the batching
@@ -115,6 +116,7 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
     fire = 0 if n_passes == 1 else 1
     wl, wedges = wedge_lattice(lattice, locs, fire)
     z_end = np.cumsum([e.length for e in lattice.elements])
+    wl_end = np.cumsum([e.length for e in wl.elements])
     limits = (delta_negative_limit, delta_positive_limit)
     starts = (delta_negative_start, delta_positive_start)
     # per (location, side) scan state, as in the reference's loop variables
@@ -125,7 +127,7 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
             st.append({"k": k, "side": side, "sign": sign, "start": starts[side], "interval": delta_step_size * sign,
                        "limit": limits[side], "lost": sign * 1.7976931348623157e308 / 2, "survived": 0.0,
                        "survivor": False, "loser": False, "lost_on_pass": -1, "x_lost": 0.0, "y_lost": 0.0,
-                       "delta_lost_at": 0.0, "active": True})
+                       "s_lost": 0.0, "delta_lost_at": 0.0, "active": True})
     effort = 0.0
     for split in range(splits + 1):
         trials = []  # (scan index, delta)
@@ -133,8 +135,9 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
             if s["active"]:
                 trials += [(j, d) for d in scan_deltas(s["start"], s["interval"], s["limit"])]
         if trials:
-            lost_pass, x_l, y_l, dpl, eff = _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial,
-                                                          y_initial, device, compact_every, track_trials)
+            lost_pass, x_l, y_l, dpl, lost_elem, eff = _track_trials(wl, wedges, st, trials, p_central, n_passes,
+                                                                     x_initial, y_initial, device, compact_every,
+                                                                     track_trials)
             effort += eff
             done = set()
             for t, (j, d) in enumerate(trials):
@@ -143,7 +146,8 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
                 s = st[j]
                 if lost_pass[t] >= 0:
                     s.update(lost_on_pass=int(lost_pass[t]), x_lost=float(x_l[t]), y_lost=float(y_l[t]),
-                             delta_lost_at=float(dpl[t]), loser=True)
+                             delta_lost_at=float(dpl[t]), loser=True,
+                             s_lost=float(wl_end[lost_elem[t]]) if lost_elem[t] >= 0 else 0.0)
                     s["lost"] = d
                     done.add(j)
                 else:
@@ -177,8 +181,9 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
         for side, label in ((0, "negative"), (1, "positive")):
             s = st[2 * k + side]
             row[label] = {"delta": s["survived"], "found": s["loser"], "lost_on_pass": s["lost_on_pass"],
-                          "x_lost": s["x_lost"], "y_lost": s["y_lost"], "delta_lost": s["lost"]
-                          if s["loser"] and abs(s["lost"]) < 1e300 else None}
+                          "x_lost": s["x_lost"], "y_lost": s["y_lost"], "s_lost": s["s_lost"],
+                          "delta_when_lost": s["delta_lost_at"],
+                          "delta_lost": s["lost"] if s["loser"] and abs(s["lost"]) < 1e300 else None}
         out.append(row)
     return out, effort
 
@@ -202,10 +207,10 @@ def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_init
     beam = Beam(coords, ids)
     if track_trials is not None:
         lost_pass, c, effort = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
-        return lost_pass, c[:, 0], c[:, 2], c[:, 5], effort
+        return lost_pass, c[:, 0], c[:, 2], c[:, 5], np.full(n, -1), effort
     with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every) as t:
         t.load_ensemble(offsets, overrides)
         res = t.track(beam)
     order = np.argsort(res.ids)
     c = res.coords[order]
-    return res.lost_pass[order], c[:, 0], c[:, 2], c[:, 5], res.effort
+    return res.lost_pass[order], c[:, 0], c[:, 2], c[:, 5], res.lost_element[order], res.effort

@@ -6,7 +6,10 @@ post-processing tools (sddsplot, sddsanalyzebeam, ...).
   t = s / (c beta), p = P0 (1 + delta), particleID; parameters Step,
   pCentral, Charge, Particles, IDSlotsPerBunch (sdds_support.c:150-170).
 - `write_losses`: the `losses` file (sdds_support.c:199-212): x, xp, y, yp, s,
-  p, particleID, Pass.  s is the end position of the element where the
+  p, particleID, Pass.
+- `write_momentum_aperture`, `write_frequency_map`, `write_aperture`: the
+  outputs of &momentum_aperture (output_mode 0), &frequency_map and the
+  line modes of &find_aperture, in their column layouts.  s is the end position of the element where the
   particle was lost (elegant additionally extrapolates aperture losses into
   the preceding drift); the coordinates are those at the loss.
 
@@ -22,7 +25,8 @@ import struct
 import numpy as np
 
 C_MKS = 2.99792458e8
-_FMT = {"double": ("d", np.float64), "long": ("i", np.int32), "string": (None, None)}
+# SDDS type -> (struct code, numpy dtype); strings are (int32 length, bytes)
+_FMT = {"double": ("d", np.float64), "long": ("i", np.int32), "short": ("h", np.int16), "string": (None, None)}
 
 
 def _quote(v: str) -> str:
@@ -30,15 +34,18 @@ def _quote(v: str) -> str:
 
 
 def write_sdds(path, parameters, columns, mode="binary", description=None):
-    """parameters: [(name, type, value, attrs)], columns: [(name, type, array,
-    attrs)], types 'double' | 'long' | 'string'; attrs: dict of units,
-    symbol, description."""
+    """parameters: [(name, type, value, attrs)], columns: [(name, type,
+    values, attrs)], types 'double' | 'long' | 'short' | 'string'; attrs:
+    dict of units, symbol, description.  Binary data are written row by row
+    (SDDS's row-major layout), so string columns work too."""
     if mode not in ("binary", "ascii"):
         raise ValueError("mode must be 'binary' or 'ascii'")
     n = len(columns[0][2]) if columns else 0
     for c in columns:
         if len(c[2]) != n:
             raise ValueError("columns of different lengths")
+        if c[1] not in _FMT:
+            raise ValueError(f"unsupported SDDS type {c[1]}")
     lines = ["SDDS1"]
     if mode == "binary":
         lines.append("!# little-endian")
@@ -58,32 +65,66 @@ def write_sdds(path, parameters, columns, mode="binary", description=None):
         if mode == "binary":
             fh.write(struct.pack("<i", n))
             for _, typ, v, _ in parameters:
-                if typ == "string":
-                    b = str(v).encode()
-                    fh.write(struct.pack("<i", len(b)) + b)
-                else:
-                    fh.write(struct.pack("<" + _FMT[typ][0], v))
-            if n:
-                rec = np.dtype([(c[0], "<" + ("f8" if c[1] == "double" else "i4")) for c in columns])
+                fh.write(_pack(typ, v))
+            if n and all(c[1] != "string" for c in columns):
+                rec = np.dtype([(c[0], "<" + np.dtype(_FMT[c[1]][1]).str[1:]) for c in columns])
                 rows = np.empty(n, dtype=rec)
                 for c in columns:
                     rows[c[0]] = c[2]
                 fh.write(rows.tobytes())
+            else:
+                for i in range(n):
+                    fh.write(b"".join(_pack(c[1], c[2][i]) for c in columns))
         else:
             out = []
             for _, typ, v, _ in parameters:
-                out.append(_quote(str(v)) if typ == "string" else repr(float(v)) if typ == "double" else str(int(v)))
+                out.append(_text(typ, v))
             out.append(f"\t{n}")
-            cols = [np.asarray(c[2]) for c in columns]
             for i in range(n):
-                out.append(" ".join(repr(float(c[i])) if col[1] == "double" else str(int(c[i]))
-                                    for c, col in zip(cols, columns)))
+                out.append(" ".join(_text(c[1], c[2][i]) for c in columns))
             fh.write(("\n".join(out) + "\n").encode())
 
 
+def _pack(typ, v):
+    if typ == "string":
+        b = str(v).encode()
+        return struct.pack("<i", len(b)) + b
+    return struct.pack("<" + _FMT[typ][0], float(v) if typ == "double" else int(v))
+
+
+def _text(typ, v):
+    if typ == "string":
+        return _quote(str(v))
+    return repr(float(v)) if typ == "double" else str(int(v))
+
+
+def _split_ascii(line):
+    """Tokens of an ASCII data line, double-quoted strings kept whole."""
+    out, i = [], 0
+    while i < len(line):
+        if line[i].isspace():
+            i += 1
+        elif line[i] == '"':
+            j, buf = i + 1, []
+            while j < len(line) and line[j] != '"':
+                if line[j] == "\\" and j + 1 < len(line):
+                    j += 1
+                buf.append(line[j])
+                j += 1
+            out.append("".join(buf))
+            i = j + 1
+        else:
+            j = i
+            while j < len(line) and not line[j].isspace():
+                j += 1
+            out.append(line[i:j])
+            i = j
+    return out
+
+
 def read_sdds(path):
-    """(parameters dict, columns dict of arrays) of a single-page file written
-    by write_sdds."""
+    """(parameters dict, columns dict) of a single-page file written by
+    write_sdds (numeric columns as arrays, string columns as lists)."""
     with open(path, "rb") as fh:
         data = fh.read()
     pos, params, cols, mode = 0, [], [], None
@@ -98,32 +139,39 @@ def read_sdds(path):
         elif line.startswith("&data"):
             mode = "binary" if "binary" in line else "ascii"
             break
+
+    def conv(typ, v):
+        return v if typ == "string" else (float(v) if typ == "double" else int(v))
+
     if mode == "binary":
         n = struct.unpack_from("<i", data, pos)[0]
         pos += 4
-        pv = {}
-        for name, typ in params:
+
+        def take(typ):
+            nonlocal pos
             if typ == "string":
                 k = struct.unpack_from("<i", data, pos)[0]
-                pv[name] = data[pos + 4:pos + 4 + k].decode()
+                v = data[pos + 4:pos + 4 + k].decode()
                 pos += 4 + k
-            else:
-                f = _FMT[typ][0]
-                pv[name] = struct.unpack_from("<" + f, data, pos)[0]
-                pos += struct.calcsize(f)
-        rec = np.dtype([(c[0], "<" + ("f8" if c[1] == "double" else "i4")) for c in cols])
-        rows = np.frombuffer(data, dtype=rec, count=n, offset=pos)
-        return pv, {c[0]: np.array(rows[c[0]]) for c in cols}
-    toks = data[pos:].decode().split("\n")
-    pv = {}
-    for (name, typ), t in zip(params, toks):
-        pv[name] = t.strip().strip('"') if typ == "string" else (float(t) if typ == "double" else int(t))
-    n = int(toks[len(params)])
-    body = [t.split() for t in toks[len(params) + 1:len(params) + 1 + n]]
+                return v
+            f = _FMT[typ][0]
+            v = struct.unpack_from("<" + f, data, pos)[0]
+            pos += struct.calcsize(f)
+            return v
+        pv = {name: take(typ) for name, typ in params}
+        rows = [[take(typ) for _, typ in cols] for _ in range(n)]
+    else:
+        toks = data[pos:].decode().split("\n")
+        pv = {}
+        for (name, typ), t in zip(params, toks):
+            pv[name] = conv(typ, t.strip().strip('"'))
+        n = int(toks[len(params)])
+        rows = [[conv(typ, v) for (_, typ), v in zip(cols, _split_ascii(t))]
+                for t in toks[len(params) + 1:len(params) + 1 + n]]
     out = {}
     for j, (name, typ) in enumerate(cols):
-        out[name] = np.array([float(r[j]) if typ == "double" else int(r[j]) for r in body],
-                             dtype=np.float64 if typ == "double" else np.int32)
+        vals = [r[j] for r in rows]
+        out[name] = vals if typ == "string" else np.array(vals, dtype=_FMT[typ][1])
     return pv, out
 
 
@@ -159,3 +207,65 @@ def write_losses(path, result, lattice, p_central, step=1, mode="binary"):
             ("particleID", "long", result.ids[lost].astype(np.int64), {}),
             ("Pass", "long", result.lost_pass[lost].astype(np.int64), {})]
     write_sdds(path, params, cols, mode, description="elegant_b200 loss output")
+
+
+def write_momentum_aperture(path, rows, step=1, mode="binary"):
+    """elegant's &momentum_aperture output, output_mode 0
+    (momentumAperture.c:189-212, :700-740), from
+    elegant_b200.momentum_aperture rows.  nuxLost/nuyLost are -1: tunes are
+    only found with forbid_resonance_crossing, which is not built."""
+    n = len(rows)
+    cols = [("ElementName", "string", [r["name"] for r in rows], {}),
+            ("s", "double", [r["s"] for r in rows], {"units": "m"}),
+            ("ElementType", "string", [r["type"] for r in rows], {}),
+            ("ElementOccurence", "long", _occurrences(rows), {})]
+    for label, side in (("Positive", "positive"), ("Negative", "negative")):
+        cols += [(f"delta{label}Found", "short", [int(r[side]["found"]) for r in rows], {}),
+                 (f"delta{label}", "double", [r[side]["delta"] for r in rows],
+                  {"symbol": "$gd$R$b" + side[:3] + "$n"}),
+                 (f"lostOnPass{label}", "long", [r[side]["lost_on_pass"] for r in rows], {}),
+                 (f"sLost{label}", "double", [r[side]["s_lost"] for r in rows], {"units": "m"}),
+                 (f"xLost{label}", "double", [r[side]["x_lost"] for r in rows], {"units": "m"}),
+                 (f"yLost{label}", "double", [r[side]["y_lost"] for r in rows], {"units": "m"}),
+                 (f"deltaLost{label}", "double", [r[side]["delta_when_lost"] for r in rows], {}),
+                 (f"nuxLost{label}", "double", [-1.0] * n, {}),
+                 (f"nuyLost{label}", "double", [-1.0] * n, {})]
+    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search")
+
+
+def _occurrences(rows):
+    seen, out = {}, []
+    for r in rows:
+        seen[r["name"]] = seen.get(r["name"], 0) + 1
+        out.append(seen[r["name"]])
+    return out
+
+
+def write_frequency_map(path, rows, step=1, include_changes=False, mode="binary"):
+    """elegant's &frequency_map output (frequencyMap.c:30-60) from
+    elegant_b200.frequency_map rows."""
+    names = ["x", "y", "delta", "nux", "nuy", "s"]
+    if include_changes:
+        names += ["dnux", "dnuy", "dnu", "dx", "dy", "diffusion", "diffusionRate"]
+    units = {"x": "m", "y": "m", "s": "m/pass", "dx": "m", "dy": "m"}
+    cols = [(k, "double", [r[k] for r in rows], {"units": units[k]} if k in units else {}) for k in names]
+    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Frequency map analysis")
+
+
+def write_aperture(path, result, step=1, mode="binary"):
+    """elegant's &find_aperture output for the line modes
+    (aperture_search.c:20-55, :1160-1215) from
+    elegant_b200.aperture.find_aperture_lines: the last survivor of each
+    line, the clipped limits, the loss point, and the Area parameter."""
+    lines = result["lines"]
+    cols = [("x", "double", [l["x"] for l in lines], {"units": "m"}),
+            ("y", "double", [l["y"] for l in lines], {"units": "m"}),
+            ("xClipped", "double", result["x_limit"], {"units": "m"}),
+            ("yClipped", "double", result["y_limit"], {"units": "m"}),
+            ("sLost", "double", [l.get("s_lost", 0.0) for l in lines], {"units": "m"}),
+            ("xLost", "double", [l["x_lost"] if l["x_lost"] is not None else 1.7976931348623157e308
+                                 for l in lines], {"units": "m"}),
+            ("yLost", "double", [l["y_lost"] if l["y_lost"] is not None else 1.7976931348623157e308
+                                 for l in lines], {"units": "m"})]
+    write_sdds(path, [("Step", "long", step, {}), ("Area", "double", result["area"], {"units": "m$a2$n"})], cols,
+               mode, description="Dynamic aperture search")

@@ -47,3 +47,31 @@ def test_losses_layout(tmp_path):
     assert cols["particleID"].tolist() == [4, 8, 21] and cols["Pass"].tolist() == [0, 5, 9]
     z = np.cumsum([e.length for e in lat.elements])
     assert cols["s"].tolist() == [z[2], z[10], z[64]]
+
+
+@pytest.mark.parametrize("mode", ["binary", "ascii"])
+def test_caller_outputs_round_trip(tmp_path, mode):
+    from elegant_b200.sdds import write_aperture, write_frequency_map, write_momentum_aperture
+    side = {"delta": 0.0123, "found": True, "lost_on_pass": 7, "x_lost": 0.02, "y_lost": 1e-6, "s_lost": 3.5,
+            "delta_when_lost": 0.0131, "delta_lost": 0.0125}
+    rows = [{"name": "QF", "type": "KQUAD", "s": 0.8, "positive": side, "negative": dict(side, delta=-0.01)},
+            {"name": "QF", "type": "KQUAD", "s": 4.6, "positive": side, "negative": dict(side, found=False)}]
+    p = tmp_path / f"ma.{mode}"
+    write_momentum_aperture(p, rows, step=2, mode=mode)
+    pv, c = read_sdds(p)
+    assert pv["Step"] == 2 and c["ElementName"] == ["QF", "QF"] and list(c["ElementOccurence"]) == [1, 2]
+    assert list(c["deltaNegative"]) == [-0.01, 0.0123] and list(c["deltaNegativeFound"]) == [1, 0]
+    assert list(c["lostOnPassPositive"]) == [7, 7] and c["deltaPositiveFound"].dtype == np.int16
+    fm = [{"x": 1e-3, "y": 2e-3, "delta": 0.0, "nux": 0.21, "nuy": 0.33, "s": 30.4, "dnux": 1e-7, "dnuy": 2e-7,
+           "dnu": 2.2e-7, "dx": 0.0, "dy": 0.0, "diffusion": -13.3, "diffusionRate": -15.0}]
+    p = tmp_path / f"fma.{mode}"
+    write_frequency_map(p, fm, include_changes=True, mode=mode)
+    _, c = read_sdds(p)
+    assert c["nux"][0] == 0.21 and c["diffusion"][0] == -13.3
+    ap = {"lines": [{"x": -0.01, "y": 0.0, "x_lost": -0.011, "y_lost": 0.0},
+                    {"x": 0.0, "y": 0.008, "x_lost": None, "y_lost": None}],
+          "x_limit": [-0.01, 0.0], "y_limit": [0.0, 0.008], "area": 4e-5}
+    p = tmp_path / f"ap.{mode}"
+    write_aperture(p, ap, mode=mode)
+    pv, c = read_sdds(p)
+    assert pv["Area"] == 4e-5 and list(c["xClipped"]) == [-0.01, 0.0] and c["xLost"][1] > 1e300
