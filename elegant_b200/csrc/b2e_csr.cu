@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include "b2e_csr.h"
 #include "b2e_roots.h"
 #include "b2e_fft.h"
@@ -198,6 +199,16 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
 
 /* histogram of c*t with the range of binParticleCoordinate (csbend.c:3047-3113):
  * shared-memory integer counts aggregated per warp, then added to global counts. */
+static const int kHistUnroll = 4;
+
+/* histogram CTAs (1024 threads) per bunch: one per 1024 particles, at most two
+ * resident CTAs per SM over all bunches (each thread then takes up to
+ * kHistUnroll particles per sweep) */
+static inline int hist_blocks(int64_t per_bunch, int nbunch) {
+  return (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 2 / std::max(nbunch, 1)),
+                                std::max<int64_t>(1, (per_bunch + 1023) / 1024));
+}
+
 __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigned int *counts_all, int nBins,
                                 double factor) {
   extern __shared__ unsigned int scount[];
@@ -218,19 +229,41 @@ __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigne
     st->ctUpper = upper;
     st->dct = dct;
   }
-  for (int64_t i = first + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i - threadIdx.x < end;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    int bin = -1;
-    if (i < end && P.lost_pass[i] < 0) {
-      long long b = (long long)((P.s[i] - lower) / dct);
-      if (b >= 0 && b <= nBins - 1)
-        bin = (int)b;
+  /* kHistUnroll particles per thread and sweep, their loads issued together
+   * (the loss word and c*t are read unconditionally within the range, so
+   * neither waits on the other); the loop bounds are uniform over the block */
+  /* (c*t - lower)/dct through the stored reciprocal, correctly rounded as the
+   * division (div_rn_recip), while dct is a normal number well inside the
+   * range where 1/dct and the remainder stay normal */
+  const double inv_dct = 1.0 / dct;
+  const bool recip_ok = dct > 1e-280 && dct < 1e280;
+  /* chunks of blockDim.x particles, chunk c to CTA c mod gridDim.x */
+  const int64_t G = gridDim.x, D = blockDim.x;
+  for (int64_t c0 = blockIdx.x; first + c0 * D < end; c0 += G * kHistUnroll) {
+    int32_t lp[kHistUnroll];
+    double ct[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; u++) {
+      const int64_t i = first + (c0 + u * G) * D + threadIdx.x;
+      lp[u] = i < end ? P.lost_pass[i] : 0;
+      ct[u] = i < end ? P.s[i] : 0.0;
     }
-    /* warp aggregation: one shared-memory atomic per distinct bin per warp */
-    unsigned int peers = __match_any_sync(0xffffffffu, bin);
-    int leader = __ffs(peers) - 1;
-    if (bin >= 0 && (int)(threadIdx.x & 31) == leader)
-      atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; u++) {
+      const int64_t i = first + (c0 + u * G) * D + threadIdx.x;
+      int bin = -1;
+      if (i < end && lp[u] < 0) {
+        const double a = ct[u] - lower;
+        long long b = (long long)(recip_ok ? div_rn_recip(a, dct, inv_dct) : a / dct);
+        if (b >= 0 && b <= nBins - 1)
+          bin = (int)b;
+      }
+      /* warp aggregation: one shared-memory atomic per distinct bin per warp */
+      unsigned int peers = __match_any_sync(0xffffffffu, bin);
+      int leader = __ffs(peers) - 1;
+      if (bin >= 0 && (int)(threadIdx.x & 31) == leader)
+        atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+    }
   }
   __syncthreads();
   for (int b = threadIdx.x; b < nBins; b += blockDim.x)
@@ -313,6 +346,50 @@ __device__ void sg_apply(const double *in, double *out, int nBins, const double 
   }
 }
 
+/* ((v[0] + v[1]) + v[2]) + ... in index order, as a serial loop forms it;
+ * the next eight values load while the current eight are added */
+__device__ __forceinline__ double ordered_sum(const double *v, int n) {
+  double s = 0;
+  int b = 0;
+  if (n >= 8) {
+    double r[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      r[k] = v[k];
+    for (b = 8; b + 8 <= n; b += 8) {
+      double q[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        q[k] = v[b + k];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        s += r[k];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        r[k] = q[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      s += r[k];
+  }
+  for (; b < n; b++)
+    s += v[b];
+  return s;
+}
+
+/* bring this thread's rows of both Savitzky-Golay tables toward L1 while the
+ * counts load, so that the two filter passes do not wait on L2 */
+__device__ __forceinline__ void prefetch_sg_rows(const WakeArgs &a) {
+  for (int b = threadIdx.x; b < a.nBins; b += blockDim.x) {
+    if (a.sgHalf > 0) {
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(a.sg_w + (size_t)b * B2E_SG_MAX_WIDTH));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(a.sg_lo + 2 * b));
+    }
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.sgd_w + (size_t)b * B2E_SG_MAX_WIDTH));
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(a.sgd_lo + 2 * b));
+  }
+}
+
 /* Filters of one kick's wake (csbend.c:2566-2591) on one CTA: Savitzky-Golay
  * smoothing of the counts, correctDistribution, density per unit ct, its
  * derivative filter and the (dct*b)^(1/3) denominators.  Leaves hist = sm,
@@ -323,35 +400,66 @@ __device__ void wake_filters(const CountT *counts, const WakeArgs &a, const doub
   double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb, *tmp = sm + 3 * nb;
   __shared__ double nBinnedD;
   __shared__ int skip;
-  if (threadIdx.x == 0) {
-    SumT s = 0;
-    for (int b = 0; b < nb; b++)
-      s += counts[b];
-    nBinnedD = 1.0 * s;
-    if (nbinned_out)
-      *nbinned_out = s;
-    skip = 0;
+  __shared__ SumT warp_sums[32];
+  prefetch_sg_rows(a);
+  if constexpr (std::is_integral<SumT>::value) {
+    /* integer counts: the total is exact in any order, so it is a block
+     * reduction (per thread, warp shuffles, then the warps' totals) */
+    SumT part = 0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      const CountT v = counts[b];
+      hist[b] = (double)v;
+      part += v;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+      part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0)
+      warp_sums[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      SumT s = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++)
+        s += warp_sums[w];
+      nBinnedD = 1.0 * s;
+      if (nbinned_out)
+        *nbinned_out = s;
+      skip = 0;
+    }
+  } else {
+    /* real-valued counts: summed in bin order, as the reference's loop */
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+      hist[b] = (double)counts[b];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      SumT s = ordered_sum(hist, nb);
+      nBinnedD = 1.0 * s;
+      if (nbinned_out)
+        *nbinned_out = s;
+      skip = 0;
+    }
   }
-  for (int b = threadIdx.x; b < nb; b += blockDim.x)
-    hist[b] = (double)counts[b];
   __syncthreads();
   if (a.lh)
     lh_pass_filters(a, sm);
   if (a.sgHalf > 0) {
     sg_apply(hist, tmp, nb, a.sg_w, a.sg_lo, a.sg_n);
     __syncthreads();
-    /* correctDistribution (csbend.c:4705-4721): sequential sum as the reference */
+    /* correctDistribution (csbend.c:4705-4721): negative bins clipped in
+     * parallel, then the sum in bin order, as the reference forms it */
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
+      if (tmp[b] < 0)
+        tmp[b] = 0;
+    __syncthreads();
+    /* thread 0 runs the serial sum while warps 1.. form the denominators */
     if (threadIdx.x == 0) {
-      double sum = 0;
-      for (int b = 0; b < nb; b++) {
-        if (tmp[b] < 0)
-          tmp[b] = 0;
-        sum += tmp[b];
-      }
+      const double sum = ordered_sum(tmp, nb);
       if (!sum)
         skip = 1;
       else
         deriv[0] = nBinnedD / sum; /* factor, parked in deriv[0] */
+    } else if (threadIdx.x >= 32) {
+      for (int b = threadIdx.x - 32; b < nb; b += blockDim.x - 32)
+        denom[b] = b2e_pow13(dct * b);
     }
     __syncthreads();
     const double factor = deriv[0];
@@ -359,10 +467,11 @@ __device__ void wake_filters(const CountT *counts, const WakeArgs &a, const doub
     __syncthreads();
     for (int b = threadIdx.x; b < nb; b += blockDim.x)
       hist[b] = sk ? tmp[b] : tmp[b] * factor;
-    __syncthreads();
   }
+  const bool denom_done = a.sgHalf > 0 && blockDim.x > 32;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-    denom[b] = b2e_pow13(dct * b);
+    if (!denom_done)
+      denom[b] = b2e_pow13(dct * b);
     hist[b] = hist[b] / dct;
     deriv[b] = hist[b];
   }
@@ -527,17 +636,20 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
 __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a) {
   extern __shared__ double sm[];
   const int bunch = blockIdx.x;
-  if (!B.active[bunch])
-    return;
+  /* the bunch's scalars load together with its active flag (all in bounds) */
+  const int active = B.active[bunch];
+  const double csr_constant = B.csr_const[bunch], igf_factor = B.csr_const[B.n + bunch];
   CsrDevState *st = B.st + bunch;
+  const double dct = st->dct;
+  if (!active)
+    return;
   WakeArgs w = a;
-  const double csr_constant = B.csr_const[bunch];
   w.csr_constant = csr_constant;
   w.c1 = csr_constant * a.length / a.nSlices;
   w.c2 = -csr_constant * a.length / a.nSlices / a.slippage13;
-  w.igf_factor = B.csr_const[B.n + bunch];
+  w.igf_factor = igf_factor;
   w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
-  wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, st->dct, sm, st->dGamma, &st->nBinned,
+  wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, dct, sm, st->dGamma, &st->nBinned,
                                      nullptr, nullptr);
 }
 
@@ -1475,7 +1587,7 @@ static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, 
       return rrc;
     CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * nb * nbunch, stream));
     const int64_t per = (n + nbunch - 1) / nbunch;
-    const int hb = (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 4 / nbunch), std::max<int64_t>(1, (per + 1023) / 1024));
+    const int hb = hist_blocks(per, nbunch);
     csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * nb, stream>>>(P, n, H, st.d_counts, nb,
                                                                                   bend.binRangeFactor);
     (*launches)++;
@@ -1666,7 +1778,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       return rrc;
     CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
     int64_t per = (n + nbunch - 1) / nbunch;
-    int hb = (int)std::min<int64_t>(std::max<int64_t>(1, 148 * 4 / nbunch), std::max<int64_t>(1, (per + 1023) / 1024));
+    int hb = hist_blocks(per, nbunch);
     csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, B, st.d_counts, ce.bins,
                                                                                        ce.binRangeFactor);
     (*launches)++;
@@ -2046,7 +2158,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     if (!more_than_one)
       continue;
     STATIC_TRY(cudaMemsetAsync(S->counts, 0, sizeof(unsigned int) * bins, s));
-    int hb = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 1023) / 1024));
+    int hb = hist_blocks(n, 1);
     csr_hist_kernel<<<dim3(hb, 1), 1024, sizeof(unsigned int) * bins, s>>>(P, n, B, S->counts, bins, brf);
     STATIC_TRY(cudaGetLastError());
     phiBend += angle / nSlices;
