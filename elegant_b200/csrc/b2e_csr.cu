@@ -632,8 +632,12 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
 }
 
 /* wake of one kick, one CTA per bunch; c1 and c2 from the bunch's CSRConstant
- * in the host expression's order (csbend.c:2664-2667) */
-__global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a) {
+ * in the host expression's order (csbend.c:2664-2667).  With recycle set the
+ * CTA also readies its bunch for the next binning pass once this one's inputs
+ * are consumed: empty c*t range keys (the histogram kernel, the only reader,
+ * has finished) and zero counts (after they are read into shared memory). */
+__global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, unsigned int *counts_all, WakeArgs a,
+                                                           int recycle) {
   extern __shared__ double sm[];
   const int bunch = blockIdx.x;
   /* the bunch's scalars load together with its active flag (all in bounds) */
@@ -641,6 +645,10 @@ __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, const u
   const double csr_constant = B.csr_const[bunch], igf_factor = B.csr_const[B.n + bunch];
   CsrDevState *st = B.st + bunch;
   const double dct = st->dct;
+  if (recycle && threadIdx.x == 0) {
+    st->ct_min_key = ~0ull;
+    st->ct_max_key = 0ull;
+  }
   if (!active)
     return;
   WakeArgs w = a;
@@ -649,8 +657,11 @@ __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, const u
   w.c2 = -csr_constant * a.length / a.nSlices / a.slippage13;
   w.igf_factor = igf_factor;
   w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
-  wake_body<unsigned int, long long>(counts_all + (size_t)bunch * a.nBins, w, dct, sm, st->dGamma, &st->nBinned,
-                                     nullptr, nullptr);
+  unsigned int *counts = counts_all + (size_t)bunch * a.nBins;
+  wake_body<unsigned int, long long>(counts, w, dct, sm, st->dGamma, &st->nBinned, nullptr, nullptr);
+  if (recycle) /* the counts were copied to shared memory before the first barrier */
+    for (int b = threadIdx.x; b < a.nBins; b += blockDim.x)
+      counts[b] = 0;
 }
 
 /* deterministic sum over the CTA (blockDim.x a power of two, red >= blockDim.x doubles) */
@@ -1765,9 +1776,16 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
   (*launches)++;
   CSR_CUDA(cudaGetLastError());
   double phiBend = st.accumulated_angle;
+  /* on the plain-integral path the wake kernel empties the range keys and the
+   * counts for the next kick; otherwise both are reset before every kick */
+  const bool recycle = any_active && !use_net;
+  if (recycle)
+    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
   for (int kick = 0; kick < ce.nSlices; kick++) {
-    csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
-    (*launches)++;
+    if (!recycle || kick == 0) {
+      csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
+      (*launches)++;
+    }
     csr_slice_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, nullptr, B, kick > 0, ce.bins, Po, pass, elem);
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
@@ -1776,7 +1794,8 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     int rrc = reduce_keys(st, B, stream, err, launches);
     if (rrc)
       return rrc;
-    CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
+    if (!recycle)
+      CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
     int64_t per = (n + nbunch - 1) / nbunch;
     int hb = hist_blocks(per, nbunch);
     csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, B, st.d_counts, ce.bins,
@@ -1839,14 +1858,16 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       st.gate_values += nbunch;
       (*launches) += 3 + 7; /* filter, pack + 6 convolutions, combine */
     } else {
-      csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a);
+      csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a, recycle ? 1 : 0);
       (*launches)++;
       CSR_CUDA(cudaGetLastError());
     }
     st.wake_values += (int64_t)ce.bins * nbunch;
   }
-  csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
-  (*launches)++;
+  if (!recycle || ce.nSlices <= 0) {
+    csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
+    (*launches)++;
+  }
   csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, ce.bins, Po, ce.rho0);
   CSR_CUDA(cudaGetLastError());
   if (any_active) {
@@ -2195,7 +2216,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     a.igf_factor = 0;
     size_t smem = sizeof(double) * (4 * bins + 8);
     STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a);
+    csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a, 0);
     STATIC_TRY(cudaGetLastError());
   }
   csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);
