@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
 }
 
 /* histogram of c*t with the range of binParticleCoordinate (csbend.c:3047-3113):
- * shared-memory integer counts aggregated per warp, then added to global counts. */
+ * shared-memory integer counts, then added to global counts. */
 static const int kHistUnroll = 4;
 
 /* histogram CTAs (1024 threads) per bunch: one per 1024 particles, at most two
@@ -258,11 +258,18 @@ __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigne
         if (b >= 0 && b <= nBins - 1)
           bin = (int)b;
       }
-      /* warp aggregation: one shared-memory atomic per distinct bin per warp */
-      unsigned int peers = __match_any_sync(0xffffffffu, bin);
-      int leader = __ffs(peers) - 1;
-      if (bin >= 0 && (int)(threadIdx.x & 31) == leader)
-        atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+      /* one shared-memory atomic per particle, unless neighbouring lanes
+       * share a bin (a beam stored in c*t order, where a warp's particles
+       * would queue on one counter): then one atomic per distinct bin */
+      const int lane = threadIdx.x & 31;
+      const int prev = __shfl_up_sync(0xffffffffu, bin, 1);
+      if (__any_sync(0xffffffffu, lane > 0 && bin >= 0 && bin == prev)) {
+        const unsigned int peers = __match_any_sync(0xffffffffu, bin);
+        if (bin >= 0 && lane == __ffs(peers) - 1)
+          atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+      } else if (bin >= 0) {
+        atomicAdd(&scount[bin], 1u);
+      }
     }
   }
   __syncthreads();

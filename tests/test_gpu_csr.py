@@ -4,7 +4,7 @@ bit-identical final coordinates and bit-identical per-kick wake arrays."""
 import numpy as np
 import pytest
 
-from elegant_b200 import Element, Lattice, Tracker, workloads as w
+from elegant_b200 import Beam, Element, Lattice, Tracker, workloads as w
 from reforacle import by_id
 
 pytestmark = pytest.mark.gpu
@@ -38,6 +38,15 @@ def test_chicane_bit_exact(ref_b2e, bins, kicks, sg):
     lat = w.chicane(bins=bins, n_kicks=kicks, sg_halfwidth=sg)
     beam = w.chicane_beam(20000, seed=bins)
     check(*run_both(ref_b2e, lat, beam))
+
+
+def test_chicane_beam_stored_in_ct_order(ref_b2e):
+    """Rows sorted by c*t: neighbouring particles share histogram bins, which
+    takes the binning's per-warp aggregation path."""
+    lat = w.chicane(bins=80, n_kicks=4)
+    beam = w.chicane_beam(20000, seed=21)
+    order = np.argsort(beam.coords[:, 4], kind="stable")
+    check(*run_both(ref_b2e, lat, Beam(beam.coords[order], beam.ids[order])))
 
 
 def test_chicane_steady_state_and_plain_sum(ref_b2e):
