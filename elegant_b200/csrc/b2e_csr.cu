@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <mutex>
 #include <type_traits>
+#include <utility>
 #include "b2e_csr.h"
 #include "b2e_roots.h"
 #include "b2e_fft.h"
@@ -152,6 +153,18 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
   beta0[i] = b0;
 }
 
+/* Programmatic dependent launch (sm_90 and later, PTX griddepcontrol): a
+ * kernel of the kick chain launched with the programmatic-serialization
+ * attribute may be scheduled while its predecessor's last CTAs still run.
+ * Each such kernel first lets its own successor be scheduled (once all of its
+ * CTAs have started), then waits until the predecessor grid has completed
+ * and its memory is visible, before touching any memory.  In a kernel
+ * launched without the attribute both instructions return at once. */
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 /* one kick: optional wake kick of the previous kick, one integrator slice,
  * c*t update, min/max of c*t (csbend.c:2385-2450, :3066-3076) */
 /* 64 registers (4 blocks of 256 per SM): twice the resident warps of the
@@ -159,6 +172,7 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
 __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64_t n, const double *beta0, const DevElem *ep,
                                  const DevAperture *ap, CsrBunches B, int after_first_kick, int nBins, double Po,
                                  int pass, int elem_index) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool alive = i < n && P.lost_pass[i] < 0;
   const int b = i < n ? bunch_of(i, B) : B.n - 1;
@@ -209,9 +223,28 @@ static inline int hist_blocks(int64_t per_bunch, int nbunch) {
                                 std::max<int64_t>(1, (per_bunch + 1023) / 1024));
 }
 
+/* launch with programmatic stream serialization (the kernel begins with
+ * chain_enter) */
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                  Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigned int *counts_all, int nBins,
                                 double factor) {
   extern __shared__ unsigned int scount[];
+  chain_enter();
   const int bunch = blockIdx.y;
   if (!B.active[bunch])
     return;
@@ -646,6 +679,7 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
 __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, unsigned int *counts_all, WakeArgs a,
                                                            int recycle) {
   extern __shared__ double sm[];
+  chain_enter();
   const int bunch = blockIdx.x;
   /* the bunch's scalars load together with its active flag (all in bounds) */
   const int active = B.active[bunch];
@@ -1793,7 +1827,8 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
       (*launches)++;
     }
-    csr_slice_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, nullptr, B, kick > 0, ce.bins, Po, pass, elem);
+    CSR_CUDA(launch_chained(csr_slice_kernel, dim3(g), dim3(256), 0, stream, P, n, (const double *)st.d_beta0, d_e,
+                            (const DevAperture *)nullptr, B, (int)(kick > 0), ce.bins, Po, pass, elem));
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
     if (!any_active)
@@ -1805,8 +1840,8 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
     int64_t per = (n + nbunch - 1) / nbunch;
     int hb = hist_blocks(per, nbunch);
-    csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * ce.bins, stream>>>(P, n, B, st.d_counts, ce.bins,
-                                                                                       ce.binRangeFactor);
+    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), sizeof(unsigned int) * ce.bins, stream, P,
+                            n, B, st.d_counts, ce.bins, ce.binRangeFactor));
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
     if (st.reducer && st.reducer(st.reducer_user, B2E_REDUCE_SUM_U32, st.d_counts, (int64_t)ce.bins * nbunch, stream)) {
@@ -1865,7 +1900,8 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       st.gate_values += nbunch;
       (*launches) += 3 + 7; /* filter, pack + 6 convolutions, combine */
     } else {
-      csr_wake_kernel<<<nbunch, 1024, wake_smem, stream>>>(B, st.d_counts, a, recycle ? 1 : 0);
+      CSR_CUDA(launch_chained(csr_wake_kernel, dim3(nbunch), dim3(1024), wake_smem, stream, B, st.d_counts, a,
+                              recycle ? 1 : 0));
       (*launches)++;
       CSR_CUDA(cudaGetLastError());
     }
