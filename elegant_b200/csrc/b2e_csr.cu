@@ -120,8 +120,21 @@ __device__ __forceinline__ double csr_kick(double CT, double X, double DP, const
   return DP;
 }
 
+/* Programmatic dependent launch (sm_90 and later, PTX griddepcontrol): a
+ * kernel of the kick chain launched with the programmatic-serialization
+ * attribute may be scheduled while its predecessor's last CTAs still run.
+ * Each such kernel first lets its own successor be scheduled (once all of its
+ * CTAs have started), then waits until the predecessor grid has completed
+ * and its memory is visible, before touching any memory.  In a kernel
+ * launched without the attribute both instructions return at once. */
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 /* entrance: offsets, tilt, c*t = s/beta, entrance edge (csbend.c:2286-2377) */
 __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const DevElem *ep, double Po) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
     return;
@@ -151,18 +164,6 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
   P.yp[i] = YP;
   P.s[i] = s;
   beta0[i] = b0;
-}
-
-/* Programmatic dependent launch (sm_90 and later, PTX griddepcontrol): a
- * kernel of the kick chain launched with the programmatic-serialization
- * attribute may be scheduled while its predecessor's last CTAs still run.
- * Each such kernel first lets its own successor be scheduled (once all of its
- * CTAs have started), then waits until the predecessor grid has completed
- * and its memory is visible, before touching any memory.  In a kernel
- * launched without the attribute both instructions return at once. */
-__device__ __forceinline__ void chain_enter() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 /* one kick: optional wake kick of the previous kick, one integrator slice,
@@ -873,6 +874,7 @@ __global__ void wake_batch_kernel(const double *counts, const double *slippage_b
 
 /* after the last kick: its wake kick and the min/max for the exit binning */
 __global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrBunches B, int nBins, double Po, double rho0) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   bool alive = i < n && P.lost_pass[i] < 0;
   const int b = i < n ? bunch_of(i, B) : B.n - 1;
@@ -889,6 +891,7 @@ __global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrBunches B, in
  * (csbend.c:2810-2955); csrWake.s0 from the exit binning's lower edge. */
 __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, CsrBunches B, double factor, double Po,
                                 int pass, int elem_index) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const DevElem &e = *ep;
   const double *c = e.c;
@@ -938,6 +941,7 @@ __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, Cs
 /* CSRDRIFT mode 0, one kick (csbend.c:3415-3502) */
 __global__ void csr_drift_kick_kernel(DevParticles P, int64_t n, CsrBunches B, double dz, double s0_incr,
                                       double factor, int apply, int nBins, double Po) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
     return;
@@ -981,6 +985,7 @@ __global__ void csr_init_state_kernel(CsrDevState *st, int n) {
  * csbend.c:3835-3848), then forward by dz; c*t = s/beta; min/max of c*t per
  * bunch (csbend.c:3876-3893) */
 __global__ void stupakov_drift_kernel(DevParticles P, int64_t n, CsrBunches B, double dz_back, double dz, double Po) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int b = i < n ? bunch_of(i, B) : B.n - 1;
   const bool mine = i < n && P.lost_pass[i] < 0 && B.mode[b];
@@ -1059,6 +1064,7 @@ __device__ __forceinline__ long long clamp_bins(double d, int nb) {
  * memory: 4 nBins + 8 doubles for the filters, nBins for phi. */
 __global__ void __launch_bounds__(1024, 1) stupakov_wake_kernel(CsrBunches B, const unsigned int *counts_all, WakeArgs a, StupakovArgs sa) {
   extern __shared__ double sm[];
+  chain_enter();
   const int bunch = blockIdx.x;
   if (!B.mode[bunch])
     return;
@@ -1111,6 +1117,7 @@ __global__ void __launch_bounds__(1024, 1) stupakov_wake_kernel(CsrBunches B, co
 
 /* kick from the wake and c*t back to s at the new velocity (csbend.c:4078-4096) */
 __global__ void stupakov_kick_kernel(DevParticles P, int64_t n, CsrBunches B, int nBins, double Po) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
     return;
@@ -1153,6 +1160,7 @@ __global__ void csr_keys_scatter_kernel(CsrBunches B, const unsigned long long *
 }
 
 __global__ void csr_s0_add_kernel(CsrBunches B, double incr) {
+  chain_enter();
   for (int b = threadIdx.x; b < B.n; b += blockDim.x)
     if (B.mode[b])
       B.st[b].s0 = B.st[b].s0 + incr;
@@ -1191,6 +1199,7 @@ cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const De
 /* exact drift of the particles of the bunches whose CSRDRIFT mode is `mode`
  * (every particle when the mode table is null) */
 __global__ void edrift_kernel(DevParticles P, int64_t n, double L, CsrBunches B, int mode) {
+  chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
     return;
@@ -1631,7 +1640,8 @@ static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, 
     sa.dz0 = dz0;
     sa.trapz = bend.trapz;
     csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
-    stupakov_drift_kernel<<<g, 256, 0, stream>>>(P, n, B, iKick == 0 ? dz_back : 0.0, dz, Po);
+    CSR_CUDA(launch_chained(stupakov_drift_kernel, dim3(g), dim3(256), 0, stream, P, n, B, iKick == 0 ? dz_back : 0.0,
+                            dz, Po));
     (*launches) += 2;
     CSR_CUDA(cudaGetLastError());
     int rrc = reduce_keys(st, B, stream, err, launches);
@@ -1640,20 +1650,21 @@ static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, 
     CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * nb * nbunch, stream));
     const int64_t per = (n + nbunch - 1) / nbunch;
     const int hb = hist_blocks(per, nbunch);
-    csr_hist_kernel<<<dim3(hb, nbunch), 1024, sizeof(unsigned int) * nb, stream>>>(P, n, H, st.d_counts, nb,
-                                                                                  bend.binRangeFactor);
+    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), sizeof(unsigned int) * nb, stream, P, n, H,
+                            st.d_counts, nb, bend.binRangeFactor));
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
     if (st.reducer && st.reducer(st.reducer_user, B2E_REDUCE_SUM_U32, st.d_counts, (int64_t)nb * nbunch, stream)) {
       err = "CSR: the all-rank reduction of the histogram failed";
       return B2E_ERR_CUDA;
     }
-    stupakov_wake_kernel<<<nbunch, 1024, smem, stream>>>(B, st.d_counts, a, sa);
-    stupakov_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, nb, Po);
+    CSR_CUDA(launch_chained(stupakov_wake_kernel, dim3(nbunch), dim3(1024), smem, stream, B,
+                            (const unsigned int *)st.d_counts, a, sa));
+    CSR_CUDA(launch_chained(stupakov_kick_kernel, dim3(g), dim3(256), 0, stream, P, n, B, nb, Po));
     (*launches) += 2;
     CSR_CUDA(cudaGetLastError());
   }
-  edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz0 / 2, B, 1);
+  CSR_CUDA(launch_chained(edrift_kernel, dim3(g), dim3(256), 0, stream, P, n, dz0 / 2, B, 1));
   (*launches)++;
   CSR_CUDA(cudaGetLastError());
   st.zLast = zStart + length;
@@ -1738,15 +1749,16 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
         dz = dz0;
       double incr = dz + dzFirst;
       double factor = (dz0 + dzFirst) / st.ds0;
-      csr_drift_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, dz, incr, factor, 1, lastBins, Po);
-      csr_s0_add_kernel<<<1, 32, 0, stream>>>(B, incr);
+      CSR_CUDA(launch_chained(csr_drift_kick_kernel, dim3(g), dim3(256), 0, stream, P, n, B, dz, incr, factor, 1,
+                              lastBins, Po));
+      CSR_CUDA(launch_chained(csr_s0_add_kernel, dim3(1), dim3(32), 0, stream, B, incr));
       (*launches) += 2;
       CSR_CUDA(cudaGetLastError());
       dzFirst = 0;
     }
     dz = dz0 / 2;
-    edrift_kernel<<<g, 256, 0, stream>>>(P, n, dz, B, 1);
-    csr_s0_add_kernel<<<1, 32, 0, stream>>>(B, dz);
+    CSR_CUDA(launch_chained(edrift_kernel, dim3(g), dim3(256), 0, stream, P, n, dz, B, 1));
+    CSR_CUDA(launch_chained(csr_s0_add_kernel, dim3(1), dim3(32), 0, stream, B, dz));
     (*launches) += 2;
     CSR_CUDA(cudaGetLastError());
     st.zLast = zStart + ce.drift_length;
@@ -1813,7 +1825,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
                                   (int)sur_smem));
   }
 
-  csr_entry_kernel<<<g, 256, 0, stream>>>(P, n, st.d_beta0, d_e, Po);
+  CSR_CUDA(launch_chained(csr_entry_kernel, dim3(g), dim3(256), 0, stream, P, n, st.d_beta0, d_e, Po));
   (*launches)++;
   CSR_CUDA(cudaGetLastError());
   double phiBend = st.accumulated_angle;
@@ -1911,14 +1923,15 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
     (*launches)++;
   }
-  csr_last_kick_kernel<<<g, 256, 0, stream>>>(P, n, B, ce.bins, Po, ce.rho0);
+  CSR_CUDA(launch_chained(csr_last_kick_kernel, dim3(g), dim3(256), 0, stream, P, n, B, ce.bins, Po, ce.rho0));
   CSR_CUDA(cudaGetLastError());
   if (any_active) {
     int rrc = reduce_keys(st, B, stream, err, launches);
     if (rrc)
       return rrc;
   }
-  csr_exit_kernel<<<g, 256, 0, stream>>>(P, n, d_e, B, ce.binRangeFactor, Po, pass, elem);
+  CSR_CUDA(launch_chained(csr_exit_kernel, dim3(g), dim3(256), 0, stream, P, n, d_e, B, ce.binRangeFactor, Po, pass,
+                          elem));
   (*launches) += 2;
   CSR_CUDA(cudaGetLastError());
   for (int b = 0; b < nbunch; b++)
