@@ -124,7 +124,16 @@ B2E_HD double b2e_reduce_pio2(double x, int *quadrant) {
   return r;
 }
 
+/* For |x| <= 2^-4 the general path below takes quadrant 0, r = x and the
+ * short kernels; the entry points test that case first and return the same
+ * values without the reduction, quadrant and NaN logic (the bend integrator's
+ * angles are nearly always that small). */
 B2E_HD void b2e_sincos(double x, double *s, double *c) {
+  if (fabs(x) <= 0x1p-4) {
+    *s = b2e_sin_kernel_small(x);
+    *c = b2e_cos_kernel_small(x);
+    return;
+  }
   int q;
   double r = b2e_reduce_pio2(x, &q), sr, cr;
   sr = b2e_sin_r(r);
@@ -156,6 +165,8 @@ B2E_HD void b2e_sincos(double x, double *s, double *c) {
 /* Single-result variants: same reduction and kernels as b2e_sincos, so each
  * returns bit-for-bit the corresponding member of the pair. */
 B2E_HD double b2e_sin(double x) {
+  if (fabs(x) <= 0x1p-4)
+    return b2e_sin_kernel_small(x);
   int q;
   double r = b2e_reduce_pio2(x, &q), v;
   if (x != x)
@@ -165,6 +176,8 @@ B2E_HD double b2e_sin(double x) {
 }
 
 B2E_HD double b2e_cos(double x) {
+  if (fabs(x) <= 0x1p-4)
+    return b2e_cos_kernel_small(x);
   int q;
   double r = b2e_reduce_pio2(x, &q), v;
   if (x != x)
