@@ -27,6 +27,8 @@ __device__ __forceinline__ double b2e_ipow(double x, int n) {
   /* integer power by repeated multiplication (the toolkit's ipow) */
   double r;
   int i;
+  if (n == 2) /* the elliptical apertures' exponent: the loop's one product */
+    return x * x;
   if (n == 0)
     return 1.0;
   r = x;
