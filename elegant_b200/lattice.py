@@ -54,7 +54,7 @@ SLOTS = {
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,
     nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6},
-    nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "Y_EXPONENT": 4},
+    nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "YEXPONENT": 4},
     nat.MARK: {},
     nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},
     nat.CSRDRIFT: {"L": 0, "N_KICKS": 1, "DZ": 2, "CSR": 3, "USE_STUPAKOV": 4},

@@ -148,7 +148,7 @@ extern "C" {
 #define B2E_MAXAMP_Y_MAX 1
 #define B2E_MAXAMP_ELLIPTICAL 2
 #define B2E_MAXAMP_EXPONENT 3
-#define B2E_MAXAMP_Y_EXPONENT 4
+#define B2E_MAXAMP_Y_EXPONENT 4 /* elegant name: YEXPONENT; 0 = EXPONENT */
 /* CHARGE (charge_param, track_data.c:2488) */
 #define B2E_CHARGE_TOTAL 0
 #define B2E_CHARGE_PER_PARTICLE 1
