@@ -54,6 +54,11 @@ __device__ __forceinline__ bool mult_aperture_ok(double xIn, double yIn, const D
     if ((ap->x_max > 0 && fabs(x) > ap->x_max) || (ap->y_max > 0 && fabs(y) > ap->y_max))
       return false;
   } else {
+    /* |x| <= x_max/4 and |y| <= y_max/4 (exact comparisons) give rounded
+     * quotients of magnitude <= 1/4, powers (exponent >= 1) <= 1/4 and a sum
+     * <= 1/2: inside, the answer the divisions below would give */
+    if (ap->xe >= 1 && ap->ye >= 1 && fabs(x) <= 0.25 * ap->x_max && fabs(y) <= 0.25 * ap->y_max)
+      return true;
     double xa = x / ap->x_max, yb = y / ap->y_max;
     if ((b2e_ipow(xa, ap->xe) + b2e_ipow(yb, ap->ye)) >= 1)
       return false;
@@ -604,6 +609,13 @@ __device__ __forceinline__ bool maxamp_ok(const Part &p, const DevAperture &a) {
   if (a.mode == 2) {
     if (isinf(p.x) || isinf(p.y) || isnan(p.x) || isnan(p.y))
       return false;
+    /* |x| <= x_max/4, |y| <= y_max/4: with exponents 1..8 and half-axes in
+     * [2^-100, 2^100] every rounded power is that of x_max/4 or less, i.e.
+     * at most 4^-n a2 (scaling by 1/4 is exact there), so each term is at
+     * most 1/4 and the particle is inside, as the divisions below find */
+    if (a.xe >= 1 && a.xe <= 8 && a.ye >= 1 && a.ye <= 8 && a.x_max >= 0x1p-100 && a.x_max <= 0x1p100 &&
+        a.y_max >= 0x1p-100 && a.y_max <= 0x1p100 && fabs(p.x) <= 0.25 * a.x_max && fabs(p.y) <= 0.25 * a.y_max)
+      return true;
     return !((b2e_ipow(p.x, a.xe) / a.a2 + b2e_ipow(p.y, a.ye) / a.b2) > 1);
   }
   return true;

@@ -76,6 +76,33 @@ def test_ring_losses_match(ref_b2e):
     assert_parity(res, rows, nl)
 
 
+@pytest.mark.parametrize("exponents", [(2, 2), (4, 6), (8, 2), (10, 4)])
+def test_ring_aperture_around_quarter_axes(ref_b2e, exponents):
+    """Particles at, just inside and just outside a quarter of the half-axes
+    (where the aperture tests stop dividing) and near the edge, for
+    elliptical and super-elliptical MAXAMP apertures."""
+    xe, ye = exponents
+    els = [Element(e.name, e.type, dict(e.params, EXPONENT=xe, YEXPONENT=ye)) if e.type == "MAXAMP" else e
+           for e in w.fodo_ring().elements]
+    lat = Lattice(els)
+    q = 0.25 * 0.02
+    edge = [q, np.nextafter(q, 1), np.nextafter(q, 0), 0.0195, 0.02, 0.0201]
+    rng = np.random.default_rng(11)
+    rows = [(sx * a, sy * b) for a in edge for b in edge for sx in (1, -1) for sy in (1, -1)]
+    rows += [tuple(v) for v in rng.uniform(-0.021, 0.021, (200, 2))]
+    n = len(rows)
+    c = np.zeros((n, 6))
+    c[:, 0] = [r[0] for r in rows]
+    c[:, 2] = [r[1] for r in rows]
+    c[:, 1] = rng.uniform(-2e-4, 2e-4, n)
+    c[:, 3] = rng.uniform(-2e-4, 2e-4, n)
+    beam = Beam(c, np.arange(1, n + 1))
+    res = gpu_track(lat, beam, w.ring_p_central(), 5)
+    ref_rows, nl, _, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 5)
+    assert 0 < nl < n
+    assert_parity(res, ref_rows, nl)
+
+
 def test_ring_misaligned_and_tilted(ref_b2e):
     lat = w.fodo_ring()
     els = []
