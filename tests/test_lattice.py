@@ -69,3 +69,14 @@ def test_ctypes_layout():
 def test_ring_optics_stable():
     tw = periodic_twiss(w.fodo_ring(rf=False))
     assert 0 < tw.tune_x < 0.5 and 0 < tw.tune_y < 0.5 and tw.beta_x > 0 and tw.beta_y > 0
+
+
+def test_maxamp_exponents_take_elegants_names():
+    """MAXAMP's EXPONENT and YEXPONENT (track_data.c:994-995) land in their
+    slots from an .lte line; YEXPONENT 0 leaves the y exponent to EXPONENT."""
+    lat = parse_lte("MA: MAXAMP, X_MAX=0.02, Y_MAX=0.01, ELLIPTICAL=1, EXPONENT=4, YEXPONENT=6\nL: LINE=(MA)\n")
+    s = lat.elements[0].slots()
+    assert s[3] == 4 and s[4] == 6
+    assert Element("MA", "MAXAMP", {}).slots()[3] == 2 and Element("MA", "MAXAMP", {}).slots()[4] == 0
+    with pytest.raises(LatticeError):
+        Element("MA", "MAXAMP", {"Y_EXPONENT": 6}).slots()
