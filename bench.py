@@ -38,8 +38,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "particle-turns/s (FP64)"
 # dram__bytes_read.sum + dram__bytes_write.sum of one ring_kernel launch on the
-# 512-instance ensemble (71.16 MB + 22.74 MB; the capture in profiles/)
-RING_TRAFFIC_BYTES = 93_907_712
+# 512-instance ensemble (71.45 MB + 20.33 MB; the latest capture in profiles/)
+RING_TRAFFIC_BYTES = 91_783_168
 UNIT = "particle-turns/s"
 
 
