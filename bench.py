@@ -12,9 +12,10 @@ default) continuing the same run; ``--steps`` steps are timed after
 - e2e: the same metric through the C ABI with host buffers (b2e_track_host:
   pinned-host -> device copy, tracking of a fresh run, device -> host copy,
   all inside the timed region).
-- roofline: FP64 pipe; algorithmic FP64 operations per particle-turn
-  (counted for this lattice, see elegant_b200/flops.py) over the measured
-  FP64 DGEMM rate of this GPU.
+- roofline: FP64; algorithmic FP64 operations per particle-turn (the
+  reference's formulas for this lattice, each elementary-function call at a
+  fixed weight: elegant_b200/flops.py) over the FP64 DGEMM rate measured on
+  this GPU in the same run.
 - cpu_baseline / --impl reference: elegant's own C tracking code
   (oracle/_ref, compiled from the reference sources) on the host cores.
 
@@ -235,7 +236,7 @@ def cpu_reference_rate(n_instances: int, seed: int, target_seconds: float, cores
     bounded sample: `cores` instances, each capped at a particle count sized
     so one process runs for about `target_seconds`."""
     rate_per_core = 1.6e4  # calibration guess, refined by the measurement itself
-    turns = 20
+    turns = 100  # the GPU step's pass count
     max_particles = max(50, int(target_seconds * rate_per_core / turns))
     insts = [[i] for i in range(cores)]
     ctx = mp.get_context("spawn")
@@ -273,7 +274,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     from elegant_b200 import Tracker, workloads as w
-    from elegant_b200.flops import flops_per_particle_turn
+    from elegant_b200.flops import ELEMENTARY_WEIGHT, counts_per_particle_turn, flops_per_particle_turn
 
     seed = 2024 + 1000 * rank
     lat, beam, offsets, overrides = w.ensemble(n_instances=args.instances, seed=seed)
@@ -420,6 +421,11 @@ def main():
                                          "profiles/ring_kernel_ensemble.md); the coordinates once per launch",
                          "algorithmic_bytes_per_launch": int(n * 96),
                          "flops_per_particle_turn": fpt,
+                         "flop_model": {"arithmetic": counts_per_particle_turn(lat)[0],
+                                        "elementary_calls": counts_per_particle_turn(lat)[1],
+                                        "elementary_weight": ELEMENTARY_WEIGHT,
+                                        "source": "elegant_b200/flops.py: the reference's formulas, +-*/ and sqrt "
+                                                  "1 each, each sin/cos/asin/tan call a fixed 20"},
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 (torch.mm float64), best of 3"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary(),
             "single_ring": single, "csr": csr, "wake_surrogate": surrogate, "bunch_train": train,

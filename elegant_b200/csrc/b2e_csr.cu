@@ -2021,8 +2021,12 @@ void csr_release(CsrState &st) {
  * The array holds per-particle entrance velocities (up to
  * B2E_STATIC_MAX_PARTICLES), the CSR binning/wake state, the histogram, the
  * Savitzky-Golay weight tables (up to B2E_STATIC_MAX_BINS bins) and the
- * element record: about 10.2 MB, resident on every GPU that loads the library
- * until the process exits.  All calls share it and it keeps the previous
+ * element record: about 10.2 MB.  Under lazy module loading (CUDA's default)
+ * a device gives it memory when this module is first used there -- the
+ * set-up in static_scratch() -- and keeps it until the process exits.  The
+ * call only enqueues work: the alive count that decides whether CSR is
+ * computed becomes the bunch's flags on the device, so the host never waits
+ * for the GPU.  All calls share the array and it keeps the previous
  * call's contents; everything that must start at zero is cleared by each
  * call.  Two calls whose work overlaps on the GPU (different streams, or
  * different host threads) race on this memory: callers must serialise them.
@@ -2045,8 +2049,13 @@ struct StaticCsrScratch {
 
 static __device__ __align__(256) unsigned char g_static_csr_scratch[sizeof(StaticCsrScratch)];
 
-/* device addresses of g_static_csr_scratch, one per device, looked up on the
- * first call made with that device current */
+/* Device addresses of g_static_csr_scratch, one per device, looked up by the
+ * first call made with that device current (the set-up step).  That lookup is
+ * also what makes CUDA load this module on the device under lazy module
+ * loading (the default), so the array and the kernels' code take their device
+ * memory at that first call, not when the library is loaded.  The cached
+ * address belongs to the device's primary context: the library must not be
+ * used on a device after cudaDeviceReset. */
 #define B2E_STATIC_MAX_DEVICES 64
 static void *g_static_addr[B2E_STATIC_MAX_DEVICES];
 static std::mutex g_static_mutex;
@@ -2077,10 +2086,14 @@ __global__ void static_set_elem_kernel(DevElem e, DevElem *dst) { *dst = e; }
 /* Savitzky-Golay weight tables for one element, on the device, with the same
  * helpers and layout as csr_configure (rows of B2E_SG_MAX_WIDTH weights;
  * interleaved (start, width) index pairs; smoothing rows then derivative rows). */
-__global__ void static_set_bunch_kernel(StaticCsrScratch *S, double csr_constant, double igf_factor, int active) {
-  S->csr_const[0] = csr_constant;
+/* The bunch's flags from the entrance count (S->counters[1] = particles alive
+ * at the entrance; CSR only for more than one, csbend.c:1987), formed on the
+ * device so that the host never waits for the count. */
+__global__ void static_set_bunch_kernel(StaticCsrScratch *S, double csr_constant, double igf_factor) {
+  const int more_than_one = S->counters[1] > 1;
+  S->csr_const[0] = more_than_one ? csr_constant : 0.0;
   S->csr_const[1] = igf_factor;
-  S->flags[0] = (unsigned char)active;
+  S->flags[0] = (unsigned char)more_than_one;
   S->flags[1] = 0;
 }
 
@@ -2131,11 +2144,12 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   if (!(errbuf && errlen > 0))
     errlen = sizeof(local_err);
   err[0] = 0;
-  if (!dev_columns || !dev_lost_pass || !dev_lost_element || !bend || n < 0 || p_central <= 0) {
+  /* n = 0 (the set-up call) touches no particle buffer: they may be NULL */
+  if (!bend || n < 0 || p_central <= 0 || (n > 0 && (!dev_columns || !dev_lost_pass || !dev_lost_element))) {
     snprintf(err, errlen, "b2e_csr_bend_static: null pointer, negative count or nonpositive p_central");
     return B2E_ERR_ARG;
   }
-  for (int c = 0; c < 6; c++)
+  for (int c = 0; c < 6 && n > 0; c++)
     if (!dev_columns[c]) {
       snprintf(err, errlen, "b2e_csr_bend_static: column %d is null", c);
       return B2E_ERR_ARG;
@@ -2171,6 +2185,10 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     snprintf(err, errlen, "b2e_csr_bend_static: Savitzky-Golay half-width too large");
     return B2E_ERR_ARG;
   }
+  if (p[B2E_BEND_IGF] != 0 && p[B2E_BEND_STEADY_STATE] == 0) {
+    snprintf(err, errlen, "b2e_csr_bend_static: Must have STEADY_STATE=1 when IGF=1");
+    return B2E_ERR_LATTICE;
+  }
   if (dev_wakes && wake_capacity < (int64_t)nSlices * bins) {
     snprintf(err, errlen, "b2e_csr_bend_static: wake buffer holds %lld values, %lld needed",
              (long long)wake_capacity, (long long)nSlices * bins);
@@ -2181,12 +2199,12 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     return B2E_ERR_CUDA;
   cudaStream_t s = (cudaStream_t)stream;
   DevParticles P;
-  P.x = dev_columns[0];
-  P.xp = dev_columns[1];
-  P.y = dev_columns[2];
-  P.yp = dev_columns[3];
-  P.s = dev_columns[4];
-  P.dp = dev_columns[5];
+  P.x = n > 0 ? dev_columns[0] : nullptr;
+  P.xp = n > 0 ? dev_columns[1] : nullptr;
+  P.y = n > 0 ? dev_columns[2] : nullptr;
+  P.yp = n > 0 ? dev_columns[3] : nullptr;
+  P.s = n > 0 ? dev_columns[4] : nullptr;
+  P.dp = n > 0 ? dev_columns[5] : nullptr;
   P.lost_pass = dev_lost_pass;
   P.lost_elem = dev_lost_element;
 
@@ -2194,29 +2212,23 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   static_sg_weights_kernel<<<(2 * bins + 127) / 128, 128, 0, s>>>(bins, sgHalf, sgOrder, sgdHalf, sgdOrder, S->sg_w,
                                                                   S->sg_idx);
   STATIC_TRY(cudaGetLastError());
-  /* particles alive at the entrance decide whether CSR is computed (csbend.c:1987) */
-  unsigned long long counters[2] = {0, 0};
+  /* particles alive at the entrance decide whether CSR is computed
+   * (csbend.c:1987): counted and turned into the bunch's flags on the device;
+   * the histogram and wake kernels do nothing for an inactive bunch */
   STATIC_TRY(cudaMemsetAsync(S->counters, 0, sizeof(S->counters), s));
   STATIC_TRY(launch_effort(dev_lost_pass, n, 0, 0, &S->counters[0], &S->counters[1], s));
-  STATIC_TRY(cudaMemcpyAsync(counters, S->counters, sizeof(counters), cudaMemcpyDeviceToHost, s));
-  STATIC_TRY(cudaStreamSynchronize(s));
-  const bool more_than_one = counters[1] > 1;
 
   const double Po = p_central;
   const double angle = fabs(p[B2E_BEND_ANGLE]), length = p[B2E_BEND_L], rho0 = d.c[CB_RHO0];
   const double brf = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
   const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
   double csr_constant = 0;
-  if (p[B2E_BEND_CSR] != 0 && more_than_one)
+  if (p[B2E_BEND_CSR] != 0)
     csr_constant = 2 * macro_particle_charge * kE / b2e_pow(3 * rho0 * rho0, 1. / 3.) / (4 * kPI * eps0 * kME * (kC * kC));
   const int g = (int)std::max<int64_t>(1, (n + 255) / 256);
   CsrDevState *dst = &S->state;
-  if (p[B2E_BEND_IGF] != 0 && p[B2E_BEND_STEADY_STATE] == 0) {
-    snprintf(err, errlen, "b2e_csr_bend_static: Must have STEADY_STATE=1 when IGF=1");
-    return B2E_ERR_LATTICE;
-  }
   static_set_bunch_kernel<<<1, 1, 0, s>>>(S, csr_constant,
-                                          -macro_particle_charge / (kME * (kC * kC)) * length / nSlices, more_than_one);
+                                          -macro_particle_charge / (kME * (kC * kC)) * length / nSlices);
   CsrBunches B;
   B.offs = nullptr;
   B.n = 1;
@@ -2225,6 +2237,10 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   B.active = &S->flags[0];
   B.mode = &S->flags[1];
 
+  /* the wake kernel's shared-memory limit is a per-function setting that the
+   * context path also changes: set it for this call's bin count */
+  const size_t wake_smem = sizeof(double) * (4 * bins + 8);
+  STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wake_smem));
   csr_entry_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, Po);
   STATIC_TRY(cudaGetLastError());
   double phiBend = 0;
@@ -2232,8 +2248,6 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);
     csr_slice_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, nullptr, B, kick > 0, bins, Po, 0, 0);
     STATIC_TRY(cudaGetLastError());
-    if (!more_than_one)
-      continue;
     STATIC_TRY(cudaMemsetAsync(S->counts, 0, sizeof(unsigned int) * bins, s));
     int hb = hist_blocks(n, 1);
     csr_hist_kernel<<<dim3(hb, 1), 1024, sizeof(unsigned int) * bins, s>>>(P, n, B, S->counts, bins, brf);
@@ -2270,9 +2284,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     a.const1 = 6.0 - b2e_log(27.0 / 4.0);
     a.q4pe = kE / (4 * kPI * eps0);
     a.igf_factor = 0;
-    size_t smem = sizeof(double) * (4 * bins + 8);
-    STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    csr_wake_kernel<<<1, 1024, smem, s>>>(B, S->counts, a, 0);
+    csr_wake_kernel<<<1, 1024, wake_smem, s>>>(B, S->counts, a, 0);
     STATIC_TRY(cudaGetLastError());
   }
   csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);

@@ -59,10 +59,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-/* Wait for the phase with the given parity to complete; false after the
- * spin limit (the status word gets `code`). */
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned int *status, unsigned int code) {
-  for (uint32_t i = 0; i < B2E_SPIN_LIMIT; i++) {
+/* Wait for the phase with the given parity to complete; false after `limit`
+ * polls (the status word gets `code`). */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned int *status, unsigned int code,
+                                          uint32_t limit = B2E_SPIN_LIMIT) {
+  for (uint32_t i = 0; i < limit; i++) {
     if (mbar_try_wait(bar, parity))
       return true;
     if (status && (i & 1023u) == 1023u && *(volatile unsigned int *)status != ST_OK)

@@ -18,6 +18,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -33,11 +34,16 @@ using namespace umma;
  * mode 0 (K-major):  D[128][64] = A[128][64] . B[64][64]^T  (K = 64)
  * mode 1 (MN-major): D[m][n] = sum_k A[m/64][k][m%64] * B[k][n], A two blocks
  *                    [2][128][64], B [128][64]  (K = 128)
+ * mode 2 (timeout drill): the same kernel, but thread 0 issues no load and
+ *                    waits on the load barrier, which nothing completes,
+ *                    for `spin_limit` polls; it then takes the kernel's
+ *                    timeout path (status ST_TIMEOUT_TMA, the epilogue
+ *                    released without an MMA, TMEM freed) and returns.
  * One CTA of 128 threads; thread 0 issues TMA and MMA, all four warps read
  * TMEM. */
 __global__ void __launch_bounds__(128, 1)
     umma_selftest_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int mode,
-                         float *D, unsigned int *status) {
+                         float *D, unsigned int *status, uint32_t spin_limit) {
   extern __shared__ __align__(1024) unsigned char dsmem[];
   unsigned char *smem = (unsigned char *)(((uintptr_t)dsmem + 1023) & ~(uintptr_t)1023);
   unsigned char *sa = smem;           /* 32 KB: A (mode 0: 16 KB) */
@@ -65,13 +71,13 @@ __global__ void __launch_bounds__(128, 1)
       mbar_expect_tx(&bar_load, 16384 + 8192);
       tma_load_3d(sa, &ta, &bar_load, 0, 0, 0);
       tma_load_3d(sb, &tb, &bar_load, 0, 0, 0);
-    } else {
+    } else if (mode == 1) {
       mbar_expect_tx(&bar_load, 16384 * 2 + 16384);
       tma_load_3d(sa, &ta, &bar_load, 0, 0, 0);
       tma_load_3d(sa + 16384, &ta, &bar_load, 0, 0, 1);
       tma_load_3d(sb, &tb, &bar_load, 0, 0, 0);
-    }
-    if (mbar_wait(&bar_load, 0, status, ST_TIMEOUT_TMA)) {
+    } /* mode 2: nothing will arrive on bar_load */
+    if (mbar_wait(&bar_load, 0, status, ST_TIMEOUT_TMA, spin_limit)) {
       tc_fence_after();
       if (mode == 0) {
         const uint32_t id = idesc_bf16(128, 64, false, false);
@@ -95,7 +101,7 @@ __global__ void __launch_bounds__(128, 1)
     }
   }
   __syncwarp();
-  const bool ok = mbar_wait(&bar_mma, 0, status, ST_TIMEOUT_MMA);
+  const bool ok = mbar_wait(&bar_mma, 0, status, ST_TIMEOUT_MMA, spin_limit);
   tc_fence_after();
   if (ok && *(volatile unsigned int *)status == ST_OK) {
     const int row = warp * 32 + (threadIdx.x & 31);
@@ -463,11 +469,15 @@ cudaError_t launch_wgrad(const CUtensorMap &t_in, const CUtensorMap &t_dz, const
 using namespace b2e;
 
 extern "C" int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b, float *dev_d, void *stream) {
-  if ((mode != 0 && mode != 1) || !dev_a || !dev_b || !dev_d)
+  if (mode < 0 || mode > 2 || (mode < 2 && (!dev_a || !dev_b || !dev_d)))
     return B2E_ERR_ARG;
   CUtensorMap ta, tb;
-  cudaError_t e;
-  if (mode == 0) {
+  memset(&ta, 0, sizeof(ta));
+  memset(&tb, 0, sizeof(tb));
+  cudaError_t e = cudaSuccess;
+  if (mode == 2) {
+    /* the drill loads nothing: no tensor maps */
+  } else if (mode == 0) {
     e = make_tmap_rows64(&ta, dev_a, 128, 1, 128);
     if (e == cudaSuccess)
       e = make_tmap_rows64(&tb, dev_b, 64, 1, 64);
@@ -485,7 +495,8 @@ extern "C" int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b,
   cudaMemsetAsync(status, 0, sizeof(unsigned int), s);
   const size_t smem = 32768 + 16384 + 1024;
   cudaFuncSetAttribute(umma_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  umma_selftest_kernel<<<1, 128, smem, s>>>(ta, tb, mode, dev_d, status);
+  /* the drill's wait gives up after 4096 polls instead of the kernels' limit */
+  umma_selftest_kernel<<<1, 128, smem, s>>>(ta, tb, mode, dev_d, status, mode == 2 ? 4096u : B2E_SPIN_LIMIT);
   e = cudaGetLastError();
   unsigned int st = 0;
   if (e == cudaSuccess)

@@ -1,50 +1,47 @@
 """Algorithmic FP64 operation count per particle-turn, for the roofline.
 
-Counted from the element maps as the reference writes them (multipole.c,
-csbend.c, simple_rfca.c, matrix.c, limit_amplitudes.c): every +, -, *, /,
-sqrt counts 1, an fma counts 2, comparisons and sign flips count 0.  The
-elementary functions count the operations of their implementations in
-elegant_b200/csrc/b2e_math.h (asin on |x| <= 2^-6: 10, on |x| <= 1/8: 24;
-sin or cos kernel on |x| <= 2^-4: 10 / 13, on |x| <= pi/4: 22 / 27; a pi/2
-reduction: 7).  A bend's substep angle decides which sin/cos kernel its
-drift takes; its sin(phi) = p_x / p is taken to be below 2^-6 (stored beams).  Division and sqrt are one
-operation here although the FP64 pipe executes each as a short Newton
-sequence, so the achieved fraction of the DGEMM peak understates pipe
-occupancy; the ncu pipe counters in profiles/ give that directly.
+The count follows the element maps as the reference writes them
+(multipole.c, csbend.c, simple_rfca.c, matrix.c, limit_amplitudes.c): every
++, -, *, / and sqrt counts 1, comparisons and sign flips 0, and every call
+of an elementary function (sin, cos, asin, tan) counts a fixed
+ELEMENTARY_WEIGHT = 20 operations, whatever implementation evaluates it --
+the order of a double-precision polynomial kernel plus its argument
+reduction.  So the figure depends on the lattice and the reference's
+formulas only: making the engine's own sin/cos/asin cheaper, or its
+divisions and square roots (each a short Newton sequence on the FP64 pipe),
+does not move it.  The ncu pipe counters in profiles/ give the hardware
+view (FP64 pipe busy, issue slots busy) beside it.
 """
 from __future__ import annotations
 
 from .lattice import Lattice
 
-ASIN_TINY = 10
-ASIN_SMALL = 24
-SIN_KERNEL = 22
-COS_KERNEL = 27
-SIN_SMALL = 10
-COS_SMALL = 13
-# largest |drift fraction| of the kick integrators: order 2, 4 (Forest-Ruth), 6 (taken as 1)
-MAX_DRIFT_FRAC = {2: 0.5, 4: 1.0 / (2.0 * (2.0 - 2.0 ** (1.0 / 3.0))), 6: 1.0}
-REDUCTION = 7
-TAN = REDUCTION + SIN_KERNEL + COS_KERNEL + 1
+ELEMENTARY_WEIGHT = 20
 
 M2S = 9            # convertMomentaToSlopes: (1+d)^2 - qx^2 - qy^2, sqrt, 2 divisions
 APERTURE_IN = 7    # checkMultAperture, elliptical: x+dx, y+dy, 2 div, 2 mul, add
 APERTURE_AFTER = 5  # elimit_amplitudes: 2 mul, 2 div, add
 DRIFT_SUB = 11     # kick-integrator drift substep: x, y (2 each), s (7)
+BEND_DRIFT_ARITH = 27  # integrate_csbend_ordn drift substep without its elementary functions
+BEND_DRIFT_CALLS = 4   # asin(QX/f), sin and cos of (ds/rho0 + phi), cos(phi)
+BEND_KICK = 14         # its kick: (1 + X/rho0), two products and divisions, the (1+d) round trip
+EDGE_ARITH, EDGE_CALLS = 8, 1   # edge focusing: tan(E - psi/(1+d)) and the products
+RFCA_ARITH, RFCA_CALLS = 44, 1  # energy kick sin(omega t + phase) and the slope update
 
 
 def _nsub(order: int) -> int:
     return {2: 2, 4: 4, 6: 8}[order]
 
 
-def element_flops(e, has_aperture: bool) -> int:
+def element_counts(e, has_aperture: bool) -> tuple[int, int]:
+    """(arithmetic operations, elementary-function calls) of one element."""
     t = e.type
     ap_after = APERTURE_AFTER if has_aperture else 0
     if t == "DRIF":
         order = int(e.get("ORDER")) or 2
-        return (11 if order >= 2 else 6) + ap_after
+        return (11 if order >= 2 else 6) + ap_after, 0
     if t == "EDRIFT":
-        return 11 + ap_after
+        return 11 + ap_after, 0
     if t in ("KQUAD", "KSEXT"):
         integ = int(e.get("INTEGRATION_ORDER"))
         n_kicks = int(e.get("N_KICKS"))
@@ -57,31 +54,32 @@ def element_flops(e, has_aperture: bool) -> int:
             kick += 4 * ((e.get("K1") != 0) + (e.get("J1") != 0))
         per_slice = (APERTURE_IN if has_aperture else 2) + nsub * DRIFT_SUB + (nsub - 1) * (kick + M2S + 4 + M2S)
         mis = 26 if (e.get("DX") or e.get("DY") or e.get("DZ")) else 0
-        return 20 + n_slices * per_slice + (APERTURE_IN if has_aperture else 2) + M2S + 1 + mis + ap_after
+        return 20 + n_slices * per_slice + (APERTURE_IN if has_aperture else 2) + M2S + 1 + mis + ap_after, 0
     if t == "CSBEND":
-        integ = int(e.get("INTEGRATION_ORDER"))
-        nsub = _nsub(integ)
+        nsub = _nsub(int(e.get("INTEGRATION_ORDER")))
         n_slices = int(e.get("N_SLICES"))
-        angle = abs(float(e.get("ANGLE"))) / max(n_slices, 1) * MAX_DRIFT_FRAC.get(integ, 1.0)
-        small = angle + 0.01 <= 2.0 ** -4  # substep angle plus a particle angle within the short kernels
-        sn, cs = (SIN_SMALL, COS_SMALL) if small else (SIN_KERNEL, COS_KERNEL)
-        drift = 4 + 1 + 2 + ASIN_TINY + 2 + sn + cs + 1 + cs + 1 + 6 + 2 + 3 + 1 + 4
-        kick = 10 + 4
-        per_slice = (5 if has_aperture else 0) + nsub * drift + (nsub - 1) * kick
-        edges = (8 + TAN) * ((e.get("EDGE1_EFFECTS") != 0) + (e.get("EDGE2_EFFECTS") != 0))
+        per_slice = (5 if has_aperture else 0) + nsub * BEND_DRIFT_ARITH + (nsub - 1) * BEND_KICK
+        n_edges = (e.get("EDGE1_EFFECTS") != 0) + (e.get("EDGE2_EFFECTS") != 0)
         entry, canon, tail = 23, 9 + 9, 5 + 15 + 30
-        return entry + canon + n_slices * per_slice + tail + edges + ap_after
+        arith = entry + canon + n_slices * per_slice + tail + EDGE_ARITH * n_edges + ap_after
+        return arith, n_slices * nsub * BEND_DRIFT_CALLS + EDGE_CALLS * n_edges
     if t == "RFCA":
-        return 10 + (2 + REDUCTION + SIN_KERNEL + 3) + 2 + 23 + 4 + ap_after
+        return RFCA_ARITH + ap_after, RFCA_CALLS
     if t == "MAXAMP":
-        return ap_after
-    return 0
+        return ap_after, 0
+    return 0, 0
+
+
+def counts_per_particle_turn(lattice: Lattice) -> tuple[int, int]:
+    arith = calls = 0
+    has_ap = any(e.type == "MAXAMP" for e in lattice.elements)
+    for e in lattice.elements:
+        a, c = element_counts(e, has_ap)
+        arith += a
+        calls += c
+    return arith, calls
 
 
 def flops_per_particle_turn(lattice: Lattice) -> int:
-    total, has_ap = 0, any(e.type == "MAXAMP" for e in lattice.elements)
-    seen_ap = False
-    for e in lattice.elements:
-        seen_ap = seen_ap or e.type == "MAXAMP"
-        total += element_flops(e, seen_ap or has_ap)
-    return total
+    arith, calls = counts_per_particle_turn(lattice)
+    return arith + ELEMENTARY_WEIGHT * calls

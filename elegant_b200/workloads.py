@@ -88,8 +88,12 @@ def radiating_ring(isr: bool = False, volt: float = 4e6, edge_angle: float = 0.0
     return Lattice(els)
 
 
-def ring_beam(n: int = 10000, seed: int = 12345, lattice: Lattice | None = None, first_id: int = 1) -> Beam:
-    tw = periodic_twiss(lattice or fodo_ring(rf=False))
+def ring_beam(n: int = 10000, seed: int = 12345, lattice: Lattice | None = None, first_id: int = 1,
+              twiss=None) -> Beam:
+    """twiss: matched optics to use instead of the periodic solution of the
+    lattice (fixture-generated beams pass the values they were made with, so
+    that the libm elementary functions of another host cannot move a bit)."""
+    tw = twiss or periodic_twiss(lattice or fodo_ring(rf=False))
     return gaussian_beam(n, seed, 1e-9, 1e-9, tw.beta_x, tw.alpha_x, tw.beta_y, tw.alpha_y, 3e-3, 1e-3,
                          eta_x=tw.eta_x, etap_x=tw.etap_x, first_id=first_id)
 
@@ -104,10 +108,11 @@ def _cut_gaussian(rng: np.random.Generator, n: int, sigma: float, cutoff: float 
 
 
 def ensemble(n_instances: int = 512, seed: int = 2024, n_min: int = 500, n_max: int = 4000,
-             lattice: Lattice | None = None):
+             lattice: Lattice | None = None, twiss=None):
     """Returns (lattice, beam, offsets, overrides) for a batched error ensemble.
 
-    overrides: list of (element_index, parameter_name, values[n_instances]).
+    overrides: list of (element_index, parameter_name, values[n_instances]);
+    twiss: as for ring_beam.
     """
     lat = lattice or fodo_ring()
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -122,7 +127,7 @@ def ensemble(n_instances: int = 512, seed: int = 2024, n_min: int = 500, n_max: 
             overrides.append((i, "FSE", _cut_gaussian(rng, n_instances, 1e-3)))
         elif e.type == "KSEXT":
             overrides.append((i, "FSE", _cut_gaussian(rng, n_instances, 1e-2)))
-    tw = periodic_twiss(Lattice([e for e in lat.elements if e.type != "RFCA"]))
+    tw = twiss or periodic_twiss(Lattice([e for e in lat.elements if e.type != "RFCA"]))
     parts = []
     next_id = 1
     for i in range(n_instances):

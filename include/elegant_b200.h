@@ -422,7 +422,10 @@ int b2e_csr_surrogate_stats(b2e_ctx *ctx, int64_t *evaluations, int64_t *fallbac
  * Runs one UMMA tile on device buffers to check the operand layouts the wake
  * network uses.  mode 0: D[128][64] = A[128][64] . B[64][64]^T; mode 1:
  * D[m][n] = sum_k A[m/64][k][m%64] * B[k][n] with A [2][128][64], B [128][64].
- * A, B: BF16 row-major; D: FP32.  No counterpart in the reference. */
+ * A, B: BF16 row-major; D: FP32.  mode 2 is a drill of the bounded waits:
+ * the kernel waits on a load that is never issued, gives up after a short
+ * poll limit, frees its tensor memory and returns B2E_ERR_TIMEOUT (buffers
+ * unused, may be NULL).  No counterpart in the reference. */
 int b2e_umma_selftest(int mode, const void *dev_a, const void *dev_b, float *dev_d, void *stream);
 
 /* ---- division self-test -------------------------------------------------
@@ -442,16 +445,24 @@ int b2e_selftest_division(const double *host_b, int32_t n_b, int64_t samples, ui
  * -1 = alive) through one CSRCSBEND, exactly as b2e_track does for that
  * element (same kernels, same results), writing the per-kick wakes
  * (N_KICKS x BINS values) to dev_wakes when it is non-NULL.  It allocates
- * nothing: all working memory is one static device array of ~10.2 MB that
- * the library image carries on every GPU that loads it, for up to
- * B2E_STATIC_MAX_PARTICLES particles and B2E_STATIC_MAX_BINS bins; larger
- * requests are rejected with B2E_ERR_ARG and a message in errbuf.  The first
- * call on a device looks up that array's device address (with the device
- * current); make that first call before any stream capture.  All calls share
- * the array and each clears what it needs; calls that overlap on the GPU
- * race on it and must be serialised by the caller.  stream is a
- * cudaStream_t (NULL = legacy default stream).  p_central is beta*gamma;
- * macro_particle_charge is CHARGE TOTAL divided by the particle count. */
+ * nothing: all working memory is one static device array of ~10.2 MB in the
+ * library image, for up to B2E_STATIC_MAX_PARTICLES particles and
+ * B2E_STATIC_MAX_BINS bins; larger requests are rejected with B2E_ERR_ARG and
+ * a message in errbuf.  The first call on a device is its set-up: with that
+ * device current it looks up the array's device address, which is also when
+ * CUDA (lazy module loading, the default) gives the array and the kernels'
+ * code their device memory; the array then stays until the process exits.  A
+ * caller whose memory pool will own the whole card makes that first call
+ * (n = 0 is enough, with NULL particle buffers) before the pool takes the
+ * memory, or runs with
+ * CUDA_MODULE_LOADING=EAGER; the first call also comes before any stream
+ * capture.  The set-up is per primary context: do not call this on a device
+ * after cudaDeviceReset.  A call only enqueues work on the stream and returns
+ * without waiting for the GPU.  All calls share the array and each clears
+ * what it needs; calls that overlap on the GPU race on it and must be
+ * serialised by the caller.  stream is a cudaStream_t (NULL = legacy default
+ * stream).  p_central is beta*gamma; macro_particle_charge is CHARGE TOTAL
+ * divided by the particle count. */
 #define B2E_STATIC_MAX_PARTICLES 1048576
 #define B2E_STATIC_MAX_BINS 2048
 int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lost_pass, int32_t *dev_lost_element, int64_t n,

@@ -1885,6 +1885,12 @@ void b2e_oracle_wake_t1(const double *counts, long nBins, double slippage_bins, 
   free(denom);
 }
 
+/* The project's Savitzky-Golay filter (b2e_sg.h) on one array, in place, for
+ * tests against independent implementations; returns 1 on success. */
+long b2e_oracle_sg_apply(double *data, long rows, long order, long nLeft, long nRight, long deriv) {
+  return b2e_sg_apply_host(data, rows, order, nLeft, nRight, deriv);
+}
+
 /* SolveForPhiStupakov restated, for unit tests of the root finders;
  * *phi_last is the carried start value (-1 before the first solve) */
 double b2e_oracle_stupakov_phi(double x, double ds, double phim, double *phi_last) {

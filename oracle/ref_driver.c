@@ -43,7 +43,10 @@ static const B2E_REF_TYPE b2e_ref_types[] = {
   {"DRIF", T_DRIF}, {"DRIFT", T_DRIF}, {"EDRIFT", T_EDRIFT}, {"KQUAD", T_KQUAD},
   {"KSEXT", T_KSEXT}, {"CSBEND", T_CSBEND}, {"SBEN", T_CSBEND}, {"RFCA", T_RFCA},
   {"MAXAMP", T_MAXAMP}, {"MARK", T_MARK}, {"CHARGE", T_CHARGE},
-  {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {"MALIGN", T_MALIGN}, {NULL, 0}};
+  {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {"MALIGN", T_MALIGN},
+  /* built but not tracked by the restated loop: lets the adapter's tests
+   * hand it an element type outside the engine's set */
+  {"SEXT", T_SEXT}, {NULL, 0}};
 
 /* offset_beam (do_tracking.c:3243-3300) restated: do_tracking.c is not part
  * of the compiled subset */
@@ -231,6 +234,62 @@ static void record_lost(double **coord, long nLeft, long nToTrack, long pass) {
 static double *wake_out = NULL;
 static long wake_cap = 0, wake_count = 0;
 
+/* Fiducial time of the last zero-length RFCA fiducialised in a run: the same
+ * findFiducialTime call, on the same particles, that simple_rf_cavity makes
+ * on its first pass (simple_rfca.c:421-431 with length 0, so s0 = zEnd and
+ * sOffset = 0).  A run split over particle slices passes it back as
+ * T_REFERENCE (simple_rfca.c:428-429), so that every slice uses the phase of
+ * the whole beam. */
+static double last_fiducial_t0 = -1;
+
+double b2e_ref_last_fiducial_t0(void) { return last_fiducial_t0; }
+
+/* Optional per-pass history of the survivors: [pass][5] = survivors, <x>,
+ * <y>, and the rms emittances sqrt(<dx^2><dx'^2> - <dx dx'>^2) per plane
+ * (the form of rms_emittance, final_props.c:844-880), recorded after the
+ * last element of every pass.  Two-pass sums in particle order. */
+static double *history_out = NULL;
+static long history_passes = 0;
+
+void b2e_ref_set_history(double *buffer, long n_passes) {
+  history_out = buffer;
+  history_passes = buffer ? n_passes : 0;
+}
+
+static void record_history(double **coord, long n, long pass) {
+  double m[4] = {0, 0, 0, 0}, s[6] = {0, 0, 0, 0, 0, 0}, *h, ex, ey;
+  long i, k;
+  if (!history_out || pass >= history_passes)
+    return;
+  h = history_out + 5 * pass;
+  h[0] = n;
+  h[1] = h[2] = h[3] = h[4] = 0;
+  if (!n)
+    return;
+  for (i = 0; i < n; i++)
+    for (k = 0; k < 4; k++)
+      m[k] += coord[i][k];
+  for (k = 0; k < 4; k++)
+    m[k] /= n;
+  for (i = 0; i < n; i++) {
+    double dx = coord[i][0] - m[0], dxp = coord[i][1] - m[1], dy = coord[i][2] - m[2], dyp = coord[i][3] - m[3];
+    s[0] += dx * dx;
+    s[1] += dxp * dxp;
+    s[2] += dx * dxp;
+    s[3] += dy * dy;
+    s[4] += dyp * dyp;
+    s[5] += dy * dyp;
+  }
+  for (k = 0; k < 6; k++)
+    s[k] /= n;
+  ex = s[0] * s[1] - s[2] * s[2];
+  ey = s[3] * s[4] - s[5] * s[5];
+  h[1] = m[0];
+  h[2] = m[2];
+  h[3] = ex > 0 ? sqrt(ex) : 0;
+  h[4] = ey > 0 ? sqrt(ey) : 0;
+}
+
 long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long np, long n_passes,
                    double *rows_out, long *n_left, double *effort, double *wake_buffer, long wake_capacity,
                    long *wake_written, char *errbuf, long errlen) {
@@ -267,6 +326,7 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
   wake_out = wake_buffer;
   wake_cap = wake_capacity;
   wake_count = 0;
+  last_fiducial_t0 = -1;
 
   if (setjmp(b2e_ref_trap)) {
     b2e_ref_trap_armed = 0;
@@ -349,9 +409,16 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
           maxampExponent = maxamp->exponent;
           maxampYExponent = maxamp->yExponent;
           break;
-        case T_RFCA:
-          nLeft = simple_rf_cavity(coord, nToTrack, (RFCA *)eptr->p_elem, NULL, &P_central, z_travel);
+        case T_RFCA: {
+          RFCA *rf = (RFCA *)eptr->p_elem;
+          if (!rf->fiducial_seen && rf->tReference == -1 && rf->length == 0) {
+            unsigned long mode = parseFiducialMode(rf->fiducial);
+            if (mode)
+              last_fiducial_t0 = findFiducialTime(coord, nToTrack, z_travel, 0.0, P_central, mode);
+          }
+          nLeft = simple_rf_cavity(coord, nToTrack, rf, NULL, &P_central, z_travel);
           break;
+        }
         case T_EDRIFT:
           exactDrift(coord, nToTrack, ((EDRIFT *)eptr->p_elem)->length);
           break;
@@ -403,6 +470,7 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
       eptr = eptr->succ;
     }
     *effort += nLeft;
+    record_history(coord, nToTrack, i_pass);
   }
 
   for (i = 0; i < np; i++)
@@ -422,3 +490,44 @@ unsigned long b2e_ref_type_flags(const char *type_name) {
   (void)compute_offsets;
   return type < 0 ? 0 : entity_description[type].flags;
 }
+
+#ifdef B2E_REF_WITH_ADAPTER
+/* The drop-in adapter (elegant_b200/adapter) driven from an element list
+ * built here from the reference's own tables, exactly as b2e_ref_track
+ * builds it: the rows go through b2e_adapter_track (the engine on the GPU)
+ * instead of the restated do_tracking loop.  Returns the adapter's status
+ * (survivors, or -1 / -2). */
+#include "b2e_adapter.h"
+
+long b2e_ref_adapter_track(const char *lattice, double p_central, double *rows_in, long np, long n_passes,
+                           double *rows_out, double *effort, char *errbuf, long errlen) {
+  ELEMENT_LIST *line;
+  double **coord;
+  long nElems = 0, i, j, status;
+  static int offsets_done = 0;
+  if (!offsets_done) {
+    compute_offsets();
+    offsets_done = 1;
+  }
+  b2e_ref_errmsg[0] = 0;
+  if (!(line = build_line(lattice, &nElems))) {
+    if (errbuf && errlen > 0)
+      snprintf(errbuf, errlen, "%s", b2e_ref_errmsg);
+    return -3;
+  }
+  coord = (double **)czarray_2d(sizeof(double), np ? np : 1, totalPropertiesPerParticle);
+  for (i = 0; i < np; i++) {
+    for (j = 0; j < 7; j++)
+      coord[i][j] = rows_in[i * 7 + j];
+    coord[i][lossPassIndex] = -1;
+    coord[i][bunchIndex] = 0;
+    coord[i][weightIndex] = 1;
+  }
+  status = b2e_adapter_track(coord, np, line, p_central, n_passes, 2, effort, errbuf, errlen);
+  for (i = 0; i < np; i++)
+    for (j = 0; j < 8; j++)
+      rows_out[i * 8 + j] = coord[i][j];
+  free_czarray_2d((void **)coord, np ? np : 1, totalPropertiesPerParticle);
+  return status;
+}
+#endif

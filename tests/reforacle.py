@@ -53,13 +53,33 @@ class RefOracle:
         else:
             self.lib = ctypes.CDLL(path)
         self.lib.b2e_ref_track.restype = ctypes.c_long
+        self.lib.b2e_ref_last_fiducial_t0.restype = ctypes.c_double
         self.math = math
+        self.last_history = None
 
-    def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0, capture_wakes=False):
+    def last_fiducial_t0(self) -> float:
+        """Fiducial time the last run's zero-length RFCA computed on its first
+        pass (findFiducialTime on the particles it received); -1 if none."""
+        return float(self.lib.b2e_ref_last_fiducial_t0())
+
+    def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0, capture_wakes=False,
+              history=False):
         """Returns (rows, n_left, effort, wakes); rows are the reference's final
         particle array (x, xp, y, yp, s, delta, id, lossPass), survivors first.
         With capture_wakes, every CSRCSBEND writes its per-kick DeltaGamma through
-        the reference's own OUTPUT_FILE path (captured in memory), returned as wakes."""
+        the reference's own OUTPUT_FILE path (captured in memory), returned as wakes.
+        With history, ``last_history`` holds [pass][survivors, <x>, <y>, ex, ey]
+        of the survivors after every pass."""
+        hist = np.zeros((max(n_passes, 1), 5)) if history else None
+        self.lib.b2e_ref_set_history(hist.ctypes.data_as(ctypes.c_void_p) if history else None,
+                                     ctypes.c_long(n_passes if history else 0))
+        try:
+            return self._track(lattice, coords, ids, p_central, n_passes, wake_capacity, capture_wakes)
+        finally:
+            self.lib.b2e_ref_set_history(None, ctypes.c_long(0))
+            self.last_history = hist[:n_passes] if history else None
+
+    def _track(self, lattice, coords, ids, p_central, n_passes, wake_capacity, capture_wakes):
         n = coords.shape[0]
         rows = np.zeros((n, 7))
         rows[:, :6] = coords
@@ -87,6 +107,59 @@ class RefOracle:
             self.lib.b2e_ref_capture_get(0, buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(k))
             return out[:n], nl.value, eff.value, buf[:k]
         return out[:n], nl.value, eff.value, wakes[: ww.value]
+
+
+def with_fiducial(lattice, t0: float):
+    """The lattice with T_REFERENCE = t0 on its RFCA elements."""
+    from elegant_b200.lattice import Element, Lattice
+    return Lattice([Element(e.name, e.type, dict(e.params, T_REFERENCE=t0)) if e.type == "RFCA" else e
+                    for e in lattice.elements])
+
+
+def _pool(processes):
+    """Spawned worker processes (never forked: the parent may hold a CUDA
+    context); a worker that dies raises BrokenProcessPool instead of hanging."""
+    import concurrent.futures
+    import multiprocessing as mp
+    return concurrent.futures.ProcessPoolExecutor(processes, mp_context=mp.get_context("spawn"))
+
+
+def _split_worker(args):
+    math, lattice, coords, ids, p_central, n_passes, history = args
+    ref = RefOracle(math)
+    rows, nl, eff, _ = ref.track(lattice, coords, ids, p_central, n_passes, history=history)
+    return rows, nl, eff, ref.last_history
+
+
+def track_split(math, lattice, coords, ids, p_central, n_passes, processes=None):
+    """The reference's tracking of one beam, spread over particle slices in
+    spawned processes.  Particles of a ring are independent except through the
+    RFCA's TMEAN fiducial (the Kahan mean over the whole beam on the first
+    pass, simple_rfca.c:179-230), so the whole beam is tracked for one pass
+    first, its fiducial time is read back and every slice is given it as
+    T_REFERENCE.  Returns (rows by slice, concatenated; n_left; effort; t0)."""
+    n = coords.shape[0]
+    ref = RefOracle(math)
+    ref.track(lattice, coords, ids, p_central, 1)
+    t0 = ref.last_fiducial_t0()
+    lat = with_fiducial(lattice, t0) if t0 != -1 else lattice
+    processes = processes or os.cpu_count() or 1
+    bounds = np.linspace(0, n, processes + 1).astype(int)
+    jobs = [(math, lat, coords[a:b], ids[a:b], p_central, n_passes, False) for a, b in zip(bounds[:-1], bounds[1:])
+            if b > a]
+    with _pool(len(jobs)) as pool:
+        res = list(pool.map(_split_worker, jobs))
+    rows = np.concatenate([r[0] for r in res])
+    return rows, sum(r[1] for r in res), sum(r[2] for r in res), t0
+
+
+def track_instances(math, jobs, processes=None):
+    """Independent reference runs in spawned processes: jobs are
+    (lattice, coords, ids, p_central, n_passes, history) tuples; returns
+    [(rows, n_left, effort, history)] in job order."""
+    processes = min(processes or os.cpu_count() or 1, len(jobs))
+    with _pool(processes) as pool:
+        return list(pool.map(_split_worker, [(math, *j) for j in jobs]))
 
 
 def by_id(rows):

@@ -68,6 +68,22 @@ def test_chicane_csrdrift_multiple_kicks(ref_b2e):
     check(*run_both(ref_b2e, Lattice(els), beam))
 
 
+def test_chicane_with_exact_drifts(ref_b2e):
+    """EDRIFT before the first dipole, between a CSRDRIFT and the next dipole
+    and after the last one (exactDrift, csbend.c:3767-3790)."""
+    lat = w.chicane(bins=150, n_kicks=5)
+    els = []
+    for e in lat.elements:
+        if e.name == "B1":
+            els.append(Element("E0", "EDRIFT", {"L": 0.3}))
+        if e.name == "B2":
+            els.append(Element("E1", "EDRIFT", {"L": 0.2}))
+        els.append(e)
+    els.append(Element("E2", "EDRIFT", {"L": 1.0}))
+    beam = w.chicane_beam(12000, seed=19)
+    check(*run_both(ref_b2e, Lattice(els), beam))
+
+
 def test_chicane_without_charge_is_plain_tracking(ref_b2e):
     lat = w.chicane(bins=100, n_kicks=3, charge=0.0)
     beam = w.chicane_beam(5000, seed=2)

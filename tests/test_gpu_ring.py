@@ -346,3 +346,18 @@ def test_lattice_too_large_for_shared_memory(ref_b2e):
     res = gpu_track(lat, beam, w.ring_p_central(), 2)
     rows, nl, _, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 2)
     assert_parity(res, rows, nl)
+
+
+def test_ring_with_exact_drifts(ref_b2e):
+    """EDRIFT (exactDrift, csbend.c:3767-3790) in place of the second drift of
+    every cell, with losses: bit-identical to the reference."""
+    els = [Element(e.name, "EDRIFT", {"L": e.params["L"]}) if e.name == "D2" else e for e in w.fodo_ring().elements]
+    lat = Lattice(els)
+    assert sum(e.type == "EDRIFT" for e in lat.elements) == 8
+    beam = Beam(np.concatenate([w.ring_beam(200, seed=6).coords, _lossy_beam(200, seed=8).coords]),
+                np.arange(1, 401))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 200 <= nl < 400
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

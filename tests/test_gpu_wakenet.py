@@ -41,6 +41,28 @@ def test_umma_operand_layouts(mode):
     assert err < 1e-3 * ref.abs().max().item(), err
 
 
+def test_bounded_wait_gives_up_and_frees_tensor_memory():
+    """The timeout drill: a kernel whose load barrier never completes stops
+    waiting after its poll limit, reports B2E_ERR_TIMEOUT through its status
+    word, frees its tensor memory and exits -- no trap, and the context stays
+    usable: the drill runs again, then a real tile computes correctly."""
+    import torch
+    lib = _lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        assert lib.b2e_umma_selftest(2, None, None, None, stream) == -6  # B2E_ERR_TIMEOUT
+    torch.cuda.synchronize()
+    g = torch.Generator().manual_seed(11)
+    a = torch.randn(128, 64, generator=g).to(torch.bfloat16)
+    b = torch.randn(64, 64, generator=g).to(torch.bfloat16)
+    d = torch.full((128, 64), float("nan"), dtype=torch.float32, device="cuda")
+    da, db = a.cuda(), b.cuda()
+    assert lib.b2e_umma_selftest(0, da.data_ptr(), db.data_ptr(), d.data_ptr(), stream) == 0
+    torch.cuda.synchronize()
+    ref = a.double() @ b.double().T
+    assert (d.cpu().double() - ref).abs().max().item() < 1e-3 * ref.abs().max().item()
+
+
 import os
 import sys
 

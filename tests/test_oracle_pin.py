@@ -269,3 +269,17 @@ def test_histogram_filter_transform_against_numpy(n, cut):
         f(ours.ctypes.data, n, *cut, clip)
         ref = _numpy_lh(h, *cut, clip)
         assert np.allclose(ours, ref, rtol=1e-11, atol=1e-11 * h.max()), (clip, np.abs(ours - ref).max())
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_with_exact_drifts(math):
+    """EDRIFT (exactDrift, csbend.c:3767-3790) in the ring, with losses."""
+    from elegant_b200 import Element, Lattice
+    lat = Lattice([Element(e.name, "EDRIFT", {"L": e.params["L"]}) if e.name == "D2" else e
+                   for e in w.fodo_ring().elements])
+    beam = lossy_beam(150, seed=13)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])

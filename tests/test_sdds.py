@@ -1,10 +1,50 @@
-"""SDDS output in elegant's phase-space and loss layouts (CPU)."""
+"""SDDS output in elegant's phase-space, loss and caller layouts (CPU).
+
+Every file is read back with tests/sdds_protocol.py, a reader written from
+the SDDS protocol apart from the writer (elegant_b200.sdds), which itself
+reads every SDDS file the reference ships (binary in both byte orders and
+ASCII, with and without row counts)."""
+import glob
+import os
+
 import numpy as np
 import pytest
 
 from elegant_b200 import workloads as w
-from elegant_b200.sdds import read_sdds, write_losses, write_phase_space
+from elegant_b200.sdds import write_losses, write_phase_space
 from elegant_b200.track import TrackResult
+from sdds_protocol import SddsFile
+
+REFERENCE = os.environ.get("ELEGANT_REFERENCE_TREE", "/root/reference")
+
+
+def read_sdds(path):
+    """(parameters, columns) of a one-page file, by the independent reader."""
+    f = SddsFile(path)
+    assert len(f.pages) == 1
+    return f.pages[0]["parameters"], f.pages[0]["columns"]
+
+
+def column_type(path, name):
+    return next(c["type"] for c in SddsFile(path).columns if c["name"] == name)
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="needs the reference tree")
+def test_reader_reads_the_reference_sdds_files():
+    """The protocol reader against files the SDDS toolkit wrote: every page
+    read to the last byte (binary) or line (ASCII), with columns of equal
+    length, in all three encodings."""
+    files = sorted(glob.glob(os.path.join(REFERENCE, "**", "*.sdds"), recursive=True))
+    assert len(files) > 50
+    modes = set()
+    for path in files:
+        f = SddsFile(path)
+        modes.add((f.mode, f.endian if f.mode == "binary" else ""))
+        assert f.pages, path
+        for page in f.pages:
+            lengths = {len(v) for v in page["columns"].values()}
+            assert len(lengths) <= 1, path
+    assert {("binary", ">"), ("binary", "<"), ("ascii", "")} <= modes
 
 
 def _result():
@@ -61,7 +101,7 @@ def test_caller_outputs_round_trip(tmp_path, mode):
     pv, c = read_sdds(p)
     assert pv["Step"] == 2 and c["ElementName"] == ["QF", "QF"] and list(c["ElementOccurence"]) == [1, 2]
     assert list(c["deltaNegative"]) == [-0.01, 0.0123] and list(c["deltaNegativeFound"]) == [1, 0]
-    assert list(c["lostOnPassPositive"]) == [7, 7] and c["deltaPositiveFound"].dtype == np.int16
+    assert list(c["lostOnPassPositive"]) == [7, 7] and column_type(p, "deltaPositiveFound") == "short"
     fm = [{"x": 1e-3, "y": 2e-3, "delta": 0.0, "nux": 0.21, "nuy": 0.33, "s": 30.4, "dnux": 1e-7, "dnuy": 2e-7,
            "dnu": 2.2e-7, "dx": 0.0, "dy": 0.0, "diffusion": -13.3, "diffusionRate": -15.0}]
     p = tmp_path / f"fma.{mode}"
