@@ -22,6 +22,7 @@ ERRORS = {
     -7: "device fault flag",
 }
 
+CSR_PAGE_HEADER = 12  # B2E_CSR_PAGE_HEADER
 # element type codes (include/elegant_b200.h)
 DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT, MALIGN = range(1, 13)
 MAX_PARAMS = 40
@@ -94,6 +95,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_load_ensemble": (c_int, [vp, ctypes.c_int32, vp, ctypes.POINTER(Override), ctypes.c_int32]),
         "b2e_ensemble_history": (c_int, [vp, vp, vp, vp, vp, vp]),
         "b2e_csr_wakes": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
+        "b2e_set_csr_pages": (c_int, [vp, ctypes.c_int32]),
+        "b2e_set_csr_timing": (c_int, [vp, ctypes.c_int32]),
+        "b2e_csr_timing": (c_int, [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+        "b2e_csr_pages": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
         "b2e_stream": (vp, [vp]),
         "b2e_kernel_launches": (i64, [vp]),
         "b2e_history_passes": (i64, [vp]),

@@ -104,6 +104,20 @@ def run(n_bunches=16, n_min=500_000, n_max=4_000_000, net_path=DEFAULT_NET, tole
             ms = sum(times) / len(times)
             r = {"run_ms": ms, "particle_kicks_per_s": n * kicks / (ms / 1e3), "per_bunch": bunch_moments(cols, lost,
                                                                                                       offsets)}
+            # one more run with the wake stage of every kick bracketed by
+            # events: the engine's own per-kick cost of this path's wake
+            # (plain kernel, or filter + network + combine), all bunches
+            for c, c0 in zip(cols, init):
+                c.copy_(c0)
+            lost.fill_(-1)
+            lost_e.fill_(-1)
+            t.set_csr_timing(True)
+            t.track_device(cols, lost, lost_e)
+            wt = t.csr_wake_timing()
+            t.set_csr_timing(False)
+            r["wake_stage_ms_per_kick"] = wt["ms_per_kick"]
+            r["wake_stage_kicks"] = wt["kicks"]
+            r["wake_stage_learned_kicks"] = wt["learned_kicks"]
             if mode == "surrogate":
                 st = t.csr_surrogate_stats()
                 errs = st["gate_errors"]
@@ -117,6 +131,8 @@ def run(n_bunches=16, n_min=500_000, n_max=4_000_000, net_path=DEFAULT_NET, tole
                                              for p, s in zip(pb, sb))
     result["emit_x_rel_diff_max"] = max(abs(s["emit_x"] - p["emit_x"]) / p["emit_x"] for p, s in zip(pb, sb))
     result["surrogate_vs_plain_time"] = result["surrogate"]["run_ms"] / result["plain"]["run_ms"]
+    result["wake_stage_learned_vs_plain_time"] = (result["surrogate"]["wake_stage_ms_per_kick"] /
+                                                  result["plain"]["wake_stage_ms_per_kick"])
     return result
 
 

@@ -949,6 +949,34 @@ extern "C" int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int6
   return csr_copy_wakes(ctx->csr, wakes, capacity, written, ctx->err);
 }
 
+extern "C" int b2e_set_csr_pages(b2e_ctx *ctx, int32_t record) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  ctx->csr.record_pages = record != 0;
+  return B2E_OK;
+}
+
+extern "C" int b2e_set_csr_timing(b2e_ctx *ctx, int32_t on) {
+  if (!ctx)
+    return B2E_ERR_ARG;
+  ctx->csr.time_wake = on != 0;
+  return B2E_OK;
+}
+
+extern "C" int b2e_csr_timing(b2e_ctx *ctx, double *wake_ms, int64_t *kicks, int64_t *learned_kicks) {
+  if (!ctx || !wake_ms || !kicks || !learned_kicks)
+    return B2E_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return csr_wake_timing(ctx->csr, wake_ms, kicks, learned_kicks, ctx->err);
+}
+
+extern "C" int b2e_csr_pages(b2e_ctx *ctx, double *pages, int64_t capacity, int64_t *written) {
+  if (!ctx || !written)
+    return B2E_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return csr_copy_pages(ctx->csr, pages, capacity, written, ctx->err);
+}
+
 extern "C" int b2e_set_csr_surrogate(b2e_ctx *ctx, b2e_wakenet *net, const double feature_scales[3], double tolerance,
                                      int32_t gate_stride) {
   if (!ctx)

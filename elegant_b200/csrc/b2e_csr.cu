@@ -191,7 +191,9 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
     Q1 = XP * f;
     Q3 = YP * f;
     const RadSite no_rad = {0, 0, 0, 0, 0, nullptr};
-    int lost = csbend_integrate<false>(X, Q1, Y, Q3, Q4, DP, c, 1, (int)c[CB_NSUB], false, ap, e, no_rad);
+    const int nsub = (int)c[CB_NSUB];
+    int lost = B2E_UNROLL >= 1 && nsub == 4 ? csbend_integrate<false, 4>(X, Q1, Y, Q3, Q4, DP, c, 1, nsub, false, ap, e, no_rad)
+                         : csbend_integrate<false>(X, Q1, Y, Q3, Q4, DP, c, 1, nsub, false, ap, e, no_rad);
     f = 1 / sqrt(((1 + DP) * (1 + DP) - Q1 * Q1) - Q3 * Q3);
     Q1 = Q1 * f;
     Q3 = Q3 * f;
@@ -319,6 +321,10 @@ struct WakeArgs {
   double slippage, slippage13, c1, c2, csr_constant;
   double length, nSlices;   /* element length and kicks: c1 and c2 of each bunch */
   double *wakelog;          /* nBins values per bunch for this kick, or null */
+  /* page record (CSRCSBEND OUTPUT_FILE): B2E_CSR_PAGE_HEADER + 4 nBins values
+   * per bunch for this kick, or null; the header's host-known fields */
+  double *pagelog;
+  double page_element, page_kick, page_angle, page_ds_kick, page_p_central, page_range_factor;
   /* integrated Green's function (csbend.c:2593-2621, :2676-2680) */
   int igf;
   double gamma2, gamma3, rho0, const1, q4pe, igf_factor;
@@ -634,15 +640,22 @@ __device__ void igf_wake(const WakeArgs &a, const double dct, const double *hist
  * are set. */
 template <typename CountT, typename SumT>
 __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double dct, double *sm, double *dgamma,
-                          SumT *nbinned_out, double *hist_out, double *deriv_out) {
+                          SumT *nbinned_out, double *hist_out, double *deriv_out, double *page = nullptr) {
   const int nb = a.nBins;
   wake_filters<CountT, SumT>(counts, a, dct, sm, nbinned_out);
   const double *hist = sm, *deriv = sm + nb, *denom = sm + 2 * nb;
+  double *page_t1 = page ? page + 2 * nb : nullptr, *page_t2 = page ? page + 3 * nb : nullptr;
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     if (hist_out)
       hist_out[b] = hist[b];
     if (deriv_out)
       deriv_out[b] = deriv[b];
+    if (page) {
+      page[b] = hist[b];
+      page[nb + b] = deriv[b];
+      page_t1[b] = 0; /* the IGF path and an empty range leave T1 and T2 at zero */
+      page_t2[b] = 0;
+    }
   }
   long long diS, diS4;
   slippage_bins(a, dct, &diS, &diS4);
@@ -669,6 +682,10 @@ __device__ void wake_body(const CountT *counts, const WakeArgs &a, const double 
     dgamma[ib] = dg;
     if (a.wakelog)
       a.wakelog[ib] = dg;
+    if (page) {
+      page_t1[ib] = T1;
+      page_t2[ib] = T2;
+    }
   }
 }
 
@@ -687,6 +704,30 @@ __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, unsigne
   const double csr_constant = B.csr_const[bunch], igf_factor = B.csr_const[B.n + bunch];
   CsrDevState *st = B.st + bunch;
   const double dct = st->dct;
+  double *page = nullptr;
+  if (a.pagelog) {
+    page = a.pagelog + (size_t)bunch * (B2E_CSR_PAGE_HEADER + 4 * a.nBins);
+    if (threadIdx.x == 0) {
+      /* the binning's range, as the histogram kernel formed it; a bunch
+       * without CSR on this kick gets element index -1 and no arrays */
+      double lower = value_of(st->ct_min_key), upper = value_of(st->ct_max_key);
+      expand_range(&lower, &upper, a.page_range_factor);
+      page[0] = active ? a.page_element : -1.0;
+      page[1] = a.page_kick;
+      page[2] = bunch;
+      page[3] = a.nBins;
+      page[4] = lower;
+      page[5] = upper;
+      page[6] = dct;
+      page[7] = a.slippage;
+      page[8] = a.page_angle;
+      page[9] = a.page_ds_kick;
+      page[10] = a.page_p_central;
+      page[11] = B.csr_const[3 * B.n + bunch];
+    }
+    __syncthreads(); /* the keys are read before they are emptied below */
+    page += B2E_CSR_PAGE_HEADER;
+  }
   if (recycle && threadIdx.x == 0) {
     st->ct_min_key = ~0ull;
     st->ct_max_key = 0ull;
@@ -700,7 +741,7 @@ __global__ void __launch_bounds__(1024, 1) csr_wake_kernel(CsrBunches B, unsigne
   w.igf_factor = igf_factor;
   w.wakelog = a.wakelog ? a.wakelog + (size_t)bunch * a.nBins : nullptr;
   unsigned int *counts = counts_all + (size_t)bunch * a.nBins;
-  wake_body<unsigned int, long long>(counts, w, dct, sm, st->dGamma, &st->nBinned, nullptr, nullptr);
+  wake_body<unsigned int, long long>(counts, w, dct, sm, st->dGamma, &st->nBinned, nullptr, nullptr, page);
   if (recycle) /* the counts were copied to shared memory before the first barrier */
     for (int b = threadIdx.x; b < a.nBins; b += blockDim.x)
       counts[b] = 0;
@@ -1393,7 +1434,7 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
   st.macro_charge.assign(n_bunches, 0.0);
   if (cudaMalloc(&st.d_state, sizeof(CsrDevState) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_counts, sizeof(unsigned int) * B2E_CSR_MAX_BINS * n_bunches) != cudaSuccess ||
-      cudaMalloc(&st.d_csr_const, 3 * sizeof(double) * n_bunches) != cudaSuccess ||
+      cudaMalloc(&st.d_csr_const, 4 * sizeof(double) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_flags, 2 * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_alive, sizeof(unsigned long long) * n_bunches) != cudaSuccess ||
       cudaMalloc(&st.d_keys, 2 * sizeof(unsigned long long) * n_bunches) != cudaSuccess) {
@@ -1401,7 +1442,7 @@ int csr_set_bunches(CsrState &st, int n_bunches, const int64_t *d_offsets, std::
     return B2E_ERR_NOMEM;
   }
   cudaMemset(st.d_state, 0, sizeof(CsrDevState) * n_bunches);
-  cudaMemset(st.d_csr_const, 0, 3 * sizeof(double) * n_bunches);
+  cudaMemset(st.d_csr_const, 0, 4 * sizeof(double) * n_bunches);
   cudaMemset(st.d_flags, 0, 2 * n_bunches);
   csr_init_state_kernel<<<1, 256>>>((CsrDevState *)st.d_state, n_bunches);
   if (cudaDeviceSynchronize() != cudaSuccess) {
@@ -1487,12 +1528,30 @@ static int reduce_keys(CsrState &st, const CsrBunches &B, cudaStream_t stream, s
 void csr_reset(CsrState &st) {
   st.wakes_host.clear();
   st.wake_values = 0;
+  st.page_values = 0;
+  st.timed_kicks = st.timed_learned = 0;
   st.gate_values = 0;
   if (st.d_sur_counts)
     cudaMemset(st.d_sur_counts, 0, 2 * sizeof(unsigned long long));
   st.accumulated_angle = 0;
   st.wake_valid.assign(st.n_bunches, 0);
   st.last_bend = -1;
+}
+
+static int ensure_pagelog(CsrState &st, int64_t values) {
+  if (values <= st.pagelog_cap)
+    return B2E_OK;
+  double *p = nullptr;
+  if (cudaMalloc(&p, sizeof(double) * values) != cudaSuccess)
+    return B2E_ERR_NOMEM;
+  if (st.d_pagelog) {
+    if (st.page_values)
+      cudaMemcpy(p, st.d_pagelog, sizeof(double) * st.page_values, cudaMemcpyDeviceToDevice);
+    cudaFree(st.d_pagelog);
+  }
+  st.d_pagelog = p;
+  st.pagelog_cap = values;
+  return B2E_OK;
 }
 
 static int ensure_wakelog(CsrState &st, int64_t values) {
@@ -1788,11 +1847,16 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     err = "CSR wake log allocation failed";
     return B2E_ERR_NOMEM;
   }
+  const int64_t page_stride = B2E_CSR_PAGE_HEADER + 4 * (int64_t)ce.bins;
+  if (st.record_pages && ensure_pagelog(st, st.page_values + (int64_t)ce.nSlices * nbunch * page_stride)) {
+    err = "CSR page record allocation failed";
+    return B2E_ERR_NOMEM;
+  }
   st.ds0 = ce.length / ce.nSlices;
   st.zLast = st.z0 = ce.z_end;
   /* CSRConstant (csbend.c:2378-2381), per bunch */
   const double eps0 = 1 / ((4 * kPI * 1e-7) * kC * kC);
-  std::vector<double> csr_constant(3 * nbunch, 0.0);
+  std::vector<double> csr_constant(4 * nbunch, 0.0);
   for (int b = 0; b < nbunch; b++) {
     if (ce.csr && flags[b])
       csr_constant[b] = 2 * st.macro_charge[b] * kE / b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) /
@@ -1801,8 +1865,10 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     csr_constant[nbunch + b] = -st.macro_charge[b] / (kME * (kC * kC)) * ce.length / ce.nSlices;
     /* GSConstant for a Stupakov CSRDRIFT (csbend.c:2999) */
     csr_constant[2 * nbunch + b] = csr_constant[b] * b2e_pow(3 * ce.rho0 * ce.rho0, 1. / 3.) / 2;
+    /* the macro-particle charge, for the page record */
+    csr_constant[3 * nbunch + b] = st.macro_charge[b];
   }
-  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), 3 * sizeof(double) * nbunch, cudaMemcpyHostToDevice,
+  CSR_CUDA(cudaMemcpyAsync(st.d_csr_const, csr_constant.data(), 4 * sizeof(double) * nbunch, cudaMemcpyHostToDevice,
                            stream));
   CSR_CUDA(cudaMemcpyAsync(st.d_flags, flags.data(), flags.size(), cudaMemcpyHostToDevice, stream));
   const double *sgw = st.d_sg + st.sg_offset[k];
@@ -1881,6 +1947,14 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     a.nSlices = ce.nSlices;
     a.c1 = a.c2 = a.csr_constant = 0; /* per bunch in the kernel */
     a.wakelog = st.d_wakelog + st.wake_values;
+    /* pages of the plain-integral kicks only (the learned wake writes none) */
+    a.pagelog = st.record_pages && !use_net ? st.d_pagelog + st.page_values : nullptr;
+    a.page_element = elem;
+    a.page_kick = kick;
+    a.page_angle = phiBend;
+    a.page_ds_kick = ce.length / ce.nSlices;
+    a.page_p_central = Po;
+    a.page_range_factor = ce.binRangeFactor;
     a.igf = ce.igf;
     set_filter_args(a, ce.lh, ce.clip, ce.lowCut0, ce.lowCut1, ce.highCut0, ce.highCut1);
     {
@@ -1893,6 +1967,16 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       a.const1 = 6.0 - b2e_log(27.0 / 4.0);
       a.q4pe = kE / (4 * kPI * eps0);
       a.igf_factor = 0;
+    }
+    cudaEvent_t ev_end = nullptr;
+    if (st.time_wake) {
+      while ((int64_t)st.wake_events.size() < 2 * (st.timed_kicks + 1)) {
+        cudaEvent_t e;
+        CSR_CUDA(cudaEventCreate(&e));
+        st.wake_events.push_back(e);
+      }
+      CSR_CUDA(cudaEventRecord(st.wake_events[2 * st.timed_kicks], stream));
+      ev_end = st.wake_events[2 * st.timed_kicks + 1];
     }
     if (use_net) {
       const int L = wakenet_bins(st.net);
@@ -1917,7 +2001,14 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       (*launches)++;
       CSR_CUDA(cudaGetLastError());
     }
+    if (ev_end) {
+      CSR_CUDA(cudaEventRecord(ev_end, stream));
+      st.timed_kicks++;
+      st.timed_learned += use_net;
+    }
     st.wake_values += (int64_t)ce.bins * nbunch;
+    if (a.pagelog)
+      st.page_values += nbunch * page_stride;
   }
   if (!recycle || ce.nSlices <= 0) {
     csr_reset_keys_kernel<<<1, 32, 0, stream>>>(B);
@@ -1945,6 +2036,38 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     err = "CSR: a bounded wait in the wake network gave up";
     return B2E_ERR_TIMEOUT;
   }
+  return B2E_OK;
+}
+
+int csr_wake_timing(CsrState &st, double *ms, int64_t *kicks, int64_t *learned, std::string &err) {
+  double total = 0;
+  for (int64_t k = 0; k < st.timed_kicks; k++) {
+    float t = 0;
+    cudaError_t e = cudaEventSynchronize(st.wake_events[2 * k + 1]);
+    if (e == cudaSuccess)
+      e = cudaEventElapsedTime(&t, st.wake_events[2 * k], st.wake_events[2 * k + 1]);
+    if (e != cudaSuccess) {
+      err = cudaGetErrorString(e);
+      return B2E_ERR_CUDA;
+    }
+    total += t;
+  }
+  *ms = total;
+  *kicks = st.timed_kicks;
+  *learned = st.timed_learned;
+  return B2E_OK;
+}
+
+int csr_copy_pages(CsrState &st, double *pages, int64_t capacity, int64_t *written, std::string &err) {
+  int64_t n = std::min<int64_t>(st.page_values, capacity);
+  if (n > 0 && pages) {
+    cudaError_t e = cudaMemcpy(pages, st.d_pagelog, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      err = cudaGetErrorString(e);
+      return B2E_ERR_CUDA;
+    }
+  }
+  *written = pages ? n : st.page_values;
   return B2E_OK;
 }
 
@@ -1994,6 +2117,15 @@ void csr_release(CsrState &st) {
     cudaFree(st.d_sg_idx);
   if (st.d_wakelog)
     cudaFree(st.d_wakelog);
+  if (st.d_pagelog)
+    cudaFree(st.d_pagelog);
+  for (cudaEvent_t e : st.wake_events)
+    cudaEventDestroy(e);
+  st.wake_events.clear();
+  st.timed_kicks = st.timed_learned = 0;
+  st.d_pagelog = nullptr;
+  st.pagelog_cap = 0;
+  st.page_values = 0;
   st.d_beta0 = nullptr;
   st.d_state = nullptr;
   st.d_counts = nullptr;

@@ -59,7 +59,7 @@ struct CsrState {
   int64_t beta0_cap = 0;
   void *d_state = nullptr;        /* CsrDevState[n_bunches] */
   unsigned int *d_counts = nullptr; /* [n_bunches][B2E_CSR_MAX_BINS] */
-  double *d_csr_const = nullptr;  /* [3][n_bunches]: CSRConstant, IGF wake factor, GSConstant */
+  double *d_csr_const = nullptr;  /* [4][n_bunches]: CSRConstant, IGF wake factor, GSConstant, macro charge */
   unsigned char *d_flags = nullptr; /* [2][n_bunches]: active, CSRDRIFT mode */
   unsigned long long *d_alive = nullptr; /* [n_bunches] */
   /* optional all-rank reduction (a bunch spread over several GPUs) */
@@ -71,6 +71,18 @@ struct CsrState {
   std::vector<size_t> sg_offset;  /* per element: offset into d_sg / d_sg_idx */
   double *d_wakelog = nullptr;
   int64_t wakelog_cap = 0;
+  /* optional page record of every plain-integral kick, for CSRCSBEND's
+   * OUTPUT_FILE: per (kick, bunch) B2E_CSR_PAGE_HEADER values then the
+   * density, its derivative, T1 and T2 over the bins */
+  bool record_pages = false;
+  double *d_pagelog = nullptr;
+  int64_t pagelog_cap = 0, page_values = 0;
+  /* optional timing of the wake stage of every CSRCSBEND kick (the plain
+   * wake kernel, or the learned wake's filter + network + combine): a pair
+   * of events per kick on the context's stream */
+  bool time_wake = false;
+  std::vector<cudaEvent_t> wake_events;
+  int64_t timed_kicks = 0, timed_learned = 0;
   double ds0 = 0, zLast = 0, z0 = 0;
   double revolution_length = 0;   /* added to a CSRDRIFT's start behind the last dipole */
   /* what the last CSRCSBEND leaves for a Stupakov CSRDRIFT (csbend.c:2991-3003):
@@ -112,6 +124,10 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
                       const std::vector<int64_t> &alive, int elem, int pass, cudaStream_t stream, std::string &err,
                       int64_t *launches);
 int csr_copy_wakes(CsrState &st, double *wakes, int64_t capacity, int64_t *written, std::string &err);
+int csr_copy_pages(CsrState &st, double *pages, int64_t capacity, int64_t *written, std::string &err);
+/* total device time of the timed wake stages of the last run, and the kicks
+ * (all, and those that took the learned wake) */
+int csr_wake_timing(CsrState &st, double *ms, int64_t *kicks, int64_t *learned, std::string &err);
 cudaError_t launch_post_element_sweep(const DevParticles &P, int64_t n, const DevAperture *ap, int pass, int elem,
                                       cudaStream_t stream);
 void csr_release(CsrState &st);

@@ -198,14 +198,90 @@ __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &
   qy = qy * (1 + dp);
 }
 
-template <bool RAD>
+/* kick `step` of a slice of the kick integrator (multipole.c:1264-1351):
+ * the canonical multipole kick of the element's order, the KSEXT K1/J1
+ * terms, momenta back to slopes and the radiation block; ORDER = 0 reads the
+ * order from the element. */
+template <bool RAD, int ORDER>
+__device__ __forceinline__ int kmult_kick(double x, double y, double &xp, double &yp, double &qx, double &qy,
+                                          double &dp, const DevElem &e, int order_rt, int step, int nSub, int slice,
+                                          const RadSite &rs) {
+  const double *c = e.c;
+  const int order = ORDER > 0 ? ORDER : order_rt;
+  const double kick = c[KM_KICK0 + step];
+  double sumFx, sumFy, dqx = 0, dqy = 0;
+  /* apply_canonical_multipole_kicks (multipole.h:213-245): coefficients
+   * (x+iy)^n/n! with signs; order 1: Fx=y, Fy=x; order 2: Fx=x*y,
+   * Fy=x^2/2-y^2/2, each accumulated from 0 in the reference's order. */
+  if (order == 1) {
+    sumFx = (1.0 * 1.0) * y;
+    sumFy = (1.0 * x) * 1.0;
+  } else {
+    double x2 = (1.0 * x) * x, y2 = (1.0 * y) * y;
+    sumFx = (1.0 * x) * y;
+    sumFy = (0.5 * x2) * 1.0;
+    sumFy = sumFy + (-0.5 * 1.0) * y2;
+  }
+  qx = qx - kick * sumFy;
+  qy = qy + kick * sumFx;
+  if (RAD) {
+    /* delta_qx, delta_qy of apply_canonical_multipole_kicks (multipole.h:237-240) */
+    dqx = dqx - kick * sumFy;
+    dqy = dqy + kick * sumFx;
+  }
+  if (e.flags & (EF_QUAD_ORDER2 | EF_SKEW_ORDER2)) {
+    /* KSEXT K1/J1 terms: quadrupole order, normal then skew (multipole.c:1272-1275) */
+    if (e.flags & EF_QUAD_ORDER2) {
+      const double k1 = c[KM_KICK1_0 + step];
+      const double fy = (1.0 * x) * 1.0, fx = (1.0 * 1.0) * y;
+      qx = qx - k1 * fy;
+      qy = qy + k1 * fx;
+      if (RAD) {
+        dqx = dqx - k1 * fy;
+        dqy = dqy + k1 * fx;
+      }
+    }
+    if (e.flags & EF_SKEW_ORDER2) {
+      const double j1 = c[KM_SKEW0 + step];
+      /* skew: swap(Fx, Fy), Fx = -Fx */
+      double fx = -((1.0 * x) * 1.0), fy = (1.0 * 1.0) * y;
+      qx = qx - j1 * fy;
+      qy = qy + j1 * fx;
+      if (RAD) {
+        dqx = dqx - j1 * fy;
+        dqy = dqy + j1 * fx;
+      }
+    }
+  }
+  if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+    return LOSS_SLOPE;
+  if (e.flags & EF_RADBLOCK) {
+    if (RAD && (e.flags & (EF_SR | EF_ISR))) {
+      kmult_radiation(qx, qy, dp, dqx, dqy, xp, yp, c, step, nSub, e.flags, rs, slice);
+    } else {
+      qx = qx / (1 + dp);
+      qy = qy / (1 + dp);
+      qx = qx * (1 + dp);
+      qy = qy * (1 + dp);
+    }
+    if (!momenta_to_slopes(xp, yp, qx, qy, dp))
+      return LOSS_SLOPE;
+  }
+  return LOSS_NONE;
+}
+
+/* NSUB > 0 / ORDER > 0: substep count and multipole order as compile-time
+ * constants (4 and 1 or 2 for KQUAD/KSEXT at the default integration order),
+ * the slice unrolled; 0 takes them from the element.  The same operations in
+ * the same order either way. */
+template <bool RAD, int NSUB = 0, int ORDER = 0>
 __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g,
                                      const RadSite &rs) {
   const double *c = e.c;
-  const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = (int)c[KM_NSUB];
+  const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = NSUB > 0 ? NSUB : (int)c[KM_NSUB];
   const double dx = c[KM_DX], dy = c[KM_DY];
   double x, xp, y, yp, s, dp, qx, qy, denom;
-  int i_kick, step;
+  int i_kick, lost;
 
   /* entrance misalignment, offsetParticlesForMisalignment mode 0 face 1 (malign_mat.c:491-497) */
   if (e.flags & EF_ENTRANCE_OFFSET)
@@ -236,71 +312,28 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
       p.y = y;
       return LOSS_APERTURE;
     }
-    for (step = 0; step < nSub; step++) {
-      const double dsh = c[KM_DSH0 + step];
-      const double kick = c[KM_KICK0 + step];
-      double sumFx, sumFy, dqx = 0, dqy = 0;
-      x = x + xp * dsh;
-      y = y + yp * dsh;
-      s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
-      if (step == nSub - 1) /* kickFrac[last] == 0 ends the slice */
-        break;
-      /* apply_canonical_multipole_kicks (multipole.h:213-245): coefficients
-       * (x+iy)^n/n! with signs; order 1: Fx=y, Fy=x; order 2: Fx=x*y,
-       * Fy=x^2/2-y^2/2, each accumulated from 0 in the reference's order. */
-      if (order == 1) {
-        sumFx = (1.0 * 1.0) * y;
-        sumFy = (1.0 * x) * 1.0;
-      } else {
-        double x2 = (1.0 * x) * x, y2 = (1.0 * y) * y;
-        sumFx = (1.0 * x) * y;
-        sumFy = (0.5 * x2) * 1.0;
-        sumFy = sumFy + (-0.5 * 1.0) * y2;
+    if constexpr (NSUB > 0) {
+#pragma unroll
+      for (int step = 0; step < NSUB; step++) {
+        const double dsh = c[KM_DSH0 + step];
+        x = x + xp * dsh;
+        y = y + yp * dsh;
+        s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
+        if (step < NSUB - 1) /* kickFrac[last] == 0 ends the slice */
+          if ((lost = kmult_kick<RAD, ORDER>(x, y, xp, yp, qx, qy, dp, e, order, step, nSub, i_kick, rs)))
+            return lost;
       }
-      qx = qx - kick * sumFy;
-      qy = qy + kick * sumFx;
-      if (RAD) {
-        /* delta_qx, delta_qy of apply_canonical_multipole_kicks (multipole.h:237-240) */
-        dqx = dqx - kick * sumFy;
-        dqy = dqy + kick * sumFx;
-      }
-      if (e.flags & (EF_QUAD_ORDER2 | EF_SKEW_ORDER2)) {
-        /* KSEXT K1/J1 terms: quadrupole order, normal then skew (multipole.c:1272-1275) */
-        if (e.flags & EF_QUAD_ORDER2) {
-          const double k1 = c[KM_KICK1_0 + step];
-          const double fy = (1.0 * x) * 1.0, fx = (1.0 * 1.0) * y;
-          qx = qx - k1 * fy;
-          qy = qy + k1 * fx;
-          if (RAD) {
-            dqx = dqx - k1 * fy;
-            dqy = dqy + k1 * fx;
-          }
-        }
-        if (e.flags & EF_SKEW_ORDER2) {
-          const double j1 = c[KM_SKEW0 + step];
-          /* skew: swap(Fx, Fy), Fx = -Fx */
-          double fx = -((1.0 * x) * 1.0), fy = (1.0 * 1.0) * y;
-          qx = qx - j1 * fy;
-          qy = qy + j1 * fx;
-          if (RAD) {
-            dqx = dqx - j1 * fy;
-            dqy = dqy + j1 * fx;
-          }
-        }
-      }
-      if (!momenta_to_slopes(xp, yp, qx, qy, dp))
-        return LOSS_SLOPE;
-      if (e.flags & EF_RADBLOCK) {
-        if (RAD && (e.flags & (EF_SR | EF_ISR))) {
-          kmult_radiation(qx, qy, dp, dqx, dqy, xp, yp, c, step, nSub, e.flags, rs, i_kick);
-        } else {
-          qx = qx / (1 + dp);
-          qy = qy / (1 + dp);
-          qx = qx * (1 + dp);
-          qy = qy * (1 + dp);
-        }
-        if (!momenta_to_slopes(xp, yp, qx, qy, dp))
-          return LOSS_SLOPE;
+    } else {
+#pragma unroll 1
+      for (int step = 0; step < nSub; step++) {
+        const double dsh = c[KM_DSH0 + step];
+        x = x + xp * dsh;
+        y = y + yp * dsh;
+        s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
+        if (step == nSub - 1) /* kickFrac[last] == 0 ends the slice */
+          break;
+        if ((lost = kmult_kick<RAD, ORDER>(x, y, xp, yp, qx, qy, dp, e, order, step, nSub, i_kick, rs)))
+          return lost;
       }
     }
   }
@@ -341,79 +374,108 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
  * pure-dipole field (Fx = 0, Fy = 1, csbend.c:106-110).  Q = (X, QX, Y, QY,
  * dist, DPoP).  `isr_block` reproduces the (QX/(1+d))*(1+d) round trip of
  * the radiation block that the negated isrConstant always enables. */
+
+/* drift substep j of a slice (csbend.c:1555-1581) */
+__device__ __forceinline__ int bend_drift(double &X, double &QX, double &Y, double QY, double &dist, double DPoP,
+                                          double rho0, double dsh_rho0) {
+  double f, sin_phi, phi, sine, cosi, tang, cos_phi, factor, arg;
+  f = (1 + DPoP) * (1 + DPoP) - QY * QY;
+  if (f <= 0)
+    return LOSS_SLOPE;
+  f = sqrt(f);
+  if (fabs(QX / f) > 1)
+    return LOSS_SLOPE;
+  sin_phi = QX / f;
+  phi = b2e_asin(sin_phi);
+  arg = dsh_rho0 + phi;
+  b2e_sincos(arg, &sine, &cosi);
+  if (cosi == 0)
+    return LOSS_SLOPE;
+  tang = sine / cosi;
+  cos_phi = b2e_cos(phi);
+  QX = f * sine;
+  factor = (((rho0 + X) * cos_phi) / f) * (tang - sin_phi / cos_phi);
+  Y = Y + QY * factor;
+  dist = dist + factor * (1 + DPoP);
+  f = cos_phi / cosi;
+  X = rho0 * (f - 1) + f * X;
+  return LOSS_NONE;
+}
+
+/* kick j of a slice (csbend.c:1591-1638) */
 template <bool RAD>
+__device__ __forceinline__ void bend_kick(double X, double &QX, double &QY, double &DPoP, const double *c, int i, int j,
+                                          int nSub, bool isr_block, const DevElem &e, const RadSite &rs) {
+  const double rho_actual = c[CB_RHO_ACTUAL];
+  const double ds = c[CB_DS0 + j];
+  /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
+  const double x_rho0 = div_rn_recip(X, c[CB_RHO0], c[CB_INV_RHO0]);
+  QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * 1.0), rho_actual, c[CB_INV_RHO_ACTUAL]);
+  {
+    /* (t * Fx) / rho_actual with Fx = 0 is a signed zero (NaN for a
+     * non-finite t): the sign of t * 0.0 flipped by rho_actual's, which
+     * is finite and nonzero in a bend -- the same value without the
+     * division */
+    const double z = ((ds) * (1 + x_rho0)) * 0.0;
+    QY = QY + (rho_actual < 0 ? -z : z);
+  }
+  if (RAD && (e.flags & (EF_SR | EF_ISR))) {
+    /* radiation after the kick (csbend.c:1603-1622), Fx = 0, Fy = 1 */
+    const double a = 1 + X * rs.rc[RB_INV_RHO0];
+    const double f = a / sqrt(((1 + DPoP) * (1 + DPoP) - QX * QX) - QY * QY);
+    const double xp = QX * f, yp = QY * f;
+    const double dsFactor = sqrt((a * a + xp * xp) + yp * yp);
+    const double F2 = 0.0 * 0.0 + 1.0 * 1.0;
+    const double deltaFactor = (1 + DPoP) * (1 + DPoP);
+    const double dsISR = rs.rc[RB_SLICE] / (nSub - 1);
+    QX = QX / (1 + DPoP);
+    QY = QY / (1 + DPoP);
+    if (e.flags & EF_SR)
+      DPoP = DPoP - (((rs.rc[RB_RAD] * deltaFactor) * F2) * ds) * dsFactor;
+    if (e.flags & EF_ISR)
+      DPoP = DPoP - (((rs.rc[RB_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISR * dsFactor)) *
+                        b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, i, j, rs.limit);
+    QX = QX * (1 + DPoP);
+    QY = QY * (1 + DPoP);
+  } else if (isr_block) {
+    QX = QX / (1 + DPoP);
+    QY = QY / (1 + DPoP);
+    QX = QX * (1 + DPoP);
+    QY = QY * (1 + DPoP);
+  }
+}
+
+/* NSUB > 0: the substep count is a compile-time constant (4 for the default
+ * INTEGRATION_ORDER=4) and the slice is unrolled; NSUB = 0 takes nSub from
+ * the element.  The same operations in the same order either way. */
+template <bool RAD, int NSUB = 0>
 __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y, double &QY, double &dist,
-                                                double &DPoP, const double *c, int nSlices, int nSub,
+                                                double &DPoP, const double *c, int nSlices, int nSub_rt,
                                                 bool isr_block, const DevAperture *ap, const DevElem &e,
                                                 const RadSite &rs) {
-  const double rho0 = c[CB_RHO0], rho_actual = c[CB_RHO_ACTUAL];
-  int i, j;
+  const double rho0 = c[CB_RHO0];
+  const int nSub = NSUB > 0 ? NSUB : nSub_rt;
+  int lost;
   dist = 0;
-  for (i = 0; i < nSlices; i++) {
+  for (int i = 0; i < nSlices; i++) {
     if (!mult_aperture_ok(X, Y, ap, e))
       return LOSS_APERTURE;
-    for (j = 0; j < nSub; j++) {
-      const double dsh_rho0 = c[CB_DSH0 + j];
-      double f, sin_phi, phi, sine, cosi, tang, cos_phi, factor, arg;
-      f = (1 + DPoP) * (1 + DPoP) - QY * QY;
-      if (f <= 0)
-        return LOSS_SLOPE;
-      f = sqrt(f);
-      if (fabs(QX / f) > 1)
-        return LOSS_SLOPE;
-      sin_phi = QX / f;
-      phi = b2e_asin(sin_phi);
-      arg = dsh_rho0 + phi;
-      b2e_sincos(arg, &sine, &cosi);
-      if (cosi == 0)
-        return LOSS_SLOPE;
-      tang = sine / cosi;
-      cos_phi = b2e_cos(phi);
-      QX = f * sine;
-      factor = (((rho0 + X) * cos_phi) / f) * (tang - sin_phi / cos_phi);
-      Y = Y + QY * factor;
-      dist = dist + factor * (1 + DPoP);
-      f = cos_phi / cosi;
-      X = rho0 * (f - 1) + f * X;
-      if (j == nSub - 1) /* kickFrac[last] == 0 ends the slice */
-        break;
-      {
-        const double ds = c[CB_DS0 + j];
-        /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
-        const double x_rho0 = div_rn_recip(X, rho0, c[CB_INV_RHO0]);
-        QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * 1.0), rho_actual, c[CB_INV_RHO_ACTUAL]);
-        {
-          /* (t * Fx) / rho_actual with Fx = 0 is a signed zero (NaN for a
-           * non-finite t): the sign of t * 0.0 flipped by rho_actual's, which
-           * is finite and nonzero in a bend -- the same value without the
-           * division */
-          const double z = ((ds) * (1 + x_rho0)) * 0.0;
-          QY = QY + (rho_actual < 0 ? -z : z);
-        }
-        if (RAD && (e.flags & (EF_SR | EF_ISR))) {
-          /* radiation after the kick (csbend.c:1603-1622), Fx = 0, Fy = 1 */
-          const double a = 1 + X * rs.rc[RB_INV_RHO0];
-          const double f = a / sqrt(((1 + DPoP) * (1 + DPoP) - QX * QX) - QY * QY);
-          const double xp = QX * f, yp = QY * f;
-          const double dsFactor = sqrt((a * a + xp * xp) + yp * yp);
-          const double F2 = 0.0 * 0.0 + 1.0 * 1.0;
-          const double deltaFactor = (1 + DPoP) * (1 + DPoP);
-          const double dsISR = rs.rc[RB_SLICE] / (nSub - 1);
-          QX = QX / (1 + DPoP);
-          QY = QY / (1 + DPoP);
-          if (e.flags & EF_SR)
-            DPoP = DPoP - (((rs.rc[RB_RAD] * deltaFactor) * F2) * ds) * dsFactor;
-          if (e.flags & EF_ISR)
-            DPoP = DPoP - (((rs.rc[RB_ISR] * deltaFactor) * b2e_isr_pow34(F2)) * sqrt(dsISR * dsFactor)) *
-                              b2e_isr_gauss(rs.seed, rs.id, rs.pass, rs.elem, i, j, rs.limit);
-          QX = QX * (1 + DPoP);
-          QY = QY * (1 + DPoP);
-        } else if (isr_block) {
-          QX = QX / (1 + DPoP);
-          QY = QY / (1 + DPoP);
-          QX = QX * (1 + DPoP);
-          QY = QY * (1 + DPoP);
-        }
+    if constexpr (NSUB > 0) {
+#pragma unroll
+      for (int j = 0; j < NSUB; j++) {
+        if ((lost = bend_drift(X, QX, Y, QY, dist, DPoP, rho0, c[CB_DSH0 + j])))
+          return lost;
+        if (j < NSUB - 1) /* kickFrac[last] == 0 ends the slice */
+          bend_kick<RAD>(X, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
+      }
+    } else {
+#pragma unroll 1
+      for (int j = 0; j < nSub; j++) {
+        if ((lost = bend_drift(X, QX, Y, QY, dist, DPoP, rho0, c[CB_DSH0 + j])))
+          return lost;
+        if (j == nSub - 1) /* kickFrac[last] == 0 ends the slice */
+          break;
+        bend_kick<RAD>(X, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
       }
     }
   }
@@ -473,7 +535,14 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   Q2 = y;
   Q3 = yp * f;
 
-  lost = csbend_integrate<RAD>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e, rs);
+#ifndef B2E_UNROLL
+#define B2E_UNROLL 2
+#endif
+  if (B2E_UNROLL >= 1 && nSub == 4)
+    lost = csbend_integrate<RAD, 4>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e,
+                                    rs);
+  else
+    lost = csbend_integrate<RAD>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e, rs);
 
   /* convertFromDipoleCanonicalCoordinates (csbend.c:1421-1429) */
   f = 1 / sqrt(((1 + dp) * (1 + dp) - Q1 * Q1) - Q3 * Q3);

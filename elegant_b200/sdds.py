@@ -37,15 +37,24 @@ def write_sdds(path, parameters, columns, mode="binary", description=None):
     """parameters: [(name, type, value, attrs)], columns: [(name, type,
     values, attrs)], types 'double' | 'long' | 'short' | 'string'; attrs:
     dict of units, symbol, description.  Binary data are written row by row
-    (SDDS's row-major layout), so string columns work too."""
+    (SDDS's row-major layout), so string columns work too.  One page."""
+    write_sdds_pages(path, [(p[0], p[1], p[3]) for p in parameters], [(c[0], c[1], c[3]) for c in columns],
+                     [([p[2] for p in parameters], [c[2] for c in columns])], mode, description)
+
+
+def write_sdds_pages(path, parameters, columns, pages, mode="binary", description=None):
+    """Several pages of one layout: parameters [(name, type, attrs)], columns
+    [(name, type, attrs)], pages [(parameter values, column arrays)] in the
+    definition orders."""
     if mode not in ("binary", "ascii"):
         raise ValueError("mode must be 'binary' or 'ascii'")
-    n = len(columns[0][2]) if columns else 0
     for c in columns:
-        if len(c[2]) != n:
-            raise ValueError("columns of different lengths")
         if c[1] not in _FMT:
             raise ValueError(f"unsupported SDDS type {c[1]}")
+    for _, cols in pages:
+        n = len(cols[0]) if cols else 0
+        if any(len(v) != n for v in cols):
+            raise ValueError("columns of different lengths")
     lines = ["SDDS1"]
     if mode == "binary":
         lines.append("!# little-endian")
@@ -55,34 +64,36 @@ def write_sdds(path, parameters, columns, mode="binary", description=None):
     def attrs_text(a):
         return "".join(f" {k}={_quote(str(v))}," for k, v in (a or {}).items())
 
-    for name, typ, _, a in parameters:
+    for name, typ, a in parameters:
         lines.append(f"&parameter name={name},{attrs_text(a)} type={typ}, &end")
-    for name, typ, _, a in columns:
+    for name, typ, a in columns:
         lines.append(f"&column name={name},{attrs_text(a)} type={typ}, &end")
     lines.append(f"&data mode={mode}, &end")
     with open(path, "wb") as fh:
         fh.write(("\n".join(lines) + "\n").encode())
-        if mode == "binary":
-            fh.write(struct.pack("<i", n))
-            for _, typ, v, _ in parameters:
-                fh.write(_pack(typ, v))
-            if n and all(c[1] != "string" for c in columns):
-                rec = np.dtype([(c[0], "<" + np.dtype(_FMT[c[1]][1]).str[1:]) for c in columns])
-                rows = np.empty(n, dtype=rec)
-                for c in columns:
-                    rows[c[0]] = c[2]
-                fh.write(rows.tobytes())
+        for values, cols in pages:
+            n = len(cols[0]) if cols else 0
+            if mode == "binary":
+                fh.write(struct.pack("<i", n))
+                for (_, typ, _), v in zip(parameters, values):
+                    fh.write(_pack(typ, v))
+                if n and all(c[1] != "string" for c in columns):
+                    rec = np.dtype([(c[0], "<" + np.dtype(_FMT[c[1]][1]).str[1:]) for c in columns])
+                    rows = np.empty(n, dtype=rec)
+                    for c, v in zip(columns, cols):
+                        rows[c[0]] = v
+                    fh.write(rows.tobytes())
+                else:
+                    for i in range(n):
+                        fh.write(b"".join(_pack(c[1], v[i]) for c, v in zip(columns, cols)))
             else:
+                out = []
+                for (_, typ, _), v in zip(parameters, values):
+                    out.append(_text(typ, v))
+                out.append(f"\t{n}")
                 for i in range(n):
-                    fh.write(b"".join(_pack(c[1], c[2][i]) for c in columns))
-        else:
-            out = []
-            for _, typ, v, _ in parameters:
-                out.append(_text(typ, v))
-            out.append(f"\t{n}")
-            for i in range(n):
-                out.append(" ".join(_text(c[1], c[2][i]) for c in columns))
-            fh.write(("\n".join(out) + "\n").encode())
+                    out.append(" ".join(_text(c[1], v[i]) for c, v in zip(columns, cols)))
+                fh.write(("\n".join(out) + "\n").encode())
 
 
 def _pack(typ, v):
@@ -269,3 +280,44 @@ def write_aperture(path, result, step=1, mode="binary"):
                                  for l in lines], {"units": "m"})]
     write_sdds(path, [("Step", "long", step, {}), ("Area", "double", result["area"], {"units": "m$a2$n"})], cols,
                mode, description="Dynamic aperture search")
+
+
+def csr_wake_columns(page):
+    """The OUTPUT_FILE columns of one CSRCSBEND kick from its page record
+    (elegant_b200.track.Tracker.csr_pages), with the reference's expressions
+    (csbend.c:2762-2806): LinearDensity = ctHist * (q c), LinearDensityDeriv
+    = ctHistDeriv * (q c^2 / dct), s = ctLower - (ctLower + ctUpper)/2 + dct
+    (i + 1/2), GammaDeriv = DeltaGamma / (L / N_KICKS)."""
+    q, dct, lo, hi = page["macro_charge"], page["dct"], page["ct_lower"], page["ct_upper"]
+    dgamma = page["dgamma"]
+    return {"s": (lo - (lo + hi) / 2.0) + dct * (np.arange(page["bins"]) + 0.5),
+            "LinearDensity": page["hist"] * (q * C_MKS),
+            "LinearDensityDeriv": page["deriv"] * ((q * (C_MKS * C_MKS)) / dct),
+            "DeltaGamma": dgamma, "GammaDeriv": dgamma / page["ds_kick"],
+            "DeltaGammaT1": page["t1"], "DeltaGammaT2": page["t2"]}
+
+
+CSR_WAKE_PARAMETERS = [("SVNVersion", "string", {"description": "SVN version number"}),
+                       ("Pass", "long", {}), ("Kick", "long", {}), ("pCentral", "double", {"units": "m$be$nc"}),
+                       ("Angle", "double", {}), ("SlippageLength", "double", {"units": "m"}),
+                       ("TotalBunchLength", "double", {"units": "m"}), ("BinSize", "double", {"units": "m"}),
+                       ("dsKick", "double", {"units": "m"}), ("DerbenevRatio", "double", {})]
+CSR_WAKE_COLUMNS = [("s", "double", {"units": "m"}), ("LinearDensity", "double", {"units": "C/s"}),
+                    ("LinearDensityDeriv", "double", {"units": "C/s$a2$n"}), ("DeltaGamma", "double", {}),
+                    ("GammaDeriv", "double", {"units": "1/m"}), ("DeltaGammaT1", "double", {}),
+                    ("DeltaGammaT2", "double", {})]
+
+
+def write_csr_wake(path, pages, mode="binary"):
+    """CSRCSBEND's OUTPUT_FILE (csbend.c:2227-2249 layout, one page per kick,
+    :2762-2806) for the page records of one element, in the order given (a
+    bunch train: bunch by bunch, as elegant writes consecutive bunches).
+    Pass is -1 and DerbenevRatio 0, as the reference writes them with its
+    Derbenev criterion off (the default)."""
+    out = []
+    for pg in pages:
+        cols = csr_wake_columns(pg)
+        values = ["elegant_b200", -1, pg["kick"], pg["p_central"], pg["angle"], pg["slippage"],
+                  pg["ct_upper"] - pg["ct_lower"], pg["dct"], pg["ds_kick"], 0.0]
+        out.append((values, [cols[c[0]] for c in CSR_WAKE_COLUMNS]))
+    write_sdds_pages(path, CSR_WAKE_PARAMETERS, CSR_WAKE_COLUMNS, out, mode, description="CSR wake output")

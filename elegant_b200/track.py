@@ -253,6 +253,54 @@ class Tracker:
                                                      errs.ctypes.data, wr.value, ctypes.byref(wr)))
         return {"evaluations": ev.value, "fallbacks": fb.value, "gate_errors": errs[: wr.value]}
 
+    def set_csr_timing(self, on: bool = True):
+        """Time the wake stage of every CSRCSBEND kick of later runs with CUDA
+        events (see csr_wake_timing)."""
+        self._check(self.lib.b2e_set_csr_timing(self._ctx, int(on)))
+
+    def csr_wake_timing(self) -> dict:
+        """Summed device time of the last run's timed wake stages: ms, kicks,
+        learned_kicks (kicks that took the learned wake), ms_per_kick."""
+        ms, k, lk = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.b2e_csr_timing(self._ctx, ctypes.byref(ms), ctypes.byref(k), ctypes.byref(lk)))
+        return {"ms": ms.value, "kicks": k.value, "learned_kicks": lk.value,
+                "ms_per_kick": ms.value / k.value if k.value else float("nan")}
+
+    def set_csr_pages(self, record: bool = True):
+        """Keep, for every plain-integral CSRCSBEND kick of later runs, what the
+        element's OUTPUT_FILE page holds (see csr_pages)."""
+        self._check(self.lib.b2e_set_csr_pages(self._ctx, int(record)))
+
+    def csr_pages(self) -> list[dict]:
+        """The page records of the last run, in kick order (bunches within a
+        kick): element index, kick, bunch, bins, the binned range (ct_lower,
+        ct_upper), dct, slippage, angle (phiBend), ds_kick, p_central,
+        macro_charge, and the arrays hist (line density per unit c*t), deriv
+        (its derivative), t1 and t2 (the wake terms), dgamma (the kick's
+        wake, from the wake log).  Kicks of a bunch without CSR are left out.
+        Plain-integral kicks only: with the learned wake bound, no pages."""
+        written = ctypes.c_int64()
+        self._check(self.lib.b2e_csr_pages(self._ctx, None, 0, ctypes.byref(written)))
+        buf = np.empty(max(written.value, 1), dtype=np.float64)
+        self._check(self.lib.b2e_csr_pages(self._ctx, buf.ctypes.data, written.value, ctypes.byref(written)))
+        nw = ctypes.c_int64()
+        self._check(self.lib.b2e_csr_wakes(self._ctx, None, 0, ctypes.byref(nw)))
+        wakes = self.csr_wakes(max(nw.value, 1))
+        pages, pos, wpos, h = [], 0, 0, nat.CSR_PAGE_HEADER
+        while pos < written.value:
+            head = buf[pos:pos + h]
+            bins = int(head[3])
+            if head[0] >= 0:  # else a bunch without CSR on this kick
+                a = buf[pos + h:pos + h + 4 * bins].reshape(4, bins)
+                pages.append({"element": int(head[0]), "kick": int(head[1]), "bunch": int(head[2]), "bins": bins,
+                              "ct_lower": head[4], "ct_upper": head[5], "dct": head[6], "slippage": head[7],
+                              "angle": head[8], "ds_kick": head[9], "p_central": head[10],
+                              "macro_charge": head[11], "hist": a[0].copy(), "deriv": a[1].copy(),
+                              "t1": a[2].copy(), "t2": a[3].copy(), "dgamma": wakes[wpos:wpos + bins].copy()})
+            pos += h + 4 * bins
+            wpos += bins  # the wake log holds every bunch of every kick in the same order
+        return pages
+
     def csr_wakes(self, capacity: int) -> np.ndarray:
         buf = np.empty(capacity, dtype=np.float64)
         written = ctypes.c_int64()

@@ -331,6 +331,36 @@ int b2e_naff(const double *dev_signals, int64_t n_signals, int32_t n_points, dou
  * CSRCSBEND kick, BINS values of dGamma (csbend.c:2673) in kick order. */
 int b2e_csr_wakes(b2e_ctx *ctx, double *wakes, int64_t capacity, int64_t *written);
 
+/* What CSRCSBEND's OUTPUT_FILE holds (csbend.c:2227-2249 layout, one page
+ * per kick written at :2762-2806).  With recording on (off by default), every
+ * plain-integral kick of the following runs keeps, per bunch, a record of
+ * B2E_CSR_PAGE_HEADER values -- element index, kick, bunch, BINS, the binned
+ * range ctLower and ctUpper, the bin width dct, the slippage length, the
+ * accumulated bend angle phiBend, the kick length L/N_KICKS, pCentral, the
+ * bunch's macro-particle charge -- followed by BINS values each of the smoothed line
+ * density per unit c*t (ctHist), its derivative (ctHistDeriv), and the wake
+ * terms T1 and T2 (csbend.c:2664-2667); a bunch without CSR on that kick
+ * has element index -1 and undefined arrays.  The file's columns follow from these:
+ * LinearDensity = ctHist * (q_macro c), LinearDensityDeriv = ctHistDeriv *
+ * (q_macro c^2 / dct), DeltaGamma = T1 + T2, GammaDeriv = DeltaGamma /
+ * (L/N_KICKS), s = ctLower - (ctLower + ctUpper)/2 + dct (i + 1/2) (the
+ * reference's expressions; elegant_b200.sdds.write_csr_wake writes the
+ * file).  b2e_csr_pages copies the records of the last run
+ * (*written = values; NULL to query).  Not with the learned wake, whose kicks
+ * record no page.  No counterpart as an API in the reference. */
+/* Timing of the CSR wake stage: with timing on, each CSRCSBEND kick of the
+ * following runs brackets its wake stage -- the plain wake kernel, or the
+ * learned wake's filter, network and combine kernels -- with CUDA events on
+ * the context's stream.  b2e_csr_timing waits for the last run's events and
+ * returns their summed device time in ms, the timed kicks and how many of
+ * them took the learned wake.  No counterpart in the reference. */
+int b2e_set_csr_timing(b2e_ctx *ctx, int32_t on);
+int b2e_csr_timing(b2e_ctx *ctx, double *wake_ms, int64_t *kicks, int64_t *learned_kicks);
+
+#define B2E_CSR_PAGE_HEADER 12
+int b2e_set_csr_pages(b2e_ctx *ctx, int32_t record);
+int b2e_csr_pages(b2e_ctx *ctx, double *pages, int64_t capacity, int64_t *written);
+
 /* ---- batched wake integral (wake-network data) ------------------------
  * For each of n_profiles histograms (dev_counts: [n_profiles][bins] real
  * counts, bin width 1) the CSRCSBEND wake pipeline of one kick

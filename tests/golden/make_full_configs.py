@@ -1,7 +1,7 @@
 """Golden results of elegant's own tracking code at the full sizes of the
 benchmark cases, and the helpers that rebuild their inputs.
 
-    python tests/golden/make_full_configs.py [ring] [chicane] [ensemble] [train]
+    python tests/golden/make_full_configs.py [ring] [edge] [chicane] [ensemble] [train]
 
 runs oracle/_ref (elegant's multipole.c, csbend.c, simple_rfca.c, ... compiled
 from the reference sources by oracle/Makefile.ref) on this host and writes
@@ -19,6 +19,10 @@ Cases (one per benchmark configuration that tracks particles):
   full_ring_libm.npz, and the same glibc run with every x moved by one ulp
   gives the ring's own sensitivity envelope.  Both runs are spread over
   particle slices with the whole beam's RFCA fiducial (reforacle.track_split).
+- edge: 2,000 particles around the ring's dynamic-aperture boundary, 1,000
+  turns: the loss pairs of both maths modes (and of glibc with x moved by one
+  ulp), which carry the loss comparison that the matched beam (no losses)
+  cannot.
 - chicane: 1,000,000 particles through the four-dipole CSR chicane (BINS=600,
   SG_HALFWIDTH=2, 4 x 20 kicks, CSRDRIFT 5/1/5 m): final coordinates and the
   digest of every per-kick wake array (DeltaGamma of CSRCSBEND's OUTPUT_FILE).
@@ -50,6 +54,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 FIXTURE = os.path.join(HERE, "full_configs.json")
 RING_LIBM = os.path.join(HERE, "full_ring_libm.npz")
 ENSEMBLE_HISTORY = os.path.join(HERE, "full_ensemble_history.npz")
+EDGE_LOSSES = os.path.join(HERE, "full_edge_losses.npz")
 CHICANE_P0 = 1000 / 0.51099895
 RING_TURNS = 1000
 ENSEMBLE_INSTANCES = 32
@@ -105,6 +110,22 @@ def twiss_from(fixture_twiss):
 def ring_inputs(twiss):
     from elegant_b200 import workloads as w
     return w.fodo_ring(), w.ring_beam(10000, seed=12345, twiss=twiss)
+
+
+def edge_inputs():
+    """2,000 particles around the ring's dynamic-aperture boundary (x 12-13.3
+    mm, |y| <= 3 mm, |delta| <= 0.5 %): most are lost between the first
+    pass and the thousandth."""
+    from elegant_b200 import workloads as w
+    from elegant_b200.beam import Beam
+    rng = np.random.Generator(np.random.PCG64(4711))
+    n = 2000
+    c = np.zeros((n, 6))
+    c[:, 0] = rng.uniform(0.012, 0.0133, n) * rng.choice([-1.0, 1.0], n)
+    c[:, 2] = rng.uniform(-0.003, 0.003, n)
+    c[:, 5] = rng.uniform(-0.005, 0.005, n)
+    c[:, 4] = rng.uniform(-0.003, 0.003, n)
+    return w.fodo_ring(), Beam(c, np.arange(1, n + 1))
 
 
 def chicane_inputs():
@@ -192,6 +213,34 @@ def make_ring(out):
     out["ring"] = res
 
 
+def make_edge(out):
+    """The dynamic-aperture edge beam, 1,000 turns: loss pairs of the
+    reference in both maths modes and of the glibc build with x moved by one
+    ulp, and the shared-maths survivors' digest."""
+    from elegant_b200 import workloads as w
+    from reforacle import track_split
+    lat, beam = edge_inputs()
+    p0 = w.ring_p_central()
+    t = time.time()
+    res = {"input": digest_beam(beam.coords, beam.ids), "turns": RING_TURNS}
+    pairs = {}
+    for math in ("b2e", "libm"):
+        rows, nl, eff, t0 = track_split(math, lat, beam.coords, beam.ids, p0, RING_TURNS)
+        c, ids, lp = rows_result(rows)
+        pairs[math] = np.asarray(lost_pairs(ids, lp), dtype=np.int64)
+        res[math] = {"n_left": int(nl), "effort": float(eff), "lost": digest_lost(ids, lp),
+                     "survivors": digest_survivors(c, ids, lp)}
+    pert = beam.coords.copy()
+    pert[:, 0] = np.nextafter(pert[:, 0], np.inf)
+    rows, _, _, _ = track_split("libm", lat, pert, beam.ids, p0, RING_TURNS)
+    _, ids, lp = rows_result(rows)
+    pairs["libm_one_ulp"] = np.asarray(lost_pairs(ids, lp), dtype=np.int64)
+    res["libm_one_ulp_lost"] = digest_lost(ids, lp)
+    np.savez_compressed(EDGE_LOSSES, **pairs)
+    res["seconds"] = time.time() - t
+    out["edge"] = res
+
+
 def make_chicane(out):
     from reforacle import RefOracle
     lat, beam = chicane_inputs()
@@ -261,8 +310,8 @@ def make_train(out):
 
 def main(which):
     out = load_fixture() if os.path.exists(FIXTURE) else {}
-    for name, fn in (("ring", make_ring), ("chicane", make_chicane), ("ensemble", make_ensemble),
-                     ("train", make_train)):
+    for name, fn in (("ring", make_ring), ("edge", make_edge), ("chicane", make_chicane),
+                     ("ensemble", make_ensemble), ("train", make_train)):
         if name in which:
             t = time.time()
             fn(out)
@@ -273,4 +322,4 @@ def main(which):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["ring", "chicane", "ensemble", "train"])
+    main(sys.argv[1:] or ["ring", "edge", "chicane", "ensemble", "train"])

@@ -109,6 +109,31 @@ class RefOracle:
         return out[:n], nl.value, eff.value, wakes[: ww.value]
 
 
+CAPTURE_COLUMNS = ["DeltaGamma", "LinearDensity", "LinearDensityDeriv", "DeltaGammaT1", "DeltaGammaT2", "s",
+                   "GammaDeriv"]
+CAPTURE_PARAMS = ["Pass", "Kick", "dsKick", "pCentral", "Angle", "SlippageLength", "TotalBunchLength", "BinSize",
+                  "DerbenevRatio"]
+
+
+def captured_pages(ref: "RefOracle") -> dict:
+    """What the last capture_wakes run's CSRCSBEND OUTPUT_FILE writer was given:
+    every column (all pages concatenated) and the parameters, one row per page."""
+    lib = ref.lib
+    lib.b2e_ref_capture_get.restype = ctypes.c_long
+    lib.b2e_ref_capture_params.restype = ctypes.c_long
+    out = {}
+    for i, name in enumerate(CAPTURE_COLUMNS):
+        k = lib.b2e_ref_capture_get(i, None, ctypes.c_long(0))
+        buf = np.zeros(max(k, 1))
+        lib.b2e_ref_capture_get(i, buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(k))
+        out[name] = buf[:k]
+    k = lib.b2e_ref_capture_params(None, ctypes.c_long(0))
+    buf = np.zeros(max(k, 1))
+    lib.b2e_ref_capture_params(buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(k))
+    out["parameters"] = buf[:k].reshape(-1, len(CAPTURE_PARAMS))
+    return out
+
+
 def with_fiducial(lattice, t0: float):
     """The lattice with T_REFERENCE = t0 on its RFCA elements."""
     from elegant_b200.lattice import Element, Lattice

@@ -386,3 +386,47 @@ def test_csr_histogram_filters_bit_exact(case):
     rows, nl, _, ref_wakes = RefOracle("b2e", private=True).track(lat, beam.coords, beam.ids, P0, 1,
                                                                   capture_wakes=True)
     check(res, wakes, rows, nl, ref_wakes)
+
+
+@pytest.mark.parametrize("variant", ["default", "steady_plain", "igf"])
+def test_csr_wake_output_file_matches_reference(ref_b2e, tmp_path, variant):
+    """CSRCSBEND's OUTPUT_FILE: the engine's page records written as SDDS by
+    elegant_b200.sdds.write_csr_wake (one file per dipole, one page per
+    kick), read back with the protocol reader of tests/sdds_protocol.py, equal
+    bit for bit to what the reference's own writer was handed on the same run
+    (every column and parameter of every page; the IGF wake has no T1/T2)."""
+    from elegant_b200.sdds import write_csr_wake
+    from reforacle import CAPTURE_PARAMS, captured_pages
+    from sdds_protocol import SddsFile
+    lat = w.chicane(bins=150, n_kicks=5)
+    extra = {"steady_plain": {"STEADY_STATE": 1, "TRAPAZOID_INTEGRATION": 0}, "igf": {"STEADY_STATE": 1, "IGF": 1},
+             "default": {}}[variant]
+    lat = Lattice([Element(e.name, e.type, dict(e.params, **extra)) if e.type == "CSRCSBEND" else e
+                   for e in lat.elements])
+    beam = w.chicane_beam(12000, seed=23)
+    with Tracker(lat, P0, 1) as t:
+        t.set_csr_pages(True)
+        t.track(beam)
+        pages = t.csr_pages()
+    ref_b2e.track(lat, beam.coords, beam.ids, P0, 1, capture_wakes=True)
+    cap = captured_pages(ref_b2e)
+    assert len(pages) == cap["parameters"].shape[0] == 4 * 5
+    read = []
+    for el in sorted({p["element"] for p in pages}):
+        path = tmp_path / f"wake_{el}.sdds"
+        write_csr_wake(path, [p for p in pages if p["element"] == el])
+        f = SddsFile(path)
+        assert [c["name"] for c in f.columns] == ["s", "LinearDensity", "LinearDensityDeriv", "DeltaGamma",
+                                                  "GammaDeriv", "DeltaGammaT1", "DeltaGammaT2"]
+        read += f.pages
+    columns = ["s", "LinearDensity", "LinearDensityDeriv", "DeltaGamma", "GammaDeriv"]
+    if variant != "igf":
+        columns += ["DeltaGammaT1", "DeltaGammaT2"]
+    for name in columns:
+        ours = np.concatenate([pg["columns"][name] for pg in read])
+        assert ours.shape == cap[name].shape, name
+        bad = np.flatnonzero(ours != cap[name])
+        assert bad.size == 0, f"{name}: {bad.size} values differ, first {bad[:5]}"
+    for k, name in enumerate(CAPTURE_PARAMS):
+        ours = np.array([pg["parameters"][name] for pg in read], dtype=np.float64)
+        assert np.array_equal(ours, cap["parameters"][:, k]), name

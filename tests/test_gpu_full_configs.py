@@ -7,6 +7,8 @@ ensemble history).
   reference with the shared elementary functions; against the reference
   with glibc's, every coordinate inside the ring's own one-ulp sensitivity
   envelope and the identical (ID, loss pass) set.
+- edge: 2,000 particles around the ring's dynamic aperture x 1,000 turns:
+  the loss set equal to both references'.
 - chicane: 1,000,000 particles, BINS=600, 80 dipole kicks: coordinates and
   every per-kick wake array bit-identical.
 - ensemble: 32 full-size instances x 1,000 turns: every instance's survivors
@@ -59,6 +61,26 @@ def test_full_ring_1000_turns(fixture):
     diff = fc._rel(ref["coords"][alive], res.coords[order][alive])
     envelope = np.asarray(g["libm"]["envelope"])
     assert (diff <= 20 * envelope + 1e-15).all(), (diff, envelope)
+
+
+def test_ring_dynamic_aperture_edge_1000_turns(fixture):
+    """2,000 particles around the dynamic-aperture boundary, 1,000 turns:
+    losses spread over the whole run; the (ID, loss pass) set equals both the
+    shared-maths and the glibc reference's (which here agree with each other
+    and with glibc after a one-ulp change of x), survivors bit-identical to
+    the shared-maths reference."""
+    g = fixture["edge"]
+    lat, beam = fc.edge_inputs()
+    assert fc.digest_beam(beam.coords, beam.ids) == g["input"]
+    with Tracker(lat, w.ring_p_central(), g["turns"]) as t:
+        res = t.track(beam)
+    lost = _lost(res)
+    assert len(lost) > 1000 and sum(p > 100 for _, p in lost) > 50
+    ref = np.load(fc.EDGE_LOSSES)
+    assert lost == ref["b2e"].tolist() == ref["libm"].tolist()
+    assert fc.digest_lost(res.ids, res.lost_pass) == g["b2e"]["lost"] == g["libm"]["lost"]
+    assert res.n_left == g["b2e"]["n_left"] and res.effort == g["b2e"]["effort"]
+    assert fc.digest_survivors(res.coords, res.ids, res.lost_pass) == g["b2e"]["survivors"]
 
 
 def test_full_chicane_1m_particles(fixture):

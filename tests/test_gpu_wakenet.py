@@ -172,3 +172,66 @@ def test_wakenet_training_reduces_loss():
             net.train_step(xi, ti, 1e-3)
         last = net.train_step(xi, ti, 1e-3, want_loss=True)
     assert last < 0.2 * first, (first, last)
+
+
+def test_learned_wake_gains_over_the_method_without_it(capsys):
+    """The trained wake network against the method without it -- the plain
+    FP64 integral that it replaces, and the same network untrained -- on
+    held-out profiles (a seed training never used), and in tracking.
+
+    Accuracy: the trained network reproduces the plain wake to well under
+    the 1 % gate on held-out profiles; untrained, the same network is off by
+    its whole output.  Time: the wake stage of every kick of a 4-bunch
+    chicane run, timed inside the engine with events around the plain wake
+    kernel, or the learned wake's filter + network + combine kernels.  Both
+    are reported; the learned stage is not asserted to be faster (it is
+    not: the plain integral is a few microseconds per bunch on one CTA)."""
+    import json as _json
+    import torch
+    from elegant_b200 import Beam, Tracker, workloads as w
+    from elegant_b200.bunch_train import DEFAULT_NET
+    from elegant_b200.wake_surrogate import WakeSurrogate, build_set, evaluate
+    from elegant_b200.wakenet import init_params
+    sur = WakeSurrogate.load(DEFAULT_NET, max_batch=256)
+    held_out = build_set(2000, sur.features.bins, seed=9001)
+    trained = evaluate(sur, held_out)
+    raw = WakeSurrogate.load(DEFAULT_NET, max_batch=256)
+    raw.net.set_params(init_params(5))
+    untrained = evaluate(raw, held_out)
+    assert trained["wake_rel_rms_mean"] < 0.01 and trained["wake_within_1pct"] > 0.95
+    assert untrained["wake_rel_rms_mean"] > 20 * trained["wake_rel_rms_mean"]
+
+    lat = w.chicane()
+    parts, next_id = [], 1
+    for k, (n, h) in enumerate(zip([200_000, 300_000, 150_000, 250_000], [-12.0, -7.0, -9.0, -14.0])):
+        b = w.chicane_beam(n, seed=60 + k, chirp=h)
+        parts.append(Beam(b.coords, np.arange(next_id, next_id + n)))
+        next_id += n
+    beam = Beam(np.concatenate([p.coords for p in parts]), np.concatenate([p.ids for p in parts]))
+    offsets = np.concatenate([[0], np.cumsum([p.n for p in parts])]).astype(np.int64)
+    stage, sigma = {}, {}
+    net16 = WakeSurrogate.load(DEFAULT_NET, max_batch=16)
+    for mode in ("plain", "learned"):
+        with Tracker(lat, 1000 / 0.51099895, 1) as t:
+            t.load_ensemble(offsets, [])
+            if mode == "learned":
+                t.set_csr_surrogate(net16, tolerance=0.01, gate_stride=16)
+            t.track(beam)  # warm-up
+            t.set_csr_timing(True)
+            res = t.track(beam)
+            stage[mode] = t.csr_wake_timing()
+            if mode == "learned":
+                stats = t.csr_surrogate_stats()
+        sigma[mode] = [res.coords[offsets[b]:offsets[b + 1], 5].std() for b in range(4)]
+    assert stage["plain"]["kicks"] == stage["learned"]["kicks"] == 80
+    assert stage["plain"]["learned_kicks"] == 0 and stage["learned"]["learned_kicks"] == 80
+    assert stats["fallbacks"] == 0
+    assert max(abs(a - b) / b for a, b in zip(sigma["learned"], sigma["plain"])) < 1e-4
+    summary = {"held_out_wake_rel_rms": {"trained": trained["wake_rel_rms_mean"],
+                                         "untrained": untrained["wake_rel_rms_mean"], "plain": 0.0},
+               "wake_stage_ms_per_kick_4_bunches": {"plain": stage["plain"]["ms_per_kick"],
+                                                    "learned": stage["learned"]["ms_per_kick"]},
+               "gate_error_p95": float(np.percentile(stats["gate_errors"], 95))}
+    with capsys.disabled():
+        print("\nlearned wake vs plain integral:", _json.dumps(summary))
+    assert stage["plain"]["ms_per_kick"] > 0 and stage["learned"]["ms_per_kick"] > 0
