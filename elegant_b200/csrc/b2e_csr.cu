@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
     Q3 = YP * f;
     const RadSite no_rad = {0, 0, 0, 0, 0, nullptr};
     const int nsub = (int)c[CB_NSUB];
-    int lost = B2E_UNROLL >= 1 && nsub == 4 ? csbend_integrate<false, 4>(X, Q1, Y, Q3, Q4, DP, c, 1, nsub, false, ap, e, no_rad)
+    int lost = nsub == 4 ? csbend_integrate<false, 4>(X, Q1, Y, Q3, Q4, DP, c, 1, nsub, false, ap, e, no_rad)
                          : csbend_integrate<false>(X, Q1, Y, Q3, Q4, DP, c, 1, nsub, false, ap, e, no_rad);
     f = 1 / sqrt(((1 + DP) * (1 + DP) - Q1 * Q1) - Q3 * Q3);
     Q1 = Q1 * f;
@@ -2425,6 +2425,83 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   STATIC_TRY(cudaGetLastError());
   STATIC_TRY(launch_post_element_sweep(P, n, nullptr, 0, 0, s));
   return B2E_OK;
+}
+
+/* Network inputs of batched profiles (b2e_wake_features), one CTA per
+ * profile: the tracking path's feature step (csr_sur_filter_kernel) on
+ * bin-unit density and derivative. */
+namespace b2e {
+__global__ void wake_features_kernel(const double *dens, const double *deriv, const double *slip, int nb,
+                                     double sc_dens, double sc_deriv, int shift, float *inputs, double *scales) {
+  __shared__ double red[1024];
+  const int p = blockIdx.x;
+  const double *h = dens + (size_t)p * nb, *d = deriv + (size_t)p * nb;
+  float *in = inputs + (size_t)p * 4 * nb;
+  double part = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    part += h[i];
+  double total = block_sum(part, red);
+  total = total > 1e-300 ? total : 1e-300;
+  part = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    const double g = d[i] / total;
+    part += g * g;
+  }
+  const double ms = block_sum(part, red) / nb;
+  double k = sqrt(ms);
+  k = 1.0 / (k > 1e-300 ? k : 1e-300);
+  const double sv = slip[p];
+  long long dis = (long long)floor(sv);
+  dis = dis < 1 ? 1 : (dis > nb ? nb : dis);
+  const float code = (float)(log2((double)dis) / log2((double)nb));
+  const double fd = k / total * sc_dens, fg = k / total * sc_deriv;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    in[i] = (float)(h[i] * fd);
+    in[nb + i] = (float)(d[i] * fg);
+    in[2 * nb + i] = code;
+    in[3 * nb + i] = shift && i + dis < nb ? (float)(h[i + dis] * fd) : 0.f;
+  }
+  if (threadIdx.x == 0) {
+    scales[2 * p] = total;
+    scales[2 * p + 1] = k;
+  }
+}
+
+__global__ void wake_t1_kernel(const float *y, const double *scales, const double *slip, int nb, double sc_target,
+                               double *t1) {
+  const int p = blockIdx.x;
+  const double total = scales[2 * p], k = scales[2 * p + 1];
+  const bool empty = slip[p] < 1; /* diS = 0: the integral is empty */
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    t1[(size_t)p * nb + i] = empty ? 0.0 : (double)y[(size_t)p * nb + i] / sc_target / k * total;
+}
+} // namespace b2e
+
+extern "C" int b2e_wake_features(const double *dev_density, const double *dev_derivative,
+                                 const double *dev_slippage_bins, int32_t n_profiles, int32_t bins,
+                                 double density_scale, double derivative_scale, int32_t shift, float *dev_inputs,
+                                 double *dev_scales, void *stream) {
+  if (!dev_density || !dev_derivative || !dev_slippage_bins || !dev_inputs || !dev_scales || n_profiles < 0 ||
+      bins < 2)
+    return B2E_ERR_ARG;
+  if (n_profiles == 0)
+    return B2E_OK;
+  b2e::wake_features_kernel<<<n_profiles, 1024, 0, (cudaStream_t)stream>>>(
+      dev_density, dev_derivative, dev_slippage_bins, bins, density_scale, derivative_scale, shift, dev_inputs,
+      dev_scales);
+  return cudaGetLastError() == cudaSuccess ? B2E_OK : B2E_ERR_CUDA;
+}
+
+extern "C" int b2e_wake_t1_from_output(const float *dev_y, const double *dev_scales, const double *dev_slippage_bins,
+                                       int32_t n_profiles, int32_t bins, double target_scale, double *dev_t1,
+                                       void *stream) {
+  if (!dev_y || !dev_scales || !dev_slippage_bins || !dev_t1 || n_profiles < 0 || bins < 2)
+    return B2E_ERR_ARG;
+  if (n_profiles == 0)
+    return B2E_OK;
+  b2e::wake_t1_kernel<<<n_profiles, 256, 0, (cudaStream_t)stream>>>(dev_y, dev_scales, dev_slippage_bins, bins,
+                                                                   target_scale, dev_t1);
+  return cudaGetLastError() == cudaSuccess ? B2E_OK : B2E_ERR_CUDA;
 }
 
 /* Batched wake integral for the wake-network data set: n_profiles histograms

@@ -200,14 +200,12 @@ __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &
 
 /* kick `step` of a slice of the kick integrator (multipole.c:1264-1351):
  * the canonical multipole kick of the element's order, the KSEXT K1/J1
- * terms, momenta back to slopes and the radiation block; ORDER = 0 reads the
- * order from the element. */
-template <bool RAD, int ORDER>
+ * terms, momenta back to slopes and the radiation block. */
+template <bool RAD>
 __device__ __forceinline__ int kmult_kick(double x, double y, double &xp, double &yp, double &qx, double &qy,
-                                          double &dp, const DevElem &e, int order_rt, int step, int nSub, int slice,
+                                          double &dp, const DevElem &e, int order, int step, int nSub, int slice,
                                           const RadSite &rs) {
   const double *c = e.c;
-  const int order = ORDER > 0 ? ORDER : order_rt;
   const double kick = c[KM_KICK0 + step];
   double sumFx, sumFy, dqx = 0, dqy = 0;
   /* apply_canonical_multipole_kicks (multipole.h:213-245): coefficients
@@ -270,15 +268,14 @@ __device__ __forceinline__ int kmult_kick(double x, double y, double &xp, double
   return LOSS_NONE;
 }
 
-/* NSUB > 0 / ORDER > 0: substep count and multipole order as compile-time
- * constants (4 and 1 or 2 for KQUAD/KSEXT at the default integration order),
- * the slice unrolled; 0 takes them from the element.  The same operations in
- * the same order either way. */
-template <bool RAD, int NSUB = 0, int ORDER = 0>
+/* The slice loop stays rolled: unrolled instances for 4 substeps measured
+ * slower in the fused ring kernel (more registers live across the unrolled
+ * body, more spills). */
+template <bool RAD>
 __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g,
                                      const RadSite &rs) {
   const double *c = e.c;
-  const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = NSUB > 0 ? NSUB : (int)c[KM_NSUB];
+  const int order = (int)c[KM_ORDER], nSlices = (int)c[KM_NSLICES], nSub = (int)c[KM_NSUB];
   const double dx = c[KM_DX], dy = c[KM_DY];
   double x, xp, y, yp, s, dp, qx, qy, denom;
   int i_kick, lost;
@@ -312,29 +309,16 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
       p.y = y;
       return LOSS_APERTURE;
     }
-    if constexpr (NSUB > 0) {
-#pragma unroll
-      for (int step = 0; step < NSUB; step++) {
-        const double dsh = c[KM_DSH0 + step];
-        x = x + xp * dsh;
-        y = y + yp * dsh;
-        s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
-        if (step < NSUB - 1) /* kickFrac[last] == 0 ends the slice */
-          if ((lost = kmult_kick<RAD, ORDER>(x, y, xp, yp, qx, qy, dp, e, order, step, nSub, i_kick, rs)))
-            return lost;
-      }
-    } else {
 #pragma unroll 1
-      for (int step = 0; step < nSub; step++) {
-        const double dsh = c[KM_DSH0 + step];
-        x = x + xp * dsh;
-        y = y + yp * dsh;
-        s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
-        if (step == nSub - 1) /* kickFrac[last] == 0 ends the slice */
-          break;
-        if ((lost = kmult_kick<RAD, ORDER>(x, y, xp, yp, qx, qy, dp, e, order, step, nSub, i_kick, rs)))
-          return lost;
-      }
+    for (int step = 0; step < nSub; step++) {
+      const double dsh = c[KM_DSH0 + step];
+      x = x + xp * dsh;
+      y = y + yp * dsh;
+      s = s + dsh * sqrt((1 + xp * xp) + yp * yp);
+      if (step == nSub - 1) /* kickFrac[last] == 0 ends the slice */
+        break;
+      if ((lost = kmult_kick<RAD>(x, y, xp, yp, qx, qy, dp, e, order, step, nSub, i_kick, rs)))
+        return lost;
     }
   }
   if (!mult_aperture_ok(x + dx, y + dy, ap, e)) {
@@ -446,8 +430,9 @@ __device__ __forceinline__ void bend_kick(double X, double &QX, double &QY, doub
 }
 
 /* NSUB > 0: the substep count is a compile-time constant (4 for the default
- * INTEGRATION_ORDER=4) and the slice is unrolled; NSUB = 0 takes nSub from
- * the element.  The same operations in the same order either way. */
+ * INTEGRATION_ORDER=4) and the slice is unrolled (the CSR slice kernel: 5 %
+ * less time per kick); NSUB = 0 takes nSub from the element.  The same
+ * operations in the same order either way. */
 template <bool RAD, int NSUB = 0>
 __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y, double &QY, double &dist,
                                                 double &DPoP, const double *c, int nSlices, int nSub_rt,
@@ -535,14 +520,9 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   Q2 = y;
   Q3 = yp * f;
 
-#ifndef B2E_UNROLL
-#define B2E_UNROLL 2
-#endif
-  if (B2E_UNROLL >= 1 && nSub == 4)
-    lost = csbend_integrate<RAD, 4>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e,
-                                    rs);
-  else
-    lost = csbend_integrate<RAD>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e, rs);
+  /* rolled here: in the fused ring kernel the unrolled slice measured
+   * slower (register pressure); the CSR slice kernel takes the unrolled one */
+  lost = csbend_integrate<RAD>(Q0, Q1, Q2, Q3, Q4, dp, c, nSlices, nSub, (e.flags & EF_RADBLOCK) != 0, ap, e, rs);
 
   /* convertFromDipoleCanonicalCoordinates (csbend.c:1421-1429) */
   f = 1 / sqrt(((1 + dp) * (1 + dp) - Q1 * Q1) - Q3 * Q3);

@@ -177,17 +177,7 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
           rs.elem = ie;
           rs.rc = rads[ie].c;
         }
-        {
-          /* the default integration order (4 substeps) and the KQUAD/KSEXT
-           * orders take unrolled instances */
-          const int ksub = (int)e.c[KM_NSUB], kord = (int)e.c[KM_ORDER];
-          if (B2E_UNROLL >= 2 && ksub == 4 && kord == 1)
-            lost = kmult<RAD, 4, 1>(p, e, ap, L.g, rs);
-          else if (B2E_UNROLL >= 2 && ksub == 4 && kord == 2)
-            lost = kmult<RAD, 4, 2>(p, e, ap, L.g, rs);
-          else
-            lost = kmult<RAD>(p, e, ap, L.g, rs);
-        }
+        lost = kmult<RAD>(p, e, ap, L.g, rs);
         break;
       case K_CSBEND:
         if (RAD) {

@@ -129,12 +129,17 @@ __global__ void __launch_bounds__(128, 1)
  *            shifted 128x64 activation boxes through a WN_STAGES-deep ring;
  *   warp 1   one thread issues UMMA 128x64x16 (4 per tap, 20 per tile) into
  *            one of two TMEM accumulators and commits to free the stage;
- *   warps 2-5 epilogue: TMEM -> registers (warp w reads lanes 32*(w%4)..),
+ *   warps 2-9 epilogue: TMEM -> registers (warp w reads lanes 32*(w%4)..;
+ *            warps 2-5 take channels 0-31, warps 6-9 channels 32-63),
  *            bias + GELU (hidden), output channel 0 (output), or times
  *            GELU'(z) of the previous layer (backward data), BF16 stores.
+ *            The erf/exp of GELU and GELU' bound the epilogue, hence two
+ *            warps per lane quadrant.
  * Bounded waits everywhere; a timeout sets the status word and every role
  * leaves its loop. */
-constexpr int CONV_THREADS = 192;
+constexpr int CONV_EPI_WARPS = 8;
+constexpr int CONV_THREADS = 64 + 32 * CONV_EPI_WARPS;
+constexpr int WG_THREADS = 192;
 constexpr size_t CONV_W_BYTES = (size_t)WN_TAPS * 64 * 128;  /* 40 KB */
 constexpr size_t CONV_STAGE_BYTES = 128 * 128;               /* 16 KB */
 constexpr size_t CONV_SMEM = 1024 + CONV_W_BYTES + WN_STAGES * CONV_STAGE_BYTES;
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     }
     for (int i = 0; i < 2; i++) {
       mbar_init(&tfull[i], 1);
-      mbar_init(&tempty[i], 4);
+      mbar_init(&tempty[i], CONV_EPI_WARPS);
     }
     mbar_init(&wbar, 1);
     fence_barrier_init();
@@ -245,37 +250,45 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
       }
     }
   } else {
-    const int q = warp & 3;
-    const int r = q * 32 + lane; /* row of the tile this thread owns */
+    const int q = warp & 3;               /* the TMEM lane quadrant this warp may read */
+    const int half = (warp - 2) >> 2;     /* channels [32 half, 32 half + 32) */
+    constexpr int NC = N == 64 ? 32 : N;  /* channels per thread */
+    const int c0 = N == 64 ? 32 * half : 0;
+    const bool works = N == 64 || half == 0; /* the output layer's channel 0: one warp per quadrant */
+    const int r = q * 32 + lane;           /* row of the tile this thread owns */
     uint32_t j = 0;
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, j++) {
       const uint32_t acc = j & 1;
       if (!mbar_wait(&tfull[acc], (j >> 1) & 1, a.status, ST_TIMEOUT_EPI))
         break;
       tc_fence_after();
-      float v[N];
-      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + acc * 64;
+      float v[NC];
+      if (works) {
+        const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + acc * 64 + c0;
 #pragma unroll
-      for (int c = 0; c < N; c += 16)
-        tmem_ld16(base + c, v + c);
-      tmem_wait_ld();
+        for (int c = 0; c < NC; c += 16)
+          tmem_ld16(base + c, v + c);
+        tmem_wait_ld();
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0)
         mbar_arrive(&tempty[acc]);
+      if (!works)
+        continue;
       const int b = tile / tpp, l0 = (tile - b * tpp) << 7;
       const size_t row = (size_t)b * a.L + l0 + r;
       if (EPI == EPI_OUTPUT) {
         a.y_out[row] = v[0] + sbias[0];
       } else if (EPI == EPI_HIDDEN) {
-        uint4 *zo = a.z_out ? reinterpret_cast<uint4 *>(a.z_out + row * 64) : nullptr;
-        uint4 *ao = reinterpret_cast<uint4 *>(a.a_out + row * 64);
+        uint4 *zo = a.z_out ? reinterpret_cast<uint4 *>(a.z_out + row * 64 + c0) : nullptr;
+        uint4 *ao = reinterpret_cast<uint4 *>(a.a_out + row * 64 + c0);
 #pragma unroll
-        for (int c = 0; c < 64; c += 8) {
+        for (int c = 0; c < NC; c += 8) {
           float z[8];
 #pragma unroll
           for (int i = 0; i < 8; i++)
-            z[i] = v[c + i] + sbias[c + i];
+            z[i] = v[c + i] + sbias[c0 + c + i];
           if (zo)
             zo[c / 8] = make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]),
                                    pack_bf16(z[6], z[7]));
@@ -283,10 +296,10 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
                                  pack_bf16(gelu_f(z[4]), gelu_f(z[5])), pack_bf16(gelu_f(z[6]), gelu_f(z[7])));
         }
       } else {
-        const uint4 *zp = reinterpret_cast<const uint4 *>(a.z_prev + row * 64);
-        uint4 *go = reinterpret_cast<uint4 *>(a.a_out + row * 64);
+        const uint4 *zp = reinterpret_cast<const uint4 *>(a.z_prev + row * 64 + c0);
+        uint4 *go = reinterpret_cast<uint4 *>(a.a_out + row * 64 + c0);
 #pragma unroll
-        for (int c = 0; c < 64; c += 8) {
+        for (int c = 0; c < NC; c += 8) {
           uint4 zz = zp[c / 8];
           const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&zz);
           float g[8];
@@ -323,7 +336,7 @@ constexpr int WG_STAGES = 2;
 constexpr size_t WG_STAGE_BYTES = 6 * CONV_STAGE_BYTES; /* 96 KB */
 constexpr size_t WG_SMEM = 1024 + WG_STAGES * WG_STAGE_BYTES;
 
-__global__ void __launch_bounds__(CONV_THREADS, 1)
+__global__ void __launch_bounds__(WG_THREADS, 1)
     wgrad_kernel(const __grid_constant__ CUtensorMap t_in, const __grid_constant__ CUtensorMap t_dz, WgradArgs a) {
   extern __shared__ __align__(1024) unsigned char dsm[];
   unsigned char *sm = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);
@@ -460,7 +473,7 @@ cudaError_t launch_wgrad(const CUtensorMap &t_in, const CUtensorMap &t_dz, const
   cudaError_t e = cudaFuncSetAttribute(wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)WG_SMEM);
   if (e != cudaSuccess)
     return e;
-  wgrad_kernel<<<grid, CONV_THREADS, WG_SMEM, s>>>(t_in, t_dz, a);
+  wgrad_kernel<<<grid, WG_THREADS, WG_SMEM, s>>>(t_in, t_dz, a);
   return cudaGetLastError();
 }
 

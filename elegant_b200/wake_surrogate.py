@@ -202,10 +202,26 @@ class WakeSurrogate:
         return s
 
     def predict_t1(self, hist, deriv, slip_bins):
-        x = self.features.inputs(hist, deriv, slip_bins)
+        """T1 of every profile by the network: the engine's feature kernel,
+        the network, and its back-transform kernel, with no host-side glue."""
+        import torch
+        n, nb = hist.shape
+        f = self.features
+        lib = self.net.lib
+        stream = torch.cuda.current_stream().cuda_stream
+        x = torch.empty((n, 4, nb), dtype=torch.float32, device=hist.device)
+        scales = torch.empty((n, 2), dtype=torch.float64, device=hist.device)
+        t1 = torch.empty((n, nb), dtype=torch.float64, device=hist.device)
+        hist, deriv, slip_bins = hist.contiguous(), deriv.contiguous(), slip_bins.contiguous()
+        rc = lib.b2e_wake_features(hist.data_ptr(), deriv.data_ptr(), slip_bins.data_ptr(), n, nb, f.dens_scale,
+                                   f.deriv_scale, int(f.shift_channel), x.data_ptr(), scales.data_ptr(), stream)
+        if rc != nat.B2E_OK:
+            raise nat.EngineError(rc, "b2e_wake_features failed")
         y = self.net.forward(x)
-        t1 = self.features.t1_from_output(y, hist, deriv)
-        t1[slip_bins < 1] = 0  # diS = 0: the integral is empty
+        rc = lib.b2e_wake_t1_from_output(y.data_ptr(), scales.data_ptr(), slip_bins.data_ptr(), n, nb,
+                                         f.target_scale, t1.data_ptr(), stream)
+        if rc != nat.B2E_OK:
+            raise nat.EngineError(rc, "b2e_wake_t1_from_output failed")
         return t1
 
 
@@ -239,7 +255,7 @@ def evaluate(sur: WakeSurrogate, data: dict) -> dict:
 def timing(sur: WakeSurrogate, data: dict, n: int, reps: int = 5) -> dict:
     """Device time per profile: the plain FP64 wake (smoothing, derivative and
     integral) against the surrogate path (the same smoothing and derivative,
-    then pack + network)."""
+    then the feature kernel, the network and the back-transform kernel)."""
     import torch
     counts, slip = data["counts"][:n].contiguous(), data["slip"][:n].contiguous()
     zero = torch.zeros_like(slip)

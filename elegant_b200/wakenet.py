@@ -52,6 +52,9 @@ def _bind(lib):
         "b2e_wakenet_train_step": (ctypes.c_int, [vp, vp, vp, i32, ctypes.c_float, ctypes.POINTER(ctypes.c_double),
                                                   vp]),
         "b2e_csr_wake_batch": (ctypes.c_int, [vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, vp, vp, vp, vp]),
+        "b2e_wake_features": (ctypes.c_int, [vp, vp, vp, i32, i32, ctypes.c_double, ctypes.c_double, i32, vp, vp,
+                                             vp]),
+        "b2e_wake_t1_from_output": (ctypes.c_int, [vp, vp, vp, i32, i32, ctypes.c_double, vp, vp]),
         "b2e_umma_selftest": (ctypes.c_int, [ctypes.c_int, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():

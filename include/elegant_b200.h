@@ -377,6 +377,23 @@ int b2e_csr_wake_batch(const double *dev_counts, const double *dev_slippage_bins
                        int32_t trapezoid, int32_t steady, double *dev_t1, double *dev_density, double *dev_derivative,
                        void *stream);
 
+/* Network inputs and back-transform for batched profiles, as the tracking
+ * path forms them per kick (one CTA per profile, no host glue):
+ * b2e_wake_features reads dev_density and dev_derivative ([n][bins] FP64,
+ * bin units, from b2e_csr_wake_batch) and the slippage in bins, and writes
+ * dev_inputs [n][4][bins] FP32 -- density and derivative over their total,
+ * times k = 1/rms(derivative/total) and the channel scales, the code
+ * log2(diS)/log2(bins) with diS = clamp(floor(s), 1, bins), and the scaled
+ * density at bin i + diS (zero past the end; all zero when shift is 0) --
+ * and dev_scales [n][2] (total, k).  b2e_wake_t1_from_output turns the
+ * network output dev_y [n][bins] back into T1 = y / target_scale / k * total
+ * (zero for a slippage under one bin).  No counterpart in the reference. */
+int b2e_wake_features(const double *dev_density, const double *dev_derivative, const double *dev_slippage_bins,
+                      int32_t n_profiles, int32_t bins, double density_scale, double derivative_scale, int32_t shift,
+                      float *dev_inputs, double *dev_scales, void *stream);
+int b2e_wake_t1_from_output(const float *dev_y, const double *dev_scales, const double *dev_slippage_bins,
+                            int32_t n_profiles, int32_t bins, double target_scale, double *dev_t1, void *stream);
+
 /* ---- wake network (learned CSR wake integral) --------------------------
  * A 6-layer 1-D convolutional network (64 channels, 5 taps, per-layer
  * dilations, GELU) that maps a binned profile -- smoothed density, its
