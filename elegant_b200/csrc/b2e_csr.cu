@@ -218,6 +218,20 @@ __global__ void __launch_bounds__(256, 4) csr_slice_kernel(DevParticles P, int64
  * shared-memory integer counts, then added to global counts. */
 static const int kHistUnroll = 4;
 
+/* Copies of the shared-memory counts per histogram CTA: warp w adds into
+ * copy w % copies, so warps of a CTA do not queue on the central bins' counters
+ * (integer counts: the sum over copies is the same in any order).  As many
+ * as fit 48 KB, at most B2E_HIST_COPIES. */
+#ifndef B2E_HIST_COPIES
+#define B2E_HIST_COPIES 8
+#endif
+static inline size_t hist_smem(int nBins) {
+  const size_t one = sizeof(unsigned int) * (size_t)nBins;
+  size_t copies = (48 * 1024) / one;
+  copies = copies < 1 ? 1 : (copies > B2E_HIST_COPIES ? B2E_HIST_COPIES : copies);
+  return copies * one;
+}
+
 /* histogram CTAs (1024 threads) per bunch: one per 1024 particles, at most two
  * resident CTAs per SM over all bunches (each thread then takes up to
  * kHistUnroll particles per sweep) */
@@ -257,7 +271,12 @@ __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigne
   double lower = value_of(st->ct_min_key), upper = value_of(st->ct_max_key), dct;
   expand_range(&lower, &upper, factor);
   dct = (upper - lower) / nBins;
-  for (int b = threadIdx.x; b < nBins; b += blockDim.x)
+  /* the launch gives copies x nBins counters (hist_smem) */
+  unsigned int smem_bytes;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(smem_bytes));
+  const int copies = (int)(smem_bytes / (sizeof(unsigned int) * nBins));
+  unsigned int *mycount = scount + (size_t)((threadIdx.x >> 5) % copies) * nBins;
+  for (int b = threadIdx.x; b < copies * nBins; b += blockDim.x)
     scount[b] = 0;
   __syncthreads();
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -302,16 +321,20 @@ __global__ void csr_hist_kernel(DevParticles P, int64_t n, CsrBunches B, unsigne
       if (__any_sync(0xffffffffu, lane > 0 && bin >= 0 && bin == prev)) {
         const unsigned int peers = __match_any_sync(0xffffffffu, bin);
         if (bin >= 0 && lane == __ffs(peers) - 1)
-          atomicAdd(&scount[bin], (unsigned int)__popc(peers));
+          atomicAdd(&mycount[bin], (unsigned int)__popc(peers));
       } else if (bin >= 0) {
-        atomicAdd(&scount[bin], 1u);
+        atomicAdd(&mycount[bin], 1u);
       }
     }
   }
   __syncthreads();
-  for (int b = threadIdx.x; b < nBins; b += blockDim.x)
-    if (scount[b])
-      atomicAdd(&counts[b], scount[b]);
+  for (int b = threadIdx.x; b < nBins; b += blockDim.x) {
+    unsigned int c = 0;
+    for (int k = 0; k < copies; k++)
+      c += scount[(size_t)k * nBins + b];
+    if (c)
+      atomicAdd(&counts[b], c);
+  }
 }
 
 struct WakeArgs {
@@ -1709,7 +1732,7 @@ static int stupakov_drift(CsrState &st, const CsrElem &ce, const CsrBunches &B, 
     CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * nb * nbunch, stream));
     const int64_t per = (n + nbunch - 1) / nbunch;
     const int hb = hist_blocks(per, nbunch);
-    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), sizeof(unsigned int) * nb, stream, P, n, H,
+    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), hist_smem(nb), stream, P, n, H,
                             st.d_counts, nb, bend.binRangeFactor));
     (*launches)++;
     CSR_CUDA(cudaGetLastError());
@@ -1918,7 +1941,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
       CSR_CUDA(cudaMemsetAsync(st.d_counts, 0, sizeof(unsigned int) * ce.bins * nbunch, stream));
     int64_t per = (n + nbunch - 1) / nbunch;
     int hb = hist_blocks(per, nbunch);
-    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), sizeof(unsigned int) * ce.bins, stream, P,
+    CSR_CUDA(launch_chained(csr_hist_kernel, dim3(hb, nbunch), dim3(1024), hist_smem(ce.bins), stream, P,
                             n, B, st.d_counts, ce.bins, ce.binRangeFactor));
     (*launches)++;
     CSR_CUDA(cudaGetLastError());

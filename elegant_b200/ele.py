@@ -1,0 +1,429 @@
+"""The subset of elegant's run file (.ele) that drives tracking on the engine.
+
+elegant reads namelist commands (namelist.h syntax: ``&name key = value,
+key[1] = value, key[0] = 3*value, ... &end``) and runs them in order
+(elegant.c, main command loop).  For a tracking job the commands on this
+path are
+
+- &run_setup (elegant.nl:21-61): lattice, use_beamline, rootname,
+  p_central / p_central_mev, default_order, random_number_seed, and the
+  phase-space files final and output (both written with the beam at the end
+  of the step: this runner has no per-pass output) and losses; ``%s`` in a
+  file name is the rootname (the .ele file's name without extension, as
+  elegant's compose_filename forms it);
+- &run_control (vary.nl:8-19): n_steps, n_passes;
+- &bunched_beam (bunched_beam.nl:9-60): Gaussian beams matched to the given
+  Twiss parameters, emittances (geometric, or normalised emit_n / beta
+  gamma), sigma_dp, sigma_s, dp_s_coupling, momentum_chirp, centroid,
+  distribution_cutoff (a Gaussian truncated at that many sigma, values
+  redrawn), enforce_rms_values (the sample's emittance made exact; its
+  Twiss parameters always are, as generate_bunch does), symmetrize (each
+  particle with its mirror images, so odd moments vanish),
+  n_particles_per_bunch;
+- &twiss_output with matched = 1 and &bunched_beam use_twiss_command_values
+  = 1: the beam is matched to the periodic Twiss parameters of the line;
+- &track: runs n_steps steps of n_passes passes.
+
+A command outside this list, or a key of these commands away from its
+default that the engine does not implement, raises EleError naming it: the
+job belongs to elegant, not to this engine.  elegant's random-number streams
+(the SDDS toolkit's generators) are not in the reference tree, so beams are
+drawn from numpy's PCG64 seeded with random_number_seed: the same
+distribution, not the same particles.
+
+CSRCSBEND OUTPUT_FILE (a string parameter of the .lte) is written through
+the engine's page records (Tracker.set_csr_pages, sdds.write_csr_wake).
+"""
+from __future__ import annotations
+
+import math
+import os
+import re
+
+import numpy as np
+
+from .beam import Beam, ME_MEV
+from .lattice import parse_lte
+
+
+class EleError(ValueError):
+    """A run file the engine does not run."""
+
+
+# ------------------------------------------------------------------ parsing ----
+def _strip_comments(text: str) -> str:
+    """Drop everything from an unquoted "!" to the end of its line."""
+    out = []
+    for line in text.splitlines():
+        quote, cut = False, len(line)
+        i = 0
+        while i < len(line):
+            ch = line[i]
+            if ch == "\\" and quote:
+                i += 2
+                continue
+            if ch == '"':
+                quote = not quote
+            elif ch == "!" and not quote:
+                cut = i
+                break
+            i += 1
+        out.append(line[:cut])
+    return "\n".join(out)
+
+
+def _quoted(body: str, pos: int):
+    """The string starting at the quote at pos (backslash escapes kept as
+    the escaped character) and the position after its closing quote."""
+    out, i = [], pos + 1
+    while i < len(body) and body[i] != '"':
+        if body[i] == "\\" and i + 1 < len(body):
+            i += 1
+        out.append(body[i])
+        i += 1
+    if i >= len(body):
+        raise EleError("unterminated string in a namelist")
+    return "".join(out), i + 1
+
+
+def _tokens(body: str):
+    """Split a namelist body into (key, index, values) assignments."""
+    pos, n = 0, len(body)
+    items = []
+    while pos < n:
+        m = re.compile(r"\s*,?\s*([A-Za-z_][A-Za-z0-9_]*)\s*(\[\s*(\d+)\s*\])?\s*=\s*").match(body, pos)
+        if not m:
+            rest = body[pos:].strip(" \t\r\n,")
+            if rest:
+                raise EleError(f"cannot parse namelist text near {rest[:40]!r}")
+            break
+        key, index = m.group(1).lower(), int(m.group(3)) if m.group(3) else 0
+        pos = m.end()
+        values = []
+        while True:
+            while pos < n and body[pos] in " \t\r\n":
+                pos += 1
+            rep = 1
+            mr = re.compile(r"(\d+)\*").match(body, pos)
+            if mr:
+                rep, pos = int(mr.group(1)), mr.end()
+            if pos < n and body[pos] == '"':
+                v, pos = _quoted(body, pos)
+            else:
+                j = pos
+                while j < n and body[j] not in ", \t\r\n":
+                    j += 1
+                v, pos = body[pos:j], j
+            values += [v] * rep
+            k = pos
+            while k < n and body[k] in " \t\r\n":
+                k += 1
+            if k < n and body[k] == ",":
+                # another value of the same key follows unless a new
+                # assignment or the end of the command does
+                if re.compile(r",\s*[A-Za-z_][A-Za-z0-9_]*\s*(\[\s*\d+\s*\])?\s*=").match(body, k) or \
+                        not body[k + 1:].strip():
+                    pos = k + 1
+                    break
+                pos = k + 1
+                continue
+            pos = k
+            break
+        items.append((key, index, values))
+    return items
+
+
+def _commands(text: str):
+    """(name, body) of every "&name ... &end", skipping quoted text."""
+    i, n = 0, len(text)
+    while True:
+        i = text.find("&", i)
+        if i < 0:
+            return
+        m = re.compile(r"&([A-Za-z_][A-Za-z0-9_]*)").match(text, i)
+        if not m or m.group(1).lower() == "end":
+            i += 1
+            continue
+        j, quote = m.end(), False
+        while j < n:
+            if text[j] == "\\" and quote:
+                j += 2
+                continue
+            if text[j] == '"':
+                quote = not quote
+            elif not quote and text.startswith("&end", j):
+                break
+            j += 1
+        yield m.group(1).lower(), text[m.end():j]
+        i = j + 4
+
+
+def parse_namelists(text: str):
+    """[(command, {key: value or [values]})] in file order; values are
+    strings, converted by the consumer against the command's defaults."""
+    text = _strip_comments(text)
+    out = []
+    for name, body in _commands(text):
+        fields = {}
+        for key, index, values in _tokens(body):
+            if index == 0 and len(values) == 1 and key not in fields:
+                fields[key] = values[0]
+            else:
+                cur = fields.get(key)
+                arr = list(cur) if isinstance(cur, list) else ([cur] if cur is not None else [])
+                while len(arr) < index + len(values):
+                    arr.append(None)
+                arr[index:index + len(values)] = values
+                fields[key] = arr
+        out.append((name, fields))
+    return out
+
+
+# ----------------------------------------------------------------- commands ----
+RUN_SETUP = {"lattice": None, "use_beamline": None, "rootname": None, "output": None, "final": None,
+             "losses": None, "default_order": 2, "random_number_seed": 987654321, "p_central": 0.0,
+             "p_central_mev": 0.0, "print_statistics": 0, "concat_order": 0, "wrap_around": 1,
+             "tracking_updates": 1, "echo_lattice": 0, "show_element_timing": 0, "monitor_memory_usage": 0,
+             "semaphore_file": None, "search_path": None, "final_pass": 0, "always_change_p0": 0,
+             "back_tracking": 0, "element_divisions": 0, "s_start": 0.0, "load_balancing_on": 0,
+             "random_sequence_no": 1, "correction_iterations": 1, "suppress_parameter_defaults": 0,
+             "combine_bunch_statistics": 0, "losses_include_global_coordinates": 0, "expand_for": None}
+RUN_SETUP_UNSUPPORTED_FILES = ("centroid", "bpm_centroid", "sigma", "acceptance", "magnets", "parameters",
+                               "rfc_reference_output")
+RUN_CONTROL = {"n_steps": 1, "n_passes": 1, "bunch_frequency": 0.0, "n_indices": 0, "n_passes_fiducial": 0,
+               "terminate_on_failure": 0, "reset_rf_for_each_step": 1, "first_is_fiducial": 0,
+               "restrict_fiducialization": 0, "reset_scattering_seed": 0}
+BUNCHED_BEAM = {"bunch": None, "n_particles_per_bunch": 1, "time_start": 0.0, "matched_to_cell": None,
+                "emit_x": 0.0, "emit_nx": 0.0, "beta_x": 1.0, "alpha_x": 0.0, "eta_x": 0.0, "etap_x": 0.0,
+                "emit_y": 0.0, "emit_ny": 0.0, "beta_y": 1.0, "alpha_y": 0.0, "eta_y": 0.0, "etap_y": 0.0,
+                "use_twiss_command_values": 0, "use_moments_output_values": 0, "po": 0.0, "sigma_dp": 0.0,
+                "sigma_s": 0.0, "dp_s_coupling": 0.0, "emit_z": 0.0, "beta_z": 0.0, "alpha_z": 0.0,
+                "momentum_chirp": 0.0, "one_random_bunch": 1, "save_initial_coordinates": 1,
+                "limit_invariants": 0, "symmetrize": 0, "halton_sequence": [0, 0, 0], "optimized_halton": 0,
+                "randomize_order": [0, 0, 0], "limit_in_4d": 0, "enforce_rms_values": [0, 0, 0],
+                "distribution_cutoff": [2.0, 2.0, 2.0],
+                "distribution_type": ["gaussian", "gaussian", "gaussian"],
+                "centroid": [0.0] * 6, "first_is_fiducial": 0, "multiply_np_by_cores": 0,
+                "halton_radix": [0] * 6}
+TRACK = {"center_on_orbit": 0, "center_momentum_also": 1, "offset_by_orbit": 0, "offset_momentum_also": 1,
+         "soft_failure": 1, "use_linear_chromatic_matrix": 0, "longitudinal_ring_only": 0, "ibs_only": 0,
+         "stop_tracking_particle_limit": -1, "check_beam_structure": 0, "interrupt_file": "%s.interrupt"}
+TWISS_OUTPUT = {"matched": 1, "filename": None, "output_at_each_step": 0, "statistics": 0, "radiation_integrals": 0,
+                "beta_x": 1.0, "alpha_x": 0.0, "eta_x": 0.0, "etap_x": 0.0, "beta_y": 1.0, "alpha_y": 0.0,
+                "eta_y": 0.0, "etap_y": 0.0, "concat_order": 0}
+# commands that change nothing the tracking path computes
+INERT = {"global_settings", "print_dictionary", "semaphores", "stop", "subprocess", "run_rpnexpr"}
+
+
+def _convert(default, value):
+    if isinstance(default, list):
+        vals = value if isinstance(value, list) else [value]
+        out = list(default)
+        for i, v in enumerate(vals):
+            if v is not None:
+                out[i] = _convert(default[i] if i < len(default) else default[-1], v)
+        return out
+    if isinstance(default, float):
+        return float(value)
+    if isinstance(default, int) and not isinstance(default, bool):
+        return int(float(value))
+    return value
+
+
+def _command(fields: dict, defaults: dict, name: str, allowed: set) -> dict:
+    out = dict(defaults)
+    for k, v in fields.items():
+        if k not in defaults:
+            raise EleError(f"&{name}: {k} is not a parameter the engine's runner knows")
+        out[k] = _convert(defaults[k], v)
+        if k not in allowed and out[k] != defaults[k]:
+            raise EleError(f"&{name}: {k} = {v!r} is not supported by the engine's runner")
+    return out
+
+
+# ------------------------------------------------------------------ beam ----
+def _truncated_normal(rng, shape, cutoff):
+    g = rng.standard_normal(shape)
+    if cutoff and cutoff > 0:
+        bad = np.abs(g) > cutoff
+        while bad.any():
+            g[bad] = rng.standard_normal(int(bad.sum()))
+            bad = np.abs(g) > cutoff
+    return g
+
+
+def _plane(u, eps, beta, alpha):
+    """transform_from_normalized_coordinates: (u, u') of unit emittance to
+    the plane's (x, x') at (beta, alpha, eps)."""
+    x = math.sqrt(eps * beta) * u[:, 0]
+    xp = math.sqrt(eps / beta) * (u[:, 1] - alpha * u[:, 0])
+    return np.stack([x, xp], axis=1)
+
+
+def _enforce_twiss(c, beta1, alpha1, emit1, enforce_rms):
+    """elegant's enforceTwissValues (generate_bunch.c:1307-1335): the linear
+    map that takes the sample's own Twiss ellipse to (beta1, alpha1), scaled
+    to emittance emit1 when enforce_rms is set."""
+    d = c - c.mean(axis=0)
+    s11, s12, s22 = (d[:, 0] ** 2).mean(), (d[:, 0] * d[:, 1]).mean(), (d[:, 1] ** 2).mean()
+    emit = math.sqrt(max(s11 * s22 - s12 * s12, 0.0))
+    if not emit or not beta1:
+        return c
+    beta, alpha = s11 / emit, -s12 / emit
+    bm = math.sqrt(beta1 * beta)
+    r11, r21, r22 = beta1 / bm, (alpha - alpha1) / bm, beta / bm
+    if enforce_rms:
+        ratio = math.sqrt(emit1 / emit)
+        r11, r21, r22 = r11 * ratio, r21 * ratio, r22 * ratio
+    out = np.empty_like(c)
+    out[:, 1] = c[:, 0] * r21 + c[:, 1] * r22
+    out[:, 0] = c[:, 0] * r11
+    return out
+
+
+def bunched_beam(bb: dict, p_central: float, seed: int, twiss=None) -> Beam:
+    """A Gaussian bunch from &bunched_beam values, generated the way
+    generate_bunch (generate_bunch.c:57-480) builds one: per plane a
+    truncated unit Gaussian (values beyond distribution_cutoff redrawn),
+    mirrored into four quadrants with symmetrize, centred, transformed to the
+    plane's (beta, alpha, emittance) -- the longitudinal plane's from
+    sigma_s, sigma_dp and dp_s_coupling (:318-349) -- and then mapped so that
+    the sample's own Twiss parameters are exactly the requested ones, its
+    emittance too with enforce_rms_values (enforceTwissValues, :1307-1335);
+    then the chirp, dispersion and centroid."""
+    n = int(bb["n_particles_per_bunch"])
+    sym = int(bb["symmetrize"])
+    if sym and n % 4:
+        raise EleError("&bunched_beam: symmetrize needs n_particles_per_bunch divisible by 4")
+    for t in bb["distribution_type"]:
+        if t.lower() != "gaussian":
+            raise EleError(f"&bunched_beam: distribution_type {t!r} is not supported by the engine's runner")
+    rng = np.random.Generator(np.random.PCG64(seed))
+    m = n // 4 if sym else n
+    cut = bb["distribution_cutoff"]
+    enforce = bb["enforce_rms_values"]
+    # mirror signs of the four copies per plane: every odd moment of a plane
+    # and every product of two planes' coordinates cancels
+    mirror = ((1, -1, 1, -1), (1, 1, -1, -1), (1, -1, -1, 1))
+    c = np.empty((n, 6))
+    specs = []
+    for k, (emit, emit_n, beta, alpha) in enumerate(
+            ((bb["emit_x"], bb["emit_nx"], bb["beta_x"], bb["alpha_x"]),
+             (bb["emit_y"], bb["emit_ny"], bb["beta_y"], bb["alpha_y"]))):
+        if twiss is not None:
+            beta, alpha = (twiss.beta_x, twiss.alpha_x) if k == 0 else (twiss.beta_y, twiss.alpha_y)
+        specs.append((emit if emit else emit_n / p_central, beta, alpha))
+    sig_s, sig_dp, coupling = bb["sigma_s"], bb["sigma_dp"], bb["dp_s_coupling"]
+    s56 = sig_dp * sig_s * coupling
+    emit_z = math.sqrt(max((sig_dp * sig_s) ** 2 - s56 * s56, 0.0))
+    specs.append((emit_z, sig_s * sig_s / emit_z, -s56 / emit_z) if emit_z else (0.0, 0.0, 0.0))
+    for k, (eps, beta, alpha) in enumerate(specs):
+        u = _truncated_normal(rng, (m, 2), cut[k])
+        if sym:
+            u = np.concatenate([u * sgn for sgn in mirror[k]])
+        u -= u.mean(axis=0)
+        if beta:
+            pl = _plane(u, eps, beta, alpha)
+            pl = _enforce_twiss(pl, beta, alpha, eps, int(enforce[k]))
+        else:  # no longitudinal emittance: independent s and delta
+            pl = u * np.array([sig_s, sig_dp])
+        c[:, 2 * k:2 * k + 2] = pl
+    c[:, 5] += bb["momentum_chirp"] * c[:, 4]
+    eta = (bb["eta_x"], bb["etap_x"], bb["eta_y"], bb["etap_y"])
+    if twiss is not None:
+        eta = (twiss.eta_x, twiss.etap_x, 0.0, 0.0)
+    for k in range(4):
+        c[:, k] += eta[k] * c[:, 5]
+    c += np.asarray(bb["centroid"], dtype=np.float64)[None, :]
+    return Beam(c, np.arange(1, n + 1, dtype=np.int64))
+
+
+# ------------------------------------------------------------------- run ----
+def _lattice_with_outputs(text: str, use: str | None):
+    """parse_lte, with CSRCSBEND OUTPUT_FILE names collected (the runner writes them)."""
+    outputs = {}
+    return parse_lte(text, use, outputs=outputs), outputs
+
+
+def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
+    """Run a .ele file's tracking job on the engine; returns a summary per
+    step (survivors, effort) and the files written."""
+    from .optics import periodic_twiss
+    from .sdds import write_csr_wake, write_losses, write_phase_space
+    from .track import Tracker
+    base = os.path.dirname(os.path.abspath(path))
+    rootname = os.path.splitext(os.path.basename(path))[0]
+    with open(path) as fh:
+        cmds = parse_namelists(fh.read())
+    rs = rc = bb = tw = None
+    summary = {"steps": [], "files": []}
+    lattice = None
+    csr_outputs = {}
+
+    def name(f):
+        if not f:
+            return None
+        return os.path.join(base, f.replace("%s", rootname))
+
+    for cmd, fields in cmds:
+        if cmd == "run_setup":
+            rs = _command(fields, {**RUN_SETUP, **{k: None for k in RUN_SETUP_UNSUPPORTED_FILES}}, cmd,
+                          {"lattice", "use_beamline", "rootname", "output", "final", "losses", "default_order",
+                           "random_number_seed", "p_central", "p_central_mev", "print_statistics"})
+            if rs["rootname"]:
+                rootname = rs["rootname"]
+            with open(os.path.join(base, rs["lattice"])) as fh:
+                lattice, csr_outputs = _lattice_with_outputs(fh.read(), rs["use_beamline"])
+        elif cmd == "run_control":
+            rc = _command(fields, RUN_CONTROL, cmd, {"n_steps", "n_passes", "reset_rf_for_each_step"})
+        elif cmd == "twiss_output":
+            tw = _command(fields, TWISS_OUTPUT, cmd, {"matched", "filename"})
+            if tw["filename"]:
+                raise EleError("&twiss_output: filename (a Twiss output file) is not supported by the engine's runner")
+        elif cmd == "bunched_beam":
+            bb = _command(fields, BUNCHED_BEAM, cmd,
+                          {"n_particles_per_bunch", "emit_x", "emit_nx", "beta_x", "alpha_x", "eta_x", "etap_x",
+                           "emit_y", "emit_ny", "beta_y", "alpha_y", "eta_y", "etap_y", "sigma_dp", "sigma_s",
+                           "dp_s_coupling", "momentum_chirp", "one_random_bunch", "symmetrize",
+                           "enforce_rms_values", "distribution_cutoff", "distribution_type", "centroid",
+                           "use_twiss_command_values", "save_initial_coordinates"})
+        elif cmd == "track":
+            _command(fields, TRACK, cmd, {"soft_failure", "interrupt_file"})
+            if rs is None or bb is None:
+                raise EleError("&track needs &run_setup and &bunched_beam before it")
+            rc = rc or dict(RUN_CONTROL)
+            p0 = rs["p_central"] or rs["p_central_mev"] / ME_MEV
+            twiss = None
+            if bb["use_twiss_command_values"]:
+                if not tw or not tw["matched"]:
+                    raise EleError("use_twiss_command_values needs &twiss_output with matched = 1")
+                twiss = periodic_twiss(lattice)
+            outs = [f for f in (name(rs["final"]), name(rs["output"])) if f]
+            losses = name(rs["losses"])
+            for step in range(rc["n_steps"]):
+                if step == 0 or not bb["one_random_bunch"]:
+                    beam = bunched_beam(bb, p0, rs["random_number_seed"] + step, twiss)
+                with Tracker(lattice, p0, rc["n_passes"], device=device, default_order=rs["default_order"]) as t:
+                    if csr_outputs:
+                        t.set_csr_pages(True)
+                    res = t.track(beam)
+                    pages = t.csr_pages() if csr_outputs else []
+                summary["steps"].append({"step": step + 1, "survivors": res.n_left, "effort": res.effort})
+                charge = next((e.get("TOTAL") for e in lattice.elements if e.type == "CHARGE"), 0.0)
+                for f in outs:
+                    write_phase_space(f, res, p0, step=step + 1, charge=charge, mode=mode)
+                if losses:
+                    write_losses(losses, res, lattice, p0, step=step + 1, mode=mode)
+                for el_name, fname in csr_outputs.items():
+                    idx = set(lattice.index(el_name))
+                    mine = [p for p in pages if p["element"] in idx]
+                    if mine:
+                        write_csr_wake(name(fname), mine, mode=mode)
+                        summary["files"].append(name(fname))
+            summary["files"] += outs + ([losses] if losses else [])
+            summary["result"] = res
+        elif cmd in INERT:
+            continue
+        else:
+            raise EleError(f"&{cmd} is not a command the engine's runner implements")
+    return summary

@@ -209,8 +209,12 @@ def _split_params(s: str) -> list[str]:
     return [x.strip() for x in out if x.strip()]
 
 
-def parse_lte(text: str, use: str | None = None) -> Lattice:
-    """Read the supported subset of elegant's .lte format and expand the used line."""
+def parse_lte(text: str, use: str | None = None, outputs: dict | None = None) -> Lattice:
+    """Read the supported subset of elegant's .lte format and expand the used line.
+
+    outputs: if given, receives CSRCSBEND OUTPUT_FILE names by element name
+    (the file is written from the engine's page records, not by the engine
+    itself); without it such a parameter is an error."""
     stmts, cur = [], ""
     for raw in text.splitlines():
         line = raw.split("!")[0].rstrip()
@@ -251,6 +255,11 @@ def parse_lte(text: str, use: str | None = None) -> Lattice:
             if "=" not in p:
                 raise LatticeError(f"cannot parse parameter {p!r} of {name}")
             k, v = p.split("=", 1)
+            if k.strip().upper() == "OUTPUT_FILE" and etype == "CSRCSBEND":
+                if outputs is None:
+                    raise LatticeError(f"OUTPUT_FILE of {name}: pass outputs= to collect it (elegant_b200.ele)")
+                outputs[name] = v.strip().strip('"')
+                continue
             params[k.strip().upper()] = _value(v)
         if etype in elements:
             base = elements[etype]

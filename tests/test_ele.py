@@ -1,0 +1,125 @@
+"""The .ele runner (elegant_b200/ele.py): namelist parsing, &bunched_beam
+statistics, what it declines (CPU), and a tracking job end to end (GPU)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from elegant_b200.ele import BUNCHED_BEAM, EleError, bunched_beam, parse_namelists, run_ele
+
+REFERENCE = os.environ.get("ELEGANT_REFERENCE_TREE", "/root/reference")
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="needs the reference tree")
+def test_every_reference_run_file_parses():
+    """All of the reference's example .ele files: comments, quoted strings
+    with escapes, repeat counts (3*"gaussian") and indexed arrays."""
+    files = sorted(glob.glob(os.path.join(REFERENCE, "**", "*.ele"), recursive=True))
+    assert len(files) > 200
+    for f in files:
+        with open(f, errors="replace") as fh:
+            cmds = parse_namelists(fh.read())
+        assert cmds, f
+    with open(os.path.join(REFERENCE, "doc/examples/bunchCompression/bunchComp/fourDipoleCSR.ele")) as fh:
+        cmds = dict(parse_namelists(fh.read()))
+    bb = cmds["bunched_beam"]
+    assert bb["distribution_type"] == ["gaussian"] * 3 and bb["distribution_cutoff"] == ["3"] * 3
+    assert bb["enforce_rms_values"] == ["1", "1", "1"] and cmds["run_setup"]["final"] == "%s.fin"
+
+
+def test_namelist_syntax():
+    text = '''! a comment
+&run_setup lattice = "a b.lte", p_central_mev = 1e3, ! trailing comment
+   final = %s.fin &end
+&bunched_beam distribution_cutoff[1] = 2*4.5, centroid[4] = 1e-3, n_particles_per_bunch=8 &end
+&track &end'''
+    cmds = parse_namelists(text)
+    assert [c for c, _ in cmds] == ["run_setup", "bunched_beam", "track"]
+    assert cmds[0][1] == {"lattice": "a b.lte", "p_central_mev": "1e3", "final": "%s.fin"}
+    assert cmds[1][1]["distribution_cutoff"] == [None, "4.5", "4.5"]
+    assert cmds[1][1]["centroid"] == [None] * 4 + ["1e-3"]
+
+
+def _bb(**kw):
+    bb = dict(BUNCHED_BEAM)
+    bb.update(kw)
+    return bb
+
+
+def test_bunched_beam_statistics():
+    p0 = 1000 / 0.51099895
+    bb = _bb(n_particles_per_bunch=40000, emit_nx=1e-6, beta_x=8.0, alpha_x=1.5, emit_y=2e-9, beta_y=3.0,
+             alpha_y=-0.5, sigma_s=1e-3, sigma_dp=1e-4, momentum_chirp=-10.0, enforce_rms_values=[1, 1, 1],
+             distribution_cutoff=[3.0, 3.0, 3.0], centroid=[1e-4, 0, 0, 0, 0, 0])
+    b = bunched_beam(bb, p0, seed=3).coords
+    x = b[:, 0] - b[:, 0].mean()
+    xp = b[:, 1] - b[:, 1].mean()
+    ex = np.sqrt((x * x).mean() * (xp * xp).mean() - (x * xp).mean() ** 2)
+    assert abs(ex / (1e-6 / p0) - 1) < 1e-12  # enforced rms: the emittance exactly
+    assert abs((x * x).mean() / (1e-6 / p0 * 8.0) - 1) < 1e-12
+    assert abs(b[:, 0].mean() - 1e-4) < 1e-15
+    assert abs(b[:, 4].std() / 1e-3 - 1) < 1e-12
+    # chirp: delta = sigma_dp g + h s
+    slope = np.polyfit(b[:, 4], b[:, 5], 1)[0]
+    assert abs(slope + 10.0) < 0.1
+    # cutoff at 2 sigma: the truncated Gaussian's values end near 2 sigma
+    # (after centring and the exact-Twiss map, a little beyond it), where
+    # 20,000 untruncated draws would reach about 4
+    raw = bunched_beam(_bb(n_particles_per_bunch=20000, distribution_cutoff=[2.0, 2.0, 2.0], sigma_s=1.0,
+                           sigma_dp=1.0), p0, seed=4).coords
+    assert np.abs(raw[:, 4]).max() < 2.1
+    sym = bunched_beam(_bb(n_particles_per_bunch=4000, emit_x=1e-9, emit_y=1e-9, sigma_s=1e-3, sigma_dp=1e-3,
+                           symmetrize=1), p0, seed=5).coords
+    assert np.abs(sym.mean(axis=0)).max() < 1e-18
+
+
+def test_runner_declines_what_it_does_not_run(tmp_path):
+    lte = tmp_path / "a.lte"
+    lte.write_text("D: DRIF, L=1\nL1: LINE=(D)\n")
+    cases = [("&run_setup lattice = a.lte, p_central = 100, sigma = %s.sig &end\n&track &end", "sigma"),
+             ("&run_setup lattice = a.lte, p_central = 100 &end\n&sasefel beta = 1 &end", "sasefel"),
+             ("&run_setup lattice = a.lte, p_central = 100 &end\n&bunched_beam distribution_type[0] = "
+              '3*"uniform-ellipse", n_particles_per_bunch = 4 &end\n&track &end', "uniform-ellipse")]
+    for text, word in cases:
+        ele = tmp_path / "job.ele"
+        ele.write_text(text)
+        with pytest.raises(EleError, match=word):
+            run_ele(str(ele))
+
+
+@pytest.mark.gpu
+def test_runner_tracks_a_chicane_job(tmp_path):
+    """A CSR chicane job written as elegant would: the final file and the
+    dipole's OUTPUT_FILE come out, and the final coordinates equal a direct
+    engine run of the same generated beam."""
+    from elegant_b200 import Tracker
+    from elegant_b200.lattice import parse_lte
+    from sdds_protocol import SddsFile
+    (tmp_path / "chic.lte").write_text(
+        'Q: CHARGE, TOTAL=1e-9\n'
+        'B1: CSRCSBEND, L=0.5, ANGLE=0.05, N_KICKS=5, BINS=150, SG_HALFWIDTH=2, OUTPUT_FILE="%s.B1.wake"\n'
+        'B2: CSRCSBEND, L=0.5, ANGLE=-0.05, N_KICKS=5, BINS=150, SG_HALFWIDTH=2\n'
+        'D1: CSRDRIFT, L=2\n'
+        'BL: LINE=(Q, B1, D1, B2)\n')
+    (tmp_path / "job.ele").write_text(
+        '&run_setup lattice = chic.lte, use_beamline = BL, p_central_mev = 1000, final = %s.fin,\n'
+        '   random_number_seed = 77 &end\n'
+        '&run_control n_passes = 1 &end\n'
+        '&bunched_beam n_particles_per_bunch = 20000, emit_nx = 1e-6, emit_ny = 1e-6, beta_x = 10,\n'
+        '   beta_y = 10, sigma_s = 1e-3, sigma_dp = 1e-4, momentum_chirp = -10, distribution_cutoff[0] = 3*3 &end\n'
+        '&track &end\n')
+    out = run_ele(str(tmp_path / "job.ele"))
+    fin = SddsFile(str(tmp_path / "job.fin"))
+    wake = SddsFile(str(tmp_path / "job.B1.wake"))
+    assert len(wake.pages) == 5 and fin.pages[0]["parameters"]["Particles"] == out["steps"][0]["survivors"]
+    bb = dict(BUNCHED_BEAM, n_particles_per_bunch=20000, emit_nx=1e-6, emit_ny=1e-6, beta_x=10.0, beta_y=10.0,
+              sigma_s=1e-3, sigma_dp=1e-4, momentum_chirp=-10.0, distribution_cutoff=[3.0, 3.0, 3.0])
+    p0 = 1000 / 0.51099895
+    beam = bunched_beam(bb, p0, seed=77)
+    lat = parse_lte((tmp_path / "chic.lte").read_text(), "BL", outputs={})
+    with Tracker(lat, p0, 1) as t:
+        ref = t.track(beam)
+    alive = ref.lost_pass < 0
+    assert np.array_equal(fin.pages[0]["columns"]["x"], ref.coords[alive, 0])
+    assert np.array_equal(fin.pages[0]["columns"]["particleID"], ref.ids[alive])
