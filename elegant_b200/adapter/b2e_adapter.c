@@ -69,7 +69,8 @@ static const b2e_param_map map_csrcsbend[] = {BEND_COMMON,
 static const b2e_param_map map_rfca[] = {{"L", B2E_RFCA_L},         {"VOLT", B2E_RFCA_VOLT},
                                          {"PHASE", B2E_RFCA_PHASE}, {"FREQ", B2E_RFCA_FREQ},
                                          {"DX", B2E_RFCA_DX},       {"DY", B2E_RFCA_DY},
-                                         {"T_REFERENCE", B2E_RFCA_T_REFERENCE}, {"PHASE_REFERENCE", -1},
+                                         {"T_REFERENCE", B2E_RFCA_T_REFERENCE}, {"N_KICKS", B2E_RFCA_N_KICKS},
+                                         {"PHASE_REFERENCE", -1},
                                          END_MAP};
 static const b2e_param_map map_maxamp[] = {{"X_MAX", B2E_MAXAMP_X_MAX},
                                            {"Y_MAX", B2E_MAXAMP_Y_MAX},

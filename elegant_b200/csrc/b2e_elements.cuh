@@ -606,35 +606,105 @@ __device__ __forceinline__ void malign(Part &p, const double *c, double p_centra
   }
 }
 
-/* ---- RFCA, zero length, single kick: trackRfCavityWithWakes
- * (simple_rfca.c:295-985) with add_to_particle_energy (:987-1006) and the
- * final removeInvalidParticles sweep (limit_amplitudes.c:274-315). */
+/* ---- RFCA: trackRfCavityWithWakes (simple_rfca.c:295-985) without wakes,
+ * change_t, Q, linearisation or end focusing (rejected at load): the
+ * zero-length kick (one section), the drift-kick-drift sections of N_KICKS
+ * > 0 (:569-700), or the matrix method (:823-945), then the final
+ * removeInvalidParticles sweep (limit_amplitudes.c:274-315). */
+__device__ __forceinline__ void rf_half_drift(Part &p, double length) {
+  p.x = p.x + (p.xp * length) / 2;
+  p.y = p.y + (p.yp * length) / 2;
+  p.s = p.s + (length / 2) * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+}
+
+/* add_to_particle_energy (simple_rfca.c:987-1006) */
+__device__ __forceinline__ void rf_add_energy(Part &p, double t, double Po, double dgamma) {
+  double P, gamma, gamma1, P1, Pz, Pz1, PRatio;
+  P = Po * (1 + p.dp);
+  gamma1 = (gamma = sqrt(P * P + 1)) + dgamma;
+  if (gamma1 <= 1)
+    gamma1 = 1 + 1e-7;
+  P1 = sqrt(gamma1 * gamma1 - 1);
+  p.dp = (P1 - Po) / Po;
+  p.s = ((t * B2E_C_MKS) * P1) / gamma1;
+  Pz = P / sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+  Pz1 = sqrt((Pz * Pz + gamma1 * gamma1) - gamma * gamma);
+  PRatio = Pz / Pz1;
+  p.xp = p.xp * PRatio;
+  p.yp = p.yp * PRatio;
+}
+
 __device__ __forceinline__ int rfca(Part &p, const DevElem &e, const DevRfState &rs, const DevGlobals &g) {
   const double *c = e.c;
   const double Po = g.p_central;
+  const double length = c[RF_LENGTH];
+  if (c[RF_DRIFT_ONLY] != 0) {
+    /* zero voltage: the exact drift over the whole length (simple_rfca.c:380-392) */
+    const double L = length * c[RF_NKICKS];
+    if (L != 0) {
+      p.x = p.x + p.xp * L;
+      p.y = p.y + p.yp * L;
+      p.s = p.s + L * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+    }
+    return LOSS_NONE;
+  }
+  const int nKicks = (int)c[RF_NKICKS];
   p.x = p.x - c[RF_DX];
   p.y = p.y - c[RF_DY];
-  if (p.dp != -1) {
-    double P, gamma, beta_i, t, dgamma, gamma1, P1, Pz, Pz1, PRatio;
-    P = Po * (1 + p.dp);
-    gamma = sqrt(P * P + 1);
-    beta_i = P / gamma;
-    t = (p.s + 0.0) / (B2E_C_MKS * beta_i) - 0.0;
-    dgamma = (c[RF_VOLT] * b2e_sin(c[RF_OMEGA] * t + rs.phase)) * 1.0;
-    /* add_to_particle_energy */
-    gamma1 = gamma + dgamma;
-    if (gamma1 <= 1)
-      gamma1 = 1 + 1e-7;
-    P1 = sqrt(gamma1 * gamma1 - 1);
-    p.dp = (P1 - Po) / Po;
-    p.s = ((t * B2E_C_MKS) * P1) / gamma1;
-    Pz = P / sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
-    Pz1 = sqrt((Pz * Pz + gamma1 * gamma1) - gamma * gamma);
-    PRatio = Pz / Pz1;
-    p.xp = p.xp * PRatio;
-    p.yp = p.yp * PRatio;
-    if (gamma + dgamma <= 1)
-      p.dp = -1;
+  for (int ik = 0; ik < nKicks; ik++) {
+    if (c[RF_MATRIX] == 0) {
+      /* a section: half drift, energy kick at its centre's time, half drift */
+      if (p.dp != -1) {
+        double P, gamma, beta_i, t, dgamma, dc4;
+        dc4 = length != 0 ? (length / 2) * sqrt((1 + p.xp * p.xp) + p.yp * p.yp) : 0;
+        P = Po * (1 + p.dp);
+        gamma = sqrt(P * P + 1);
+        beta_i = P / gamma;
+        t = (p.s + dc4) / (B2E_C_MKS * beta_i) - 0.0;
+        dgamma = (c[RF_VOLT] * b2e_sin(c[RF_OMEGA] * ((t - 0.0) - ik * c[RF_DTLIGHT]) + rs.phase)) * 1.0;
+        if (length != 0)
+          rf_half_drift(p, length);
+        rf_add_energy(p, t, Po, dgamma);
+        if (gamma + dgamma <= 1)
+          p.dp = -1;
+      }
+      if (length != 0)
+        rf_half_drift(p, length); /* the final drift takes every particle */
+    } else {
+      /* matrix method, momentum-based body focusing (simple_rfca.c:855-945) */
+      double P, gamma, beta_i, t, dgamma, dP, ds1, R12, R22, x, xp;
+      const double R11 = 1, R21 = 0;
+      P = Po * (1 + p.dp);
+      gamma = sqrt(P * P + 1);
+      beta_i = P / gamma;
+      ds1 = (length / 2) * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+      t = (p.s + ds1) / (B2E_C_MKS * beta_i) - 0.0;
+      {
+        const double arg = c[RF_OMEGA] * ((t - 0.0) - ik * c[RF_DTLIGHT]) + rs.phase;
+        const double sin_phase = b2e_sin(arg);
+        dgamma = c[RF_VOLT] * sin_phase;
+      }
+      dP = sqrt((gamma + dgamma) * (gamma + dgamma) - 1) - P;
+      R22 = 1 / (1 + dP / P);
+      if (fabs(dP / P) > 1e-14)
+        R12 = length * ((P / dP) * b2e_log(1 + dP / P));
+      else
+        R12 = length;
+      p.s = p.s + ds1;
+      x = p.x;
+      xp = p.xp;
+      p.x = x * R11 + xp * R12;
+      p.xp = x * R21 + xp * R22;
+      x = p.y;
+      xp = p.yp;
+      p.y = x * R11 + xp * R12;
+      p.yp = x * R21 + xp * R22;
+      p.s = p.s + (length / 2) * sqrt((1 + p.xp * p.xp) + p.yp * p.yp);
+      p.dp = ((P + dP) - Po) / Po;
+      if ((gamma = gamma + dgamma) <= 1)
+        p.dp = -1;
+      p.s = (((P + dP) / gamma) * p.s) / beta_i;
+    }
   }
   p.x = p.x + c[RF_DX];
   p.y = p.y + c[RF_DY];

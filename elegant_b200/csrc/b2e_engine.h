@@ -116,6 +116,11 @@ enum {
 #define RF_T_REFERENCE 5
 #define RF_SOFFSET 6    /* length/2 used by the fiducial sum */
 #define RF_SLOT 7       /* index into the per-instance RF state table */
+#define RF_LENGTH 8     /* length of one kick's section, L/nKicks */
+#define RF_NKICKS 9
+#define RF_MATRIX 10    /* 1: matrix method (nonzero L, N_KICKS <= 0) */
+#define RF_DTLIGHT 11   /* RF_LENGTH / c */
+#define RF_DRIFT_ONLY 12 /* VOLT = 0: an exact drift over L (nothing for L = 0) */
 
 /* MALIGN constant slots */
 #define MA_DX 0

@@ -409,20 +409,36 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
 
 static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
   const double *p = el.p;
-  if (p[B2E_RFCA_L] != 0)
-    return "RFCA with nonzero length is not supported by this engine";
   if (p[B2E_RFCA_FREQ] == 0)
     return "RFCA with zero frequency is not supported by this engine";
+  if (p[B2E_RFCA_L] < 0)
+    return "RFCA with negative length (backtracking) is not supported by this engine";
   d.kind = K_RFCA;
+  /* nKicks = length ? N_KICKS : 1, the matrix method for nKicks <= 0;
+   * length and volt per section (simple_rfca.c:403-409) */
+  const double L = p[B2E_RFCA_L];
+  long nKicks = L != 0 ? (long)p[B2E_RFCA_N_KICKS] : 1;
+  int matrix = 0;
+  if (nKicks <= 0) {
+    matrix = 1;
+    nKicks = 1;
+  }
+  const double length = L / nKicks;
   /* volt = VOLT/(1e6*particleMassMV*particleRelSign)/nKicks, omega = PIx2*FREQ (simple_rfca.c:384-394) */
-  d.c[RF_VOLT] = p[B2E_RFCA_VOLT] / (1e6 * kME_MEV * 1) / 1;
+  d.c[RF_VOLT] = p[B2E_RFCA_VOLT] / (1e6 * kME_MEV * 1) / nKicks;
   d.c[RF_OMEGA] = (2 * kPI) * p[B2E_RFCA_FREQ];
   d.c[RF_PHASE_DEG_RAD] = p[B2E_RFCA_PHASE] * kPI / 180.0;
   d.c[RF_DX] = p[B2E_RFCA_DX];
   d.c[RF_DY] = p[B2E_RFCA_DY];
   d.c[RF_T_REFERENCE] = p[B2E_RFCA_T_REFERENCE];
-  d.c[RF_SOFFSET] = 0.0 / 2; /* length/2 with length 0 */
+  d.c[RF_SOFFSET] = length / 2; /* findFiducialTime's sOffset (simple_rfca.c:431) */
   d.c[RF_SLOT] = slot;
+  d.c[RF_LENGTH] = length;
+  d.c[RF_NKICKS] = (double)nKicks;
+  d.c[RF_MATRIX] = matrix;
+  d.c[RF_DTLIGHT] = length / kC_MKS;
+  /* VOLT = 0: an exact drift over L and nothing else (simple_rfca.c:380-392) */
+  d.c[RF_DRIFT_ONLY] = p[B2E_RFCA_VOLT] == 0;
   return "";
 }
 

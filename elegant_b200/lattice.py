@@ -53,7 +53,7 @@ SLOTS = {
     nat.KSEXT: dict(_KMULT, K2=1, K1=10, J1=11),
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,
-    nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6},
+    nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6, "N_KICKS": 7},
     nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "YEXPONENT": 4},
     nat.MARK: {},
     nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},

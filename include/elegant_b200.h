@@ -143,6 +143,7 @@ extern "C" {
 #define B2E_RFCA_DX 4
 #define B2E_RFCA_DY 5
 #define B2E_RFCA_T_REFERENCE 6
+#define B2E_RFCA_N_KICKS 7 /* with L > 0: 0 = matrix method, else drift-kick-drift sections (simple_rfca.c:403-408) */
 /* MAXAMP (maxamp_param, track_data.c:990) */
 #define B2E_MAXAMP_X_MAX 0
 #define B2E_MAXAMP_Y_MAX 1

@@ -881,7 +881,10 @@ static void malign_track(double **c, long np, const b2e_element *e, double Po) {
   }
 }
 
-/* ---- RFCA (zero length, TMEAN fiducial) ---------------------------------- */
+/* ---- RFCA (TMEAN fiducial): trackRfCavityWithWakes, simple_rfca.c:295-985 --
+ * the zero-length kick, drift-kick-drift sections for L > 0 with N_KICKS > 0
+ * (:569-700), the matrix method for L > 0 with N_KICKS <= 0 (:823-945), and
+ * VOLT = 0 as a plain drift (:380-392); no wakes, Q, change_t, end focus. */
 typedef struct {
   int seen;
   double phase_fiducial;
@@ -890,11 +893,29 @@ typedef struct {
 static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, double Po) {
   const double *p = e->p;
   double omega = (2 * PI_) * p[B2E_RFCA_FREQ];
-  double volt = p[B2E_RFCA_VOLT] / (1e6 * ME_MEV * 1) / 1;
-  double phase, t0;
-  long ip, itop;
+  double volt = p[B2E_RFCA_VOLT] / (1e6 * ME_MEV * 1);
+  double length = p[B2E_RFCA_L], dtLight, phase, t0;
+  long ip, itop, nKicks, ik;
+  int matrixMethod = 0;
   if (np <= 0)
     return np;
+  if (p[B2E_RFCA_VOLT] == 0) {
+    if (length)
+      for (ip = 0; ip < np; ip++) {
+        c[ip][0] += c[ip][1] * length;
+        c[ip][2] += c[ip][3] * length;
+        c[ip][4] += length * sqrt(1 + SQR(c[ip][1]) + SQR(c[ip][3]));
+      }
+    return np;
+  }
+  nKicks = length ? (long)p[B2E_RFCA_N_KICKS] : 1;
+  if (nKicks <= 0) {
+    matrixMethod = 1;
+    nKicks = 1;
+  }
+  length /= nKicks;
+  volt /= nKicks;
+  dtLight = length / C_MKS;
   if (!rs->seen) {
     if (p[B2E_RFCA_T_REFERENCE] != -1)
       t0 = p[B2E_RFCA_T_REFERENCE];
@@ -902,7 +923,7 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
       double tsum = 0, error = 0;
       for (ip = 0; ip < np; ip++) {
         double pp = Po * (1 + c[ip][5]);
-        double b = (c[ip][4] + 0.0 / 2) / (C_MKS * (pp / sqrt(pp * pp + 1)));
+        double b = (c[ip][4] + length / 2) / (C_MKS * (pp / sqrt(pp * pp + 1)));
         double Y = b + error, sum = tsum + Y;
         error = Y - (sum - tsum);
         tsum = sum;
@@ -918,28 +939,74 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
     c[ip][0] -= p[B2E_RFCA_DX];
     c[ip][2] -= p[B2E_RFCA_DY];
   }
-  for (ip = 0; ip < np; ip++) {
-    double *coord = c[ip], P, gamma, beta_i, t, dgamma, gamma1, P1, Pz, Pz1;
-    if (coord[5] == -1)
-      continue;
-    P = Po * (1 + coord[5]);
-    beta_i = P / (gamma = sqrt(SQR(P) + 1));
-    t = (coord[4] + 0) / (C_MKS * beta_i) - 0;
-    dgamma = volt * M_SIN(omega * (t - 0 - 0 * 0.0) + phase) * 1;
-    /* add_to_particle_energy */
-    P = Po * (1 + coord[5]);
-    gamma1 = (gamma = sqrt(P * P + 1)) + dgamma;
-    if (gamma1 <= 1)
-      gamma1 = 1 + 1e-7;
-    P1 = sqrt(gamma1 * gamma1 - 1);
-    coord[5] = (P1 - Po) / Po;
-    coord[4] = t * C_MKS * P1 / gamma1;
-    Pz = P / sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
-    Pz1 = sqrt(Pz * Pz + gamma1 * gamma1 - gamma * gamma);
-    coord[1] *= Pz / Pz1;
-    coord[3] *= Pz / Pz1;
-    if ((gamma1 = gamma + dgamma) <= 1)
-      coord[5] = -1;
+  for (ik = 0; ik < nKicks; ik++) {
+    if (!matrixMethod) {
+      for (ip = 0; ip < np; ip++) {
+        double *coord = c[ip], P, gamma, beta_i, t, dgamma, gamma1, P1, Pz, Pz1, dc4;
+        if (coord[5] == -1)
+          continue;
+        dc4 = length ? length / 2 * sqrt(1 + SQR(coord[1]) + SQR(coord[3])) : 0;
+        P = Po * (1 + coord[5]);
+        beta_i = P / (gamma = sqrt(SQR(P) + 1));
+        t = (coord[4] + dc4) / (C_MKS * beta_i) - 0;
+        dgamma = volt * M_SIN(omega * (t - 0 - ik * dtLight) + phase) * 1;
+        if (length) {
+          coord[0] += coord[1] * length / 2;
+          coord[2] += coord[3] * length / 2;
+          coord[4] += length / 2 * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+        }
+        /* add_to_particle_energy */
+        P = Po * (1 + coord[5]);
+        gamma1 = (gamma = sqrt(P * P + 1)) + dgamma;
+        if (gamma1 <= 1)
+          gamma1 = 1 + 1e-7;
+        P1 = sqrt(gamma1 * gamma1 - 1);
+        coord[5] = (P1 - Po) / Po;
+        coord[4] = t * C_MKS * P1 / gamma1;
+        Pz = P / sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+        Pz1 = sqrt(Pz * Pz + gamma1 * gamma1 - gamma * gamma);
+        coord[1] *= Pz / Pz1;
+        coord[3] *= Pz / Pz1;
+        if ((gamma1 = gamma + dgamma) <= 1)
+          coord[5] = -1;
+      }
+      if (length)
+        for (ip = 0; ip < np; ip++) {
+          c[ip][0] += c[ip][1] * length / 2;
+          c[ip][2] += c[ip][3] * length / 2;
+          c[ip][4] += length / 2 * sqrt(1 + SQR(c[ip][1]) + SQR(c[ip][3]));
+        }
+    } else {
+      for (ip = 0; ip < np; ip++) {
+        double *coord = c[ip], P, gamma, beta_i, t, dgamma, dP, ds1, sin_phase, R11 = 1, R21 = 0, R12, R22, x, xp;
+        P = Po * (1 + coord[5]);
+        beta_i = P / (gamma = sqrt(SQR(P) + 1));
+        ds1 = length / 2 * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+        t = (coord[4] + ds1) / (C_MKS * beta_i) - 0;
+        sin_phase = M_SIN(omega * (t - 0 - ik * dtLight) + phase);
+        dgamma = (volt * 1) * sin_phase;
+        dP = sqrt(SQR(gamma + dgamma) - 1) - P;
+        R22 = 1 / (1 + dP / P);
+        if (fabs(dP / P) > 1e-14)
+          R12 = length * (P / dP * M_LOG(1 + dP / P));
+        else
+          R12 = length;
+        coord[4] += ds1;
+        x = coord[0];
+        xp = coord[1];
+        coord[0] = x * R11 + xp * R12;
+        coord[1] = x * R21 + xp * R22;
+        x = coord[2];
+        xp = coord[3];
+        coord[2] = x * R11 + xp * R12;
+        coord[3] = x * R21 + xp * R22;
+        coord[4] += length / 2 * sqrt(1 + SQR(coord[1]) + SQR(coord[3]));
+        coord[5] = (P + dP - Po) / Po;
+        if ((gamma += dgamma) <= 1)
+          coord[5] = -1;
+        coord[4] = (P + dP) / gamma * coord[4] / beta_i;
+      }
+    }
   }
   itop = np - 1;
   for (ip = 0; ip < np; ip++) {

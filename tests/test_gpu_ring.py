@@ -361,3 +361,20 @@ def test_ring_with_exact_drifts(ref_b2e):
     assert 200 <= nl < 400
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+@pytest.mark.parametrize("rf", [{"L": 0.5, "N_KICKS": 0}, {"L": 0.5, "N_KICKS": 5}, {"VOLT": 0.0},
+                                {"L": 0.4, "VOLT": 0.0}], ids=["matrix", "kicks", "no_volt", "no_volt_drift"])
+def test_ring_rf_cavity_with_length(ref_b2e, rf):
+    """RFCA with a length by the matrix method and by drift-kick-drift
+    sections, and at zero voltage, bit-identical to the reference over 60
+    turns with losses."""
+    els = [Element(e.name, e.type, dict(e.params, **rf)) if e.type == "RFCA" else e for e in w.fodo_ring().elements]
+    lat = Lattice(els)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=31).coords, _lossy_beam(150, seed=32).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 150 <= nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

@@ -283,3 +283,25 @@ def test_port_reproduces_reference_with_exact_drifts(math):
     assert n1 == n2 and e1 == e2 and n1 < beam.n
     assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+
+
+def _ring_with_cavity(**rf):
+    from elegant_b200 import Element, Lattice
+    return Lattice([Element(e.name, e.type, dict(e.params, **rf)) if e.type == "RFCA" else e
+                    for e in w.fodo_ring().elements])
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("rf", [{"L": 0.5, "N_KICKS": 0}, {"L": 0.5, "N_KICKS": 5}, {"VOLT": 0.0},
+                                {"L": 0.4, "VOLT": 0.0}], ids=["matrix", "kicks", "no_volt", "no_volt_drift"])
+def test_port_reproduces_reference_rf_cavity_with_length(math, rf):
+    """RFCA with a length: the matrix method (N_KICKS = 0, simple_rfca.c:823-945),
+    drift-kick-drift sections (N_KICKS > 0, :569-700), and zero voltage
+    (:380-392), with losses."""
+    lat = _ring_with_cavity(**rf)
+    beam = lossy_beam(160, seed=17)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
