@@ -155,8 +155,13 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
   s = s / b0;
   if (e.flags & EF_EDGE1) {
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    XP = XP + (c[CB_TAN_E1] / rho) * X;
-    YP = YP - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * Y;
+    if (e.flags & EF_EDGE_ORDER2) {
+      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], c[CB_SEC2_E1],
+                       c[CB_EDGE_N], -1);
+    } else {
+      XP = XP + (c[CB_TAN_E1] / rho) * X;
+      YP = YP - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * Y;
+    }
   }
   P.x[i] = X;
   P.xp[i] = XP;
@@ -985,16 +990,21 @@ __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, Cs
   }
   if (e.flags & EF_EDGE2) {
     rho = (1 + DP) * c[CB_RHO_ACTUAL];
-    XP = XP + (c[CB_TAN_E2] / rho) * X;
-    YP = YP - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + DP)) / rho) * Y;
+    if (e.flags & EF_EDGE_ORDER2) {
+      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI2] * (1 + DP), c[CB_TAN_E2], c[CB_E2], c[CB_SEC2_E2],
+                       c[CB_EDGE_N], 1);
+    } else {
+      XP = XP + (c[CB_TAN_E2] / rho) * X;
+      YP = YP - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + DP)) / rho) * Y;
+    }
   }
-  x = (X * ct - Y * sn) + 0.0;
-  y = (X * sn + Y * ct) + 0.0;
-  xp = (XP * ct - YP * sn) + 0.0;
-  yp = (XP * sn + YP * ct) + 0.0;
+  x = (X * ct - Y * sn) + c[CB_ETILT0];
+  y = (X * sn + Y * ct) + c[CB_ETILT0 + 2];
+  xp = (XP * ct - YP * sn) + c[CB_ETILT0 + 1];
+  yp = (XP * sn + YP * ct) + c[CB_ETILT0 + 3];
   x = x + (c[CB_DXF] + c[CB_DZF] * xp);
   y = y + (c[CB_DYF] + c[CB_DZF] * yp);
-  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + 0.0);
+  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + c[CB_ETILT0 + 4]);
   P.x[i] = x;
   P.xp[i] = xp;
   P.y[i] = y;

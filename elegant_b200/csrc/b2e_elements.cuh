@@ -481,6 +481,30 @@ __device__ __forceinline__ double bend_edge_radiation(double x, double xp, doubl
   return (dp_prime * x) * tan_e;
 }
 
+/* Second-order dipole edge (K. L. Brown's non-symplectic map; csbend.c:4266-4307)
+ * for EDGE_ORDER >= 2: which = -1 at the entrance, +1 at the exit; rho is
+ * (1+delta)*rho_actual and psi the fringe angle times (1+delta).  The pole-face
+ * curvature term (H1/H2) is zero in this engine. */
+static __device__ __noinline__ void bend_edge_order2(double &x, double &xp, double &y, double &yp, double rho, double psi,
+                                              double tan_b, double beta, double sec2, double n, int which) {
+  const double w = (double)which, mw = (double)(-which);
+  const double h = 1 / rho, h2 = h * h, tan2 = tan_b * tan_b;
+  const double R21 = h * tan_b, R43 = -h * b2e_tan(beta - psi);
+  const double T111 = ((w * h) / 2) * tan2;
+  const double T133 = ((mw * h) / 2) * sec2;
+  const double T211 = which == -1 ? ((-n) * h2) * tan_b : ((-h2) * (n + tan2 / 2)) * tan_b;
+  const double T221 = (mw * h) * tan2, T331 = T221, T441 = -T221;
+  const double T233 = which == -1 ? (h2 * ((n + .5) + tan2)) * tan_b : (h2 * (n - tan2 / 2)) * tan_b;
+  const double T243 = (w * h) * tan2;
+  const double T431 = (h2 * (2 * n + (which == 1 ? sec2 : 0))) * tan_b;
+  const double T432 = (w * h) * sec2;
+  const double x0 = x, xp0 = xp, y0 = y, yp0 = yp;
+  x = (x0 + T111 * (x0 * x0)) + T133 * (y0 * y0);
+  xp = ((((xp0 + R21 * x0) + T211 * (x0 * x0)) + (T221 * x0) * xp0) + T233 * (y0 * y0)) + (T243 * y0) * yp0;
+  y = y0 + (T331 * x0) * y0;
+  yp = (((yp0 + R43 * y0) + (T441 * yp0) * x0) + (T431 * x0) * y0) + (T432 * xp0) * y0;
+}
+
 template <bool RAD>
 __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevAperture *ap, const DevGlobals &g,
                                       const RadSite &rs) {
@@ -504,9 +528,14 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE1) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    delta_xp = (c[CB_TAN_E1] / rho) * x;
-    xp = xp + delta_xp;
-    yp = yp - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * y;
+    if (e.flags & EF_EDGE_ORDER2) {
+      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], c[CB_SEC2_E1],
+                       c[CB_EDGE_N], -1);
+    } else {
+      delta_xp = (c[CB_TAN_E1] / rho) * x;
+      xp = xp + delta_xp;
+      yp = yp - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * y;
+    }
   }
 
   /* anticipate the radiation error of integrating the sector (csbend.c:1211-1216) */
@@ -556,17 +585,22 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE2) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    delta_xp = (c[CB_TAN_E2] / rho) * x;
-    xp = xp + delta_xp;
-    yp = yp - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + dp)) / rho) * y;
+    if (e.flags & EF_EDGE_ORDER2) {
+      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI2] * (1 + dp), c[CB_TAN_E2], c[CB_E2], c[CB_SEC2_E2],
+                       c[CB_EDGE_N], 1);
+    } else {
+      delta_xp = (c[CB_TAN_E2] / rho) * x;
+      xp = xp + delta_xp;
+      yp = yp - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + dp)) / rho) * y;
+    }
   }
 
-  /* back to the lab frame (csbend.c:1379-1388) */
-  p.x = (x * ct - y * st) + 0.0;
-  p.y = (x * st + y * ct) + 0.0;
-  p.xp = (xp * ct - yp * st) + 0.0;
-  p.yp = (xp * st + yp * ct) + 0.0;
-  p.s = s + 0.0;
+  /* back to the lab frame, plus the ETILT exit offsets (csbend.c:1359-1364) */
+  p.x = (x * ct - y * st) + c[CB_ETILT0];
+  p.y = (x * st + y * ct) + c[CB_ETILT0 + 2];
+  p.xp = (xp * ct - yp * st) + c[CB_ETILT0 + 1];
+  p.yp = (xp * st + yp * ct) + c[CB_ETILT0 + 3];
+  p.s = s + c[CB_ETILT0 + 4];
   p.dp = dp;
   p.x = p.x + (c[CB_DXF] + c[CB_DZF] * p.xp);
   p.y = p.y + (c[CB_DYF] + c[CB_DZF] * p.yp);

@@ -20,7 +20,7 @@
 #include <stdint.h>
 #include "../../include/elegant_b200.h"
 
-#define B2E_NC 40 /* constants per compiled element */
+#define B2E_NC 44 /* constants per compiled element (a DevElem stays a multiple of 16 bytes) */
 
 /* Compiled element kinds (device dispatch) */
 enum {
@@ -51,6 +51,7 @@ enum {
 #define EF_REVERSE_TILT 0x400   /* nonzero reverse tilt in the internal aperture check */
 #define EF_SR 0x800             /* KMULT / CSBEND: classical synchrotron radiation (SYNCH_RAD) */
 #define EF_ISR 0x1000           /* KMULT / CSBEND: quantum excitation (ISR) */
+#define EF_EDGE_ORDER2 0x2000   /* CSBEND: edges by the second-order map (EDGE_ORDER >= 2) */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -92,6 +93,10 @@ enum {
 #define CB_DZF 33
 #define CB_INV_RHO0 34  /* RN(1/rho0), for X/rho0 by div_rn_recip */
 #define CB_INV_RHO_ACTUAL 35 /* RN(1/rho_actual) */
+#define CB_ETILT0 36    /* exit offsets of ETILT (x, xp, y, yp, s), 36..40; zero without ETILT */
+#define CB_SEC2_E1 41   /* sqr(1/cos(e1)), second-order edges */
+#define CB_SEC2_E2 42   /* sqr(1/cos(e2)) */
+#define CB_EDGE_N 43    /* field index n = -b1/h of the second-order edge map */
 
 
 /* Radiation constants of a KMULT / CSBEND, in a table beside the element

@@ -264,6 +264,60 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
   return "";
 }
 
+/* ETILT: the bend is rolled by etilt about its entrance axis, so the exit
+ * face's centre moves off the design orbit.  Offsets (x, x', y, y', s) of that
+ * centre in the bend frame, then turned by -tilt into the frame the exit
+ * rotation leaves the particles in (csbend.c:4723-4769, the turn is
+ * tilt_matrices.c:123-150).  Zero when etilt is zero. */
+static void etilt_exit_offsets(double out[5], double rho0, double angle, double etilt, double tilt) {
+  for (int k = 0; k < 5; k++)
+    out[k] = 0;
+  if (etilt == 0)
+    return;
+  const double roll = -etilt; /* ETILT's sign convention is TILT's */
+  const double sa = b2e_sin(angle), ca = b2e_cos(angle), ta = b2e_tan(angle);
+  const double cr = b2e_cos(roll), sr = b2e_sin(roll);
+  /* exit centre of the rolled arc (a) and the unit tangent's out-of-plane
+   * part (uz); the in-plane parts are not needed */
+  const double ax = ((1 - ca) * rho0) * (cr - 1), az = ((1 - ca) * rho0) * sr;
+  const double norm = sqrt((sa * cr) * (sa * cr) + ca * ca);
+  const double uz = (sa * sr) / norm;
+  /* where the tangent line from a meets the design exit plane (b), the path
+   * length along it (dz) and the slope of the line in the bend plane */
+  const double tan_alpha = (1. / ta) / cr;
+  const double bx = (ax * tan_alpha) / (ta + tan_alpha);
+  const double by = -bx * ta;
+  const double dz = sqrt((bx - ax) * (bx - ax) + by * by);
+  out[0] = sqrt(bx * bx + by * by);
+  out[1] = b2e_tan(atan(tan_alpha) - (kPI / 2 - angle));
+  out[2] = az + uz * dz;
+  out[3] = uz;
+  out[4] = dz * sqrt(1 + uz * uz);
+  /* into the tilted frame: a turn by -tilt, with the exact quarter turns */
+  const double turn = -tilt;
+  double c, s;
+  if (turn == 0 || fabs(fabs(turn) - 2 * kPI) < 1e-12)
+    return;
+  if (fabs(fabs(turn) - kPI) < 1e-12) {
+    c = -1;
+    s = 0;
+  } else if (fabs(turn - kPI / 2) < 1e-12) {
+    c = 0;
+    s = 1;
+  } else if (fabs(turn + kPI / 2) < 1e-12) {
+    c = 0;
+    s = -1;
+  } else {
+    c = b2e_cos(turn);
+    s = b2e_sin(turn);
+  }
+  const double x = out[0], xp = out[1], y = out[2], yp = out[3];
+  out[0] = x * c + y * s;
+  out[2] = -x * s + y * c;
+  out[1] = xp * c + yp * s;
+  out[3] = -xp * s + yp * c;
+}
+
 static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2, double Po, DevElem &d,
                                   DevRad &r) {
   const double *p = el.p;
@@ -283,8 +337,6 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     return "CSBEND N_SLICES must be >= 1";
   if (p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0)
     return "CSBEND with K1/K2 field terms is not supported by this engine";
-  if ((edge1 || edge2) && p[B2E_BEND_EDGE_ORDER] > 1)
-    return "CSBEND EDGE_ORDER>1 is not supported by this engine";
   if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
     return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
   /* csbend.c:933-950: negative angle folded into a PI tilt */
@@ -305,8 +357,6 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
   }
   if (fabs(rho0) > 1e6)
     return "CSBEND with radius > 1e6 is not supported (use EDRIFT)";
-  if (etilt != 0)
-    return "CSBEND ETILT is not supported by this engine";
   fse = p[B2E_BEND_FSE] + 0.0;
   h = 1 / rho0;
   if (fabs(fse + 1) < 1e-12)
@@ -367,13 +417,26 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
   d.c[CB_DXF] = p[B2E_BEND_DX] * b2e_cos(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * b2e_sin(p[B2E_BEND_ANGLE]);
   d.c[CB_DZF] = p[B2E_BEND_DX] * b2e_sin(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * b2e_cos(p[B2E_BEND_ANGLE]);
   d.c[CB_DYF] = p[B2E_BEND_DY];
-  /* dcoord_etilt (computeEtiltCentroidOffset) is zero: ETILT is rejected above */
+  etilt_exit_offsets(d.c + CB_ETILT0, rho0, angle, etilt, tilt);
   d.c[CB_INV_RHO0] = 1 / rho0;
   d.c[CB_INV_RHO_ACTUAL] = 1 / rho_actual;
   if (edge1)
     d.flags |= EF_EDGE1;
   if (edge2)
     d.flags |= EF_EDGE2;
+  if ((edge1 || edge2) && p[B2E_BEND_EDGE_ORDER] >= 2) {
+    /* second-order edges (apply_edge_effects, csbend.c:4266-4307): the
+     * per-element parts; b1 = K1*rho0 (csbend.c:825), sign-flipped with a
+     * negative angle (:879-882), gives n = -b1/h (:929) */
+    double b1 = p[B2E_BEND_K1] * (length / p[B2E_BEND_ANGLE]);
+    if (p[B2E_BEND_ANGLE] < 0)
+      b1 *= -1;
+    const double sec1 = 1. / b2e_cos(e1), sec2 = 1. / b2e_cos(e2);
+    d.flags |= EF_EDGE_ORDER2;
+    d.c[CB_SEC2_E1] = sec1 * sec1;
+    d.c[CB_SEC2_E2] = sec2 * sec2;
+    d.c[CB_EDGE_N] = -b1 / h;
+  }
   if (-tilt != 0) {
     d.flags |= EF_REVERSE_TILT;
     d.rev_cos = b2e_cos(-tilt);

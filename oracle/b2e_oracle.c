@@ -666,12 +666,94 @@ static int same_bend(const b2e_element *a, const b2e_element *b) {
   return a->type == b->type && strncmp(a->name, b->name, sizeof(a->name)) == 0;
 }
 
+/* apply_edge_effects (csbend.c:4266-4307): K. L. Brown's second-order edge,
+ * used for EDGE_ORDER >= 2; he (H1/H2) is zero here. */
+static void edge_order2(double *x, double *xp, double *y, double *yp, double rho, double n, double beta,
+                        double psi, long which_edge) {
+  double h, tan_beta, tan2_beta, sec_beta, sec2_beta, h2, R21, R43;
+  double T111, T133, T211, T441, T331, T221, T233, T243, T431, T432, x0, xp0, y0, yp0;
+  h = 1 / rho;
+  R21 = h * (tan_beta = M_TAN(beta));
+  R43 = -h * M_TAN(beta - psi);
+  h2 = SQR(h);
+  T111 = which_edge * h / 2 * (tan2_beta = SQR(tan_beta));
+  sec_beta = 1. / M_COS(beta);
+  sec2_beta = SQR(sec_beta);
+  T133 = -which_edge * h / 2 * sec2_beta;
+  T211 = which_edge == -1 ? -n * h2 * tan_beta : -h2 * (n + tan2_beta / 2) * tan_beta;
+  T441 = -(T331 = T221 = -which_edge * h * tan2_beta);
+  T233 = which_edge == -1 ? h2 * (n + .5 + tan2_beta) * tan_beta : h2 * (n - tan2_beta / 2) * tan_beta;
+  T243 = which_edge * h * tan2_beta;
+  T431 = h2 * (2 * n + (which_edge == 1 ? sec2_beta : 0)) * tan_beta;
+  T432 = which_edge * h * sec2_beta;
+  x0 = *x;
+  xp0 = *xp;
+  y0 = *y;
+  yp0 = *yp;
+  *x = x0 + T111 * SQR(x0) + T133 * SQR(y0);
+  *xp = xp0 + R21 * x0 + T211 * SQR(x0) + T221 * x0 * xp0 + T233 * SQR(y0) + T243 * y0 * yp0;
+  *y = y0 + T331 * x0 * y0;
+  *yp = yp0 + R43 * y0 + T441 * yp0 * x0 + T431 * x0 * y0 + T432 * xp0 * y0;
+}
+
+/* computeEtiltCentroidOffset (csbend.c:4723-4769) with the closing
+ * rotateCoordinatesForMisalignment(-tilt) (tilt_matrices.c:123-150):
+ * exit-face offsets of a bend rolled by ETILT. */
+static void etilt_offsets(double *d, double rho0, double angle, double etilt, double tilt) {
+  double q1a, q3a, qp1, qp2, qp3, k, tan_alpha, q1b, q2b, dz, x, xp, y, yp, ca, sa, rot;
+  int i;
+  for (i = 0; i < 6; i++)
+    d[i] = 0;
+  if (!etilt)
+    return;
+  etilt *= -1;
+  q1a = (1 - M_COS(angle)) * rho0 * (M_COS(etilt) - 1);
+  q3a = (1 - M_COS(angle)) * rho0 * M_SIN(etilt);
+  qp1 = M_SIN(angle) * M_COS(etilt);
+  qp2 = M_COS(angle);
+  k = sqrt(SQR(qp1) + SQR(qp2));
+  qp3 = M_SIN(angle) * M_SIN(etilt) / k;
+  tan_alpha = 1. / M_TAN(angle) / M_COS(etilt);
+  q1b = q1a * tan_alpha / (M_TAN(angle) + tan_alpha);
+  q2b = -q1b * M_TAN(angle);
+  dz = sqrt(SQR(q1b - q1a) + SQR(q2b - 0));
+  d[0] = sqrt(SQR(q1b) + SQR(q2b));
+  d[1] = M_TAN(atan(tan_alpha) - (PI_ / 2 - angle));
+  d[2] = q3a + qp3 * dz;
+  d[3] = qp3;
+  d[4] = dz * sqrt(1 + SQR(qp3));
+  rot = -tilt;
+  if (!rot || fabs(fabs(rot) - 2 * PI_) < 1e-12)
+    return;
+  if (fabs(fabs(rot) - PI_) < 1e-12) {
+    ca = -1;
+    sa = 0;
+  } else if (fabs(rot - PI_ / 2) < 1e-12) {
+    ca = 0;
+    sa = 1;
+  } else if (fabs(rot + PI_ / 2) < 1e-12) {
+    ca = 0;
+    sa = -1;
+  } else {
+    ca = M_COS(rot);
+    sa = M_SIN(rot);
+  }
+  x = d[0];
+  xp = d[1];
+  y = d[2];
+  yp = d[3];
+  d[0] = x * ca + y * sa;
+  d[2] = -x * sa + y * ca;
+  d[1] = xp * ca + yp * sa;
+  d[3] = -xp * sa + yp * ca;
+}
+
 static long csbend_track(double **c, long np, const b2e_element *el, int idx, const b2e_element *all, int n_all,
                          double Po, double z_start, const MaxAmp *ma, int pass) {
   const double *p = el->p;
   double angle, e1, e2, tilt, rho0, rho_actual, fse, h, psi1, psi2, Kg1, Kg2, ttilt, ct, st;
   BendRad br;
-  double dxi, dyi, dzi, dxf, dyf, dzf, length = p[B2E_BEND_L];
+  double dxi, dyi, dzi, dxf, dyf, dzf, det[6], n_index, length = p[B2E_BEND_L];
   int edge1 = 0, edge2 = 0, j, integ = (int)p[B2E_BEND_INTEGRATION_ORDER];
   long nSlices = (long)p[B2E_BEND_N_SLICES], ip, itop;
   MultAp ap;
@@ -718,6 +800,11 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   setup_mult_ap(&ap, -tilt, ma);
   fse = p[B2E_BEND_FSE] + 0.0;
   h = 1 / rho0;
+  /* n = -b[1]/h with b[1] = K1*rho0, sign-flipped for a negative angle (csbend.c:825, :879-882, :929) */
+  n_index = p[B2E_BEND_K1] * (length / p[B2E_BEND_ANGLE]);
+  if (p[B2E_BEND_ANGLE] < 0)
+    n_index *= -1;
+  n_index = -n_index / h;
   if (fabs(fse + 1) < 1e-12)
     fse = -1 + 1e-12;
   rho_actual = 1 / ((1 + fse) * h);
@@ -751,6 +838,7 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   dxf = p[B2E_BEND_DX] * M_COS(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * M_SIN(p[B2E_BEND_ANGLE]);
   dzf = p[B2E_BEND_DX] * M_SIN(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * M_COS(p[B2E_BEND_ANGLE]);
   dyf = p[B2E_BEND_DY];
+  etilt_offsets(det, rho0, angle, p[B2E_BEND_ETILT], tilt);
   /* csbend.c:964-977 */
   br.rad_coef = 0;
   if (p[B2E_BEND_SYNCH_RAD])
@@ -776,8 +864,12 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     dp = dp0 = coord[5];
     if (edge1) {
       rho = (1 + dp) * rho_actual;
-      xp += M_TAN(e1) / rho * x;
-      yp -= M_TAN(e1 - psi1 / (1 + dp)) / rho * y;
+      if (p[B2E_BEND_EDGE_ORDER] >= 2)
+        edge_order2(&x, &xp, &y, &yp, rho, n_index, e1, psi1 * (1 + dp), -1);
+      else {
+        xp += M_TAN(e1) / rho * x;
+        yp -= M_TAN(e1 - psi1 / (1 + dp)) / rho * y;
+      }
     }
     Qi[0] = x;
     Qi[1] = xp;
@@ -828,14 +920,18 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     dp = Qf[5];
     if (edge2) {
       rho = (1 + dp) * rho_actual;
-      xp += M_TAN(e2) / rho * x;
-      yp -= M_TAN(e2 - psi2 / (1 + dp)) / rho * y;
+      if (p[B2E_BEND_EDGE_ORDER] >= 2)
+        edge_order2(&x, &xp, &y, &yp, rho, n_index, e2, psi2 * (1 + dp), 1);
+      else {
+        xp += M_TAN(e2) / rho * x;
+        yp -= M_TAN(e2 - psi2 / (1 + dp)) / rho * y;
+      }
     }
-    coord[0] = x * ct - y * st + 0.0;
-    coord[2] = x * st + y * ct + 0.0;
-    coord[1] = xp * ct - yp * st + 0.0;
-    coord[3] = xp * st + yp * ct + 0.0;
-    coord[4] = s + 0.0;
+    coord[0] = x * ct - y * st + det[0];
+    coord[2] = x * st + y * ct + det[2];
+    coord[1] = xp * ct - yp * st + det[1];
+    coord[3] = xp * st + yp * ct + det[3];
+    coord[4] = s + det[4];
     coord[5] = dp;
     coord[0] += dxf + dzf * coord[1];
     coord[2] += dyf + dzf * coord[3];
@@ -1137,7 +1233,7 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   long sgHalf = (long)p[B2E_BEND_SG_HALFWIDTH], sgOrder = (long)p[B2E_BEND_SG_ORDER];
   long sgdHalf = (long)p[B2E_BEND_SGDERIV_HALFWIDTH], sgdOrder = (long)p[B2E_BEND_SGDERIV_ORDER];
   double angle, e1, e2, tilt, rho0, rho_actual, fse, h, psi1, psi2, Kg, ttilt, ct, st;
-  double dxi, dyi, dzi, dxf, dyf, dzf, CSRConstant, phiBend, ctLower = 0, ctUpper = 0, dct = 0;
+  double dxi, dyi, dzi, dxf, dyf, dzf, det[6], n_index, CSRConstant, phiBend, ctLower = 0, ctUpper = 0, dct = 0;
   double brf = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
   double *beta0, *ctHist, *ctHistDeriv, *denom, *T1, *T2;
   int more_than_one = np > 1, same_pre = 0;
@@ -1198,6 +1294,11 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   }
   setup_mult_ap(&ap, -tilt, ma);
   h = 1 / rho0;
+  /* n = -b[1]/h with b[1] = K1*rho0, sign-flipped for a negative angle (csbend.c:825, :879-882, :929) */
+  n_index = p[B2E_BEND_K1] * (length / p[B2E_BEND_ANGLE]);
+  if (p[B2E_BEND_ANGLE] < 0)
+    n_index *= -1;
+  n_index = -n_index / h;
   fse = p[B2E_BEND_FSE];
   rho_actual = fse > -1 ? 1 / ((1 + fse) * h) : 1e16 / h;
   Kg = 2 * p[B2E_BEND_HGAP] * p[B2E_BEND_FINT];
@@ -1230,6 +1331,7 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
   dxf = p[B2E_BEND_DX] * M_COS(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * M_SIN(p[B2E_BEND_ANGLE]);
   dzf = p[B2E_BEND_DX] * M_SIN(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * M_COS(p[B2E_BEND_ANGLE]);
   dyf = p[B2E_BEND_DY];
+  etilt_offsets(det, rho0, angle, p[B2E_BEND_ETILT], tilt);
   beta0 = malloc(sizeof(double) * (np ? np : 1));
   ctHist = calloc(nBins, sizeof(double));
   ctHistDeriv = calloc(nBins, sizeof(double));
@@ -1265,8 +1367,12 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
     x[4] /= beta0[ip];
     if (edge1) {
       rho = (1 + x[5]) * rho_actual;
-      x[1] += M_TAN(e1) / rho * x[0];
-      x[3] -= M_TAN(e1 - psi1 / (1 + x[5])) / rho * x[2];
+      if (p[B2E_BEND_EDGE_ORDER] >= 2)
+        edge_order2(&x[0], &x[1], &x[2], &x[3], rho, n_index, e1, psi1 * (1 + x[5]), -1);
+      else {
+        x[1] += M_TAN(e1) / rho * x[0];
+        x[3] -= M_TAN(e1 - psi1 / (1 + x[5])) / rho * x[2];
+      }
     }
   }
   CSRConstant = 0;
@@ -1464,20 +1570,24 @@ static long csrcsbend_track(double **c, long np, const b2e_element *el, int idx,
     }
     if (edge2) {
       rho = (1 + x[5]) * rho_actual;
-      x[1] += M_TAN(e2) / rho * x[0];
-      x[3] -= M_TAN(e2 - psi2 / (1 + x[5])) / rho * x[2];
+      if (p[B2E_BEND_EDGE_ORDER] >= 2)
+        edge_order2(&x[0], &x[1], &x[2], &x[3], rho, n_index, e2, psi2 * (1 + x[5]), 1);
+      else {
+        x[1] += M_TAN(e2) / rho * x[0];
+        x[3] -= M_TAN(e2 - psi2 / (1 + x[5])) / rho * x[2];
+      }
     }
-    X = x[0] * ct - x[2] * st + 0.0;
-    Y = x[0] * st + x[2] * ct + 0.0;
-    XP = x[1] * ct - x[3] * st + 0.0;
-    YP = x[1] * st + x[3] * ct + 0.0;
+    X = x[0] * ct - x[2] * st + det[0];
+    Y = x[0] * st + x[2] * ct + det[2];
+    XP = x[1] * ct - x[3] * st + det[1];
+    YP = x[1] * st + x[3] * ct + det[3];
     x[0] = X;
     x[2] = Y;
     x[1] = XP;
     x[3] = YP;
     x[0] += dxf + dzf * x[1];
     x[2] += dyf + dzf * x[3];
-    x[4] += dzf * sqrt(1 + SQR(x[1]) + SQR(x[3])) + 0.0;
+    x[4] += dzf * sqrt(1 + SQR(x[1]) + SQR(x[3])) + det[4];
   }
   if (more_than_one) {
     cw->valid = 1;

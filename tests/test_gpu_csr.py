@@ -84,6 +84,26 @@ def test_chicane_with_exact_drifts(ref_b2e):
     check(*run_both(ref_b2e, Lattice(els), beam))
 
 
+def test_chicane_with_rolled_dipoles(ref_b2e):
+    """ETILT on every CSRCSBEND (two with a TILT as well): the exit-face
+    offsets (csbend.c:2942-2952), wakes and coordinates bit-identical."""
+    lat = w.chicane(bins=150, n_kicks=5)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, ETILT=1e-3 * (1 + i % 3), TILT=0.02 * (i % 2)))
+                   if e.type == "CSRCSBEND" else e for i, e in enumerate(lat.elements)])
+    beam = w.chicane_beam(15000, seed=29)
+    check(*run_both(ref_b2e, lat, beam))
+
+
+def test_chicane_with_second_order_edges(ref_b2e):
+    """EDGE_ORDER=2 (apply_edge_effects, csbend.c:4266-4307) at the CSR
+    dipoles' entrance and exit, with edge angles and a fringe integral."""
+    lat = w.chicane(bins=150, n_kicks=5)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, EDGE_ORDER=2, E1=0.02, E2=0.03, HGAP=0.01, FINT=0.4))
+                   if e.type == "CSRCSBEND" else e for e in lat.elements])
+    beam = w.chicane_beam(15000, seed=43)
+    check(*run_both(ref_b2e, lat, beam))
+
+
 def test_chicane_without_charge_is_plain_tracking(ref_b2e):
     lat = w.chicane(bins=100, n_kicks=3, charge=0.0)
     beam = w.chicane_beam(5000, seed=2)

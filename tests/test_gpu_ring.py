@@ -378,3 +378,45 @@ def test_ring_rf_cavity_with_length(ref_b2e, rf):
     assert 150 <= nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+def test_ring_with_rolled_dipoles(ref_b2e):
+    """CSBEND ETILT (exit-face offsets, csbend.c:4723-4769 and :1359-1364)
+    alone, with TILT and a misalignment, with edge angles, with DZ; 60 turns
+    with losses, bit-identical to the reference."""
+    errs = [{"ETILT": 2e-3}, {"ETILT": -1.5e-3, "TILT": 0.05, "DX": 1e-4},
+            {"ETILT": 1e-3, "E1": 0.1, "E2": 0.08}, {"ETILT": 5e-4, "DZ": 2e-4}]
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            e = Element(e.name + str(k), e.type, dict(e.params, **errs[k % len(errs)]))
+            k += 1
+        els.append(e)
+    lat = Lattice(els)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=33).coords, _lossy_beam(150, seed=34).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 100 <= nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff
+
+
+def test_ring_with_second_order_edges(ref_b2e):
+    """EDGE_ORDER=2 on every dipole, with edge angles and a fringe integral:
+    60 turns with losses, bit-identical to the reference."""
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            e = Element(e.name + str(k), e.type, dict(e.params, EDGE_ORDER=2, E1=0.12 - 0.05 * (k % 3),
+                                                      E2=0.09 * (k % 2), HGAP=0.02, FINT=0.5))
+            k += 1
+        els.append(e)
+    lat = Lattice(els)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=35).coords, _lossy_beam(150, seed=36).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 100 <= nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

@@ -305,3 +305,82 @@ def test_port_reproduces_reference_rf_cavity_with_length(math, rf):
     assert n1 == n2 and e1 == e2 and n1 < beam.n
     assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+
+
+def _ring_with_bend_errors():
+    """The ring with its dipoles rolled by ETILT: one alone, one with a TILT
+    as well, one folded into a negative angle (tilt + PI), one with a quarter
+    turn of TILT (the exact-rotation branch)."""
+    from elegant_b200 import Element, Lattice
+    errs = [{"ETILT": 2e-3}, {"ETILT": -1.5e-3, "TILT": 0.05, "DX": 1e-4},
+            {"ETILT": 1e-3, "E1": 0.1, "E2": 0.08}, {"ETILT": 5e-4, "DZ": 2e-4}]
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            e = Element(e.name + str(k), e.type, dict(e.params, **errs[k % len(errs)]))
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_rolled_bends(math):
+    """CSBEND ETILT: the exit-face offsets of computeEtiltCentroidOffset
+    (csbend.c:4723-4769) added after the exit rotation (:1359-1364), with
+    losses."""
+    lat = _ring_with_bend_errors()
+    beam = lossy_beam(150, seed=19)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    # the roll moves the orbit: the same beam ends elsewhere without it
+    r0, n0, _, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_csr_rolled_bends(math):
+    """CSRCSBEND ETILT: the offsets at the CSR exit (csbend.c:2942-2952),
+    negative-angle dipoles included."""
+    from elegant_b200 import Element, Lattice
+    lat = w.chicane(bins=120, n_kicks=4, sg_halfwidth=2)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, ETILT=1e-3 * (1 + i % 3), TILT=0.02 * (i % 2)))
+                   if e.type == "CSRCSBEND" else e for i, e in enumerate(lat.elements)])
+    beam = w.chicane_beam(5000, seed=23)
+    p0 = 1000 / 0.51099895
+    r1, n1, e1, w1 = RefOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    r2, n2, e2, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    assert n1 == n2 and w1.size == w2.size > 0
+    assert np.array_equal(w1, w2)
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_second_order_edges(math):
+    """EDGE_ORDER=2 (apply_edge_effects, csbend.c:4266-4307) on ring dipoles
+    with edge angles and a fringe integral, with losses; and on CSRCSBENDs."""
+    from elegant_b200 import Element, Lattice
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            e = Element(e.name + str(k), e.type, dict(e.params, EDGE_ORDER=2, E1=0.12 - 0.05 * (k % 3),
+                                                      E2=0.09 * (k % 2), HGAP=0.02, FINT=0.5))
+            k += 1
+        els.append(e)
+    beam = lossy_beam(150, seed=37)
+    r1, n1, e1, _ = RefOracle(math).track(Lattice(els), beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(Lattice(els), beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    lat = w.chicane(bins=120, n_kicks=4, sg_halfwidth=2)
+    lat = Lattice([Element(e.name, e.type, dict(e.params, EDGE_ORDER=2, E1=0.02, E2=0.03, HGAP=0.01, FINT=0.4))
+                   if e.type == "CSRCSBEND" else e for e in lat.elements])
+    beam = w.chicane_beam(5000, seed=41)
+    p0 = 1000 / 0.51099895
+    r1, n1, _, w1 = RefOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    r2, n2, _, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
+    assert n1 == n2 and np.array_equal(w1, w2)
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
