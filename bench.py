@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-turns/s (FP64)"
 # dram__bytes_read.sum + dram__bytes_write.sum of one ring_kernel launch on the
 # 512-instance ensemble (71.45 MB + 20.33 MB; the latest capture in profiles/)
-RING_TRAFFIC_BYTES = 91_783_168
+RING_TRAFFIC_BYTES = 91_491_328
 UNIT = "particle-turns/s"
 
 
