@@ -87,7 +87,7 @@ struct b2e_ctx {
   /* external (device) particle pointers for b2e_track_device */
   DevParticles ext{};
   bool use_ext = false;
-  bool radiates = false; /* some element of some instance has SYNCH_RAD or ISR */
+  bool radiates = false; /* some element of some instance reads the DevRad table (any_radiation) */
   CsrState csr;
   int pass_counter = 0; /* next pass to track in the current run */
   int64_t launches = 0; /* kernels launched by this context */
@@ -258,9 +258,12 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
   return B2E_OK;
 }
 
+/* the lattice needs the ring kernel's RAD instantiation: some element
+ * radiates, or is a bend with K1/K2 field terms, ETILT or second-order edges
+ * (all read the DevRad table) */
 static bool any_radiation(const std::vector<DevElem> &elems) {
   for (const DevElem &d : elems)
-    if (d.flags & (EF_SR | EF_ISR))
+    if (d.flags & (EF_SR | EF_ISR | EF_FIELD | EF_ETILT | EF_EDGE_ORDER2))
       return true;
   return false;
 }

@@ -133,7 +133,8 @@ __device__ __forceinline__ void chain_enter() {
 }
 
 /* entrance: offsets, tilt, c*t = s/beta, entrance edge (csbend.c:2286-2377) */
-__global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const DevElem *ep, double Po) {
+__global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const DevElem *ep, BendExtra bx,
+                                 double Po) {
   chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n || P.lost_pass[i] >= 0)
@@ -156,8 +157,8 @@ __global__ void csr_entry_kernel(DevParticles P, int64_t n, double *beta0, const
   if (e.flags & EF_EDGE1) {
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
     if (e.flags & EF_EDGE_ORDER2) {
-      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], c[CB_SEC2_E1],
-                       c[CB_EDGE_N], -1);
+      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], bx.c[BX_SEC2_E1],
+                       bx.c[BX_EDGE_N], -1);
     } else {
       XP = XP + (c[CB_TAN_E1] / rho) * X;
       YP = YP - (b2e_tan(c[CB_E1] - c[CB_PSI1] / (1 + dp)) / rho) * Y;
@@ -961,7 +962,8 @@ __global__ void csr_last_kick_kernel(DevParticles P, int64_t n, CsrBunches B, in
 
 /* exit: c*t -> s at the final velocity, exit edge, back to the lab frame
  * (csbend.c:2810-2955); csrWake.s0 from the exit binning's lower edge. */
-__global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, CsrBunches B, double factor, double Po,
+__global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, BendExtra bx, CsrBunches B, double factor,
+                                double Po,
                                 int pass, int elem_index) {
   chain_enter();
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -994,20 +996,21 @@ __global__ void csr_exit_kernel(DevParticles P, int64_t n, const DevElem *ep, Cs
   if (e.flags & EF_EDGE2) {
     rho = (1 + DP) * c[CB_RHO_ACTUAL];
     if (e.flags & EF_EDGE_ORDER2) {
-      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI2] * (1 + DP), c[CB_TAN_E2], c[CB_E2], c[CB_SEC2_E2],
-                       c[CB_EDGE_N], 1);
+      bend_edge_order2(X, XP, Y, YP, rho, c[CB_PSI2] * (1 + DP), c[CB_TAN_E2], c[CB_E2], bx.c[BX_SEC2_E2],
+                       bx.c[BX_EDGE_N], 1);
     } else {
       XP = XP + (c[CB_TAN_E2] / rho) * X;
       YP = YP - (b2e_tan(c[CB_E2] - c[CB_PSI2] / (1 + DP)) / rho) * Y;
     }
   }
-  x = (X * ct - Y * sn) + c[CB_ETILT0];
-  y = (X * sn + Y * ct) + c[CB_ETILT0 + 2];
-  xp = (XP * ct - YP * sn) + c[CB_ETILT0 + 1];
-  yp = (XP * sn + YP * ct) + c[CB_ETILT0 + 3];
+  /* the ETILT offsets are zero without ETILT */
+  x = (X * ct - Y * sn) + bx.c[BX_ETILT0];
+  y = (X * sn + Y * ct) + bx.c[BX_ETILT0 + 2];
+  xp = (XP * ct - YP * sn) + bx.c[BX_ETILT0 + 1];
+  yp = (XP * sn + YP * ct) + bx.c[BX_ETILT0 + 3];
   x = x + (c[CB_DXF] + c[CB_DZF] * xp);
   y = y + (c[CB_DYF] + c[CB_DZF] * yp);
-  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + c[CB_ETILT0 + 4]);
+  s = s + (c[CB_DZF] * sqrt((1 + xp * xp) + yp * yp) + bx.c[BX_ETILT0 + 4]);
   P.x[i] = x;
   P.xp[i] = xp;
   P.y[i] = y;
@@ -1358,6 +1361,7 @@ int csr_configure(CsrState &st, const b2e_element *el, int n, const CompiledLatt
       ce.rho0 = d.c[CB_RHO0];
       ce.binRangeFactor = p[B2E_BEND_BIN_RANGE_FACTOR] < 1.1 ? 1.1 : p[B2E_BEND_BIN_RANGE_FACTOR];
       ce.dzf = d.c[CB_DZF];
+      memcpy(ce.bx.c, lat.rads[idx].c + RB_EXTRA0, sizeof(ce.bx.c));
       ce.z_end = d.z_end;
       /* SAME_BEND_PRECEDES of determine_bend_flags (bend_matrix.c:1342-1363):
        * MARKs in between are transparent */
@@ -1927,7 +1931,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
                                   (int)sur_smem));
   }
 
-  CSR_CUDA(launch_chained(csr_entry_kernel, dim3(g), dim3(256), 0, stream, P, n, st.d_beta0, d_e, Po));
+  CSR_CUDA(launch_chained(csr_entry_kernel, dim3(g), dim3(256), 0, stream, P, n, st.d_beta0, d_e, ce.bx, Po));
   (*launches)++;
   CSR_CUDA(cudaGetLastError());
   double phiBend = st.accumulated_angle;
@@ -2057,7 +2061,7 @@ int csr_track_element(CsrState &st, const DevElem *d_elems, const DevElem &h_ele
     if (rrc)
       return rrc;
   }
-  CSR_CUDA(launch_chained(csr_exit_kernel, dim3(g), dim3(256), 0, stream, P, n, d_e, B, ce.binRangeFactor, Po, pass,
+  CSR_CUDA(launch_chained(csr_exit_kernel, dim3(g), dim3(256), 0, stream, P, n, d_e, ce.bx, B, ce.binRangeFactor, Po, pass,
                           elem));
   (*launches) += 2;
   CSR_CUDA(cudaGetLastError());
@@ -2328,7 +2332,8 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
     return B2E_ERR_ARG;
   }
   DevElem d;
-  const char *msg = compile_single_csr_bend(*bend, d);
+  BendExtra bx;
+  const char *msg = compile_single_csr_bend(*bend, d, bx);
   if (msg) {
     snprintf(err, errlen, "b2e_csr_bend_static: %s", msg);
     return B2E_ERR_LATTICE;
@@ -2409,7 +2414,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
    * context path also changes: set it for this call's bin count */
   const size_t wake_smem = sizeof(double) * (4 * bins + 8);
   STATIC_TRY(cudaFuncSetAttribute(csr_wake_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wake_smem));
-  csr_entry_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, Po);
+  csr_entry_kernel<<<g, 256, 0, s>>>(P, n, S->beta0, &S->elem, bx, Po);
   STATIC_TRY(cudaGetLastError());
   double phiBend = 0;
   for (int kick = 0; kick < nSlices; kick++) {
@@ -2457,7 +2462,7 @@ extern "C" int b2e_csr_bend_static(double *const dev_columns[6], int32_t *dev_lo
   }
   csr_reset_keys_kernel<<<1, 32, 0, s>>>(B);
   csr_last_kick_kernel<<<g, 256, 0, s>>>(P, n, B, bins, Po, rho0);
-  csr_exit_kernel<<<g, 256, 0, s>>>(P, n, &S->elem, B, brf, Po, 0, 0);
+  csr_exit_kernel<<<g, 256, 0, s>>>(P, n, &S->elem, bx, B, brf, Po, 0, 0);
   STATIC_TRY(cudaGetLastError());
   STATIC_TRY(launch_post_element_sweep(P, n, nullptr, 0, 0, s));
   return B2E_OK;

@@ -32,6 +32,7 @@ struct CsrElem {
   int bins = 0, nSlices = 0, nSub = 0, sgHalf = 0, sgOrder = 1, sgdHalf = 1, sgdOrder = 1;
   int trapz = 1, steady = 0, csr = 1, same_bend_precedes = 0, bin_once = 0, igf = 0;
   double angle = 0, length = 0, rho0 = 0, binRangeFactor = 1.2, dzf = 0, z_end = 0;
+  BendExtra bx = {};  /* ETILT offsets and second-order edge constants */
   /* histogram filters (applyLHPassFilters), csbend.c:2557-2562 */
   int lh = 0, clip = 1;
   double lowCut0 = -1, lowCut1 = -1, highCut0 = -1, highCut1 = -1;

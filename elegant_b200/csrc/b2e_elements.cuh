@@ -386,16 +386,50 @@ __device__ __forceinline__ int bend_drift(double &X, double &QX, double &Y, doub
   return LOSS_NONE;
 }
 
+/* Scaled fields of a bend with K1/K2 (computeCSBENDFields, the TURBO_MODE
+ * form of csbend.c:101-150, normal terms, expansion order 4): the sums over
+ * x^i y^j in the reference's order, i outer, each term (F*x^i)*y^j with the
+ * powers as repeated products.  F: the 15 coefficients of bend_field_terms. */
+__device__ __forceinline__ void bend_fields(double x, double y, const double *F, double &Fx, double &Fy) {
+  const double y2 = y * y, y3 = y2 * y, y4 = y3 * y;
+  const double x2 = x * x, x3 = x2 * x, x4 = x3 * x;
+  double sx = 0, sy = 0;
+  sx = sx + F[0] * y;
+  sx = sx + F[1] * y3;
+  sy = sy + F[6];
+  sy = sy + F[7] * y2;
+  sy = sy + F[8] * y4;
+  sx = sx + (F[2] * x) * y;
+  sx = sx + (F[3] * x) * y3;
+  sy = sy + F[9] * x;
+  sy = sy + (F[10] * x) * y2;
+  sx = sx + (F[4] * x2) * y;
+  sy = sy + F[11] * x2;
+  sy = sy + (F[12] * x2) * y2;
+  sx = sx + (F[5] * x3) * y;
+  sy = sy + F[13] * x3;
+  sy = sy + F[14] * x4;
+  Fx = sx;
+  Fy = sy;
+}
+
 /* kick j of a slice (csbend.c:1591-1638) */
 template <bool RAD>
-__device__ __forceinline__ void bend_kick(double X, double &QX, double &QY, double &DPoP, const double *c, int i, int j,
-                                          int nSub, bool isr_block, const DevElem &e, const RadSite &rs) {
+__device__ __forceinline__ void bend_kick(double X, double Y, double &QX, double &QY, double &DPoP, const double *c,
+                                          int i, int j, int nSub, bool isr_block, const DevElem &e,
+                                          const RadSite &rs) {
   const double rho_actual = c[CB_RHO_ACTUAL];
   const double ds = c[CB_DS0 + j];
-  /* QX += -ds*(1+X/rho0)*Fy/rho_actual with Fy = 1; QY += ... * Fx with Fx = 0 */
   const double x_rho0 = div_rn_recip(X, c[CB_RHO0], c[CB_INV_RHO0]);
-  QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * 1.0), rho_actual, c[CB_INV_RHO_ACTUAL]);
-  {
+  double Fx = 0, Fy = 1;
+  if (RAD && (e.flags & EF_FIELD)) {
+    /* QX += -ds*(1+X/rho0)*Fy/rho_actual; QY += ds*(1+X/rho0)*Fx/rho_actual */
+    bend_fields(X, Y, rs.rc + RB_FIELD0, Fx, Fy);
+    QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * Fy), rho_actual, c[CB_INV_RHO_ACTUAL]);
+    QY = QY + div_rn_recip(((ds * (1 + x_rho0)) * Fx), rho_actual, c[CB_INV_RHO_ACTUAL]);
+  } else {
+    /* Fy = 1, Fx = 0 */
+    QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * 1.0), rho_actual, c[CB_INV_RHO_ACTUAL]);
     /* (t * Fx) / rho_actual with Fx = 0 is a signed zero (NaN for a
      * non-finite t): the sign of t * 0.0 flipped by rho_actual's, which
      * is finite and nonzero in a bend -- the same value without the
@@ -404,12 +438,12 @@ __device__ __forceinline__ void bend_kick(double X, double &QX, double &QY, doub
     QY = QY + (rho_actual < 0 ? -z : z);
   }
   if (RAD && (e.flags & (EF_SR | EF_ISR))) {
-    /* radiation after the kick (csbend.c:1603-1622), Fx = 0, Fy = 1 */
+    /* radiation after the kick (csbend.c:1603-1622) */
     const double a = 1 + X * rs.rc[RB_INV_RHO0];
     const double f = a / sqrt(((1 + DPoP) * (1 + DPoP) - QX * QX) - QY * QY);
     const double xp = QX * f, yp = QY * f;
     const double dsFactor = sqrt((a * a + xp * xp) + yp * yp);
-    const double F2 = 0.0 * 0.0 + 1.0 * 1.0;
+    const double F2 = Fx * Fx + Fy * Fy;
     const double deltaFactor = (1 + DPoP) * (1 + DPoP);
     const double dsISR = rs.rc[RB_SLICE] / (nSub - 1);
     QX = QX / (1 + DPoP);
@@ -451,7 +485,7 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
         if ((lost = bend_drift(X, QX, Y, QY, dist, DPoP, rho0, c[CB_DSH0 + j])))
           return lost;
         if (j < NSUB - 1) /* kickFrac[last] == 0 ends the slice */
-          bend_kick<RAD>(X, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
+          bend_kick<RAD>(X, Y, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
       }
     } else {
 #pragma unroll 1
@@ -460,7 +494,7 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
           return lost;
         if (j == nSub - 1) /* kickFrac[last] == 0 ends the slice */
           break;
-        bend_kick<RAD>(X, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
+        bend_kick<RAD>(X, Y, QX, QY, DPoP, c, i, j, nSub, isr_block, e, rs);
       }
     }
   }
@@ -472,11 +506,15 @@ __device__ __forceinline__ int csbend_integrate(double &X, double &QX, double &Y
 /* ---- CSBEND: track_through_csbend (csbend.c:665-1409), malignMethod 0,
  * edge method 1 at edge order 1, no synchrotron radiation. */
 /* dp_prime * x * tan(e) of the radiation edge corrections (csbend.c:1211-1216,
- * :1265-1276), Fx = 0, Fy = 1 */
-__device__ __forceinline__ double bend_edge_radiation(double x, double xp, double yp, double dp, double tan_e,
-                                                      const double *c, const double *rc) {
+ * :1265-1276), with the fields at (x, y) */
+__device__ __forceinline__ double bend_edge_radiation(double x, double y, double xp, double yp, double dp,
+                                                      double tan_e, const double *c, const double *rc,
+                                                      unsigned flags) {
+  double Fx = 0, Fy = 1;
+  if (flags & EF_FIELD)
+    bend_fields(x, y, rc + RB_FIELD0, Fx, Fy);
   const double a = 1 + x / c[CB_RHO0];
-  const double dp_prime = ((-rc[RB_RAD]) * (0.0 * 0.0 + 1.0 * 1.0)) * ((1 + dp) * (1 + dp)) *
+  const double dp_prime = ((-rc[RB_RAD]) * (Fx * Fx + Fy * Fy)) * ((1 + dp) * (1 + dp)) *
                           sqrt((a * a + xp * xp) + yp * yp);
   return (dp_prime * x) * tan_e;
 }
@@ -528,9 +566,12 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE1) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    if (e.flags & EF_EDGE_ORDER2) {
-      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], c[CB_SEC2_E1],
-                       c[CB_EDGE_N], -1);
+    /* EF_EDGE_ORDER2 and EF_ETILT lattices run the RAD instantiation, which
+     * has the DevRad table with the BendExtra constants */
+    if (RAD && (e.flags & EF_EDGE_ORDER2)) {
+      const double *bx = rs.rc + RB_EXTRA0;
+      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], bx[BX_SEC2_E1],
+                       bx[BX_EDGE_N], -1);
     } else {
       delta_xp = (c[CB_TAN_E1] / rho) * x;
       xp = xp + delta_xp;
@@ -540,7 +581,7 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
 
   /* anticipate the radiation error of integrating the sector (csbend.c:1211-1216) */
   if (RAD && (e.flags & EF_EDGE1) && (e.flags & EF_SR) && c[CB_E1] != 0)
-    dp = dp - bend_edge_radiation(x, xp, yp, dp, c[CB_TAN_E1], c, rs.rc);
+    dp = dp - bend_edge_radiation(x, y, xp, yp, dp, c[CB_TAN_E1], c, rs.rc, e.flags);
 
   /* convertToDipoleCanonicalCoordinates (csbend.c:1411-1419) */
   f = (1 + dp) / sqrt((1 + xp * xp) + yp * yp);
@@ -568,7 +609,7 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   }
   /* correct the radiation error of the sector at the exit (csbend.c:1265-1276) */
   if (RAD && (e.flags & EF_EDGE2) && (e.flags & EF_SR) && c[CB_E2] != 0)
-    dp = dp - bend_edge_radiation(Q0, Q1, Q3, dp, c[CB_TAN_E2], c, rs.rc);
+    dp = dp - bend_edge_radiation(Q0, Q2, Q1, Q3, dp, c[CB_TAN_E2], c, rs.rc, e.flags);
 
   if (e.flags & EF_RADBLOCK) {
     /* time-of-flight velocity fix (csbend.c:1278-1288) */
@@ -585,9 +626,10 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE2) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    if (e.flags & EF_EDGE_ORDER2) {
-      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI2] * (1 + dp), c[CB_TAN_E2], c[CB_E2], c[CB_SEC2_E2],
-                       c[CB_EDGE_N], 1);
+    if (RAD && (e.flags & EF_EDGE_ORDER2)) {
+      const double *bx = rs.rc + RB_EXTRA0;
+      bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI2] * (1 + dp), c[CB_TAN_E2], c[CB_E2], bx[BX_SEC2_E2],
+                       bx[BX_EDGE_N], 1);
     } else {
       delta_xp = (c[CB_TAN_E2] / rho) * x;
       xp = xp + delta_xp;
@@ -595,12 +637,22 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
     }
   }
 
-  /* back to the lab frame, plus the ETILT exit offsets (csbend.c:1359-1364) */
-  p.x = (x * ct - y * st) + c[CB_ETILT0];
-  p.y = (x * st + y * ct) + c[CB_ETILT0 + 2];
-  p.xp = (xp * ct - yp * st) + c[CB_ETILT0 + 1];
-  p.yp = (xp * st + yp * ct) + c[CB_ETILT0 + 3];
-  p.s = s + c[CB_ETILT0 + 4];
+  /* back to the lab frame, plus the ETILT exit offsets (csbend.c:1359-1364;
+   * zero without ETILT) */
+  if (RAD && (e.flags & EF_ETILT)) {
+    const double *bx = rs.rc + RB_EXTRA0;
+    p.x = (x * ct - y * st) + bx[BX_ETILT0];
+    p.y = (x * st + y * ct) + bx[BX_ETILT0 + 2];
+    p.xp = (xp * ct - yp * st) + bx[BX_ETILT0 + 1];
+    p.yp = (xp * st + yp * ct) + bx[BX_ETILT0 + 3];
+    p.s = s + bx[BX_ETILT0 + 4];
+  } else {
+    p.x = (x * ct - y * st) + 0.0;
+    p.y = (x * st + y * ct) + 0.0;
+    p.xp = (xp * ct - yp * st) + 0.0;
+    p.yp = (xp * st + yp * ct) + 0.0;
+    p.s = s + 0.0;
+  }
   p.dp = dp;
   p.x = p.x + (c[CB_DXF] + c[CB_DZF] * p.xp);
   p.y = p.y + (c[CB_DYF] + c[CB_DZF] * p.yp);

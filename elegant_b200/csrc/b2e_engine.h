@@ -20,7 +20,7 @@
 #include <stdint.h>
 #include "../../include/elegant_b200.h"
 
-#define B2E_NC 44 /* constants per compiled element (a DevElem stays a multiple of 16 bytes) */
+#define B2E_NC 40 /* constants per compiled element */
 
 /* Compiled element kinds (device dispatch) */
 enum {
@@ -51,7 +51,9 @@ enum {
 #define EF_REVERSE_TILT 0x400   /* nonzero reverse tilt in the internal aperture check */
 #define EF_SR 0x800             /* KMULT / CSBEND: classical synchrotron radiation (SYNCH_RAD) */
 #define EF_ISR 0x1000           /* KMULT / CSBEND: quantum excitation (ISR) */
-#define EF_EDGE_ORDER2 0x2000   /* CSBEND: edges by the second-order map (EDGE_ORDER >= 2) */
+#define EF_EDGE_ORDER2 0x2000   /* CSBEND: edges by the second-order map (EDGE_ORDER >= 2; BendExtra) */
+#define EF_FIELD 0x4000         /* CSBEND: K1/K2 field terms (coefficients in the DevRad table) */
+#define EF_ETILT 0x8000         /* CSBEND: ETILT exit offsets (BendExtra) */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -93,16 +95,27 @@ enum {
 #define CB_DZF 33
 #define CB_INV_RHO0 34  /* RN(1/rho0), for X/rho0 by div_rn_recip */
 #define CB_INV_RHO_ACTUAL 35 /* RN(1/rho_actual) */
-#define CB_ETILT0 36    /* exit offsets of ETILT (x, xp, y, yp, s), 36..40; zero without ETILT */
-#define CB_SEC2_E1 41   /* sqr(1/cos(e1)), second-order edges */
-#define CB_SEC2_E2 42   /* sqr(1/cos(e2)) */
-#define CB_EDGE_N 43    /* field index n = -b1/h of the second-order edge map */
+
+/* A bend's rarely used constants (ETILT, second-order edges), kept out of
+ * the element record that the ring kernel stages in shared memory: in the
+ * DevRad table for the ring kernel (RB_EXTRA0), as a kernel argument for the
+ * CSR kernels. */
+#define BX_ETILT0 0     /* exit offsets of ETILT (x, xp, y, yp, s), 0..4; zero without ETILT */
+#define BX_SEC2_E1 5    /* sqr(1/cos(e1)), second-order edges */
+#define BX_SEC2_E2 6    /* sqr(1/cos(e2)) */
+#define BX_EDGE_N 7     /* field index n = -b1/h of the second-order edge map */
+#define B2E_NBX 8
+typedef struct {
+  double c[B2E_NBX];
+} BendExtra;
 
 
-/* Radiation constants of a KMULT / CSBEND, in a table beside the element
- * records ([instance][element] DevRad): only radiating lattices read them, so
- * the records the ring kernel stages in shared memory stay small. */
-#define B2E_NRAD 12
+/* Radiation constants of a KMULT / CSBEND, and a CSBEND's field-expansion
+ * coefficients, in a table beside the element records ([instance][element]
+ * DevRad): only lattices that radiate or have bends with K1/K2 read it (the
+ * ring kernel's RAD instantiation), so the records the ring kernel stages in
+ * shared memory stay small. */
+#define B2E_NRAD 36
 #define RK_KFRAC0 0     /* KMULT: kickFrac[j], j = 0..7 */
 #define RK_RAD 8        /* rad_coef (multipole.c:789) */
 #define RK_ISR 9        /* isr_coef, > 0 only when ISR is applied (:790-795) */
@@ -111,6 +124,9 @@ enum {
 #define RB_ISR 1        /* isrConstant, > 0 only when ISR is applied (:972-975) */
 #define RB_SLICE 2      /* s = length / N_SLICES, for dsISR (:1614) */
 #define RB_INV_RHO0 3   /* 1. / rho0 (:1605) */
+#define RB_FIELD0 12    /* CSBEND with K1/K2: the 15 field-expansion coefficients the
+                         * field sums use, 12..26 (bend_fields has the order) */
+#define RB_EXTRA0 28    /* the bend's BendExtra constants, 28..35 */
 
 /* RFCA constant slots */
 #define RF_VOLT 0       /* volt/(1e6*mc^2[MV]*sign)/nKicks */

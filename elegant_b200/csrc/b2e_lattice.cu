@@ -112,6 +112,7 @@ void element_defaults(int type, double *p) {
     p[B2E_BEND_EDGE1_EFFECTS] = 1;
     p[B2E_BEND_EDGE2_EFFECTS] = 1;
     p[B2E_BEND_EDGE_ORDER] = 1;
+    p[B2E_BEND_NONLINEAR] = 1;          /* track_data.c:1927, :2008 */
     p[B2E_BEND_ISR1PART] = 1;           /* track_data.c:1966, :2039 */
     if (type == B2E_CSRCSBEND) {
       p[B2E_BEND_BIN_RANGE_FACTOR] = 1.2; /* csrcsbend_param, track_data.c:1982-2060 */
@@ -264,6 +265,40 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
   return "";
 }
 
+/* Field expansion of a sector bend with quadrupole and sextupole terms
+ * (computeCSBENDFieldCoefficients, csbend.c:186-663): b0 the dipole
+ * correction (xKick/angle: a signed zero here), b1 = K1*rho0, b2 = K2*rho0,
+ * normal terms only, h1 the curvature.  The field sums of a normal-only
+ * expansion to order 4 read 15 coefficients; each is formed with the
+ * expansion's own terms in their order, the zero octupole and decapole terms
+ * (b3, b4) included, so that signed zeros round alike.  Without NONLINEAR
+ * only the linear ones are set.  Layout: Fx(0,1) Fx(0,3) Fx(1,1) Fx(1,3)
+ * Fx(2,1) Fx(3,1) Fy(0,0) Fy(0,2) Fy(0,4) Fy(1,0) Fy(1,2) Fy(2,0) Fy(2,2)
+ * Fy(3,0) Fy(4,0), Fx(i,j) the coefficient of x^i y^j. */
+static void bend_field_terms(double *F, double b0, double b1, double b2, double h1, bool nonlinear) {
+  const double b3 = 0, b4 = 0;
+  const double h2 = h1 * h1, h3 = h2 * h1;
+  for (int k = 0; k < 15; k++)
+    F[k] = 0;
+  F[0] = b1;
+  F[6] = 1 - b0;
+  F[9] = b1;
+  if (!nonlinear)
+    return;
+  F[1] = (h2 * b1) / 6 - (h1 * b2) / 6 - b3 / 6;
+  F[2] = b2;
+  F[3] = -(h3 * b1) / 3 + (h2 * b2) / 3 - (h1 * b3) / 6 - b4 / 6;
+  F[4] = b3 / 2;
+  F[5] = b4 / 6;
+  F[7] = -(h1 * b1) / 2 - b2 / 2;
+  F[8] = (h3 * b1) / 24 - (h2 * b2) / 24 + (h1 * b3) / 12 + b4 / 24;
+  F[10] = (h2 * b1) / 2 - (h1 * b2) / 2 - b3 / 2;
+  F[11] = b2 / 2;
+  F[12] = -(h3 * b1) / 2 + (h2 * b2) / 2 - (h1 * b3) / 4 - b4 / 4;
+  F[13] = b3 / 6;
+  F[14] = b4 / 24;
+}
+
 /* ETILT: the bend is rolled by etilt about its entrance axis, so the exit
  * face's centre moves off the design orbit.  Offsets (x, x', y, y', s) of that
  * centre in the bend frame, then turned by -tilt into the frame the exit
@@ -335,8 +370,9 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     return "CSBEND integration_order is invalid--must be 2, 4, or 6";
   if (nSlices < 1)
     return "CSBEND N_SLICES must be >= 1";
-  if (p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0)
-    return "CSBEND with K1/K2 field terms is not supported by this engine";
+  const bool fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0;
+  if (fields && el.type == B2E_CSRCSBEND)
+    return "CSRCSBEND with K1/K2 field terms is not supported by this engine";
   if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
     return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
   /* csbend.c:933-950: negative angle folded into a PI tilt */
@@ -417,7 +453,10 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
   d.c[CB_DXF] = p[B2E_BEND_DX] * b2e_cos(p[B2E_BEND_ANGLE]) + p[B2E_BEND_DZ] * b2e_sin(p[B2E_BEND_ANGLE]);
   d.c[CB_DZF] = p[B2E_BEND_DX] * b2e_sin(p[B2E_BEND_ANGLE]) - p[B2E_BEND_DZ] * b2e_cos(p[B2E_BEND_ANGLE]);
   d.c[CB_DYF] = p[B2E_BEND_DY];
-  etilt_exit_offsets(d.c + CB_ETILT0, rho0, angle, etilt, tilt);
+  double *bx = r.c + RB_EXTRA0;
+  etilt_exit_offsets(bx + BX_ETILT0, rho0, angle, etilt, tilt);
+  if (etilt != 0)
+    d.flags |= EF_ETILT;
   d.c[CB_INV_RHO0] = 1 / rho0;
   d.c[CB_INV_RHO_ACTUAL] = 1 / rho_actual;
   if (edge1)
@@ -429,13 +468,15 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
      * per-element parts; b1 = K1*rho0 (csbend.c:825), sign-flipped with a
      * negative angle (:879-882), gives n = -b1/h (:929) */
     double b1 = p[B2E_BEND_K1] * (length / p[B2E_BEND_ANGLE]);
+    if (el.type == B2E_CSBEND)
+      b1 *= ((1 + p[B2E_BEND_FSE]) + 0) / ((1 + p[B2E_BEND_FSE]) + 0);
     if (p[B2E_BEND_ANGLE] < 0)
       b1 *= -1;
     const double sec1 = 1. / b2e_cos(e1), sec2 = 1. / b2e_cos(e2);
     d.flags |= EF_EDGE_ORDER2;
-    d.c[CB_SEC2_E1] = sec1 * sec1;
-    d.c[CB_SEC2_E2] = sec2 * sec2;
-    d.c[CB_EDGE_N] = -b1 / h;
+    bx[BX_SEC2_E1] = sec1 * sec1;
+    bx[BX_SEC2_E2] = sec2 * sec2;
+    bx[BX_EDGE_N] = -b1 / h;
   }
   if (-tilt != 0) {
     d.flags |= EF_REVERSE_TILT;
@@ -459,6 +500,19 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     r.c[RB_ISR] = isr_const;
     r.c[RB_SLICE] = s;
     r.c[RB_INV_RHO0] = 1. / rho0;
+    if (fields) {
+      /* b[] as track_through_csbend forms it (csbend.c:824-882): K*rho0 with
+       * the signed angle, the FSE ratios (1 + fse)/(1 + fse), the quadrupole
+       * term negated with a negative angle; b0 = xKick/angle */
+      const double rho_signed = length / p[B2E_BEND_ANGLE];
+      double b1 = p[B2E_BEND_K1] * rho_signed, b2 = p[B2E_BEND_K2] * rho_signed;
+      b1 *= ((1 + p[B2E_BEND_FSE]) + 0) / ((1 + p[B2E_BEND_FSE]) + 0);
+      b2 *= (1 + p[B2E_BEND_FSE]) / ((1 + p[B2E_BEND_FSE]) + 0);
+      if (p[B2E_BEND_ANGLE] < 0)
+        b1 *= -1;
+      bend_field_terms(r.c + RB_FIELD0, 0.0 / p[B2E_BEND_ANGLE], b1, b2, h, p[B2E_BEND_NONLINEAR] != 0);
+      d.flags |= EF_FIELD;
+    }
     d.flags |= EF_RADBLOCK;
     if (rad_coef != 0)
       d.flags |= EF_SR;
@@ -508,19 +562,21 @@ static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
 /* One CSRCSBEND standing alone (both edges active as its parameters say),
  * compiled into `d` without any container; returns nullptr on success or a
  * static message. */
-const char *compile_single_csr_bend(const b2e_element &el, DevElem &d) {
+const char *compile_single_csr_bend(const b2e_element &el, DevElem &d, BendExtra &bx) {
   static thread_local char msg[256];
   if (el.type != B2E_CSRCSBEND)
     return "element is not a CSRCSBEND";
   memset(&d, 0, sizeof(d));
   d.ap_pass0 = d.ap_later = -1;
-  DevRad unused_rad;
+  DevRad rad;
+  memset(&rad, 0, sizeof(rad));
   std::string e = compile_csbend(el, el.p[B2E_BEND_EDGE1_EFFECTS] != 0, el.p[B2E_BEND_EDGE2_EFFECTS] != 0, 0.0, d,
-                                 unused_rad);
+                                 rad);
   if (!e.empty()) {
     snprintf(msg, sizeof(msg), "%s", e.c_str());
     return msg;
   }
+  memcpy(bx.c, rad.c + RB_EXTRA0, sizeof(bx.c));
   if (d.kind != K_CSRCSBEND)
     return "CSRCSBEND with zero angle is a drift; nothing to do here";
   d.z_end = el.p[B2E_BEND_L];

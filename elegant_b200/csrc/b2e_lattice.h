@@ -32,7 +32,7 @@ struct CompiledLattice {
 };
 
 /* One standalone CSRCSBEND -> DevElem; nullptr on success, else a message. */
-const char *compile_single_csr_bend(const b2e_element &el, DevElem &d);
+const char *compile_single_csr_bend(const b2e_element &el, DevElem &d, BendExtra &bx);
 
 /* Returns an empty string on success, else a description of the problem. */
 std::string compile_lattice(const b2e_element *elements, int n, const b2e_run_options &opt, CompiledLattice &out);

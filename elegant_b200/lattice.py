@@ -39,7 +39,8 @@ _KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, 
           "INTEGRATION_ORDER": 9, "SYNCH_RAD": 12, "ISR": 13, "ISR1PART": 14}
 _BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "DY": 7, "DZ": 8, "FSE": 9,
          "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
-         "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18, "SYNCH_RAD": 35, "ISR": 36, "ISR1PART": 37}
+         "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18, "NONLINEAR": 19, "SYNCH_RAD": 35, "ISR": 36,
+         "ISR1PART": 37}
 _CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=23, SGDERIV_HALFWIDTH=24,
                 SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29, IGF=30,
                 LOW_FREQUENCY_CUTOFF0=31, LOW_FREQUENCY_CUTOFF1=32, HIGH_FREQUENCY_CUTOFF0=33,
@@ -67,9 +68,9 @@ DEFAULTS = {
     nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1},
     nat.KSEXT: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1},
     nat.CSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
-                 "EDGE_ORDER": 1, "ISR1PART": 1},
+                 "EDGE_ORDER": 1, "NONLINEAR": 1, "ISR1PART": 1},
     nat.CSRCSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
-                    "EDGE_ORDER": 1, "ISR1PART": 1, "BIN_RANGE_FACTOR": 1.2, "SG_ORDER": 1, "TRAPAZOID_INTEGRATION": 1, "CSR": 1,
+                    "EDGE_ORDER": 1, "NONLINEAR": 1, "ISR1PART": 1, "BIN_RANGE_FACTOR": 1.2, "SG_ORDER": 1, "TRAPAZOID_INTEGRATION": 1, "CSR": 1,
                     "CLIP_NEGATIVE_BINS": 1, "LOW_FREQUENCY_CUTOFF0": -1, "LOW_FREQUENCY_CUTOFF1": -1,
                     "HIGH_FREQUENCY_CUTOFF0": -1, "HIGH_FREQUENCY_CUTOFF1": -1},
     nat.RFCA: {"FREQ": 500e6, "T_REFERENCE": -1},

@@ -111,6 +111,7 @@ extern "C" {
 #define B2E_BEND_EDGE_ORDER 16
 #define B2E_BEND_K1 17
 #define B2E_BEND_K2 18
+#define B2E_BEND_NONLINEAR 19 /* CSBEND: 1 (default) includes the nonlinear expansion terms of K1/K2 */
 /* CSRCSBEND-only slots */
 #define B2E_BEND_BINS 20
 #define B2E_BEND_BIN_RANGE_FACTOR 21

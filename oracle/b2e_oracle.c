@@ -593,7 +593,64 @@ typedef struct {
   double rad_coef, isr;
   int64_t id;
   int pass, elem;
+  int fields;                /* K1/K2 present: the expansion below is used */
+  double Fx_xy[5][5], Fy_xy[5][5];
 } BendRad;
+
+/* computeCSBENDFieldCoefficients (csbend.c:186-663) for normal quadrupole and
+ * sextupole terms (b[1] = K1 rho0, b[2] = K2 rho0, b[0] the dipole
+ * correction), expansion order 4, the entries the field sums read. */
+static void bend_field_table(BendRad *br, const double *b_in, double h1, int nonlinear) {
+  double h[4], b[4];
+  int i;
+  memset(br->Fx_xy, 0, sizeof(br->Fx_xy));
+  memset(br->Fy_xy, 0, sizeof(br->Fy_xy));
+  h[0] = 1;
+  for (i = 1; i < 4; i++)
+    h[i] = h[i - 1] * h1;
+  br->Fy_xy[0][0] = 1 - b_in[0];
+  for (i = 0; i < 4; i++)
+    b[i] = b_in[i + 1]; /* b[0] the quadrupole term from here on */
+  br->Fx_xy[0][1] = b[0];
+  br->Fy_xy[1][0] = b[0];
+  if (!nonlinear)
+    return;
+  br->Fy_xy[0][2] = -(h[1] * b[0]) / 2 - b[1] / 2;
+  br->Fy_xy[0][4] = (h[3] * b[0]) / 24 - (h[2] * b[1]) / 24 + (h[1] * b[2]) / 12 + b[3] / 24;
+  br->Fy_xy[1][2] = (h[2] * b[0]) / 2 - (h[1] * b[1]) / 2 - b[2] / 2;
+  br->Fy_xy[2][0] = b[1] / 2;
+  br->Fy_xy[2][2] = -(h[3] * b[0]) / 2 + (h[2] * b[1]) / 2 - (h[1] * b[2]) / 4 - b[3] / 4;
+  br->Fy_xy[3][0] = b[2] / 6;
+  br->Fy_xy[4][0] = b[3] / 24;
+  br->Fx_xy[1][1] = b[1];
+  br->Fx_xy[0][3] = (h[2] * b[0]) / 6 - (h[1] * b[1]) / 6 - b[2] / 6;
+  br->Fx_xy[1][3] = -(h[3] * b[0]) / 3 + (h[2] * b[1]) / 3 - (h[1] * b[2]) / 6 - b[3] / 6;
+  br->Fx_xy[2][1] = b[2] / 2;
+  br->Fx_xy[3][1] = b[3] / 6;
+}
+
+/* computeCSBENDFields, TURBO_MODE form (csbend.c:101-150), normal terms */
+static void bend_fields_at(const BendRad *br, double x, double y, double *Fx, double *Fy) {
+  double yp[5], xt = 1, sumFx = 0, sumFy = 0;
+  int i, j;
+  if (!br || !br->fields) {
+    *Fx = 0;
+    *Fy = 1;
+    return;
+  }
+  yp[0] = 1;
+  for (i = 1; i < 5; i++)
+    yp[i] = yp[i - 1] * y;
+  for (i = 0; i < 5; i++) {
+    for (j = 1; j < 5 - i; j += 2)
+      sumFx += br->Fx_xy[i][j] * xt * yp[j];
+    for (j = 0; j < 5 - i; j += 2)
+      sumFy += br->Fy_xy[i][j] * xt * yp[j];
+    xt *= x;
+  }
+  *Fx = sumFx;
+  *Fy = sumFy;
+}
 
 static int csbend_integrate(double *Qf, const double *Qi, double s, long n, double rho0, double rho_actual,
                             const MultAp *ap, int integ, int isr_block, double *dz_lost, const BendRad *br) {
@@ -632,15 +689,17 @@ static int csbend_integrate(double *Qf, const double *Qi, double s, long n, doub
       if (kf[j] == 0)
         break;
       ds = s * kf[j];
-      /* pure dipole: Fx = 0, Fy = 1 */
-      Qf[1] += -ds * (1 + Qf[0] / rho0) * 1.0 / rho_actual;
-      Qf[3] += ds * (1 + Qf[0] / rho0) * 0.0 / rho_actual;
+      {
+        double Fx, Fy;
+        bend_fields_at(br, Qf[0], Qf[2], &Fx, &Fy);
+        Qf[1] += -ds * (1 + Qf[0] / rho0) * Fy / rho_actual;
+        Qf[3] += ds * (1 + Qf[0] / rho0) * Fx / rho_actual;
       if (isr_block) {
-        /* csbend.c:1603-1622 with Fx = 0, Fy = 1 */
+        /* csbend.c:1603-1622 */
         double f = (1 + Qf[0] * (1. / rho0)) / sqrt(SQR(1 + Qf[5]) - SQR(Qf[1]) - SQR(Qf[3]));
         double xp = Qf[1] * f, yp = Qf[3] * f;
         double dsFactor = sqrt(SQR(1 + Qf[0] * (1. / rho0)) + SQR(xp) + SQR(yp));
-        double F2 = SQR(0.0) + SQR(1.0);
+        double F2 = SQR(Fx) + SQR(Fy);
         double deltaFactor = SQR(1 + Qf[5]);
         double dsISR = s / (nSub - 1);
         Qf[1] /= (1 + Qf[5]);
@@ -652,6 +711,7 @@ static int csbend_integrate(double *Qf, const double *Qi, double s, long n, doub
                    b2e_isr_gauss(g_isr_seed, br->id, br->pass, br->elem, i, j, g_sr_limit);
         Qf[1] *= (1 + Qf[5]);
         Qf[3] *= (1 + Qf[5]);
+      }
       }
     }
   }
@@ -802,6 +862,7 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   h = 1 / rho0;
   /* n = -b[1]/h with b[1] = K1*rho0, sign-flipped for a negative angle (csbend.c:825, :879-882, :929) */
   n_index = p[B2E_BEND_K1] * (length / p[B2E_BEND_ANGLE]);
+  n_index *= (1 + p[B2E_BEND_FSE] + 0) / (1 + p[B2E_BEND_FSE] + 0);
   if (p[B2E_BEND_ANGLE] < 0)
     n_index *= -1;
   n_index = -n_index / h;
@@ -848,6 +909,22 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     br.isr *= -1;
   br.pass = pass;
   br.elem = idx;
+  /* b[] of the field expansion (csbend.c:824-882): K*rho0 with the signed
+   * angle, the FSE ratios, odd terms negated with a negative angle */
+  br.fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0;
+  if (br.fields) {
+    double b[5] = {0, 0, 0, 0, 0}, rs = length / p[B2E_BEND_ANGLE];
+    b[1] = p[B2E_BEND_K1] * rs;
+    b[2] = p[B2E_BEND_K2] * rs;
+    b[1] *= (1 + p[B2E_BEND_FSE] + 0) / (1 + p[B2E_BEND_FSE] + 0);
+    b[2] *= (1 + p[B2E_BEND_FSE]) / (1 + p[B2E_BEND_FSE] + 0);
+    b[0] = 0.0 / p[B2E_BEND_ANGLE];
+    if (p[B2E_BEND_ANGLE] < 0) {
+      b[1] *= -1;
+      b[3] *= -1;
+    }
+    bend_field_table(&br, b, h, p[B2E_BEND_NONLINEAR] != 0);
+  }
   itop = np - 1;
   for (ip = 0; ip <= itop; ip++) {
     double *coord = c[ip], x, y, xp, yp, s, dp, dp0, Qi[6], Qf[6], rho, f, dz_lost;
@@ -879,8 +956,9 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     Qi[5] = dp;
     if (edge1 && e1 != 0 && br.rad_coef) {
       /* csbend.c:1211-1216 */
-      double dp_prime = -br.rad_coef * (SQR(0.0) + SQR(1.0)) * SQR(1 + dp) *
-                        sqrt(SQR(1 + x / rho0) + SQR(xp) + SQR(yp));
+      double Fx, Fy, dp_prime;
+      bend_fields_at(&br, x, y, &Fx, &Fy);
+      dp_prime = -br.rad_coef * (SQR(Fx) + SQR(Fy)) * SQR(1 + dp) * sqrt(SQR(1 + x / rho0) + SQR(xp) + SQR(yp));
       Qi[5] -= dp_prime * x * M_TAN(e1);
     }
     f = (1 + Qi[5]) / sqrt(1 + SQR(Qi[1]) + SQR(Qi[3]));
@@ -904,8 +982,10 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     }
     if (edge2 && e2 != 0 && br.rad_coef) {
       /* csbend.c:1265-1276 */
-      double dp_prime = -br.rad_coef * (SQR(0.0) + SQR(1.0)) * SQR(1 + Qf[5]) *
-                        sqrt(SQR(1 + Qf[0] / rho0) + SQR(Qf[1]) + SQR(Qf[3]));
+      double Fx, Fy, dp_prime;
+      bend_fields_at(&br, Qf[0], Qf[2], &Fx, &Fy);
+      dp_prime = -br.rad_coef * (SQR(Fx) + SQR(Fy)) * SQR(1 + Qf[5]) *
+                 sqrt(SQR(1 + Qf[0] / rho0) + SQR(Qf[1]) + SQR(Qf[3]));
       Qf[5] -= dp_prime * Qf[0] * M_TAN(e2);
     }
     {

@@ -68,9 +68,9 @@ def test_csr_elements_take_no_per_instance_overrides():
 
 
 @pytest.mark.parametrize("typ, params, words", [
-    ("CSBEND", {"L": 1.0, "ANGLE": 0.1, "K1": 0.5}, "K1"),
-    ("CSBEND", {"L": 1.0, "ANGLE": 0.1, "EDGE_ORDER": 2}, "EDGE_ORDER"),
-    ("RFCA", {"L": 0.2, "VOLT": 1e6, "FREQ": 5e8}, "length"),
+    ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 100, "K1": 0.5}, "K1"),
+    ("CSBEND", {"L": 1.0, "ANGLE": 0.1, "EDGE1_EFFECTS": 2}, "EDGE"),
+    ("RFCA", {"L": -0.2, "VOLT": 1e6, "FREQ": 5e8}, "negative length"),
     ("KQUAD", {"L": 0.2, "K1": 1.0, "INTEGRATION_ORDER": 3}, "INTEGRATION_ORDER"),
     ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 100, "IGF": 1}, "STEADY_STATE"),
     ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 1}, "bins"),

@@ -420,3 +420,32 @@ def test_ring_with_second_order_edges(ref_b2e):
     assert 100 <= nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+@pytest.mark.parametrize("case", ["plain", "negative_angle", "synch_rad"])
+def test_ring_with_gradient_dipoles(ref_b2e, case):
+    """CSBEND with K1/K2 field terms (the expansion of csbend.c:186-663, the
+    field sums :101-150 in the kick and, with SYNCH_RAD, in the radiation and
+    edge corrections), NONLINEAR=0 on some, second-order edges on some,
+    negative angles: 60 turns with losses, bit-identical to the reference."""
+    import math
+    errs = [{"K1": 0.15, "K2": 2.0}, {"K1": -0.2, "NONLINEAR": 0}, {"K2": -3.0, "EDGE_ORDER": 2, "E1": 0.1},
+            {"K1": 0.1, "K2": 1.0, "FSE": 1e-3}]
+    base = w.radiating_ring(edge_angle=0.05) if case == "synch_rad" else w.fodo_ring()
+    els, k = [], 0
+    for e in base.elements:
+        if e.type == "CSBEND":
+            params = dict(e.params, **errs[k % len(errs)])
+            if case == "negative_angle" and k % 2:
+                params.update(ANGLE=-params["ANGLE"], TILT=math.pi)
+            e = Element(e.name + str(k), e.type, params)
+            k += 1
+        els.append(e)
+    lat = Lattice(els)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=51).coords, _lossy_beam(150, seed=52).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

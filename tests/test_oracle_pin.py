@@ -8,6 +8,8 @@
   many turns no further apart than a one-ulp perturbation of the initial
   coordinates grows by itself under the reference with glibc.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -384,3 +386,46 @@ def test_port_reproduces_reference_second_order_edges(math):
     r2, n2, _, w2 = PortOracle(math).track(lat, beam.coords, beam.ids, p0, 1, capture_wakes=True)
     assert n1 == n2 and np.array_equal(w1, w2)
     assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+
+
+def _ring_with_gradient_dipoles(base=None, negative=False):
+    """The ring with combined-function dipoles: K1 and K2 in the bends
+    (computeCSBENDFields' expansion), one of them NONLINEAR=0, one with
+    second-order edges (the edge map's n = -b1/h), one with an FSE;
+    negative=True folds every other dipole into a negative angle (a TILT of
+    PI)."""
+    from elegant_b200 import Element, Lattice
+    errs = [{"K1": 0.15, "K2": 2.0}, {"K1": -0.2, "NONLINEAR": 0}, {"K2": -3.0, "EDGE_ORDER": 2, "E1": 0.1},
+            {"K1": 0.1, "K2": 1.0, "FSE": 1e-3}]
+    els, k = [], 0
+    for e in (base or w.fodo_ring()).elements:
+        if e.type == "CSBEND":
+            params = dict(e.params, **errs[k % len(errs)])
+            if negative and k % 2:
+                params.update(ANGLE=-params["ANGLE"], TILT=math.pi)
+            e = Element(e.name + str(k), e.type, params)
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+def _mixed_beam(seed):
+    return Beam(np.concatenate([w.ring_beam(100, seed=seed).coords, lossy_beam(100, seed=seed + 1).coords]),
+                np.arange(1, 201))
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("case", ["plain", "negative_angle", "synch_rad"])
+def test_port_reproduces_reference_gradient_dipoles(math, case):
+    """CSBEND with K1/K2 field terms (csbend.c:101-150, :186-663, the kick
+    :1591-1601 and the radiation :1603-1622, :1211-1276), with losses."""
+    base = w.radiating_ring(edge_angle=0.05) if case == "synch_rad" else None
+    lat = _ring_with_gradient_dipoles(base, negative=case == "negative_angle")
+    beam = _mixed_beam(47)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    r0, n0, _, _ = RefOracle(math).track(base or w.fodo_ring(), beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
