@@ -22,7 +22,13 @@ path are
   n_particles_per_bunch;
 - &twiss_output with matched = 1 and &bunched_beam use_twiss_command_values
   = 1: the beam is matched to the periodic Twiss parameters of the line;
-- &track: runs n_steps steps of n_passes passes.
+- &track: runs n_steps steps of n_passes passes;
+- &find_aperture (aperture_search.nl): the many-particle mode, the one- to
+  eleven-line modes and n-line, slope mode (xmin == xmax) and
+  optimization_mode (the area only, no file), with setup_aperture_search's
+  checks; the output file per step;
+- &momentum_aperture (momentumAperture.nl): every key but
+  forbid_resonance_crossing, fiducialize included; output_mode 0 or 1.
 
 A command outside this list, or a key of these commands away from its
 default that the engine does not implement, raises EleError naming it: the
@@ -211,8 +217,71 @@ TRACK = {"center_on_orbit": 0, "center_momentum_also": 1, "offset_by_orbit": 0, 
 TWISS_OUTPUT = {"matched": 1, "filename": None, "output_at_each_step": 0, "statistics": 0, "radiation_integrals": 0,
                 "beta_x": 1.0, "alpha_x": 0.0, "eta_x": 0.0, "etap_x": 0.0, "beta_y": 1.0, "alpha_y": 0.0,
                 "eta_y": 0.0, "etap_y": 0.0, "concat_order": 0}
+FIND_APERTURE = {"output": None, "search_output": None, "boundary": None, "mode": "many-particle", "xmin": -0.1,
+                 "xmax": 0.1, "xpmin": 0.0, "xpmax": 0.0, "ymin": 0.0, "ymax": 0.1, "ypmin": 0.0, "ypmax": 0.0,
+                 "nx": 21, "n_splits": 0, "split_fraction": 0.5, "desired_resolution": 0.01, "ny": 11,
+                 "verbosity": 0, "assume_nonincreasing": 0, "offset_by_orbit": 0, "n_lines": 11, "full_plane": 0,
+                 "optimization_mode": 0}
+MOMENTUM_APERTURE = {"output": None, "x_initial": 1e-5, "y_initial": 1e-5, "delta_negative_limit": -0.10,
+                     "delta_positive_limit": 0.10, "delta_negative_start": 0.0, "delta_positive_start": 0.0,
+                     "delta_step_size": 0.0025, "splits": 1, "steps_back": 1, "split_step_divisor": 10,
+                     "skip_elements": 0, "process_elements": 2147483647, "s_start": 0.0, "s_end": 1.7976931348623157e308,
+                     "include_name_pattern": None, "include_type_pattern": None, "fiducialize": 0, "verbosity": 1,
+                     "soft_failure": 0, "output_mode": 0, "forbid_resonance_crossing": 0,
+                     "allow_watch_file_output": 0}
 # commands that change nothing the tracking path computes
 INERT = {"global_settings", "print_dictionary", "semaphores", "stop", "subprocess", "run_rpnexpr"}
+LINE_MODE_LINES = {"one-line": 1, "two-line": 2, "three-line": 3, "five-line": 5, "seven-line": 7, "nine-line": 9,
+                   "eleven-line": 11}
+
+
+def _check_find_aperture(fa: dict) -> tuple[str, bool, int]:
+    """setup_aperture_search's checks (aperture_search.c:118-170).  Returns
+    (mode, slope mode, lines)."""
+    if not fa["output"] and not fa["optimization_mode"]:
+        raise EleError("&find_aperture: no output filename specified (required if optimization_mode=0)")
+    slope = fa["xmin"] == fa["xmax"]
+    if slope:
+        if fa["xpmin"] == fa["xpmax"] or fa["ypmin"] == fa["ypmax"]:
+            raise EleError("&find_aperture: if xmin==xmax, must not have xpmin==xpmax or ypmin==ypmax")
+        if fa["ymin"] != fa["ymax"]:
+            raise EleError("&find_aperture: if xmin==xmax, must also have ymin==ymax")
+    else:
+        if fa["xmin"] >= fa["xmax"]:
+            raise EleError("&find_aperture: xmin >= xmax")
+        if fa["ymin"] >= fa["ymax"]:
+            raise EleError("&find_aperture: ymin >= ymax")
+        if fa["xpmin"] != fa["xpmax"] or fa["ypmin"] != fa["ypmax"]:
+            raise EleError("&find_aperture: if xmin!=xmax, must have xpmin==xpmax and ypmin==ypmax")
+    if fa["nx"] < 3:
+        raise EleError("&find_aperture: nx < 3")
+    if fa["ny"] < 2:
+        raise EleError("&find_aperture: ny < 2")
+    if fa["n_splits"]:
+        if not 0 < fa["split_fraction"] < 1:
+            raise EleError("&find_aperture: split_fraction must be greater than 0 and less than 1")
+        if not 0 < fa["desired_resolution"] < 1:
+            raise EleError("&find_aperture: desired_resolution must be greater than 0 and less than 1")
+        if fa["desired_resolution"] * (fa["xmax"] - fa["xmin"]) > (fa["xmax"] - fa["xmin"]) / (fa["nx"] - 1):
+            raise EleError("&find_aperture: desired_resolution is larger than coarse mesh")
+    mode = fa["mode"]
+    if mode == "n-line":
+        lines = fa["n_lines"]
+    elif mode in LINE_MODE_LINES:
+        lines = LINE_MODE_LINES[mode]
+    elif mode == "many-particle":
+        lines = 0
+    else:
+        raise EleError(f"&find_aperture: mode {mode!r} is not supported by the engine's runner")
+    if slope and mode != "n-line":
+        raise EleError('&find_aperture: slope-based aperture search only supported for mode="n-line"')
+    if fa["full_plane"] and mode == "many-particle":
+        raise EleError("&find_aperture: full_plane=1 is only supported for line-based modes at present")
+    if fa["optimization_mode"] and (mode in ("many-particle", "one-line", "two-line") or
+                                    (mode == "n-line" and lines < 3)):
+        raise EleError("&find_aperture: dynamic aperture optimization requires use of n-line mode with at "
+                       "least 3 lines")
+    return mode, slope, lines
 
 
 def _convert(default, value):
@@ -348,9 +417,13 @@ def _lattice_with_outputs(text: str, use: str | None):
 def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
     """Run a .ele file's tracking job on the engine; returns a summary per
     step (survivors, effort) and the files written."""
+    from .aperture import find_aperture_lines, find_aperture_mp
+    from .momentum_aperture import momentum_aperture
     from .optics import periodic_twiss
-    from .sdds import write_csr_wake, write_losses, write_phase_space
+    from .sdds import (write_aperture, write_aperture_mp, write_csr_wake, write_losses, write_momentum_aperture,
+                       write_phase_space)
     from .track import Tracker
+    mode_io = mode
     base = os.path.dirname(os.path.abspath(path))
     rootname = os.path.splitext(os.path.basename(path))[0]
     with open(path) as fh:
@@ -422,6 +495,60 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                         summary["files"].append(name(fname))
             summary["files"] += outs + ([losses] if losses else [])
             summary["result"] = res
+        elif cmd == "find_aperture":
+            fa = _command(fields, FIND_APERTURE, cmd,
+                          {"output", "mode", "xmin", "xmax", "xpmin", "xpmax", "ymin", "ymax", "ypmin", "ypmax", "nx",
+                           "ny", "n_splits", "split_fraction", "desired_resolution", "verbosity", "n_lines",
+                           "full_plane", "optimization_mode"})
+            if rs is None:
+                raise EleError("&find_aperture needs &run_setup before it")
+            mode, slope, lines = _check_find_aperture(fa)
+            rc = rc or dict(RUN_CONTROL)
+            p0 = rs["p_central"] or rs["p_central_mev"] / ME_MEV
+            out = name(fa["output"]) if not fa["optimization_mode"] else None
+            for step in range(rc["n_steps"]):
+                if mode == "many-particle":
+                    res, effort = find_aperture_mp(lattice, p0, rc["n_passes"], fa["xmin"], fa["xmax"], fa["ymin"],
+                                                   fa["ymax"], fa["nx"], fa["ny"], device=device)
+                    if out:
+                        write_aperture_mp(out, res[0], step=step + 1, mode=mode_io)
+                    summary["steps"].append({"step": step + 1, "boundary": res[0]["boundary"], "effort": effort})
+                else:
+                    res = find_aperture_lines(lattice, p0, rc["n_passes"], lines=lines, xmax=fa["xmax"],
+                                              ymax=fa["ymax"], nx=fa["nx"], n_splits=fa["n_splits"],
+                                              split_fraction=fa["split_fraction"], full_plane=bool(fa["full_plane"]),
+                                              device=device, slope=slope, xpmax=fa["xpmax"], ypmax=fa["ypmax"])
+                    if out:
+                        write_aperture(out, res, step=step + 1, mode=mode_io)
+                    summary["steps"].append({"step": step + 1, "area": res["area"], "lines": res["lines"]})
+                summary["result"] = res
+            if out:
+                summary["files"].append(out)
+        elif cmd == "momentum_aperture":
+            ma = _command(fields, MOMENTUM_APERTURE, cmd, set(MOMENTUM_APERTURE) - {"forbid_resonance_crossing"})
+            if rs is None:
+                raise EleError("&momentum_aperture needs &run_setup before it")
+            if ma["output_mode"] not in (0, 1):
+                raise EleError("&momentum_aperture: output_mode=2 is elegant's MPI-only mode "
+                               "(not available in serial elegant)")
+            if not ma["output"]:
+                raise EleError("&momentum_aperture: no output filename specified")
+            rc = rc or dict(RUN_CONTROL)
+            p0 = rs["p_central"] or rs["p_central_mev"] / ME_MEV
+            out = name(ma["output"])
+            kw = {k: ma[k] for k in ("x_initial", "y_initial", "delta_negative_limit", "delta_positive_limit",
+                                     "delta_negative_start", "delta_positive_start", "delta_step_size", "splits",
+                                     "steps_back", "split_step_divisor", "skip_elements", "process_elements",
+                                     "s_start", "s_end", "include_name_pattern", "include_type_pattern")}
+            for step in range(rc["n_steps"]):
+                try:
+                    rows, effort = momentum_aperture(lattice, p0, rc["n_passes"], soft_failure=bool(ma["soft_failure"]),
+                                                     fiducialize=bool(ma["fiducialize"]), device=device, **kw)
+                except ValueError as e:
+                    raise EleError(f"&momentum_aperture: {e}") from e
+                write_momentum_aperture(out, rows, step=step + 1, mode=mode_io, output_mode=ma["output_mode"])
+                summary["steps"].append({"step": step + 1, "rows": rows, "effort": effort})
+            summary["files"].append(out)
         elif cmd in INERT:
             continue
         else:

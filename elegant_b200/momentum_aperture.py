@@ -22,9 +22,23 @@ offset_beam changes nothing).  The deltas come from the same repeated
 additions, so the first loss of each scan, the last survivor before it and
 the next level's start are the reference's, bit for bit.
 
-Not built: fiducialize = 1, forbid_resonance_crossing (needs tunes from
-turn-by-turn data), output modes 1 and 2, include patterns with wildcards
-other than '*' and '?'.
+fiducialize = 1 (:385-410, :527, :560-566): one on-momentum particle from
+the origin is tracked first and sets the RF phase references, which every
+trial then keeps.  Batched: each instance carries that fiducial particle as
+its first row and the trial as its second; the engine takes the phase
+reference from the first row alone (fiducial_particles = 1), and the wedge
+acts on the trial's particle ID only (MALIGN START_PID = END_PID), so the
+fiducial row runs the reference's fiducial run (one pass) in every
+instance.  A fiducial particle lost on that pass stops the search, as in
+the reference.
+
+output_mode 1 (one row per element and side, :141-160, :715-731) is a layout
+of the same results (elegant_b200.sdds.write_momentum_aperture); output_mode
+2 is the reference's MPI-only mode (:185, "not available in serial
+elegant"): the batched engine is this module's parallel form.
+
+Not built: forbid_resonance_crossing (needs tunes from turn-by-turn data),
+include patterns with wildcards other than '*' and '?'.
 """
 from __future__ import annotations
 
@@ -95,16 +109,18 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
                       delta_positive_start=0.0, delta_step_size=0.0025, splits=1, steps_back=1,
                       split_step_divisor=10, s_start=0.0, s_end=math.inf, include_name_pattern=None,
                       include_type_pattern=None, skip_elements=0, process_elements=2 ** 31 - 1,
-                      soft_failure=False, device=0, compact_every=0, track_trials=None):
+                      soft_failure=False, fiducialize=False, device=0, compact_every=0, track_trials=None):
     """Returns one dict per selected element: name, type, s (its end),
-    index, and per side ('negative', 'positive'): delta (last survivor),
+    index, occurrence (1-based among the elements of its name), and per side
+    ('negative', 'positive'): delta (last survivor),
     found (a loss was found), lost_on_pass, x_lost, y_lost, s_lost (end of
     the element of the loss), delta_when_lost (the particle's delta there),
     delta_lost (the first lost trial's offset).  Also returns the number of
     particle-turns tracked.  track_trials(lattice, offsets, overrides, beam,
     p_central, n_passes) -> (lost_pass, coords at the end or at loss, effort),
     rows in beam order, replaces the engine (used to check the batching
-    against a CPU tracker)."""
+    against a CPU tracker); with fiducialize the beam has two rows per
+    instance, the fiducial particle first."""
     if delta_negative_limit >= 0 or delta_positive_limit <= 0 or delta_negative_start > 0 or \
             delta_positive_start < 0 or delta_step_size <= 0 or splits < 0 or s_start >= s_end:
         raise ValueError("momentum_aperture: invalid limits, starts, step, splits or s range "
@@ -137,7 +153,7 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
         if trials:
             lost_pass, x_l, y_l, dpl, lost_elem, eff = _track_trials(wl, wedges, st, trials, p_central, n_passes,
                                                                      x_initial, y_initial, device, compact_every,
-                                                                     track_trials)
+                                                                     track_trials, fiducialize)
             effort += eff
             done = set()
             for t, (j, d) in enumerate(trials):
@@ -177,7 +193,8 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
     out = []
     for k, i in enumerate(locs):
         e = lattice.elements[i]
-        row = {"index": i, "name": e.name, "type": e.type, "s": float(z_end[i])}
+        occurrence = sum(1 for f in lattice.elements[:i + 1] if f.name == e.name)
+        row = {"index": i, "name": e.name, "type": e.type, "s": float(z_end[i]), "occurrence": occurrence}
         for side, label in ((0, "negative"), (1, "positive")):
             s = st[2 * k + side]
             row[label] = {"delta": s["survived"], "found": s["loser"], "lost_on_pass": s["lost_on_pass"],
@@ -189,28 +206,44 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
 
 
 def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_initial, device, compact_every,
-                  track_trials=None):
-    """One engine run, one instance (one particle) per trial."""
+                  track_trials=None, fiducialize=False):
+    """One engine run, one instance per trial: the trial's particle alone, or
+    (fiducialize) the fiducial particle, ID 2t+1, then the trial's, ID 2t+2.
+    Returns the trials' loss passes, x, y and delta (at the end or at the
+    loss), loss elements and the effort."""
     n = len(trials)
-    coords = np.zeros((n, 6))
-    ids = np.arange(1, n + 1, dtype=np.int64)
-    offsets = np.arange(n + 1, dtype=np.int64)
+    per = 2 if fiducialize else 1
+    coords = np.zeros((per * n, 6))
+    ids = np.arange(1, per * n + 1, dtype=np.int64)
+    offsets = np.arange(0, per * n + 1, per, dtype=np.int64)
+    trial_id = ids[per - 1::per].astype(np.float64)
     overrides = []
     for w_k, wi in enumerate(wedges):
         dx = np.zeros(n)
         dy = np.zeros(n)
         dp = np.zeros(n)
+        pid = np.full(n, -1.0)
         for t, (j, d) in enumerate(trials):
             if st[j]["k"] == w_k:
                 dx[t], dy[t], dp[t] = x_initial, y_initial, d
+                pid[t] = trial_id[t]
         overrides += [(wi, "DX", dx), (wi, "DY", dy), (wi, "DP", dp)]
+        if fiducialize:
+            overrides += [(wi, "START_PID", pid), (wi, "END_PID", pid)]
     beam = Beam(coords, ids)
     if track_trials is not None:
         lost_pass, c, effort = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
-        return lost_pass, c[:, 0], c[:, 2], c[:, 5], np.full(n, -1), effort
-    with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every) as t:
-        t.load_ensemble(offsets, overrides)
-        res = t.track(beam)
-    order = np.argsort(res.ids)
-    c = res.coords[order]
-    return res.lost_pass[order], c[:, 0], c[:, 2], c[:, 5], res.lost_element[order], res.effort
+        lost_elem = np.full(per * n, -1)
+    else:
+        with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every,
+                     fiducial_particles=1 if fiducialize else 0) as t:
+            t.load_ensemble(offsets, overrides)
+            res = t.track(beam)
+        order = np.argsort(res.ids)
+        lost_pass, c, lost_elem, effort = res.lost_pass[order], res.coords[order], res.lost_element[order], res.effort
+    if fiducialize:
+        # the reference's fiducial run is one pass (momentumAperture.c:396-404)
+        if (lost_pass[0::2] == 0).any():
+            raise RuntimeError("Fiducial particle lost. Don't know what to do. (momentumAperture.c:400-404)")
+        lost_pass, c, lost_elem = lost_pass[1::2], c[1::2], lost_elem[1::2]
+    return lost_pass, c[:, 0], c[:, 2], c[:, 5], lost_elem, effort

@@ -220,16 +220,39 @@ def write_losses(path, result, lattice, p_central, step=1, mode="binary"):
     write_sdds(path, params, cols, mode, description="elegant_b200 loss output")
 
 
-def write_momentum_aperture(path, rows, step=1, mode="binary"):
-    """elegant's &momentum_aperture output, output_mode 0
-    (momentumAperture.c:189-212, :700-740), from
-    elegant_b200.momentum_aperture rows.  nuxLost/nuyLost are -1: tunes are
-    only found with forbid_resonance_crossing, which is not built."""
+def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0):
+    """elegant's &momentum_aperture output from elegant_b200.momentum_aperture
+    rows: output_mode 0, one row per element with both sides
+    (momentumAperture.c:189-212, :692-714), or output_mode 1, one row per
+    element and side, negative (direction -1) first (:141-160, :715-731).
+    nuxLost/nuyLost are -1: tunes are only found with
+    forbid_resonance_crossing, which is not built."""
     n = len(rows)
+    occ = [r["occurrence"] for r in rows] if rows and "occurrence" in rows[0] else _occurrences(rows)
+    if output_mode == 1:
+        sides = [(r, o, d, side) for r, o in zip(rows, occ) for d, side in ((-1, "negative"), (1, "positive"))]
+        cols = [("ElementName", "string", [r["name"] for r, _, _, _ in sides], {}),
+                ("s", "double", [r["s"] for r, _, _, _ in sides], {"units": "m"}),
+                ("ElementType", "string", [r["type"] for r, _, _, _ in sides], {}),
+                ("ElementOccurence", "long", [o for _, o, _, _ in sides], {}),
+                ("direction", "short", [d for _, _, d, _ in sides], {}),
+                ("deltaFound", "short", [int(r[sd]["found"]) for r, _, _, sd in sides], {}),
+                ("delta", "double", [r[sd]["delta"] for r, _, _, sd in sides], {"symbol": "$gd$R$blimit$n"}),
+                ("lostOnPass", "long", [r[sd]["lost_on_pass"] for r, _, _, sd in sides], {}),
+                ("sLost", "double", [r[sd]["s_lost"] for r, _, _, sd in sides], {"units": "m"}),
+                ("xLost", "double", [r[sd]["x_lost"] for r, _, _, sd in sides], {"units": "m"}),
+                ("yLost", "double", [r[sd]["y_lost"] for r, _, _, sd in sides], {"units": "m"}),
+                ("deltaLost", "double", [r[sd]["delta_when_lost"] for r, _, _, sd in sides], {}),
+                ("nuxLost", "double", [-1.0] * len(sides), {}),
+                ("nuyLost", "double", [-1.0] * len(sides), {})]
+        write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search")
+        return
+    if output_mode != 0:
+        raise ValueError("output_mode 2 is the reference's MPI-only mode (momentumAperture.c:185)")
     cols = [("ElementName", "string", [r["name"] for r in rows], {}),
             ("s", "double", [r["s"] for r in rows], {"units": "m"}),
             ("ElementType", "string", [r["type"] for r in rows], {}),
-            ("ElementOccurence", "long", _occurrences(rows), {})]
+            ("ElementOccurence", "long", occ, {})]
     for label, side in (("Positive", "positive"), ("Negative", "negative")):
         cols += [(f"delta{label}Found", "short", [int(r[side]["found"]) for r in rows], {}),
                  (f"delta{label}", "double", [r[side]["delta"] for r in rows],
@@ -269,17 +292,45 @@ def write_aperture(path, result, step=1, mode="binary"):
     elegant_b200.aperture.find_aperture_lines: the last survivor of each
     line, the clipped limits, the loss point, and the Area parameter."""
     lines = result["lines"]
-    cols = [("x", "double", [l["x"] for l in lines], {"units": "m"}),
-            ("y", "double", [l["y"] for l in lines], {"units": "m"}),
-            ("xClipped", "double", result["x_limit"], {"units": "m"}),
-            ("yClipped", "double", result["y_limit"], {"units": "m"}),
+    if result.get("slope"):
+        # slope mode's columns and parameter (aperture_search.c:32-39, :53-57)
+        head = [("xp", "double", [l["x"] for l in lines], {}),
+                ("yp", "double", [l["y"] for l in lines], {}),
+                ("xpClipped", "double", result["x_limit"], {}),
+                ("ypClipped", "double", result["y_limit"], {})]
+        area_attrs = {}
+    else:
+        head = [("x", "double", [l["x"] for l in lines], {"symbol": "x", "units": "m"}),
+                ("y", "double", [l["y"] for l in lines], {"symbol": "y", "units": "m"}),
+                ("xClipped", "double", result["x_limit"], {"symbol": "xClipped", "units": "m"}),
+                ("yClipped", "double", result["y_limit"], {"symbol": "yClipped", "units": "m"})]
+        area_attrs = {"units": "m$a2$n"}
+    cols = head + [
             ("sLost", "double", [l.get("s_lost", 0.0) for l in lines], {"units": "m"}),
             ("xLost", "double", [l["x_lost"] if l["x_lost"] is not None else 1.7976931348623157e308
                                  for l in lines], {"units": "m"}),
             ("yLost", "double", [l["y_lost"] if l["y_lost"] is not None else 1.7976931348623157e308
                                  for l in lines], {"units": "m"})]
-    write_sdds(path, [("Step", "long", step, {}), ("Area", "double", result["area"], {"units": "m$a2$n"})], cols,
+    write_sdds(path, [("Step", "long", step, {}), ("Area", "double", result["area"], area_attrs)], cols,
                mode, description="Dynamic aperture search")
+
+
+def write_aperture_mp(path, result, step=1, mode="binary"):
+    """elegant's &find_aperture output for mode = "many-particle"
+    (aperture_search.c:520-552) from one elegant_b200.aperture.find_aperture_mp
+    result: the boundary points (left scan, then right scan from the top) in
+    x and y; the other columns of the layout and the Area are zero there."""
+    pts = result["boundary"]
+    n = len(pts)
+    cols = [("x", "double", [p[0] for p in pts], {"symbol": "x", "units": "m"}),
+            ("y", "double", [p[1] for p in pts], {"symbol": "y", "units": "m"}),
+            ("xClipped", "double", [0.0] * n, {"symbol": "xClipped", "units": "m"}),
+            ("yClipped", "double", [0.0] * n, {"symbol": "yClipped", "units": "m"}),
+            ("sLost", "double", [0.0] * n, {"units": "m"}),
+            ("xLost", "double", [0.0] * n, {"units": "m"}),
+            ("yLost", "double", [0.0] * n, {"units": "m"})]
+    write_sdds(path, [("Step", "long", step, {}), ("Area", "double", 0.0, {"units": "m$a2$n"})], cols, mode,
+               description="Dynamic aperture search")
 
 
 def csr_wake_columns(page):

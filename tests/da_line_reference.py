@@ -9,8 +9,12 @@ from elegant_b200.aperture import line_factors
 
 
 def serial_line_search(oracle, lattice, p_central, n_passes, lines=11, xmax=0.1, ymax=0.1, nx=21, n_splits=0,
-                       split_fraction=0.5, full_plane=False):
+                       split_fraction=0.5, full_plane=False, slope=False, xpmax=0.0, ypmax=0.0):
+    """slope=True: the lines in (x', y') up to (xpmax, ypmax) (aperture_search.c:1029-1035, :1070-1076)."""
     fx, fy = line_factors(lines, full_plane)
+    if slope:
+        xmax, ymax = xpmax, ypmax
+    cx, cy = (1, 3) if slope else (0, 2)
     origin_stable = False
     out = []
     for line in range(lines):
@@ -33,8 +37,8 @@ def serial_line_search(oracle, lattice, p_central, n_passes, lines=11, xmax=0.1,
             for index in range(steps):
                 if index != 0 or split != 0 or not origin_stable:
                     c = np.zeros((1, 6))
-                    c[0, 0] = index * dx + x0
-                    c[0, 2] = index * dy + y0
+                    c[0, cx] = index * dx + x0
+                    c[0, cy] = index * dy + y0
                     rows, n_left, _ = oracle.track(lattice, c, np.array([1]), p_central, n_passes)[:3]
                     if n_left == 0:
                         lost_pass = int(rows[0, 7])

@@ -41,6 +41,30 @@ def test_batched_lines_equal_serial_walk(lines, splits, full):
     assert got["area"] > 0
 
 
+@pytest.mark.parametrize("lines,splits", [(7, 1), (3, 0)])
+def test_slope_mode_lines_equal_serial_walk(lines, splits, tmp_path):
+    """Slope mode (xmin == xmax): the lines in (x', y'), points offsetting the
+    slopes (aperture_search.c:1029-1035, :1070-1076); and its output file's
+    column set (:32-39), read with the independent SDDS reader."""
+    from elegant_b200.sdds import write_aperture
+    from sdds_protocol import SddsFile
+    lat = w.fodo_ring(rf=False)
+    ref = RefOracle("b2e")
+    kw = dict(lines=lines, nx=11, n_splits=splits, slope=True, xpmax=4e-3, ypmax=3e-3)
+    serial, origin = serial_line_search(ref, lat, P0, 30, **kw)
+    got = find_aperture_lines(lat, P0, 30, track_points=_oracle_points(ref), **kw)
+    assert got["origin_stable"] == origin and got["slope"]
+    for g, s in zip(got["lines"], serial):
+        assert (g["x"], g["y"], g["lost_pass"]) == s
+    assert any(g["lost_pass"] >= 0 for g in got["lines"])
+    write_aperture(str(tmp_path / "da.sdds"), got)
+    page = SddsFile(str(tmp_path / "da.sdds")).pages[0]
+    assert [k for k in page["columns"]][:4] == ["xp", "yp", "xpClipped", "ypClipped"]
+    assert list(page["columns"]["xp"]) == [g["x"] for g in got["lines"]]
+    with pytest.raises(ValueError):
+        find_aperture_lines(lat, P0, 30, lines=3, slope=True, xpmax=1e-3, ypmax=0.0)
+
+
 @pytest.mark.parametrize("full", [False, True])
 def test_trim_and_area_equal_elegant(full):
     lib = RefOracle("libm").lib

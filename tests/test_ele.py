@@ -123,3 +123,61 @@ def test_runner_tracks_a_chicane_job(tmp_path):
     alive = ref.lost_pass < 0
     assert np.array_equal(fin.pages[0]["columns"]["x"], ref.coords[alive, 0])
     assert np.array_equal(fin.pages[0]["columns"]["particleID"], ref.ids[alive])
+
+
+def test_find_aperture_checks():
+    """setup_aperture_search's input checks (aperture_search.c:118-170)."""
+    from elegant_b200.ele import FIND_APERTURE, _check_find_aperture
+    ok = dict(FIND_APERTURE, output="%s.aper", mode="n-line", n_lines=7)
+    assert _check_find_aperture(ok) == ("n-line", False, 7)
+    assert _check_find_aperture(dict(ok, xmin=0.0, xmax=0.0, xpmax=1e-3, ypmax=1e-3, ymin=0.0, ymax=0.0)) == \
+        ("n-line", True, 7)
+    assert _check_find_aperture(dict(ok, mode="five-line")) == ("five-line", False, 5)
+    bad = [(dict(ok, output=None), "no output"), (dict(ok, xmin=0.2), "xmin >= xmax"),
+           (dict(ok, xmin=0.0, xmax=0.0, xpmax=1e-3), "must not have xpmin==xpmax"),
+           (dict(ok, mode="three-line", xmin=0.0, xmax=0.0, xpmax=1e-3, ypmax=1e-3, ymax=0.0), "slope-based"),
+           (dict(ok, nx=2), "nx < 3"), (dict(ok, n_splits=1, split_fraction=1.5), "split_fraction"),
+           (dict(ok, optimization_mode=1, n_lines=2), "optimization"),
+           (dict(ok, mode="single-particle"), "single-particle")]
+    for fa, words in bad:
+        with pytest.raises(EleError, match=words):
+            _check_find_aperture(fa)
+
+
+@pytest.mark.gpu
+def test_runner_aperture_commands(tmp_path):
+    """&find_aperture (n-line, and slope mode with optimization_mode) and
+    &momentum_aperture (fiducialize, output_mode 1) from a run file: the
+    files written equal the direct calls."""
+    from elegant_b200 import workloads as w
+    from elegant_b200.aperture import find_aperture_lines
+    from elegant_b200.momentum_aperture import momentum_aperture
+    from sdds_protocol import SddsFile
+    lat = w.fodo_ring(rf=False)
+    lines = []
+    for e in lat.elements:
+        kv = ", ".join(f"{k}={v!r}" for k, v in e.params.items())
+        lines.append(f"{e.name}: {e.type}" + (f", {kv}" if kv else ""))
+    names = " ".join(e.name for e in lat.elements)
+    (tmp_path / "ring.lte").write_text("\n".join(lines) + f"\nRING: LINE=({names.replace(' ', ', ')})\n")
+    p0 = w.ring_p_central()
+    (tmp_path / "da.ele").write_text(
+        f'&run_setup lattice = ring.lte, use_beamline = RING, p_central = {p0!r} &end\n'
+        '&run_control n_passes = 40 &end\n'
+        '&find_aperture output = %s.aper, mode = "n-line", n_lines = 7, xmax = 0.03, ymax = 0.02, nx = 13,\n'
+        '   n_splits = 1 &end\n'
+        '&momentum_aperture output = %s.mmap, include_type_pattern = "KQUAD", process_elements = 2,\n'
+        '   delta_step_size = 0.0015, fiducialize = 1, output_mode = 1 &end\n'
+        '&find_aperture mode = "n-line", n_lines = 5, xmin = 0, xmax = 0, ymin = 0, ymax = 0, xpmax = 4e-3,\n'
+        '   ypmax = 3e-3, nx = 11, optimization_mode = 1 &end\n')
+    out = run_ele(str(tmp_path / "da.ele"))
+    aper = SddsFile(str(tmp_path / "da.aper")).pages[0]
+    want = find_aperture_lines(lat, p0, 40, lines=7, xmax=0.03, ymax=0.02, nx=13, n_splits=1)
+    assert list(aper["columns"]["x"]) == [l["x"] for l in want["lines"]]
+    assert aper["parameters"]["Area"] == want["area"]
+    mmap = SddsFile(str(tmp_path / "da.mmap")).pages[0]
+    rows, _ = momentum_aperture(lat, p0, 40, include_type_pattern="KQUAD", process_elements=2,
+                                delta_step_size=0.0015, fiducialize=True)
+    assert list(mmap["columns"]["delta"]) == [r[s]["delta"] for r in rows for s in ("negative", "positive")]
+    slope = find_aperture_lines(lat, p0, 40, lines=5, nx=11, slope=True, xpmax=4e-3, ypmax=3e-3)
+    assert out["steps"][-1]["area"] == slope["area"]

@@ -27,6 +27,23 @@ def test_momentum_aperture_matches_serial_scan(ref_b2e, passes):
             assert (got["delta"], got["delta_lost"], got["lost_on_pass"]) == s[side], (row["name"], label)
 
 
+@pytest.mark.parametrize("passes", [1, 40])
+def test_fiducialized_momentum_aperture_matches_serial_scan(ref_b2e, passes):
+    """fiducialize = 1 on the device (a fiducial row per instance,
+    fiducial_particles = 1, the wedge on the trial's ID) against the serial
+    scan with one fiducial particle's phase for all trials."""
+    from test_momentum_aperture import mid_rf_ring
+    lat = mid_rf_ring() if passes == 1 else w.fodo_ring()
+    kw = dict(include_type_pattern="K*", process_elements=4, delta_step_size=0.0015, splits=2)
+    serial = serial_momentum_aperture(ref_b2e, lat, P0, passes, fiducialize=True, **kw)
+    rows, effort = momentum_aperture(lat, P0, passes, fiducialize=True, **kw)
+    assert effort > 0 and len(rows) == 4
+    for row, s in zip(rows, serial):
+        for side, label in ((0, "negative"), (1, "positive")):
+            got = row[label]
+            assert (got["delta"], got["delta_lost"], got["lost_on_pass"]) == s[side], (row["name"], label)
+
+
 def test_malign_element_bit_exact(ref_b2e):
     """MALIGN (offset_beam) on one pass and on every pass, with a particle-ID
     window, through the ring: equal to the reference driver."""

@@ -39,3 +39,52 @@ def test_batched_search_matches_the_serial_scan():
             got = row[label]
             assert (got["delta"], got["delta_lost"], got["lost_on_pass"]) == s[side], (row["name"], label)
         assert row["negative"]["delta"] < 0 < row["positive"]["delta"]
+
+
+def mid_rf_ring():
+    """The ring with its cavity moved into the third cell and made short
+    (50 GHz, 20 MV): on a single pass a trial reaches it with its momentum
+    offset, so the RF phase reference decides the energy it gets."""
+    from elegant_b200 import Element, Lattice
+    base = w.fodo_ring()
+    rf = next(e for e in base.elements if e.type == "RFCA")
+    els = [e for e in base.elements if e.type != "RFCA"]
+    return Lattice(els[:24] + [Element("RF", "RFCA", dict(rf.params, FREQ=5e10, VOLT=2e7))] + els[24:])
+
+
+def test_fiducialized_search_matches_the_serial_scan():
+    """fiducialize = 1: one fiducial particle's RF phase for every trial
+    (momentumAperture.c:385-410, :560-566).  The batched form (a fiducial row
+    in every instance, the wedge on the trial's ID only) against the serial
+    scan on the reference build, on one pass of mid_rf_ring, where the phase
+    reference changes the answer; on 40 passes of the plain ring the wedge
+    fires on pass 1, after each trial has set its own phase on pass 0 on the
+    design orbit, and both settings agree."""
+    kw = dict(include_type_pattern="KQUAD", process_elements=2, delta_step_size=0.0015, splits=2)
+    ref = RefOracle("b2e")
+    for lat, passes in ((mid_rf_ring(), 1), (w.fodo_ring(), 40)):
+        serial = serial_momentum_aperture(ref, lat, P0, passes, fiducialize=True, **kw)
+        rows, _ = momentum_aperture(lat, P0, passes, track_trials=oracle_trials(ref), fiducialize=True, **kw)
+        for row, s in zip(rows, serial):
+            for side, label in ((0, "negative"), (1, "positive")):
+                got = row[label]
+                assert (got["delta"], got["delta_lost"], got["lost_on_pass"]) == s[side], (row["name"], label)
+        plain = serial_momentum_aperture(ref, lat, P0, passes, **kw)
+        assert (plain != serial) == (passes == 1)
+
+
+def test_output_mode_1_layout(tmp_path):
+    """One row per element and side, negative first (momentumAperture.c:141-160,
+    :715-731), read back with the independent SDDS reader."""
+    from elegant_b200.sdds import write_momentum_aperture
+    from sdds_protocol import SddsFile
+    side = {"delta": -0.01, "found": True, "lost_on_pass": 3, "x_lost": 1e-3, "y_lost": 0.0, "s_lost": 2.5,
+            "delta_when_lost": -0.011, "delta_lost": -0.0115}
+    rows = [{"name": "QF", "type": "KQUAD", "s": 1.3, "occurrence": 2, "negative": side,
+             "positive": dict(side, delta=0.02, found=False, lost_on_pass=-1)}]
+    write_momentum_aperture(str(tmp_path / "ma1.sdds"), rows, output_mode=1)
+    page = SddsFile(str(tmp_path / "ma1.sdds")).pages[0]
+    c = page["columns"]
+    assert list(c["direction"]) == [-1, 1] and list(c["deltaFound"]) == [1, 0]
+    assert list(c["delta"]) == [-0.01, 0.02] and list(c["ElementOccurence"]) == [2, 2]
+    assert list(c["lostOnPass"]) == [3, -1] and list(c["ElementName"]) == ["QF", "QF"]
