@@ -20,6 +20,10 @@ path are
   Twiss parameters always are, as generate_bunch does), symmetrize (each
   particle with its mirror images, so odd moments vanish),
   n_particles_per_bunch;
+- &sdds_beam (sdds_beam.nl): an elegant phase-space file (x, xp, y, yp, t,
+  p, optionally particleID), one page per step after n_tables_to_skip (the
+  first with reuse_bunch), sample_interval, p_lower/p_upper, converted as
+  elegant converts point particles (elegant_b200.sdds.beam_from_sdds);
 - &twiss_output with matched = 1 and &bunched_beam use_twiss_command_values
   = 1: the beam is matched to the periodic Twiss parameters of the line;
 - &track: runs n_steps steps of n_passes passes;
@@ -217,6 +221,12 @@ TRACK = {"center_on_orbit": 0, "center_momentum_also": 1, "offset_by_orbit": 0, 
 TWISS_OUTPUT = {"matched": 1, "filename": None, "output_at_each_step": 0, "statistics": 0, "radiation_integrals": 0,
                 "beta_x": 1.0, "alpha_x": 0.0, "eta_x": 0.0, "etap_x": 0.0, "beta_y": 1.0, "alpha_y": 0.0,
                 "eta_y": 0.0, "etap_y": 0.0, "concat_order": 0}
+SDDS_BEAM = {"input": None, "input_list": None, "input_type": "elegant", "selection_parameter": None,
+             "selection_string": None, "one_random_bunch": 0, "n_particles_per_ring": 0, "reuse_bunch": 0,
+             "prebunched": -1, "track_pages_separately": 0, "use_bunched_mode": 0, "fiducialization_bunch": 0,
+             "sample_interval": 1, "n_tables_to_skip": 0, "center_transversely": 0, "center_arrival_time": 0,
+             "reverse_t_sign": 0, "sample_fraction": 1.0, "p_lower": 0.0, "p_upper": 0.0,
+             "save_initial_coordinates": 1, "n_duplicates": 0, "duplicate_stagger": [0.0] * 6}
 FIND_APERTURE = {"output": None, "search_output": None, "boundary": None, "mode": "many-particle", "xmin": -0.1,
                  "xmax": 0.1, "xpmin": 0.0, "xpmax": 0.0, "ymin": 0.0, "ymax": 0.1, "ypmin": 0.0, "ypmax": 0.0,
                  "nx": 21, "n_splits": 0, "split_fraction": 0.5, "desired_resolution": 0.01, "ny": 11,
@@ -420,15 +430,15 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
     from .aperture import find_aperture_lines, find_aperture_mp
     from .momentum_aperture import momentum_aperture
     from .optics import periodic_twiss
-    from .sdds import (write_aperture, write_aperture_mp, write_csr_wake, write_losses, write_momentum_aperture,
-                       write_phase_space)
+    from .sdds import (beam_from_sdds, write_aperture, write_aperture_mp, write_csr_wake, write_losses,
+                       write_momentum_aperture, write_phase_space)
     from .track import Tracker
     mode_io = mode
     base = os.path.dirname(os.path.abspath(path))
     rootname = os.path.splitext(os.path.basename(path))[0]
     with open(path) as fh:
         cmds = parse_namelists(fh.read())
-    rs = rc = bb = tw = None
+    rs = rc = bb = tw = sb = None
     summary = {"steps": [], "files": []}
     lattice = None
     csr_outputs = {}
@@ -454,27 +464,46 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
             if tw["filename"]:
                 raise EleError("&twiss_output: filename (a Twiss output file) is not supported by the engine's runner")
         elif cmd == "bunched_beam":
+            sb = None
             bb = _command(fields, BUNCHED_BEAM, cmd,
                           {"n_particles_per_bunch", "emit_x", "emit_nx", "beta_x", "alpha_x", "eta_x", "etap_x",
                            "emit_y", "emit_ny", "beta_y", "alpha_y", "eta_y", "etap_y", "sigma_dp", "sigma_s",
                            "dp_s_coupling", "momentum_chirp", "one_random_bunch", "symmetrize",
                            "enforce_rms_values", "distribution_cutoff", "distribution_type", "centroid",
                            "use_twiss_command_values", "save_initial_coordinates"})
+        elif cmd == "sdds_beam":
+            sb = _command(fields, SDDS_BEAM, cmd, {"input", "input_type", "n_tables_to_skip", "sample_interval",
+                                                   "p_lower", "p_upper", "reuse_bunch", "save_initial_coordinates"})
+            if not sb["input"]:
+                raise EleError("&sdds_beam: no input file given")
+            if sb["input_type"] != "elegant":
+                raise EleError(f"&sdds_beam: input_type {sb['input_type']!r} is not supported by the engine's runner")
+            bb = None
         elif cmd == "track":
             _command(fields, TRACK, cmd, {"soft_failure", "interrupt_file"})
-            if rs is None or bb is None:
-                raise EleError("&track needs &run_setup and &bunched_beam before it")
+            if rs is None or (bb is None and sb is None):
+                raise EleError("&track needs &run_setup and &bunched_beam or &sdds_beam before it")
             rc = rc or dict(RUN_CONTROL)
             p0 = rs["p_central"] or rs["p_central_mev"] / ME_MEV
             twiss = None
-            if bb["use_twiss_command_values"]:
+            if bb is not None and bb["use_twiss_command_values"]:
                 if not tw or not tw["matched"]:
                     raise EleError("use_twiss_command_values needs &twiss_output with matched = 1")
                 twiss = periodic_twiss(lattice)
             outs = [f for f in (name(rs["final"]), name(rs["output"])) if f]
             losses = name(rs["losses"])
             for step in range(rc["n_steps"]):
-                if step == 0 or not bb["one_random_bunch"]:
+                if bb is None:
+                    # one page per step, after n_tables_to_skip; reuse_bunch keeps the first
+                    # (sdds_beam.c: new_sdds_beam)
+                    page = sb["n_tables_to_skip"] + (0 if sb["reuse_bunch"] else step)
+                    try:
+                        beam = beam_from_sdds(name(sb["input"]), p0, page=page,
+                                              sample_interval=sb["sample_interval"], p_lower=sb["p_lower"],
+                                              p_upper=sb["p_upper"])
+                    except ValueError as e:
+                        raise EleError(f"&sdds_beam: {e}") from e
+                elif step == 0 or not bb["one_random_bunch"]:
                     beam = bunched_beam(bb, p0, rs["random_number_seed"] + step, twiss)
                 with Tracker(lattice, p0, rc["n_passes"], device=device, default_order=rs["default_order"]) as t:
                     if csr_outputs:
@@ -484,14 +513,14 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                 summary["steps"].append({"step": step + 1, "survivors": res.n_left, "effort": res.effort})
                 charge = next((e.get("TOTAL") for e in lattice.elements if e.type == "CHARGE"), 0.0)
                 for f in outs:
-                    write_phase_space(f, res, p0, step=step + 1, charge=charge, mode=mode)
+                    write_phase_space(f, res, p0, step=step + 1, charge=charge, mode=mode, append=step > 0)
                 if losses:
-                    write_losses(losses, res, lattice, p0, step=step + 1, mode=mode)
+                    write_losses(losses, res, lattice, p0, step=step + 1, mode=mode, append=step > 0)
                 for el_name, fname in csr_outputs.items():
                     idx = set(lattice.index(el_name))
                     mine = [p for p in pages if p["element"] in idx]
                     if mine:
-                        write_csr_wake(name(fname), mine, mode=mode)
+                        write_csr_wake(name(fname), mine, mode=mode, append=step > 0)
                         summary["files"].append(name(fname))
             summary["files"] += outs + ([losses] if losses else [])
             summary["result"] = res
@@ -511,7 +540,7 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                     res, effort = find_aperture_mp(lattice, p0, rc["n_passes"], fa["xmin"], fa["xmax"], fa["ymin"],
                                                    fa["ymax"], fa["nx"], fa["ny"], device=device)
                     if out:
-                        write_aperture_mp(out, res[0], step=step + 1, mode=mode_io)
+                        write_aperture_mp(out, res[0], step=step + 1, mode=mode_io, append=step > 0)
                     summary["steps"].append({"step": step + 1, "boundary": res[0]["boundary"], "effort": effort})
                 else:
                     res = find_aperture_lines(lattice, p0, rc["n_passes"], lines=lines, xmax=fa["xmax"],
@@ -519,7 +548,7 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                                               split_fraction=fa["split_fraction"], full_plane=bool(fa["full_plane"]),
                                               device=device, slope=slope, xpmax=fa["xpmax"], ypmax=fa["ypmax"])
                     if out:
-                        write_aperture(out, res, step=step + 1, mode=mode_io)
+                        write_aperture(out, res, step=step + 1, mode=mode_io, append=step > 0)
                     summary["steps"].append({"step": step + 1, "area": res["area"], "lines": res["lines"]})
                 summary["result"] = res
             if out:
@@ -546,7 +575,8 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                                                      fiducialize=bool(ma["fiducialize"]), device=device, **kw)
                 except ValueError as e:
                     raise EleError(f"&momentum_aperture: {e}") from e
-                write_momentum_aperture(out, rows, step=step + 1, mode=mode_io, output_mode=ma["output_mode"])
+                write_momentum_aperture(out, rows, step=step + 1, mode=mode_io, output_mode=ma["output_mode"],
+                                        append=step > 0)
                 summary["steps"].append({"step": step + 1, "rows": rows, "effort": effort})
             summary["files"].append(out)
         elif cmd in INERT:

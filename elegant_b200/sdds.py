@@ -20,6 +20,7 @@ round trips), not arbitrary SDDS.
 """
 from __future__ import annotations
 
+import os
 import struct
 
 import numpy as np
@@ -33,19 +34,22 @@ def _quote(v: str) -> str:
     return '"' + v.replace('"', '\\"') + '"'
 
 
-def write_sdds(path, parameters, columns, mode="binary", description=None):
+def write_sdds(path, parameters, columns, mode="binary", description=None, append=False):
     """parameters: [(name, type, value, attrs)], columns: [(name, type,
     values, attrs)], types 'double' | 'long' | 'short' | 'string'; attrs:
     dict of units, symbol, description.  Binary data are written row by row
-    (SDDS's row-major layout), so string columns work too.  One page."""
+    (SDDS's row-major layout), so string columns work too.  One page;
+    append=True adds it to an existing file of the same layout (elegant's
+    one page per step)."""
     write_sdds_pages(path, [(p[0], p[1], p[3]) for p in parameters], [(c[0], c[1], c[3]) for c in columns],
-                     [([p[2] for p in parameters], [c[2] for c in columns])], mode, description)
+                     [([p[2] for p in parameters], [c[2] for c in columns])], mode, description, append)
 
 
-def write_sdds_pages(path, parameters, columns, pages, mode="binary", description=None):
+def write_sdds_pages(path, parameters, columns, pages, mode="binary", description=None, append=False):
     """Several pages of one layout: parameters [(name, type, attrs)], columns
     [(name, type, attrs)], pages [(parameter values, column arrays)] in the
-    definition orders."""
+    definition orders.  append=True and an existing file: the pages are
+    added after its last page (the caller keeps the layout the same)."""
     if mode not in ("binary", "ascii"):
         raise ValueError("mode must be 'binary' or 'ascii'")
     for c in columns:
@@ -69,8 +73,10 @@ def write_sdds_pages(path, parameters, columns, pages, mode="binary", descriptio
     for name, typ, a in columns:
         lines.append(f"&column name={name},{attrs_text(a)} type={typ}, &end")
     lines.append(f"&data mode={mode}, &end")
-    with open(path, "wb") as fh:
-        fh.write(("\n".join(lines) + "\n").encode())
+    adding = append and os.path.exists(path)
+    with open(path, "ab" if adding else "wb") as fh:
+        if not adding:
+            fh.write(("\n".join(lines) + "\n").encode())
         for values, cols in pages:
             n = len(cols[0]) if cols else 0
             if mode == "binary":
@@ -186,7 +192,7 @@ def read_sdds(path):
     return pv, out
 
 
-def write_phase_space(path, result, p_central, step=1, charge=0.0, mode="binary"):
+def write_phase_space(path, result, p_central, step=1, charge=0.0, mode="binary", append=False):
     """elegant's `final`/`output` file for the survivors of a TrackResult."""
     alive = result.lost_pass < 0
     c = result.coords[alive]
@@ -202,10 +208,10 @@ def write_phase_space(path, result, p_central, step=1, charge=0.0, mode="binary"
             ("y", "double", c[:, 2], {"units": "m"}), ("yp", "double", c[:, 3], {"symbol": "y'"}),
             ("t", "double", t, {"units": "s"}), ("p", "double", p, {"units": "m$be$nc"}),
             ("particleID", "long", result.ids[alive].astype(np.int64), {})]
-    write_sdds(path, params, cols, mode, description="elegant_b200 phase-space output")
+    write_sdds(path, params, cols, mode, description="elegant_b200 phase-space output", append=append)
 
 
-def write_losses(path, result, lattice, p_central, step=1, mode="binary"):
+def write_losses(path, result, lattice, p_central, step=1, mode="binary", append=False):
     """elegant's `losses` file for the lost particles of a TrackResult."""
     lost = result.lost_pass >= 0
     c = result.coords[lost]
@@ -217,10 +223,10 @@ def write_losses(path, result, lattice, p_central, step=1, mode="binary"):
             ("s", "double", s, {"units": "m"}), ("p", "double", p_central * (1 + c[:, 5]), {"units": "m$be$nc"}),
             ("particleID", "long", result.ids[lost].astype(np.int64), {}),
             ("Pass", "long", result.lost_pass[lost].astype(np.int64), {})]
-    write_sdds(path, params, cols, mode, description="elegant_b200 loss output")
+    write_sdds(path, params, cols, mode, description="elegant_b200 loss output", append=append)
 
 
-def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0):
+def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, append=False):
     """elegant's &momentum_aperture output from elegant_b200.momentum_aperture
     rows: output_mode 0, one row per element with both sides
     (momentumAperture.c:189-212, :692-714), or output_mode 1, one row per
@@ -245,7 +251,8 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0):
                 ("deltaLost", "double", [r[sd]["delta_when_lost"] for r, _, _, sd in sides], {}),
                 ("nuxLost", "double", [-1.0] * len(sides), {}),
                 ("nuyLost", "double", [-1.0] * len(sides), {})]
-        write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search")
+        write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
+                   append=append)
         return
     if output_mode != 0:
         raise ValueError("output_mode 2 is the reference's MPI-only mode (momentumAperture.c:185)")
@@ -264,7 +271,8 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0):
                  (f"deltaLost{label}", "double", [r[side]["delta_when_lost"] for r in rows], {}),
                  (f"nuxLost{label}", "double", [-1.0] * n, {}),
                  (f"nuyLost{label}", "double", [-1.0] * n, {})]
-    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search")
+    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
+                   append=append)
 
 
 def _occurrences(rows):
@@ -275,7 +283,7 @@ def _occurrences(rows):
     return out
 
 
-def write_frequency_map(path, rows, step=1, include_changes=False, mode="binary"):
+def write_frequency_map(path, rows, step=1, include_changes=False, mode="binary", append=False):
     """elegant's &frequency_map output (frequencyMap.c:30-60) from
     elegant_b200.frequency_map rows."""
     names = ["x", "y", "delta", "nux", "nuy", "s"]
@@ -283,10 +291,10 @@ def write_frequency_map(path, rows, step=1, include_changes=False, mode="binary"
         names += ["dnux", "dnuy", "dnu", "dx", "dy", "diffusion", "diffusionRate"]
     units = {"x": "m", "y": "m", "s": "m/pass", "dx": "m", "dy": "m"}
     cols = [(k, "double", [r[k] for r in rows], {"units": units[k]} if k in units else {}) for k in names]
-    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Frequency map analysis")
+    write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Frequency map analysis", append=append)
 
 
-def write_aperture(path, result, step=1, mode="binary"):
+def write_aperture(path, result, step=1, mode="binary", append=False):
     """elegant's &find_aperture output for the line modes
     (aperture_search.c:20-55, :1160-1215) from
     elegant_b200.aperture.find_aperture_lines: the last survivor of each
@@ -312,10 +320,10 @@ def write_aperture(path, result, step=1, mode="binary"):
             ("yLost", "double", [l["y_lost"] if l["y_lost"] is not None else 1.7976931348623157e308
                                  for l in lines], {"units": "m"})]
     write_sdds(path, [("Step", "long", step, {}), ("Area", "double", result["area"], area_attrs)], cols,
-               mode, description="Dynamic aperture search")
+               mode, description="Dynamic aperture search", append=append)
 
 
-def write_aperture_mp(path, result, step=1, mode="binary"):
+def write_aperture_mp(path, result, step=1, mode="binary", append=False):
     """elegant's &find_aperture output for mode = "many-particle"
     (aperture_search.c:520-552) from one elegant_b200.aperture.find_aperture_mp
     result: the boundary points (left scan, then right scan from the top) in
@@ -330,7 +338,7 @@ def write_aperture_mp(path, result, step=1, mode="binary"):
             ("xLost", "double", [0.0] * n, {"units": "m"}),
             ("yLost", "double", [0.0] * n, {"units": "m"})]
     write_sdds(path, [("Step", "long", step, {}), ("Area", "double", 0.0, {"units": "m$a2$n"})], cols, mode,
-               description="Dynamic aperture search")
+               description="Dynamic aperture search", append=append)
 
 
 def csr_wake_columns(page):
@@ -359,7 +367,7 @@ CSR_WAKE_COLUMNS = [("s", "double", {"units": "m"}), ("LinearDensity", "double",
                     ("DeltaGammaT2", "double", {})]
 
 
-def write_csr_wake(path, pages, mode="binary"):
+def write_csr_wake(path, pages, mode="binary", append=False):
     """CSRCSBEND's OUTPUT_FILE (csbend.c:2227-2249 layout, one page per kick,
     :2762-2806) for the page records of one element, in the order given (a
     bunch train: bunch by bunch, as elegant writes consecutive bunches).
@@ -371,4 +379,246 @@ def write_csr_wake(path, pages, mode="binary"):
         values = ["elegant_b200", -1, pg["kick"], pg["p_central"], pg["angle"], pg["slippage"],
                   pg["ct_upper"] - pg["ct_lower"], pg["dct"], pg["ds_kick"], 0.0]
         out.append((values, [cols[c[0]] for c in CSR_WAKE_COLUMNS]))
-    write_sdds_pages(path, CSR_WAKE_PARAMETERS, CSR_WAKE_COLUMNS, out, mode, description="CSR wake output")
+    write_sdds_pages(path, CSR_WAKE_PARAMETERS, CSR_WAKE_COLUMNS, out, mode, description="CSR wake output",
+                     append=append)
+
+
+# ---------------------------------------------------------------- input ----
+# SDDS type -> numpy dtype code (the byte order is added per file)
+_NP = {"double": "f8", "float": "f4", "long": "i4", "ulong": "u4", "long64": "i8", "ulong64": "u8", "short": "i2",
+       "ushort": "u2", "char": "S1"}
+
+
+def _fields(body: str) -> dict:
+    """key=value pairs of one namelist body; values may be double-quoted
+    (with backslash escapes) and are separated by commas or white space."""
+    out, i, n = {}, 0, len(body)
+    while i < n:
+        if body[i] in " \t\r\n,":
+            i += 1
+            continue
+        eq = body.find("=", i)
+        if eq < 0:
+            break
+        key = body[i:eq].strip().lower()
+        i = eq + 1
+        while i < n and body[i] in " \t":
+            i += 1
+        if i < n and body[i] == '"':
+            j, buf = i + 1, []
+            while j < n and body[j] != '"':
+                if body[j] == "\\" and j + 1 < n:
+                    j += 1
+                buf.append(body[j])
+                j += 1
+            out[key] = "".join(buf)
+            i = j + 1
+        else:
+            j = i
+            while j < n and body[j] not in " \t\r\n,":
+                j += 1
+            out[key] = body[i:j]
+            i = j
+    return out
+
+
+def _ascii_tokens(text: str):
+    """White-space separated tokens; double-quoted ones kept whole."""
+    toks, i, n = [], 0, len(text)
+    while i < n:
+        c = text[i]
+        if c.isspace():
+            i += 1
+        elif c == '"':
+            j, buf = i + 1, []
+            while j < n and text[j] != '"':
+                if text[j] == "\\" and j + 1 < n:
+                    j += 1
+                buf.append(text[j])
+                j += 1
+            toks.append("".join(buf))
+            i = j + 1
+        else:
+            j = i
+            while j < n and not text[j].isspace():
+                j += 1
+            toks.append(text[i:j])
+            i = j
+    return toks
+
+
+def _scalar(typ, tok):
+    if typ == "string":
+        return tok
+    if typ == "char":
+        return tok[:1]
+    return float(tok) if typ in ("double", "float") else int(tok)
+
+
+def read_sdds_pages(path):
+    """Every page of an SDDS file as a list of (parameters, columns) dicts,
+    numeric columns as numpy arrays (native byte order), string columns as
+    lists; fixed_value parameters included.  Handles protocol versions 1-5,
+    binary data of either byte order (the "!# big-endian" meta-comment),
+    row- or column-major binary pages, 64-bit row counts, and ASCII data with
+    or without row counts.  Arrays (&array) are not supported."""
+    with open(path, "rb") as fh:
+        raw = fh.read()
+    nl = raw.index(b"\n")
+    first = raw[:nl].decode("latin-1").strip()
+    if not (first.startswith("SDDS") and first[4:].isdigit()):
+        raise ValueError(f"{path}: not an SDDS file")
+    pos, order, pending = nl + 1, "<", ""
+    params, cols, data = [], [], None
+    while data is None:
+        nl = raw.find(b"\n", pos)
+        if nl < 0:
+            raise ValueError(f"{path}: header without &data")
+        line = raw[pos:nl].decode("latin-1").strip()
+        pos = nl + 1
+        if line.startswith("!"):
+            order = ">" if "big-endian" in line else ("<" if "little-endian" in line else order)
+            continue
+        pending = f"{pending} {line}".strip()
+        while "&end" in pending:
+            k = pending.index("&end")
+            cmd, pending = pending[:k].strip(), pending[k + 4:].strip()
+            name, _, body = cmd.partition(" ")
+            f = _fields(body)
+            if name == "&parameter":
+                params.append(f)
+            elif name == "&column":
+                cols.append(f)
+            elif name == "&array":
+                raise ValueError(f"{path}: SDDS arrays are not supported")
+            elif name == "&data":
+                data = f
+                break
+    mode = data.get("mode", "ascii").lower()
+    for f in params + cols:
+        f["type"] = f.get("type", "double").lower()
+    stored = [p for p in params if "fixed_value" not in p]
+    fixed = {p["name"]: _scalar(p["type"], p["fixed_value"]) for p in params if "fixed_value" in p}
+    pages = []
+    if mode == "binary":
+        col_major = data.get("column_major_order", "0") not in ("0", "")
+        numeric = all(c["type"] != "string" for c in cols)
+        while pos + 4 <= len(raw):
+            n = int(np.frombuffer(raw, order + "i4", 1, pos)[0])
+            pos += 4
+            if n == -2 ** 31:
+                n = int(np.frombuffer(raw, order + "i8", 1, pos)[0])
+                pos += 8
+            pv = dict(fixed)
+            for p in stored:
+                pv[p["name"]], pos = _binary_value(raw, pos, order, p["type"])
+            cv = {}
+            if col_major:
+                for c in cols:
+                    if c["type"] == "string":
+                        vals = []
+                        for _ in range(n):
+                            v, pos = _binary_value(raw, pos, order, "string")
+                            vals.append(v)
+                        cv[c["name"]] = vals
+                    else:
+                        dt = np.dtype(order + _NP[c["type"]])
+                        cv[c["name"]] = np.frombuffer(raw, dt, n, pos).astype(dt.newbyteorder("="))
+                        pos += n * dt.itemsize
+            elif numeric:
+                dt = np.dtype([(c["name"], order + _NP[c["type"]]) for c in cols])
+                rows = np.frombuffer(raw, dt, n, pos)
+                pos += n * dt.itemsize
+                for c in cols:
+                    cv[c["name"]] = rows[c["name"]].astype(rows[c["name"]].dtype.newbyteorder("="))
+            else:
+                vals = {c["name"]: [] for c in cols}
+                for _ in range(n):
+                    for c in cols:
+                        v, pos = _binary_value(raw, pos, order, c["type"])
+                        vals[c["name"]].append(v)
+                cv = {c["name"]: (vals[c["name"]] if c["type"] == "string" else
+                                  np.array(vals[c["name"]], dtype=_NP[c["type"]])) for c in cols}
+            pages.append((pv, cv))
+    else:
+        lines = raw[pos:].decode("latin-1").split("\n")
+        skip = int(data.get("additional_header_lines", "0") or 0)
+        li = skip
+        no_counts = data.get("no_row_counts", "0") not in ("0", "")
+        while True:
+            while li < len(lines) and (not lines[li].strip() or lines[li].lstrip().startswith("!")):
+                li += 1
+            if li >= len(lines):
+                break
+            pv = dict(fixed)
+            for p in stored:
+                t = lines[li].strip()
+                li += 1
+                pv[p["name"]] = _scalar(p["type"], t[1:-1] if p["type"] == "string" and t.startswith('"') else t)
+            if no_counts:
+                body = []
+                while li < len(lines) and lines[li].strip():
+                    body.append(lines[li])
+                    li += 1
+            else:
+                while li < len(lines) and not lines[li].strip():
+                    li += 1
+                n = int(lines[li].split()[0])
+                li += 1
+                body = lines[li:li + n * int(data.get("lines_per_row", "1") or 1)]
+                li += len(body)
+            toks = _ascii_tokens(" ".join(body))
+            k = len(cols)
+            n = len(toks) // k if k else 0
+            cv = {}
+            for j, c in enumerate(cols):
+                vals = [_scalar(c["type"], t) for t in toks[j::k][:n]]
+                cv[c["name"]] = vals if c["type"] == "string" else np.array(vals, dtype=_NP[c["type"]])
+            pages.append((pv, cv))
+    return pages
+
+
+def _binary_value(raw, pos, order, typ):
+    if typ == "string":
+        k = int(np.frombuffer(raw, order + "i4", 1, pos)[0])
+        return raw[pos + 4:pos + 4 + k].decode("latin-1"), pos + 4 + k
+    dt = np.dtype(order + _NP[typ])
+    v = np.frombuffer(raw, dt, 1, pos)[0]
+    return (v.decode("latin-1") if typ == "char" else v.item()), pos + dt.itemsize
+
+
+def beam_from_sdds(path, p_central, page=0, sample_interval=1, p_lower=0.0, p_upper=0.0, t_offset=0.0):
+    """The particles of one page of an elegant phase-space file (columns x,
+    xp, y, yp, t, p and optionally particleID), as &sdds_beam reads point
+    particles (sdds_beam.c:408-440): s = (t_offset + t) c p / gamma with
+    gamma = sqrt(p^2 + 1), delta = (p - p_central) / p_central, every
+    sample_interval-th row, rows with p outside [p_lower, p_upper] dropped
+    when p_lower is set; IDs from particleID, else the row numbers 1, 2, ...
+    of the page."""
+    from .beam import Beam
+    pages = read_sdds_pages(path)
+    if page >= len(pages):
+        raise ValueError(f"{path}: page {page} requested, {len(pages)} in the file")
+    _, c = pages[page]
+    for name in ("x", "xp", "y", "yp", "t", "p"):
+        if name not in c:
+            raise ValueError(f"{path}: column {name} missing (sdds_beam.c:840-870)")
+    n = len(c["x"])
+    rows = np.arange(0, n, max(1, int(sample_interval)))
+    p = np.asarray(c["p"], dtype=np.float64)[rows]
+    keep = np.ones(rows.size, dtype=bool)
+    if p_lower:
+        keep = ~((p_lower > p) | (p_upper < p))
+    rows, p = rows[keep], p[keep]
+    gamma = np.sqrt(p * p + 1)
+    coords = np.empty((rows.size, 6))
+    for j, name in enumerate(("x", "xp", "y", "yp")):
+        coords[:, j] = np.asarray(c[name], dtype=np.float64)[rows]
+    coords[:, 4] = (t_offset + np.asarray(c["t"], dtype=np.float64)[rows]) * C_MKS * p / gamma
+    coords[:, 5] = (p - p_central) / p_central
+    if not np.isfinite(coords).all():
+        raise ValueError(f"{path}: NaN or Infinity detected in initial particle data (sdds_beam.c:441-448)")
+    # without a particleID column the reader numbers the rows as it reads
+    # them, before sampling (sdds_beam.c:1005-1007)
+    ids = np.asarray(c["particleID"], dtype=np.int64)[rows] if "particleID" in c else (rows + 1).astype(np.int64)
+    return Beam(coords, ids)

@@ -181,3 +181,48 @@ def test_runner_aperture_commands(tmp_path):
     assert list(mmap["columns"]["delta"]) == [r[s]["delta"] for r in rows for s in ("negative", "positive")]
     slope = find_aperture_lines(lat, p0, 40, lines=5, nx=11, slope=True, xpmax=4e-3, ypmax=3e-3)
     assert out["steps"][-1]["area"] == slope["area"]
+
+
+def test_runner_sdds_beam_checks(tmp_path):
+    (tmp_path / "a.lte").write_text("D: DRIF, L=1\nL1: LINE=(D)\n")
+    cases = [('&sdds_beam input = b.sdds, input_type = "spiffe" &end', "spiffe"),
+             ("&sdds_beam input = b.sdds, center_arrival_time = 1 &end", "center_arrival_time"),
+             ("&sdds_beam &end", "no input")]
+    for text, word in cases:
+        (tmp_path / "job.ele").write_text("&run_setup lattice = a.lte, p_central = 100 &end\n" + text + "\n&track &end")
+        with pytest.raises(EleError, match=word):
+            run_ele(str(tmp_path / "job.ele"))
+
+
+@pytest.mark.gpu
+def test_runner_tracks_an_sdds_beam(tmp_path):
+    """&sdds_beam + &track: a phase-space file written by the engine (t, p
+    columns), read back page by page (two steps, two pages), tracked; the
+    final file equals tracking beam_from_sdds directly."""
+    from elegant_b200 import Tracker, workloads as w
+    from elegant_b200.sdds import beam_from_sdds, write_phase_space
+    from elegant_b200.track import TrackResult
+    from sdds_protocol import SddsFile
+    lat = w.fodo_ring(rf=False)
+    p0 = w.ring_p_central()
+    lines = [f"{e.name}: {e.type}, " + ", ".join(f"{k}={v!r}" for k, v in e.params.items()) for e in lat.elements]
+    (tmp_path / "ring.lte").write_text("\n".join(lines) + "\nRING: LINE=(" + ", ".join(e.name for e in lat.elements)
+                                       + ")\n")
+    path = str(tmp_path / "in.sdds")
+    for step in (1, 2):
+        b = w.ring_beam(3000, seed=60 + step)
+        res = TrackResult(b.coords, b.ids, np.full(b.n, -1, np.int32), np.full(b.n, -1, np.int32), b.n, 0.0)
+        write_phase_space(path, res, p0, step=step, append=step > 1)
+    (tmp_path / "job.ele").write_text(
+        f"&run_setup lattice = ring.lte, use_beamline = RING, p_central = {p0!r}, final = %s.fin &end\n"
+        "&run_control n_passes = 20, n_steps = 2 &end\n"
+        "&sdds_beam input = in.sdds &end\n&track &end\n")
+    run_ele(str(tmp_path / "job.ele"))
+    fin = SddsFile(str(tmp_path / "job.fin"))
+    assert len(fin.pages) == 2
+    for k in range(2):
+        beam = beam_from_sdds(path, p0, page=k)
+        with Tracker(lat, p0, 20) as t:
+            ref = t.track(beam)
+        alive = ref.lost_pass < 0
+        assert np.array_equal(fin.pages[k]["columns"]["x"], ref.coords[alive, 0])

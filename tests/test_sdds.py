@@ -115,3 +115,72 @@ def test_caller_outputs_round_trip(tmp_path, mode):
     write_aperture(p, ap, mode=mode)
     pv, c = read_sdds(p)
     assert pv["Area"] == 4e-5 and list(c["xClipped"]) == [-0.01, 0.0] and c["xLost"][1] > 1e300
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="needs the reference tree")
+def test_product_reader_agrees_with_the_protocol_reader_on_reference_files():
+    """elegant_b200.sdds.read_sdds_pages (the engine's input reader) against
+    the independent protocol reader on every SDDS file in the reference tree
+    (ASCII and binary, both byte orders, fixed-value parameters, float,
+    short and string columns): every page, column and parameter equal, float
+    columns compared at their declared 32-bit width."""
+    from elegant_b200.sdds import read_sdds_pages
+    files = sorted(glob.glob(os.path.join(REFERENCE, "**", "*.sdds"), recursive=True))
+    assert len(files) > 50
+    checked = 0
+    for f in files:
+        mine = read_sdds_pages(f)
+        ref = SddsFile(f)
+        assert len(mine) == len(ref.pages), f
+        for (pv, cv), page in zip(mine, ref.pages):
+            for k, v in page["columns"].items():
+                got = cv[k]
+                if isinstance(got, list):
+                    assert list(v) == got, (f, k)
+                else:
+                    assert np.array_equal(np.asarray(v, dtype=got.dtype), got, equal_nan=True), (f, k)
+            for k, v in page["parameters"].items():
+                assert v == pv[k] or (v != v and pv[k] != pv[k]), (f, k)
+        checked += 1
+    assert checked == len(files)
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="needs the reference tree")
+def test_beam_from_an_elegant_phase_space_file():
+    """&sdds_beam's point-particle conversion (sdds_beam.c:408-440) of the
+    reference's own big-endian beam file: s = t c p / gamma, delta =
+    (p - p0)/p0, IDs by row, every sample_interval-th row, the p window."""
+    from elegant_b200.sdds import beam_from_sdds
+    f = os.path.join(REFERENCE, "doc/examples/full457MeV/beamFile.sdds")
+    page = SddsFile(f).pages[0]["columns"]
+    p = np.asarray(page["p"])
+    p0 = float(np.median(p))
+    b = beam_from_sdds(f, p0)
+    assert b.n == len(p) and np.array_equal(b.ids, np.arange(1, b.n + 1))
+    assert np.array_equal(b.coords[:, 0], np.asarray(page["x"]))
+    assert np.array_equal(b.coords[:, 4], np.asarray(page["t"]) * 2.99792458e8 * p / np.sqrt(p * p + 1))
+    assert np.array_equal(b.coords[:, 5], (p - p0) / p0)
+    half = beam_from_sdds(f, p0, sample_interval=2, p_lower=p0 * 0.999, p_upper=p0 * 1.001)
+    sel = np.arange(0, len(p), 2)
+    sel = sel[(p[sel] >= p0 * 0.999) & (p[sel] <= p0 * 1.001)]
+    assert np.array_equal(half.coords[:, 1], np.asarray(page["xp"])[sel])
+    assert np.array_equal(half.ids, sel + 1)
+
+
+@pytest.mark.parametrize("mode", ["binary", "ascii"])
+def test_pages_appended_per_step(tmp_path, mode):
+    """One page per step, as elegant writes its final/losses files: the second
+    step appended to the first, read back by the protocol reader and by the
+    engine's own input reader."""
+    from elegant_b200.sdds import read_sdds_pages
+    path = str(tmp_path / f"steps.{mode}")
+    for step, seed in ((1, 5), (2, 6)):
+        b = w.ring_beam(50 + step, seed=seed)
+        res = TrackResult(b.coords, b.ids, np.full(b.n, -1, np.int32), np.full(b.n, -1, np.int32), b.n, 0.0)
+        write_phase_space(path, res, 1000.0, step=step, mode=mode, append=step > 1)
+    f = SddsFile(path)
+    assert [p["parameters"]["Step"] for p in f.pages] == [1, 2]
+    assert [len(p["columns"]["x"]) for p in f.pages] == [51, 52]
+    mine = read_sdds_pages(path)
+    assert [pv["Step"] for pv, _ in mine] == [1, 2]
+    assert np.array_equal(mine[1][1]["x"], f.pages[1]["columns"]["x"])
