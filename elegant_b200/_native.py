@@ -24,7 +24,7 @@ ERRORS = {
 
 CSR_PAGE_HEADER = 12  # B2E_CSR_PAGE_HEADER
 # element type codes (include/elegant_b200.h)
-DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT, MALIGN = range(1, 13)
+DRIF, EDRIFT, KQUAD, KSEXT, CSBEND, RFCA, MAXAMP, MARK, CHARGE, CSRCSBEND, CSRDRIFT, MALIGN, WATCH = range(1, 14)
 MAX_PARAMS = 40
 RING_VARIANTS = 17
 
@@ -107,6 +107,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "b2e_csr_surrogate_stats": (c_int, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), vp, i64,
                                             ctypes.POINTER(i64)]),
         "b2e_tbt": (c_int, [vp, vp, i64, ctypes.POINTER(i64)]),
+        "b2e_set_watch": (c_int, [vp, i64]),
+        "b2e_watch_records": (c_int, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(i64), vp, vp,
+                                      ctypes.c_int32]),
+        "b2e_watch_data": (c_int, [vp, ctypes.c_int32, vp]),
         "b2e_tbt_tunes": (c_int, [vp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, vp]),
         "b2e_naff": (c_int, [vp, i64, ctypes.c_int32, vp, vp, vp, vp]),
         "b2e_element_defaults": (c_int, [ctypes.c_int32, vp]),

@@ -131,6 +131,10 @@ static int engine_type(long type, const b2e_param_map **map) {
   case T_MALIGN:
     *map = map_malign;
     return B2E_MALIGN;
+  case T_WATCH:
+    /* a disabled WATCH only (see b2e_adapter_track): a marker */
+    *map = map_mark;
+    return B2E_MARK;
   default:
     return 0;
   }
@@ -216,6 +220,12 @@ long b2e_adapter_track(double **coord, long np, ELEMENT_LIST *first, double P_ce
       say(why, why_len, "%s: element type %s is not supported by the engine", eptr->name, entity_name[eptr->type]);
       return -1;
     }
+    /* elegant writes WATCH output itself (dump_watch_particles, at each
+     * pass): a line with an active WATCH stays with elegant */
+    if (eptr->type == T_WATCH && !((WATCH *)eptr->p_elem)->disable) {
+      say(why, why_len, "%s: WATCH output is written by elegant%s", eptr->name, "");
+      return -1;
+    }
     if (eptr->type == T_RFCA) {
       long ref = ((RFCA *)eptr->p_elem)->phase_reference;
       for (j = 0; j < n_rf && ref; j++)
@@ -233,6 +243,8 @@ long b2e_adapter_track(double **coord, long np, ELEMENT_LIST *first, double P_ce
     const int code = engine_type(eptr->type, &map);
     b2e_element_defaults(code, &el[i]);
     strncpy(el[i].name, eptr->name, sizeof(el[i].name) - 1);
+    if (eptr->type == T_WATCH)
+      continue; /* disabled: its other parameters shape no output */
     if (fill_parameters(&el[i], eptr, map, why, why_len)) {
       free(el);
       return -1;

@@ -113,6 +113,14 @@ struct b2e_ctx {
   DevBuf<int64_t> d_cmp_ids;
   DevBuf<int32_t> d_cmp_lost_pass, d_cmp_lost_elem;
   DevBuf<int> d_alive_inst;
+  /* WATCH recording (b2e_set_watch): [records][7][watch_rows] of the last call */
+  int64_t watch_max_bytes = 0;
+  DevBuf<double> d_watch;
+  DevBuf<int64_t> d_watch_rec0;
+  DevBuf<int32_t> d_watch_first;
+  std::vector<int32_t> watch_rec_elem, watch_rec_pass;
+  int64_t watch_rows = 0;
+  bool watch_on = false;
 };
 
 static int fail(b2e_ctx *ctx, int code, const char *fmt, ...) {
@@ -269,7 +277,7 @@ static bool any_radiation(const std::vector<DevElem> &elems) {
 }
 
 extern "C" int b2e_element_defaults(int32_t type, b2e_element *element) {
-  if (!element || type < B2E_DRIF || type > B2E_MALIGN)
+  if (!element || type < B2E_DRIF || type > B2E_WATCH)
     return B2E_ERR_ARG;
   element->type = type;
   element->reserved = 0;
@@ -330,6 +338,9 @@ extern "C" int b2e_load_ensemble(b2e_ctx *ctx, int32_t n_instances, const int64_
     if (t == B2E_CSRCSBEND || t == B2E_CSRDRIFT)
       return fail(ctx, B2E_ERR_LATTICE,
                   "b2e_load_ensemble: CSR elements are shared by all bunches and take no per-instance overrides");
+    if (t == B2E_WATCH)
+      return fail(ctx, B2E_ERR_LATTICE,
+                  "b2e_load_ensemble: WATCH elements record every instance alike and take no per-instance overrides");
   }
   ctx->n_inst = n_instances;
   ctx->inst_offsets.assign(offsets, offsets + n_instances + 1);
@@ -431,6 +442,7 @@ static int autotune_ring(b2e_ctx *ctx, const RingLaunch &Lreal, bool staged, siz
   CUDA_TRY(ctx, ctx->d_scratch.ensure((size_t)n * 6));
   CUDA_TRY(ctx, ctx->d_scratch_loss.ensure((size_t)n * 2));
   RingLaunch L = Lreal;
+  L.watch = nullptr; /* the trials record nothing */
   double *cols[6] = {Lreal.P.x, Lreal.P.xp, Lreal.P.y, Lreal.P.yp, Lreal.P.s, Lreal.P.dp};
   L.P.x = ctx->d_scratch.ptr;
   L.P.xp = L.P.x + n;
@@ -541,6 +553,10 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.ids = ctx->use_ext ? nullptr : ctx->d_ids.ptr;
   L.isr_seed = ctx->opt.isr_seed;
   L.sr_limit = ctx->opt.sr_gaussian_limit == 0 ? 3.0 : ctx->opt.sr_gaussian_limit;
+  L.watch = ctx->watch_on ? ctx->d_watch.ptr : nullptr;
+  L.watch_rows = ctx->watch_rows;
+  L.watch_rec0 = ctx->d_watch_rec0.ptr;
+  L.watch_first = ctx->d_watch_first.ptr;
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
@@ -624,6 +640,47 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_tbt.ptr, 0xff, sizeof(double) * (size_t)ctx->tbt_records * 4 * ctx->n,
                                   ctx->stream)); /* NaN until written */
     CUDA_TRY(ctx, launch_tbt_start(particle_view(ctx), ctx->n, ctx->d_tbt.ptr, ctx->stream));
+  }
+  /* WATCH records of this call: for each recording WATCH, its passes in
+   * [p0, npass), record numbers in WATCH order then pass order */
+  ctx->watch_rec_elem.clear();
+  ctx->watch_rec_pass.clear();
+  ctx->watch_on = false;
+  if (ctx->watch_max_bytes > 0 && !ctx->lat.watch_elements.empty()) {
+    const size_t nw = ctx->lat.watch_elements.size();
+    std::vector<int64_t> rec0(nw);
+    std::vector<int32_t> first(nw, -1);
+    for (size_t k = 0; k < nw; k++) {
+      const DevElem &d = ctx->lat.elems[ctx->lat.watch_elements[k]];
+      const long start = (long)d.c[WA_START], end = (long)d.c[WA_END], step = (long)d.c[WA_INTERVAL];
+      long f = start >= p0 ? start : start + ((p0 - start + step - 1) / step) * step;
+      rec0[k] = (int64_t)ctx->watch_rec_pass.size();
+      for (long q = f; q < npass && (end < 0 || q <= end); q += step) {
+        if (first[k] < 0)
+          first[k] = (int32_t)q;
+        ctx->watch_rec_elem.push_back(ctx->lat.watch_elements[k]);
+        ctx->watch_rec_pass.push_back((int32_t)q);
+      }
+    }
+    const size_t records = ctx->watch_rec_pass.size();
+    const double need = (double)records * 7 * (double)ctx->n * sizeof(double);
+    if (need > (double)ctx->watch_max_bytes)
+      return fail(ctx, B2E_ERR_ARG, "WATCH output of this call needs %.0f bytes of device memory; b2e_set_watch allows "
+                  "%lld", need, (long long)ctx->watch_max_bytes);
+    if (records > 0 && ctx->n > 0) {
+      ctx->watch_rows = ctx->n;
+      CUDA_TRY(ctx, ctx->d_watch.ensure(records * 7 * (size_t)ctx->n));
+      CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_watch.ptr, 0xff, sizeof(double) * records * 7 * (size_t)ctx->n,
+                                    ctx->stream)); /* NaN until a live particle writes */
+      CUDA_TRY(ctx, ctx->d_watch_rec0.ensure(nw));
+      CUDA_TRY(ctx, ctx->d_watch_first.ensure(nw));
+      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_watch_rec0.ptr, rec0.data(), sizeof(int64_t) * nw, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_watch_first.ptr, first.data(), sizeof(int32_t) * nw,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+      CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream)); /* the host vectors go out of scope */
+      ctx->watch_on = true;
+    }
   }
   if (record) {
     if (!ctx->lat.csr_elements.empty())
@@ -884,6 +941,39 @@ extern "C" int b2e_ensemble_history(b2e_ctx *ctx, int64_t *survivors, double *cx
 
 extern "C" int64_t b2e_history_passes(const b2e_ctx *ctx) {
   return ctx && ctx->n_inst > 0 ? (int64_t)(ctx->history.size() / ((size_t)ctx->n_inst * 5)) : -1;
+}
+
+extern "C" int b2e_set_watch(b2e_ctx *ctx, int64_t max_bytes) {
+  if (!ctx || max_bytes < 0)
+    return B2E_ERR_ARG;
+  ctx->watch_max_bytes = max_bytes;
+  return B2E_OK;
+}
+
+extern "C" int b2e_watch_records(b2e_ctx *ctx, int32_t *n_records, int64_t *rows, int32_t *elements, int32_t *passes,
+                                 int32_t capacity) {
+  if (!ctx || !n_records || !rows)
+    return B2E_ERR_ARG;
+  const int32_t nr = ctx->watch_on ? (int32_t)ctx->watch_rec_pass.size() : 0;
+  *n_records = nr;
+  *rows = ctx->watch_on ? ctx->watch_rows : 0;
+  for (int32_t r = 0; r < nr && r < capacity; r++) {
+    if (elements)
+      elements[r] = ctx->watch_rec_elem[r];
+    if (passes)
+      passes[r] = ctx->watch_rec_pass[r];
+  }
+  return B2E_OK;
+}
+
+extern "C" int b2e_watch_data(b2e_ctx *ctx, int32_t record, double *host_out) {
+  if (!ctx || !host_out || !ctx->watch_on || record < 0 || record >= (int32_t)ctx->watch_rec_pass.size())
+    return B2E_ERR_ARG;
+  const size_t len = 7 * (size_t)ctx->watch_rows;
+  CUDA_TRY(ctx, cudaMemcpyAsync(host_out, ctx->d_watch.ptr + (size_t)record * len, sizeof(double) * len,
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return B2E_OK;
 }
 
 extern "C" int b2e_tbt(b2e_ctx *ctx, double *host_out, int64_t capacity, int64_t *written) {

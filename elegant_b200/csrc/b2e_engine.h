@@ -34,7 +34,8 @@ enum {
   K_MAXAMP,
   K_CSRCSBEND, /* collective: handled by the CSR driver, never in the ring kernel */
   K_CSRDRIFT,
-  K_MALIGN     /* offset_beam on one pass (or every pass) */
+  K_MALIGN,    /* offset_beam on one pass (or every pass) */
+  K_WATCH      /* coordinate-mode WATCH: records the live particles on its passes */
 };
 
 /* Flags */
@@ -142,6 +143,12 @@ typedef struct {
 #define RF_MATRIX 10    /* 1: matrix method (nonzero L, N_KICKS <= 0) */
 #define RF_DTLIGHT 11   /* RF_LENGTH / c */
 #define RF_DRIFT_ONLY 12 /* VOLT = 0: an exact drift over L (nothing for L = 0) */
+
+/* WATCH constant slots */
+#define WA_START 0      /* first pass recorded */
+#define WA_END 1        /* last pass recorded, -1: no end */
+#define WA_INTERVAL 2
+#define WA_ORDINAL 3    /* index among the lattice's recording WATCH elements */
 
 /* MALIGN constant slots */
 #define MA_DX 0

@@ -37,6 +37,15 @@ struct RingLaunch {
   double *tbt;
   int tbt_pass0, tbt_records;
   int64_t tbt_rows;
+  /* WATCH records [record][7][watch_rows]: x, x', y, y', s, delta and the
+   * particle ID (a double; NaN where no live particle wrote); WATCH ordinal k
+   * writes record watch_rec0[k] + (pass - watch_first[k]) / interval on the
+   * passes it records from watch_first[k] on; null: WATCH elements are
+   * markers */
+  double *watch;
+  int64_t watch_rows;
+  const int64_t *watch_rec0;
+  const int32_t *watch_first;
 };
 
 /* variant 1..B2E_RING_VARIANTS selects the occupancy target and the barrier

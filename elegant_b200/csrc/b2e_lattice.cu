@@ -142,6 +142,19 @@ void element_defaults(int type, double *p) {
     p[B2E_MALIGN_START_PID] = -1;
     p[B2E_MALIGN_END_PID] = -1;
     break;
+  case B2E_WATCH:
+    p[B2E_WATCH_END_PASS] = -1;         /* track_data.c:881-895 */
+    p[B2E_WATCH_INTERVAL] = 1;
+    p[B2E_WATCH_FRACTION] = 1;
+    p[B2E_WATCH_START_PID] = -1;
+    p[B2E_WATCH_END_PID] = -1;
+    p[B2E_WATCH_SPARSE_INTERVAL] = 1;
+    p[B2E_WATCH_X_DATA] = 1;
+    p[B2E_WATCH_Y_DATA] = 1;
+    p[B2E_WATCH_LONGIT_DATA] = 1;
+    p[B2E_WATCH_FLUSH_INTERVAL] = 100;
+    p[B2E_WATCH_REFERENCE_FREQUENCY] = -1;
+    break;
   default:
     break;
   }
@@ -692,6 +705,35 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
       d.c[MA_START_PID] = (double)s_pid;
       d.c[MA_END_PID] = (double)e_pid;
       d.c[MA_C] = kC_MKS;
+      break;
+    }
+    case B2E_WATCH: {
+      /* a WATCH never changes the particles; NO_APERTURE (track_data.c:3941) */
+      d.flags |= EF_NO_APERTURE;
+      const long s_pid = (long)p[B2E_WATCH_START_PID], e_pid = (long)p[B2E_WATCH_END_PID];
+      if (p[B2E_WATCH_DISABLE] != 0) {
+        d.kind = K_NONE;
+        break;
+      }
+      if (p[B2E_WATCH_MODE] != 0)
+        err = "WATCH modes other than coordinates are not supported by this engine";
+      else if (p[B2E_WATCH_FRACTION] != 1)
+        err = "WATCH FRACTION other than 1 is not supported by this engine";
+      else if (p[B2E_WATCH_SPARSE_INTERVAL] > 1)
+        err = "WATCH SPARSE_INTERVAL other than 1 is not supported by this engine";
+      else if ((long)p[B2E_WATCH_INTERVAL] < 1)
+        err = "WATCH INTERVAL must be at least 1";
+      /* dump_watch_particles' checks (sdds_support.c:755-758) */
+      else if (s_pid >= 0 && s_pid > e_pid)
+        err = "WATCH startPID>endPID";
+      else if ((e_pid >= 0 && s_pid < 0) || (s_pid >= 0 && e_pid < 0))
+        err = "WATCH invalid startPID, endPID";
+      d.kind = K_WATCH;
+      d.c[WA_START] = (double)(long)p[B2E_WATCH_START_PASS];
+      d.c[WA_END] = (double)(long)p[B2E_WATCH_END_PASS];
+      d.c[WA_INTERVAL] = (double)(long)p[B2E_WATCH_INTERVAL];
+      d.c[WA_ORDINAL] = (double)out.watch_elements.size();
+      out.watch_elements.push_back(i);
       break;
     }
     default:

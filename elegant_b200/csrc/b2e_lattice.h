@@ -27,6 +27,7 @@ struct CompiledLattice {
   std::vector<DevAperture> aps;
   std::vector<int> rf_elements;    /* element indices of RFCA, in lattice order */
   std::vector<int> csr_elements;   /* CSRCSBEND / CSRDRIFT indices */
+  std::vector<int> watch_elements; /* recording WATCH indices, in lattice order (WA_ORDINAL) */
   int n_rf = 0;
   double total_length = 0;
 };

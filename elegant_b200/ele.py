@@ -42,7 +42,9 @@ drawn from numpy's PCG64 seeded with random_number_seed: the same
 distribution, not the same particles.
 
 CSRCSBEND OUTPUT_FILE (a string parameter of the .lte) is written through
-the engine's page records (Tracker.set_csr_pages, sdds.write_csr_wake).
+the engine's page records (Tracker.set_csr_pages, sdds.write_csr_wake);
+coordinate-mode WATCH elements (FILENAME) through the engine's WATCH records
+(Tracker.set_watch, sdds.write_watch), one page per recorded pass.
 """
 from __future__ import annotations
 
@@ -239,6 +241,8 @@ MOMENTUM_APERTURE = {"output": None, "x_initial": 1e-5, "y_initial": 1e-5, "delt
                      "include_name_pattern": None, "include_type_pattern": None, "fiducialize": 0, "verbosity": 1,
                      "soft_failure": 0, "output_mode": 0, "forbid_resonance_crossing": 0,
                      "allow_watch_file_output": 0}
+# device memory the runner lets WATCH recording take per step
+WATCH_BUDGET_BYTES = 8 << 30
 # commands that change nothing the tracking path computes
 INERT = {"global_settings", "print_dictionary", "semaphores", "stop", "subprocess", "run_rpnexpr"}
 LINE_MODE_LINES = {"one-line": 1, "two-line": 2, "three-line": 3, "five-line": 5, "seven-line": 7, "nine-line": 9,
@@ -431,7 +435,7 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
     from .momentum_aperture import momentum_aperture
     from .optics import periodic_twiss
     from .sdds import (beam_from_sdds, write_aperture, write_aperture_mp, write_csr_wake, write_losses,
-                       write_momentum_aperture, write_phase_space)
+                       write_momentum_aperture, write_phase_space, write_watch)
     from .track import Tracker
     mode_io = mode
     base = os.path.dirname(os.path.abspath(path))
@@ -492,6 +496,14 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                 twiss = periodic_twiss(lattice)
             outs = [f for f in (name(rs["final"]), name(rs["output"])) if f]
             losses = name(rs["losses"])
+            watches = [(i, e) for i, e in enumerate(lattice.elements) if e.type == "WATCH" and not e.get("DISABLE")]
+            for _, e in watches:
+                if not e.strings.get("FILENAME"):
+                    raise EleError(f"WATCH {e.name}: no FILENAME")
+                if e.get("AUTO_REFERENCE") or e.get("INDEX_OFFSET"):
+                    raise EleError(f"WATCH {e.name}: AUTO_REFERENCE and INDEX_OFFSET are not supported by the "
+                                   "engine's runner")
+            z_end = np.cumsum([e.length for e in lattice.elements])
             for step in range(rc["n_steps"]):
                 if bb is None:
                     # one page per step, after n_tables_to_skip; reuse_bunch keeps the first
@@ -508,14 +520,24 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                 with Tracker(lattice, p0, rc["n_passes"], device=device, default_order=rs["default_order"]) as t:
                     if csr_outputs:
                         t.set_csr_pages(True)
+                    if watches:
+                        t.set_watch(WATCH_BUDGET_BYTES)
                     res = t.track(beam)
                     pages = t.csr_pages() if csr_outputs else []
+                    records = t.watch() if watches else []
                 summary["steps"].append({"step": step + 1, "survivors": res.n_left, "effort": res.effort})
                 charge = next((e.get("TOTAL") for e in lattice.elements if e.type == "CHARGE"), 0.0)
                 for f in outs:
                     write_phase_space(f, res, p0, step=step + 1, charge=charge, mode=mode, append=step > 0)
                 if losses:
                     write_losses(losses, res, lattice, p0, step=step + 1, mode=mode, append=step > 0)
+                macro = charge / beam.n if beam.n else 0.0
+                for i, e in watches:
+                    write_watch(name(e.strings["FILENAME"]), [r for r in records if r["element"] == i], p0,
+                                float(z_end[i]), lattice.total_length, step=step + 1, charge=macro, watch=e.params,
+                                mode=mode, append=step > 0)
+                    if step == 0:
+                        summary["files"].append(name(e.strings["FILENAME"]))
                 for el_name, fname in csr_outputs.items():
                     idx = set(lattice.index(el_name))
                     mine = [p for p in pages if p["element"] in idx]

@@ -30,10 +30,12 @@ TYPES = {
     "DRIF": nat.DRIF, "DRIFT": nat.DRIF, "EDRIFT": nat.EDRIFT, "KQUAD": nat.KQUAD, "KSEXT": nat.KSEXT,
     "CSBEND": nat.CSBEND, "RFCA": nat.RFCA, "MAXAMP": nat.MAXAMP, "MARK": nat.MARK, "MARKER": nat.MARK,
     "CHARGE": nat.CHARGE, "CSRCSBEND": nat.CSRCSBEND, "CSRDRIFT": nat.CSRDRIFT, "MALIGN": nat.MALIGN,
+    "WATCH": nat.WATCH,
 }
 TYPE_NAMES = {nat.DRIF: "DRIF", nat.EDRIFT: "EDRIFT", nat.KQUAD: "KQUAD", nat.KSEXT: "KSEXT",
               nat.CSBEND: "CSBEND", nat.RFCA: "RFCA", nat.MAXAMP: "MAXAMP", nat.MARK: "MARK",
-              nat.CHARGE: "CHARGE", nat.CSRCSBEND: "CSRCSBEND", nat.CSRDRIFT: "CSRDRIFT", nat.MALIGN: "MALIGN"}
+              nat.CHARGE: "CHARGE", nat.CSRCSBEND: "CSRCSBEND", nat.CSRDRIFT: "CSRDRIFT", nat.MALIGN: "MALIGN",
+              nat.WATCH: "WATCH"}
 
 _KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, "N_SLICES": 8,
           "INTEGRATION_ORDER": 9, "SYNCH_RAD": 12, "ISR": 13, "ISR1PART": 14}
@@ -61,7 +63,17 @@ SLOTS = {
     nat.CSRDRIFT: {"L": 0, "N_KICKS": 1, "DZ": 2, "CSR": 3, "USE_STUPAKOV": 4},
     nat.MALIGN: {"DXP": 0, "DYP": 1, "DX": 2, "DY": 3, "DZ": 4, "DT": 5, "DP": 6, "DE": 7, "ON_PASS": 8,
                  "START_PID": 9, "END_PID": 10},
+    # WATCH: slots 0-8 are the engine's (include/elegant_b200.h); 9-17 only
+    # shape the output file (elegant_b200.sdds.write_watch)
+    nat.WATCH: {"START_PASS": 0, "END_PASS": 1, "INTERVAL": 2, "DISABLE": 3, "MODE": 4, "FRACTION": 5,
+                "START_PID": 6, "END_PID": 7, "SPARSE_INTERVAL": 8, "X_DATA": 9, "Y_DATA": 10, "LONGIT_DATA": 11,
+                "EXCLUDE_SLOPES": 12, "FLUSH_INTERVAL": 13, "USE_DISCONNECT": 14, "INDEX_OFFSET": 15,
+                "REFERENCE_FREQUENCY": 16, "AUTO_REFERENCE": 17},
 }
+# string-valued parameters, kept beside the numeric slots
+STRING_PARAMS = {nat.WATCH: ("FILENAME", "LABEL")}
+# WATCH MODE strings (matched by prefix, as elegant's match_string) -> B2E_WATCH_MODE codes
+WATCH_MODES = (("coord", 0), ("param", 1), ("centroid", 2), ("fft", 3))
 
 # defaults from the reference's parameter tables (only nonzero ones listed)
 DEFAULTS = {
@@ -77,6 +89,8 @@ DEFAULTS = {
     nat.MAXAMP: {"EXPONENT": 2},
     nat.CSRDRIFT: {"N_KICKS": 1, "CSR": 1},
     nat.MALIGN: {"ON_PASS": -1, "START_PID": -1, "END_PID": -1},
+    nat.WATCH: {"END_PASS": -1, "INTERVAL": 1, "FRACTION": 1, "START_PID": -1, "END_PID": -1, "SPARSE_INTERVAL": 1,
+                "X_DATA": 1, "Y_DATA": 1, "LONGIT_DATA": 1, "FLUSH_INTERVAL": 100, "REFERENCE_FREQUENCY": -1},
 }
 
 LENGTH_TYPES = {nat.DRIF, nat.EDRIFT, nat.KQUAD, nat.KSEXT, nat.CSBEND, nat.RFCA, nat.CSRCSBEND, nat.CSRDRIFT}
@@ -89,6 +103,7 @@ class Element:
     name: str
     type: str
     params: dict = field(default_factory=dict)
+    strings: dict = field(default_factory=dict)
 
     def __post_init__(self):
         self.type = self.type.upper()
@@ -97,14 +112,25 @@ class Element:
         code = TYPES[self.type]
         self.type = TYPE_NAMES[code]
         clean = {}
+        strings = {k.upper(): str(v) for k, v in self.strings.items()}
         for k, v in self.params.items():
             k = k.upper()
+            if k in STRING_PARAMS.get(code, ()):
+                strings[k] = str(v).strip('"')
+                continue
+            if k == "MODE" and code == nat.WATCH and isinstance(v, str):
+                m = v.strip('"').strip().lower()
+                codes = [c for prefix, c in WATCH_MODES if m and (prefix.startswith(m) or m.startswith(prefix))]
+                if not codes:
+                    raise LatticeError(f"WATCH {self.name}: unknown MODE {v!r}")
+                v = codes[0]
             if k not in SLOTS[code]:
                 raise LatticeError(f"parameter {k} of {self.type} {self.name} is not supported by the engine")
             if k == "N_KICKS" and code in (nat.CSBEND, nat.CSRCSBEND):
                 k = "N_SLICES"  # alias sharing storage (track_data.c:1925, :2006)
             clean[k] = float(v)
         self.params = clean
+        self.strings = strings
 
     @property
     def code(self) -> int:
@@ -129,7 +155,10 @@ class Element:
         return p
 
     def to_lte(self) -> str:
-        items = [f"{k}={v!r}" for k, v in self.params.items()]
+        names = {c: n for n, c in (("coordinates", 0), ("parameters", 1), ("centroids", 2), ("fft", 3))}
+        items = [f'{k}="{names.get(int(v), "coordinates")}"' if (k == "MODE" and self.code == nat.WATCH)
+                 else f"{k}={v!r}" for k, v in self.params.items()]
+        items += [f'{k}="{v}"' for k, v in self.strings.items()]
         return f"{self.name}: {self.type}" + ("".join(", " + i for i in items))
 
 
@@ -261,10 +290,14 @@ def parse_lte(text: str, use: str | None = None, outputs: dict | None = None) ->
                     raise LatticeError(f"OUTPUT_FILE of {name}: pass outputs= to collect it (elegant_b200.ele)")
                 outputs[name] = v.strip().strip('"')
                 continue
+            if etype == "WATCH" and k.strip().upper() in ("FILENAME", "LABEL", "MODE"):
+                params[k.strip().upper()] = v.strip().strip('"')
+                continue
             params[k.strip().upper()] = _value(v)
         if etype in elements:
             base = elements[etype]
             merged = dict(base.params)
+            merged.update(base.strings)
             merged.update(params)
             elements[name] = Element(name, base.type, merged)
         else:

@@ -20,6 +20,7 @@ round trips), not arbitrary SDDS.
 """
 from __future__ import annotations
 
+import math
 import os
 import struct
 
@@ -209,6 +210,83 @@ def write_phase_space(path, result, p_central, step=1, charge=0.0, mode="binary"
             ("t", "double", t, {"units": "s"}), ("p", "double", p, {"units": "m$be$nc"}),
             ("particleID", "long", result.ids[alive].astype(np.int64), {})]
     write_sdds(path, params, cols, mode, description="elegant_b200 phase-space output", append=append)
+
+
+def watch_pass_central_times(passes, z, length, p_central, reference_frequency=-1.0):
+    """PassCentralTime of a WATCH on each of `passes` (ascending) of one step,
+    as dump_watch_particles carries it (sdds_support.c:714-736): z beta^-1/c on
+    pass 0, then one revolution time per pass added with Kahan's compensated
+    sum, each rounded to the RF bucket when reference_frequency > 0."""
+    root = math.sqrt(p_central * p_central + 1)
+    t0 = z * root / (C_MKS * (p_central + 1e-32))
+    err = 0.0
+    last, out = 0, []
+    for q in passes:
+        for _ in range(q - last):
+            dt = length * root / (C_MKS * (p_central + 1e-32))
+            if reference_frequency > 0:
+                dt = float(int(dt * reference_frequency + 0.5)) / reference_frequency
+            y = dt + err
+            total = t0 + y
+            err = y - (total - t0)
+            t0 = total
+        last = q
+        out.append(t0)
+    return out
+
+
+def write_watch(path, records, p_central, z, length, step=1, charge=0.0, watch=None, mode="binary", append=False):
+    """A coordinate-mode WATCH file (SDDS_WatchPointSetup, sdds_support.c:403-520;
+    dump_watch_particles :703-860), one page per recorded pass, from the
+    records of one WATCH (elegant_b200.track.Tracker.watch entries of that
+    element, in pass order): columns x, xp, y, yp (X_DATA, Y_DATA; slopes
+    left out with EXCLUDE_SLOPES), t = s/(c beta), p = P0 (1 + delta) and
+    dt = t - PassCentralTime (LONGIT_DATA), particleID; parameters Step,
+    pCentral, Charge (macro charge x particles), Particles, IDSlotsPerBunch,
+    SampledCharge, SampledParticles, Pass, PassLength, PassCentralTime, s.
+    watch: the element's numeric parameters (X_DATA, START_PID, ...).
+    Rows are the particles by ascending ID (elegant keeps its array order);
+    START_PID/END_PID select rows."""
+    w = dict(watch or {})
+    get = lambda k, d: w.get(k, d)
+    x_data, y_data, longit = get("X_DATA", 1), get("Y_DATA", 1), get("LONGIT_DATA", 1)
+    slopes = not get("EXCLUDE_SLOPES", 0)
+    s_pid, e_pid = get("START_PID", -1), get("END_PID", -1)
+    cols_def = []
+    if x_data:
+        cols_def += [("x", "double", {"units": "m"})] + ([("xp", "double", {})] if slopes else [])
+    if y_data:
+        cols_def += [("y", "double", {"units": "m"})] + ([("yp", "double", {})] if slopes else [])
+    if longit:
+        cols_def += [("t", "double", {"units": "s"}), ("p", "double", {"units": "m$be$nc"}),
+                     ("dt", "double", {"units": "s"})]
+    cols_def += [("particleID", "long", {})]
+    params_def = [("Step", "long", {"description": "Simulation step"}),
+                  ("pCentral", "double", {"symbol": "p$bcen$n", "units": "m$be$nc",
+                                          "description": "Reference beta*gamma"}),
+                  ("Charge", "double", {"units": "C", "description": "Bunch charge before sampling"}),
+                  ("Particles", "long", {"description": "Number of particles before sampling"}),
+                  ("IDSlotsPerBunch", "long", {"description": "Number of particle ID slots reserved to a bunch"}),
+                  ("SampledCharge", "double", {"units": "C", "description": "Sampled charge"}),
+                  ("SampledParticles", "long", {"description": "Sampled number of particles"}),
+                  ("Pass", "long", {}), ("PassLength", "double", {"units": "m"}),
+                  ("PassCentralTime", "double", {"units": "s"}), ("s", "double", {"units": "m"})]
+    times = watch_pass_central_times([r["pass"] for r in records], z, length, p_central,
+                                     get("REFERENCE_FREQUENCY", -1.0))
+    pages = []
+    for r, t0 in zip(records, times):
+        c, ids = r["coords"], r["ids"]
+        if s_pid >= 0 or e_pid >= 0:
+            keep = (ids >= s_pid) & (ids <= e_pid)
+            c, ids = c[keep], ids[keep]
+        p = p_central * (1 + c[:, 5])
+        t = c[:, 4] / (C_MKS * p / np.sqrt(p * p + 1))
+        by = {"x": c[:, 0], "xp": c[:, 1], "y": c[:, 2], "yp": c[:, 3], "t": t, "p": p, "dt": t - t0,
+              "particleID": ids.astype(np.int64)}
+        n = len(ids)
+        pages.append(([step, p_central, charge * n, n, 0, charge * n, n, r["pass"], length, t0, z],
+                      [by[name] for name, _, _ in cols_def]))
+    write_sdds_pages(path, params_def, cols_def, pages, mode, description="watch-point phase space", append=append)
 
 
 def write_losses(path, result, lattice, p_central, step=1, mode="binary", append=False):

@@ -204,6 +204,33 @@ class Tracker:
         self._check(self.lib.b2e_tbt(self._ctx, out.ctypes.data, n.value, ctypes.byref(n)))
         return out.reshape(-1, 4, self._n)
 
+    def set_watch(self, max_bytes: int):
+        """Record WATCH elements (coordinate mode) in the following calls,
+        within max_bytes of device memory (b2e_set_watch); 0 turns it off."""
+        self._check(self.lib.b2e_set_watch(self._ctx, int(max_bytes)))
+
+    def watch(self) -> list:
+        """The WATCH records of the last call, in WATCH (lattice) order then
+        pass order: dicts with element (index), pass, ids and coords (n, 6)
+        of the particles alive at the element, by ascending ID."""
+        nr = ctypes.c_int32()
+        rows = ctypes.c_int64()
+        self._check(self.lib.b2e_watch_records(self._ctx, ctypes.byref(nr), ctypes.byref(rows), None, None, 0))
+        elems = np.empty(nr.value, dtype=np.int32)
+        passes = np.empty(nr.value, dtype=np.int32)
+        self._check(self.lib.b2e_watch_records(self._ctx, ctypes.byref(nr), ctypes.byref(rows), elems.ctypes.data,
+                                               passes.ctypes.data, nr.value))
+        out = []
+        buf = np.empty((7, rows.value), dtype=np.float64)
+        for r in range(nr.value):
+            self._check(self.lib.b2e_watch_data(self._ctx, r, buf.ctypes.data))
+            live = ~np.isnan(buf[6])
+            ids = buf[6, live].astype(np.int64)
+            order = np.argsort(ids, kind="stable")
+            out.append({"element": int(elems[r]), "pass": int(passes[r]), "ids": ids[order],
+                        "coords": buf[:6, live].T[order].copy()})
+        return out
+
     def tbt_tunes(self, first_record: int, n_records: int) -> dict:
         """Tunes (NAFF + half-plane from the x/x' phases) of every row over
         records [first_record, first_record + n_records); -1 where the

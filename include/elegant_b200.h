@@ -64,6 +64,7 @@ extern "C" {
 #define B2E_CSRCSBEND 10
 #define B2E_CSRDRIFT 11
 #define B2E_MALIGN 12
+#define B2E_WATCH 13
 
 #define B2E_MAX_PARAMS 40
 #define B2E_RING_VARIANTS 17
@@ -173,6 +174,32 @@ extern "C" {
 #define B2E_MALIGN_ON_PASS 8   /* default -1 */
 #define B2E_MALIGN_START_PID 9 /* default -1: every particle */
 #define B2E_MALIGN_END_PID 10  /* default -1 */
+/* WATCH (watch_param, track_data.c:880-900), coordinate mode: after every
+ * INTERVAL-th pass from START_PASS to END_PASS (inclusive, -1: no end) the
+ * coordinates of the particles alive at the element are recorded when
+ * b2e_set_watch enables it (the element never changes them).  DISABLE = 1
+ * makes it a marker.  The engine rejects the other modes, FRACTION != 1 and
+ * SPARSE_INTERVAL != 1; START_PID/END_PID select rows of the output, not
+ * the recording. */
+#define B2E_WATCH_START_PASS 0
+#define B2E_WATCH_END_PASS 1      /* default -1 */
+#define B2E_WATCH_INTERVAL 2      /* default 1 */
+#define B2E_WATCH_DISABLE 3
+#define B2E_WATCH_MODE 4          /* 0 = "coordinates", 1 = "parameter", 2 = "centroid", 3 = "fft" */
+#define B2E_WATCH_FRACTION 5      /* default 1 */
+#define B2E_WATCH_START_PID 6     /* default -1 */
+#define B2E_WATCH_END_PID 7       /* default -1 */
+#define B2E_WATCH_SPARSE_INTERVAL 8 /* default 1 */
+/* shape only the output file, which the caller writes (the engine ignores them) */
+#define B2E_WATCH_X_DATA 9        /* default 1 */
+#define B2E_WATCH_Y_DATA 10       /* default 1 */
+#define B2E_WATCH_LONGIT_DATA 11  /* default 1 */
+#define B2E_WATCH_EXCLUDE_SLOPES 12
+#define B2E_WATCH_FLUSH_INTERVAL 13 /* default 100 */
+#define B2E_WATCH_USE_DISCONNECT 14
+#define B2E_WATCH_INDEX_OFFSET 15
+#define B2E_WATCH_REFERENCE_FREQUENCY 16 /* default -1 */
+#define B2E_WATCH_AUTO_REFERENCE 17
 
 typedef struct {
   int32_t type;             /* B2E_DRIF ... */
@@ -308,6 +335,22 @@ int64_t b2e_history_passes(const b2e_ctx *ctx);
  * Replaces the per-turn bookkeeping of computeTunesFromTracking
  * (twiss.cc:3885-3925). */
 int b2e_tbt(b2e_ctx *ctx, double *host_out, int64_t capacity, int64_t *written);
+
+/* WATCH coordinate recording (dump_watch_particles, sdds_support.c:703-860,
+ * called at do_tracking.c:1585-1635).  b2e_set_watch(max_bytes > 0) turns it
+ * on: each b2e_track / b2e_track_host call then keeps, for every WATCH
+ * element (lattice order) and every pass of the call it records, one record
+ * of 7 columns x rows (the context's particle rows): x, x', y, y', s, delta
+ * and the particle ID as a double, NaN in the rows of particles not alive
+ * at the element.  A call whose records would exceed max_bytes fails with
+ * B2E_ERR_ARG before tracking.  b2e_watch_records gives the number of
+ * records, the row count and each record's element index and pass (up to
+ * capacity entries); b2e_watch_data copies one record ([7][rows]) to host
+ * memory.  Not with per-instance overrides of WATCH elements. */
+int b2e_set_watch(b2e_ctx *ctx, int64_t max_bytes);
+int b2e_watch_records(b2e_ctx *ctx, int32_t *n_records, int64_t *rows, int32_t *elements, int32_t *passes,
+                      int32_t capacity);
+int b2e_watch_data(b2e_ctx *ctx, int32_t record, double *host_out);
 
 /* Tunes of every particle from records [first_record, first_record +
  * n_records) of the turn-by-turn data, as computeTunesFromTracking does

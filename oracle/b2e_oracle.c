@@ -1948,7 +1948,7 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
     for (k = 0; k < n_el && nToTrack; k++) {
       const b2e_element *e = &el[k];
       const double *p = e->p;
-      int no_aperture = (e->type == B2E_MARK || e->type == B2E_CHARGE);
+      int no_aperture = (e->type == B2E_MARK || e->type == B2E_CHARGE || e->type == B2E_WATCH);
       double L = 0;
       switch (e->type) {
       case B2E_DRIF:

@@ -46,7 +46,7 @@ static const B2E_REF_TYPE b2e_ref_types[] = {
   {"CSRCSBEND", T_CSRCSBEND}, {"CSRDRIFT", T_CSRDRIFT}, {"MALIGN", T_MALIGN},
   /* built but not tracked by the restated loop: lets the adapter's tests
    * hand it an element type outside the engine's set */
-  {"SEXT", T_SEXT}, {NULL, 0}};
+  {"SEXT", T_SEXT}, {"WATCH", T_WATCH}, {NULL, 0}};
 
 /* offset_beam (do_tracking.c:3243-3300) restated: do_tracking.c is not part
  * of the compiled subset */
@@ -251,6 +251,38 @@ double b2e_ref_last_fiducial_t0(void) { return last_fiducial_t0; }
 static double *history_out = NULL;
 static long history_passes = 0;
 
+/* WATCH capture (test infrastructure): at each coordinate-mode WATCH on the
+ * passes dump_watch_particles writes (sdds_support.c:738-741), the rows it is
+ * handed (the particles alive at the element, do_tracking.c:1626-1629) are
+ * copied as (element index, pass, particleID, x, xp, y, yp, s, delta). */
+static double *watch_buf = NULL;
+static long watch_cap = 0, watch_count = 0;
+
+void b2e_ref_set_watch(double *buffer, long capacity_rows) {
+  watch_buf = buffer;
+  watch_cap = capacity_rows;
+  watch_count = 0;
+}
+
+long b2e_ref_watch_rows(void) { return watch_count; }
+
+static void capture_watch(const WATCH *w, long elem_index, long pass, double **coord, long n) {
+  long i, j;
+  if (!watch_buf || w->disable)
+    return;
+  if (!(pass >= w->start_pass && (pass - w->start_pass) % w->interval == 0 && (w->end_pass < 0 || pass <= w->end_pass)))
+    return;
+  for (i = 0; i < n && watch_count < watch_cap; i++) {
+    double *r = watch_buf + watch_count * 9;
+    r[0] = elem_index;
+    r[1] = pass;
+    r[2] = coord[i][6];
+    for (j = 0; j < 6; j++)
+      r[3 + j] = coord[i][j];
+    watch_count++;
+  }
+}
+
 void b2e_ref_set_history(double *buffer, long n_passes) {
   history_out = buffer;
   history_passes = buffer ? n_passes : 0;
@@ -359,9 +391,11 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
 
   for (i_pass = 0; i_pass < n_passes; i_pass++) {
     long nParticlesStartPass = nToTrack;
+    long elem_index = -1;
     z = z_travel = last_z = line->beg_pos;
     eptr = line;
     while (eptr && nToTrack) {
+      elem_index++;
       unsigned long classFlags = entity_description[eptr->type].flags;
       last_z = z;
       if (classFlags & HAS_LENGTH && eptr->p_elem) {
@@ -394,6 +428,9 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
           }
           break;
         case T_MARK:
+          break;
+        case T_WATCH:
+          capture_watch((WATCH *)eptr->p_elem, elem_index, i_pass, coord, nToTrack);
           break;
         case T_MALIGN:
           /* do_tracking.c:1818-1821 */

@@ -62,6 +62,20 @@ class RefOracle:
         pass (findFiducialTime on the particles it received); -1 if none."""
         return float(self.lib.b2e_ref_last_fiducial_t0())
 
+    def watch_rows(self):
+        """The rows the last run's WATCH elements were handed (set_watch):
+        array [k][9] = element index, pass, particleID, x, xp, y, yp, s, delta."""
+        self.lib.b2e_ref_watch_rows.restype = ctypes.c_long
+        k = self.lib.b2e_ref_watch_rows()
+        return self._watch[:k].copy()
+
+    def set_watch(self, capacity_rows: int):
+        """Capture the coordinate-mode WATCH rows of the following runs (up to
+        capacity_rows rows); 0 turns it off."""
+        self._watch = np.zeros((max(capacity_rows, 1), 9))
+        self.lib.b2e_ref_set_watch(self._watch.ctypes.data_as(ctypes.c_void_p) if capacity_rows else None,
+                                   ctypes.c_long(capacity_rows))
+
     def track(self, lattice, coords, ids, p_central, n_passes, wake_capacity=0, capture_wakes=False,
               history=False):
         """Returns (rows, n_left, effort, wakes); rows are the reference's final

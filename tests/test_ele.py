@@ -226,3 +226,39 @@ def test_runner_tracks_an_sdds_beam(tmp_path):
             ref = t.track(beam)
         alive = ref.lost_pass < 0
         assert np.array_equal(fin.pages[k]["columns"]["x"], ref.coords[alive, 0])
+
+
+@pytest.mark.gpu
+def test_runner_writes_watch_files(tmp_path):
+    """A WATCH with FILENAME in the .lte: the runner writes one page per
+    recorded pass; the rows equal the engine's WATCH records."""
+    from elegant_b200 import Tracker, workloads as w
+    from elegant_b200.lattice import parse_lte
+    from sdds_protocol import SddsFile
+    lat = w.fodo_ring(rf=False)
+    lines = [f"{e.name}: {e.type}, " + ", ".join(f"{k}={v!r}" for k, v in e.params.items()) for e in lat.elements]
+    lines.append('W1: WATCH, FILENAME="%s.w1", INTERVAL=2, START_PASS=1, END_PASS=7')
+    names = [e.name for e in lat.elements]
+    names.insert(10, "W1")
+    (tmp_path / "ring.lte").write_text("\n".join(lines) + "\nRING: LINE=(" + ", ".join(names) + ")\n")
+    p0 = w.ring_p_central()
+    (tmp_path / "job.ele").write_text(
+        f"&run_setup lattice = ring.lte, use_beamline = RING, p_central = {p0!r}, random_number_seed = 5 &end\n"
+        "&run_control n_passes = 10 &end\n"
+        "&bunched_beam n_particles_per_bunch = 2000, emit_x = 1e-8, emit_y = 1e-8, beta_x = 10, beta_y = 10,\n"
+        "   sigma_dp = 1e-3, sigma_s = 1e-3 &end\n&track &end\n")
+    run_ele(str(tmp_path / "job.ele"))
+    f = SddsFile(str(tmp_path / "job.w1"))
+    assert [pg["parameters"]["Pass"] for pg in f.pages] == [1, 3, 5, 7]
+    lat2 = parse_lte((tmp_path / "ring.lte").read_text(), "RING")
+    from elegant_b200.ele import BUNCHED_BEAM
+    bb = dict(BUNCHED_BEAM, n_particles_per_bunch=2000, emit_x=1e-8, emit_y=1e-8, beta_x=10.0, beta_y=10.0,
+              sigma_dp=1e-3, sigma_s=1e-3)
+    beam = bunched_beam(bb, p0, seed=5)
+    with Tracker(lat2, p0, 10) as t:
+        t.set_watch(1 << 30)
+        t.track(beam)
+        recs = t.watch()
+    for pg, r in zip(f.pages, recs):
+        assert np.array_equal(pg["columns"]["x"], r["coords"][:, 0])
+        assert np.array_equal(pg["columns"]["particleID"], r["ids"])

@@ -449,3 +449,43 @@ def test_ring_with_gradient_dipoles(ref_b2e, case):
     assert 0 < nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+@pytest.mark.parametrize("kw", [{}, {"compact_every": 2}, {"passes_per_launch": 3}],
+                         ids=["fused", "compacted", "split_launches"])
+def test_watch_records_equal_the_reference(ref_b2e, kw):
+    """WATCH elements (coordinate mode): on the passes each writes
+    (START_PASS, INTERVAL, END_PASS), the particles alive at it and their
+    coordinates equal what the reference hands dump_watch_particles, bit for
+    bit; the tracking itself is unchanged by them.  With compaction the rows
+    move between launches and the records follow the IDs."""
+    from test_oracle_pin import _ring_with_watches
+    lat = _ring_with_watches()
+    beam = Beam(np.concatenate([w.ring_beam(300, seed=55).coords, _lossy_beam(300, seed=56).coords]),
+                np.arange(1, 601))
+    ref_b2e.set_watch(2_000_000)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 12)
+    ref_rows = ref_b2e.watch_rows()
+    ref_b2e.set_watch(0)
+    with Tracker(lat, w.ring_p_central(), 12, **kw) as t:
+        t.set_watch(1 << 30)
+        res = t.track(beam)
+        recs = t.watch()
+    assert_parity(res, rows, nl)
+    w1, w2 = lat.index("W1")[0], lat.index("W2")[0]
+    assert [(r["element"], r["pass"]) for r in recs] == [(w1, q) for q in (1, 4, 7, 10)] + [(w2, q) for q in range(5)]
+    for r in recs:
+        sel = ref_rows[(ref_rows[:, 0] == r["element"]) & (ref_rows[:, 1] == r["pass"])]
+        sel = sel[np.argsort(sel[:, 2], kind="stable")]
+        assert np.array_equal(r["ids"], sel[:, 2].astype(np.int64)), (r["element"], r["pass"])
+        assert np.array_equal(r["coords"], sel[:, 3:9]), (r["element"], r["pass"])
+
+
+def test_watch_budget_is_enforced():
+    from elegant_b200._native import EngineError
+    from test_oracle_pin import _ring_with_watches
+    beam = w.ring_beam(1000, seed=57)
+    with Tracker(_ring_with_watches(), w.ring_p_central(), 12) as t:
+        t.set_watch(1000)
+        with pytest.raises(EngineError, match="WATCH"):
+            t.track(beam)

@@ -429,3 +429,39 @@ def test_port_reproduces_reference_gradient_dipoles(math, case):
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
     r0, n0, _, _ = RefOracle(math).track(base or w.fodo_ring(), beam.coords, beam.ids, P0, 20)
     assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
+
+
+def _ring_with_watches():
+    from elegant_b200 import Element, Lattice
+    els = list(w.fodo_ring().elements)
+    els.insert(3, Element("W1", "WATCH", {"FILENAME": "%s.w1", "INTERVAL": 3, "START_PASS": 1}))
+    els.insert(30, Element("W2", "WATCH", {"FILENAME": "%s.w2", "END_PASS": 4}))
+    els.append(Element("W3", "WATCH", {"FILENAME": "%s.w3", "DISABLE": 1}))
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_with_watches(math):
+    """WATCH elements change no coordinate and no loss (do_tracking.c:1585-1635,
+    NO_APERTURE); the reference's WATCH rows (what dump_watch_particles is
+    handed) are the particles alive there on the passes it writes
+    (sdds_support.c:738-741)."""
+    lat = _ring_with_watches()
+    beam = lossy_beam(150, seed=53)
+    ref = RefOracle(math)
+    ref.set_watch(100000)
+    r1, n1, e1, _ = ref.track(lat, beam.coords, beam.ids, P0, 12)
+    rows = ref.watch_rows()
+    ref.set_watch(0)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 12)
+    r0, n0, e0, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 12)
+    assert n1 == n2 == n0 and e1 == e2 == e0 and n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7]) and np.array_equal(r1[:, 6:8], r0[:, 6:8])
+    w1, w2 = lat.index("W1")[0], lat.index("W2")[0]
+    assert sorted(set(rows[rows[:, 0] == w1, 1])) == [1, 4, 7, 10]
+    assert sorted(set(rows[rows[:, 0] == w2, 1])) == [0, 1, 2, 3, 4]
+    assert not (rows[:, 0] == lat.index("W3")[0]).any()
+    # the particles at W2 on pass 0 are the beam less those lost before it
+    first = rows[(rows[:, 0] == w2) & (rows[:, 1] == 0)]
+    lost_early = {int(i) for i, lp in zip(r1[:, 6], r1[:, 7]) if lp == 0}
+    assert set(first[:, 2].astype(int)) <= set(beam.ids) - (lost_early - set(first[:, 2].astype(int)))

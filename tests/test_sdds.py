@@ -184,3 +184,36 @@ def test_pages_appended_per_step(tmp_path, mode):
     mine = read_sdds_pages(path)
     assert [pv["Step"] for pv, _ in mine] == [1, 2]
     assert np.array_equal(mine[1][1]["x"], f.pages[1]["columns"]["x"])
+
+
+def test_watch_file_layout(tmp_path):
+    """write_watch: dump_watch_particles' columns and parameters
+    (sdds_support.c:403-520, :703-860), EXCLUDE_SLOPES and the PID window,
+    PassCentralTime as the Kahan-summed revolution times."""
+    from elegant_b200.sdds import watch_pass_central_times, write_watch
+    rng = np.random.default_rng(9)
+    recs = []
+    for q in (0, 3, 6):
+        n = 20 - q
+        c = rng.normal(0, 1e-3, (n, 6))
+        recs.append({"pass": q, "ids": np.arange(1, n + 1), "coords": c})
+    p0, z, length = 2000.0, 7.5, 30.4
+    write_watch(str(tmp_path / "w.sdds"), recs, p0, z, length, step=2, charge=1e-12,
+                watch={"EXCLUDE_SLOPES": 1, "START_PID": 3, "END_PID": 15})
+    f = SddsFile(str(tmp_path / "w.sdds"))
+    names = [c["name"] for c in f.columns]
+    assert names == ["x", "y", "t", "p", "dt", "particleID"]
+    t0 = watch_pass_central_times([0, 3, 6], z, length, p0)
+    root = np.sqrt(p0 * p0 + 1)
+    # the Kahan sum of three equal steps against plain arithmetic: within an ulp
+    assert abs(t0[2] - (z + 6 * length) * root / (2.99792458e8 * p0)) < 1e-20
+    for page, r, t in zip(f.pages, recs, t0):
+        keep = (r["ids"] >= 3) & (r["ids"] <= 15)
+        prm = page["parameters"]
+        assert prm["Pass"] == r["pass"] and prm["Step"] == 2 and prm["Particles"] == keep.sum()
+        assert prm["PassCentralTime"] == t and prm["s"] == z and prm["PassLength"] == length
+        assert abs(prm["Charge"] - 1e-12 * keep.sum()) < 1e-24
+        assert np.array_equal(page["columns"]["particleID"], r["ids"][keep])
+        pp = p0 * (1 + r["coords"][keep, 5])
+        tt = r["coords"][keep, 4] / (2.99792458e8 * pp / np.sqrt(pp * pp + 1))
+        assert np.array_equal(page["columns"]["t"], tt) and np.array_equal(page["columns"]["dt"], tt - t)
