@@ -116,8 +116,8 @@ struct b2e_ctx {
   /* WATCH recording (b2e_set_watch): [records][7][watch_rows] of the last call */
   int64_t watch_max_bytes = 0;
   DevBuf<double> d_watch;
-  DevBuf<int64_t> d_watch_rec0;
-  DevBuf<int32_t> d_watch_first;
+  std::vector<int64_t> watch_rec0;   /* per WATCH ordinal: record of its first pass in the call */
+  std::vector<int32_t> watch_first;  /* per WATCH ordinal: first pass it records in the call, -1: none */
   std::vector<int32_t> watch_rec_elem, watch_rec_pass;
   int64_t watch_rows = 0;
   bool watch_on = false;
@@ -442,7 +442,6 @@ static int autotune_ring(b2e_ctx *ctx, const RingLaunch &Lreal, bool staged, siz
   CUDA_TRY(ctx, ctx->d_scratch.ensure((size_t)n * 6));
   CUDA_TRY(ctx, ctx->d_scratch_loss.ensure((size_t)n * 2));
   RingLaunch L = Lreal;
-  L.watch = nullptr; /* the trials record nothing */
   double *cols[6] = {Lreal.P.x, Lreal.P.xp, Lreal.P.y, Lreal.P.yp, Lreal.P.s, Lreal.P.dp};
   L.P.x = ctx->d_scratch.ptr;
   L.P.xp = L.P.x + n;
@@ -553,10 +552,6 @@ static int run_ring_range(b2e_ctx *ctx, int pb, int eb, int pe, int ee) {
   L.ids = ctx->use_ext ? nullptr : ctx->d_ids.ptr;
   L.isr_seed = ctx->opt.isr_seed;
   L.sr_limit = ctx->opt.sr_gaussian_limit == 0 ? 3.0 : ctx->opt.sr_gaussian_limit;
-  L.watch = ctx->watch_on ? ctx->d_watch.ptr : nullptr;
-  L.watch_rows = ctx->watch_rows;
-  L.watch_rec0 = ctx->d_watch_rec0.ptr;
-  L.watch_first = ctx->d_watch_first.ptr;
   size_t smem = sizeof(DevElem) * ne + sizeof(DevAperture) * L.n_aps;
   bool staged = smem <= 200 * 1024;
   int ppl = ctx->opt.passes_per_launch > 0 ? ctx->opt.passes_per_launch : (1 << 30);
@@ -620,6 +615,17 @@ static int count_alive(b2e_ctx *ctx, int64_t *n_alive) {
   return B2E_OK;
 }
 
+/* Record number of WATCH element ie on pass p in this call, -1 if it does not
+ * record then (START_PASS, INTERVAL, END_PASS; sdds_support.c:738-741). */
+static int watch_record_of(const b2e_ctx *ctx, int ie, int p) {
+  const DevElem &d = ctx->lat.elems[ie];
+  const int k = (int)d.c[WA_ORDINAL], step = (int)d.c[WA_INTERVAL], end = (int)d.c[WA_END];
+  const int first = ctx->watch_first[k];
+  if (first < 0 || p < first || (p - first) % step != 0 || (end >= 0 && p > end))
+    return -1;
+  return (int)(ctx->watch_rec0[k] + (p - first) / step);
+}
+
 static int track_impl(b2e_ctx *ctx, double *effort) {
   const int ne = (int)ctx->lat.elems.size();
   const int p0 = ctx->pass_counter;
@@ -648,8 +654,10 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
   ctx->watch_on = false;
   if (ctx->watch_max_bytes > 0 && !ctx->lat.watch_elements.empty()) {
     const size_t nw = ctx->lat.watch_elements.size();
-    std::vector<int64_t> rec0(nw);
-    std::vector<int32_t> first(nw, -1);
+    std::vector<int64_t> &rec0 = ctx->watch_rec0;
+    std::vector<int32_t> &first = ctx->watch_first;
+    rec0.assign(nw, 0);
+    first.assign(nw, -1);
     for (size_t k = 0; k < nw; k++) {
       const DevElem &d = ctx->lat.elems[ctx->lat.watch_elements[k]];
       const long start = (long)d.c[WA_START], end = (long)d.c[WA_END], step = (long)d.c[WA_INTERVAL];
@@ -671,14 +679,7 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       ctx->watch_rows = ctx->n;
       CUDA_TRY(ctx, ctx->d_watch.ensure(records * 7 * (size_t)ctx->n));
       CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_watch.ptr, 0xff, sizeof(double) * records * 7 * (size_t)ctx->n,
-                                    ctx->stream)); /* NaN until a live particle writes */
-      CUDA_TRY(ctx, ctx->d_watch_rec0.ensure(nw));
-      CUDA_TRY(ctx, ctx->d_watch_first.ensure(nw));
-      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_watch_rec0.ptr, rec0.data(), sizeof(int64_t) * nw, cudaMemcpyHostToDevice,
-                                    ctx->stream));
-      CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_watch_first.ptr, first.data(), sizeof(int32_t) * nw,
-                                    cudaMemcpyHostToDevice, ctx->stream));
-      CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream)); /* the host vectors go out of scope */
+                                    ctx->stream)); /* NaN in the rows of lost particles */
       ctx->watch_on = true;
     }
   }
@@ -720,11 +721,12 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       ctx->csr.macro_charge[b] = q;
     }
   }
-  /* stop points: every RFCA on pass 0 (fiducial), every CSR element on every pass */
-  int p = p0, e = 0;
+  /* stop points: every RFCA on pass 0 (fiducial), every CSR element on every
+   * pass, every recording WATCH on the passes it records */
+  int p = p0, e = 0, watched_e = -1, watched_p = -1;
   size_t next_rf = 0;
   while (p < npass) {
-    int stop_e = ne, stop_kind = 0; /* 1 = RFCA fiducial, 2 = CSR element */
+    int stop_e = ne, stop_kind = 0; /* 1 = RFCA fiducial, 2 = CSR element, 3 = WATCH record */
     for (int ie = e; ie < ne; ie++) {
       if (p == 0 && next_rf < ctx->lat.rf_elements.size() && ctx->lat.rf_elements[next_rf] == ie) {
         stop_e = ie;
@@ -736,11 +738,18 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
         stop_kind = 2;
         break;
       }
+      if (ctx->watch_on && ctx->lat.elems[ie].kind == K_WATCH && !(ie == watched_e && p == watched_p) &&
+          watch_record_of(ctx, ie, p) >= 0) {
+        stop_e = ie;
+        stop_kind = 3;
+        break;
+      }
     }
     if (stop_kind == 0) {
       /* nothing collective ahead on this pass; if the lattice has no CSR
-       * elements, run all remaining passes in fused launches */
-      int last_pass = ctx->lat.csr_elements.empty() ? npass - 1 : p;
+       * elements (and no WATCH records), run all remaining passes in fused
+       * launches */
+      int last_pass = ctx->lat.csr_elements.empty() && !ctx->watch_on ? npass - 1 : p;
       int rc = run_ring_range(ctx, p, e, last_pass, ne);
       if (rc)
         return rc;
@@ -753,7 +762,13 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       if (rc)
         return rc;
     }
-    if (stop_kind == 1) {
+    if (stop_kind == 3) {
+      /* the particles alive at the WATCH on this pass (do_tracking.c:1626-1629) */
+      const int r = watch_record_of(ctx, stop_e, p);
+      CUDA_TRY(ctx, launch_watch_copy(particle_view(ctx), ctx->use_ext ? nullptr : ctx->d_ids.ptr, ctx->n,
+                                      ctx->d_watch.ptr + (size_t)r * 7 * ctx->watch_rows, ctx->stream));
+      ctx->launches++;
+    } else if (stop_kind == 1) {
       ctx->launches++;
       CUDA_TRY(ctx, launch_fiducial(particle_view(ctx), ctx->d_inst_offsets.ptr, ctx->n_inst, ctx->d_elems.ptr, ne,
                                     stop_e, ctx->d_rf.ptr, ctx->lat.n_rf, ctx->opt.p_central,
@@ -780,6 +795,14 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       CUDA_TRY(ctx, launch_post_element_sweep(particle_view(ctx), ctx->n, iap >= 0 ? ctx->d_aps.ptr + iap : nullptr,
                                               p, stop_e, ctx->stream));
       ctx->launches++;
+    }
+    if (stop_kind == 3) {
+      /* the WATCH element itself (a no-op, then the after-element checks)
+       * goes with the next ring launch */
+      watched_e = stop_e;
+      watched_p = p;
+      e = stop_e;
+      continue;
     }
     e = stop_e + 1;
     if (e >= ne) {

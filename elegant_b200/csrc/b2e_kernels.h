@@ -37,15 +37,6 @@ struct RingLaunch {
   double *tbt;
   int tbt_pass0, tbt_records;
   int64_t tbt_rows;
-  /* WATCH records [record][7][watch_rows]: x, x', y, y', s, delta and the
-   * particle ID (a double; NaN where no live particle wrote); WATCH ordinal k
-   * writes record watch_rec0[k] + (pass - watch_first[k]) / interval on the
-   * passes it records from watch_first[k] on; null: WATCH elements are
-   * markers */
-  double *watch;
-  int64_t watch_rows;
-  const int64_t *watch_rec0;
-  const int32_t *watch_first;
 };
 
 /* variant 1..B2E_RING_VARIANTS selects the occupancy target and the barrier
@@ -59,6 +50,8 @@ cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticle
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
                             int64_t max_rows, cudaStream_t stream);
+/* one WATCH record [7][n]: x..delta and ID (double) of the live rows */
+cudaError_t launch_watch_copy(DevParticles P, const int64_t *ids, int64_t n, double *out, cudaStream_t stream);
 /* turn-by-turn record 0: x, x', y, y' of every row */
 cudaError_t launch_tbt_start(DevParticles P, int64_t n, double *tbt, cudaStream_t stream);
 /* NAFF (b2e_naff.cu): signals [n_signals][N] -> frequency, amplitude, phase */

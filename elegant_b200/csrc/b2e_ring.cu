@@ -82,27 +82,6 @@ __device__ __forceinline__ void tile_moments(const Part &p, bool alive, double *
  * memory record.  The arithmetic is identical in every variant.  HIST records
  * the per-pass tile moments (it needs SYNC >= 1); when SYNC >= 1 every thread
  * stays in the pass loop until the whole tile is lost. */
-/* A coordinate-mode WATCH on one of its passes writes the particle's
- * coordinates and ID into its record (RingLaunch.watch); out of line, so that
- * the element loop's register allocation does not carry it. */
-static __device__ __noinline__ void watch_record(double *watch, int64_t rows, const int64_t *rec0,
-                                                 const int32_t *first_pass, const int64_t *ids, const double *c,
-                                                 int pass, int64_t ip, double x, double xp, double y, double yp,
-                                                 double s, double dp) {
-  const int k = (int)c[WA_ORDINAL], first = first_pass[k], step = (int)c[WA_INTERVAL];
-  const int end = (int)c[WA_END];
-  if (first < 0 || pass < first || (pass - first) % step != 0 || (end >= 0 && pass > end))
-    return;
-  double *o = watch + (size_t)(rec0[k] + (pass - first) / step) * 7 * rows + ip;
-  o[0] = x;
-  o[rows] = xp;
-  o[2 * rows] = y;
-  o[3 * rows] = yp;
-  o[4 * rows] = s;
-  o[5 * rows] = dp;
-  o[6 * rows] = (double)(ids ? ids[ip] : ip + 1);
-}
-
 template <bool STAGED, int MINB, int SYNC, bool HIST, int TPB, bool RAD = false>
 __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
   static_assert(!HIST || SYNC >= 1, "history needs the per-pass barrier");
@@ -232,10 +211,7 @@ __global__ void __launch_bounds__(128 * TPB, MINB) ring_kernel(RingLaunch L) {
           lost = rfca(p, e, rs, L.g);
         break;
       }
-      default:
-        if (e.kind == K_WATCH && L.watch)
-          watch_record(L.watch, L.watch_rows, L.watch_rec0, L.watch_first, L.ids, e.c, pass, ip, p.x, p.xp, p.y,
-                       p.yp, p.s, p.dp);
+      default: /* MARK, CHARGE, WATCH (recorded between launches) */
         break;
       }
       if (!lost && !(e.flags & EF_NO_APERTURE) && ap && !maxamp_ok(p, *ap))
@@ -574,6 +550,29 @@ __global__ void tbt_start_kernel(DevParticles P, int64_t n, double *tbt) {
   tbt[n + i] = live ? P.xp[i] : NAN;
   tbt[2 * n + i] = live ? P.y[i] : NAN;
   tbt[3 * n + i] = live ? P.yp[i] : NAN;
+}
+
+/* WATCH record of the particles alive at a WATCH element (the ring launches
+ * stop there on its passes): x..delta and the ID as a double, NaN (left from
+ * the fill) in the rows of lost particles. */
+__global__ void watch_copy_kernel(DevParticles P, const int64_t *ids, int64_t n, double *out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n || P.lost_pass[i] >= 0)
+    return;
+  out[i] = P.x[i];
+  out[n + i] = P.xp[i];
+  out[2 * n + i] = P.y[i];
+  out[3 * n + i] = P.yp[i];
+  out[4 * n + i] = P.s[i];
+  out[5 * n + i] = P.dp[i];
+  out[6 * n + i] = (double)(ids ? ids[i] : i + 1);
+}
+
+cudaError_t launch_watch_copy(DevParticles P, const int64_t *ids, int64_t n, double *out, cudaStream_t stream) {
+  if (n <= 0)
+    return cudaSuccess;
+  watch_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(P, ids, n, out);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_tbt_start(DevParticles P, int64_t n, double *tbt, cudaStream_t stream) {

@@ -346,7 +346,9 @@ int b2e_tbt(b2e_ctx *ctx, double *host_out, int64_t capacity, int64_t *written);
  * B2E_ERR_ARG before tracking.  b2e_watch_records gives the number of
  * records, the row count and each record's element index and pass (up to
  * capacity entries); b2e_watch_data copies one record ([7][rows]) to host
- * memory.  Not with per-instance overrides of WATCH elements. */
+ * memory.  A recording call launches the ring kernel at least once per pass
+ * (it stops at each recording WATCH).  Not with per-instance overrides of
+ * WATCH elements. */
 int b2e_set_watch(b2e_ctx *ctx, int64_t max_bytes);
 int b2e_watch_records(b2e_ctx *ctx, int32_t *n_records, int64_t *rows, int32_t *elements, int32_t *passes,
                       int32_t capacity);
