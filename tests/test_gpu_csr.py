@@ -450,3 +450,33 @@ def test_csr_wake_output_file_matches_reference(ref_b2e, tmp_path, variant):
     for k, name in enumerate(CAPTURE_PARAMS):
         ours = np.array([pg["parameters"][name] for pg in read], dtype=np.float64)
         assert np.array_equal(ours, cap["parameters"][:, k]), name
+
+
+def test_watch_points_in_a_chicane(ref_b2e):
+    """WATCH elements between and after the CSR dipoles: the particles the
+    reference hands dump_watch_particles there, bit for bit, and the tracking
+    unchanged."""
+    lat = w.chicane(bins=150, n_kicks=5)
+    els = []
+    for e in lat.elements:
+        els.append(e)
+        if e.name in ("B2", "B4"):
+            els.append(Element("W" + e.name, "WATCH", {"FILENAME": "%s.w"}))
+    lat = Lattice(els)
+    beam = w.chicane_beam(12000, seed=61)
+    ref_b2e.set_watch(100000)
+    rows, nl, _, ref_wakes = ref_b2e.track(lat, beam.coords, beam.ids, P0, 1, capture_wakes=True)
+    ref_rows = ref_b2e.watch_rows()
+    ref_b2e.set_watch(0)
+    with Tracker(lat, P0, 1) as t:
+        t.set_watch(1 << 28)
+        res = t.track(beam)
+        wakes = t.csr_wakes(10_000_000)
+        recs = t.watch()
+    check(res, wakes, rows, nl, ref_wakes)
+    assert [r["element"] for r in recs] == lat.index("WB2") + lat.index("WB4")
+    for r in recs:
+        sel = ref_rows[ref_rows[:, 0] == r["element"]]
+        sel = sel[np.argsort(sel[:, 2], kind="stable")]
+        assert np.array_equal(r["ids"], sel[:, 2].astype(np.int64))
+        assert np.array_equal(r["coords"], sel[:, 3:9])
