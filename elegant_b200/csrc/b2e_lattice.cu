@@ -715,8 +715,8 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
         d.kind = K_NONE;
         break;
       }
-      if (p[B2E_WATCH_MODE] != 0)
-        err = "WATCH modes other than coordinates are not supported by this engine";
+      if (p[B2E_WATCH_MODE] != 0 && p[B2E_WATCH_MODE] != 1 && p[B2E_WATCH_MODE] != 2)
+        err = "WATCH fft mode is not supported by this engine";
       else if (p[B2E_WATCH_FRACTION] != 1)
         err = "WATCH FRACTION other than 1 is not supported by this engine";
       else if (p[B2E_WATCH_SPARSE_INTERVAL] > 1)

@@ -134,7 +134,8 @@ __global__ void __launch_bounds__(128, 1)
  *            bias + GELU (hidden), output channel 0 (output), or times
  *            GELU'(z) of the previous layer (backward data), BF16 stores.
  *            The erf/exp of GELU and GELU' bound the epilogue, hence two
- *            warps per lane quadrant.
+ *            warps per lane quadrant; launch bounds of two CTAs per SM
+ *            (96 registers, no spills) keep 16 epilogue warps per SM.
  * Bounded waits everywhere; a timeout sets the status word and every role
  * leaves its loop. */
 constexpr int CONV_EPI_WARPS = 8;
@@ -155,7 +156,7 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 }
 
 template <int EPI>
-__global__ void __launch_bounds__(CONV_THREADS, 1)
+__global__ void __launch_bounds__(CONV_THREADS, 2)
     conv_kernel(const __grid_constant__ CUtensorMap t_in, const __grid_constant__ CUtensorMap t_w, ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char dsm[];
   unsigned char *sm = (unsigned char *)(((uintptr_t)dsm + 1023) & ~(uintptr_t)1023);

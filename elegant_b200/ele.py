@@ -535,7 +535,8 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                 for i, e in watches:
                     write_watch(name(e.strings["FILENAME"]), [r for r in records if r["element"] == i], p0,
                                 float(z_end[i]), lattice.total_length, step=step + 1, charge=macro, watch=e.params,
-                                mode=mode, append=step > 0)
+                                mode=mode, append=step > 0, original_particles=beam.n,
+                                previous_element=lattice.elements[i - 1].name if i > 0 else None)
                     if step == 0:
                         summary["files"].append(name(e.strings["FILENAME"]))
                 for el_name, fname in csr_outputs.items():

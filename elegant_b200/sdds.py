@@ -235,8 +235,132 @@ def watch_pass_central_times(passes, z, length, p_central, reference_frequency=-
     return out
 
 
-def write_watch(path, records, p_central, z, length, step=1, charge=0.0, watch=None, mode="binary", append=False):
-    """A coordinate-mode WATCH file (SDDS_WatchPointSetup, sdds_support.c:403-520;
+ME_MEV = 0.51099895000  # electron rest energy (particleMassMV), CODATA 2018
+# the second moments accumulate_beam_sums forms with BEAM_SUMS_SPARSE
+# (compute_centroids.c:300-307): the diagonal blocks and the correlations
+# with delta (and s with t)
+_SPARSE = [(0, 0), (0, 1), (0, 5), (1, 1), (1, 5), (2, 2), (2, 3), (2, 5), (3, 3), (3, 5), (4, 4), (4, 5), (4, 6),
+           (5, 5), (6, 6)]
+
+
+def watch_statistics(coords, ids, p_central, start_pid=-1, end_pid=-1):
+    """The beam statistics of one WATCH record in parameter/centroid mode
+    (dump_watch_parameters, sdds_support.c:881-1160): centroids of x..delta
+    and of t = s sqrt(P^2+1)/(c P) (computeTimeCoordinates, trwake.c:532),
+    the sparse second-moment matrix about them (accumulate_beam_sums,
+    compute_centroids.c:286-490), the emittances (computeEmitTwissFromSigma-
+    Matrix, sdds_support.c:2303-2340; rms_longitudinal_emittance,
+    final_props.c:944-990), and Ct, pAverage, KAverage.  Particles in the
+    START_PID/END_PID window only.  Sums here are numpy's (pairwise), where
+    elegant sums in its array order with Kahan's compensation: the results
+    agree to rounding, not bit for bit."""
+    c = np.asarray(coords, dtype=np.float64)
+    ids = np.asarray(ids)
+    win = np.ones(len(ids), dtype=bool) if (start_pid < 0 and end_pid < 0) else (ids >= start_pid) & (ids <= end_pid)
+    x = c[win]
+    n = len(x)
+    out = {"n": n}
+    if n == 0:
+        out.update(centroid=np.zeros(7), sigma=np.zeros((7, 7)), Ct=0.0, pAverage=float("nan"),
+                   KAverage=float("nan"), ex=0.0, ey=0.0, ecx=0.0, ecy=0.0, el=0.0)
+        return out
+    P = p_central * (x[:, 5] + 1)
+    t = x[:, 4] * np.sqrt(P * P + 1) / (C_MKS * P)
+    cols = [x[:, k] for k in range(6)] + [t]
+    cen = np.array([v.sum() / n for v in cols])
+    dev = [cols[k] - cen[k] for k in range(7)]
+    sig = np.zeros((7, 7))
+    for i, j in _SPARSE:
+        sig[i, j] = sig[j, i] = (dev[i] * dev[j]).sum() / n
+    out["centroid"], out["sigma"] = cen, sig
+
+    def emit(plane):
+        e = sig[plane, plane] * sig[plane + 1, plane + 1] - sig[plane, plane + 1] ** 2
+        e = math.sqrt(e) if e > 0 else 0.0
+        if sig[5, 5]:
+            ec = e * e - (sig[plane, 5] ** 2 * sig[plane + 1, plane + 1]
+                          - 2 * sig[plane, plane + 1] * sig[plane, 5] * sig[plane + 1, 5]
+                          + sig[plane + 1, 5] ** 2 * sig[plane, plane]) / sig[5, 5]
+            ec = math.sqrt(ec) if ec > 0 else 0.0
+        else:
+            ec = e
+        return e, ec
+
+    out["ex"], out["ecx"] = emit(0)
+    out["ey"], out["ecy"] = emit(2)
+    # rms_longitudinal_emittance: its own window test (startPID >= endPID is
+    # "every particle") and t = s / (beta c)
+    lwin = np.ones(len(ids), dtype=bool) if start_pid >= end_pid else (ids >= start_pid) & (ids <= end_pid)
+    xl = c[lwin]
+    Pl = p_central * (1 + xl[:, 5])
+    tl = xl[:, 4] / (Pl / np.sqrt(Pl * Pl + 1) * C_MKS)
+    dt, dd = tl - tl.mean(), xl[:, 5] - xl[:, 5].mean()
+    e2 = (dt * dt).sum() * (dd * dd).sum() - (dt * dd).sum() ** 2
+    out["el"] = (math.sqrt(e2) if e2 > 0 else 0.0) / len(xl) if len(xl) else 0.0
+    # Ct, pAverage, KAverage (sdds_support.c:1075-1130): t = s / (p/sqrt(p^2+1) c)
+    tt = x[:, 4] / (P / np.sqrt(P * P + 1) * C_MKS)
+    out["Ct"] = tt.sum() / n
+    out["pAverage"] = P.sum() / n
+    out["KAverage"] = (np.sqrt(P * P + 1).sum() / n - 1) * ME_MEV
+    return out
+
+
+_WATCH_PARAM_COLS = [("Step", "long", {}), ("Pass", "long", {}), ("ElapsedTime", "double", {"units": "s"}),
+                     ("ElapsedCoreTime", "double", {"units": "s"}), ("MemoryUsage", "long", {"units": "kB"}),
+                     ("Cx", "double", {"symbol": "<x>", "units": "m"}), ("Cxp", "double", {"symbol": "<x'>"}),
+                     ("Cy", "double", {"symbol": "<y>", "units": "m"}), ("Cyp", "double", {"symbol": "<y'>"}),
+                     ("Cs", "double", {"symbol": "<s>", "units": "m"}), ("Cdelta", "double", {"symbol": "<$gd$r>"}),
+                     ("Ct", "double", {"symbol": "<t>", "units": "s"}),
+                     ("dCt", "double", {"symbol": "$gD$r<t>", "units": "s"}), ("Particles", "long", {}),
+                     ("Charge", "double", {"units": "C"}), ("Transmission", "double", {}),
+                     ("pCentral", "double", {"symbol": "p$bcen$n", "units": "m$be$nc"}),
+                     ("pAverage", "double", {"symbol": "p$bave$n", "units": "m$be$nc"}),
+                     ("KAverage", "double", {"symbol": "K$bave$n", "units": "MeV"}),
+                     ("Sx", "double", {"units": "m"}), ("Sxp", "double", {}), ("Sy", "double", {"units": "m"}),
+                     ("Syp", "double", {}), ("Ss", "double", {"units": "m"}), ("Sdelta", "double", {}),
+                     ("St", "double", {"units": "s"}), ("ex", "double", {"units": "m"}),
+                     ("ey", "double", {"units": "m"}), ("el", "double", {"units": "s"}),
+                     ("ecx", "double", {"units": "m"}), ("ecy", "double", {"units": "m"})]
+
+
+def _write_watch_parameters(path, records, p_central, z, length, step, charge, w, mode, append, original_particles,
+                            previous_element):
+    """Parameter (31 columns) or centroid (the first 19) mode: one page per
+    step, one row per recorded pass (sdds_support.c:359-393, :538-585,
+    :881-1160)."""
+    centroid_only = int(w.get("MODE", 1)) == 2
+    cols_def = _WATCH_PARAM_COLS[:19] if centroid_only else _WATCH_PARAM_COLS
+    times = watch_pass_central_times([r["pass"] for r in records], z, length, p_central,
+                                     w.get("REFERENCE_FREQUENCY", -1.0))
+    rows = {name: [] for name, _, _ in cols_def}
+    for r, t0 in zip(records, times):
+        st = watch_statistics(r["coords"], r["ids"], p_central, w.get("START_PID", -1), w.get("END_PID", -1))
+        cen, sig = st["centroid"], st["sigma"]
+        vals = {"Step": step, "Pass": r["pass"], "ElapsedTime": 0.0, "ElapsedCoreTime": 0.0, "MemoryUsage": 0,
+                "Cx": cen[0], "Cxp": cen[1], "Cy": cen[2], "Cyp": cen[3], "Cs": cen[4], "Cdelta": cen[5],
+                "Ct": st["Ct"], "dCt": st["Ct"] - t0, "Particles": st["n"], "Charge": charge * st["n"],
+                "Transmission": len(r["ids"]) / original_particles if original_particles else 0.0,
+                "pCentral": p_central, "pAverage": st["pAverage"], "KAverage": st["KAverage"],
+                "Sx": math.sqrt(sig[0, 0]), "Sxp": math.sqrt(sig[1, 1]), "Sy": math.sqrt(sig[2, 2]),
+                "Syp": math.sqrt(sig[3, 3]), "Ss": math.sqrt(sig[4, 4]), "Sdelta": math.sqrt(sig[5, 5]),
+                "St": math.sqrt(sig[6, 6]), "ex": st["ex"], "ey": st["ey"], "el": st["el"], "ecx": st["ecx"],
+                "ecy": st["ecy"]}
+        for name, _, _ in cols_def:
+            rows[name].append(vals[name])
+    params_def = [("Step", "long", {"description": "Simulation step"}), ("s", "double", {"units": "m"}),
+                  ("PreviousElementName", "string", {})]
+    write_sdds_pages(path, params_def, cols_def,
+                     [([step, z, previous_element or "_BEG_"], [rows[name] for name, _, _ in cols_def])],
+                     mode, description="watch-point " + ("centroids" if centroid_only else "parameters"),
+                     append=append)
+
+
+def write_watch(path, records, p_central, z, length, step=1, charge=0.0, watch=None, mode="binary", append=False,
+                original_particles=0, previous_element=None):
+    """A WATCH file.  Parameter and centroid modes: one page per step with a
+    row per recorded pass (_write_watch_parameters; original_particles, the
+    step's initial count, gives Transmission).  Coordinate mode
+    (SDDS_WatchPointSetup, sdds_support.c:403-520;
     dump_watch_particles :703-860), one page per recorded pass, from the
     records of one WATCH (elegant_b200.track.Tracker.watch entries of that
     element, in pass order): columns x, xp, y, yp (X_DATA, Y_DATA; slopes
@@ -248,6 +372,12 @@ def write_watch(path, records, p_central, z, length, step=1, charge=0.0, watch=N
     Rows are the particles by ascending ID (elegant keeps its array order);
     START_PID/END_PID select rows."""
     w = dict(watch or {})
+    if int(w.get("MODE", 0)) in (1, 2):
+        _write_watch_parameters(path, records, p_central, z, length, step, charge, w, mode, append,
+                                original_particles, previous_element)
+        return
+    if int(w.get("MODE", 0)) != 0:
+        raise ValueError("WATCH fft mode is not written by this module")
     get = lambda k, d: w.get(k, d)
     x_data, y_data, longit = get("X_DATA", 1), get("Y_DATA", 1), get("LONGIT_DATA", 1)
     slopes = not get("EXCLUDE_SLOPES", 0)

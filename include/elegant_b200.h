@@ -174,13 +174,14 @@ extern "C" {
 #define B2E_MALIGN_ON_PASS 8   /* default -1 */
 #define B2E_MALIGN_START_PID 9 /* default -1: every particle */
 #define B2E_MALIGN_END_PID 10  /* default -1 */
-/* WATCH (watch_param, track_data.c:880-900), coordinate mode: after every
- * INTERVAL-th pass from START_PASS to END_PASS (inclusive, -1: no end) the
- * coordinates of the particles alive at the element are recorded when
- * b2e_set_watch enables it (the element never changes them).  DISABLE = 1
- * makes it a marker.  The engine rejects the other modes, FRACTION != 1 and
- * SPARSE_INTERVAL != 1; START_PID/END_PID select rows of the output, not
- * the recording. */
+/* WATCH (watch_param, track_data.c:880-900): on every INTERVAL-th pass from
+ * START_PASS to END_PASS (inclusive, -1: no end) the coordinates of the
+ * particles alive at the element are recorded when b2e_set_watch enables it
+ * (the element never changes them); the coordinate, parameter and centroid
+ * modes all record coordinates (the caller reduces them, e.g.
+ * elegant_b200.sdds.write_watch).  DISABLE = 1 makes it a marker.  The
+ * engine rejects the fft mode, FRACTION != 1 and SPARSE_INTERVAL != 1;
+ * START_PID/END_PID select rows of the output, not the recording. */
 #define B2E_WATCH_START_PASS 0
 #define B2E_WATCH_END_PASS 1      /* default -1 */
 #define B2E_WATCH_INTERVAL 2      /* default 1 */

@@ -283,6 +283,31 @@ static void capture_watch(const WATCH *w, long elem_index, long pass, double **c
   }
 }
 
+/* accumulate_beam_sums (compute_centroids.c:286-490) on rows [n][7] (x, xp,
+ * y, yp, s, delta, particleID) as dump_watch_parameters calls it
+ * (sdds_support.c:979-981): centroid[7] and the sparse sigma[7][7]. */
+long b2e_ref_beam_sums(const double *rows, long n, double Po, long startPID, long endPID, double *centroid,
+                       double *sigma) {
+  double **coord = (double **)czarray_2d(sizeof(double), n ? n : 1, totalPropertiesPerParticle);
+  BEAM_SUMS *sums;
+  long i, j;
+  for (i = 0; i < n; i++)
+    for (j = 0; j < 7; j++)
+      coord[i][j] = rows[i * 7 + j];
+  sums = allocateBeamSums(0, 1);
+  zero_beam_sums(sums, 1);
+  accumulate_beam_sums(sums, coord, n, Po, 0.0, NULL, 0.0, 0.0, startPID, endPID,
+                       BEAM_SUMS_SPARSE | BEAM_SUMS_NOMINMAX);
+  for (i = 0; i < 7; i++) {
+    centroid[i] = sums->centroid[i];
+    for (j = 0; j < 7; j++)
+      sigma[i * 7 + j] = sums->beamSums2->sigma[i][j];
+  }
+  j = sums->n_part;
+  free_czarray_2d((void **)coord, n ? n : 1, totalPropertiesPerParticle);
+  return j;
+}
+
 void b2e_ref_set_history(double *buffer, long n_passes) {
   history_out = buffer;
   history_passes = buffer ? n_passes : 0;

@@ -251,3 +251,28 @@ long bitsSet(unsigned long data) {
   }
   return n;
 }
+
+/* ---- beam sums (compute_centroids.c, compiled for the WATCH statistics) --- */
+/* exactNormalizedEmittance (global_settings exact_normalized_emittance) is
+ * defined in track_data.c: 0, elegant's default */
+/* computeTimeCoordinates (trwake.c:532-590, serial branch): t = s sqrt(P^2+1)/(c P)
+ * for every particle and their Kahan mean */
+double computeTimeCoordinates(double *time, double Po, double **part, long np) {
+  double tmean = 0, error = 0, P;
+  long ip;
+  for (ip = 0; ip < np; ip++) {
+    P = Po * (part[ip][5] + 1);
+    time[ip] = part[ip][4] * sqrt(sqr(P) + 1) / (c_mks * P);
+    tmean = KahanPlus(tmean, time[ip], &error);
+  }
+  return np ? tmean / np : 0;
+}
+
+void computeTimeCoordinatesOnly(double *time, double Po, double **part, long np) {
+  long ip;
+  double P;
+  for (ip = 0; ip < np; ip++) {
+    P = Po * (part[ip][5] + 1);
+    time[ip] = part[ip][4] * sqrt(sqr(P) + 1) / (c_mks * P);
+  }
+}

@@ -217,3 +217,69 @@ def test_watch_file_layout(tmp_path):
         pp = p0 * (1 + r["coords"][keep, 5])
         tt = r["coords"][keep, 4] / (2.99792458e8 * pp / np.sqrt(pp * pp + 1))
         assert np.array_equal(page["columns"]["t"], tt) and np.array_equal(page["columns"]["dt"], tt - t)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(os.path.dirname(__file__), "..", "oracle", "_ref")),
+                    reason="needs oracle/_ref")
+@pytest.mark.parametrize("window", [(-1, -1), (20, 700)])
+def test_watch_statistics_against_accumulate_beam_sums(window):
+    """The parameter/centroid-mode reduction against elegant's own
+    accumulate_beam_sums (compute_centroids.c, compiled into the reference
+    build) on the same rows: centroids of x..delta and t, and the sparse
+    second moments, to rounding (elegant sums with Kahan's compensation in
+    its array order, numpy pairwise)."""
+    import ctypes
+    from elegant_b200.sdds import watch_statistics
+    from reforacle import RefOracle
+    lib = RefOracle("libm").lib
+    f = lib.b2e_ref_beam_sums
+    f.restype = ctypes.c_long
+    rng = np.random.default_rng(17)
+    n, p0 = 1000, 2000.0
+    c = np.column_stack([rng.normal(0, 1e-3, n), rng.normal(0, 1e-4, n), rng.normal(0, 5e-4, n),
+                         rng.normal(0, 5e-5, n), rng.normal(3.0, 1e-3, n), rng.normal(0, 1e-3, n)])
+    c[:, 0] += 2.0 * c[:, 5]  # dispersion, so that ecx differs from ex
+    ids = rng.permutation(n) + 1
+    rows = np.column_stack([c, ids]).astype(np.float64).copy()
+    cen = np.zeros(7)
+    sig = np.zeros(49)
+    npc = f(rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.c_double(p0), ctypes.c_long(window[0]),
+            ctypes.c_long(window[1]), cen.ctypes.data_as(ctypes.c_void_p), sig.ctypes.data_as(ctypes.c_void_p))
+    st = watch_statistics(c, ids, p0, *window)
+    assert st["n"] == npc and npc > 0
+    assert np.allclose(st["centroid"], cen, rtol=1e-12, atol=1e-18)
+    sig = sig.reshape(7, 7)
+    assert np.allclose(st["sigma"], sig, rtol=1e-11, atol=1e-30)
+    assert (st["sigma"] == 0).sum() == (sig == 0).sum()  # the same sparse pattern
+    assert st["ecx"] < st["ex"]
+
+
+@pytest.mark.parametrize("wmode", [1, 2], ids=["parameter", "centroid"])
+def test_watch_parameter_and_centroid_layouts(tmp_path, wmode):
+    """Parameter mode: 31 columns, centroid mode: the first 19
+    (sdds_support.c:359-393); one page per step, one row per recorded pass,
+    the values from watch_statistics."""
+    from elegant_b200.sdds import watch_pass_central_times, watch_statistics, write_watch
+    rng = np.random.default_rng(3)
+    recs = [{"pass": q, "ids": np.arange(1, 101 - q), "coords": rng.normal(0, 1e-3, (100 - q, 6))}
+            for q in (0, 2, 4)]
+    path = str(tmp_path / "wp.sdds")
+    for step in (1, 2):
+        write_watch(path, recs, 2000.0, 4.0, 30.4, step=step, charge=1e-12, watch={"MODE": wmode},
+                    original_particles=100, previous_element="QF", append=step > 1)
+    f = SddsFile(path)
+    assert len(f.pages) == 2
+    names = [c["name"] for c in f.columns]
+    assert len(names) == (31 if wmode == 1 else 19) and names[:6] == ["Step", "Pass", "ElapsedTime",
+                                                                       "ElapsedCoreTime", "MemoryUsage", "Cx"]
+    page = f.pages[1]
+    assert page["parameters"]["Step"] == 2 and page["parameters"]["PreviousElementName"] == "QF"
+    col = page["columns"]
+    assert list(col["Pass"]) == [0, 2, 4] and list(col["Particles"]) == [100, 98, 96]
+    t0 = watch_pass_central_times([0, 2, 4], 4.0, 30.4, 2000.0)
+    for k, r in enumerate(recs):
+        st = watch_statistics(r["coords"], r["ids"], 2000.0)
+        assert col["Cx"][k] == st["centroid"][0] and col["dCt"][k] == st["Ct"] - t0[k]
+        assert col["Transmission"][k] == len(r["ids"]) / 100
+        if wmode == 1:
+            assert col["Sx"][k] == np.sqrt(st["sigma"][0, 0]) and col["ex"][k] == st["ex"]
