@@ -238,8 +238,10 @@ def test_runner_writes_watch_files(tmp_path):
     lat = w.fodo_ring(rf=False)
     lines = [f"{e.name}: {e.type}, " + ", ".join(f"{k}={v!r}" for k, v in e.params.items()) for e in lat.elements]
     lines.append('W1: WATCH, FILENAME="%s.w1", INTERVAL=2, START_PASS=1, END_PASS=7')
+    lines.append('W2: WATCH, FILENAME="%s.w2", MODE="parameter"')
     names = [e.name for e in lat.elements]
     names.insert(10, "W1")
+    names.append("W2")
     (tmp_path / "ring.lte").write_text("\n".join(lines) + "\nRING: LINE=(" + ", ".join(names) + ")\n")
     p0 = w.ring_p_central()
     (tmp_path / "job.ele").write_text(
@@ -259,6 +261,16 @@ def test_runner_writes_watch_files(tmp_path):
         t.set_watch(1 << 30)
         t.track(beam)
         recs = t.watch()
-    for pg, r in zip(f.pages, recs):
+    w1 = [r for r in recs if r["element"] == lat2.index("W1")[0]]
+    for pg, r in zip(f.pages, w1):
         assert np.array_equal(pg["columns"]["x"], r["coords"][:, 0])
         assert np.array_equal(pg["columns"]["particleID"], r["ids"])
+    # parameter mode: one page, a row per pass, the statistics of the records
+    from elegant_b200.sdds import watch_statistics
+    w2 = [r for r in recs if r["element"] == lat2.index("W2")[0]]
+    f2 = SddsFile(str(tmp_path / "job.w2"))
+    assert len(f2.pages) == 1 and list(f2.pages[0]["columns"]["Pass"]) == list(range(10)) == [r["pass"] for r in w2]
+    for k, r in enumerate(w2):
+        st = watch_statistics(r["coords"], r["ids"], p0)
+        assert f2.pages[0]["columns"]["Cx"][k] == st["centroid"][0]
+        assert f2.pages[0]["columns"]["ex"][k] == st["ex"]
