@@ -517,14 +517,32 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                         raise EleError(f"&sdds_beam: {e}") from e
                 elif step == 0 or not bb["one_random_bunch"]:
                     beam = bunched_beam(bb, p0, rs["random_number_seed"] + step, twiss)
-                with Tracker(lattice, p0, rc["n_passes"], device=device, default_order=rs["default_order"]) as t:
+                # WATCH records take device memory per recorded pass: the passes
+                # run in calls of `chunk` passes that each fit the budget
+                n_passes = rc["n_passes"]
+                chunk = n_passes
+                if watches:
+                    per_pass = len(watches) * 7 * 8 * max(beam.n, 1)
+                    limit = max(1, WATCH_BUDGET_BYTES // per_pass)
+                    chunk = max(d for d in range(1, n_passes + 1) if n_passes % d == 0 and d <= limit)
+                with Tracker(lattice, p0, chunk, device=device, default_order=rs["default_order"]) as t:
                     if csr_outputs:
                         t.set_csr_pages(True)
+                    records = []
                     if watches:
                         t.set_watch(WATCH_BUDGET_BYTES)
-                    res = t.track(beam)
+                    if chunk == n_passes:
+                        res = t.track(beam)
+                        records = t.watch() if watches else []
+                    else:
+                        t.upload(beam)
+                        effort = 0.0
+                        for _ in range(n_passes // chunk):
+                            effort += t.continue_tracking()
+                            records += t.watch()
+                        res = t.download()
+                        res.effort = effort
                     pages = t.csr_pages() if csr_outputs else []
-                    records = t.watch() if watches else []
                 summary["steps"].append({"step": step + 1, "survivors": res.n_left, "effort": res.effort})
                 charge = next((e.get("TOTAL") for e in lattice.elements if e.type == "CHARGE"), 0.0)
                 for f in outs:

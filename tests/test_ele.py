@@ -274,3 +274,38 @@ def test_runner_writes_watch_files(tmp_path):
         st = watch_statistics(r["coords"], r["ids"], p0)
         assert f2.pages[0]["columns"]["Cx"][k] == st["centroid"][0]
         assert f2.pages[0]["columns"]["ex"][k] == st["ex"]
+
+
+@pytest.mark.gpu
+def test_runner_watch_files_under_a_small_budget(tmp_path, monkeypatch):
+    """A device-memory budget smaller than the run's WATCH records: the runner
+    tracks in calls of fewer passes (continuing the same run) and the files
+    are the same as with the whole run in one call."""
+    import elegant_b200.ele as ele
+    from elegant_b200 import workloads as w
+    from sdds_protocol import SddsFile
+    lat = w.fodo_ring(rf=False)
+    lines = [f"{e.name}: {e.type}, " + ", ".join(f"{k}={v!r}" for k, v in e.params.items()) for e in lat.elements]
+    lines += ['W1: WATCH, FILENAME="%s.w1"', 'W2: WATCH, FILENAME="%s.w2", MODE="centroid"']
+    names = [e.name for e in lat.elements]
+    names.insert(7, "W1")
+    names.append("W2")
+    (tmp_path / "ring.lte").write_text("\n".join(lines) + "\nRING: LINE=(" + ", ".join(names) + ")\n")
+    p0 = w.ring_p_central()
+    job = (f"&run_setup lattice = ring.lte, use_beamline = RING, p_central = {p0!r}, final = %s.fin,\n"
+           "   random_number_seed = 9 &end\n&run_control n_passes = 12 &end\n"
+           "&bunched_beam n_particles_per_bunch = 1000, emit_x = 5e-8, emit_y = 5e-8, beta_x = 10, beta_y = 10,\n"
+           "   sigma_dp = 3e-3, sigma_s = 1e-3 &end\n&track &end\n")
+    (tmp_path / "a.ele").write_text(job)
+    (tmp_path / "b.ele").write_text(job)
+    run_ele(str(tmp_path / "a.ele"))
+    monkeypatch.setattr(ele, "WATCH_BUDGET_BYTES", 2 * 7 * 8 * 1000 * 3)  # three passes per call
+    run_ele(str(tmp_path / "b.ele"))
+    for ext in ("w1", "w2", "fin"):
+        fa, fb = SddsFile(str(tmp_path / f"a.{ext}")), SddsFile(str(tmp_path / f"b.{ext}"))
+        assert len(fa.pages) == len(fb.pages)
+        for pa, pb in zip(fa.pages, fb.pages):
+            for k, v in pa["columns"].items():
+                if k in ("ElapsedTime", "ElapsedCoreTime", "MemoryUsage"):
+                    continue
+                assert np.array_equal(np.asarray(v), np.asarray(pb["columns"][k])), (ext, k)
