@@ -32,7 +32,8 @@ path are
   optimization_mode (the area only, no file), with setup_aperture_search's
   checks; the output file per step;
 - &momentum_aperture (momentumAperture.nl): every key but
-  forbid_resonance_crossing, fiducialize included; output_mode 0 or 1.
+  forbid_resonance_crossing, fiducialize included; output_mode 0, 1, and 2
+  (Pelegant's grid search, run here on the batched engine).
 
 A command outside this list, or a key of these commands away from its
 default that the engine does not implement, raises EleError naming it: the
@@ -432,7 +433,7 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
     """Run a .ele file's tracking job on the engine; returns a summary per
     step (survivors, effort) and the files written."""
     from .aperture import find_aperture_lines, find_aperture_mp
-    from .momentum_aperture import momentum_aperture
+    from .momentum_aperture import local_momentum_acceptance, momentum_aperture
     from .optics import periodic_twiss
     from .sdds import (beam_from_sdds, write_aperture, write_aperture_mp, write_csr_wake, write_losses,
                        write_momentum_aperture, write_phase_space, write_watch)
@@ -598,9 +599,8 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
             ma = _command(fields, MOMENTUM_APERTURE, cmd, set(MOMENTUM_APERTURE) - {"forbid_resonance_crossing"})
             if rs is None:
                 raise EleError("&momentum_aperture needs &run_setup before it")
-            if ma["output_mode"] not in (0, 1):
-                raise EleError("&momentum_aperture: output_mode=2 is elegant's MPI-only mode "
-                               "(not available in serial elegant)")
+            if ma["output_mode"] not in (0, 1, 2):
+                raise EleError("&momentum_aperture: output_mode must be 0, 1 or 2")
             if not ma["output"]:
                 raise EleError("&momentum_aperture: no output filename specified")
             rc = rc or dict(RUN_CONTROL)
@@ -612,8 +612,17 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                                      "s_start", "s_end", "include_name_pattern", "include_type_pattern")}
             for step in range(rc["n_steps"]):
                 try:
-                    rows, effort = momentum_aperture(lattice, p0, rc["n_passes"], soft_failure=bool(ma["soft_failure"]),
-                                                     fiducialize=bool(ma["fiducialize"]), device=device, **kw)
+                    if ma["output_mode"] == 2:
+                        # the grid search of multiparticleLocalMomentumAcceptance (Pelegant's mode):
+                        # splits, steps_back, split_step_divisor, fiducialize and soft_failure unused
+                        rows, effort = local_momentum_acceptance(
+                            lattice, p0, rc["n_passes"], device=device,
+                            **{k: v for k, v in kw.items()
+                               if k not in ("splits", "steps_back", "split_step_divisor")})
+                    else:
+                        rows, effort = momentum_aperture(lattice, p0, rc["n_passes"],
+                                                         soft_failure=bool(ma["soft_failure"]),
+                                                         fiducialize=bool(ma["fiducialize"]), device=device, **kw)
                 except ValueError as e:
                     raise EleError(f"&momentum_aperture: {e}") from e
                 write_momentum_aperture(out, rows, step=step + 1, mode=mode_io, output_mode=ma["output_mode"],

@@ -33,9 +33,12 @@ instance.  A fiducial particle lost on that pass stops the search, as in
 the reference.
 
 output_mode 1 (one row per element and side, :141-160, :715-731) is a layout
-of the same results (elegant_b200.sdds.write_momentum_aperture); output_mode
-2 is the reference's MPI-only mode (:185, "not available in serial
-elegant"): the batched engine is this module's parallel form.
+of the same results (elegant_b200.sdds.write_momentum_aperture).
+
+output_mode 2 (multiparticleLocalMomentumAcceptance, :840-1120, Pelegant
+only) tracks a fixed grid of deltas at every selected element in one beam
+and takes, per element and side, the lost delta nearest zero, one step back:
+local_momentum_acceptance.
 
 Not built: forbid_resonance_crossing (needs tunes from turn-by-turn data),
 include patterns with wildcards other than '*' and '?'.
@@ -247,3 +250,150 @@ def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_init
             raise RuntimeError("Fiducial particle lost. Don't know what to do. (momentumAperture.c:400-404)")
         lost_pass, c, lost_elem = lost_pass[1::2], c[1::2], lost_elem[1::2]
     return lost_pass, c[:, 0], c[:, 2], c[:, 5], lost_elem, effort
+
+
+def _has_wildcards(pattern: str) -> bool:
+    return any(c in pattern for c in "*?[")
+
+
+def acceptance_grid(delta_negative_limit: float, delta_positive_limit: float, delta_negative_start: float,
+                    delta_positive_start: float, delta_step_size: float):
+    """output_mode 2's delta grid (momentumAperture.c:864-866, :823-827):
+    n_delta points over both sides, the step that spans them exactly, the
+    index where the positive side starts, and the delta of each index, all
+    with the reference's operations (C's truncation to long included)."""
+    span = (delta_positive_limit - delta_positive_start) + (delta_negative_start - delta_negative_limit)
+    n_delta = int(span / delta_step_size + 1)
+    if n_delta < 2:
+        raise ValueError("momentum_aperture: the delta grid needs two points or more")
+    step = span / (n_delta - 1)
+    cutover = int((delta_negative_start - delta_negative_limit) / step + 0.5)
+    deltas = [delta_negative_limit + i * step if i < cutover else delta_positive_start + (i - cutover) * step
+              for i in range(n_delta)]
+    return n_delta, step, cutover, deltas
+
+
+def omni_wedge_lattice(lattice: Lattice, locations, fire_on_pass: int, n_delta: int, x_initial: float,
+                       y_initial: float) -> tuple[Lattice, list[int]]:
+    """The lattice with a MALIGN wedge at the entrance of each selected
+    element, where the omni wedge of output_mode 2 acts (do_tracking.c:839-844
+    calls it before the element; momentumOffsetFunctionOmni,
+    momentumAperture.c:801-833): on the firing pass it offsets by (x_initial,
+    y_initial, delta) the particles whose ID falls in the element's block of
+    n_delta IDs.  Returns it and the wedges' element indices."""
+    at_loc = {i: k for k, i in enumerate(locations)}
+    els, wedges = [], []
+    for i, e in enumerate(lattice.elements):
+        if i in at_loc:
+            k = at_loc[i]
+            wedges.append(len(els))
+            els.append(Element(f"{WEDGE}{i}", "MALIGN", {"ON_PASS": fire_on_pass, "DX": x_initial, "DY": y_initial,
+                                                         "START_PID": k * n_delta,
+                                                         "END_PID": k * n_delta + n_delta - 1}))
+        els.append(e)
+    return Lattice(els), wedges
+
+
+def local_momentum_acceptance(lattice: Lattice, p_central: float, n_passes: int, x_initial=1e-5, y_initial=1e-5,
+                              delta_negative_limit=-0.10, delta_positive_limit=0.10, delta_negative_start=0.0,
+                              delta_positive_start=0.0, delta_step_size=0.0025, s_start=0.0, s_end=math.inf,
+                              include_name_pattern=None, include_type_pattern=None, skip_elements=0,
+                              process_elements=2 ** 31 - 1, starting_coord=None, device=0, compact_every=0,
+                              track_trials=None):
+    """&momentum_aperture output_mode 2 (multiparticleLocalMomentumAcceptance,
+    momentumAperture.c:840-1120) on the batched engine.
+
+    The reference tracks one fiducial particle for one pass
+    (FIRST_BEAM_IS_FIDUCIAL, :899-913), then one beam holding, for each of
+    the n_elem selected elements and each of the grid's n_delta deltas, a
+    particle with ID ie*n_delta + idelta starting at starting_coord (zero by
+    default); on pass 1 (pass 0 for a one-pass run) the particles of element
+    ie are offset by (x_initial, y_initial, delta) as they enter it.  Every
+    lost particle then bounds its element's side: the lost delta nearest
+    zero (delta >= 0 is the positive side, :1069-1081), and the reported
+    limit is one grid step back from it (:1090-1093); a side without a loss
+    reports +-DBL_MAX.
+
+    Batched: one ensemble instance per grid delta, holding the fiducial
+    particle first (the engine takes the RF phase reference from it alone,
+    fiducial_particles = 1; its ID lies outside every wedge's block) and then
+    one particle per selected element; the wedges carry the instance's delta
+    as a per-instance DP override.  Every instance's fiducial row runs the
+    same first pass as the reference's fiducial run.
+
+    Returns one dict per selected element: index, name, type, s (its end),
+    occurrence, and per side ('negative', 'positive'): delta (the reported
+    limit), found, delta_lost (the nearest lost delta, None if none); and the
+    particle-turns tracked.  track_trials(lattice, offsets, overrides, beam,
+    p_central, n_passes) -> (lost_pass, coords, effort), rows in beam order,
+    replaces the engine."""
+    if delta_negative_limit >= 0 or delta_positive_limit <= 0 or delta_negative_start > 0 or \
+            delta_positive_start < 0 or delta_step_size <= 0 or s_start >= s_end or \
+            abs(delta_negative_limit - delta_negative_start) <= delta_step_size / 2 or \
+            delta_positive_limit - delta_positive_start <= delta_step_size / 2:
+        raise ValueError("momentum_aperture: invalid limits, starts, step or s range (momentumAperture.c:80-101)")
+    if include_name_pattern is not None and _has_wildcards(include_name_pattern):
+        raise ValueError("Can't have wildcards in name pattern for output_mode=2")
+    if include_type_pattern is not None:
+        raise ValueError("Can't used include_type_pattern for output_mode=2")
+    locs = select_elements(lattice, s_start, s_end, include_name_pattern, None, skip_elements, process_elements)
+    if not locs:
+        raise ValueError("no elements found between s_start and s_end for momentum aperture computation")
+    n_delta, step, cutover, deltas = acceptance_grid(delta_negative_limit, delta_positive_limit,
+                                                     delta_negative_start, delta_positive_start, delta_step_size)
+    n_elem = len(locs)
+    n_total = n_elem * n_delta
+    fire = 0 if n_passes == 1 else 1
+    wl, wedges = omni_wedge_lattice(lattice, locs, fire, n_delta, x_initial, y_initial)
+
+    per = n_elem + 1
+    start = np.zeros(6) if starting_coord is None else np.asarray(starting_coord, dtype=np.float64)[:6]
+    coords = np.tile(start, (per * n_delta, 1))
+    ids = np.empty(per * n_delta, dtype=np.int64)
+    for idelta in range(n_delta):
+        ids[idelta * per] = n_total + idelta  # the fiducial particle: outside every wedge's ID block
+        ids[idelta * per + 1:(idelta + 1) * per] = np.arange(n_elem, dtype=np.int64) * n_delta + idelta
+    offsets = np.arange(0, per * n_delta + 1, per, dtype=np.int64)
+    dp = np.asarray(deltas, dtype=np.float64)
+    overrides = [(wi, "DP", dp) for wi in wedges]
+    beam = Beam(coords, ids)
+    if track_trials is not None:
+        lost_pass, _, effort = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
+        lost_pass = np.asarray(lost_pass)
+        out_ids = ids
+    else:
+        with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every,
+                     fiducial_particles=1) as t:
+            t.load_ensemble(offsets, overrides)
+            res = t.track(beam)
+        lost_pass, out_ids, effort = res.lost_pass, res.ids, res.effort
+
+    fid = out_ids >= n_total
+    if (lost_pass[fid] == 0).any():
+        # the reference's fiducial run is one pass (momentumAperture.c:907-913)
+        raise RuntimeError("Fiducial particle lost. Don't know what to do. (momentumAperture.c:907-913)")
+    big = 1.7976931348623157e308
+    lost_at = [[-big, big] for _ in range(n_elem)]  # deltaLost[side][ie] (:1041-1044)
+    found = [[False, False] for _ in range(n_elem)]
+    for pid, lp in zip(out_ids[~fid], lost_pass[~fid]):
+        if lp < 0:
+            continue
+        idelta = int(pid) % n_delta
+        ie = (int(pid) - idelta) // n_delta
+        d = deltas[idelta]
+        side = 1 if d >= 0 else 0
+        if not found[ie][side] or (d < lost_at[ie][side] if side else d > lost_at[ie][side]):
+            found[ie][side] = True
+            lost_at[ie][side] = d
+    z_end = np.cumsum([e.length for e in lattice.elements])
+    out = []
+    for k, i in enumerate(locs):
+        e = lattice.elements[i]
+        occurrence = sum(1 for f in lattice.elements[:i + 1] if f.name == e.name)
+        row = {"index": i, "name": e.name, "type": e.type, "s": float(z_end[i]), "occurrence": occurrence}
+        for side, label in ((0, "negative"), (1, "positive")):
+            lost = lost_at[k][side]
+            row[label] = {"delta": lost + step if side == 0 else lost - step, "found": found[k][side],
+                          "delta_lost": lost if found[k][side] else None}
+        out.append(row)
+    return out, effort

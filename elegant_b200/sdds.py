@@ -438,7 +438,9 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, ap
     """elegant's &momentum_aperture output from elegant_b200.momentum_aperture
     rows: output_mode 0, one row per element with both sides
     (momentumAperture.c:189-212, :692-714), or output_mode 1, one row per
-    element and side, negative (direction -1) first (:141-160, :715-731).
+    element and side, negative (direction -1) first (:141-160, :715-731);
+    output_mode 2 from local_momentum_acceptance rows, the two limits per
+    element (:163-180).
     nuxLost/nuyLost are -1: tunes are only found with
     forbid_resonance_crossing, which is not built."""
     n = len(rows)
@@ -462,8 +464,19 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, ap
         write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
                    append=append)
         return
+    if output_mode == 2:
+        # multiparticleLocalMomentumAcceptance's page (momentumAperture.c:163-180, :1084-1099)
+        cols = [("ElementName", "string", [r["name"] for r in rows], {}),
+                ("s", "double", [r["s"] for r in rows], {"units": "m"}),
+                ("ElementType", "string", [r["type"] for r in rows], {}),
+                ("ElementOccurence", "long", occ, {}),
+                ("deltaPositive", "double", [r["positive"]["delta"] for r in rows], {"symbol": "$gd$R$bpos$n"}),
+                ("deltaNegative", "double", [r["negative"]["delta"] for r in rows], {"symbol": "$gd$R$bneg$n"})]
+        write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
+                   append=append)
+        return
     if output_mode != 0:
-        raise ValueError("output_mode 2 is the reference's MPI-only mode (momentumAperture.c:185)")
+        raise ValueError("output_mode must be 0, 1 or 2")
     cols = [("ElementName", "string", [r["name"] for r in rows], {}),
             ("s", "double", [r["s"] for r in rows], {"units": "m"}),
             ("ElementType", "string", [r["type"] for r in rows], {}),

@@ -99,3 +99,74 @@ def oracle_trials(oracle):
                 lost[r] = int(rows[0, 7])
         return lost, coords, math.nan
     return run
+
+
+def serial_local_acceptance(oracle, lattice, p_central, n_passes, x_initial=1e-5, y_initial=1e-5,
+                            delta_negative_limit=-0.10, delta_positive_limit=0.10, delta_negative_start=0.0,
+                            delta_positive_start=0.0, delta_step_size=0.0025, **select):
+    """&momentum_aperture output_mode 2 (multiparticleLocalMomentumAcceptance,
+    momentumAperture.c:840-1100) restated one particle per oracle run: the
+    grid of :864-866 and :823-827, the offset at the selected element's
+    entrance on the firing pass (:801-833), the one-pass fiducial run's RF
+    phase for every particle (:899-913), the nearest loss per side
+    (:1053-1082) and one grid step back (:1090-1093).  Per selected element:
+    ((deltaNegative, nearest negative loss or None), (deltaPositive, ...))."""
+    span = (delta_positive_limit - delta_positive_start) + (delta_negative_start - delta_negative_limit)
+    n_delta = int(span / delta_step_size + 1)
+    step = span / (n_delta - 1)
+    cut = int((delta_negative_start - delta_negative_limit) / step + 0.5)
+    locs = select_elements(lattice, **select)
+    fire = 0 if n_passes == 1 else 1
+    t0 = fiducial_time(oracle, lattice, p_central) if any(e.type == "RFCA" for e in lattice.elements) else None
+    big = 1.7976931348623157e308
+    out = []
+    for i in locs:
+        lost = [-big, big]
+        found = [False, False]
+        for idelta in range(n_delta):
+            delta = delta_negative_limit + idelta * step if idelta < cut else \
+                delta_positive_start + (idelta - cut) * step
+            els = list(lattice.elements)
+            els.insert(i, Element("WEDGE", "MALIGN", {"DX": x_initial, "DY": y_initial, "DP": delta,
+                                                      "ON_PASS": fire}))
+            lat = Lattice(els)
+            if t0 is not None:
+                lat = with_fiducial(lat, t0)
+            _, n_left, _ = oracle.track(lat, np.zeros((1, 6)), np.array([1]), p_central, n_passes)[:3]
+            if n_left == 0:
+                side = 1 if delta >= 0 else 0
+                if not found[side] or (delta < lost[side] if side else delta > lost[side]):
+                    found[side], lost[side] = True, delta
+        out.append(((lost[0] + step, lost[0] if found[0] else None),
+                    (lost[1] - step, lost[1] if found[1] else None)))
+    return out
+
+
+def oracle_instances(oracle):
+    """track_trials for elegant_b200.momentum_aperture.local_momentum_acceptance
+    on a CPU oracle: each instance (its overrides applied) in its own run;
+    its first row is the fiducial particle, whose one-pass run gives the RFCA
+    fiducial time the other rows keep as T_REFERENCE."""
+    def run(wl, offsets, overrides, beam, p_central, n_passes):
+        lost = np.full(beam.n, -1, dtype=np.int32)
+        coords = np.zeros((beam.n, 6))
+        has_rf = any(e.type == "RFCA" for e in wl.elements)
+        t0 = fiducial_time(oracle, wl, p_central) if has_rf else None
+        for t in range(len(offsets) - 1):
+            els = list(wl.elements)
+            for (ie, name, values) in overrides:
+                e = els[ie]
+                els[ie] = Element(e.name, e.type, dict(e.params, **{name: float(values[t])}))
+            lat = Lattice(els)
+            if t0 is not None:
+                lat = with_fiducial(lat, t0)
+            a, b = offsets[t] + 1, offsets[t + 1]
+            rows, n_left, _ = oracle.track(lat, beam.coords[a:b], beam.ids[a:b], p_central, n_passes)[:3]
+            pos = {int(pid): k for k, pid in enumerate(beam.ids[a:b])}
+            for j, r in enumerate(rows):
+                k = a + pos[int(r[6])]
+                coords[k] = r[:6]
+                if j >= n_left:  # survivors first, then the lost rows with their pass
+                    lost[k] = int(r[7])
+        return lost, coords, math.nan
+    return run

@@ -147,11 +147,11 @@ def test_find_aperture_checks():
 @pytest.mark.gpu
 def test_runner_aperture_commands(tmp_path):
     """&find_aperture (n-line, and slope mode with optimization_mode) and
-    &momentum_aperture (fiducialize, output_mode 1) from a run file: the
-    files written equal the direct calls."""
+    &momentum_aperture (fiducialize, output_mode 1; output_mode 2) from a
+    run file: the files written equal the direct calls."""
     from elegant_b200 import workloads as w
     from elegant_b200.aperture import find_aperture_lines
-    from elegant_b200.momentum_aperture import momentum_aperture
+    from elegant_b200.momentum_aperture import local_momentum_acceptance, momentum_aperture
     from sdds_protocol import SddsFile
     lat = w.fodo_ring(rf=False)
     lines = []
@@ -169,7 +169,9 @@ def test_runner_aperture_commands(tmp_path):
         '&momentum_aperture output = %s.mmap, include_type_pattern = "KQUAD", process_elements = 2,\n'
         '   delta_step_size = 0.0015, fiducialize = 1, output_mode = 1 &end\n'
         '&find_aperture mode = "n-line", n_lines = 5, xmin = 0, xmax = 0, ymin = 0, ymax = 0, xpmax = 4e-3,\n'
-        '   ypmax = 3e-3, nx = 11, optimization_mode = 1 &end\n')
+        '   ypmax = 3e-3, nx = 11, optimization_mode = 1 &end\n'
+        '&momentum_aperture output = %s.lma, s_start = 2, process_elements = 3, delta_step_size = 0.001,\n'
+        '   delta_negative_limit = -0.02, delta_positive_limit = 0.02, output_mode = 2 &end\n')
     out = run_ele(str(tmp_path / "da.ele"))
     aper = SddsFile(str(tmp_path / "da.aper")).pages[0]
     want = find_aperture_lines(lat, p0, 40, lines=7, xmax=0.03, ymax=0.02, nx=13, n_splits=1)
@@ -180,7 +182,13 @@ def test_runner_aperture_commands(tmp_path):
                                 delta_step_size=0.0015, fiducialize=True)
     assert list(mmap["columns"]["delta"]) == [r[s]["delta"] for r in rows for s in ("negative", "positive")]
     slope = find_aperture_lines(lat, p0, 40, lines=5, nx=11, slope=True, xpmax=4e-3, ypmax=3e-3)
-    assert out["steps"][-1]["area"] == slope["area"]
+    assert out["steps"][-2]["area"] == slope["area"]
+    lma = SddsFile(str(tmp_path / "da.lma")).pages[0]["columns"]
+    rows, _ = local_momentum_acceptance(lat, p0, 40, s_start=2.0, process_elements=3, delta_step_size=0.001,
+                                        delta_negative_limit=-0.02, delta_positive_limit=0.02)
+    assert list(lma["deltaPositive"]) == [r["positive"]["delta"] for r in rows]
+    assert list(lma["deltaNegative"]) == [r["negative"]["delta"] for r in rows]
+    assert list(lma["ElementName"]) == [r["name"] for r in rows]
 
 
 def test_runner_sdds_beam_checks(tmp_path):

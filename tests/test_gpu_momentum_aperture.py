@@ -61,3 +61,21 @@ def test_malign_element_bit_exact(ref_b2e):
     assert res.n_left == nl
     alive = ref_loss < 0
     assert np.array_equal(res.coords[order][alive], ref_c[alive])
+
+
+@pytest.mark.parametrize("passes", [1, 40])
+def test_local_acceptance_matches_serial_restatement(ref_b2e, passes):
+    """output_mode 2 on the device (one instance per grid delta, a fiducial
+    row first, the wedges on each element's ID block) against one reference
+    run per particle with the fiducial particle's RF phase."""
+    from elegant_b200.momentum_aperture import local_momentum_acceptance
+    from ma_reference import serial_local_acceptance
+    from test_momentum_aperture import mid_rf_ring
+    lat = mid_rf_ring() if passes == 1 else w.fodo_ring()
+    kw = dict(process_elements=8, delta_step_size=0.0005, delta_negative_limit=-0.02, delta_positive_limit=0.02)
+    serial = serial_local_acceptance(ref_b2e, lat, P0, passes, **kw)
+    rows, effort = local_momentum_acceptance(lat, P0, passes, **kw)
+    assert effort > 0 and len(rows) == len(serial) == 8
+    for row, s in zip(rows, serial):
+        for side, label in ((0, "negative"), (1, "positive")):
+            assert (row[label]["delta"], row[label]["delta_lost"]) == s[side], (row["name"], label)

@@ -88,3 +88,65 @@ def test_output_mode_1_layout(tmp_path):
     assert list(c["direction"]) == [-1, 1] and list(c["deltaFound"]) == [1, 0]
     assert list(c["delta"]) == [-0.01, 0.02] and list(c["ElementOccurence"]) == [2, 2]
     assert list(c["lostOnPass"]) == [3, -1] and list(c["ElementName"]) == ["QF", "QF"]
+
+
+def test_local_acceptance_grid():
+    """output_mode 2's grid (momentumAperture.c:864-866, :823-827) with the
+    reference's operations: 81 points over +-0.1 at 0.0025, the positive
+    side from index 40; and starts away from zero."""
+    from elegant_b200.momentum_aperture import acceptance_grid
+    n, step, cut, deltas = acceptance_grid(-0.1, 0.1, 0.0, 0.0, 0.0025)
+    assert (n, cut) == (81, 40) and step == 0.2 / 80
+    assert deltas[0] == -0.1 and deltas[39] == -0.1 + 39 * step and deltas[40] == 0.0 and deltas[80] == 40 * step
+    n, step, cut, deltas = acceptance_grid(-0.05, 0.04, -0.01, 0.02, 0.003)
+    assert n == int(((0.04 - 0.02) + (-0.01 + 0.05)) / 0.003 + 1) and deltas[cut] == 0.02
+    assert all(d < 0 for d in deltas[:cut]) and all(d >= 0.02 for d in deltas[cut:])
+
+
+def test_local_acceptance_matches_the_serial_restatement():
+    """output_mode 2 (multiparticleLocalMomentumAcceptance): the batched form
+    (one instance per grid delta, a fiducial row first, the wedge at each
+    selected element's entrance on its ID block) against one oracle run per
+    particle, on one pass of mid_rf_ring (the fiducial's RF phase matters)
+    and 40 passes of the ring."""
+    from elegant_b200.momentum_aperture import local_momentum_acceptance
+    from ma_reference import oracle_instances, serial_local_acceptance
+    ref = RefOracle("b2e")
+    kw = dict(process_elements=3, delta_step_size=0.0007, delta_negative_limit=-0.02, delta_positive_limit=0.02,
+              s_start=2.0)
+    for lat, passes in ((mid_rf_ring(), 1), (w.fodo_ring(), 40)):
+        serial = serial_local_acceptance(ref, lat, P0, passes, **kw)
+        rows, _ = local_momentum_acceptance(lat, P0, passes, track_trials=oracle_instances(ref), **kw)
+        assert len(rows) == len(serial) == 3
+        for row, s in zip(rows, serial):
+            for side, label in ((0, "negative"), (1, "positive")):
+                assert (row[label]["delta"], row[label]["delta_lost"]) == s[side], (row["name"], label)
+        assert any(r["positive"]["found"] or r["negative"]["found"] for r in rows)
+
+
+def test_local_acceptance_checks():
+    import pytest
+    from elegant_b200.momentum_aperture import local_momentum_acceptance
+    lat = w.fodo_ring()
+    with pytest.raises(ValueError, match="wildcards"):
+        local_momentum_acceptance(lat, P0, 1, include_name_pattern="Q*")
+    with pytest.raises(ValueError, match="include_type_pattern"):
+        local_momentum_acceptance(lat, P0, 1, include_type_pattern="KQUAD")
+    with pytest.raises(ValueError, match="invalid"):
+        local_momentum_acceptance(lat, P0, 1, delta_negative_start=-0.0999)
+
+
+def test_output_mode_2_layout(tmp_path):
+    """The two limits per element (momentumAperture.c:163-180), read back
+    with the independent SDDS reader."""
+    from elegant_b200.sdds import write_momentum_aperture
+    from sdds_protocol import SddsFile
+    rows = [{"name": "QF", "type": "KQUAD", "s": 1.3, "occurrence": 2,
+             "negative": {"delta": -0.01, "found": True, "delta_lost": -0.011},
+             "positive": {"delta": 1.7976931348623157e308, "found": False, "delta_lost": None}}]
+    write_momentum_aperture(str(tmp_path / "ma2.sdds"), rows, step=3, output_mode=2)
+    page = SddsFile(str(tmp_path / "ma2.sdds")).pages[0]
+    c = page["columns"]
+    assert list(c) == ["ElementName", "s", "ElementType", "ElementOccurence", "deltaPositive", "deltaNegative"]
+    assert list(c["deltaNegative"]) == [-0.01] and list(c["deltaPositive"]) == [1.7976931348623157e308]
+    assert page["parameters"]["Step"] == 3 and list(c["ElementOccurence"]) == [2]
