@@ -31,9 +31,9 @@ path are
   eleven-line modes and n-line, slope mode (xmin == xmax) and
   optimization_mode (the area only, no file), with setup_aperture_search's
   checks; the output file per step;
-- &momentum_aperture (momentumAperture.nl): every key but
-  forbid_resonance_crossing, fiducialize included; output_mode 0, 1, and 2
-  (Pelegant's grid search, run here on the batched engine).
+- &momentum_aperture (momentumAperture.nl): every key, fiducialize and
+  forbid_resonance_crossing included; output_mode 0, 1, and 2 (Pelegant's
+  grid search, run here on the batched engine).
 
 A command outside this list, or a key of these commands away from its
 default that the engine does not implement, raises EleError naming it: the
@@ -596,7 +596,7 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
             if out:
                 summary["files"].append(out)
         elif cmd == "momentum_aperture":
-            ma = _command(fields, MOMENTUM_APERTURE, cmd, set(MOMENTUM_APERTURE) - {"forbid_resonance_crossing"})
+            ma = _command(fields, MOMENTUM_APERTURE, cmd, set(MOMENTUM_APERTURE))
             if rs is None:
                 raise EleError("&momentum_aperture needs &run_setup before it")
             if ma["output_mode"] not in (0, 1, 2):
@@ -620,9 +620,10 @@ def run_ele(path: str, device: int = 0, mode: str = "binary") -> dict:
                             **{k: v for k, v in kw.items()
                                if k not in ("splits", "steps_back", "split_step_divisor")})
                     else:
-                        rows, effort = momentum_aperture(lattice, p0, rc["n_passes"],
-                                                         soft_failure=bool(ma["soft_failure"]),
-                                                         fiducialize=bool(ma["fiducialize"]), device=device, **kw)
+                        rows, effort = momentum_aperture(
+                            lattice, p0, rc["n_passes"], soft_failure=bool(ma["soft_failure"]),
+                            fiducialize=bool(ma["fiducialize"]),
+                            forbid_resonance_crossing=bool(ma["forbid_resonance_crossing"]), device=device, **kw)
                 except ValueError as e:
                     raise EleError(f"&momentum_aperture: {e}") from e
                 write_momentum_aperture(out, rows, step=step + 1, mode=mode_io, output_mode=ma["output_mode"],

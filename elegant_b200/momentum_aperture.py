@@ -40,8 +40,22 @@ only) tracks a fixed grid of deltas at every selected element in one beam
 and takes, per element and side, the lost delta nearest zero, one step back:
 local_momentum_acceptance.
 
-Not built: forbid_resonance_crossing (needs tunes from turn-by-turn data),
-include patterns with wildcards other than '*' and '?'.
+Tunes (:569-603, determineTunesFromTrackingData :1125-1162): the reference
+records every trial's x, x', y, y' at the wedge from the firing pass on and,
+for a particle that survives more than two recorded turns, takes its tunes
+by NAFF with adjustTuneHalfPlane; the last survivor's tunes are the nuxLost /
+nuyLost columns.  Here the engine records the turns at the end of each pass
+(record_tbt; the same turns, so the same tunes up to NAFF's resolution) and
+the NAFF kernel gives the tunes.  forbid_resonance_crossing (:515-538,
+:569-590): the tunes of a zero-delta trial at each element are the nominal
+ones, and a trial whose tunes cannot be found, or whose integer part of
+twice a tune differs from the nominal one, counts as lost; for such a
+trial the reference reports its final coordinates and whatever loss pass
+its coordinate array held from an earlier trial (reported here as -1).
+The NAFF kernel takes 4 to 8192 turns: with three recorded turns (4
+passes) the reference finds tunes and this module reports -1.
+
+Not built: include patterns with wildcards other than '*' and '?'.
 """
 from __future__ import annotations
 
@@ -112,18 +126,21 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
                       delta_positive_start=0.0, delta_step_size=0.0025, splits=1, steps_back=1,
                       split_step_divisor=10, s_start=0.0, s_end=math.inf, include_name_pattern=None,
                       include_type_pattern=None, skip_elements=0, process_elements=2 ** 31 - 1,
-                      soft_failure=False, fiducialize=False, device=0, compact_every=0, track_trials=None):
+                      soft_failure=False, fiducialize=False, forbid_resonance_crossing=False, device=0,
+                      compact_every=0, track_trials=None):
     """Returns one dict per selected element: name, type, s (its end),
     index, occurrence (1-based among the elements of its name), and per side
     ('negative', 'positive'): delta (last survivor),
     found (a loss was found), lost_on_pass, x_lost, y_lost, s_lost (end of
     the element of the loss), delta_when_lost (the particle's delta there),
-    delta_lost (the first lost trial's offset).  Also returns the number of
-    particle-turns tracked.  track_trials(lattice, offsets, overrides, beam,
-    p_central, n_passes) -> (lost_pass, coords at the end or at loss, effort),
-    rows in beam order, replaces the engine (used to check the batching
-    against a CPU tracker); with fiducialize the beam has two rows per
-    instance, the fiducial particle first."""
+    delta_lost (the first lost trial's offset), nux and nuy (the last
+    survivor's tunes: 0 without a survivor, -1 when none were found).  Also
+    returns the number of particle-turns tracked.  track_trials(lattice,
+    offsets, overrides, beam, p_central, n_passes) -> (lost_pass, coords at
+    the end or at loss, effort[, (nux, nuy)]), rows in beam order, replaces
+    the engine (used to check the batching against a CPU tracker); with
+    fiducialize the beam has two rows per instance, the fiducial particle
+    first; without the tunes item every trial's tunes are -1."""
     if delta_negative_limit >= 0 or delta_positive_limit <= 0 or delta_negative_start > 0 or \
             delta_positive_start < 0 or delta_step_size <= 0 or splits < 0 or s_start >= s_end:
         raise ValueError("momentum_aperture: invalid limits, starts, step, splits or s range "
@@ -133,6 +150,16 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
     if not locs:
         raise ValueError("no elements found between s_start and s_end for momentum aperture computation")
     fire = 0 if n_passes == 1 else 1
+    # turns recorded from the firing pass on; tunes when more than two (momentumAperture.c:568)
+    n_turns = n_passes - fire
+    tune_window = None
+    if n_turns > 2:
+        collective = any(e.type in ("CSRCSBEND", "CSRDRIFT") for e in lattice.elements)
+        if 4 <= n_turns <= 8192 and compact_every == 0 and not collective:
+            tune_window = (fire + 1, n_turns)
+        elif forbid_resonance_crossing:
+            raise ValueError("forbid_resonance_crossing needs 4 to 8192 recorded turns (n_passes 5 to 8193), "
+                             "no compact_every and no CSR elements")
     wl, wedges = wedge_lattice(lattice, locs, fire)
     z_end = np.cumsum([e.length for e in lattice.elements])
     wl_end = np.cumsum([e.length for e in wl.elements])
@@ -146,32 +173,52 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
             st.append({"k": k, "side": side, "sign": sign, "start": starts[side], "interval": delta_step_size * sign,
                        "limit": limits[side], "lost": sign * 1.7976931348623157e308 / 2, "survived": 0.0,
                        "survivor": False, "loser": False, "lost_on_pass": -1, "x_lost": 0.0, "y_lost": 0.0,
-                       "s_lost": 0.0, "delta_lost_at": 0.0, "active": True})
+                       "s_lost": 0.0, "delta_lost_at": 0.0, "active": True, "nux": 0.0, "nuy": 0.0})
     effort = 0.0
+    nominal = None
+    if forbid_resonance_crossing and tune_window is not None:
+        # the nominal tunes: a zero-delta trial at each element (momentumAperture.c:515-538)
+        lp, _, _, eff, tunes = _track_trials(wl, wedges, st, [(2 * k, 0.0) for k in range(len(locs))], p_central,
+                                             n_passes, x_initial, y_initial, device, 0, track_trials, fiducialize,
+                                             tune_window)
+        effort += eff
+        nominal = list(zip(*tunes)) if tunes is not None else None
+        if nominal is None or (lp >= 0).any() or not all(_tunes_found(nu) for nu in nominal):
+            raise RuntimeError("Fiducial particle tune is undefined. (momentumAperture.c:529-533)")
     for split in range(splits + 1):
         trials = []  # (scan index, delta)
         for j, s in enumerate(st):
             if s["active"]:
                 trials += [(j, d) for d in scan_deltas(s["start"], s["interval"], s["limit"])]
         if trials:
-            lost_pass, x_l, y_l, dpl, lost_elem, eff = _track_trials(wl, wedges, st, trials, p_central, n_passes,
-                                                                     x_initial, y_initial, device, compact_every,
-                                                                     track_trials, fiducialize)
+            lost_pass, c, lost_elem, eff, tunes = _track_trials(wl, wedges, st, trials, p_central, n_passes,
+                                                                x_initial, y_initial, device, compact_every,
+                                                                track_trials, fiducialize, tune_window)
             effort += eff
+            x_l, y_l, s_fin, dpl = c[:, 0], c[:, 2], c[:, 4], c[:, 5]
             done = set()
             for t, (j, d) in enumerate(trials):
                 if j in done:
                     continue
                 s = st[j]
+                nu = (float(tunes[0][t]), float(tunes[1][t])) if tunes is not None else (-1.0, -1.0)
                 if lost_pass[t] >= 0:
                     s.update(lost_on_pass=int(lost_pass[t]), x_lost=float(x_l[t]), y_lost=float(y_l[t]),
                              delta_lost_at=float(dpl[t]), loser=True,
                              s_lost=float(wl_end[lost_elem[t]]) if lost_elem[t] >= 0 else 0.0)
                     s["lost"] = d
                     done.add(j)
+                elif nominal is not None and _crosses(nu, nominal[s["k"]]):
+                    # counted as lost with its final coordinates (momentumAperture.c:569-612)
+                    s.update(lost_on_pass=-1, x_lost=float(x_l[t]), y_lost=float(y_l[t]),
+                             delta_lost_at=(float(dpl[t]) - p_central) / p_central, loser=True,
+                             s_lost=float(s_fin[t]))
+                    s["lost"] = d
+                    done.add(j)
                 else:
                     s["survived"] = d
                     s["survivor"] = True
+                    s["nux"], s["nuy"] = nu
         for s in st:
             if not s["active"]:
                 continue
@@ -203,17 +250,32 @@ def momentum_aperture(lattice: Lattice, p_central: float, n_passes: int, x_initi
             row[label] = {"delta": s["survived"], "found": s["loser"], "lost_on_pass": s["lost_on_pass"],
                           "x_lost": s["x_lost"], "y_lost": s["y_lost"], "s_lost": s["s_lost"],
                           "delta_when_lost": s["delta_lost_at"],
-                          "delta_lost": s["lost"] if s["loser"] and abs(s["lost"]) < 1e300 else None}
+                          "delta_lost": s["lost"] if s["loser"] and abs(s["lost"]) < 1e300 else None,
+                          "nux": s["nux"], "nuy": s["nuy"]}
         out.append(row)
     return out, effort
 
 
+def _tunes_found(nu) -> bool:
+    return all(0.0 <= v <= 1.0 for v in nu)
+
+
+def _crosses(nu, nominal) -> bool:
+    """forbid_resonance_crossing's test (momentumAperture.c:569-590): no tunes,
+    or a different integer part of twice either tune (C truncation)."""
+    if not _tunes_found(nu):
+        return True
+    return int(2 * nu[0]) != int(2 * nominal[0]) or int(2 * nu[1]) != int(2 * nominal[1])
+
+
 def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_initial, device, compact_every,
-                  track_trials=None, fiducialize=False):
+                  track_trials=None, fiducialize=False, tune_window=None):
     """One engine run, one instance per trial: the trial's particle alone, or
     (fiducialize) the fiducial particle, ID 2t+1, then the trial's, ID 2t+2.
-    Returns the trials' loss passes, x, y and delta (at the end or at the
-    loss), loss elements and the effort."""
+    Returns the trials' loss passes, coordinates (at the end or at the
+    loss, n x 6), loss elements, the effort and, with tune_window = (first
+    record, records), the trials' tunes (nux, nuy) from the turn-by-turn
+    records (None when the tracker gives none)."""
     n = len(trials)
     per = 2 if fiducialize else 1
     coords = np.zeros((per * n, 6))
@@ -234,14 +296,21 @@ def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_init
         if fiducialize:
             overrides += [(wi, "START_PID", pid), (wi, "END_PID", pid)]
     beam = Beam(coords, ids)
+    tunes = None
     if track_trials is not None:
-        lost_pass, c, effort = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
+        got = track_trials(wl, offsets, overrides, beam, p_central, n_passes)
+        lost_pass, c, effort = got[:3]
+        if tune_window is not None and len(got) > 3:
+            tunes = (np.asarray(got[3][0], dtype=np.float64), np.asarray(got[3][1], dtype=np.float64))
         lost_elem = np.full(per * n, -1)
     else:
         with Tracker(wl, p_central, n_passes, device=device, compact_every=compact_every,
-                     fiducial_particles=1 if fiducialize else 0) as t:
+                     fiducial_particles=1 if fiducialize else 0, record_tbt=tune_window is not None) as t:
             t.load_ensemble(offsets, overrides)
             res = t.track(beam)
+            if tune_window is not None:
+                nu = t.tbt_tunes(*tune_window)  # rows in upload order: no compaction with record_tbt
+                tunes = (nu["nux"], nu["nuy"])
         order = np.argsort(res.ids)
         lost_pass, c, lost_elem, effort = res.lost_pass[order], res.coords[order], res.lost_element[order], res.effort
     if fiducialize:
@@ -249,7 +318,9 @@ def _track_trials(wl, wedges, st, trials, p_central, n_passes, x_initial, y_init
         if (lost_pass[0::2] == 0).any():
             raise RuntimeError("Fiducial particle lost. Don't know what to do. (momentumAperture.c:400-404)")
         lost_pass, c, lost_elem = lost_pass[1::2], c[1::2], lost_elem[1::2]
-    return lost_pass, c[:, 0], c[:, 2], c[:, 5], lost_elem, effort
+        if tunes is not None:
+            tunes = (tunes[0][1::2], tunes[1][1::2])
+    return lost_pass, c, lost_elem, effort, tunes
 
 
 def _has_wildcards(pattern: str) -> bool:

@@ -440,9 +440,8 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, ap
     (momentumAperture.c:189-212, :692-714), or output_mode 1, one row per
     element and side, negative (direction -1) first (:141-160, :715-731);
     output_mode 2 from local_momentum_acceptance rows, the two limits per
-    element (:163-180).
-    nuxLost/nuyLost are -1: tunes are only found with
-    forbid_resonance_crossing, which is not built."""
+    element (:163-180).  nuxLost/nuyLost are the last survivor's tunes
+    (-1 where rows carry none)."""
     n = len(rows)
     occ = [r["occurrence"] for r in rows] if rows and "occurrence" in rows[0] else _occurrences(rows)
     if output_mode == 1:
@@ -459,8 +458,8 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, ap
                 ("xLost", "double", [r[sd]["x_lost"] for r, _, _, sd in sides], {"units": "m"}),
                 ("yLost", "double", [r[sd]["y_lost"] for r, _, _, sd in sides], {"units": "m"}),
                 ("deltaLost", "double", [r[sd]["delta_when_lost"] for r, _, _, sd in sides], {}),
-                ("nuxLost", "double", [-1.0] * len(sides), {}),
-                ("nuyLost", "double", [-1.0] * len(sides), {})]
+                ("nuxLost", "double", [r[sd].get("nux", -1.0) for r, _, _, sd in sides], {}),
+                ("nuyLost", "double", [r[sd].get("nuy", -1.0) for r, _, _, sd in sides], {})]
         write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
                    append=append)
         return
@@ -490,8 +489,8 @@ def write_momentum_aperture(path, rows, step=1, mode="binary", output_mode=0, ap
                  (f"xLost{label}", "double", [r[side]["x_lost"] for r in rows], {"units": "m"}),
                  (f"yLost{label}", "double", [r[side]["y_lost"] for r in rows], {"units": "m"}),
                  (f"deltaLost{label}", "double", [r[side]["delta_when_lost"] for r in rows], {}),
-                 (f"nuxLost{label}", "double", [-1.0] * n, {}),
-                 (f"nuyLost{label}", "double", [-1.0] * n, {})]
+                 (f"nuxLost{label}", "double", [r[side].get("nux", -1.0) for r in rows], {}),
+                 (f"nuyLost{label}", "double", [r[side].get("nuy", -1.0) for r in rows], {})]
     write_sdds(path, [("Step", "long", step, {})], cols, mode, description="Momentum aperture search",
                    append=append)
 

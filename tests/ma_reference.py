@@ -170,3 +170,95 @@ def oracle_instances(oracle):
                     lost[k] = int(r[7])
         return lost, coords, math.nan
     return run
+
+
+def serial_scan_with_tunes(run_trial, lattice, n_passes, forbid, x_initial=1e-5, y_initial=1e-5,
+                           delta_negative_limit=-0.10, delta_positive_limit=0.10, delta_step_size=0.0025,
+                           splits=1, steps_back=1, split_step_divisor=10, **select):
+    """The reference's scan (momentumAperture.c:456-657) with its tune logic
+    (:515-603): run_trial(lattice with the wedge, n_passes) -> (lost,
+    lost_on_pass, tunes or None).  With forbid, a zero-delta trial gives the
+    nominal tunes; a surviving trial without tunes, or with another integer
+    part of twice a tune, counts as lost (loss pass -1).  The last survivor's
+    tunes are kept (0 before any survivor, -1 when none were found).  Per
+    selected element and side: (deltaSurvived, deltaLost or None,
+    lostOnPass, nux, nuy)."""
+    locs = select_elements(lattice, **select)
+    wl, wedges = wedge_lattice(lattice, locs, 0 if n_passes == 1 else 1)
+    out = []
+    for k, _ in enumerate(locs):
+        nominal = None
+        if forbid:
+            lost, _, nominal = run_trial(_with_wedge(wl, wedges[k], x_initial, y_initial, 0.0), n_passes)
+            assert not lost and nominal is not None, "Fiducial particle tune is undefined"
+        row = []
+        for side in (0, 1):
+            sign = -1 if side == 0 else 1
+            delta_start = 0.0
+            delta_lost = sign * 1.7976931348623157e308 / 2
+            interval = delta_step_size * sign
+            limit = delta_negative_limit if side == 0 else delta_positive_limit
+            survived, lost_on_pass, nu = 0.0, -1, (0.0, 0.0)
+            for split in range(splits + 1):
+                delta = delta_start
+                while abs(delta) <= abs(limit):
+                    lost, lp, tunes = run_trial(_with_wedge(wl, wedges[k], x_initial, y_initial, delta), n_passes)
+                    t = tunes if tunes is not None else (-1.0, -1.0)
+                    if not lost and forbid and (not all(0 <= v <= 1 for v in t) or
+                                                int(2 * t[0]) != int(2 * nominal[0]) or
+                                                int(2 * t[1]) != int(2 * nominal[1])):
+                        lost, lp = True, -1
+                    if lost:
+                        lost_on_pass, delta_lost = lp, delta
+                        break
+                    survived, nu = delta, t
+                    delta += interval
+                delta_start = survived - steps_back * interval
+                interval /= split_step_divisor
+                delta_start += interval
+                limit = delta_lost
+                if (delta_start < 0 and sign == 1) or (delta_start > 0 and sign == -1):
+                    delta_start = 0
+            row.append((survived, delta_lost if abs(delta_lost) < 1e300 else None, lost_on_pass, nu[0], nu[1]))
+        out.append(row)
+    return out
+
+
+def synthetic_tunes(dp: float):
+    """Stand-in tunes of a surviving trial with momentum offset dp, for
+    testing the tune bookkeeping on the CPU: x near the half integer with a
+    large chromaticity, y far from it."""
+    return ((0.455 + 30.0 * dp) % 1.0, 0.277 + 5.0 * dp)
+
+
+def oracle_trials_with_tunes(oracle):
+    """oracle_trials plus stand-in tunes (synthetic_tunes of the instance's
+    wedge offset) for every surviving row, -1 for lost rows."""
+    base = oracle_trials(oracle)
+
+    def run(wl, offsets, overrides, beam, p_central, n_passes):
+        lost, coords, effort = base(wl, offsets, overrides, beam, p_central, n_passes)
+        dps = np.zeros(len(offsets) - 1)
+        for (_, name, values) in overrides:
+            if name == "DP":
+                dps += np.asarray(values)
+        nux = np.full(beam.n, -1.0)
+        nuy = np.full(beam.n, -1.0)
+        for t in range(len(offsets) - 1):
+            for r in range(offsets[t], offsets[t + 1]):
+                if lost[r] < 0:
+                    nux[r], nuy[r] = synthetic_tunes(dps[t])
+        return lost, coords, effort, (nux, nuy)
+    return run
+
+
+def oracle_run_trial(oracle, p_central):
+    """run_trial for serial_scan_with_tunes on a CPU oracle with
+    synthetic_tunes of the wedge's DP."""
+    def run(lat, n_passes):
+        dp = sum(e.params.get("DP", 0.0) for e in lat.elements if e.type == "MALIGN")  # one wedge is set
+        rows, n_left, _ = oracle.track(lat, np.zeros((1, 6)), np.array([1]), p_central, n_passes)[:3]
+        if n_left == 0:
+            return True, int(rows[0, 7]), None
+        return False, -1, synthetic_tunes(dp)
+    return run

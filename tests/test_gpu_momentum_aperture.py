@@ -79,3 +79,39 @@ def test_local_acceptance_matches_serial_restatement(ref_b2e, passes):
     for row, s in zip(rows, serial):
         for side, label in ((0, "negative"), (1, "positive")):
             assert (row[label]["delta"], row[label]["delta_lost"]) == s[side], (row["name"], label)
+
+
+def _engine_run_trial(n_passes_window_first=2):
+    """run_trial for ma_reference.serial_scan_with_tunes on the engine: one
+    particle per run, its tunes from the turns recorded after the firing
+    pass (records 2..n_passes)."""
+    from elegant_b200.beam import Beam
+
+    def run(lat, n_passes):
+        with Tracker(lat, P0, n_passes, record_tbt=True) as t:
+            res = t.track(Beam(np.zeros((1, 6)), np.array([1], dtype=np.int64)))
+            if res.lost_pass[0] >= 0:
+                return True, int(res.lost_pass[0]), None
+            nu = t.tbt_tunes(n_passes_window_first, n_passes - 1)
+        v = (float(nu["nux"][0]), float(nu["nuy"][0]))
+        return False, -1, v if all(0 <= x <= 1 for x in v) else None
+    return run
+
+
+@pytest.mark.parametrize("forbid", [False, True])
+def test_momentum_aperture_tunes_match_serial_scan(forbid):
+    """The last survivor's tunes (nuxLost/nuyLost) and forbid_resonance_crossing
+    (momentumAperture.c:515-603) in the batched search against the
+    reference's scan run one trial at a time on the engine with the same
+    turn-by-turn NAFF; near-half-integer horizontal tune (0.455)."""
+    from ma_reference import serial_scan_with_tunes
+    lat = w.fodo_ring()
+    kw = dict(include_type_pattern="K*", process_elements=3, delta_step_size=0.0015, splits=1)
+    serial = serial_scan_with_tunes(_engine_run_trial(), lat, 64, forbid, **kw)
+    rows, _ = momentum_aperture(lat, P0, 64, forbid_resonance_crossing=forbid, **kw)
+    for row, s in zip(rows, serial):
+        for side, label in ((0, "negative"), (1, "positive")):
+            got = row[label]
+            assert (got["delta"], got["delta_lost"], got["lost_on_pass"], got["nux"], got["nuy"]) == s[side], \
+                (row["name"], label)
+            assert 0.4 < got["nux"] < 0.6 and 0.2 < got["nuy"] < 0.35

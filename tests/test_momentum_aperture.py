@@ -150,3 +150,27 @@ def test_output_mode_2_layout(tmp_path):
     assert list(c) == ["ElementName", "s", "ElementType", "ElementOccurence", "deltaPositive", "deltaNegative"]
     assert list(c["deltaNegative"]) == [-0.01] and list(c["deltaPositive"]) == [1.7976931348623157e308]
     assert page["parameters"]["Step"] == 3 and list(c["ElementOccurence"]) == [2]
+
+
+def test_forbid_resonance_crossing_bookkeeping():
+    """forbid_resonance_crossing (momentumAperture.c:515-603) on the CPU with
+    stand-in tunes (tune x crosses the half integer at delta = +0.0015 and
+    -0.0152): the batched search against the reference's scan, losses,
+    crossings and the last survivor's tunes; without forbid the tunes are
+    only reported."""
+    from ma_reference import oracle_run_trial, oracle_trials_with_tunes, serial_scan_with_tunes
+    lat = w.fodo_ring()
+    kw = dict(include_type_pattern="KQUAD", process_elements=2, delta_step_size=0.002, splits=2)
+    ref = RefOracle("b2e")
+    for forbid in (True, False):
+        serial = serial_scan_with_tunes(oracle_run_trial(ref, P0), lat, 40, forbid, **kw)
+        rows, _ = momentum_aperture(lat, P0, 40, track_trials=oracle_trials_with_tunes(ref),
+                                    forbid_resonance_crossing=forbid, **kw)
+        for row, s in zip(rows, serial):
+            for side, label in ((0, "negative"), (1, "positive")):
+                got = row[label]
+                assert (got["delta"], got["delta_lost"], got["lost_on_pass"], got["nux"], got["nuy"]) == s[side]
+        if forbid:
+            assert all(r["positive"]["delta"] < 0.0015 and r["positive"]["lost_on_pass"] == -1 for r in rows)
+        else:
+            assert all(r["positive"]["nux"] > 0.5 for r in rows)
