@@ -30,8 +30,13 @@ static const b2e_param_map map_edrift[] = {{"L", B2E_EDRIFT_L}, END_MAP};
   {"L", B2E_KMULT_L}, {"TILT", B2E_KMULT_TILT}, {"DX", B2E_KMULT_DX}, {"DY", B2E_KMULT_DY}, {"DZ", B2E_KMULT_DZ}, \
       {"FSE", B2E_KMULT_FSE}, {"N_KICKS", B2E_KMULT_N_KICKS}, {"N_SLICES", B2E_KMULT_N_SLICES},                    \
       {"INTEGRATION_ORDER", B2E_KMULT_INTEGRATION_ORDER}, {"SYNCH_RAD", B2E_KMULT_SYNCH_RAD},                     \
-      {"ISR", B2E_KMULT_ISR}, {"ISR1PART", B2E_KMULT_ISR1PART}
-static const b2e_param_map map_kquad[] = {KMULT_COMMON, {"K1", B2E_KMULT_K}, END_MAP};
+      {"ISR", B2E_KMULT_ISR}, {"ISR1PART", B2E_KMULT_ISR1PART}, {"HKICK", B2E_KMULT_HKICK},                        \
+      {"VKICK", B2E_KMULT_VKICK}, {"HCALIBRATION", B2E_KMULT_HCALIBRATION},                                       \
+      {"VCALIBRATION", B2E_KMULT_VCALIBRATION}, {"BORE", B2E_KMULT_BORE}, {"B", B2E_KMULT_B},                     \
+      /* read by no tracking code: optimizer flags, PITCH/YAW under MALIGN_METHOD 0 */                           \
+      {"HSTEERING", -1}, {"VSTEERING", -1}, {"SQRT_ORDER", -1}, {"PITCH", -1}, {"YAW", -1}
+static const b2e_param_map map_kquad[] = {KMULT_COMMON, {"K1", B2E_KMULT_K}, {"SR_IN_ORDINARY_MATRIX", -1},
+                                          {"TRACKING_MATRIX", -1}, END_MAP};
 static const b2e_param_map map_ksext[] = {KMULT_COMMON,
                                           {"K2", B2E_KMULT_K},
                                           {"K1", B2E_KMULT_K1_OF_KSEXT},

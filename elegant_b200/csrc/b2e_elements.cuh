@@ -170,8 +170,8 @@ struct RadSite {
 };
 
 /* radiation after a kick (multipole.c:1320-1349): the momenta scaled by
- * 1/(1+delta), F2 from this substep's kick, the classical loss with
- * SYNCH_RAD and a Gaussian ISR kick with ISR; xkick = ykick = 0 */
+ * 1/(1+delta), F2 from this substep's kick and the steering kicks, the
+ * classical loss with SYNCH_RAD and a Gaussian ISR kick with ISR */
 __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &dp, double dqx, double dqy,
                                                 double xp, double yp, const double *c, int step, int nSub,
                                                 unsigned flags, const RadSite &rs, int slice) {
@@ -183,7 +183,7 @@ __device__ __forceinline__ void kmult_radiation(double &qx, double &qy, double &
   dqx = dqx / kfrac;
   dqy = dqy / kfrac;
   {
-    const double a = dqx / drift - 0.0 / drift, b = dqy / drift + 0.0 / drift;
+    const double a = dqx / drift - rs.rc[RK_XKICK] / drift, b = dqy / drift + rs.rc[RK_YKICK] / drift;
     F2 = a * a + b * b;
   }
   dsFactor = sqrt((1 + xp * xp) + yp * yp);
@@ -249,6 +249,22 @@ __device__ __forceinline__ int kmult_kick(double x, double y, double &xp, double
         dqx = dqx - j1 * fy;
         dqy = dqy + j1 * fx;
       }
+    }
+  }
+  if (RAD && (e.flags & EF_STEERING)) {
+    /* HKICK/VKICK as order-0 canonical kicks, normal then skew
+     * (multipole.c:1281-1284): sum_Fy = 1, sum_Fx = 0; skew swaps them and
+     * negates, so the vertical kick enters qy through -1 */
+    const double kfrac = rs.rc[RK_KFRAC0 + step], xk = rs.rc[RK_XKICK], yk = rs.rc[RK_YKICK];
+    if (xk != 0) {
+      const double k = -xk * kfrac;
+      qx = qx - k * 1.0;
+      qy = qy + k * 0.0;
+    }
+    if (yk != 0) {
+      const double k = -yk * kfrac;
+      qx = qx - k * 0.0;
+      qy = qy + k * -1.0;
     }
   }
   if (!momenta_to_slopes(xp, yp, qx, qy, dp))

@@ -55,6 +55,7 @@ enum {
 #define EF_EDGE_ORDER2 0x2000   /* CSBEND: edges by the second-order map (EDGE_ORDER >= 2; BendExtra) */
 #define EF_FIELD 0x4000         /* CSBEND: K1/K2 field terms (coefficients in the DevRad table) */
 #define EF_ETILT 0x8000         /* CSBEND: ETILT exit offsets (BendExtra) */
+#define EF_STEERING 0x10000     /* KMULT: HKICK/VKICK steering kicks (per-part kicks in the DevRad table) */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -111,16 +112,19 @@ typedef struct {
 } BendExtra;
 
 
-/* Radiation constants of a KMULT / CSBEND, and a CSBEND's field-expansion
- * coefficients, in a table beside the element records ([instance][element]
- * DevRad): only lattices that radiate or have bends with K1/K2 read it (the
- * ring kernel's RAD instantiation), so the records the ring kernel stages in
- * shared memory stay small. */
+/* Radiation constants of a KMULT / CSBEND, a KMULT's steering kicks and a
+ * CSBEND's field-expansion coefficients, in a table beside the element
+ * records ([instance][element] DevRad): only lattices that radiate, steer
+ * in a KQUAD/KSEXT or have bends with K1/K2 read it (the ring kernel's RAD
+ * instantiation), so the records the ring kernel stages in shared memory
+ * stay small. */
 #define B2E_NRAD 36
 #define RK_KFRAC0 0     /* KMULT: kickFrac[j], j = 0..7 */
 #define RK_RAD 8        /* rad_coef (multipole.c:789) */
 #define RK_ISR 9        /* isr_coef, > 0 only when ISR is applied (:790-795) */
 #define RK_DRIFT 10     /* slice drift length (:1189) */
+#define RK_XKICK 11     /* HKICK*HCALIBRATION/n_parts, the steering kick per slice (:785, :1190) */
+#define RK_YKICK 12     /* VKICK*VCALIBRATION/n_parts (:786, :1191) */
 #define RB_RAD 0        /* CSBEND: rad_coef (csbend.c:967-970) */
 #define RB_ISR 1        /* isrConstant, > 0 only when ISR is applied (:972-975) */
 #define RB_SLICE 2      /* s = length / N_SLICES, for dsISR (:1614) */

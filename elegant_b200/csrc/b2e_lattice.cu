@@ -103,6 +103,8 @@ void element_defaults(int type, double *p) {
     p[B2E_KMULT_N_SLICES] = 1;          /* track_data.c:1234, :1130 */
     p[B2E_KMULT_INTEGRATION_ORDER] = 4; /* :1253, :1153 */
     p[B2E_KMULT_ISR1PART] = 1;          /* :1257, :1157 */
+    p[B2E_KMULT_HCALIBRATION] = 1;      /* :1238, :1138 */
+    p[B2E_KMULT_VCALIBRATION] = 1;      /* :1239, :1139 */
     break;
   case B2E_CSBEND:
   case B2E_CSRCSBEND:
@@ -209,7 +211,16 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
   d.c[KM_ORDER] = el.type == B2E_KQUAD ? 1 : 2;
   d.c[KM_NSLICES] = (double)nSlices;
   d.c[KM_NSUB] = nSub;
-  KnL = (p[B2E_KMULT_K] * L) * (1 + p[B2E_KMULT_FSE]);
+  if (p[B2E_KMULT_BORE] != 0) {
+    /* strength from the pole-tip field (multipole.c:771-773, :834-836):
+     * KnL = n! B(a)/a^n * L/(B rho) * (1+FSE), electrons (charge e_mks) */
+    const double rigidity = kE_MKS / (kME_MKS * kC_MKS * Po), a = p[B2E_KMULT_BORE];
+    if (el.type == B2E_KQUAD)
+      KnL = ((p[B2E_KMULT_B] / a) * rigidity * L) * (1 + p[B2E_KMULT_FSE]);
+    else
+      KnL = ((2 * p[B2E_KMULT_B] / (a * a)) * rigidity * L) * (1 + p[B2E_KMULT_FSE]);
+  } else
+    KnL = (p[B2E_KMULT_K] * L) * (1 + p[B2E_KMULT_FSE]);
   drift = L / nSlices;
   for (int j = 0; j < 8; j++) {
     d.c[KM_DSH0 + j] = j < nSub ? drift * drift_frac[j] : 0;
@@ -266,6 +277,13 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
     r.c[RK_RAD] = rad_coef;
     r.c[RK_ISR] = isr_coef;
     r.c[RK_DRIFT] = drift;
+    /* steering (multipole.c:785-786, :1190-1191): applied as dipole kicks
+     * -xkick*kickFrac[step] after the multipole kicks (:1281-1284), and
+     * part of F2 in the radiation block (:1333) */
+    r.c[RK_XKICK] = (p[B2E_KMULT_HKICK] * p[B2E_KMULT_HCALIBRATION]) / nSlices;
+    r.c[RK_YKICK] = (p[B2E_KMULT_VKICK] * p[B2E_KMULT_VCALIBRATION]) / nSlices;
+    if (r.c[RK_XKICK] != 0 || r.c[RK_YKICK] != 0)
+      d.flags |= EF_STEERING;
     for (int j = 0; j < 8; j++)
       r.c[RK_KFRAC0 + j] = j < nSub ? kick_frac[j] : 0;
     if ((rad_coef != 0 || isr_coef != 0) && drift != 0)

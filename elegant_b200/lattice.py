@@ -38,7 +38,8 @@ TYPE_NAMES = {nat.DRIF: "DRIF", nat.EDRIFT: "EDRIFT", nat.KQUAD: "KQUAD", nat.KS
               nat.WATCH: "WATCH"}
 
 _KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, "N_SLICES": 8,
-          "INTEGRATION_ORDER": 9, "SYNCH_RAD": 12, "ISR": 13, "ISR1PART": 14}
+          "INTEGRATION_ORDER": 9, "SYNCH_RAD": 12, "ISR": 13, "ISR1PART": 14, "HKICK": 15, "VKICK": 16,
+          "HCALIBRATION": 17, "VCALIBRATION": 18, "BORE": 19, "B": 20}
 _BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "DY": 7, "DZ": 8, "FSE": 9,
          "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
          "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18, "NONLINEAR": 19, "SYNCH_RAD": 35, "ISR": 36,
@@ -70,6 +71,11 @@ SLOTS = {
                 "EXCLUDE_SLOPES": 12, "FLUSH_INTERVAL": 13, "USE_DISCONNECT": 14, "INDEX_OFFSET": 15,
                 "REFERENCE_FREQUENCY": 16, "AUTO_REFERENCE": 17},
 }
+# parameters the reference's tracking of these elements never reads (optimizer
+# flags, matrix-only options, PITCH/YAW under MALIGN_METHOD 0, malign_mat.c:494-505):
+# accepted and kept, without an engine slot
+_KMULT_IGNORED = ("HSTEERING", "VSTEERING", "SQRT_ORDER", "PITCH", "YAW")
+IGNORED = {nat.KQUAD: _KMULT_IGNORED + ("SR_IN_ORDINARY_MATRIX", "TRACKING_MATRIX"), nat.KSEXT: _KMULT_IGNORED}
 # string-valued parameters, kept beside the numeric slots
 STRING_PARAMS = {nat.WATCH: ("FILENAME", "LABEL")}
 # WATCH MODE strings (matched by prefix, as elegant's match_string) -> B2E_WATCH_MODE codes
@@ -77,8 +83,8 @@ WATCH_MODES = (("coord", 0), ("param", 1), ("centroid", 2), ("fft", 3))
 
 # defaults from the reference's parameter tables (only nonzero ones listed)
 DEFAULTS = {
-    nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1},
-    nat.KSEXT: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1},
+    nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1, "HCALIBRATION": 1, "VCALIBRATION": 1},
+    nat.KSEXT: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1, "HCALIBRATION": 1, "VCALIBRATION": 1},
     nat.CSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
                  "EDGE_ORDER": 1, "NONLINEAR": 1, "ISR1PART": 1},
     nat.CSRCSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
@@ -124,7 +130,7 @@ class Element:
                 if not codes:
                     raise LatticeError(f"WATCH {self.name}: unknown MODE {v!r}")
                 v = codes[0]
-            if k not in SLOTS[code]:
+            if k not in SLOTS[code] and k not in IGNORED.get(code, ()):
                 raise LatticeError(f"parameter {k} of {self.type} {self.name} is not supported by the engine")
             if k == "N_KICKS" and code in (nat.CSBEND, nat.CSRCSBEND):
                 k = "N_SLICES"  # alias sharing storage (track_data.c:1925, :2006)
@@ -151,7 +157,8 @@ class Element:
         for k, v in DEFAULTS.get(self.code, {}).items():
             p[SLOTS[self.code][k]] = float(v)
         for k, v in self.params.items():
-            p[SLOTS[self.code][k]] = v
+            if k in SLOTS[self.code]:
+                p[SLOTS[self.code][k]] = v
         return p
 
     def to_lte(self) -> str:

@@ -92,6 +92,12 @@ extern "C" {
 #define B2E_KMULT_SYNCH_RAD 12    /* classical synchrotron radiation (multipole.c:1320-1349) */
 #define B2E_KMULT_ISR 13          /* incoherent synchrotron radiation (quantum excitation) */
 #define B2E_KMULT_ISR1PART 14     /* ISR also for a one-particle beam (default 1; 0 is not supported) */
+#define B2E_KMULT_HKICK 15        /* horizontal steering kick (rad), spread over the integrator's kicks */
+#define B2E_KMULT_VKICK 16        /* vertical steering kick (rad) */
+#define B2E_KMULT_HCALIBRATION 17 /* factor on HKICK (default 1) */
+#define B2E_KMULT_VCALIBRATION 18 /* factor on VKICK (default 1) */
+#define B2E_KMULT_BORE 19         /* bore radius (m); nonzero: the strength comes from the pole-tip field B */
+#define B2E_KMULT_B 20            /* pole-tip field (T), used when BORE is nonzero */
 /* CSBEND (csbend_param, track_data.c:1893) and CSRCSBEND (csrcsbend_param, :1982) */
 #define B2E_BEND_L 0
 #define B2E_BEND_ANGLE 1

@@ -413,7 +413,7 @@ static void canonical_kick(double *qx, double *qy, double *dqx, double *dqy, dou
 static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma,
                         int pass, int elem) {
   const double *p = e->p;
-  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt, rad_coef = 0, isr_coef;
+  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt, rad_coef = 0, isr_coef, xkick, ykick;
   long order[3] = {0, 0, 0}, nSlices, n_kicks, ip, itop;
   int skew[3] = {0, 0, 0}, integ, nSub, radblock;
   MultAp ap;
@@ -426,12 +426,20 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
   dy = p[B2E_KMULT_DY];
   dz = p[B2E_KMULT_DZ];
   tilt = p[B2E_KMULT_TILT];
+  /* multipole.c:771-773, :834-837: with a bore radius, the strength from the pole-tip field */
   if (e->type == B2E_KQUAD) {
     order[0] = 1;
-    KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
+    if (p[B2E_KMULT_BORE])
+      KnL[0] = p[B2E_KMULT_B] / p[B2E_KMULT_BORE] * (E_MKS / (ME_MKS * C_MKS * Po)) * drift * (1 + p[B2E_KMULT_FSE]);
+    else
+      KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
   } else {
     order[0] = 2;
-    KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
+    if (p[B2E_KMULT_BORE])
+      KnL[0] = 2 * p[B2E_KMULT_B] / SQR(p[B2E_KMULT_BORE]) * (E_MKS / (ME_MKS * C_MKS * Po)) * drift *
+               (1 + p[B2E_KMULT_FSE]);
+    else
+      KnL[0] = p[B2E_KMULT_K] * drift * (1 + p[B2E_KMULT_FSE]);
     if (p[B2E_KMULT_K1_OF_KSEXT]) {
       KnL[1] = p[B2E_KMULT_K1_OF_KSEXT] * drift;
       order[1] = 1;
@@ -450,6 +458,9 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
     } else
       nSlices = n_kicks;
   }
+  /* steering, per slice (multipole.c:785-786, :1190-1191) */
+  xkick = p[B2E_KMULT_HKICK] * p[B2E_KMULT_HCALIBRATION] / nSlices;
+  ykick = p[B2E_KMULT_VKICK] * p[B2E_KMULT_VCALIBRATION] / nSlices;
   setup_mult_ap(&ap, -tilt, ma);
   /* entrance misalignment, mode 0 face 1 */
   if (dx || dy || dz)
@@ -514,19 +525,27 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
             for (io = 0; io < 3; io++)
               if (KnL[io])
                 canonical_kick(&qx, &qy, &dqx, &dqy, x, y, order[io], KnL[io] / nSlices * kf[step], skew[io]);
+            {
+              /* steering kicks, not part of delta_qx/delta_qy (multipole.c:1281-1284) */
+              double ux = 0, uy = 0;
+              if (xkick)
+                canonical_kick(&qx, &qy, &ux, &uy, x, y, 0, -xkick * kf[step], 0);
+              if (ykick)
+                canonical_kick(&qx, &qy, &ux, &uy, x, y, 0, -ykick * kf[step], 1);
+            }
             if (!m2s(&xp, &yp, qx, qy, dpv)) {
               lost = 1;
               break;
             }
             if (radblock && dr) {
-              /* multipole.c:1320-1349, xkick = ykick = 0 */
+              /* multipole.c:1320-1349 */
               double deltaFactor, F2, dsFactor, dsISRFactor;
               qx /= (1 + dpv);
               qy /= (1 + dpv);
               deltaFactor = SQR(1 + dpv);
               dqx /= kf[step];
               dqy /= kf[step];
-              F2 = SQR(dqx / dr - 0.0 / dr) + SQR(dqy / dr + 0.0 / dr);
+              F2 = SQR(dqx / dr - xkick / dr) + SQR(dqy / dr + ykick / dr);
               dsFactor = sqrt(1 + SQR(xp) + SQR(yp));
               dsISRFactor = dsFactor * dr / (nSub - 1);
               dsFactor *= dr * kf[step];

@@ -489,3 +489,57 @@ def test_watch_budget_is_enforced():
         t.set_watch(1000)
         with pytest.raises(EngineError, match="WATCH"):
             t.track(beam)
+
+
+@pytest.mark.parametrize("case", ["plain", "synch_rad"])
+def test_ring_with_steering(ref_b2e, case):
+    """KQUAD/KSEXT correctors (HKICK, VKICK, calibrations; multipole.c:785-786,
+    :1190-1191, :1281-1284), a pole-tip strength from BORE and B (:771-773,
+    :834-837), and with SYNCH_RAD the steering kicks in F2 (:1333): 60 turns
+    with losses, bit-identical to the reference."""
+    from test_oracle_pin import _ring_with_steering
+    base = None
+    if case == "synch_rad":
+        base = Lattice([Element(e.name, e.type, dict(e.params, SYNCH_RAD=1)) if e.type in ("KQUAD", "KSEXT") else e
+                        for e in w.fodo_ring().elements])
+    lat = _ring_with_steering(base)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=61).coords, _lossy_beam(150, seed=62).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff
+
+
+def test_ensemble_of_corrector_settings(ref_b2e):
+    """Per-instance HKICK/VKICK overrides (an ensemble of orbit-corrector
+    settings): each instance equal to the reference run with its settings."""
+    lat = w.fodo_ring()
+    quads = [i for i, e in enumerate(lat.elements) if e.type == "KQUAD"]
+    n_inst = 5
+    rng = np.random.default_rng(17)
+    overrides = []
+    for i in quads[:6]:
+        overrides.append((i, "HKICK", rng.normal(0, 1e-4, n_inst)))
+        overrides.append((i, "VKICK", rng.normal(0, 1e-4, n_inst)))
+    overrides[0][2][0] = 0.0  # an instance without that corrector
+    counts = [40, 64, 90, 33, 128]
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    beam = Beam(_lossy_beam(int(offsets[-1]), seed=63).coords * 0.5, np.arange(1, int(offsets[-1]) + 1))
+    with Tracker(lat, w.ring_p_central(), 15) as t:
+        t.load_ensemble(offsets, overrides)
+        res = t.track(beam)
+    for k in range(n_inst):
+        sl = slice(offsets[k], offsets[k + 1])
+        els = []
+        for j, e in enumerate(lat.elements):
+            params = dict(e.params)
+            for (ie, name, vals) in overrides:
+                if ie == j:
+                    params[name] = float(vals[k])
+            els.append(Element(e.name, e.type, params))
+        rows, nl, _, _ = ref_b2e.track(Lattice(els), beam.coords[sl], beam.ids[sl], w.ring_p_central(), 15)
+        sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
+                        int((res.lost_pass[sl] < 0).sum()), 0.0)
+        assert_parity(sub, rows, nl)

@@ -465,3 +465,47 @@ def test_port_reproduces_reference_with_watches(math):
     first = rows[(rows[:, 0] == w2) & (rows[:, 1] == 0)]
     lost_early = {int(i) for i, lp in zip(r1[:, 6], r1[:, 7]) if lp == 0}
     assert set(first[:, 2].astype(int)) <= set(beam.ids) - (lost_early - set(first[:, 2].astype(int)))
+
+
+def _ring_with_steering(base=None):
+    """The ring with correctors in its multipoles (multipole.c:785-786,
+    :848-849, :1190-1191, :1281-1284): HKICK/VKICK with calibrations on the
+    quadrupoles and sextupoles, one quadrupole tilted, one strength from a
+    pole-tip field and bore (:771-773, :834-837), and parameters the tracking
+    ignores (HSTEERING, PITCH under MALIGN_METHOD 0)."""
+    from elegant_b200 import Element, Lattice
+    els, k = [], 0
+    for e in (base or w.fodo_ring()).elements:
+        if e.type in ("KQUAD", "KSEXT"):
+            extra = [{"HKICK": 2e-4, "HSTEERING": 1}, {"VKICK": -1.5e-4, "VCALIBRATION": 1.1},
+                     {"HKICK": -1e-4, "VKICK": 5e-5, "HCALIBRATION": 0.9, "TILT": 0.01, "PITCH": 1e-3},
+                     {}][k % 4]
+            if e.type == "KQUAD" and k == 5:
+                extra = {"BORE": 0.02, "B": 0.2 * e.params["K1"] / 1.2, "FSE": 1e-3}
+            if e.type == "KSEXT" and k == 7:
+                extra = {"BORE": 0.03, "B": 0.01, "HKICK": 1e-4}
+            e = Element(e.name + str(k), e.type, dict(e.params, **extra))
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("case", ["plain", "synch_rad"])
+def test_port_reproduces_reference_steering(math, case):
+    """KQUAD/KSEXT HKICK, VKICK, calibrations and pole-tip strengths, with
+    the steering kicks inside the radiation's F2 when SYNCH_RAD is on."""
+    base = None
+    if case == "synch_rad":
+        from elegant_b200 import Element, Lattice
+        base = Lattice([Element(e.name, e.type, dict(e.params, SYNCH_RAD=1)) if e.type in ("KQUAD", "KSEXT") else e
+                        for e in w.fodo_ring().elements])
+    lat = _ring_with_steering(base)
+    beam = _mixed_beam(61)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    r0, n0, _, _ = RefOracle(math).track(base or w.fodo_ring(), beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
