@@ -178,10 +178,18 @@ static int fill_parameters(b2e_element *el, const ELEMENT_LIST *eptr, const b2e_
     case IS_STRING: {
       const char *s = *(char *const *)where;
       is_default = (!s && !par[i].string) || (s && par[i].string && strcmp(s, par[i].string) == 0);
-      /* RFCA FIDUCIAL: unset means "tmean", the mode the engine implements */
-      if (!is_default && eptr->type == T_RFCA && strcmp(par[i].name, "FIDUCIAL") == 0 && s &&
-          strcmp(s, "tmean") == 0)
-        is_default = 1;
+      /* RFCA FIDUCIAL: elegant's own parser (parseFiducialMode, simple_rfca.c:35-48) picks the
+       * mode; light, tmean and pmaximum go to the engine's slot, anything else declines */
+      if (eptr->type == T_RFCA && strcmp(par[i].name, "FIDUCIAL") == 0) {
+        const unsigned long mode = parseFiducialMode((char *)s);
+        if (mode & FID_MODE_LIGHT)
+          el->p[B2E_RFCA_FIDUCIAL] = B2E_FIDUCIAL_LIGHT;
+        else if (mode & FID_MODE_PMAX)
+          el->p[B2E_RFCA_FIDUCIAL] = B2E_FIDUCIAL_PMAXIMUM;
+        else if (mode & FID_MODE_TMEAN)
+          el->p[B2E_RFCA_FIDUCIAL] = B2E_FIDUCIAL_TMEAN;
+        is_default = (mode & (FID_MODE_LIGHT | FID_MODE_PMAX | FID_MODE_TMEAN)) != 0;
+      }
       break;
     }
     default:

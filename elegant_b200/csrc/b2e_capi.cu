@@ -772,7 +772,7 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
       ctx->launches++;
       CUDA_TRY(ctx, launch_fiducial(particle_view(ctx), ctx->d_inst_offsets.ptr, ctx->n_inst, ctx->d_elems.ptr, ne,
                                     stop_e, ctx->d_rf.ptr, ctx->lat.n_rf, ctx->opt.p_central,
-                                    ctx->opt.fiducial_particles, ctx->stream));
+                                    ctx->opt.fiducial_particles, ctx->d_flag.ptr, ctx->stream));
       next_rf++;
       /* the RFCA itself is tracked by the next ring launch */
       int rc = run_ring_range(ctx, p, stop_e, p, stop_e + 1);
@@ -836,6 +836,9 @@ static int track_impl(b2e_ctx *ctx, double *effort) {
   CUDA_TRY(ctx, cudaMemcpyAsync(counters, ctx->d_counters.ptr, sizeof(counters), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flag.ptr, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (flag & 2u)
+    return fail(ctx, B2E_ERR_DEVICE, "No available particle for RF cavity fiducialization (FIDUCIAL=pmaximum: "
+                "no particle after the first has a higher momentum)");
   if (flag)
     return fail(ctx, B2E_ERR_DEVICE, "device reported error flag 0x%x (RFCA fiducial missing)", flag);
   if (effort)

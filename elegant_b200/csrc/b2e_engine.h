@@ -147,6 +147,8 @@ typedef struct {
 #define RF_MATRIX 10    /* 1: matrix method (nonzero L, N_KICKS <= 0) */
 #define RF_DTLIGHT 11   /* RF_LENGTH / c */
 #define RF_DRIFT_ONLY 12 /* VOLT = 0: an exact drift over L (nothing for L = 0) */
+#define RF_FID_MODE 13  /* B2E_FIDUCIAL_* */
+#define RF_L_TOTAL 14   /* L, for the light fiducial's zEnd - L */
 
 /* WATCH constant slots */
 #define WA_START 0      /* first pass recorded */

@@ -49,7 +49,7 @@ cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticle
                            const int64_t *offs, int n_inst, int *alive_out, cudaStream_t stream);
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
-                            int64_t max_rows, cudaStream_t stream);
+                            int64_t max_rows, unsigned int *error_flag, cudaStream_t stream);
 /* one WATCH record [7][n]: x..delta and ID (double) of the live rows */
 cudaError_t launch_watch_copy(DevParticles P, const int64_t *ids, int64_t n, double *out, cudaStream_t stream);
 /* turn-by-turn record 0: x, x', y, y' of every row */

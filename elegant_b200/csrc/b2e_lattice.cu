@@ -561,6 +561,10 @@ static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
     return "RFCA with zero frequency is not supported by this engine";
   if (p[B2E_RFCA_L] < 0)
     return "RFCA with negative length (backtracking) is not supported by this engine";
+  const int fid = (int)p[B2E_RFCA_FIDUCIAL];
+  if (fid != p[B2E_RFCA_FIDUCIAL] || fid < B2E_FIDUCIAL_TMEAN || fid > B2E_FIDUCIAL_PMAXIMUM)
+    return "RFCA FIDUCIAL must be tmean, light or pmaximum (first ends every serial elegant run: "
+           "simple_rfca.c:103-111)";
   d.kind = K_RFCA;
   /* nKicks = length ? N_KICKS : 1, the matrix method for nKicks <= 0;
    * length and volt per section (simple_rfca.c:403-409) */
@@ -587,6 +591,8 @@ static std::string compile_rfca(const b2e_element &el, int slot, DevElem &d) {
   d.c[RF_DTLIGHT] = length / kC_MKS;
   /* VOLT = 0: an exact drift over L and nothing else (simple_rfca.c:380-392) */
   d.c[RF_DRIFT_ONLY] = p[B2E_RFCA_VOLT] == 0;
+  d.c[RF_FID_MODE] = fid;
+  d.c[RF_L_TOTAL] = L;
   return "";
 }
 

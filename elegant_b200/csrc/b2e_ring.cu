@@ -310,16 +310,21 @@ cudaError_t launch_history_merge(const double *partials, int hist_passes, const 
   return cudaGetLastError();
 }
 
-/* RFCA fiducial time, TMEAN mode (findFiducialTime, simple_rfca.c:177-230):
+/* RFCA fiducial time (findFiducialTime, simple_rfca.c:62-257).  TMEAN:
  * Kahan-compensated mean of (s + sOffset)/(c*beta) over the particles that
  * reach the cavity on the first pass, summed in particle order.  One thread
  * per instance walks its particles sequentially so the sum is the
  * reference's serial Kahan sum, bit for bit, when no particle was lost
  * upstream on that pass (elegant's swap-to-tail would otherwise reorder the
- * survivors). */
+ * survivors).  LIGHT: (zEnd - L + sOffset)/c (:97-100).  PMAXIMUM (:126-147):
+ * the arrival time of the particle with the highest delta, found as the
+ * reference's loop does: the first particle's delta is the starting best and
+ * only a later, strictly higher one is taken, so a beam whose first particle
+ * is highest has no fiducial particle (the reference stops there; here bit 2
+ * of the error flag is set and the cavity stays unset). */
 __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                                    int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
-                                   int64_t max_rows) {
+                                   int64_t max_rows, unsigned int *error_flag) {
   const int inst = blockIdx.x * blockDim.x + threadIdx.x;
   if (inst >= n_inst)
     return;
@@ -330,18 +335,47 @@ __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, 
   double tsum = 0, error = 0;
   int64_t nsum = 0;
   const int64_t first = inst_offsets[inst], end = inst_offsets[inst + 1];
-  for (int64_t ip = first; ip < end && (max_rows <= 0 || ip - first < max_rows); ip++) {
-    if (P.lost_pass[ip] >= 0)
-      continue;
-    double pp = p_central * (1 + P.dp[ip]);
-    double beta = pp / sqrt(pp * pp + 1); /* beta_from_delta, do_tracking.c:95 */
-    double b = (P.s[ip] + sOffset) / (B2E_C_MKS * beta);
-    /* KahanPlus (kahan.c:28-35) */
-    double Y = b + error;
-    double sum = tsum + Y;
-    error = Y - (sum - tsum);
-    tsum = sum;
-    nsum++;
+  const int mode = (int)e.c[RF_FID_MODE];
+  if (mode == B2E_FIDUCIAL_LIGHT) {
+    tsum = ((e.z_end - e.c[RF_L_TOTAL]) + sOffset) / B2E_C_MKS;
+    nsum = 1;
+  } else if (mode == B2E_FIDUCIAL_PMAXIMUM) {
+    double best = 0;
+    int64_t ibest = -1;
+    bool seen = false;
+    for (int64_t ip = first; ip < end && (max_rows <= 0 || ip - first < max_rows); ip++) {
+      if (P.lost_pass[ip] >= 0)
+        continue;
+      if (!seen) {
+        best = P.dp[ip];
+        seen = true;
+      } else if (best < P.dp[ip]) {
+        best = P.dp[ip];
+        ibest = ip;
+      }
+    }
+    if (ibest >= 0) {
+      double pp = p_central * (1 + P.dp[ibest]);
+      double beta = pp / sqrt(pp * pp + 1);
+      tsum = (P.s[ibest] + sOffset) / (B2E_C_MKS * beta);
+      nsum = 1;
+    } else if (seen && e.c[RF_T_REFERENCE] == -1) {
+      atomicOr(error_flag, 2u);
+    }
+  } else {
+    for (int64_t ip = first; ip < end && (max_rows <= 0 || ip - first < max_rows); ip++) {
+      if (P.lost_pass[ip] >= 0)
+        continue;
+      double pp = p_central * (1 + P.dp[ip]);
+      double beta = pp / sqrt(pp * pp + 1); /* beta_from_delta, do_tracking.c:95 */
+      double b = (P.s[ip] + sOffset) / (B2E_C_MKS * beta);
+      /* KahanPlus (kahan.c:28-35) */
+      double Y = b + error;
+      double sum = tsum + Y;
+      error = Y - (sum - tsum);
+      tsum = sum;
+      nsum++;
+    }
   }
   if (e.c[RF_T_REFERENCE] != -1) {
     /* explicit T_REFERENCE replaces the fiducial search */
@@ -534,10 +568,10 @@ cudaError_t launch_compact(DevParticles src, const int64_t *ids_src, DevParticle
 
 cudaError_t launch_fiducial(DevParticles P, const int64_t *inst_offsets, int n_inst, const DevElem *elems,
                             int n_elems, int elem_index, DevRfState *rf, int n_rf, double p_central,
-                            int64_t max_rows, cudaStream_t stream) {
+                            int64_t max_rows, unsigned int *error_flag, cudaStream_t stream) {
   int tpb = 64, nb = (n_inst + tpb - 1) / tpb;
   rf_fiducial_kernel<<<nb, tpb, 0, stream>>>(P, inst_offsets, n_inst, elems, n_elems, elem_index, rf, n_rf,
-                                             p_central, max_rows);
+                                             p_central, max_rows, error_flag);
   return cudaGetLastError();
 }
 

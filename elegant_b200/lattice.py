@@ -57,7 +57,8 @@ SLOTS = {
     nat.KSEXT: dict(_KMULT, K2=1, K1=10, J1=11),
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,
-    nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6, "N_KICKS": 7},
+    nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6, "N_KICKS": 7,
+               "FIDUCIAL": 8},
     nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "YEXPONENT": 4},
     nat.MARK: {},
     nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},
@@ -80,6 +81,19 @@ IGNORED = {nat.KQUAD: _KMULT_IGNORED + ("SR_IN_ORDINARY_MATRIX", "TRACKING_MATRI
 STRING_PARAMS = {nat.WATCH: ("FILENAME", "LABEL")}
 # WATCH MODE strings (matched by prefix, as elegant's match_string) -> B2E_WATCH_MODE codes
 WATCH_MODES = (("coord", 0), ("param", 1), ("centroid", 2), ("fft", 3))
+# RFCA FIDUCIAL strings (simple_rfca.c:22-27; exact name or unique prefix) -> B2E_FIDUCIAL_* codes
+FIDUCIAL_MODES = (("light", 1), ("tmean", 0), ("first", None), ("pmaximum", 2))
+
+
+def _fiducial_code(name: str, element: str) -> int:
+    m = name.strip('"').strip().lower()
+    hits = [c for n, c in FIDUCIAL_MODES if n == m] or [c for n, c in FIDUCIAL_MODES if m and n.startswith(m)]
+    if len(hits) != 1:
+        raise LatticeError(f"RFCA {element}: invalid fiducial mode {name!r} (light, tmean, first, pmaximum)")
+    if hits[0] is None:
+        raise LatticeError(f"RFCA {element}: FIDUCIAL=first ends every serial elegant run "
+                           "(simple_rfca.c:103-111); use tmean, light or pmaximum")
+    return hits[0]
 
 # defaults from the reference's parameter tables (only nonzero ones listed)
 DEFAULTS = {
@@ -130,6 +144,8 @@ class Element:
                 if not codes:
                     raise LatticeError(f"WATCH {self.name}: unknown MODE {v!r}")
                 v = codes[0]
+            if k == "FIDUCIAL" and code == nat.RFCA and isinstance(v, str):
+                v = _fiducial_code(v, self.name)
             if k not in SLOTS[code] and k not in IGNORED.get(code, ()):
                 raise LatticeError(f"parameter {k} of {self.type} {self.name} is not supported by the engine")
             if k == "N_KICKS" and code in (nat.CSBEND, nat.CSRCSBEND):
@@ -163,7 +179,9 @@ class Element:
 
     def to_lte(self) -> str:
         names = {c: n for n, c in (("coordinates", 0), ("parameters", 1), ("centroids", 2), ("fft", 3))}
+        fid = {c: n for n, c in FIDUCIAL_MODES}
         items = [f'{k}="{names.get(int(v), "coordinates")}"' if (k == "MODE" and self.code == nat.WATCH)
+                 else f'{k}="{fid[int(v)]}"' if (k == "FIDUCIAL" and self.code == nat.RFCA)
                  else f"{k}={v!r}" for k, v in self.params.items()]
         items += [f'{k}="{v}"' for k, v in self.strings.items()]
         return f"{self.name}: {self.type}" + ("".join(", " + i for i in items))

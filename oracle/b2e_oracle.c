@@ -1076,16 +1076,18 @@ static void malign_track(double **c, long np, const b2e_element *e, double Po) {
   }
 }
 
-/* ---- RFCA (TMEAN fiducial): trackRfCavityWithWakes, simple_rfca.c:295-985 --
+/* ---- RFCA: trackRfCavityWithWakes, simple_rfca.c:295-985 --------------------
  * the zero-length kick, drift-kick-drift sections for L > 0 with N_KICKS > 0
  * (:569-700), the matrix method for L > 0 with N_KICKS <= 0 (:823-945), and
- * VOLT = 0 as a plain drift (:380-392); no wakes, Q, change_t, end focus. */
+ * VOLT = 0 as a plain drift (:380-392); no wakes, Q, change_t, end focus.
+ * Fiducial modes of findFiducialTime (:62-257): TMEAN, LIGHT and PMAXIMUM
+ * (FIRST ends every serial run, :103-111, and is rejected at load). */
 typedef struct {
   int seen;
   double phase_fiducial;
 } RfState;
 
-static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, double Po) {
+static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, double Po, double zEnd) {
   const double *p = e->p;
   double omega = (2 * PI_) * p[B2E_RFCA_FREQ];
   double volt = p[B2E_RFCA_VOLT] / (1e6 * ME_MEV * 1);
@@ -1114,7 +1116,21 @@ static long rfca_track(double **c, long np, const b2e_element *e, RfState *rs, d
   if (!rs->seen) {
     if (p[B2E_RFCA_T_REFERENCE] != -1)
       t0 = p[B2E_RFCA_T_REFERENCE];
-    else {
+    else if (p[B2E_RFCA_FIDUCIAL] == B2E_FIDUCIAL_LIGHT)
+      t0 = (zEnd - p[B2E_RFCA_L] + length / 2) / C_MKS;
+    else if (p[B2E_RFCA_FIDUCIAL] == B2E_FIDUCIAL_PMAXIMUM) {
+      double best = c[0][5], pp;
+      long ibest = -1;
+      for (ip = 0; ip < np; ip++)
+        if (best < c[ip][5]) {
+          best = c[ip][5];
+          ibest = ip;
+        }
+      if (ibest < 0)
+        return -1; /* "No available particle for RF cavity fiducialization" */
+      pp = Po * (1 + c[ibest][5]);
+      t0 = (c[ibest][4] + length / 2) / (C_MKS * (pp / sqrt(pp * pp + 1)));
+    } else {
       double tsum = 0, error = 0;
       for (ip = 0; ip < np; ip++) {
         double pp = Po * (1 + c[ip][5]);
@@ -1936,7 +1952,8 @@ static long csrdrift_track(double **c, long np, const b2e_element *el, double Po
 
 /* ---- do_tracking restated ------------------------------------------------ */
 /* rows: np x 8 (x, xp, y, yp, s, delta, id, lossPass); lossPass must be -1 on
- * input.  Returns survivors; rows are left in the reference's array order.
+ * input.  Returns survivors (-1 when an RFCA finds no fiducial particle);
+ * rows are left in the reference's array order.
  * wakes (optional): every CSRCSBEND kick's dGamma, in order. */
 long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int n_passes, int default_order,
                           double *rows, long np, double *effort, double *wakes, long wake_cap, long *n_wakes) {
@@ -2002,7 +2019,11 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
           nLeft = csbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, &ma, pass);
           break;
         case B2E_RFCA:
-          nLeft = rfca_track(c, nToTrack, e, &rf[k], p_central);
+          nLeft = rfca_track(c, nToTrack, e, &rf[k], p_central, z);
+          if (nLeft < 0) {
+            nToTrack = -1; /* no fiducial particle (FIDUCIAL=pmaximum): the reference stops */
+            goto finish;
+          }
           break;
         case B2E_MAXAMP:
           ma.present = 1;
@@ -2049,6 +2070,7 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
     }
     *effort += nToTrack;
   }
+finish:
   if (n_wakes)
     *n_wakes = cw.n_wakes;
   if (wakes && cw.wakes)

@@ -23,9 +23,12 @@ REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 
 def lattice_spec(lattice) -> str:
     """Element list in the driver's 'NAME:TYPE KEY=VALUE ...;' syntax."""
+    from elegant_b200.lattice import FIDUCIAL_MODES
+    fid = {c: n for n, c in FIDUCIAL_MODES}
     items = []
     for e in lattice.elements:
-        kv = " ".join(f"{k}={v!r}" for k, v in e.params.items())
+        kv = " ".join(f"{k}={fid[int(v)]}" if (k == "FIDUCIAL" and e.type == "RFCA") else f"{k}={v!r}"
+                      for k, v in e.params.items())
         items.append(f"{e.name}:{e.type} {kv}".strip())
     return ";".join(items)
 
@@ -263,6 +266,8 @@ class PortOracle:
                                            rows.ctypes.data_as(ctypes.c_void_p), ctypes.c_long(n), ctypes.byref(eff),
                                            wakes.ctypes.data_as(ctypes.c_void_p) if capture_wakes else None,
                                            ctypes.c_long(cap), ctypes.byref(nw))
+        if nl < 0:
+            raise RuntimeError("port oracle failed: No available particle for RF cavity fiducialization")
         if capture_wakes:
             return rows[:n], nl, eff.value, wakes[: nw.value]
         return rows[:n], nl, eff.value

@@ -543,3 +543,35 @@ def test_ensemble_of_corrector_settings(ref_b2e):
         sub = type(res)(res.coords[sl], res.ids[sl], res.lost_pass[sl], res.lost_element[sl],
                         int((res.lost_pass[sl] < 0).sum()), 0.0)
         assert_parity(sub, rows, nl)
+
+
+@pytest.mark.parametrize("mode", ["light", "pmaximum"])
+def test_ring_fiducial_modes(ref_b2e, mode):
+    """RFCA FIDUCIAL light and pmaximum (findFiducialTime, simple_rfca.c:97-147)
+    on a zero-length cavity mid-ring and one with a length: 40 turns with
+    losses, bit-identical to the reference; and as per-instance ensembles."""
+    base = list(w.fodo_ring().elements)
+    rf = next(e for e in base if e.type == "RFCA")
+    els = [e for e in base if e.type != "RFCA"]
+    els.insert(20, Element("RF1", "RFCA", dict(rf.params, FIDUCIAL=mode)))
+    els.append(Element("RF2", "RFCA", dict(rf.params, L=0.4, N_KICKS=4, VOLT=5e5, FIDUCIAL=mode)))
+    lat = Lattice(els)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=71).coords, _lossy_beam(150, seed=72).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 40)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 40)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff
+
+
+def test_ring_fiducial_pmaximum_without_a_particle_is_an_error():
+    """A beam whose first particle has the highest delta leaves pmaximum no
+    fiducial particle: the reference stops; the engine returns an error."""
+    from elegant_b200._native import EngineError
+    lat = Lattice([Element("D", "DRIF", {"L": 1.0}),
+                   Element("RF", "RFCA", {"VOLT": 1e6, "FREQ": 5e8, "FIDUCIAL": "pmaximum"})])
+    coords = np.zeros((3, 6))
+    coords[:, 5] = [1e-3, 0.0, -1e-3]
+    with pytest.raises(EngineError, match="No available particle"):
+        gpu_track(lat, Beam(coords, np.arange(1, 4)), w.ring_p_central(), 2)

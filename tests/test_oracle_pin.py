@@ -509,3 +509,57 @@ def test_port_reproduces_reference_steering(math, case):
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
     r0, n0, _, _ = RefOracle(math).track(base or w.fodo_ring(), beam.coords, beam.ids, P0, 20)
     assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("mode", ["light", "pmax", "tm"])
+def test_port_reproduces_reference_fiducial_modes(math, mode):
+    """RFCA FIDUCIAL (findFiducialTime, simple_rfca.c:62-257): light (zEnd - L
+    + sOffset over c), pmaximum (the highest-delta particle after the first),
+    tmean by an abbreviation; a zero-length cavity mid-ring and one with a
+    length, with losses."""
+    from elegant_b200 import Element, Lattice
+    base = list(w.fodo_ring().elements)
+    rf = next(e for e in base if e.type == "RFCA")
+    els = [e for e in base if e.type != "RFCA"]
+    els.insert(20, Element("RF1", "RFCA", dict(rf.params, FIDUCIAL=mode)))
+    els.append(Element("RF2", "RFCA", dict(rf.params, L=0.4, N_KICKS=4, VOLT=5e5, FIDUCIAL=mode)))
+    lat = Lattice(els)
+    beam = _mixed_beam(71)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 15)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 15)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    if mode != "tm":
+        r0, n0, _, _ = RefOracle(math).track(Lattice([Element(e.name, e.type, dict(e.params, FIDUCIAL="tmean"))
+                                                      if e.type == "RFCA" else e for e in lat.elements]),
+                                             beam.coords, beam.ids, P0, 15)
+        assert not np.array_equal(r0[:min(n0, n1), :6], r1[:min(n0, n1), :6])
+
+
+def test_fiducial_pmaximum_without_a_particle_fails_like_the_reference():
+    """pmaximum takes only a particle after the first with a higher delta
+    (simple_rfca.c:126-147): a beam whose first particle is highest stops the
+    reference, and the oracle too."""
+    from elegant_b200 import Element, Lattice
+    lat = Lattice([Element("D", "DRIF", {"L": 1.0}),
+                   Element("RF", "RFCA", {"VOLT": 1e6, "FREQ": 5e8, "FIDUCIAL": "pmaximum"})])
+    coords = np.zeros((3, 6))
+    coords[:, 5] = [1e-3, 0.0, -1e-3]
+    with pytest.raises(RuntimeError, match="fiducial"):
+        RefOracle("b2e").track(lat, coords, np.arange(1, 4), P0, 2)
+    with pytest.raises(RuntimeError, match="fiducial"):
+        PortOracle("b2e").track(lat, coords, np.arange(1, 4), P0, 2)
+    coords[:, 5] = [0.0, 1e-3, 1e-3]
+    RefOracle("b2e").track(lat, coords, np.arange(1, 4), P0, 2)
+
+
+def test_fiducial_mode_first_is_rejected():
+    from elegant_b200 import Element
+    from elegant_b200.lattice import LatticeError
+    with pytest.raises(LatticeError, match="first"):
+        Element("RF", "RFCA", {"VOLT": 1e6, "FIDUCIAL": "first"})
+    with pytest.raises(LatticeError, match="invalid fiducial"):
+        Element("RF", "RFCA", {"VOLT": 1e6, "FIDUCIAL": "median"})
+    assert Element("RF", "RFCA", {"FIDUCIAL": "p"}).params["FIDUCIAL"] == 2
