@@ -298,7 +298,7 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
 
 /* Field expansion of a sector bend with quadrupole and sextupole terms
  * (computeCSBENDFieldCoefficients, csbend.c:186-663): b0 the dipole
- * correction (xKick/angle: a signed zero here), b1 = K1*rho0, b2 = K2*rho0,
+ * correction (XKICK/angle, a signed zero without XKICK), b1 = K1*rho0, b2 = K2*rho0,
  * normal terms only, h1 the curvature.  The field sums of a normal-only
  * expansion to order 4 read 15 coefficients; each is formed with the
  * expansion's own terms in their order, the zero octupole and decapole terms
@@ -401,9 +401,11 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     return "CSBEND integration_order is invalid--must be 2, 4, or 6";
   if (nSlices < 1)
     return "CSBEND N_SLICES must be >= 1";
-  const bool fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0;
+  /* the expansion runs when any b[] is nonzero (hasNormal, csbend.c:205-210),
+   * b0 = XKICK/ANGLE included */
+  const bool fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0;
   if (fields && el.type == B2E_CSRCSBEND)
-    return "CSRCSBEND with K1/K2 field terms is not supported by this engine";
+    return "CSRCSBEND with K1/K2/XKICK field terms is not supported by this engine";
   if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
     return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
   /* csbend.c:933-950: negative angle folded into a PI tilt */
@@ -534,14 +536,15 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     if (fields) {
       /* b[] as track_through_csbend forms it (csbend.c:824-882): K*rho0 with
        * the signed angle, the FSE ratios (1 + fse)/(1 + fse), the quadrupole
-       * term negated with a negative angle; b0 = xKick/angle */
+       * term negated with a negative angle; b0 = XKICK/angle (:867) */
       const double rho_signed = length / p[B2E_BEND_ANGLE];
       double b1 = p[B2E_BEND_K1] * rho_signed, b2 = p[B2E_BEND_K2] * rho_signed;
       b1 *= ((1 + p[B2E_BEND_FSE]) + 0) / ((1 + p[B2E_BEND_FSE]) + 0);
       b2 *= (1 + p[B2E_BEND_FSE]) / ((1 + p[B2E_BEND_FSE]) + 0);
       if (p[B2E_BEND_ANGLE] < 0)
         b1 *= -1;
-      bend_field_terms(r.c + RB_FIELD0, 0.0 / p[B2E_BEND_ANGLE], b1, b2, h, p[B2E_BEND_NONLINEAR] != 0);
+      bend_field_terms(r.c + RB_FIELD0, p[B2E_BEND_XKICK] / p[B2E_BEND_ANGLE], b1, b2, h,
+                       p[B2E_BEND_NONLINEAR] != 0);
       d.flags |= EF_FIELD;
     }
     d.flags |= EF_RADBLOCK;

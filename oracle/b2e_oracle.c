@@ -930,14 +930,14 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   br.elem = idx;
   /* b[] of the field expansion (csbend.c:824-882): K*rho0 with the signed
    * angle, the FSE ratios, odd terms negated with a negative angle */
-  br.fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0;
+  br.fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0;
   if (br.fields) {
     double b[5] = {0, 0, 0, 0, 0}, rs = length / p[B2E_BEND_ANGLE];
     b[1] = p[B2E_BEND_K1] * rs;
     b[2] = p[B2E_BEND_K2] * rs;
     b[1] *= (1 + p[B2E_BEND_FSE] + 0) / (1 + p[B2E_BEND_FSE] + 0);
     b[2] *= (1 + p[B2E_BEND_FSE]) / (1 + p[B2E_BEND_FSE] + 0);
-    b[0] = 0.0 / p[B2E_BEND_ANGLE];
+    b[0] = p[B2E_BEND_XKICK] / p[B2E_BEND_ANGLE]; /* csbend.c:867 */
     if (p[B2E_BEND_ANGLE] < 0) {
       b[1] *= -1;
       b[3] *= -1;

@@ -575,3 +575,19 @@ def test_ring_fiducial_pmaximum_without_a_particle_is_an_error():
     coords[:, 5] = [1e-3, 0.0, -1e-3]
     with pytest.raises(EngineError, match="No available particle"):
         gpu_track(lat, Beam(coords, np.arange(1, 4)), w.ring_p_central(), 2)
+
+
+@pytest.mark.parametrize("negative", [False, True])
+def test_ring_with_bend_steering(ref_b2e, negative):
+    """CSBEND XKICK (the expansion's b0 = XKICK/ANGLE, csbend.c:867, in the
+    field sums of the kick), alone and with K1, with negative angles: 60
+    turns with losses, bit-identical to the reference."""
+    from test_oracle_pin import _ring_with_bend_steering
+    lat = _ring_with_bend_steering(negative)
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=81).coords, _lossy_beam(150, seed=82).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

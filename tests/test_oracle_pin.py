@@ -563,3 +563,34 @@ def test_fiducial_mode_first_is_rejected():
     with pytest.raises(LatticeError, match="invalid fiducial"):
         Element("RF", "RFCA", {"VOLT": 1e6, "FIDUCIAL": "median"})
     assert Element("RF", "RFCA", {"FIDUCIAL": "p"}).params["FIDUCIAL"] == 2
+
+
+def _ring_with_bend_steering(negative=False):
+    """Bends with XKICK (the field term b0 = XKICK/ANGLE, csbend.c:867), alone
+    or with K1; every other bend folded to a negative angle when asked."""
+    from elegant_b200 import Element, Lattice
+    errs = [{"XKICK": 2e-4}, {"XKICK": -1e-4, "K1": 0.1}, {}, {"XKICK": 5e-5, "NONLINEAR": 0}]
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            params = dict(e.params, **errs[k % len(errs)])
+            if negative and k % 2:
+                params.update(ANGLE=-params["ANGLE"], TILT=math.pi)
+            e = Element(e.name + str(k), e.type, params)
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+@pytest.mark.parametrize("negative", [False, True])
+def test_port_reproduces_reference_bend_steering(math, negative):
+    lat = _ring_with_bend_steering(negative)
+    beam = _mixed_beam(81)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    r0, n0, _, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
