@@ -35,8 +35,27 @@ static const b2e_param_map map_edrift[] = {{"L", B2E_EDRIFT_L}, END_MAP};
       {"VCALIBRATION", B2E_KMULT_VCALIBRATION}, {"BORE", B2E_KMULT_BORE}, {"B", B2E_KMULT_B},                     \
       /* read by no tracking code: optimizer flags, PITCH/YAW under MALIGN_METHOD 0 */                           \
       {"HSTEERING", -1}, {"VSTEERING", -1}, {"SQRT_ORDER", -1}, {"PITCH", -1}, {"YAW", -1}
-static const b2e_param_map map_kquad[] = {KMULT_COMMON, {"K1", B2E_KMULT_K}, {"SR_IN_ORDINARY_MATRIX", -1},
-                                          {"TRACKING_MATRIX", -1}, END_MAP};
+static const b2e_param_map map_kquad[] = {KMULT_COMMON,
+                                          {"K1", B2E_KMULT_K},
+                                          {"SR_IN_ORDINARY_MATRIX", -1},
+                                          {"TRACKING_MATRIX", -1},
+                                          {"EDGE1_EFFECTS", B2E_KMULT_EDGE1_EFFECTS},
+                                          {"EDGE2_EFFECTS", B2E_KMULT_EDGE2_EFFECTS},
+                                          {"EDGE1_LINEAR", B2E_KMULT_EDGE1_LINEAR},
+                                          {"EDGE2_LINEAR", B2E_KMULT_EDGE2_LINEAR},
+                                          {"EDGE1_NONLINEAR_FACTOR", B2E_KMULT_EDGE1_NONLINEAR_FACTOR},
+                                          {"EDGE2_NONLINEAR_FACTOR", B2E_KMULT_EDGE2_NONLINEAR_FACTOR},
+                                          {"I0P", B2E_KMULT_I0P},
+                                          {"I1P", B2E_KMULT_I0P + 1},
+                                          {"I2P", B2E_KMULT_I0P + 2},
+                                          {"I3P", B2E_KMULT_I0P + 3},
+                                          {"LAMBDA2P", B2E_KMULT_I0P + 4},
+                                          {"I0M", B2E_KMULT_I0M},
+                                          {"I1M", B2E_KMULT_I0M + 1},
+                                          {"I2M", B2E_KMULT_I0M + 2},
+                                          {"I3M", B2E_KMULT_I0M + 3},
+                                          {"LAMBDA2M", B2E_KMULT_I0M + 4},
+                                          END_MAP};
 static const b2e_param_map map_ksext[] = {KMULT_COMMON,
                                           {"K2", B2E_KMULT_K},
                                           {"K1", B2E_KMULT_K1_OF_KSEXT},

@@ -267,11 +267,12 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
 }
 
 /* the lattice needs the ring kernel's RAD instantiation: some element
- * radiates, steers (KQUAD/KSEXT HKICK/VKICK), or is a bend with K1/K2 field
- * terms, ETILT or second-order edges (all read the DevRad table) */
+ * radiates, steers (KQUAD/KSEXT HKICK/VKICK), is a KQUAD with fringe fields,
+ * or is a bend with field terms, ETILT or second-order edges (all read the
+ * DevRad table) */
 static bool any_radiation(const std::vector<DevElem> &elems) {
   for (const DevElem &d : elems)
-    if (d.flags & (EF_SR | EF_ISR | EF_FIELD | EF_ETILT | EF_EDGE_ORDER2 | EF_STEERING))
+    if (d.flags & (EF_SR | EF_ISR | EF_FIELD | EF_ETILT | EF_EDGE_ORDER2 | EF_STEERING | EF_QFRINGE1 | EF_QFRINGE2))
       return true;
   return false;
 }

@@ -10,6 +10,7 @@
  */
 #ifndef B2E_ELEMENTS_CUH
 #define B2E_ELEMENTS_CUH
+#include <float.h>
 #include "b2e_rng.h"
 #include "b2e_engine.h"
 #include "b2e_math.h"
@@ -284,6 +285,80 @@ __device__ __forceinline__ int kmult_kick(double x, double y, double &xp, double
   return LOSS_NONE;
 }
 
+/* KQUAD fringe field of one face (quadFringe, fringe.c:24-175): slopes to
+ * momenta, the linear map of the first partial fringe matrix, the leading
+ * nonlinear generator (edge effects 2) scaled by the nonlinear factor, the
+ * second matrix, back to slopes (DBL_MAX where that fails).  At the entrance
+ * the two matrices trade places with their diagonals swapped (:50-60). */
+__device__ __forceinline__ void quad_fringe(Part &p, const double *rc, int in, int order, bool linear, double nlf) {
+  const double *A = rc + (in < 0 ? RK_QF_M2 : RK_QF_M1), *B = rc + (in < 0 ? RK_QF_M1 : RK_QF_M2);
+  double a00 = A[0], a11 = A[3], a22 = A[4], a33 = A[7], b00 = B[0], b11 = B[3], b22 = B[4], b33 = B[7];
+  if (in < 0) {
+    double t = a00;
+    a00 = a11;
+    a11 = t;
+    t = a22;
+    a22 = a33;
+    a33 = t;
+    t = b00;
+    b00 = b11;
+    b11 = t;
+    t = b22;
+    b22 = b33;
+    b33 = t;
+  }
+  const double delta = p.dp, xp = p.xp, yp = p.yp;
+  const double denom = sqrt((1 + xp * xp) + yp * yp);
+  const double v1 = (1 + delta) * xp / denom, v3 = (1 + delta) * yp / denom;
+  double x, px, y, py;
+  if (linear) {
+    x = a00 * p.x + A[1] * v1;
+    px = A[2] * p.x + a11 * v1;
+    y = a22 * p.y + A[5] * v3;
+    py = A[6] * p.y + a33 * v3;
+  } else {
+    x = p.x;
+    px = v1;
+    y = p.y;
+    py = v3;
+  }
+  const double a = -in * rc[RK_QF_K1] / (12 * (1 + delta));
+  double dx = 0, dpx = 0, dy = 0, dpy = 0, ds = 0;
+  if (order > 1) {
+    const double x2 = x * x, x3 = x2 * x, y2 = y * y, y3 = y2 * y;
+    dpx = 3 * a * (-px * x2 + 2 * py * x * y - px * y2);
+    dpy = 3 * a * (py * x2 - 2 * px * x * y + py * y2);
+    dx = a * (x3 + 3 * x * y2);
+    dy = a * (-3 * x2 * y - y3);
+    ds = (a / (1 + delta)) * (3 * py * y * x2 - px * x3 - 3 * px * x * y2 + py * y3);
+  }
+  x += nlf * dx;
+  px += nlf * dpx;
+  y += nlf * dy;
+  py += nlf * dpy;
+  double qx, qy;
+  if (linear) {
+    p.x = b00 * x + B[1] * px;
+    qx = B[2] * x + b11 * px;
+    p.y = b22 * y + B[5] * py;
+    qy = B[6] * y + b33 * py;
+  } else {
+    p.x = x;
+    qx = px;
+    p.y = y;
+    qy = py;
+  }
+  p.s -= nlf * ds;
+  const double d2 = (1 + delta) * (1 + delta) - qx * qx - qy * qy;
+  if (d2 > 0) {
+    const double r = sqrt(d2);
+    p.xp = qx / r;
+    p.yp = qy / r;
+  } else {
+    p.xp = p.yp = DBL_MAX;
+  }
+}
+
 /* The slice loop stays rolled: unrolled instances for 4 substeps measured
  * slower in the fused ring kernel (more registers live across the unrolled
  * body, more spills). */
@@ -301,6 +376,8 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
     offset_misalign(p, dx, dy, c[KM_DZ]);
   if (e.flags & EF_ENTRANCE_ROTATE)
     rotate_misalign(p, c[KM_COS_TILT], c[KM_SIN_TILT]);
+  if (RAD && (e.flags & EF_QFRINGE1)) /* multipole.c:1031-1037 */
+    quad_fringe(p, rs.rc, -1, (int)rs.rc[RK_QF_EDGE1], rs.rc[RK_QF_LIN1] != 0, rs.rc[RK_QF_NLF1]);
 
   x = p.x;
   xp = p.xp;
@@ -360,6 +437,8 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
     return LOSS_NAN;
   if (fabs(x) > g.coord_limit || fabs(y) > g.coord_limit || fabs(xp) > g.slope_limit || fabs(yp) > g.slope_limit)
     return LOSS_LIMIT;
+  if (RAD && (e.flags & EF_QFRINGE2)) /* multipole.c:1088-1094 */
+    quad_fringe(p, rs.rc, 1, (int)rs.rc[RK_QF_EDGE2], rs.rc[RK_QF_LIN2] != 0, rs.rc[RK_QF_NLF2]);
   /* exit misalignment, face 2 (malign_mat.c:498-503) */
   if (e.flags & EF_EXIT_MISALIGN) {
     if (e.flags & EF_ENTRANCE_ROTATE)

@@ -56,6 +56,8 @@ enum {
 #define EF_FIELD 0x4000         /* CSBEND: K1/K2 field terms (coefficients in the DevRad table) */
 #define EF_ETILT 0x8000         /* CSBEND: ETILT exit offsets (BendExtra) */
 #define EF_STEERING 0x10000     /* KMULT: HKICK/VKICK steering kicks (per-part kicks in the DevRad table) */
+#define EF_QFRINGE1 0x20000     /* KQUAD: entrance fringe (quadFringe; matrices in the DevRad table) */
+#define EF_QFRINGE2 0x40000     /* KQUAD: exit fringe */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -125,6 +127,15 @@ typedef struct {
 #define RK_DRIFT 10     /* slice drift length (:1189) */
 #define RK_XKICK 11     /* HKICK*HCALIBRATION/n_parts, the steering kick per slice (:785, :1190) */
 #define RK_YKICK 12     /* VKICK*VCALIBRATION/n_parts (:786, :1191) */
+#define RK_QF_K1 13     /* KQUAD fringe (fringe.c:24-175): K1 without FSE */
+#define RK_QF_M1 14     /* quadPartialFringeMatrix part 1 (I*M): R00 R01 R10 R11 R22 R23 R32 R33, 14..21 */
+#define RK_QF_M2 22     /* part 2 (I*P), 22..29 */
+#define RK_QF_EDGE1 30  /* EDGE1_EFFECTS, EDGE2_EFFECTS */
+#define RK_QF_EDGE2 31
+#define RK_QF_LIN1 32   /* EDGE1_LINEAR, EDGE2_LINEAR */
+#define RK_QF_LIN2 33
+#define RK_QF_NLF1 34   /* EDGE1/2_NONLINEAR_FACTOR */
+#define RK_QF_NLF2 35
 #define RB_RAD 0        /* CSBEND: rad_coef (csbend.c:967-970) */
 #define RB_ISR 1        /* isrConstant, > 0 only when ISR is applied (:972-975) */
 #define RB_SLICE 2      /* s = length / N_SLICES, for dsISR (:1614) */

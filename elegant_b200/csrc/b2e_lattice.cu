@@ -105,6 +105,12 @@ void element_defaults(int type, double *p) {
     p[B2E_KMULT_ISR1PART] = 1;          /* :1257, :1157 */
     p[B2E_KMULT_HCALIBRATION] = 1;      /* :1238, :1138 */
     p[B2E_KMULT_VCALIBRATION] = 1;      /* :1239, :1139 */
+    if (type == B2E_KQUAD) {
+      p[B2E_KMULT_EDGE1_LINEAR] = 1; /* :1272-1275 */
+      p[B2E_KMULT_EDGE2_LINEAR] = 1;
+      p[B2E_KMULT_EDGE1_NONLINEAR_FACTOR] = 1;
+      p[B2E_KMULT_EDGE2_NONLINEAR_FACTOR] = 1;
+    }
     break;
   case B2E_CSBEND:
   case B2E_CSRCSBEND:
@@ -187,6 +193,38 @@ static void bend_edge_flags(const b2e_element *el, int n, int i, bool *edge1, bo
   }
   *edge1 = el[i].p[B2E_BEND_EDGE1_EFFECTS] != 0 && !same_pre;
   *edge2 = el[i].p[B2E_BEND_EDGE2_EFFECTS] != 0 && !same_post;
+}
+
+/* quadPartialFringeMatrix (fringe.c:229-271) with inFringe = 1, as quadFringe
+ * forms it: part 1 from the I*M integrals, part 2 from the I*P integrals;
+ * out = R00 R01 R10 R11 R22 R23 R32 R33 */
+static void quad_fringe_matrix(double out[8], double K1, const double *fi, int part) {
+  const double K1sqr = K1 * K1;
+  double J1x, J2x, J3x, J1y, J2y, J3y;
+  if (part == 1) {
+    J1x = 1 * (K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+    J2x = 1 * K1 * fi[2];
+    J3x = 1 * K1sqr * (fi[2] + fi[4] + fi[0] * fi[1]);
+    K1 = -K1;
+    J1y = 1 * (K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+  } else {
+    J1x = 1 * (K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+    J2x = 1 * K1 * fi[2];
+    J3x = 1 * K1sqr * (fi[4] - fi[0] * fi[1]);
+    K1 = -K1;
+    J1y = 1 * (K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+  }
+  J2y = -J2x;
+  J3y = J3x;
+  const double ex = exp(J1x), ey = exp(J1y);
+  out[0] = ex;
+  out[1] = J2x / ex;
+  out[2] = ex * J3x;
+  out[3] = (1 + J2x * J3x) / ex;
+  out[4] = ey;
+  out[5] = J2y / ey;
+  out[6] = ey * J3y;
+  out[7] = (1 + J2y * J3y) / ey;
 }
 
 static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, DevRad &r) {
@@ -292,6 +330,31 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
       d.flags |= EF_SR;
     if (isr_coef > 0 && drift != 0)
       d.flags |= EF_ISR;
+  }
+  /* KQUAD fringe fields (multipole.c:1031-1037, :1088-1094; quadFringe, fringe.c:24-175) */
+  {
+    const double e1 = p[B2E_KMULT_EDGE1_EFFECTS], e2 = p[B2E_KMULT_EDGE2_EFFECTS];
+    if (el.type != B2E_KQUAD && (e1 != 0 || e2 != 0))
+      return "EDGE_EFFECTS apply to KQUAD only";
+    /* a value <= 0 turns the fringe off (multipole.c:1033, :1090) */
+    for (double v : {e1, e2})
+      if (v > 2 || v != floor(v))
+        return "KQUAD EDGE[12]_EFFECTS above 2 (higher-order fringe terms) is not supported by this engine";
+    if (e1 > 0 || e2 > 0) {
+      r.c[RK_QF_K1] = p[B2E_KMULT_K];
+      quad_fringe_matrix(r.c + RK_QF_M1, p[B2E_KMULT_K], p + B2E_KMULT_I0M, 1);
+      quad_fringe_matrix(r.c + RK_QF_M2, p[B2E_KMULT_K], p + B2E_KMULT_I0P, 2);
+      r.c[RK_QF_EDGE1] = e1;
+      r.c[RK_QF_EDGE2] = e2;
+      r.c[RK_QF_LIN1] = p[B2E_KMULT_EDGE1_LINEAR];
+      r.c[RK_QF_LIN2] = p[B2E_KMULT_EDGE2_LINEAR];
+      r.c[RK_QF_NLF1] = p[B2E_KMULT_EDGE1_NONLINEAR_FACTOR];
+      r.c[RK_QF_NLF2] = p[B2E_KMULT_EDGE2_NONLINEAR_FACTOR];
+      if (e1 > 0)
+        d.flags |= EF_QFRINGE1;
+      if (e2 > 0)
+        d.flags |= EF_QFRINGE2;
+    }
   }
   return "";
 }

@@ -53,7 +53,9 @@ _CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=2
 SLOTS = {
     nat.DRIF: {"L": 0, "ORDER": 1},
     nat.EDRIFT: {"L": 0},
-    nat.KQUAD: dict(_KMULT, K1=1),
+    nat.KQUAD: dict(_KMULT, K1=1, EDGE1_EFFECTS=21, EDGE2_EFFECTS=22, EDGE1_LINEAR=23, EDGE2_LINEAR=24,
+                    EDGE1_NONLINEAR_FACTOR=25, EDGE2_NONLINEAR_FACTOR=26, I0P=27, I1P=28, I2P=29, I3P=30,
+                    LAMBDA2P=31, I0M=32, I1M=33, I2M=34, I3M=35, LAMBDA2M=36),
     nat.KSEXT: dict(_KMULT, K2=1, K1=10, J1=11),
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,
@@ -97,7 +99,8 @@ def _fiducial_code(name: str, element: str) -> int:
 
 # defaults from the reference's parameter tables (only nonzero ones listed)
 DEFAULTS = {
-    nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1, "HCALIBRATION": 1, "VCALIBRATION": 1},
+    nat.KQUAD: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1, "HCALIBRATION": 1, "VCALIBRATION": 1,
+                "EDGE1_LINEAR": 1, "EDGE2_LINEAR": 1, "EDGE1_NONLINEAR_FACTOR": 1, "EDGE2_NONLINEAR_FACTOR": 1},
     nat.KSEXT: {"N_SLICES": 1, "INTEGRATION_ORDER": 4, "ISR1PART": 1, "HCALIBRATION": 1, "VCALIBRATION": 1},
     nat.CSBEND: {"FINT": 0.5, "N_SLICES": 4, "INTEGRATION_ORDER": 4, "EDGE1_EFFECTS": 1, "EDGE2_EFFECTS": 1,
                  "EDGE_ORDER": 1, "NONLINEAR": 1, "ISR1PART": 1},

@@ -98,6 +98,18 @@ extern "C" {
 #define B2E_KMULT_VCALIBRATION 18 /* factor on VKICK (default 1) */
 #define B2E_KMULT_BORE 19         /* bore radius (m); nonzero: the strength comes from the pole-tip field B */
 #define B2E_KMULT_B 20            /* pole-tip field (T), used when BORE is nonzero */
+/* KQUAD fringe fields (quadFringe, fringe.c:24-175): EDGE[12]_EFFECTS +-1 linear,
+ * +-2 linear and third order (negative: without the x, y terms); the fringe
+ * integrals I0..I3 and LAMBDA2 of each side, the linear part on/off, a factor
+ * on the nonlinear part */
+#define B2E_KMULT_EDGE1_EFFECTS 21
+#define B2E_KMULT_EDGE2_EFFECTS 22
+#define B2E_KMULT_EDGE1_LINEAR 23            /* default 1 */
+#define B2E_KMULT_EDGE2_LINEAR 24            /* default 1 */
+#define B2E_KMULT_EDGE1_NONLINEAR_FACTOR 25  /* default 1 */
+#define B2E_KMULT_EDGE2_NONLINEAR_FACTOR 26  /* default 1 */
+#define B2E_KMULT_I0P 27 /* I0P, I1P, I2P, I3P, LAMBDA2P: 27..31 */
+#define B2E_KMULT_I0M 32 /* I0M, I1M, I2M, I3M, LAMBDA2M: 32..36 */
 /* CSBEND (csbend_param, track_data.c:1893) and CSRCSBEND (csrcsbend_param, :1982) */
 #define B2E_BEND_L 0
 #define B2E_BEND_ANGLE 1

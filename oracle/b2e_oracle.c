@@ -410,6 +410,99 @@ static void canonical_kick(double *qx, double *qy, double *dqx, double *dqy, dou
   *dqy += KnL * sFx;
 }
 
+/* quadPartialFringeMatrix (fringe.c:229-271), inFringe = 1:
+ * R00 R01 R10 R11 R22 R23 R32 R33 */
+static void qf_matrix(double *R, double K1, const double *fi, int part) {
+  double J1x, J2x, J3x, J1y, J2y, J3y, K1sqr = SQR(K1), ex, ey;
+  if (part == 1) {
+    J1x = 1 * (K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+    J2x = 1 * K1 * fi[2];
+    J3x = 1 * K1sqr * (fi[2] + fi[4] + fi[0] * fi[1]);
+    K1 = -K1;
+    J1y = 1 * (K1 * fi[1] - 2 * K1sqr * fi[3] / 3. - K1sqr * fi[0] * fi[2] / 2);
+  } else {
+    J1x = 1 * (K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+    J2x = 1 * K1 * fi[2];
+    J3x = 1 * K1sqr * (fi[4] - fi[0] * fi[1]);
+    K1 = -K1;
+    J1y = 1 * (K1 * fi[1] + K1sqr * fi[0] * fi[2] / 2);
+  }
+  J2y = -J2x;
+  J3y = J3x;
+  R[0] = ex = exp(J1x);
+  R[1] = J2x / ex;
+  R[2] = ex * J3x;
+  R[3] = (1 + J2x * J3x) / ex;
+  R[4] = ey = exp(J1y);
+  R[5] = J2y / ey;
+  R[6] = ey * J3y;
+  R[7] = (1 + J2y * J3y) / ey;
+}
+
+/* quadFringe (fringe.c:24-175) for higherOrder 1 and 2, forward tracking */
+static void qf_track(double **c, long np, double K1, const double *fiM, const double *fiP, int inFringe,
+                     int higherOrder, int linearFlag, double nlf) {
+  double M1[8], M2[8], *A = M1, *B = M2, t;
+  long ip;
+  if (linearFlag) {
+    qf_matrix(M1, K1, fiM, 1);
+    qf_matrix(M2, K1, fiP, 2);
+    if (inFringe == -1) {
+      t = M1[0], M1[0] = M1[3], M1[3] = t;
+      t = M1[4], M1[4] = M1[7], M1[7] = t;
+      t = M2[0], M2[0] = M2[3], M2[3] = t;
+      t = M2[4], M2[4] = M2[7], M2[7] = t;
+      A = M2;
+      B = M1;
+    }
+  }
+  for (ip = 0; ip < np; ip++) {
+    double *v = c[ip], delta = v[5], xp = v[1], yp = v[3], denom, x, px, y, py, a;
+    double dx = 0, dpx = 0, dy = 0, dpy = 0, ds = 0;
+    denom = sqrt(1 + SQR(xp) + SQR(yp));
+    v[1] = (1 + delta) * xp / denom;
+    v[3] = (1 + delta) * yp / denom;
+    if (linearFlag) {
+      x = A[0] * v[0] + A[1] * v[1];
+      px = A[2] * v[0] + A[3] * v[1];
+      y = A[4] * v[2] + A[5] * v[3];
+      py = A[6] * v[2] + A[7] * v[3];
+    } else {
+      x = v[0], px = v[1], y = v[2], py = v[3];
+    }
+    a = -inFringe * K1 / (12 * (1 + delta));
+    if (higherOrder > 1) {
+      double x2 = x * x, x3 = x2 * x, y2 = y * y, y3 = y2 * y;
+      dpx = 3 * a * (-px * x2 + 2 * py * x * y - px * y2);
+      dpy = 3 * a * (py * x2 - 2 * px * x * y + py * y2);
+      dx = a * (x3 + 3 * x * y2);
+      dy = a * (-3 * x2 * y - y3);
+      ds = (a / (1 + delta)) * (3 * py * y * x2 - px * x3 - 3 * px * x * y2 + py * y3);
+    }
+    x += nlf * dx;
+    px += nlf * dpx;
+    y += nlf * dy;
+    py += nlf * dpy;
+    if (linearFlag) {
+      v[0] = B[0] * x + B[1] * px;
+      v[1] = B[2] * x + B[3] * px;
+      v[2] = B[4] * y + B[5] * py;
+      v[3] = B[6] * y + B[7] * py;
+    } else {
+      v[0] = x, v[1] = px, v[2] = y, v[3] = py;
+    }
+    v[4] -= nlf * ds;
+    px = v[1];
+    py = v[3];
+    if ((denom = SQR(1 + delta) - SQR(px) - SQR(py)) > 0) {
+      denom = sqrt(denom);
+      v[1] = px / denom;
+      v[3] = py / denom;
+    } else
+      v[1] = v[3] = DBL_MAX;
+  }
+}
+
 static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma,
                         int pass, int elem) {
   const double *p = e->p;
@@ -467,6 +560,10 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
     offset_beam(c, np, dx, dy, dz);
   if (tilt)
     rotate_beam(c, np, tilt);
+  /* KQUAD entrance fringe on every particle (multipole.c:1031-1037) */
+  if (e->type == B2E_KQUAD && p[B2E_KMULT_EDGE1_EFFECTS] > 0)
+    qf_track(c, np, p[B2E_KMULT_K], p + B2E_KMULT_I0M, p + B2E_KMULT_I0P, -1, (int)p[B2E_KMULT_EDGE1_EFFECTS],
+             (int)p[B2E_KMULT_EDGE1_LINEAR], p[B2E_KMULT_EDGE1_NONLINEAR_FACTOR]);
   /* multipole.c:788-800 */
   if (p[B2E_KMULT_SYNCH_RAD])
     rad_coef = SQR(E_MKS) * POW3(Po) / (6 * PI_ * EPS0_MKS * SQR(C_MKS) * ME_MKS);
@@ -595,7 +692,11 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
       ip--;
     }
   }
-  /* exit misalignment, face 2, applied to all np rows like the reference */
+  /* KQUAD exit fringe (multipole.c:1088-1094) and the exit misalignment,
+   * face 2, applied to all np rows like the reference */
+  if (e->type == B2E_KQUAD && p[B2E_KMULT_EDGE2_EFFECTS] > 0)
+    qf_track(c, np, p[B2E_KMULT_K], p + B2E_KMULT_I0M, p + B2E_KMULT_I0P, 1, (int)p[B2E_KMULT_EDGE2_EFFECTS],
+             (int)p[B2E_KMULT_EDGE2_LINEAR], p[B2E_KMULT_EDGE2_NONLINEAR_FACTOR]);
   if (dx || dy || dz || tilt) {
     if (tilt)
       rotate_beam(c, np, -tilt);

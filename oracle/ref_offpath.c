@@ -61,7 +61,6 @@ OFFPATH(performSliceAnalysisOutput)
 OFFPATH(pointIsInsideContour)
 OFFPATH(pop_log)
 OFFPATH(push_log)
-OFFPATH(quadFringe)
 OFFPATH(rpn)
 OFFPATH(rpn_clear)
 OFFPATH(simplexMin)

@@ -71,7 +71,7 @@ def _ring_variant():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["ring", "ring_variant", "steering", "chicane"])
+@pytest.mark.parametrize("case", ["ring", "ring_variant", "steering", "quad_fringes", "chicane"])
 def test_adapter_equals_reference_tracking(adapter, ref_b2e, case):
     from elegant_b200.beam import Beam
     if case == "chicane":
@@ -80,6 +80,9 @@ def test_adapter_equals_reference_tracking(adapter, ref_b2e, case):
         if case == "steering":
             from test_oracle_pin import _ring_with_steering
             lat = _ring_with_steering()  # HKICK/VKICK, calibrations, BORE/B, HSTEERING and PITCH through the tables
+        elif case == "quad_fringes":
+            from test_oracle_pin import _ring_with_quad_fringes
+            lat = _ring_with_quad_fringes()
         else:
             lat = w.fodo_ring() if case == "ring" else _ring_variant()
         good, bad = w.ring_beam(150, seed=4), _lossy(150, seed=5)
@@ -107,6 +110,7 @@ def test_adapter_declines_what_the_engine_cannot_take(adapter):
         ("D:DRIF L=0.5;S:SEXT L=0.2 K2=3", "SEXT"),
         ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 PITCH=0.001 MALIGN_METHOD=1", "MALIGN_METHOD"),
         ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 LEFFECTIVE=0.25", "LEFFECTIVE"),
+        ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 RADIAL=1", "RADIAL"),
         ("B:CSBEND L=1 ANGLE=0.1 FINT1=0.3", "FINT1"),
         ("B:CSRCSBEND L=0.5 ANGLE=0.05 BINS=100 OUTPUT_FILE=wake.sdds", "OUTPUT_FILE"),
         ("R:RFCA VOLT=1e6 FREQ=5e8 FIDUCIAL=first", "FIDUCIAL"),

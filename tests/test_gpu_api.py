@@ -74,6 +74,8 @@ def test_csr_elements_take_no_per_instance_overrides():
     ("KQUAD", {"L": 0.2, "K1": 1.0, "INTEGRATION_ORDER": 3}, "INTEGRATION_ORDER"),
     ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 100, "IGF": 1}, "STEADY_STATE"),
     ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 1}, "bins"),
+    ("KQUAD", {"L": 0.2, "K1": 1.0, "EDGE1_EFFECTS": 3}, "EDGE"),
+    ("CSRCSBEND", {"L": 0.5, "ANGLE": 0.05, "BINS": 100, "XKICK": 1e-4}, "XKICK"),
 ])
 def test_unsupported_parameters_are_rejected_at_load(typ, params, words):
     lat = Lattice([Element("D", "DRIF", {"L": 1.0}), Element("X", typ, params)])

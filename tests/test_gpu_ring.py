@@ -591,3 +591,19 @@ def test_ring_with_bend_steering(ref_b2e, negative):
     assert 0 < nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+def test_ring_with_quad_fringes(ref_b2e):
+    """KQUAD fringe fields (quadFringe, fringe.c:24-175, at multipole.c:1031-1037
+    and :1088-1094): linear and third-order, with and without the linear
+    part, a nonlinear factor, misaligned, one face only: 60 turns with
+    losses, bit-identical to the reference (elegant's fringe.c compiled in)."""
+    from test_oracle_pin import _ring_with_quad_fringes
+    lat = _ring_with_quad_fringes()
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=91).coords, _lossy_beam(150, seed=92).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 60)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

@@ -594,3 +594,37 @@ def test_port_reproduces_reference_bend_steering(math, negative):
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
     r0, n0, _, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 20)
     assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
+
+
+def _ring_with_quad_fringes():
+    """Quadrupoles with fringe fields (quadFringe, fringe.c:24-175): linear
+    (EDGE_EFFECTS 1) and linear + third order (2) with fringe integrals, one
+    without the linear part, one with a nonlinear factor, one with the
+    entrance only, one with a negative (off) value."""
+    from elegant_b200 import Element, Lattice
+    fi = {"I0P": 0.02, "I1P": 1e-3, "I2P": 2e-5, "I3P": 1e-6, "LAMBDA2P": 3e-6,
+          "I0M": 0.025, "I1M": -1e-3, "I2M": 1e-5, "I3M": -2e-6, "LAMBDA2M": 1e-6}
+    variants = [dict(fi, EDGE1_EFFECTS=1, EDGE2_EFFECTS=1), dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2),
+                dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, EDGE1_LINEAR=0, EDGE2_LINEAR=0),
+                dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, EDGE2_NONLINEAR_FACTOR=0.5, DX=1e-4, TILT=0.01),
+                {"EDGE1_EFFECTS": 2}, {"EDGE1_EFFECTS": -1, "EDGE2_EFFECTS": 2}]
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "KQUAD":
+            e = Element(e.name + str(k), e.type, dict(e.params, **variants[k % len(variants)]))
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_quad_fringes(math):
+    lat = _ring_with_quad_fringes()
+    beam = _mixed_beam(91)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    r0, n0, _, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
