@@ -55,6 +55,7 @@ static const b2e_param_map map_kquad[] = {KMULT_COMMON,
                                           {"I2M", B2E_KMULT_I0M + 2},
                                           {"I3M", B2E_KMULT_I0M + 3},
                                           {"LAMBDA2M", B2E_KMULT_I0M + 4},
+                                          {"LEFFECTIVE", B2E_KMULT_LEFFECTIVE},
                                           END_MAP};
 static const b2e_param_map map_ksext[] = {KMULT_COMMON,
                                           {"K2", B2E_KMULT_K},

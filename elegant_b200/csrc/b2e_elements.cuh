@@ -376,6 +376,8 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
     offset_misalign(p, dx, dy, c[KM_DZ]);
   if (e.flags & EF_ENTRANCE_ROTATE)
     rotate_misalign(p, c[KM_COS_TILT], c[KM_SIN_TILT]);
+  if (RAD && (e.flags & EF_END_DRIFT)) /* multipole.c:1028-1030 */
+    edrift(p, c[KM_LEND]);
   if (RAD && (e.flags & EF_QFRINGE1)) /* multipole.c:1031-1037 */
     quad_fringe(p, rs.rc, -1, (int)rs.rc[RK_QF_EDGE1], rs.rc[RK_QF_LIN1] != 0, rs.rc[RK_QF_NLF1]);
 
@@ -439,6 +441,8 @@ __device__ __forceinline__ int kmult(Part &p, const DevElem &e, const DevApertur
     return LOSS_LIMIT;
   if (RAD && (e.flags & EF_QFRINGE2)) /* multipole.c:1088-1094 */
     quad_fringe(p, rs.rc, 1, (int)rs.rc[RK_QF_EDGE2], rs.rc[RK_QF_LIN2] != 0, rs.rc[RK_QF_NLF2]);
+  if (RAD && (e.flags & EF_END_DRIFT)) /* multipole.c:1098-1100 */
+    edrift(p, c[KM_LEND]);
   /* exit misalignment, face 2 (malign_mat.c:498-503) */
   if (e.flags & EF_EXIT_MISALIGN) {
     if (e.flags & EF_ENTRANCE_ROTATE)

@@ -58,6 +58,7 @@ enum {
 #define EF_STEERING 0x10000     /* KMULT: HKICK/VKICK steering kicks (per-part kicks in the DevRad table) */
 #define EF_QFRINGE1 0x20000     /* KQUAD: entrance fringe (quadFringe; matrices in the DevRad table) */
 #define EF_QFRINGE2 0x40000     /* KQUAD: exit fringe */
+#define EF_END_DRIFT 0x80000    /* KQUAD with LEFFECTIVE: exact end drifts (KM_LEND) */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -66,6 +67,7 @@ enum {
 #define KM_DSH0 3        /* drift*driftFrac[j], j = 0..7 -> 3..10 */
 #define KM_KICK0 11      /* KnL/nSlices*kickFrac[j], j = 0..7 -> 11..18 (0 terminates) */
 #define KM_KICK1_0 19    /* secondary K1 term per substep, 19..25 (KSEXT K1) */
+#define KM_LEND 26       /* (L - LEFFECTIVE)/2, the end drifts of a KQUAD with LEFFECTIVE */
 #define KM_DX 27
 #define KM_DY 28
 #define KM_DZ 29

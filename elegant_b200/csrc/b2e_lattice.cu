@@ -230,7 +230,15 @@ static void quad_fringe_matrix(double out[8], double K1, const double *fi, int p
 static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, DevRad &r) {
   const double *p = el.p;
   double drift_frac[8], kick_frac[8];
-  const double L = p[B2E_KMULT_L];
+  /* a KQUAD with LEFFECTIVE > 0 integrates over the effective length between
+   * two exact drifts (multipole.c:766-770, :1028-1030, :1098-1100) */
+  const double L = el.type == B2E_KQUAD && p[B2E_KMULT_LEFFECTIVE] > 0 ? p[B2E_KMULT_LEFFECTIVE] : p[B2E_KMULT_L];
+  if (el.type != B2E_KQUAD && p[B2E_KMULT_LEFFECTIVE] != 0)
+    return "LEFFECTIVE applies to KQUAD only";
+  if (L != p[B2E_KMULT_L]) {
+    d.c[KM_LEND] = (p[B2E_KMULT_L] - L) / 2;
+    d.flags |= EF_END_DRIFT;
+  }
   int integ = (int)p[B2E_KMULT_INTEGRATION_ORDER];
   long n_kicks = (long)p[B2E_KMULT_N_KICKS], nSlices = (long)p[B2E_KMULT_N_SLICES];
   int nSub = integrator_fractions(integ, drift_frac, kick_frac);
@@ -310,7 +318,7 @@ static std::string compile_kmult(const b2e_element &el, double Po, DevElem &d, D
     isr_coef = kRE_MKS * sqrt(55.0 / (24 * sqrt(3)) * pow5_host(Po) * 137.0359895);
     if (!isr)
       isr_coef *= -1;
-    if (L < 1e-6 && (isr || sr))
+    if (p[B2E_KMULT_L] < 1e-6 && (isr || sr))
       rad_coef = isr_coef = 0;
     r.c[RK_RAD] = rad_coef;
     r.c[RK_ISR] = isr_coef;

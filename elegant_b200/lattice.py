@@ -55,7 +55,7 @@ SLOTS = {
     nat.EDRIFT: {"L": 0},
     nat.KQUAD: dict(_KMULT, K1=1, EDGE1_EFFECTS=21, EDGE2_EFFECTS=22, EDGE1_LINEAR=23, EDGE2_LINEAR=24,
                     EDGE1_NONLINEAR_FACTOR=25, EDGE2_NONLINEAR_FACTOR=26, I0P=27, I1P=28, I2P=29, I3P=30,
-                    LAMBDA2P=31, I0M=32, I1M=33, I2M=34, I3M=35, LAMBDA2M=36),
+                    LAMBDA2P=31, I0M=32, I1M=33, I2M=34, I3M=35, LAMBDA2M=36, LEFFECTIVE=37),
     nat.KSEXT: dict(_KMULT, K2=1, K1=10, J1=11),
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,

@@ -110,6 +110,7 @@ extern "C" {
 #define B2E_KMULT_EDGE2_NONLINEAR_FACTOR 26  /* default 1 */
 #define B2E_KMULT_I0P 27 /* I0P, I1P, I2P, I3P, LAMBDA2P: 27..31 */
 #define B2E_KMULT_I0M 32 /* I0M, I1M, I2M, I3M, LAMBDA2M: 32..36 */
+#define B2E_KMULT_LEFFECTIVE 37 /* KQUAD effective length (> 0: exact end drifts of (L - LEFFECTIVE)/2) */
 /* CSBEND (csbend_param, track_data.c:1893) and CSRCSBEND (csrcsbend_param, :1982) */
 #define B2E_BEND_L 0
 #define B2E_BEND_ANGLE 1

@@ -506,12 +506,19 @@ static void qf_track(double **c, long np, double K1, const double *fiM, const do
 static long kmult_track(double **c, long np, const b2e_element *e, double Po, double z_start, const MaxAmp *ma,
                         int pass, int elem) {
   const double *p = e->p;
-  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt, rad_coef = 0, isr_coef, xkick, ykick;
+  double KnL[3] = {0, 0, 0}, df[8], kf[8], drift, dx, dy, dz, tilt, rad_coef = 0, isr_coef, xkick, ykick, lEnd = 0;
+  int doEndDrift = 0;
   long order[3] = {0, 0, 0}, nSlices, n_kicks, ip, itop;
   int skew[3] = {0, 0, 0}, integ, nSub, radblock;
   MultAp ap;
   double dzLoss = 0;
   drift = p[B2E_KMULT_L];
+  if (e->type == B2E_KQUAD && p[B2E_KMULT_LEFFECTIVE] > 0) {
+    /* multipole.c:766-770: the effective length, exact end drifts of the rest */
+    drift = p[B2E_KMULT_LEFFECTIVE];
+    lEnd = (p[B2E_KMULT_L] - drift) / 2;
+    doEndDrift = 1;
+  }
   integ = (int)p[B2E_KMULT_INTEGRATION_ORDER];
   nSlices = (long)p[B2E_KMULT_N_SLICES];
   n_kicks = (long)p[B2E_KMULT_N_KICKS];
@@ -560,6 +567,8 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
     offset_beam(c, np, dx, dy, dz);
   if (tilt)
     rotate_beam(c, np, tilt);
+  if (doEndDrift)
+    exact_drift(c, np, lEnd);
   /* KQUAD entrance fringe on every particle (multipole.c:1031-1037) */
   if (e->type == B2E_KQUAD && p[B2E_KMULT_EDGE1_EFFECTS] > 0)
     qf_track(c, np, p[B2E_KMULT_K], p + B2E_KMULT_I0M, p + B2E_KMULT_I0P, -1, (int)p[B2E_KMULT_EDGE1_EFFECTS],
@@ -570,7 +579,7 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
   isr_coef = RE_MKS * sqrt(55.0 / (24 * sqrt(3)) * POW5(Po) * 137.0359895);
   if (!p[B2E_KMULT_ISR])
     isr_coef *= -1;
-  if (drift < 1e-6 && (p[B2E_KMULT_ISR] || p[B2E_KMULT_SYNCH_RAD]))
+  if (p[B2E_KMULT_L] < 1e-6 && (p[B2E_KMULT_ISR] || p[B2E_KMULT_SYNCH_RAD]))
     rad_coef = isr_coef = 0;
   radblock = rad_coef || isr_coef;
   itop = np - 1;
@@ -697,6 +706,8 @@ static long kmult_track(double **c, long np, const b2e_element *e, double Po, do
   if (e->type == B2E_KQUAD && p[B2E_KMULT_EDGE2_EFFECTS] > 0)
     qf_track(c, np, p[B2E_KMULT_K], p + B2E_KMULT_I0M, p + B2E_KMULT_I0P, 1, (int)p[B2E_KMULT_EDGE2_EFFECTS],
              (int)p[B2E_KMULT_EDGE2_LINEAR], p[B2E_KMULT_EDGE2_NONLINEAR_FACTOR]);
+  if (doEndDrift)
+    exact_drift(c, np, lEnd);
   if (dx || dy || dz || tilt) {
     if (tilt)
       rotate_beam(c, np, -tilt);

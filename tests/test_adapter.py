@@ -109,7 +109,6 @@ def test_adapter_declines_what_the_engine_cannot_take(adapter):
     cases = [
         ("D:DRIF L=0.5;S:SEXT L=0.2 K2=3", "SEXT"),
         ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 PITCH=0.001 MALIGN_METHOD=1", "MALIGN_METHOD"),
-        ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 LEFFECTIVE=0.25", "LEFFECTIVE"),
         ("D:DRIF L=0.5;Q:KQUAD L=0.3 K1=1.0 RADIAL=1", "RADIAL"),
         ("B:CSBEND L=1 ANGLE=0.1 FINT1=0.3", "FINT1"),
         ("B:CSRCSBEND L=0.5 ANGLE=0.05 BINS=100 OUTPUT_FILE=wake.sdds", "OUTPUT_FILE"),

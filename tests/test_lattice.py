@@ -48,7 +48,7 @@ def test_unsupported_inputs_fail_loudly():
     with pytest.raises(LatticeError):
         Element("W", "WIGGLER", {})
     with pytest.raises(LatticeError):
-        Element("Q", "KQUAD", {"L": 0.3, "LEFFECTIVE": 0.25})
+        Element("Q", "KQUAD", {"L": 0.3, "RADIAL": 1})
     with pytest.raises(LatticeError):
         parse_lte("A: DRIF, L=1\nL1: LINE=(A, B)\nUSE, L1\n")
 

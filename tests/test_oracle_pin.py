@@ -600,14 +600,17 @@ def _ring_with_quad_fringes():
     """Quadrupoles with fringe fields (quadFringe, fringe.c:24-175): linear
     (EDGE_EFFECTS 1) and linear + third order (2) with fringe integrals, one
     without the linear part, one with a nonlinear factor, one with the
-    entrance only, one with a negative (off) value."""
+    entrance only, one with a negative (off) value; and effective lengths
+    (LEFFECTIVE: exact end drifts, multipole.c:766-770, :1028-1030), one
+    radiating."""
     from elegant_b200 import Element, Lattice
     fi = {"I0P": 0.02, "I1P": 1e-3, "I2P": 2e-5, "I3P": 1e-6, "LAMBDA2P": 3e-6,
           "I0M": 0.025, "I1M": -1e-3, "I2M": 1e-5, "I3M": -2e-6, "LAMBDA2M": 1e-6}
     variants = [dict(fi, EDGE1_EFFECTS=1, EDGE2_EFFECTS=1), dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2),
                 dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, EDGE1_LINEAR=0, EDGE2_LINEAR=0),
                 dict(fi, EDGE1_EFFECTS=2, EDGE2_EFFECTS=2, EDGE2_NONLINEAR_FACTOR=0.5, DX=1e-4, TILT=0.01),
-                {"EDGE1_EFFECTS": 2}, {"EDGE1_EFFECTS": -1, "EDGE2_EFFECTS": 2}]
+                {"EDGE1_EFFECTS": 2, "LEFFECTIVE": 0.26}, {"EDGE1_EFFECTS": -1, "EDGE2_EFFECTS": 2},
+                {"LEFFECTIVE": 0.27, "SYNCH_RAD": 1}]
     els, k = [], 0
     for e in w.fodo_ring().elements:
         if e.type == "KQUAD":
