@@ -69,7 +69,7 @@ static const b2e_param_map map_ksext[] = {KMULT_COMMON,
       {"N_KICKS", B2E_BEND_N_SLICES}, {"INTEGRATION_ORDER", B2E_BEND_INTEGRATION_ORDER},                         \
       {"EDGE1_EFFECTS", B2E_BEND_EDGE1_EFFECTS}, {"EDGE2_EFFECTS", B2E_BEND_EDGE2_EFFECTS},                        \
       {"EDGE_ORDER", B2E_BEND_EDGE_ORDER}, {"K1", B2E_BEND_K1}, {"K2", B2E_BEND_K2},                        \
-      {"NONLINEAR", B2E_BEND_NONLINEAR}, {"XKICK", B2E_BEND_XKICK}
+      {"NONLINEAR", B2E_BEND_NONLINEAR}, {"XKICK", B2E_BEND_XKICK}, {"YKICK", B2E_BEND_YKICK}
 static const b2e_param_map map_csbend[] = {
     BEND_COMMON, {"SYNCH_RAD", B2E_BEND_SYNCH_RAD}, {"ISR", B2E_BEND_ISR}, {"ISR1PART", B2E_BEND_ISR1PART}, END_MAP};
 static const b2e_param_map map_csrcsbend[] = {BEND_COMMON,

@@ -489,10 +489,11 @@ __device__ __forceinline__ int bend_drift(double &X, double &QX, double &Y, doub
  * form of csbend.c:101-150, normal terms, expansion order 4): the sums over
  * x^i y^j in the reference's order, i outer, each term (F*x^i)*y^j with the
  * powers as repeated products.  F: the 15 coefficients of bend_field_terms. */
-__device__ __forceinline__ void bend_fields(double x, double y, const double *F, double &Fx, double &Fy) {
+__device__ __forceinline__ void bend_fields(double x, double y, const double *F, double fx0, double &Fx,
+                                            double &Fy) {
   const double y2 = y * y, y3 = y2 * y, y4 = y3 * y;
   const double x2 = x * x, x3 = x2 * x, x4 = x3 * x;
-  double sx = 0, sy = 0;
+  double sx = fx0, sy = 0;
   sx = sx + F[0] * y;
   sx = sx + F[1] * y3;
   sy = sy + F[6];
@@ -523,7 +524,7 @@ __device__ __forceinline__ void bend_kick(double X, double Y, double &QX, double
   double Fx = 0, Fy = 1;
   if (RAD && (e.flags & EF_FIELD)) {
     /* QX += -ds*(1+X/rho0)*Fy/rho_actual; QY += ds*(1+X/rho0)*Fx/rho_actual */
-    bend_fields(X, Y, rs.rc + RB_FIELD0, Fx, Fy);
+    bend_fields(X, Y, rs.rc + RB_FIELD0, (e.flags & EF_SKEW_KICK) ? rs.rc[RB_SKEW0] : 0.0, Fx, Fy);
     QX = QX + div_rn_recip((((-ds) * (1 + x_rho0)) * Fy), rho_actual, c[CB_INV_RHO_ACTUAL]);
     QY = QY + div_rn_recip(((ds * (1 + x_rho0)) * Fx), rho_actual, c[CB_INV_RHO_ACTUAL]);
   } else {
@@ -611,7 +612,7 @@ __device__ __forceinline__ double bend_edge_radiation(double x, double y, double
                                                       unsigned flags) {
   double Fx = 0, Fy = 1;
   if (flags & EF_FIELD)
-    bend_fields(x, y, rc + RB_FIELD0, Fx, Fy);
+    bend_fields(x, y, rc + RB_FIELD0, (flags & EF_SKEW_KICK) ? rc[RB_SKEW0] : 0.0, Fx, Fy);
   const double a = 1 + x / c[CB_RHO0];
   const double dp_prime = ((-rc[RB_RAD]) * (Fx * Fx + Fy * Fy)) * ((1 + dp) * (1 + dp)) *
                           sqrt((a * a + xp * xp) + yp * yp);

@@ -59,6 +59,7 @@ enum {
 #define EF_QFRINGE1 0x20000     /* KQUAD: entrance fringe (quadFringe; matrices in the DevRad table) */
 #define EF_QFRINGE2 0x40000     /* KQUAD: exit fringe */
 #define EF_END_DRIFT 0x80000    /* KQUAD with LEFFECTIVE: exact end drifts (KM_LEND) */
+#define EF_SKEW_KICK 0x100000   /* CSBEND with YKICK: the skew dipole term RB_SKEW0 in Fx */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */
@@ -144,6 +145,7 @@ typedef struct {
 #define RB_INV_RHO0 3   /* 1. / rho0 (:1605) */
 #define RB_FIELD0 12    /* CSBEND with K1/K2: the 15 field-expansion coefficients the
                          * field sums use, 12..26 (bend_fields has the order) */
+#define RB_SKEW0 27     /* CSBEND: c0 = YKICK/angle, the only skew coefficient (Fx at x^0 y^0) */
 #define RB_EXTRA0 28    /* the bend's BendExtra constants, 28..35 */
 
 /* RFCA constant slots */

@@ -474,9 +474,10 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     return "CSBEND N_SLICES must be >= 1";
   /* the expansion runs when any b[] is nonzero (hasNormal, csbend.c:205-210),
    * b0 = XKICK/ANGLE included */
-  const bool fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0;
+  const bool fields =
+      p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0 || p[B2E_BEND_YKICK] != 0;
   if (fields && el.type == B2E_CSRCSBEND)
-    return "CSRCSBEND with K1/K2/XKICK field terms is not supported by this engine";
+    return "CSRCSBEND with K1/K2/XKICK/YKICK field terms is not supported by this engine";
   if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
     return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
   /* csbend.c:933-950: negative angle folded into a PI tilt */
@@ -616,6 +617,13 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
         b1 *= -1;
       bend_field_terms(r.c + RB_FIELD0, p[B2E_BEND_XKICK] / p[B2E_BEND_ANGLE], b1, b2, h,
                        p[B2E_BEND_NONLINEAR] != 0);
+      /* c0 = YKICK/angle (:868): with it the reference sums every (i, j) of
+       * the expansion (hasSkew, csbend.c:124-135); the other skew entries are
+       * zero, so the sums are the normal ones with c0 first in Fx */
+      if (p[B2E_BEND_YKICK] != 0) {
+        r.c[RB_SKEW0] = p[B2E_BEND_YKICK] / p[B2E_BEND_ANGLE];
+        d.flags |= EF_SKEW_KICK;
+      }
       d.flags |= EF_FIELD;
     }
     d.flags |= EF_RADBLOCK;

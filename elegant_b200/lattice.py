@@ -43,7 +43,7 @@ _KMULT = {"L": 0, "TILT": 2, "DX": 3, "DY": 4, "DZ": 5, "FSE": 6, "N_KICKS": 7, 
 _BEND = {"L": 0, "ANGLE": 1, "E1": 2, "E2": 3, "TILT": 4, "ETILT": 5, "DX": 6, "DY": 7, "DZ": 8, "FSE": 9,
          "HGAP": 10, "FINT": 11, "N_SLICES": 12, "N_KICKS": 12, "INTEGRATION_ORDER": 13, "EDGE1_EFFECTS": 14,
          "EDGE2_EFFECTS": 15, "EDGE_ORDER": 16, "K1": 17, "K2": 18, "NONLINEAR": 19, "SYNCH_RAD": 35, "ISR": 36,
-         "ISR1PART": 37, "XKICK": 38}
+         "ISR1PART": 37, "XKICK": 38, "YKICK": 39}
 _CSRBEND = dict(_BEND, BINS=20, BIN_RANGE_FACTOR=21, SG_HALFWIDTH=22, SG_ORDER=23, SGDERIV_HALFWIDTH=24,
                 SGDERIV_ORDER=25, TRAPAZOID_INTEGRATION=26, STEADY_STATE=27, CSR=28, CLIP_NEGATIVE_BINS=29, IGF=30,
                 LOW_FREQUENCY_CUTOFF0=31, LOW_FREQUENCY_CUTOFF1=32, HIGH_FREQUENCY_CUTOFF0=33,

@@ -157,6 +157,7 @@ extern "C" {
 #define B2E_BEND_ISR 36
 #define B2E_BEND_ISR1PART 37
 #define B2E_BEND_XKICK 38 /* CSBEND bend-plane steering: the field term b0 = XKICK/ANGLE (csbend.c:867) */
+#define B2E_BEND_YKICK 39 /* CSBEND non-bend-plane steering: the skew term c0 = YKICK/ANGLE (csbend.c:868) */
 /* RFCA (rfca_param, track_data.c:576) */
 #define B2E_RFCA_L 0
 #define B2E_RFCA_VOLT 1

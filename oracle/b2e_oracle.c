@@ -724,7 +724,8 @@ typedef struct {
   double rad_coef, isr;
   int64_t id;
   int pass, elem;
-  int fields;                /* K1/K2 present: the expansion below is used */
+  int fields;                /* K1/K2/XKICK/YKICK present: the expansion below is used */
+  int skew;                  /* YKICK: Fx_xy[0][0] = c0, every (i, j) summed (hasSkew) */
   double Fx_xy[5][5], Fy_xy[5][5];
 } BendRad;
 
@@ -772,6 +773,19 @@ static void bend_fields_at(const BendRad *br, double x, double y, double *Fx, do
   yp[0] = 1;
   for (i = 1; i < 5; i++)
     yp[i] = yp[i - 1] * y;
+  if (br->skew) {
+    /* csbend.c:124-135: every j */
+    for (i = 0; i < 5; i++) {
+      for (j = 0; j < 5 - i; j++) {
+        sumFx += br->Fx_xy[i][j] * xt * yp[j];
+        sumFy += br->Fy_xy[i][j] * xt * yp[j];
+      }
+      xt *= x;
+    }
+    *Fx = sumFx;
+    *Fy = sumFy;
+    return;
+  }
   for (i = 0; i < 5; i++) {
     for (j = 1; j < 5 - i; j += 2)
       sumFx += br->Fx_xy[i][j] * xt * yp[j];
@@ -1042,7 +1056,8 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
   br.elem = idx;
   /* b[] of the field expansion (csbend.c:824-882): K*rho0 with the signed
    * angle, the FSE ratios, odd terms negated with a negative angle */
-  br.fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0;
+  br.fields = p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0 || p[B2E_BEND_YKICK] != 0;
+  br.skew = p[B2E_BEND_YKICK] != 0;
   if (br.fields) {
     double b[5] = {0, 0, 0, 0, 0}, rs = length / p[B2E_BEND_ANGLE];
     b[1] = p[B2E_BEND_K1] * rs;
@@ -1055,6 +1070,7 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
       b[3] *= -1;
     }
     bend_field_table(&br, b, h, p[B2E_BEND_NONLINEAR] != 0);
+    br.Fx_xy[0][0] = p[B2E_BEND_YKICK] / p[B2E_BEND_ANGLE]; /* c[0], csbend.c:227, :868 */
   }
   itop = np - 1;
   for (ip = 0; ip <= itop; ip++) {

@@ -566,10 +566,13 @@ def test_fiducial_mode_first_is_rejected():
 
 
 def _ring_with_bend_steering(negative=False):
-    """Bends with XKICK (the field term b0 = XKICK/ANGLE, csbend.c:867), alone
-    or with K1; every other bend folded to a negative angle when asked."""
+    """Bends with XKICK (the field term b0 = XKICK/ANGLE, csbend.c:867) and
+    YKICK (the skew term c0 = YKICK/ANGLE, :868, which makes the reference
+    sum every term of the expansion), alone or with K1/K2; every other bend
+    folded to a negative angle when asked."""
     from elegant_b200 import Element, Lattice
-    errs = [{"XKICK": 2e-4}, {"XKICK": -1e-4, "K1": 0.1}, {}, {"XKICK": 5e-5, "NONLINEAR": 0}]
+    errs = [{"XKICK": 2e-4}, {"XKICK": -1e-4, "K1": 0.1}, {"YKICK": 1.5e-4}, {"XKICK": 5e-5, "NONLINEAR": 0},
+            {"YKICK": -1e-4, "K2": 0.5}, {}]
     els, k = [], 0
     for e in w.fodo_ring().elements:
         if e.type == "CSBEND":
