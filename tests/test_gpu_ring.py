@@ -579,15 +579,17 @@ def test_ring_fiducial_pmaximum_without_a_particle_is_an_error():
 
 @pytest.mark.parametrize("negative", [False, True])
 def test_ring_with_bend_steering(ref_b2e, negative):
-    """CSBEND XKICK (the expansion's b0 = XKICK/ANGLE, csbend.c:867, in the
-    field sums of the kick), alone and with K1, with negative angles: 60
-    turns with losses, bit-identical to the reference."""
+    """CSBEND XKICK and YKICK (the expansion's b0 = XKICK/ANGLE and c0 =
+    YKICK/ANGLE, csbend.c:867-868, in the field sums of the kick), alone and
+    with K1/K2, with negative angles: 30 turns with losses, bit-identical to
+    the reference."""
     from test_oracle_pin import _ring_with_bend_steering
     lat = _ring_with_bend_steering(negative)
     beam = Beam(np.concatenate([w.ring_beam(150, seed=81).coords, _lossy_beam(150, seed=82).coords]),
                 np.arange(1, 301))
-    res = gpu_track(lat, beam, w.ring_p_central(), 60)
-    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 60)
+    # 30 turns: the uncorrected vertical kicks drive every particle out by turn 40
+    res = gpu_track(lat, beam, w.ring_p_central(), 30)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 30)
     assert 0 < nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
