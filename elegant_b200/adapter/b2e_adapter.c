@@ -89,14 +89,13 @@ static const b2e_param_map map_csrcsbend[] = {BEND_COMMON,
                                               {"HIGH_FREQUENCY_CUTOFF0", B2E_BEND_HIGH_FREQUENCY_CUTOFF0},
                                               {"HIGH_FREQUENCY_CUTOFF1", B2E_BEND_HIGH_FREQUENCY_CUTOFF1},
                                               END_MAP};
-/* PHASE_REFERENCE links cavities to one phase; the engine fiducialises each
- * cavity on its own, which is what a reference number no other cavity in
- * the line shares gives (checked in b2e_adapter_track). */
+/* PHASE_REFERENCE links cavities to one phase: the engine gives the later
+ * cavities of a group the first one's fiducial phase, as elegant does. */
 static const b2e_param_map map_rfca[] = {{"L", B2E_RFCA_L},         {"VOLT", B2E_RFCA_VOLT},
                                          {"PHASE", B2E_RFCA_PHASE}, {"FREQ", B2E_RFCA_FREQ},
                                          {"DX", B2E_RFCA_DX},       {"DY", B2E_RFCA_DY},
                                          {"T_REFERENCE", B2E_RFCA_T_REFERENCE}, {"N_KICKS", B2E_RFCA_N_KICKS},
-                                         {"PHASE_REFERENCE", -1},
+                                         {"PHASE_REFERENCE", B2E_RFCA_PHASE_REFERENCE},
                                          END_MAP};
 static const b2e_param_map map_maxamp[] = {{"X_MAX", B2E_MAXAMP_X_MAX},
                                            {"Y_MAX", B2E_MAXAMP_Y_MAX},
@@ -239,7 +238,7 @@ void b2e_adapter_release(void) {
 long b2e_adapter_track(double **coord, long np, ELEMENT_LIST *first, double P_central, long n_passes,
                        long default_order, double *effort_out, char *why, long why_len) {
   ELEMENT_LIST *eptr;
-  long n = 0, i, j, rf_refs[64], n_rf = 0;
+  long n = 0, i, j;
   b2e_element *el;
   b2e_run_options opt;
   double *cols[6] = {NULL, NULL, NULL, NULL, NULL, NULL}, effort = 0, *rows = NULL;
@@ -258,16 +257,6 @@ long b2e_adapter_track(double **coord, long np, ELEMENT_LIST *first, double P_ce
     if (eptr->type == T_WATCH && !((WATCH *)eptr->p_elem)->disable) {
       say(why, why_len, "%s: WATCH output is written by elegant%s", eptr->name, "");
       return -1;
-    }
-    if (eptr->type == T_RFCA) {
-      long ref = ((RFCA *)eptr->p_elem)->phase_reference;
-      for (j = 0; j < n_rf && ref; j++)
-        if (rf_refs[j] == ref) {
-          say(why, why_len, "%s: cavities share PHASE_REFERENCE%s", eptr->name, "");
-          return -1;
-        }
-      if (n_rf < 64)
-        rf_refs[n_rf++] = ref;
     }
   }
   el = (b2e_element *)calloc(n ? n : 1, sizeof(*el));

@@ -164,6 +164,7 @@ typedef struct {
 #define RF_DRIFT_ONLY 12 /* VOLT = 0: an exact drift over L (nothing for L = 0) */
 #define RF_FID_MODE 13  /* B2E_FIDUCIAL_* */
 #define RF_L_TOTAL 14   /* L, for the light fiducial's zEnd - L */
+#define RF_LEADER 15    /* RF state slot of the first cavity with the same PHASE_REFERENCE, -1: none */
 
 /* WATCH constant slots */
 #define WA_START 0      /* first pass recorded */
@@ -213,7 +214,7 @@ typedef struct {
 
 /* Per RFCA per instance: fiducial time and phase (phase_reference.c state). */
 typedef struct {
-  double t0;      /* -phase_fiducial/omega */
+  double phase_fiducial; /* -omega*t0 of the fiducial time (the phase reference other cavities may share) */
   double phase;   /* phase_fiducial + PHASE*PI/180 */
   int32_t set, pad;
 } DevRfState;

@@ -3,6 +3,7 @@
  */
 #include <math.h>
 #include <string.h>
+#include <map>
 #include <string>
 #include "b2e_lattice.h"
 #include "b2e_rng.h"
@@ -710,6 +711,7 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
     memset(&r, 0, sizeof(r));
   int last_ap = -1;
   double z = 0;
+  std::map<long, int> phase_groups; /* PHASE_REFERENCE -> RF state slot of its first cavity */
   for (int i = 0; i < n; i++) {
     DevElem &d = out.elems[i];
     memset(&d, 0, sizeof(d));
@@ -749,6 +751,14 @@ std::string compile_lattice(const b2e_element *el, int n, const b2e_run_options 
     }
     case B2E_RFCA:
       err = compile_rfca(el[i], out.n_rf, d);
+      d.c[RF_LEADER] = -1;
+      if (const long ref = (long)p[B2E_RFCA_PHASE_REFERENCE]) {
+        auto it = phase_groups.find(ref);
+        if (it != phase_groups.end())
+          d.c[RF_LEADER] = it->second;
+        else
+          phase_groups[ref] = out.n_rf;
+      }
       out.rf_elements.push_back(i);
       out.n_rf++;
       z += p[B2E_RFCA_L];

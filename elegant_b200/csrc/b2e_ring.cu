@@ -332,6 +332,16 @@ __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, 
   const double sOffset = e.c[RF_SOFFSET];
   const int slot = (int)e.c[RF_SLOT];
   DevRfState &rs = rf[(size_t)inst * n_rf + slot];
+  const int leader = (int)e.c[RF_LEADER];
+  if (leader >= 0) {
+    /* a later cavity of a PHASE_REFERENCE group: the group's phase
+     * (REF_PHASE_RETURNED, simple_rfca.c:419-421) plus its own PHASE */
+    const DevRfState &ls = rf[(size_t)inst * n_rf + leader];
+    rs.phase_fiducial = ls.phase_fiducial;
+    rs.phase = ls.phase_fiducial + e.c[RF_PHASE_DEG_RAD];
+    rs.set = ls.set;
+    return;
+  }
   double tsum = 0, error = 0;
   int64_t nsum = 0;
   const int64_t first = inst_offsets[inst], end = inst_offsets[inst + 1];
@@ -386,7 +396,7 @@ __global__ void rf_fiducial_kernel(DevParticles P, const int64_t *inst_offsets, 
     const double omega = e.c[RF_OMEGA];
     double t0 = tsum / nsum;
     double phase_fiducial = -omega * t0;
-    rs.t0 = -phase_fiducial / omega;
+    rs.phase_fiducial = phase_fiducial;
     rs.phase = phase_fiducial + e.c[RF_PHASE_DEG_RAD];
     rs.set = 1;
   } else {

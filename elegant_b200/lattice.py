@@ -60,7 +60,7 @@ SLOTS = {
     nat.CSBEND: _BEND,
     nat.CSRCSBEND: _CSRBEND,
     nat.RFCA: {"L": 0, "VOLT": 1, "PHASE": 2, "FREQ": 3, "DX": 4, "DY": 5, "T_REFERENCE": 6, "N_KICKS": 7,
-               "FIDUCIAL": 8},
+               "FIDUCIAL": 8, "PHASE_REFERENCE": 9},
     nat.MAXAMP: {"X_MAX": 0, "Y_MAX": 1, "ELLIPTICAL": 2, "EXPONENT": 3, "YEXPONENT": 4},
     nat.MARK: {},
     nat.CHARGE: {"TOTAL": 0, "PER_PARTICLE": 1},

@@ -168,6 +168,8 @@ extern "C" {
 #define B2E_RFCA_T_REFERENCE 6
 #define B2E_RFCA_N_KICKS 7 /* with L > 0: 0 = matrix method, else drift-kick-drift sections (simple_rfca.c:403-408) */
 #define B2E_RFCA_FIDUCIAL 8 /* FIDUCIAL mode (simple_rfca.c:22-27, :62-257): B2E_FIDUCIAL_* */
+#define B2E_RFCA_PHASE_REFERENCE 9 /* nonzero: cavities with the same number share the first one's fiducial
+                                    * phase (get/set_phase_reference, simple_rfca.c:410-470) */
 #define B2E_FIDUCIAL_TMEAN 0    /* mean arrival time, Kahan sum (the default) */
 #define B2E_FIDUCIAL_LIGHT 1    /* (zEnd - L + L/2/nKicks)/c */
 #define B2E_FIDUCIAL_PMAXIMUM 2 /* arrival time of the highest-momentum particle */

@@ -2091,6 +2091,20 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
   MaxAmp ma;
   CsrWake cw;
   RfState *rf = calloc(n_el ? n_el : 1, sizeof(RfState));
+  /* cavities sharing a nonzero PHASE_REFERENCE use the first one's state
+   * (get_phase_reference / set_phase_reference, simple_rfca.c:410-470) */
+  int *rf_of = malloc(sizeof(int) * (n_el ? n_el : 1));
+  for (k = 0; k < n_el; k++) {
+    rf_of[k] = k;
+    if (el[k].type == B2E_RFCA && el[k].p[B2E_RFCA_PHASE_REFERENCE] != 0) {
+      int j;
+      for (j = 0; j < k; j++)
+        if (el[j].type == B2E_RFCA && el[j].p[B2E_RFCA_PHASE_REFERENCE] == el[k].p[B2E_RFCA_PHASE_REFERENCE]) {
+          rf_of[k] = j;
+          break;
+        }
+    }
+  }
   memset(&ma, 0, sizeof(ma));
   memset(&cw, 0, sizeof(cw));
   cw.phiLast = -1;
@@ -2147,7 +2161,7 @@ long b2e_oracle_track_csr(const b2e_element *el, int n_el, double p_central, int
           nLeft = csbend_track(c, nToTrack, e, k, el, n_el, p_central, last_z, &ma, pass);
           break;
         case B2E_RFCA:
-          nLeft = rfca_track(c, nToTrack, e, &rf[k], p_central, z);
+          nLeft = rfca_track(c, nToTrack, e, &rf[rf_of[k]], p_central, z);
           if (nLeft < 0) {
             nToTrack = -1; /* no fiducial particle (FIDUCIAL=pmaximum): the reference stops */
             goto finish;
@@ -2206,6 +2220,7 @@ finish:
   free(cw.wakes);
   free(cw.dGamma);
   free(rf);
+  free(rf_of);
   free(c);
   return nToTrack;
 }

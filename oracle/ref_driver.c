@@ -384,6 +384,7 @@ long b2e_ref_track(const char *lattice, double p_central, double *rows_in, long 
   wake_cap = wake_capacity;
   wake_count = 0;
   last_fiducial_t0 = -1;
+  delete_phase_references(); /* each run starts as a new elegant run: no phase reference set */
 
   if (setjmp(b2e_ref_trap)) {
     b2e_ref_trap_armed = 0;

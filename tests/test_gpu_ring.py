@@ -609,3 +609,18 @@ def test_ring_with_quad_fringes(ref_b2e):
     assert 0 < nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+def test_ring_with_linked_cavities(ref_b2e):
+    """RFCA PHASE_REFERENCE groups (simple_rfca.c:410-470): later cavities of
+    a group take the first one's fiducial phase; 40 turns with losses,
+    bit-identical to the reference, and per-instance ensembles alike."""
+    from test_oracle_pin import _ring_with_linked_cavities
+    lat = _ring_with_linked_cavities()
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=101).coords, _lossy_beam(150, seed=102).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 40)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 40)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

@@ -634,3 +634,36 @@ def test_port_reproduces_reference_quad_fringes(math):
     assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
     r0, n0, _, _ = RefOracle(math).track(w.fodo_ring(), beam.coords, beam.ids, P0, 20)
     assert not np.array_equal(r0[:min(n0, n1), :4], r1[:min(n0, n1), :4])
+
+
+def _ring_with_linked_cavities():
+    """Three extra cavities: two sharing PHASE_REFERENCE 7 with the ring's own
+    cavity (each with its own PHASE and one at another frequency), one
+    alone; the group's later cavities take the first one's fiducial phase
+    (simple_rfca.c:410-470)."""
+    from elegant_b200 import Element, Lattice
+    base = list(w.fodo_ring().elements)
+    rf = next(e for e in base if e.type == "RFCA")
+    els = [e for e in base if e.type != "RFCA"]
+    els.insert(10, Element("RFA", "RFCA", dict(rf.params, VOLT=3e5, PHASE_REFERENCE=7)))
+    els.insert(30, Element("RFB", "RFCA", dict(rf.params, VOLT=2e5, PHASE=170.0, FREQ=rf.params["FREQ"] * 2,
+                                               PHASE_REFERENCE=7)))
+    els.insert(45, Element("RFC", "RFCA", dict(rf.params, VOLT=2e5, PHASE=175.0, PHASE_REFERENCE=9)))
+    els.append(Element("RF", "RFCA", dict(rf.params, PHASE=178.0, PHASE_REFERENCE=7)))
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_linked_cavities(math):
+    lat = _ring_with_linked_cavities()
+    beam = _mixed_beam(101)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
+    from elegant_b200 import Element, Lattice
+    unlinked = Lattice([Element(e.name, e.type, {k: v for k, v in e.params.items() if k != "PHASE_REFERENCE"})
+                        for e in lat.elements])
+    r0, n0, _, _ = RefOracle(math).track(unlinked, beam.coords, beam.ids, P0, 20)
+    assert not np.array_equal(r0[:min(n0, n1), :6], r1[:min(n0, n1), :6])
