@@ -318,7 +318,8 @@ def parse_lte(text: str, use: str | None = None, outputs: dict | None = None) ->
                     raise LatticeError(f"OUTPUT_FILE of {name}: pass outputs= to collect it (elegant_b200.ele)")
                 outputs[name] = v.strip().strip('"')
                 continue
-            if etype == "WATCH" and k.strip().upper() in ("FILENAME", "LABEL", "MODE"):
+            if (etype == "WATCH" and k.strip().upper() in ("FILENAME", "LABEL", "MODE")) or \
+                    (etype == "RFCA" and k.strip().upper() == "FIDUCIAL"):
                 params[k.strip().upper()] = v.strip().strip('"')
                 continue
             params[k.strip().upper()] = _value(v)

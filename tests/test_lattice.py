@@ -80,3 +80,20 @@ def test_maxamp_exponents_take_elegants_names():
     assert Element("MA", "MAXAMP", {}).slots()[3] == 2 and Element("MA", "MAXAMP", {}).slots()[4] == 0
     with pytest.raises(LatticeError):
         Element("MA", "MAXAMP", {"Y_EXPONENT": 6}).slots()
+
+
+def test_lte_parameters_of_the_wider_element_set():
+    """.lte text with the RFCA fiducial string and phase group, KQUAD
+    correctors, fringe integrals and effective length, CSBEND steering:
+    parsed into engine slots and written back unchanged."""
+    text = ('D: DRIF, L=1\nRF: RFCA, VOLT=1e6, FREQ=5e8, FIDUCIAL="light", PHASE_REFERENCE=3\n'
+            'Q: KQUAD, L=0.3, K1=1, HKICK=1e-4, EDGE1_EFFECTS=2, I0P=0.01, LEFFECTIVE=0.28, HSTEERING=1\n'
+            'B: CSBEND, L=1, ANGLE=0.1, XKICK=1e-4, YKICK=2e-5\nL1: LINE=(D,RF,Q,B)\nUSE, L1\n')
+    lat = parse_lte(text)
+    rf, q, b = lat.elements[1], lat.elements[2], lat.elements[3]
+    assert rf.params["FIDUCIAL"] == 1 and rf.slots()[9] == 3  # B2E_RFCA_FIDUCIAL, B2E_RFCA_PHASE_REFERENCE
+    # B2E_KMULT_HKICK, _EDGE1_EFFECTS, _LEFFECTIVE, _EDGE1_LINEAR (default 1); B2E_BEND_XKICK, _YKICK
+    assert q.slots()[15] == 1e-4 and q.slots()[21] == 2 and q.slots()[37] == 0.28 and q.slots()[23] == 1
+    assert b.slots()[38] == 1e-4 and b.slots()[39] == 2e-5
+    again = parse_lte(lat.to_lte())
+    assert [e.params for e in again.elements] == [e.params for e in lat.elements]
