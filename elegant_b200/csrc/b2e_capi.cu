@@ -273,7 +273,7 @@ static int upload_lattice_tables(b2e_ctx *ctx) {
 static bool any_radiation(const std::vector<DevElem> &elems) {
   for (const DevElem &d : elems)
     if (d.flags & (EF_SR | EF_ISR | EF_FIELD | EF_ETILT | EF_EDGE_ORDER2 | EF_STEERING | EF_QFRINGE1 | EF_QFRINGE2 | \
-                   EF_END_DRIFT))
+                   EF_END_DRIFT | EF_EDGE1_SIMPLE | EF_EDGE2_SIMPLE))
       return true;
   return false;
 }

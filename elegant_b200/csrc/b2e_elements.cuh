@@ -513,6 +513,22 @@ __device__ __forceinline__ void bend_fields(double x, double y, const double *F,
   Fy = sy;
 }
 
+/* EDGE_EFFECTS 3 (applySimpleDipoleEdgeKick, csbend.c:5639-5665; no kick
+ * limit, unexpanded Hamiltonian): the linear edge kick applied to the
+ * canonical momenta */
+__device__ __forceinline__ void bend_edge_simple(double &xp, double &yp, double x, double y, double dp,
+                                                 double rho, double tan_e, double e, double psi) {
+  double f = (1 + dp) / sqrt((1 + xp * xp) + yp * yp);
+  double qx = xp * f, qy = yp * f;
+  const double dqx = (tan_e / rho) * x;
+  const double dqy = (-b2e_tan(e - psi / (1 + dp)) / rho) * y;
+  qx = qx + dqx;
+  qy = qy + dqy;
+  f = 1 / sqrt(((1 + dp) * (1 + dp) - qx * qx) - qy * qy);
+  xp = qx * f;
+  yp = qy * f;
+}
+
 /* kick j of a slice (csbend.c:1591-1638) */
 template <bool RAD>
 __device__ __forceinline__ void bend_kick(double X, double Y, double &QX, double &QY, double &DPoP, const double *c,
@@ -666,9 +682,11 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE1) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    /* EF_EDGE_ORDER2 and EF_ETILT lattices run the RAD instantiation, which
-     * has the DevRad table with the BendExtra constants */
-    if (RAD && (e.flags & EF_EDGE_ORDER2)) {
+    /* EF_EDGE_ORDER2, EF_EDGE1_SIMPLE and EF_ETILT lattices run the RAD
+     * instantiation, which has the DevRad table with the BendExtra constants */
+    if (RAD && (e.flags & EF_EDGE1_SIMPLE)) {
+      bend_edge_simple(xp, yp, x, y, dp, c[CB_RHO_ACTUAL], c[CB_TAN_E1], c[CB_E1], c[CB_PSI1]);
+    } else if (RAD && (e.flags & EF_EDGE_ORDER2)) {
       const double *bx = rs.rc + RB_EXTRA0;
       bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI1] * (1 + dp), c[CB_TAN_E1], c[CB_E1], bx[BX_SEC2_E1],
                        bx[BX_EDGE_N], -1);
@@ -726,7 +744,9 @@ __device__ __forceinline__ int csbend(Part &p, const DevElem &e, const DevApertu
   if (e.flags & EF_EDGE2) {
     double delta_xp;
     rho = (1 + dp) * c[CB_RHO_ACTUAL];
-    if (RAD && (e.flags & EF_EDGE_ORDER2)) {
+    if (RAD && (e.flags & EF_EDGE2_SIMPLE)) {
+      bend_edge_simple(xp, yp, x, y, dp, c[CB_RHO_ACTUAL], c[CB_TAN_E2], c[CB_E2], c[CB_PSI2]);
+    } else if (RAD && (e.flags & EF_EDGE_ORDER2)) {
       const double *bx = rs.rc + RB_EXTRA0;
       bend_edge_order2(x, xp, y, yp, rho, c[CB_PSI2] * (1 + dp), c[CB_TAN_E2], c[CB_E2], bx[BX_SEC2_E2],
                        bx[BX_EDGE_N], 1);

@@ -60,6 +60,8 @@ enum {
 #define EF_QFRINGE2 0x40000     /* KQUAD: exit fringe */
 #define EF_END_DRIFT 0x80000    /* KQUAD with LEFFECTIVE: exact end drifts (KM_LEND) */
 #define EF_SKEW_KICK 0x100000   /* CSBEND with YKICK: the skew dipole term RB_SKEW0 in Fx */
+#define EF_EDGE1_SIMPLE 0x200000 /* CSBEND EDGE1_EFFECTS 3: applySimpleDipoleEdgeKick */
+#define EF_EDGE2_SIMPLE 0x400000 /* CSBEND EDGE2_EFFECTS 3 */
 
 /* KMULT constant slots */
 #define KM_ORDER 0       /* 1 quad, 2 sext */

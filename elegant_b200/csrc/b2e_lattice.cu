@@ -479,8 +479,12 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
       p[B2E_BEND_K1] != 0 || p[B2E_BEND_K2] != 0 || p[B2E_BEND_XKICK] != 0 || p[B2E_BEND_YKICK] != 0;
   if (fields && el.type == B2E_CSRCSBEND)
     return "CSRCSBEND with K1/K2/XKICK/YKICK field terms is not supported by this engine";
-  if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1))
-    return "CSBEND EDGE[12]_EFFECTS other than 0 or 1 is not supported by this engine";
+  /* method 1 (K. L. Brown's edge matrix, to first or second order) and, on
+   * CSBEND, method 3 (applySimpleDipoleEdgeKick, csbend.c:5639-5665) */
+  const bool simple1 = edge1 && p[B2E_BEND_EDGE1_EFFECTS] == 3 && el.type == B2E_CSBEND;
+  const bool simple2 = edge2 && p[B2E_BEND_EDGE2_EFFECTS] == 3 && el.type == B2E_CSBEND;
+  if ((edge1 && p[B2E_BEND_EDGE1_EFFECTS] != 1 && !simple1) || (edge2 && p[B2E_BEND_EDGE2_EFFECTS] != 1 && !simple2))
+    return "CSBEND EDGE[12]_EFFECTS other than 0, 1 or 3 (3 on CSBEND only) is not supported by this engine";
   /* csbend.c:933-950: negative angle folded into a PI tilt */
   if (p[B2E_BEND_ANGLE] < 0) {
     angle = -p[B2E_BEND_ANGLE];
@@ -569,6 +573,10 @@ static std::string compile_csbend(const b2e_element &el, bool edge1, bool edge2,
     d.flags |= EF_EDGE1;
   if (edge2)
     d.flags |= EF_EDGE2;
+  if (simple1)
+    d.flags |= EF_EDGE1_SIMPLE;
+  if (simple2)
+    d.flags |= EF_EDGE2_SIMPLE;
   if ((edge1 || edge2) && p[B2E_BEND_EDGE_ORDER] >= 2) {
     /* second-order edges (apply_edge_effects, csbend.c:4266-4307): the
      * per-element parts; b1 = K1*rho0 (csbend.c:825), sign-flipped with a

@@ -867,6 +867,21 @@ static int csbend_integrate(double *Qf, const double *Qi, double s, long n, doub
   return 1;
 }
 
+/* applySimpleDipoleEdgeKick (csbend.c:5639-5665), EDGE_EFFECTS 3, no kick
+ * limit, unexpanded Hamiltonian: the linear edge kick on the canonical
+ * momenta */
+static void simple_edge_kick(double *xp, double *yp, double x, double y, double delta, double rho, double ea,
+                             double psi) {
+  double f = (1 + delta) / sqrt(1 + SQR(*xp) + SQR(*yp)), qx = *xp * f, qy = *yp * f, dqx, dqy;
+  dqx = M_TAN(ea) / rho * x;
+  dqy = -M_TAN(ea - psi / (1 + delta)) / rho * y;
+  qx += dqx;
+  qy += dqy;
+  f = 1 / sqrt(SQR(1 + delta) - SQR(qx) - SQR(qy));
+  *xp = qx * f;
+  *yp = qy * f;
+}
+
 static int same_bend(const b2e_element *a, const b2e_element *b) {
   return a->type == b->type && strncmp(a->name, b->name, sizeof(a->name)) == 0;
 }
@@ -1086,7 +1101,9 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     yp = -coord[1] * st + coord[3] * ct;
     s = coord[4];
     dp = dp0 = coord[5];
-    if (edge1) {
+    if (edge1 && p[B2E_BEND_EDGE1_EFFECTS] == 3)
+      simple_edge_kick(&xp, &yp, x, y, dp, rho_actual, e1, psi1);
+    else if (edge1) {
       rho = (1 + dp) * rho_actual;
       if (p[B2E_BEND_EDGE_ORDER] >= 2)
         edge_order2(&x, &xp, &y, &yp, rho, n_index, e1, psi1 * (1 + dp), -1);
@@ -1145,7 +1162,9 @@ static long csbend_track(double **c, long np, const b2e_element *el, int idx, co
     y = Qf[2];
     yp = Qf[3];
     dp = Qf[5];
-    if (edge2) {
+    if (edge2 && p[B2E_BEND_EDGE2_EFFECTS] == 3)
+      simple_edge_kick(&xp, &yp, x, y, dp, rho_actual, e2, psi2);
+    else if (edge2) {
       rho = (1 + dp) * rho_actual;
       if (p[B2E_BEND_EDGE_ORDER] >= 2)
         edge_order2(&x, &xp, &y, &yp, rho, n_index, e2, psi2 * (1 + dp), 1);

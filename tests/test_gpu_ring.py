@@ -624,3 +624,17 @@ def test_ring_with_linked_cavities(ref_b2e):
     assert 0 < nl < 300
     assert_parity(res, rows, nl)
     assert res.effort == eff
+
+
+def test_ring_with_simple_edges(ref_b2e):
+    """CSBEND EDGE_EFFECTS 3 (applySimpleDipoleEdgeKick, csbend.c:5639-5665):
+    40 turns with losses, bit-identical to the reference."""
+    from test_oracle_pin import _ring_with_simple_edges
+    lat = _ring_with_simple_edges()
+    beam = Beam(np.concatenate([w.ring_beam(150, seed=111).coords, _lossy_beam(150, seed=112).coords]),
+                np.arange(1, 301))
+    res = gpu_track(lat, beam, w.ring_p_central(), 40)
+    rows, nl, eff, _ = ref_b2e.track(lat, beam.coords, beam.ids, w.ring_p_central(), 40)
+    assert 0 < nl < 300
+    assert_parity(res, rows, nl)
+    assert res.effort == eff

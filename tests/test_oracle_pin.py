@@ -667,3 +667,30 @@ def test_port_reproduces_reference_linked_cavities(math):
                         for e in lat.elements])
     r0, n0, _, _ = RefOracle(math).track(unlinked, beam.coords, beam.ids, P0, 20)
     assert not np.array_equal(r0[:min(n0, n1), :6], r1[:min(n0, n1), :6])
+
+
+def _ring_with_simple_edges():
+    """Bends with EDGE_EFFECTS 3 (applySimpleDipoleEdgeKick, csbend.c:5639-5665)
+    on one or both faces, with edge angles and a fringe gap, one radiating."""
+    from elegant_b200 import Element, Lattice
+    variants = [{"EDGE1_EFFECTS": 3, "EDGE2_EFFECTS": 3, "E1": 0.05, "E2": 0.03, "HGAP": 0.01},
+                {"EDGE1_EFFECTS": 3, "E1": -0.04}, {"EDGE2_EFFECTS": 3, "E2": 0.06, "HGAP": 0.02, "FINT": 0.4},
+                {"EDGE1_EFFECTS": 3, "EDGE2_EFFECTS": 3, "E1": 0.02, "E2": 0.02, "SYNCH_RAD": 1}]
+    els, k = [], 0
+    for e in w.fodo_ring().elements:
+        if e.type == "CSBEND":
+            e = Element(e.name + str(k), e.type, dict(e.params, **variants[k % len(variants)]))
+            k += 1
+        els.append(e)
+    return Lattice(els)
+
+
+@pytest.mark.parametrize("math", ["libm", "b2e"])
+def test_port_reproduces_reference_simple_edges(math):
+    lat = _ring_with_simple_edges()
+    beam = _mixed_beam(111)
+    r1, n1, e1, _ = RefOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    r2, n2, e2 = PortOracle(math).track(lat, beam.coords, beam.ids, P0, 20)
+    assert n1 == n2 and e1 == e2 and 0 < n1 < beam.n
+    assert np.array_equal(r1[:n1, :7], r2[:n2, :7])
+    assert np.array_equal(r1[:, 6:8], r2[:, 6:8])
